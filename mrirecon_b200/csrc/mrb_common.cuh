@@ -1,0 +1,105 @@
+// Shared helpers for the mrirecon_b200 CUDA library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/mrirecon_b200.h"
+
+namespace mrb {
+
+// ---------------------------------------------------------------------------
+// error reporting: every entry point returns a status and records a message
+// ---------------------------------------------------------------------------
+void set_error(const char* fmt, ...);
+int fail(int code, const char* fmt, ...);
+
+#define MRB_CUDA_TRY(expr)                                                          \
+  do {                                                                              \
+    cudaError_t _e = (expr);                                                        \
+    if (_e != cudaSuccess)                                                          \
+      return ::mrb::fail(MRB_ECUDA, "%s:%d %s: %s", __FILE__, __LINE__, #expr,     \
+                         cudaGetErrorString(_e));                                   \
+  } while (0)
+
+#define MRB_LAUNCH_CHECK() MRB_CUDA_TRY(cudaGetLastError())
+
+#define MRB_REQUIRE(cond, ...)                                                      \
+  do {                                                                              \
+    if (!(cond)) return ::mrb::fail(MRB_EINVAL, __VA_ARGS__);                       \
+  } while (0)
+
+inline int ceil_div_i(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+
+// Device buffer owned by a plan.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  int ensure(size_t n) {
+    if (n <= bytes) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    if (n == 0) return 0;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return fail(MRB_ENOMEM, "cudaMalloc(%zu) failed: %s", n, cudaGetErrorString(e));
+    }
+    bytes = n;
+    return 0;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// Kaiser-Bessel window as a polynomial in z = 1 - (2d/W)^2.
+// phi(d) = I0(beta*sqrt(z)) / I0(beta) = sum_k c_k z^k with
+// c_k = (beta^2/4)^k / (k!)^2 / I0(beta)  (power series of I0, A&S 9.6.10),
+// coefficients computed on the host in double precision.  z < 0 is clamped to
+// 0, as the reference clamps its argument (ptnufft.py:87-88).
+// ---------------------------------------------------------------------------
+constexpr int KB_MAX_TERMS = 32;
+
+struct KBPoly {
+  float c[KB_MAX_TERMS];
+  int n;          // number of terms
+  float inv_half_w2;  // (2/W)^2
+};
+
+__device__ __forceinline__ float kb_eval(const KBPoly& p, float d) {
+  float z = fmaxf(0.0f, 1.0f - d * d * p.inv_half_w2);
+  float acc = p.c[p.n - 1];
+#pragma unroll 4
+  for (int k = p.n - 2; k >= 0; --k) acc = fmaf(acc, z, p.c[k]);
+  return acc;
+}
+
+// Host: fill the polynomial for (W, beta).
+void kb_poly_init(KBPoly& p, int W, double beta);
+
+// Reference float32 arithmetic for grid coordinates (ptnufft.py:151-153):
+// u = w / float32(2pi) + 0.5 ; gx = u * G ; clamp(gx, 0, float32(G - 1e-6)).
+__device__ __forceinline__ float ref_grid_coord(float w, float Gf, float gmax) {
+  float u = __fadd_rn(__fdiv_rn(w, 6.28318548202514648f), 0.5f);
+  float g = __fmul_rn(u, Gf);
+  return fminf(fmaxf(g, 0.0f), gmax);
+}
+
+__device__ __forceinline__ int wrap_i(int n, int G) {
+  int r = n % G;
+  return r < 0 ? r + G : r;
+}
+
+}  // namespace mrb

@@ -1,0 +1,1045 @@
+// Kaiser-Bessel NUFFT for B200 (sm_100a): binning, forward interp, adjoint
+// spread, fused SENSE/deapodisation/pad and crop/coil-combine, cuFFT for the
+// dense oversampled transform.
+//
+// Conventions (corrected form of graspcg/nufft/backends/ptnufft.py):
+//   gx_d   = clamp((w_d / float32(2pi) + 0.5) * G_d, 0, float32(G_d - 1e-6))
+//            in float32, same operation order as ptnufft.py:151-153;
+//   nodes  n = floor(gx) + o, o in [-W/2+1, W/2], distance d = gx - n,
+//            weight phi(d) (KB, ptnufft.py:79-90 / :125), index n mod G;
+//   image pixel i sits at node i + G/2 - S//2 (centred coordinate i - S//2);
+//   fftshift o FFT o ifftshift is applied as (-1)^(sum n) on the input and
+//   (-1)^(sum k) * prod (-1)^(G_d/2) on the output of the unshifted FFT.
+//
+// Layouts: x (nb, 1, *S), maps (C, *S), y (nb, C, K), grid (nb, C, *G), all
+// complex64 row-major.  Frame be of an nb-batch uses trajectory frame
+// be / (nb / B) (graspcg/nufft/backends/torchkb.py:151-166).
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "mrb_common.cuh"
+
+using mrb::DevBuf;
+using mrb::KBPoly;
+
+struct mrb_plan {
+  int nd = 2;
+  int S[3] = {1, 1, 1};
+  int G[3] = {1, 1, 1};
+  int C = 1;
+  int B = 1;
+  int64_t K = 0;
+  int W = 4;
+  double osf = 2.0;
+  int ortho = 1;
+  float scale = 1.f;
+  float gsign = 1.f;
+  KBPoly kb{};
+  double beta = 0.0;
+  // options
+  int tile = 16;
+  int coils_per_item = 4;
+  int interp_mode = 0;
+  // state
+  bool have_points = false;
+  bool have_maps = false;
+  DevBuf gx;          // (B, nd, K) float
+  DevBuf entries;     // (n_entries) int32 sample index, sorted by (frame, tile)
+  DevBuf tile_start;  // (B * ntiles + 1) int32
+  DevBuf sorted_k;    // (B, K) int32 samples sorted by tile of their base node
+  int64_t n_entries = 0;
+  int64_t touched = 0;
+  int ntile_d[3] = {1, 1, 1};
+  int ntiles = 1;
+  DevBuf maps;        // (C, *S) float2
+  DevBuf invdeap;     // concatenated per-dim 1/Phi, S[0] + S[1] (+ S[2]) floats
+  DevBuf wfwd, wadj;  // (B, K) float
+  bool has_wfwd = false, has_wadj = false;
+  DevBuf grid;        // (nb, C, *G) float2
+  cufftHandle fft = 0;
+  int fft_batch = 0;
+  DevBuf tmp;         // scratch for set_points
+
+  int64_t gtot() const {
+    int64_t t = 1;
+    for (int d = 0; d < nd; ++d) t *= G[d];
+    return t;
+  }
+  int64_t stot() const {
+    int64_t t = 1;
+    for (int d = 0; d < nd; ++d) t *= S[d];
+    return t;
+  }
+};
+
+namespace {
+
+struct Geo {
+  int nd;
+  int S[3];
+  int G[3];
+  float Gf[3];
+  float gmax[3];
+  int off[3];        // G/2 - S//2
+  int C;
+  int B;
+  long long K;
+  long long gtot;
+  long long stot;
+};
+
+Geo make_geo(const mrb_plan* p) {
+  Geo g{};
+  g.nd = p->nd;
+  for (int d = 0; d < 3; ++d) {
+    g.S[d] = p->S[d];
+    g.G[d] = p->G[d];
+    g.Gf[d] = (float)p->G[d];
+    g.gmax[d] = (float)((double)p->G[d] - 1e-6);
+    g.off[d] = p->G[d] / 2 - p->S[d] / 2;
+  }
+  g.C = p->C;
+  g.B = p->B;
+  g.K = p->K;
+  g.gtot = p->gtot();
+  g.stot = p->stot();
+  return g;
+}
+
+__device__ __forceinline__ int frame_of(int be, int nb, int B) {
+  if (B == 1) return 0;
+  return be / (nb / B);
+}
+
+// ---------------------------------------------------------------------------
+// set-up kernels
+// ---------------------------------------------------------------------------
+__global__ void coords_kernel(const float* __restrict__ traj, float* __restrict__ gx, Geo g) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)g.B * g.nd * g.K;
+  if (i >= n) return;
+  int d = (int)((i / g.K) % g.nd);
+  gx[i] = mrb::ref_grid_coord(traj[i], g.Gf[d], g.gmax[d]);
+}
+
+constexpr int MAX_TOUCH = 4;   // W = 4 nodes per dim touch at most 4 tiles
+
+struct TileGeo {
+  int T;
+  int nt[3];
+  int ntiles;
+  int lo_off;   // W/2 - 1
+  int hi_off;   // W/2
+};
+
+// distinct tiles touched along one dim by nodes base-lo_off .. base+hi_off
+// (wrapped); up to 3 when a narrow partial last tile sits inside the span.
+__device__ __forceinline__ int dim_tiles(int base, int G, int T, int nt, int lo_off, int hi_off, int* ts) {
+  int n = 0;
+  for (int v = base - lo_off; v <= base + hi_off; ++v) {
+    int t = mrb::wrap_i(v, G) / T;
+    bool seen = false;
+    for (int j = 0; j < n; ++j) seen = seen || (ts[j] == t);
+    if (!seen) ts[n++] = t;
+  }
+  return n;
+}
+
+__global__ void entry_count_kernel(const float* __restrict__ gx, int* __restrict__ cnt, Geo g, TileGeo tg) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)g.B * g.K;
+  if (i >= n) return;
+  int b = (int)(i / g.K);
+  long long k = i - (long long)b * g.K;
+  int c = 1;
+  int ts[MAX_TOUCH];
+  for (int d = 0; d < g.nd; ++d) {
+    int base = (int)floorf(gx[((long long)b * g.nd + d) * g.K + k]);
+    c *= dim_tiles(base, g.G[d], tg.T, tg.nt[d], tg.lo_off, tg.hi_off, ts);
+  }
+  cnt[i] = c;
+}
+
+__global__ void entry_fill_kernel(const float* __restrict__ gx, const int* __restrict__ offs,
+                                  unsigned* __restrict__ keys, int* __restrict__ vals, Geo g, TileGeo tg) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)g.B * g.K;
+  if (i >= n) return;
+  int b = (int)(i / g.K);
+  int k = (int)(i - (long long)b * g.K);
+  int ts[3][MAX_TOUCH], nn[3];
+  for (int d = 0; d < 3; ++d) { ts[d][0] = 0; nn[d] = 1; }
+  for (int d = 0; d < g.nd; ++d) {
+    int base = (int)floorf(gx[((long long)b * g.nd + d) * g.K + k]);
+    nn[d] = dim_tiles(base, g.G[d], tg.T, tg.nt[d], tg.lo_off, tg.hi_off, ts[d]);
+  }
+  int o = offs[i];
+  for (int a0 = 0; a0 < nn[0]; ++a0)
+    for (int a1 = 0; a1 < nn[1]; ++a1)
+      for (int a2 = 0; a2 < nn[2]; ++a2) {
+        int t = ts[0][a0];
+        if (g.nd > 1) t = t * tg.nt[1] + ts[1][a1];
+        if (g.nd > 2) t = t * tg.nt[2] + ts[2][a2];
+        keys[o] = (unsigned)(b * tg.ntiles + t);
+        vals[o] = k;
+        ++o;
+      }
+}
+
+__global__ void tile_start_kernel(const unsigned* __restrict__ keys, long long n, int* __restrict__ start,
+                                  int nkeys) {
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  int key = (int)keys[e];
+  int prev = e ? (int)keys[e - 1] : -1;
+  for (int t = prev + 1; t <= key; ++t) start[t] = (int)e;
+  if (e == n - 1)
+    for (int t = key + 1; t <= nkeys; ++t) start[t] = (int)n;
+}
+
+__global__ void fill_int_kernel(int* p, long long n, int v) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+// touched-cell count (for roofline bookkeeping): marks cells in a bitmap
+__global__ void touch_kernel(const float* __restrict__ gx, unsigned* __restrict__ bits, Geo g, int W, int b) {
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= g.K) return;
+  int base[3] = {0, 0, 0};
+  for (int d = 0; d < g.nd; ++d) base[d] = (int)floorf(gx[((long long)b * g.nd + d) * g.K + k]);
+  int lo = W / 2 - 1;
+  int n2 = g.nd > 2 ? W : 1, n1 = g.nd > 1 ? W : 1;
+  for (int a = 0; a < W; ++a)
+    for (int c = 0; c < n1; ++c)
+      for (int e = 0; e < n2; ++e) {
+        long long idx = mrb::wrap_i(base[0] - lo + a, g.G[0]);
+        if (g.nd > 1) idx = idx * g.G[1] + mrb::wrap_i(base[1] - lo + c, g.G[1]);
+        if (g.nd > 2) idx = idx * g.G[2] + mrb::wrap_i(base[2] - lo + e, g.G[2]);
+        atomicOr(&bits[idx >> 5], 1u << (idx & 31));
+      }
+}
+
+__global__ void popc_kernel(const unsigned* __restrict__ bits, long long nwords,
+                            unsigned long long* __restrict__ out) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int c = 0;
+  if (i < nwords) c = __popc(bits[i]);
+  c = __reduce_add_sync(0xffffffffu, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, (unsigned long long)c);
+}
+
+__global__ void dcf_weight_kernel(const float* __restrict__ dcf, float* __restrict__ w, long long n, int sq) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float v = dcf[i];
+  w[i] = sq ? sqrtf(fmaxf(v, 0.f)) : v;
+}
+
+// ---------------------------------------------------------------------------
+// forward: SENSE * deapod * sign, zero-padded into the grid
+// ---------------------------------------------------------------------------
+template <int ND>
+__global__ void pre_fft_kernel(const float2* __restrict__ x, const float2* __restrict__ maps,
+                               const float* __restrict__ invdeap, float4* __restrict__ grid, Geo g, int nb,
+                               int coil_images) {
+  // one thread per pair of cells along the last dim
+  const int Gl = g.G[ND - 1];
+  const int half = Gl >> 1;
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long pairs_per_vol = g.gtot >> 1;
+  long long total = pairs_per_vol * g.C * nb;
+  if (i >= total) return;
+  long long vol = i / pairs_per_vol;          // be*C + c
+  long long r = i - vol * pairs_per_vol;
+  int c = (int)(vol % g.C);
+  int be = (int)(vol / g.C);
+  int nl = (int)(r % half) * 2;
+  long long rest = r / half;
+  int n[3] = {0, 0, 0};
+  n[ND - 1] = nl;
+  if (ND == 2) {
+    n[0] = (int)rest;
+  } else {
+    n[1] = (int)(rest % g.G[1]);
+    n[0] = (int)(rest / g.G[1]);
+  }
+  float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+  bool inside = true;
+  int ii[3];
+  float dap = 1.f;
+  int dap_off = 0;
+  int parity = 0;
+  for (int d = 0; d < ND - 1; ++d) {
+    ii[d] = n[d] - g.off[d];
+    inside = inside && (unsigned)ii[d] < (unsigned)g.S[d];
+    if (inside) dap *= invdeap[dap_off + ii[d]];
+    dap_off += g.S[d];
+    parity += n[d];
+  }
+  if (inside) {
+    long long base = 0;
+    for (int d = 0; d < ND - 1; ++d) base = base * g.S[d] + ii[d];
+    const int Sl = g.S[ND - 1];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int il = nl + h - g.off[ND - 1];
+      if ((unsigned)il < (unsigned)Sl) {
+        long long pix = base * Sl + il;
+        float2 xv, mv;
+        if (coil_images) {
+          xv = x[((long long)be * g.C + c) * g.stot + pix];
+          mv = make_float2(1.f, 0.f);
+        } else {
+          xv = x[(long long)be * g.stot + pix];
+          mv = maps[(long long)c * g.stot + pix];
+        }
+        float s = dap * invdeap[dap_off + il] * (((parity + nl + h) & 1) ? -1.f : 1.f);
+        float re = (xv.x * mv.x - xv.y * mv.y) * s;
+        float im = (xv.x * mv.y + xv.y * mv.x) * s;
+        if (h == 0) { out.x = re; out.y = im; } else { out.z = re; out.w = im; }
+      }
+    }
+  }
+  grid[i] = out;
+}
+
+// ---------------------------------------------------------------------------
+// adjoint: crop * deapod * sign * conj(maps), summed over coils
+// ---------------------------------------------------------------------------
+template <int ND>
+__global__ void post_ifft_kernel(const float2* __restrict__ grid, const float2* __restrict__ maps,
+                                 const float* __restrict__ invdeap, float2* __restrict__ x, Geo g, int nb,
+                                 float scale) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long total = g.stot * nb;
+  if (i >= total) return;
+  int be = (int)(i / g.stot);
+  long long pix = i - (long long)be * g.stot;
+  int ii[3];
+  long long rem = pix;
+  for (int d = ND - 1; d >= 0; --d) {
+    ii[d] = (int)(rem % g.S[d]);
+    rem /= g.S[d];
+  }
+  float dap = scale;
+  int dap_off = 0, parity = 0;
+  long long cell = 0;
+  for (int d = 0; d < ND; ++d) {
+    dap *= invdeap[dap_off + ii[d]];
+    dap_off += g.S[d];
+    int n = ii[d] + g.off[d];
+    parity += n;
+    cell = cell * g.G[d] + n;
+  }
+  if (parity & 1) dap = -dap;
+  float re = 0.f, im = 0.f;
+  const float2* gp = grid + (long long)be * g.C * g.gtot + cell;
+  for (int c = 0; c < g.C; ++c) {
+    float2 v = gp[(long long)c * g.gtot];
+    float2 m = maps[(long long)c * g.stot + pix];
+    re += m.x * v.x + m.y * v.y;
+    im += m.x * v.y - m.y * v.x;
+  }
+  x[i] = make_float2(re * dap, im * dap);
+}
+
+// ---------------------------------------------------------------------------
+// forward interp: one thread per sample, all coils (W = 4)
+// ---------------------------------------------------------------------------
+struct InterpArgs {
+  const float2* grid;
+  const float* gx;
+  const float* wfwd;   // (B, K) or null
+  const int* order;    // (B, K) sample order or null (acquisition order)
+  float2* y;
+  int nb;
+  float scale;
+  float gsign;
+};
+
+template <int ND>
+__global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly kb) {
+  constexpr int W = 4;
+  long long kk = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int be = blockIdx.y;
+  if (kk >= g.K) return;
+  int b = frame_of(be, a.nb, g.B);
+  long long k = a.order ? a.order[(long long)b * g.K + kk] : kk;
+  float w[ND][W];
+  int nidx[ND][W];
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    float x = a.gx[((long long)b * ND + d) * g.K + k];
+    int base = (int)floorf(x);
+#pragma unroll
+    for (int o = 0; o < W; ++o) {
+      int n = base - (W / 2 - 1) + o;
+      float wd = mrb::kb_eval(kb, x - (float)n);
+      w[d][o] = (n & 1) ? -wd : wd;
+      nidx[d][o] = mrb::wrap_i(n, g.G[d]);
+    }
+  }
+  float s = a.scale * a.gsign;
+  if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
+  const float2* gb = a.grid + (long long)be * g.C * g.gtot;
+  for (int c = 0; c < g.C; ++c) {
+    const float2* gc = gb + (long long)c * g.gtot;
+    float re = 0.f, im = 0.f;
+    if (ND == 2) {
+#pragma unroll
+      for (int i0 = 0; i0 < W; ++i0) {
+        const float2* row = gc + (long long)nidx[0][i0] * g.G[1];
+        float r2 = 0.f, i2 = 0.f;
+#pragma unroll
+        for (int i1 = 0; i1 < W; ++i1) {
+          float2 v = __ldg(row + nidx[ND - 1][i1]);
+          r2 = fmaf(w[ND - 1][i1], v.x, r2);
+          i2 = fmaf(w[ND - 1][i1], v.y, i2);
+        }
+        re = fmaf(w[0][i0], r2, re);
+        im = fmaf(w[0][i0], i2, im);
+      }
+    } else {
+#pragma unroll
+      for (int i0 = 0; i0 < W; ++i0) {
+        float r1 = 0.f, im1 = 0.f;
+#pragma unroll
+        for (int i1 = 0; i1 < W; ++i1) {
+          const float2* row = gc + ((long long)nidx[0][i0] * g.G[1] + nidx[ND > 2 ? 1 : 0][i1]) * g.G[ND - 1];
+          float r2 = 0.f, i2 = 0.f;
+#pragma unroll
+          for (int i2x = 0; i2x < W; ++i2x) {
+            float2 v = __ldg(row + nidx[ND - 1][i2x]);
+            r2 = fmaf(w[ND - 1][i2x], v.x, r2);
+            i2 = fmaf(w[ND - 1][i2x], v.y, i2);
+          }
+          r1 = fmaf(w[ND > 2 ? 1 : 0][i1], r2, r1);
+          im1 = fmaf(w[ND > 2 ? 1 : 0][i1], i2, im1);
+        }
+        re = fmaf(w[0][i0], r1, re);
+        im = fmaf(w[0][i0], im1, im);
+      }
+    }
+    a.y[((long long)be * g.C + c) * g.K + k] = make_float2(re * s, im * s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// adjoint spread (2D, W = 4): one warp owns one output tile of T x T cells for
+// a group of coils, walks the tile's sample list in order and accumulates in
+// shared memory without atomics (lane = 16 taps x 2 coil lanes; a __syncwarp
+// orders consecutive samples), then writes every cell of the tile once.
+// Deterministic; each grid cell is written by exactly one warp.
+// ---------------------------------------------------------------------------
+struct SpreadArgs {
+  const float2* y;
+  const float* gx;
+  const float* wadj;
+  const int* entries;
+  const int* tile_start;
+  float2* grid;
+  int nb;
+  int cpi;     // coils per work item
+  int ngroups; // ceil(C / cpi)
+  float gsign;
+};
+
+constexpr int SPREAD_WARPS = 4;
+
+__global__ void __launch_bounds__(SPREAD_WARPS * 32) spread2d_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
+  extern __shared__ float2 sm[];
+  const int T = tg.T;
+  const int RS = T + 4;                 // padded row stride (bank spread for 4x4 taps)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long long item = (long long)blockIdx.x * SPREAD_WARPS + warp;
+  long long nitems = (long long)a.nb * tg.ntiles * a.ngroups;
+  if (item >= nitems) return;
+  int grp = (int)(item % a.ngroups);
+  long long rest = item / a.ngroups;
+  int tile = (int)(rest % tg.ntiles);
+  int be = (int)(rest / tg.ntiles);
+  int b = frame_of(be, a.nb, g.B);
+  int c0 = grp * a.cpi;
+  int nc = min(a.cpi, g.C - c0);
+  int tx0 = (tile / tg.nt[1]) * T;
+  int ty0 = (tile % tg.nt[1]) * T;
+  float2* acc = sm + (long long)warp * a.cpi * T * RS;
+  const int ncell = nc * T * RS;
+  for (int i = lane; i < ncell; i += 32) acc[i] = make_float2(0.f, 0.f);
+  __syncwarp();
+
+  const int key = b * tg.ntiles + tile;
+  const int e0 = a.tile_start[key], e1 = a.tile_start[key + 1];
+  const int tap = lane & 15, csub = lane >> 4;
+  const int ox = tap >> 2, oy = tap & 3;
+  const float* gx0p = a.gx + (long long)b * 2 * g.K;
+  const float* gx1p = gx0p + g.K;
+  const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
+  for (int e = e0; e < e1; ++e) {
+    int k = a.entries[e];
+    float x0 = gx0p[k], x1 = gx1p[k];
+    int n0 = (int)floorf(x0) - 1 + ox;
+    int n1 = (int)floorf(x1) - 1 + oy;
+    int lx = mrb::wrap_i(n0, g.G[0]) - tx0;
+    int ly = mrb::wrap_i(n1, g.G[1]) - ty0;
+    bool in = (unsigned)lx < (unsigned)T && (unsigned)ly < (unsigned)T;
+    float w = mrb::kb_eval(kb, x0 - (float)n0) * mrb::kb_eval(kb, x1 - (float)n1) * a.gsign;
+    if ((n0 + n1) & 1) w = -w;
+    if (a.wadj) w *= a.wadj[(long long)b * g.K + k];
+    if (in) {
+      for (int cl = csub; cl < nc; cl += 2) {
+        float2 v = yb[(long long)cl * g.K + k];
+        float2* p = acc + ((long long)cl * T + lx) * RS + ly;
+        float2 t = *p;
+        t.x = fmaf(w, v.x, t.x);
+        t.y = fmaf(w, v.y, t.y);
+        *p = t;
+      }
+    }
+    __syncwarp();
+  }
+  // write the whole tile once (zeros included)
+  float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
+  const int cells = nc * T * T;
+  for (int i = lane; i < cells; i += 32) {
+    int cl = i / (T * T);
+    int r = i - cl * T * T;
+    int lx = r / T, ly = r - lx * T;
+    int gx_ = tx0 + lx, gy_ = ty0 + ly;
+    if (gx_ < g.G[0] && gy_ < g.G[1])
+      gout[(long long)cl * g.gtot + (long long)gx_ * g.G[1] + gy_] = acc[((long long)cl * T + lx) * RS + ly];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// adjoint spread (3D, W = 4): same ownership scheme with T^3 tiles; lanes
+// cover 64 taps as 2 passes of 32, one coil at a time.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(SPREAD_WARPS * 32) spread3d_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
+  extern __shared__ float2 sm[];
+  const int T = tg.T;
+  const int T3 = T * T * T;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  long long item = (long long)blockIdx.x * SPREAD_WARPS + warp;
+  long long nitems = (long long)a.nb * tg.ntiles * a.ngroups;
+  if (item >= nitems) return;
+  int grp = (int)(item % a.ngroups);
+  long long rest = item / a.ngroups;
+  int tile = (int)(rest % tg.ntiles);
+  int be = (int)(rest / tg.ntiles);
+  int b = frame_of(be, a.nb, g.B);
+  int c0 = grp * a.cpi;
+  int nc = min(a.cpi, g.C - c0);
+  int t2 = tile % tg.nt[2];
+  int t1 = (tile / tg.nt[2]) % tg.nt[1];
+  int t0 = tile / (tg.nt[2] * tg.nt[1]);
+  int o0 = t0 * T, o1 = t1 * T, o2 = t2 * T;
+  float2* acc = sm + (long long)warp * a.cpi * T3;
+  const int ncell = nc * T3;
+  for (int i = lane; i < ncell; i += 32) acc[i] = make_float2(0.f, 0.f);
+  __syncwarp();
+  const int key = b * tg.ntiles + tile;
+  const int e0 = a.tile_start[key], e1 = a.tile_start[key + 1];
+  const float* gxp = a.gx + (long long)b * 3 * g.K;
+  const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
+  for (int e = e0; e < e1; ++e) {
+    int k = a.entries[e];
+    float x0 = gxp[k], x1 = gxp[g.K + k], x2 = gxp[2 * g.K + k];
+    int b0 = (int)floorf(x0) - 1, b1 = (int)floorf(x1) - 1, b2 = (int)floorf(x2) - 1;
+    float wadj = a.wadj ? a.wadj[(long long)b * g.K + k] : 1.f;
+#pragma unroll
+    for (int pass = 0; pass < 2; ++pass) {
+      int tap = lane + 32 * pass;
+      int a0 = tap >> 4, a1 = (tap >> 2) & 3, a2 = tap & 3;
+      int n0 = b0 + a0, n1 = b1 + a1, n2 = b2 + a2;
+      int l0 = mrb::wrap_i(n0, g.G[0]) - o0;
+      int l1 = mrb::wrap_i(n1, g.G[1]) - o1;
+      int l2 = mrb::wrap_i(n2, g.G[2]) - o2;
+      bool in = (unsigned)l0 < (unsigned)T && (unsigned)l1 < (unsigned)T && (unsigned)l2 < (unsigned)T;
+      if (in) {
+        float w = mrb::kb_eval(kb, x0 - (float)n0) * mrb::kb_eval(kb, x1 - (float)n1) *
+                  mrb::kb_eval(kb, x2 - (float)n2) * a.gsign * wadj;
+        if ((n0 + n1 + n2) & 1) w = -w;
+        int cell = (l0 * T + l1) * T + l2;
+        for (int cl = 0; cl < nc; ++cl) {
+          float2 v = yb[(long long)cl * g.K + k];
+          float2* p = acc + (long long)cl * T3 + cell;
+          float2 t = *p;
+          t.x = fmaf(w, v.x, t.x);
+          t.y = fmaf(w, v.y, t.y);
+          *p = t;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
+  for (int i = lane; i < ncell; i += 32) {
+    int cl = i / T3;
+    int r = i - cl * T3;
+    int l0 = r / (T * T), l1 = (r / T) % T, l2 = r % T;
+    int n0 = o0 + l0, n1 = o1 + l1, n2 = o2 + l2;
+    if (n0 < g.G[0] && n1 < g.G[1] && n2 < g.G[2])
+      gout[(long long)cl * g.gtot + ((long long)n0 * g.G[1] + n1) * g.G[2] + n2] = acc[i];
+  }
+}
+
+// literal / corrected index tables for one frame
+__global__ void grid_index_kernel(const float* __restrict__ traj, int nd, int G0, int G1, int G2, long long K,
+                                  int W, int conv, long long* __restrict__ out) {
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  int G[3] = {G0, G1, G2};
+  long long n[3][16];
+  for (int d = 0; d < nd; ++d) {
+    float gx = mrb::ref_grid_coord(traj[(long long)d * K + k], (float)G[d], (float)((double)G[d] - 1e-6));
+    for (int o = 0; o < W; ++o) {
+      long long v;
+      if (conv == MRB_IDX_REFERENCE) {
+        float off = (float)(o - W / 2);
+        v = (long long)floorf(__fadd_rn(gx, off));
+      } else {
+        v = (long long)floorf(gx) + (o - (W / 2 - 1));
+      }
+      long long r = v % G[d];
+      n[d][o] = r < 0 ? r + G[d] : r;
+    }
+  }
+  long long W2 = (long long)W * W;
+  long long per = nd == 2 ? W2 : W2 * W;
+  long long* row = out + k * per;
+  if (nd == 2) {
+    for (int a = 0; a < W; ++a)
+      for (int b = 0; b < W; ++b)
+        row[a * W + b] = conv == MRB_IDX_REFERENCE ? n[0][a] + (long long)G0 * n[1][b]
+                                                   : n[0][a] * G1 + n[1][b];
+  } else {
+    for (int a = 0; a < W; ++a)
+      for (int b = 0; b < W; ++b)
+        for (int c = 0; c < W; ++c)
+          row[(a * W + b) * W + c] = conv == MRB_IDX_REFERENCE
+                                         ? n[0][a] + (long long)G0 * n[1][b] + (long long)G0 * G1 * n[2][c]
+                                         : (n[0][a] * G1 + n[1][b]) * G2 + n[2][c];
+  }
+}
+
+__global__ void cell_base_kernel(const float* __restrict__ gx, int* __restrict__ out, long long n) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = (int)floorf(gx[i]);
+}
+
+int grid_blocks(long long n, int bs) { return (int)((n + bs - 1) / bs); }
+
+int ensure_fft(mrb_plan* p, int nb) {
+  int batch = nb * p->C;
+  if (p->fft && p->fft_batch == batch) return 0;
+  if (p->fft) {
+    cufftDestroy(p->fft);
+    p->fft = 0;
+  }
+  int n[3] = {p->G[0], p->G[1], p->G[2]};
+  int dist = (int)p->gtot();
+  cufftResult r = cufftPlanMany(&p->fft, p->nd, n, nullptr, 1, dist, nullptr, 1, dist, CUFFT_C2C, batch);
+  if (r != CUFFT_SUCCESS) {
+    p->fft = 0;
+    return mrb::fail(MRB_ECUFFT, "cufftPlanMany failed (%d) for batch %d", (int)r, batch);
+  }
+  p->fft_batch = batch;
+  return 0;
+}
+
+int check_ready(mrb_plan* p) {
+  if (!p) return mrb::fail(MRB_EINVAL, "null plan");
+  if (!p->have_points) return mrb::fail(MRB_ESTATE, "plan has no trajectory (call mrb_plan_set_points)");
+  if (!p->have_maps) return mrb::fail(MRB_ESTATE, "plan has no coil maps (call mrb_plan_set_maps)");
+  return 0;
+}
+
+int check_nb(mrb_plan* p, int nb) {
+  if (nb <= 0) return mrb::fail(MRB_EINVAL, "batch must be positive (got %d)", nb);
+  if (p->B != 1 && nb % p->B != 0)
+    return mrb::fail(MRB_EINVAL, "omega batch %d incompatible with requested %d", p->B, nb);
+  return 0;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int B, int64_t K, int W, double osf,
+                               int norm_ortho) {
+  if (!out) return mrb::fail(MRB_EINVAL, "null output pointer");
+  *out = nullptr;
+  MRB_REQUIRE(nd == 2 || nd == 3, "nd must be 2 or 3 (got %d)", nd);
+  MRB_REQUIRE(S != nullptr, "null image shape");
+  MRB_REQUIRE(C >= 1 && B >= 1 && K >= 1, "C, B, K must be positive");
+  MRB_REQUIRE(W == 4, "kernel width %d not supported (W = 4)", W);
+  MRB_REQUIRE(osf >= 1.0 && osf <= 4.0, "osf out of range");
+  mrb_plan* p = new mrb_plan();
+  p->nd = nd;
+  for (int d = 0; d < nd; ++d) {
+    if (S[d] < 2) {
+      delete p;
+      return mrb::fail(MRB_EINVAL, "image dim %d must be >= 2", d);
+    }
+    p->S[d] = S[d];
+    p->G[d] = (int)std::ceil(osf * (double)S[d]);
+    if (p->G[d] % 2) {
+      delete p;
+      return mrb::fail(MRB_EINVAL, "oversampled grid dim %d = %d must be even", d, p->G[d]);
+    }
+  }
+  p->C = C;
+  p->B = B;
+  p->K = K;
+  p->W = W;
+  p->osf = osf;
+  p->ortho = norm_ortho ? 1 : 0;
+  p->scale = norm_ortho ? (float)(1.0 / std::sqrt((double)p->gtot())) : 1.f;
+  int hs = 0;
+  for (int d = 0; d < nd; ++d) hs += p->G[d] / 2;
+  p->gsign = (hs & 1) ? -1.f : 1.f;
+  p->beta = M_PI * std::sqrt(std::pow((W / osf) * (osf - 0.5), 2) - 0.8);   // ptnufft.py:125
+  mrb::kb_poly_init(p->kb, W, p->beta);
+  p->tile = nd == 2 ? 16 : 8;
+  p->coils_per_item = nd == 2 ? std::min(C, 4) : std::min(C, 2);
+  // deapodisation: closed-form FT of the truncated KB window
+  std::vector<float> dap;
+  double i0b = 0.0;
+  {
+    double q = 0.25 * p->beta * p->beta, term = 1.0, sum = 1.0;
+    for (int k = 1; k < 200; ++k) {
+      term *= q / ((double)k * k);
+      sum += term;
+      if (term < 1e-18 * sum) break;
+    }
+    i0b = sum;
+  }
+  for (int d = 0; d < nd; ++d) {
+    for (int i = 0; i < S[d]; ++i) {
+      double r = (double)(i - S[d] / 2);
+      double a = p->beta * p->beta - std::pow(M_PI * W * r / p->G[d], 2);
+      double ph;
+      if (a > 0) ph = std::sinh(std::sqrt(a)) / std::sqrt(a);
+      else if (a < 0) ph = std::sin(std::sqrt(-a)) / std::sqrt(-a);
+      else ph = 1.0;
+      ph *= W / i0b;
+      dap.push_back((float)(1.0 / ph));
+    }
+  }
+  int rc = p->invdeap.ensure(dap.size() * sizeof(float));
+  if (!rc && cudaMemcpy(p->invdeap.p, dap.data(), dap.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = mrb::fail(MRB_ECUDA, "copying deapodisation failed");
+  if (rc) {
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return 0;
+}
+
+extern "C" int mrb_plan_destroy(mrb_plan* p) {
+  if (!p) return 0;
+  if (p->fft) cufftDestroy(p->fft);
+  for (DevBuf* b : {&p->gx, &p->entries, &p->tile_start, &p->sorted_k, &p->maps, &p->invdeap, &p->wfwd,
+                    &p->wadj, &p->grid, &p->tmp})
+    b->release();
+  delete p;
+  return 0;
+}
+
+extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
+  MRB_REQUIRE(p != nullptr, "null plan");
+  switch (key) {
+    case 0:
+      MRB_REQUIRE(value == 4 || value == 8 || value == 16 || value == 32, "tile edge must be 4, 8, 16 or 32");
+      MRB_REQUIRE(p->nd == 2 || value <= 8, "3D tile edge must be <= 8");
+      p->tile = (int)value;
+      p->have_points = false;   // lists depend on the tile
+      return 0;
+    case 1:
+      MRB_REQUIRE(value >= 1 && value <= 64, "coils per item out of range");
+      p->coils_per_item = (int)std::min<int64_t>(value, p->C);
+      return 0;
+    case 2:
+      MRB_REQUIRE(value == 0 || value == 1, "interp mode must be 0 or 1");
+      p->interp_mode = (int)value;
+      return 0;
+    default:
+      return mrb::fail(MRB_EINVAL, "unknown option %d", key);
+  }
+}
+
+extern "C" int mrb_plan_set_points(mrb_plan* p, const float* traj, mrb_stream_t stream) {
+  MRB_REQUIRE(p != nullptr && traj != nullptr, "null plan or trajectory");
+  cudaStream_t st = (cudaStream_t)stream;
+  Geo g = make_geo(p);
+  const long long nBK = (long long)p->B * p->K;
+  const long long nall = nBK * p->nd;
+  int rc;
+  if ((rc = p->gx.ensure(nall * sizeof(float)))) return rc;
+  coords_kernel<<<grid_blocks(nall, 256), 256, 0, st>>>(traj, p->gx.as<float>(), g);
+  MRB_LAUNCH_CHECK();
+
+  TileGeo tg{};
+  tg.T = p->tile;
+  tg.ntiles = 1;
+  for (int d = 0; d < 3; ++d) tg.nt[d] = 1;
+  for (int d = 0; d < p->nd; ++d) {
+    tg.nt[d] = (p->G[d] + tg.T - 1) / tg.T;
+    tg.ntiles *= tg.nt[d];
+  }
+  tg.lo_off = p->W / 2 - 1;
+  tg.hi_off = p->W / 2;
+  MRB_REQUIRE((long long)p->B * tg.ntiles < (1LL << 31), "too many tiles");
+  p->ntiles = tg.ntiles;
+  for (int d = 0; d < 3; ++d) p->ntile_d[d] = tg.nt[d];
+
+  // counts + exclusive scan
+  DevBuf cnt, offs;
+  if ((rc = cnt.ensure((nBK + 1) * sizeof(int)))) return rc;
+  if ((rc = offs.ensure((nBK + 1) * sizeof(int)))) { cnt.release(); return rc; }
+  entry_count_kernel<<<grid_blocks(nBK, 256), 256, 0, st>>>(p->gx.as<float>(), cnt.as<int>(), g, tg);
+  fill_int_kernel<<<1, 1, 0, st>>>(cnt.as<int>() + nBK, 1, 0);
+  size_t tmp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, cnt.as<int>(), offs.as<int>(), (int)(nBK + 1), st);
+  if ((rc = p->tmp.ensure(tmp_bytes))) return rc;
+  cub::DeviceScan::ExclusiveSum(p->tmp.p, tmp_bytes, cnt.as<int>(), offs.as<int>(), (int)(nBK + 1), st);
+  MRB_LAUNCH_CHECK();
+  int n_entries = 0;
+  MRB_CUDA_TRY(cudaMemcpyAsync(&n_entries, offs.as<int>() + nBK, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MRB_CUDA_TRY(cudaStreamSynchronize(st));
+  p->n_entries = n_entries;
+
+  DevBuf keys, keys_sorted, vals;
+  if ((rc = keys.ensure((size_t)std::max(n_entries, 1) * sizeof(unsigned)))) return rc;
+  if ((rc = keys_sorted.ensure((size_t)std::max(n_entries, 1) * sizeof(unsigned)))) return rc;
+  if ((rc = vals.ensure((size_t)std::max(n_entries, 1) * sizeof(int)))) return rc;
+  if ((rc = p->entries.ensure((size_t)std::max(n_entries, 1) * sizeof(int)))) return rc;
+  if ((rc = p->tile_start.ensure(((size_t)p->B * tg.ntiles + 1) * sizeof(int)))) return rc;
+  entry_fill_kernel<<<grid_blocks(nBK, 256), 256, 0, st>>>(p->gx.as<float>(), offs.as<int>(), keys.as<unsigned>(),
+                                                           vals.as<int>(), g, tg);
+  MRB_LAUNCH_CHECK();
+  int nkeys = p->B * tg.ntiles;
+  int end_bit = 1;
+  while ((1LL << end_bit) <= nkeys) ++end_bit;
+  tmp_bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys.as<unsigned>(), keys_sorted.as<unsigned>(),
+                                  vals.as<int>(), p->entries.as<int>(), n_entries, 0, end_bit, st);
+  if ((rc = p->tmp.ensure(tmp_bytes))) return rc;
+  cub::DeviceRadixSort::SortPairs(p->tmp.p, tmp_bytes, keys.as<unsigned>(), keys_sorted.as<unsigned>(),
+                                  vals.as<int>(), p->entries.as<int>(), n_entries, 0, end_bit, st);
+  MRB_LAUNCH_CHECK();
+  if (n_entries > 0) {
+    tile_start_kernel<<<grid_blocks(n_entries, 256), 256, 0, st>>>(keys_sorted.as<unsigned>(), n_entries,
+                                                                   p->tile_start.as<int>(), nkeys);
+  } else {
+    fill_int_kernel<<<grid_blocks(nkeys + 1, 256), 256, 0, st>>>(p->tile_start.as<int>(), nkeys + 1, 0);
+  }
+  MRB_LAUNCH_CHECK();
+
+  // touched cells (sum over frames), for the roofline bookkeeping
+  {
+    long long nwords = (p->gtot() + 31) / 32;
+    DevBuf bits, cntd;
+    if ((rc = bits.ensure(nwords * sizeof(unsigned)))) return rc;
+    if ((rc = cntd.ensure(sizeof(unsigned long long)))) return rc;
+    MRB_CUDA_TRY(cudaMemsetAsync(cntd.p, 0, sizeof(unsigned long long), st));
+    for (int b = 0; b < p->B; ++b) {
+      MRB_CUDA_TRY(cudaMemsetAsync(bits.p, 0, nwords * sizeof(unsigned), st));
+      touch_kernel<<<grid_blocks(p->K, 256), 256, 0, st>>>(p->gx.as<float>(), bits.as<unsigned>(), g, p->W, b);
+      popc_kernel<<<grid_blocks(nwords, 256), 256, 0, st>>>(bits.as<unsigned>(), nwords,
+                                                            cntd.as<unsigned long long>());
+    }
+    MRB_LAUNCH_CHECK();
+    unsigned long long touched = 0;
+    MRB_CUDA_TRY(cudaMemcpyAsync(&touched, cntd.p, sizeof(touched), cudaMemcpyDeviceToHost, st));
+    MRB_CUDA_TRY(cudaStreamSynchronize(st));
+    p->touched = (int64_t)touched;
+  }
+  MRB_CUDA_TRY(cudaStreamSynchronize(st));
+  p->have_points = true;
+  return 0;
+}
+
+extern "C" int mrb_plan_set_dcf(mrb_plan* p, const float* dcf, int mode, int apply_fwd, int apply_adj,
+                                mrb_stream_t stream) {
+  MRB_REQUIRE(p != nullptr, "null plan");
+  MRB_REQUIRE(mode >= 0 && mode <= 2, "bad dcf mode %d", mode);
+  cudaStream_t st = (cudaStream_t)stream;
+  p->has_wfwd = p->has_wadj = false;
+  if (!dcf || mode == MRB_DCF_NONE) return 0;
+  long long n = (long long)p->B * p->K;
+  int rc;
+  if (mode == MRB_DCF_BALANCED) {
+    if ((rc = p->wfwd.ensure(n * sizeof(float)))) return rc;
+    dcf_weight_kernel<<<grid_blocks(n, 256), 256, 0, st>>>(dcf, p->wfwd.as<float>(), n, 1);
+    if ((rc = p->wadj.ensure(n * sizeof(float)))) return rc;
+    dcf_weight_kernel<<<grid_blocks(n, 256), 256, 0, st>>>(dcf, p->wadj.as<float>(), n, 1);
+    p->has_wfwd = p->has_wadj = true;
+  } else {
+    if (apply_fwd) {
+      if ((rc = p->wfwd.ensure(n * sizeof(float)))) return rc;
+      dcf_weight_kernel<<<grid_blocks(n, 256), 256, 0, st>>>(dcf, p->wfwd.as<float>(), n, 0);
+      p->has_wfwd = true;
+    }
+    if (apply_adj) {
+      if ((rc = p->wadj.ensure(n * sizeof(float)))) return rc;
+      dcf_weight_kernel<<<grid_blocks(n, 256), 256, 0, st>>>(dcf, p->wadj.as<float>(), n, 0);
+      p->has_wadj = true;
+    }
+  }
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_plan_set_maps(mrb_plan* p, const void* maps, mrb_stream_t stream) {
+  MRB_REQUIRE(p != nullptr && maps != nullptr, "null plan or maps");
+  size_t bytes = (size_t)p->C * p->stot() * sizeof(float2);
+  int rc;
+  if ((rc = p->maps.ensure(bytes))) return rc;
+  MRB_CUDA_TRY(cudaMemcpyAsync(p->maps.p, maps, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  p->have_maps = true;
+  return 0;
+}
+
+static int ensure_grid(mrb_plan* p, int nb) {
+  size_t bytes = (size_t)nb * p->C * p->gtot() * sizeof(float2);
+  int rc = p->grid.ensure(bytes);
+  if (rc) return rc;
+  return ensure_fft(p, nb);
+}
+
+static int forward_impl(mrb_plan* p, const void* x, void* y, int nb, cudaStream_t st, int coil_images) {
+  int rc;
+  if ((rc = check_ready(p))) return rc;
+  if ((rc = check_nb(p, nb))) return rc;
+  MRB_REQUIRE(x != nullptr && y != nullptr, "null x or y");
+  if ((rc = ensure_grid(p, nb))) return rc;
+  Geo g = make_geo(p);
+  long long pairs = (long long)nb * p->C * (p->gtot() / 2);
+  if (p->nd == 2)
+    pre_fft_kernel<2><<<grid_blocks(pairs, 256), 256, 0, st>>>(
+        (const float2*)x, p->maps.as<float2>(), p->invdeap.as<float>(), p->grid.as<float4>(), g, nb, coil_images);
+  else
+    pre_fft_kernel<3><<<grid_blocks(pairs, 256), 256, 0, st>>>(
+        (const float2*)x, p->maps.as<float2>(), p->invdeap.as<float>(), p->grid.as<float4>(), g, nb, coil_images);
+  MRB_LAUNCH_CHECK();
+  cufftResult r = cufftSetStream(p->fft, st);
+  if (r == CUFFT_SUCCESS) r = cufftExecC2C(p->fft, p->grid.as<cufftComplex>(), p->grid.as<cufftComplex>(), CUFFT_FORWARD);
+  if (r != CUFFT_SUCCESS) return mrb::fail(MRB_ECUFFT, "cufftExecC2C forward failed (%d)", (int)r);
+  InterpArgs a{};
+  a.grid = p->grid.as<float2>();
+  a.gx = p->gx.as<float>();
+  a.wfwd = p->has_wfwd ? p->wfwd.as<float>() : nullptr;
+  a.order = nullptr;
+  a.y = (float2*)y;
+  a.nb = nb;
+  a.scale = p->scale;
+  a.gsign = p->gsign;
+  dim3 grid(grid_blocks(p->K, 256), nb);
+  if (p->nd == 2) interp_kernel<2><<<grid, 256, 0, st>>>(a, g, p->kb);
+  else interp_kernel<3><<<grid, 256, 0, st>>>(a, g, p->kb);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_nufft_forward(mrb_plan* p, const void* x, void* y, int nb, mrb_stream_t stream) {
+  return forward_impl(p, x, y, nb, (cudaStream_t)stream, 0);
+}
+
+extern "C" int mrb_nufft_forward_coils(mrb_plan* p, const void* x, void* y, int nb, mrb_stream_t stream) {
+  return forward_impl(p, x, y, nb, (cudaStream_t)stream, 1);
+}
+
+extern "C" int mrb_nufft_adjoint(mrb_plan* p, const void* y, void* x, int nb, mrb_stream_t stream) {
+  int rc;
+  if ((rc = check_ready(p))) return rc;
+  if ((rc = check_nb(p, nb))) return rc;
+  MRB_REQUIRE(x != nullptr && y != nullptr, "null x or y");
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((rc = ensure_grid(p, nb))) return rc;
+  Geo g = make_geo(p);
+  TileGeo tg{};
+  tg.T = p->tile;
+  tg.ntiles = p->ntiles;
+  for (int d = 0; d < 3; ++d) tg.nt[d] = p->ntile_d[d];
+  tg.lo_off = p->W / 2 - 1;
+  tg.hi_off = p->W / 2;
+  SpreadArgs a{};
+  a.y = (const float2*)y;
+  a.gx = p->gx.as<float>();
+  a.wadj = p->has_wadj ? p->wadj.as<float>() : nullptr;
+  a.entries = p->entries.as<int>();
+  a.tile_start = p->tile_start.as<int>();
+  a.grid = p->grid.as<float2>();
+  a.nb = nb;
+  a.cpi = p->coils_per_item;
+  a.ngroups = (p->C + a.cpi - 1) / a.cpi;
+  a.gsign = p->gsign;
+  long long items = (long long)nb * tg.ntiles * a.ngroups;
+  int blocks = grid_blocks(items, SPREAD_WARPS);
+  if (p->nd == 2) {
+    size_t smem = (size_t)SPREAD_WARPS * a.cpi * tg.T * (tg.T + 4) * sizeof(float2);
+    if (smem > 48 * 1024)
+      MRB_CUDA_TRY(cudaFuncSetAttribute(spread2d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MRB_REQUIRE(smem <= 227 * 1024, "spread tile needs %zu bytes of shared memory", smem);
+    spread2d_kernel<<<blocks, SPREAD_WARPS * 32, smem, st>>>(a, g, tg, p->kb);
+  } else {
+    size_t smem = (size_t)SPREAD_WARPS * a.cpi * tg.T * tg.T * tg.T * sizeof(float2);
+    if (smem > 48 * 1024)
+      MRB_CUDA_TRY(cudaFuncSetAttribute(spread3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MRB_REQUIRE(smem <= 227 * 1024, "spread tile needs %zu bytes of shared memory", smem);
+    spread3d_kernel<<<blocks, SPREAD_WARPS * 32, smem, st>>>(a, g, tg, p->kb);
+  }
+  MRB_LAUNCH_CHECK();
+  cufftResult r = cufftSetStream(p->fft, st);
+  if (r == CUFFT_SUCCESS) r = cufftExecC2C(p->fft, p->grid.as<cufftComplex>(), p->grid.as<cufftComplex>(), CUFFT_INVERSE);
+  if (r != CUFFT_SUCCESS) return mrb::fail(MRB_ECUFFT, "cufftExecC2C inverse failed (%d)", (int)r);
+  long long total = p->stot() * nb;
+  if (p->nd == 2)
+    post_ifft_kernel<2><<<grid_blocks(total, 256), 256, 0, st>>>(p->grid.as<float2>(), p->maps.as<float2>(),
+                                                                 p->invdeap.as<float>(), (float2*)x, g, nb, p->scale);
+  else
+    post_ifft_kernel<3><<<grid_blocks(total, 256), 256, 0, st>>>(p->grid.as<float2>(), p->maps.as<float2>(),
+                                                                 p->invdeap.as<float>(), (float2*)x, g, nb, p->scale);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_plan_info(mrb_plan* p, int64_t* out, int nout) {
+  MRB_REQUIRE(p != nullptr && out != nullptr, "null plan or output");
+  int64_t v[6] = {p->n_entries, p->ntiles, p->touched, p->tile, p->coils_per_item, p->gtot()};
+  for (int i = 0; i < nout && i < 6; ++i) out[i] = v[i];
+  return 0;
+}
+
+extern "C" int mrb_plan_cell_base(mrb_plan* p, int32_t* out, mrb_stream_t stream) {
+  MRB_REQUIRE(p != nullptr && out != nullptr, "null plan or output");
+  if (!p->have_points) return mrb::fail(MRB_ESTATE, "plan has no trajectory");
+  long long n = (long long)p->B * p->nd * p->K;
+  cell_base_kernel<<<grid_blocks(n, 256), 256, 0, (cudaStream_t)stream>>>(p->gx.as<float>(), out, n);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_grid_indices(const float* traj, int nd, const int* G, int64_t K, int W, int convention,
+                                int64_t* idx, mrb_stream_t stream) {
+  MRB_REQUIRE(traj != nullptr && G != nullptr && idx != nullptr, "null pointer");
+  MRB_REQUIRE(nd == 2 || nd == 3, "nd must be 2 or 3");
+  MRB_REQUIRE(W >= 2 && W <= 16 && W % 2 == 0, "W must be even and <= 16");
+  MRB_REQUIRE(convention == MRB_IDX_REFERENCE || convention == MRB_IDX_CORRECTED, "bad convention");
+  for (int d = 0; d < nd; ++d) MRB_REQUIRE(G[d] >= 1, "bad grid");
+  grid_index_kernel<<<grid_blocks(K, 128), 128, 0, (cudaStream_t)stream>>>(
+      traj, nd, G[0], G[1], nd > 2 ? G[2] : 1, K, W, convention, (long long*)idx);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}

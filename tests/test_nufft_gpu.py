@@ -1,0 +1,214 @@
+"""NUFFT parity on the GPU: CUDA path (through the C ABI) vs the CPU oracle.
+
+Tolerances: bin/cell indices bit-exact; forward/adjoint rel-L2 <= 1e-5 against
+the oracle's FP64 KB gridding with the same conventions (the stated target);
+KB approximation error vs the FP64 NUDFT <= 2e-3 (W=4, osf=2 gives ~6e-4).
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden, rel
+from oracle import kb as okb
+from oracle.nudft import nudft_forward, nudft_adjoint
+from mrirecon_b200 import phantoms
+from mrirecon_b200.nufft import B200NUFFTAdapter, grid_indices, NUFFT, NUFFTConfig
+from mrirecon_b200.layout import AxisSpec
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def _rand_c(shape, seed, dtype=torch.complex128):
+    g = torch.Generator().manual_seed(seed)
+    return (torch.randn(shape, generator=g, dtype=torch.float64)
+            + 1j * torch.randn(shape, generator=g, dtype=torch.float64)).to(dtype)
+
+
+def _adapter(maps, traj, dcf=None, dev="cuda", **kw):
+    ad = B200NUFFTAdapter(ndim=maps.ndim - 1, **kw)
+    ad.prepare(tuple(maps.shape), traj.to(dev), None if dcf is None else dcf.to(dev),
+               maps.to(dev, torch.complex64), torch.complex64, torch.device(dev))
+    return ad
+
+
+@pytest.mark.parametrize("case", ["2d_32", "2d_24x40", "3d_12x10x8"])
+def test_reference_grid_indices_bit_exact(cuda, case):
+    g = golden("ptnufft_idx.npz")
+    traj, G, idx = g[f"{case}_traj"], tuple(int(v) for v in g[f"{case}_grid"]), g[f"{case}_idx"]
+    for b in range(traj.shape[0]):
+        mine = grid_indices(torch.from_numpy(traj[b]).to(cuda), G, 4, "reference").cpu().numpy()
+        assert np.array_equal(mine, idx[b].astype(np.int64))
+
+
+@pytest.mark.parametrize("S,K", [((32, 32), 1500), ((24, 40), 1500), ((12, 10, 8), 500)])
+def test_corrected_indices_and_cell_base_bit_exact(cuda, S, K):
+    g = golden("ptnufft_idx.npz")
+    key = {2: "2d_32", 3: "3d_12x10x8"}[len(S)]
+    traj = torch.from_numpy(g[f"{key}_traj"])[:, :, :K]
+    G = okb.grid_shape(S, 2.0)
+    # stand-alone table
+    for b in range(traj.shape[0]):
+        mine = grid_indices(traj[b].to(cuda), G, 4, "corrected").cpu().numpy()
+        o = okb.KBNufft(torch.ones((1,) + S, dtype=torch.complex128), traj[b:b + 1], None)
+        assert np.array_equal(mine, o.idx[0].numpy())
+    # the plan's binning key
+    ad = _adapter(torch.ones((1,) + S, dtype=torch.complex64), traj)
+    base = ad.plan.cell_base().cpu().numpy()
+    for b in range(traj.shape[0]):
+        assert np.array_equal(base[b], okb.cell_base(traj[b].numpy(), G).astype(np.int32))
+
+
+def _check_pair(maps, traj, dcf=None, nb=None, seed=1, **kw):
+    dev = "cuda"
+    B, nd, K = traj.shape
+    nb = nb or B
+    S = tuple(maps.shape[1:])
+    C = maps.shape[0]
+    ad = _adapter(maps, traj, dcf, **kw)
+    orc = okb.KBNufft(maps.to(torch.complex128), traj, dcf, dtype=torch.complex128,
+                      dcf_mode=kw.get("dcf_mode", "balanced"), apply_dcf_in_fwd=kw.get("apply_dcf_in_fwd", False),
+                      apply_dcf_in_adj=kw.get("apply_dcf_in_adj", True), norm=kw.get("norm", "ortho"))
+    x = _rand_c((nb, 1) + S, seed)
+    y = _rand_c((nb, C, K), seed + 1)
+    yg = ad.A(x.to(dev, torch.complex64))
+    xg = ad.AH(y.to(dev, torch.complex64))
+    ya, xa = orc.A(x), orc.AH(y)
+    assert rel(yg, ya) < TOL, f"forward rel {rel(yg, ya):.3e}"
+    assert rel(xg, xa) < TOL, f"adjoint rel {rel(xg, xa):.3e}"
+    if kw.get("dcf_mode", "balanced") != "standard":      # standard DCF is one-sided: not an adjoint pair
+        lhs = torch.vdot(yg.cpu().to(torch.complex128).reshape(-1), y.reshape(-1))
+        rhs = torch.vdot(x.reshape(-1), xg.cpu().to(torch.complex128).reshape(-1))
+        assert abs(complex(lhs / rhs) - 1) < 1e-5
+    return ad
+
+
+@pytest.mark.parametrize("S", [(32, 32), (24, 40), (31, 33), (64, 48), (33, 35), (17, 9)])
+def test_forward_adjoint_vs_oracle_2d(cuda, S):
+    C = 3
+    maps = _rand_c((C,) + S, 5, torch.complex64)
+    traj = phantoms.random_traj(2, 2, 1200, seed=3)
+    _check_pair(maps, traj)
+
+
+def test_radial_edges_and_wrap(cuda):
+    """Golden-angle spokes hit k = -pi exactly (wraps to the far grid edge)."""
+    maps = phantoms.coil_maps(48, 4).to(torch.complex64)
+    traj = torch.stack([phantoms.golden_angle_radial(9, 96, 9 * f) for f in range(3)])
+    _check_pair(maps, traj)
+
+
+@pytest.mark.parametrize("mode,fwd,adj", [("balanced", False, True), ("standard", True, False),
+                                          ("standard", False, True), ("none", False, True)])
+def test_dcf_modes(cuda, mode, fwd, adj):
+    maps = _rand_c((2, 20, 20), 8, torch.complex64)
+    traj = phantoms.random_traj(2, 2, 500, seed=9)
+    dcf = torch.rand(2, 500, generator=torch.Generator().manual_seed(2)) + 0.1
+    _check_pair(maps, traj, dcf, dcf_mode=mode, apply_dcf_in_fwd=fwd, apply_dcf_in_adj=adj)
+
+
+def test_beff_repeat_interleave(cuda):
+    """B_eff = 2*B uses trajectory frame be // 2 (torchkb _expand_omega)."""
+    maps = _rand_c((2, 16, 16), 4, torch.complex64)
+    traj = phantoms.random_traj(2, 2, 400, seed=4)
+    _check_pair(maps, traj, nb=4)
+
+
+def test_unnormalised(cuda):
+    maps = _rand_c((2, 16, 18), 6, torch.complex64)
+    traj = phantoms.random_traj(1, 2, 400, seed=6)
+    _check_pair(maps, traj, norm="none")
+
+
+@pytest.mark.parametrize("tile,cpi", [(8, 1), (16, 2), (32, 3), (4, 4)])
+def test_tiling_options_identical(cuda, tile, cpi):
+    """Every tile / coil-group choice gives the same (deterministic) grid."""
+    maps = phantoms.coil_maps(64, 5).to(torch.complex64)
+    traj = phantoms.grasp_trajectory(2, 13, 128)
+    y = _rand_c((2, 5, traj.shape[-1]), 3, torch.complex64).to(cuda)
+    ref = _adapter(maps, traj).AH(y)
+    ad = _adapter(maps, traj, tile=tile, coils_per_item=cpi)
+    out = ad.AH(y)
+    assert rel(out, ref) < 1e-6
+    out2 = ad.AH(y)
+    assert torch.equal(out, out2)
+
+
+def test_3d_vs_oracle(cuda):
+    S = (12, 10, 8)
+    maps = _rand_c((2,) + S, 12, torch.complex64)
+    traj = phantoms.random_traj(2, 3, 700, seed=13)
+    _check_pair(maps, traj)
+
+
+def test_vs_nudft_fixture(cuda):
+    """KB approximation error against the reference's _nudft_A ground truth."""
+    g = golden("nudft_a.npz")
+    maps, x = torch.from_numpy(g["maps"]), torch.from_numpy(g["x"])
+    traj, dcf = torch.from_numpy(g["traj"]), torch.from_numpy(g["dcf"])
+    ad = _adapter(maps.to(torch.complex64), traj.unsqueeze(0), dcf.unsqueeze(0), norm="none")
+    y = ad.A(x.to(cuda, torch.complex64))
+    assert rel(y, torch.from_numpy(g["y"])) < 2e-3
+    yy = _rand_c(tuple(y.shape), 3)
+    xa = ad.AH(yy.to(cuda, torch.complex64))
+    xt = nudft_adjoint(maps, yy, traj, dcf)
+    assert rel(xa, xt) < 2e-3
+
+
+def test_front_end_layouts(cuda):
+    """User layout (B, L, coil, X, Y) / (B, L, coil, K) through the NUFFT front-end."""
+    B, L, C, S, K = 2, 2, 3, (20, 24), 300
+    maps = _rand_c((C,) + S, 21, torch.complex64)
+    traj = phantoms.random_traj(B, 2, K, seed=22)
+    axis = AxisSpec(image_labels=("B", "L", "coil", "X", "Y"), kspace_labels=("B", "L", "coil", "K"),
+                    image_fft_labels=("X", "Y"), coil_label="coil")
+    op = NUFFT(maps.to(cuda), traj.to(cuda), None, axis=axis,
+               config=NUFFTConfig(ndim=2, traj_units="rad"), device=cuda)
+    assert op.roles_image.resolve_axes("spatial") == (3, 4)
+    x = _rand_c((B, L, 1) + S, 23, torch.complex64).to(cuda)
+    y = torch.empty((B, L, C, K), dtype=torch.complex64, device=cuda)
+    op.A(x, out=y)
+    orc = okb.KBNufft(maps, traj, None, dtype=torch.complex128)
+    ya = orc.A(x.cpu().reshape(B * L, 1, *S)).reshape(B, L, C, K)
+    assert rel(y, ya) < TOL
+    xh = torch.empty_like(x)
+    op.AH(y, out=xh)
+    xa = orc.AH(y.cpu().reshape(B * L, C, K).to(torch.complex128)).reshape(B, L, 1, *S)
+    assert rel(xh, xa) < TOL
+    # permuted user layout (coil first in k-space)
+    axis2 = AxisSpec(image=("B", "X", "Y"), kspace=("coil", "B", "K"), image_fft=("X", "Y"), coil="coil")
+    op2 = NUFFT(maps.to(cuda), traj.to(cuda), None, axis=axis2, config=NUFFTConfig(ndim=2, traj_units="rad"))
+    x2 = x[:, 0, 0]
+    y2 = op2.A(x2)
+    assert tuple(y2.shape) == (C, B, K)
+    assert rel(y2.permute(1, 0, 2), orc.A(x2.cpu().unsqueeze(1))) < TOL
+
+
+def test_errors_are_raised(cuda):
+    maps = _rand_c((2, 16, 16), 1, torch.complex64)
+    traj = phantoms.random_traj(2, 2, 100, seed=1)
+    ad = _adapter(maps, traj)
+    with pytest.raises(ValueError):
+        ad.A(torch.zeros((3, 1, 16, 16), dtype=torch.complex64, device=cuda))   # B mismatch
+    with pytest.raises(ValueError):
+        ad.AH(torch.zeros((2, 3, 100), dtype=torch.complex64, device=cuda))      # coil mismatch
+    with pytest.raises(ValueError):
+        ad.A(torch.zeros((2, 1, 16, 16), dtype=torch.complex64, device=cuda),
+             out=torch.zeros((2, 2, 99), dtype=torch.complex64, device=cuda))
+    with pytest.raises(RuntimeError):
+        ad.A(torch.zeros((2, 1, 16, 16), dtype=torch.complex64))                 # CPU tensor
+
+
+def test_coil_images_forward(cuda):
+    """Cin == C: per-coil images, maps not applied (torchkb.py:244-247)."""
+    C, S = 3, (16, 20)
+    maps = _rand_c((C,) + S, 31, torch.complex64)
+    traj = phantoms.random_traj(1, 2, 300, seed=32)
+    ad = _adapter(maps, traj)
+    xc = _rand_c((1, C) + S, 33)
+    y = ad.A(xc.to(cuda, torch.complex64))
+    orc = okb.KBNufft(torch.ones((1,) + S, dtype=torch.complex128), traj, None)
+    ya = torch.cat([orc.A(xc[:, c:c + 1]) for c in range(C)], dim=1)
+    assert rel(y, ya) < TOL

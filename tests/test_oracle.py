@@ -1,0 +1,98 @@
+"""The CPU oracle pinned against the reference's own outputs (golden fixtures)."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden, rel
+from oracle import kb as okb
+from oracle.nudft import nudft_forward, nudft_adjoint
+from oracle.tv import tv_energy_grad
+from oracle.ncg import NCGOracle, NCGConfig, TVSpec
+
+
+@pytest.mark.parametrize("case", ["2d_32", "2d_24x40", "3d_12x10x8"])
+def test_ptnufft_indices_bit_exact(case):
+    g = golden("ptnufft_idx.npz")
+    traj, G, idx = g[f"{case}_traj"], tuple(int(v) for v in g[f"{case}_grid"]), g[f"{case}_idx"]
+    for b in range(traj.shape[0]):
+        mine = okb.ptnufft_indices(traj[b], G, 4)
+        assert np.array_equal(mine.astype(np.int64), idx[b].astype(np.int64))
+
+
+def test_beta_matches_reference():
+    g = golden("ptnufft_idx.npz")
+    assert okb.kb_beta(4, 2.0) == pytest.approx(float(g["2d_32_beta"]), rel=0, abs=1e-12)
+
+
+def test_nudft_forward_matches_reference_ground_truth():
+    g = golden("nudft_a.npz")
+    maps, x = torch.from_numpy(g["maps"]), torch.from_numpy(g["x"])
+    traj, dcf = torch.from_numpy(g["traj"]), torch.from_numpy(g["dcf"])
+    y = nudft_forward(maps, x, traj, dcf)
+    assert rel(y, torch.from_numpy(g["y"])) < 1e-13
+
+
+def test_nudft_adjoint_is_true_adjoint():
+    g = golden("nudft_a.npz")
+    maps, x = torch.from_numpy(g["maps"]), torch.from_numpy(g["x"])
+    traj, dcf = torch.from_numpy(g["traj"]), torch.from_numpy(g["dcf"])
+    y = nudft_forward(maps, x, traj, dcf)
+    yy = torch.randn_like(y)
+    lhs = torch.vdot(y.reshape(-1), yy.reshape(-1))
+    rhs = torch.vdot(x.reshape(-1), nudft_adjoint(maps, yy, traj, dcf).reshape(-1))
+    assert abs(lhs / rhs - 1) < 1e-12
+
+
+@pytest.mark.parametrize("S", [(16, 20), (15, 17)])
+def test_kb_oracle_vs_nudft(S):
+    torch.manual_seed(0)
+    C, K = 2, 700
+    maps = torch.randn((C,) + S, dtype=torch.complex128)
+    traj = (torch.rand(1, 2, K) * 2 * math.pi - math.pi)
+    x = torch.randn((1, 1) + S, dtype=torch.complex128)
+    op = okb.KBNufft(maps, traj, None, norm="none")
+    assert rel(op.A(x), nudft_forward(maps, x, traj[0])) < 1.5e-3
+    yy = torch.randn((1, C, K), dtype=torch.complex128)
+    assert rel(op.AH(yy), nudft_adjoint(maps, yy, traj[0])) < 1.5e-3
+    lhs = torch.vdot(op.A(x).reshape(-1), yy.reshape(-1))
+    rhs = torch.vdot(x.reshape(-1), op.AH(yy).reshape(-1))
+    assert abs(lhs / rhs - 1) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["iso_sp", "aniso_sp", "aw_sp", "temporal", "iso_3ax"])
+@pytest.mark.parametrize("dt", ["c64", "c128"])
+def test_tv_oracle_matches_reference(name, dt):
+    g = golden("tv.npz")
+    x = torch.from_numpy(g[f"x_{dt}"])
+    axes = tuple(int(a) for a in g[f"{name}_axes"])
+    p = dict(iso_sp=(1e-3, 1e-3, True, None), aniso_sp=(2e-3, 1e-2, False, None),
+             aw_sp=(1e-3, 1e-3, True, (2.0, 0.5)), temporal=(5e-3, 1e-3, True, None),
+             iso_3ax=(3e-3, 1e-3, True, None))[name]
+    E, gr = tv_energy_grad(x, axes, p[0], p[1], p[2], p[3])
+    tol = 1e-5 if dt == "c64" else 1e-12
+    assert abs(float(E) - float(g[f"{name}_{dt}_E"])) <= tol * abs(float(g[f"{name}_{dt}_E"]))
+    assert rel(gr, torch.from_numpy(g[f"{name}_{dt}_g"])) < tol
+
+
+@pytest.mark.parametrize("run,direction,ls,iters", [("fr_armijo", "fr", "armijo", 12),
+                                                     ("prplus_armijo", "prplus", "armijo", 8),
+                                                     ("dy_armijo", "dy", "armijo", 8),
+                                                     ("fr_wolfe", "fr", "wolfe", 6)])
+def test_ncg_oracle_reproduces_reference_history(run, direction, ls, iters):
+    g = golden("ncg_small.npz")
+    maps, traj = torch.from_numpy(g["maps"]), torch.from_numpy(g["traj"])
+    y = torch.from_numpy(g["y"])
+    k = okb.KBNufft(maps, traj, None, dtype=torch.complex64, norm="ortho")
+    o = NCGOracle(lambda x: k.A(x).to(torch.complex64), lambda v: k.AH(v).to(torch.complex64), y,
+                  torch.zeros((y.shape[0], 1) + tuple(maps.shape[1:]), dtype=torch.complex64),
+                  [TVSpec((2, 3), 1e-3), TVSpec((0,), 5e-3)],
+                  NCGConfig(direction=direction, ls_name=ls, max_iter=iters, tol_g=0.0, tol_step=0.0))
+    o.run()
+    f_ref = g[f"{run}_f"]
+    assert len(o.hist) == len(f_ref)
+    np.testing.assert_allclose([h["f"] for h in o.hist], f_ref, rtol=2e-5)
+    np.testing.assert_array_equal([h["step"] for h in o.hist], g[f"{run}_step"])
+    np.testing.assert_allclose([h["xnorm"] for h in o.hist], g[f"{run}_xnorm"], rtol=1e-4)
+    assert rel(o.x, torch.from_numpy(g[f"{run}_x"])) < 1e-4
