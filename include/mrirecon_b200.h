@@ -42,6 +42,9 @@ enum { MRB_IDX_REFERENCE = 0, MRB_IDX_CORRECTED = 1 };
 
 int mrb_version(void);
 const char* mrb_last_error(void);
+/* Number of kernel launches this library has issued in the process (host
+ * side; a launch recorded into a CUDA graph counts once, at capture). */
+int64_t mrb_launch_count(void);
 
 /* ------------------------------------------------------------------------
  * NUFFT plan (Kaiser-Bessel, oversampled grid, SENSE coils, B frames)
@@ -88,6 +91,12 @@ int mrb_nufft_forward_coils(mrb_plan* plan, const void* x, void* y, int nb, mrb_
  * Replaces: TorchKbNUFFTAdapter.AH  graspcg/nufft/backends/torchkb.py:272-323 */
 int mrb_nufft_adjoint(mrb_plan* plan, const void* y, void* x, int nb, mrb_stream_t stream);
 
+/* One stage of the operators, for timing and tuning: stage 0 = pre-FFT
+ * (SENSE, deapodisation, zero-pad; x -> grid), 1 = forward FFT, 2 = interp
+ * (grid -> y), 3 = spread (y -> grid), 4 = inverse FFT, 5 = post-IFFT (crop,
+ * deapodisation, conj-maps coil sum; grid -> x).  The grid is the plan's. */
+int mrb_nufft_stage(mrb_plan* plan, int stage, const void* x, void* y, int nb, mrb_stream_t stream);
+
 /* Plan facts for tests and the bench (host copies, synchronous):
  * out[0] = number of spread entries, out[1] = tiles per frame,
  * out[2] = touched grid cells summed over frames, out[3] = spread tile edge,
@@ -106,6 +115,87 @@ int mrb_plan_cell_base(mrb_plan* plan, int32_t* out, mrb_stream_t stream);
  * integer-node, row-major table the operators use. */
 int mrb_grid_indices(const float* traj, int nd, const int* G, int64_t K, int W, int convention,
                      int64_t* idx, mrb_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Scratch for the FP64 reductions.  Every reducing entry point below takes
+ * a caller-owned device workspace `ws` of at least mrb_workspace_bytes()
+ * bytes (block partials); calls on one stream may share it.
+ * ---------------------------------------------------------------------- */
+int mrb_workspace_bytes(int64_t* bytes);
+
+/* out[j] = sum_i Re(conj(a_j[i]) * b_j[i]) / (diag_j ? diag_j[i % ndiag] : 1),
+ * FP64, j < npairs <= 8, n complex64 elements each; deterministic.
+ * Replaces: dot_real0 / dot_precond0  graspcg/numerics/utils.py:94-206
+ *           dot_chunked               graspcg/ops/dot.py:5-71 */
+int mrb_dots_f64(int64_t n, int npairs, const void* const* a, const void* const* b,
+                 const float* const* diag, int64_t ndiag, double* out, void* ws, mrb_stream_t stream);
+
+/* k-space passes over n complex64 samples (t from t_dev if non-NULL, else t_host;
+ * the pass is skipped when skip != NULL and *skip != 0):
+ *   mode 0: out[0..2] = |r|^2, Re<r,Ad>, |Ad|^2 (FP64)
+ *   mode 1: r = Ax + t*Ad - y (Ad may be NULL), out[0] = |r|^2
+ *   mode 2: r += t*Ad
+ * Replaces: _ker_residual_energy_  graspcg/ops/objective.py:31-45 */
+int mrb_kspace_pass(int mode, int64_t n, void* r, const void* Ad, const void* Ax, const void* y,
+                    const double* t_dev, double t_host, const double* skip, double* out, void* ws,
+                    mrb_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Regularisation: fused Huber-TV energy + gradient
+ * ---------------------------------------------------------------------- */
+typedef struct mrb_tv_term {
+  int enabled;
+  int isotropic;         /* l2 coupling across axes if non-zero */
+  float weight;          /* lambda */
+  float eps;             /* Huber knee */
+  int naxes;             /* <= 4 */
+  int axes[4];           /* axis ids of the (F, 1, *S) image: 0 = frame, 2.. = spatial */
+  float axis_weights[4]; /* per-axis scale of the forward differences */
+} mrb_tv_term;
+
+/* At z = x + t*d (d may be NULL) for an image (F, 1, *S) complex64 with
+ * nd spatial dims: g_out = g_base + t*g_dir - sum_T lambda_T div p_T
+ * (g_base/g_dir/g_out may be NULL), and FP64 reductions into out[0..10]:
+ *   out[0..3]  lambda_T * sum e_T for the enabled terms in order
+ *   out[4] Re<g,d>  out[5] <g,g/D>  out[6] |z|^2  out[7] |d|^2
+ *   out[8] <g_prev,g/D>  out[9] <g_prev,g_prev/D>  out[10] Re<d,g_prev>
+ * The pass is skipped when skip != NULL and (*skip == 0 if skip_if_zero
+ * else *skip != 0).
+ * Replaces: TVND.energy_grad_fixed_axes  graspcg/regularization/tv_nd.py:54-88
+ *           (stencils graspcg/ops/ndops.py:28-148), RegManager.energy_and_grad
+ *           graspcg/regularization/manager.py:38-142 for one shard, and the
+ *           reg/slope part of Objective.f_g_tensor graspcg/ops/objective.py:255-291 */
+int mrb_tv_grad(int nd, const int* S, int F, const mrb_tv_term* terms, int nterms, const void* x,
+                const void* d, const double* t_dev, double t_host, const void* g_base, const void* g_dir,
+                void* g_out, const float* diag, int64_t ndiag, const void* g_prev, const double* skip,
+                int skip_if_zero, double* out, void* ws, mrb_stream_t stream);
+
+/* Sum of the TV energies at z = x + ts[j]*d for j < J <= 24 (dev ts),
+ * out[j] (FP64); one pass over x and d.  Skipped when *skip != 0.
+ * Replaces the per-trial regulariser evaluations of the Armijo loop
+ * graspcg/numerics/line_search.py:57-72. */
+int mrb_tv_multi(int nd, const int* S, int F, const mrb_tv_term* terms, int nterms, const void* x,
+                 const void* d, const double* ts, int J, const double* skip, double* out, void* ws,
+                 mrb_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Device-resident NCG controller.  `slots` is a device array of
+ * mrb_ncg_slot_count() doubles (t, ls_ok, done, reason, iter, f0, g0d, ...);
+ * `cfg` is a DEVICE array of 10 doubles {c1, ls_beta, ls_max_iter (<= 23),
+ * max_iter, tol_g, tol_step, stop_window, stop_tol, direction (0 FR, 1 PR+,
+ * 2 DY), history rows}, read by the kernels (a captured graph sees edits).  Replaces CGSolver.run graspcg/solvers/cg.py:162-246,
+ * _armijo graspcg/numerics/line_search.py:24-79 and the directions of
+ * graspcg/numerics/directions.py:75-162 without host synchronisation.
+ * ---------------------------------------------------------------------- */
+int mrb_ncg_slot_count(int64_t* slots, int64_t* hist_cols);
+int mrb_ncg_set_steps(double* ts, int J, double beta, mrb_stream_t stream);
+int mrb_ncg_armijo_select(double* slots, const double* cfg, mrb_stream_t stream);
+int mrb_ncg_control(double* slots, double* hist, const double* cfg, int nterms, int have_ft,
+                    mrb_stream_t stream);
+int mrb_ncg_update(int64_t n, void* x, void* d, const void* g, void* gr, const void* gAd, void* g_prev,
+                   const float* diag, int64_t ndiag, double* slots, void* ws, mrb_stream_t stream);
+int mrb_ncg_steepest(int64_t n, void* d, const void* g, void* g_prev, const float* diag, int64_t ndiag,
+                     double* out, void* ws, mrb_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -41,6 +41,8 @@ class TVTerm(ct.Structure):
 _SIGS = {
     "mrb_version": (ct.c_int, []),
     "mrb_last_error": (ct.c_char_p, []),
+    "mrb_launch_count": (ct.c_int64, []),
+    "mrb_nufft_stage": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p]),
     "mrb_plan_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, c_int_p, ct.c_int, ct.c_int, ct.c_int64,
                                    ct.c_int, ct.c_double, ct.c_int]),
     "mrb_plan_destroy": (ct.c_int, [ct.c_void_p]),
@@ -55,6 +57,25 @@ _SIGS = {
     "mrb_plan_cell_base": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mrb_grid_indices": (ct.c_int, [ct.c_void_p, ct.c_int, c_int_p, ct.c_int64, ct.c_int, ct.c_int, ct.c_void_p,
                                     ct.c_void_p]),
+    "mrb_workspace_bytes": (ct.c_int, [c_int64_p]),
+    "mrb_dots_f64": (ct.c_int, [ct.c_int64, ct.c_int, ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_void_p),
+                                ct.POINTER(ct.c_void_p), ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mrb_kspace_pass": (ct.c_int, [ct.c_int, ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                   ct.c_void_p, ct.c_double, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mrb_tv_grad": (ct.c_int, [ct.c_int, c_int_p, ct.c_int, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p,
+                               ct.c_void_p, ct.c_double, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                               ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p,
+                               ct.c_void_p]),
+    "mrb_tv_multi": (ct.c_int, [ct.c_int, c_int_p, ct.c_int, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p,
+                                ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mrb_ncg_slot_count": (ct.c_int, [c_int64_p, c_int64_p]),
+    "mrb_ncg_set_steps": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double, ct.c_void_p]),
+    "mrb_ncg_armijo_select": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mrb_ncg_control": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p]),
+    "mrb_ncg_update": (ct.c_int, [ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                  ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mrb_ncg_steepest": (ct.c_int, [ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64,
+                                    ct.c_void_p, ct.c_void_p, ct.c_void_p]),
 }
 
 
@@ -96,6 +117,23 @@ def check(rc: int, what: str = "") -> None:
 
 def stream_ptr(device=None) -> int:
     return int(torch.cuda.current_stream(device).cuda_stream)
+
+
+def launch_count() -> int:
+    """Kernel launches issued by the library so far (graph captures count once)."""
+    return int(load().mrb_launch_count())
+
+
+def workspace_bytes() -> int:
+    v = ct.c_int64()
+    check(load().mrb_workspace_bytes(ct.byref(v)), "workspace_bytes")
+    return int(v.value)
+
+
+def ncg_slot_count():
+    a, b = ct.c_int64(), ct.c_int64()
+    check(load().mrb_ncg_slot_count(ct.byref(a), ct.byref(b)), "ncg_slot_count")
+    return int(a.value), int(b.value)
 
 
 def ptr(t) -> int:

@@ -1,6 +1,7 @@
 // Error state, KB polynomial set-up and version entry points.
 #include <cmath>
 #include <cstdarg>
+#include <atomic>
 #include <cstring>
 
 #include "mrb_common.cuh"
@@ -8,6 +9,9 @@
 namespace mrb {
 
 static thread_local char g_err[1024] = "";
+static std::atomic<long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -53,4 +57,5 @@ void kb_poly_init(KBPoly& p, int W, double beta) {
 }  // namespace mrb
 
 extern "C" int mrb_version(void) { return 1; }
+extern "C" int64_t mrb_launch_count(void) { return (int64_t)mrb::g_launches.load(); }
 extern "C" const char* mrb_last_error(void) { return mrb::g_err; }

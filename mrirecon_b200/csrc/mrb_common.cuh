@@ -24,7 +24,14 @@ int fail(int code, const char* fmt, ...);
                          cudaGetErrorString(_e));                                   \
   } while (0)
 
-#define MRB_LAUNCH_CHECK() MRB_CUDA_TRY(cudaGetLastError())
+// every kernel launch of the library goes through MRB_LAUNCH_CHECK, which also
+// counts it (host-side; launches recorded into a CUDA graph count once).
+void count_launch();
+#define MRB_LAUNCH_CHECK()          \
+  do {                              \
+    ::mrb::count_launch();          \
+    MRB_CUDA_TRY(cudaGetLastError()); \
+  } while (0)
 
 #define MRB_REQUIRE(cond, ...)                                                      \
   do {                                                                              \

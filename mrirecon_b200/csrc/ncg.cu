@@ -1,0 +1,871 @@
+// Objective, Huber-TV and NCG kernels for B200 (sm_100a).
+//
+// Image tensors are (F, 1, *S) complex64 (frames, size-1 coil slot, nd
+// spatial dims), k-space tensors (nb, C, K) complex64.  Regularisers are
+// evaluated at z = x + t*d without modifying x; all scalar reductions (dots,
+// energies, objective) are accumulated in FP64 with a fixed block partition
+// and a fixed final order, so results are bitwise reproducible.
+//
+// Reference semantics (graspcg = timodelgado/mrirecon):
+//   TV             regularization/tv_nd.py:54-88, ops/ndops.py:28-148
+//   objective      ops/objective.py:31-45, 184-291
+//   Armijo         numerics/line_search.py:24-79
+//   FR/PR+/DY      numerics/directions.py:75-162 (FR seeds rho_prev with the
+//                  current rho on its first update, so its first beta is 1)
+//   converged      solvers/utils.py:40-43
+//   history        solvers/utils.py:64-87 (running sums of the norms)
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "mrb_common.cuh"
+
+namespace {
+
+constexpr int RED_THREADS = 256;
+constexpr int RED_MAX_BLOCKS = 1184;   // 8 x 148 SMs
+constexpr int RED_MAX_VALS = 32;
+
+__host__ __device__ inline int red_blocks(long long n, int per_thread) {
+  long long b = (n + (long long)RED_THREADS * per_thread - 1) / ((long long)RED_THREADS * per_thread);
+  if (b < 1) b = 1;
+  if (b > RED_MAX_BLOCKS) b = RED_MAX_BLOCKS;
+  return (int)b;
+}
+
+// Block-level FP64 reduction of NV values; lane/warp order fixed.
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* __restrict__ partials) {
+  __shared__ double sh[RED_THREADS / 32][NV];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double s = v[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) sh[warp][j] = s;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    for (int j = 0; j < NV; ++j) {
+      double s = lane < RED_THREADS / 32 ? sh[lane][j] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (lane == 0) partials[(long long)blockIdx.x * NV + j] = s;
+    }
+  }
+}
+
+// out[j] (=|+=) sum over nblocks of partials[b][j]; one warp per value.
+__global__ void finalize_kernel(const double* __restrict__ partials, int nblocks, int stride, int nv,
+                                double* __restrict__ out, int accumulate, const double* __restrict__ skip) {
+  if (skip && *skip != 0.0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int j = warp; j < nv; j += blockDim.x >> 5) {
+    double s = 0.0;
+    for (int b = lane; b < nblocks; b += 32) s += partials[(long long)b * stride + j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) out[j] = accumulate ? out[j] + s : s;
+  }
+}
+
+// partials are laid out [block][stride]; the first nv values of each row are summed
+int finalize(const double* partials, int nblocks, int stride, int nv, double* out, int accumulate,
+             const double* skip, cudaStream_t st) {
+  finalize_kernel<<<1, 256, 0, st>>>(partials, nblocks, stride, nv, out, accumulate, skip);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+__device__ __forceinline__ double skipped(const double* flag) { return flag ? *flag : 0.0; }
+
+// ---------------------------------------------------------------------------
+// generic dots: out[j] = sum Re(conj(a_j) b_j) / diag_j
+// ---------------------------------------------------------------------------
+struct DotArgs {
+  const float2* a[8];
+  const float2* b[8];
+  const float* diag[8];
+  long long ndiag;
+  long long n;
+  int npairs;
+};
+
+template <int NP>
+__global__ void __launch_bounds__(RED_THREADS) dots_kernel(DotArgs a, double* __restrict__ partials) {
+  double acc[NP];
+#pragma unroll
+  for (int j = 0; j < NP; ++j) acc[j] = 0.0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+      float2 u = a.a[j][i], v = a.b[j][i];
+      float r = u.x * v.x + u.y * v.y;
+      if (a.diag[j]) r /= a.diag[j][i % a.ndiag];
+      acc[j] += (double)r;
+    }
+  }
+  block_reduce_store<NP>(acc, partials);
+}
+
+// ---------------------------------------------------------------------------
+// k-space passes
+// ---------------------------------------------------------------------------
+// mode 0: scalars e_rr = |r|^2, e_rd = Re<r,Ad>, e_dd = |Ad|^2
+// mode 1: r = Ax + t*Ad - y, returns |r|^2 (reference residual, objective.py:31-45)
+// mode 2: r += t*Ad (accepted step; t from the device), no reduction
+__global__ void __launch_bounds__(RED_THREADS) kspace_kernel(int mode, long long n, float2* __restrict__ r,
+                                                             const float2* __restrict__ Ad,
+                                                             const float2* __restrict__ Ax,
+                                                             const float2* __restrict__ y, const double* t_dev,
+                                                             double t_host, const double* skip,
+                                                             double* __restrict__ partials) {
+  double acc[3] = {0.0, 0.0, 0.0};
+  bool sk = skipped(skip) != 0.0;
+  float t = (float)(t_dev ? *t_dev : t_host);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (!sk) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+      if (mode == 0) {
+        float2 a = r[i], b = Ad[i];
+        acc[0] += (double)(a.x * a.x + a.y * a.y);
+        acc[1] += (double)(a.x * b.x + a.y * b.y);
+        acc[2] += (double)(b.x * b.x + b.y * b.y);
+      } else if (mode == 1) {
+        float2 d = Ad ? Ad[i] : make_float2(0.f, 0.f);
+        float2 a = Ax[i], yy = y[i];
+        // same operation order as the reference: r = Ad; r *= t; r += Ax; r -= y
+        float rx = __fadd_rn(__fadd_rn(__fmul_rn(d.x, t), a.x), -yy.x);
+        float ry = __fadd_rn(__fadd_rn(__fmul_rn(d.y, t), a.y), -yy.y);
+        r[i] = make_float2(rx, ry);
+        acc[0] += (double)(rx * rx + ry * ry);
+      } else {
+        float2 a = r[i], b = Ad[i];
+        a.x = fmaf(t, b.x, a.x);
+        a.y = fmaf(t, b.y, a.y);
+        r[i] = a;
+      }
+    }
+  }
+  if (mode == 2) return;
+  if (mode == 1) {
+    double v1[1] = {acc[0]};
+    block_reduce_store<1>(v1, partials);
+  } else {
+    block_reduce_store<3>(acc, partials);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Huber TV at z = x + t*d
+// ---------------------------------------------------------------------------
+// The terms are compiled on the host into
+//   slots: the distinct image axes the terms difference along (<= 4), and
+//   units: one per isotropic term, one per axis of an anisotropic term
+//          (<= 8), each with lambda, eps and a weight per slot (0 = unused).
+// A unit's energy density is sqrt(sum_s w_s^2 |D_s z|^2 + eps^2) - eps and its
+// flux p_s = w_s D_s z / max(sqrt(.), 1e-12) (ndops.py:66-135, tv_nd.py:59-86);
+// the gradient adds -lambda * sum_s (p_s(v) - p_s(v - e_s)), p_s(v - e_s) = 0
+// on the first slice (bwd_diff, ndops.py:45-59).  All loops run over the
+// compile-time maxima with runtime guards so every array stays in registers.
+constexpr int MAX_TERMS = 4;     // user-visible terms (energy slots out[0..3])
+constexpr int NSLOT = 4;
+constexpr int NUNIT = 8;
+
+struct TVPlan {
+  int F;
+  unsigned n;                    // voxels (F * prod S), < 2^31
+  int ns;                        // slots in use
+  unsigned stride[NSLOT];
+  int size[NSLOT];
+  int nu;                        // units in use
+  float w[NUNIT][NSLOT];         // per-slot weight of each unit (0 = not in unit)
+  float lam[NUNIT];
+  float eps[NUNIT];
+  int term_of[NUNIT];            // user term each unit belongs to
+  unsigned diag_mask;            // bit (s*NSLOT+s2): some unit couples slots s and s2
+};
+
+__device__ __forceinline__ float2 zload(const float2* __restrict__ x, const float2* __restrict__ d, float t,
+                                        unsigned i) {
+  float2 v = x[i];
+  if (d) {
+    float2 w = d[i];
+    v.x = fmaf(t, w.x, v.x);
+    v.y = fmaf(t, w.y, v.y);
+  }
+  return v;
+}
+
+// Gradient pass: g_out = g_base + t*g_dir - sum_u lam_u div p_u  at z = x + t d,
+// with FP64 reductions:
+//   slot 0..MAX_TERMS-1  E_T = lam_T * sum e_T
+//   then gdot = Re<g,d>, rho = <g,g/D>, zn2 = |z|^2, dn2 = |d|^2,
+//        gpg = <g_prev,g/D>, gpgp = <g_prev,g_prev/D>, dgp = Re<d,g_prev>
+constexpr int GP_NV = MAX_TERMS + 7;
+
+struct GradArgs {
+  const float2* x;
+  const float2* d;
+  const double* t_dev;
+  double t_host;
+  const float2* g_base;
+  const float2* g_dir;
+  float2* g_out;
+  const float* diag;     // (ndiag) broadcast, or null
+  long long ndiag;
+  const float2* g_prev;
+  const double* skip;
+  int skip_if_zero;
+};
+
+__global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P, double* __restrict__ partials) {
+  double acc[GP_NV];
+#pragma unroll
+  for (int j = 0; j < GP_NV; ++j) acc[j] = 0.0;
+  bool sk = false;
+  if (a.skip) sk = a.skip_if_zero ? (*a.skip == 0.0) : (*a.skip != 0.0);
+  const float t = (float)(a.t_dev ? *a.t_dev : a.t_host);
+  const unsigned stride_all = gridDim.x * blockDim.x;
+  if (!sk) {
+    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < P.n; v += stride_all) {
+      int c[NSLOT];
+      bool hn[NSLOT], hp[NSLOT];
+      float2 zn[NSLOT], zp[NSLOT];
+      const float2 zv = zload(a.x, a.d, t, v);
+#pragma unroll
+      for (int s = 0; s < NSLOT; ++s) {
+        c[s] = 0;
+        hn[s] = hp[s] = false;
+        zn[s] = zp[s] = make_float2(0.f, 0.f);
+        if (s < P.ns) {
+          c[s] = (int)((v / P.stride[s]) % (unsigned)P.size[s]);
+          hn[s] = c[s] + 1 < P.size[s];
+          hp[s] = c[s] > 0;
+          if (hn[s]) zn[s] = zload(a.x, a.d, t, v + P.stride[s]);
+          if (hp[s]) zp[s] = zload(a.x, a.d, t, v - P.stride[s]);
+        }
+      }
+      // forward differences at v
+      float2 D[NSLOT];
+#pragma unroll
+      for (int s = 0; s < NSLOT; ++s)
+        D[s] = hn[s] ? make_float2(zn[s].x - zv.x, zn[s].y - zv.y) : make_float2(0.f, 0.f);
+      // forward differences at v - e_s, along every slot s2: Dp[s][s2]
+      float2 Dp[NSLOT][NSLOT];
+#pragma unroll
+      for (int s = 0; s < NSLOT; ++s) {
+#pragma unroll
+        for (int s2 = 0; s2 < NSLOT; ++s2) {
+          Dp[s][s2] = make_float2(0.f, 0.f);
+          if (!hp[s]) continue;
+          if (s2 == s) {
+            Dp[s][s2] = make_float2(zv.x - zp[s].x, zv.y - zp[s].y);
+          } else if ((P.diag_mask >> (s * NSLOT + s2)) & 1u) {
+            if (hn[s2]) {
+              float2 zd = zload(a.x, a.d, t, v - P.stride[s] + P.stride[s2]);
+              Dp[s][s2] = make_float2(zd.x - zp[s].x, zd.y - zp[s].y);
+            }
+          }
+        }
+      }
+      float gx = 0.f, gy = 0.f;
+      if (a.g_base) { float2 b = a.g_base[v]; gx = b.x; gy = b.y; }
+      if (a.g_dir) { float2 b = a.g_dir[v]; gx = fmaf(t, b.x, gx); gy = fmaf(t, b.y, gy); }
+#pragma unroll
+      for (int u = 0; u < NUNIT; ++u) {
+        if (u >= P.nu) continue;
+        const float e2 = P.eps[u] * P.eps[u];
+        float ss = 0.f;
+#pragma unroll
+        for (int s = 0; s < NSLOT; ++s) {
+          const float w = P.w[u][s];
+          float2 q = make_float2(w * D[s].x, w * D[s].y);
+          ss += q.x * q.x + q.y * q.y;
+        }
+        const float den = sqrtf(ss + e2);
+        const float inv = 1.f / fmaxf(den, 1e-12f);
+        const int ti = P.term_of[u];
+#pragma unroll
+        for (int tt = 0; tt < MAX_TERMS; ++tt)
+          if (tt == ti) acc[tt] += (double)(P.lam[u] * (den - P.eps[u]));
+        float dx = 0.f, dy = 0.f;
+#pragma unroll
+        for (int s = 0; s < NSLOT; ++s) {
+          const float w = P.w[u][s];
+          if (w == 0.f) continue;
+          dx += w * D[s].x * inv;
+          dy += w * D[s].y * inv;
+          if (hp[s]) {
+            float ssp = 0.f;
+#pragma unroll
+            for (int s2 = 0; s2 < NSLOT; ++s2) {
+              const float w2 = P.w[u][s2];
+              float2 q = make_float2(w2 * Dp[s][s2].x, w2 * Dp[s][s2].y);
+              ssp += q.x * q.x + q.y * q.y;
+            }
+            const float invp = 1.f / fmaxf(sqrtf(ssp + e2), 1e-12f);
+            dx -= w * Dp[s][s].x * invp;
+            dy -= w * Dp[s][s].y * invp;
+          }
+        }
+        gx = fmaf(-P.lam[u], dx, gx);
+        gy = fmaf(-P.lam[u], dy, gy);
+      }
+      if (a.g_out) a.g_out[v] = make_float2(gx, gy);
+      float2 dv = a.d ? a.d[v] : make_float2(0.f, 0.f);
+      const float Dv = a.diag ? a.diag[v % a.ndiag] : 1.f;
+      const int o = MAX_TERMS;
+      acc[o + 0] += (double)(gx * dv.x + gy * dv.y);
+      acc[o + 1] += (double)((gx * gx + gy * gy) / Dv);
+      acc[o + 2] += (double)(zv.x * zv.x + zv.y * zv.y);
+      acc[o + 3] += (double)(dv.x * dv.x + dv.y * dv.y);
+      if (a.g_prev) {
+        float2 gp = a.g_prev[v];
+        acc[o + 4] += (double)((gp.x * gx + gp.y * gy) / Dv);
+        acc[o + 5] += (double)((gp.x * gp.x + gp.y * gp.y) / Dv);
+        acc[o + 6] += (double)(dv.x * gp.x + dv.y * gp.y);
+      }
+    }
+  }
+  block_reduce_store<GP_NV>(acc, partials);
+}
+
+// Sum of all unit energies at z = x + t_j d for J <= MT_MAX_J step sizes, one
+// pass: per slot the differences A = D x, B = D d are loaded once and
+// D z(t_j) = A + t_j B is formed in registers for every t_j.
+constexpr int MT_MAX_J = 24;
+
+__global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __restrict__ x,
+                                                               const float2* __restrict__ d,
+                                                               const double* __restrict__ ts, int J, TVPlan P,
+                                                               const double* skip, double* __restrict__ partials) {
+  double acc[MT_MAX_J];
+#pragma unroll
+  for (int j = 0; j < MT_MAX_J; ++j) acc[j] = 0.0;
+  const bool sk = skipped(skip) != 0.0;
+  float tf[MT_MAX_J];
+#pragma unroll
+  for (int j = 0; j < MT_MAX_J; ++j) tf[j] = j < J ? (float)ts[j] : 0.f;
+  const unsigned stride_all = gridDim.x * blockDim.x;
+  if (!sk) {
+    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < P.n; v += stride_all) {
+      const float2 xv = x[v], dv = d[v];
+      float2 A[NSLOT], B[NSLOT];
+#pragma unroll
+      for (int s = 0; s < NSLOT; ++s) {
+        A[s] = B[s] = make_float2(0.f, 0.f);
+        if (s < P.ns) {
+          int c = (int)((v / P.stride[s]) % (unsigned)P.size[s]);
+          if (c + 1 < P.size[s]) {
+            float2 xn = x[v + P.stride[s]], dn = d[v + P.stride[s]];
+            A[s] = make_float2(xn.x - xv.x, xn.y - xv.y);
+            B[s] = make_float2(dn.x - dv.x, dn.y - dv.y);
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < MT_MAX_J; ++j) {
+        if (j >= J) continue;
+        const float t = tf[j];
+        float m[NSLOT];
+#pragma unroll
+        for (int s = 0; s < NSLOT; ++s) {
+          float ax = fmaf(t, B[s].x, A[s].x), ay = fmaf(t, B[s].y, A[s].y);
+          m[s] = ax * ax + ay * ay;
+        }
+        float e = 0.f;
+#pragma unroll
+        for (int u = 0; u < NUNIT; ++u) {
+          if (u >= P.nu) continue;
+          float ss = 0.f;
+#pragma unroll
+          for (int s = 0; s < NSLOT; ++s) ss = fmaf(P.w[u][s] * P.w[u][s], m[s], ss);
+          e += P.lam[u] * (sqrtf(ss + P.eps[u] * P.eps[u]) - P.eps[u]);
+        }
+        acc[j] += (double)e;
+      }
+    }
+  }
+  block_reduce_store<MT_MAX_J>(acc, partials);
+}
+
+// ---------------------------------------------------------------------------
+// NCG controller kernels (single thread; scalar slots in `s`)
+// ---------------------------------------------------------------------------
+enum Slot {
+  S_T = 0, S_LS_OK, S_DONE, S_REASON, S_ITER, S_F0, S_G0D, S_FT, S_GDT,
+  S_ERR, S_ERD, S_EDD, S_RHO_PREV, S_RHO_INIT, S_BETA,
+  S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL,
+  S_RED = 24,            // reduction outputs of the gradient pass (GP_NV values)
+  S_EJ = 48,             // multi-t energies (MT_MAX_J values)
+  S_G0D_NEXT = 80,
+  S_COUNT = 96
+};
+
+struct NCGCfg {
+  double c1;
+  double ls_beta;
+  int ls_max_iter;
+  int max_iter;
+  double tol_g;
+  double tol_step;
+  int stop_window;       // 0 = off
+  double stop_tol;
+  int direction;         // 0 FR, 1 PR+, 2 DY
+  int nhist;             // history row capacity
+};
+
+constexpr int HIST_COLS = 11;  // f0, gdot0, gdot_t, t, cum_x, cum_g, cum_s, xn, gn, sn, f_t
+
+// cfg lives in device memory (so a captured graph sees later edits)
+__device__ __forceinline__ NCGCfg load_cfg(const double* c) {
+  NCGCfg g;
+  g.c1 = c[0];
+  g.ls_beta = c[1];
+  g.ls_max_iter = (int)c[2];
+  g.max_iter = (int)c[3];
+  g.tol_g = c[4];
+  g.tol_step = c[5];
+  g.stop_window = (int)c[6];
+  g.stop_tol = c[7];
+  g.direction = (int)c[8];
+  g.nhist = (int)c[9];
+  return g;
+}
+
+// Armijo selection on the multi-t energies: t_0 = 0, t_j = beta^(j-1).
+__global__ void armijo_select_kernel(double* s, const double* cfg_dev) {
+  if (threadIdx.x != 0) return;
+  const NCGCfg cfg = load_cfg(cfg_dev);
+  if (s[S_DONE] != 0.0) {
+    s[S_LS_OK] = 0.0;
+    return;
+  }
+  const double err = s[S_ERR], erd = s[S_ERD], edd = s[S_EDD];
+  const double f0 = 0.5 * err + s[S_EJ + 0];
+  const double g0d = s[S_G0D];
+  s[S_F0] = f0;
+  bool bad = !(g0d < 0.0) || isnan(g0d) || isinf(g0d);
+  if (bad) {
+    s[S_LS_OK] = 0.0;
+    s[S_DONE] = 1.0;
+    s[S_REASON] = 1.0;
+    s[S_T] = 0.0;
+    return;
+  }
+  double t = 1.0;
+  const int jmax = cfg.ls_max_iter < MT_MAX_J - 1 ? cfg.ls_max_iter : MT_MAX_J - 1;
+  for (int j = 1; j <= jmax; ++j) {
+    double ft = 0.5 * (err + 2.0 * t * erd + t * t * edd) + s[S_EJ + j];
+    if (ft <= f0 + cfg.c1 * t * g0d) {
+      s[S_T] = t;
+      s[S_FT] = ft;
+      s[S_LS_OK] = 1.0;
+      s[S_NTRIAL] = (double)j;
+      return;
+    }
+    t *= cfg.ls_beta;
+  }
+  s[S_T] = t;
+  s[S_LS_OK] = 0.0;
+  s[S_DONE] = 1.0;
+  s[S_REASON] = 1.0;
+}
+
+// After the gradient pass at the accepted t: history row, stopping tests and
+// the direction coefficient beta.
+__global__ void ncg_control_kernel(double* s, double* hist, const double* cfg_dev, int nterms, int have_ft) {
+  if (threadIdx.x != 0) return;
+  const NCGCfg cfg = load_cfg(cfg_dev);
+  if (s[S_LS_OK] == 0.0) return;
+  const double* r = s + S_RED;
+  double Esum = 0.0;
+  for (int i = 0; i < nterms; ++i) Esum += r[i];
+  const double gdot = r[MAX_TERMS + 0], rho = r[MAX_TERMS + 1];
+  const double xn = sqrt(fmax(r[MAX_TERMS + 2], 0.0)), sn = sqrt(fmax(r[MAX_TERMS + 3], 0.0));
+  const double gn = sqrt(fmax(rho, 0.0));
+  if (!have_ft) {
+    // objective at the accepted point from the k-space scalars
+    double t = s[S_T];
+    s[S_FT] = 0.5 * (s[S_ERR] + 2.0 * t * s[S_ERD] + t * t * s[S_EDD]) + Esum;
+  }
+  s[S_GDT] = gdot;
+  s[S_CUM_X] += xn;
+  s[S_CUM_G] += gn;
+  s[S_CUM_S] += sn;
+  int k = (int)s[S_ITER];
+  if (k < cfg.nhist) {
+    double* h = hist + (long long)k * HIST_COLS;
+    h[0] = s[S_F0];
+    h[1] = s[S_G0D];
+    h[2] = gdot;
+    h[3] = s[S_T];
+    h[4] = s[S_CUM_X];
+    h[5] = s[S_CUM_G];
+    h[6] = s[S_CUM_S];
+    h[7] = xn;
+    h[8] = gn;
+    h[9] = sn;
+    h[10] = s[S_FT];
+  }
+  s[S_ITER] = (double)(k + 1);
+  // reference convergence test (solvers/utils.py:40-43)
+  if (gn <= (1.0 + xn) * cfg.tol_g && sn <= (1.0 + xn) * cfg.tol_step) {
+    s[S_DONE] = 1.0;
+    s[S_REASON] = 2.0;
+    return;
+  }
+  // windowed relative objective change on the accepted objectives
+  if (cfg.stop_window > 0 && k + 1 >= cfg.stop_window && k < cfg.nhist) {
+    double fk = hist[(long long)k * HIST_COLS + 10];
+    int kk = k + 1 - cfg.stop_window;    // accepted-objective index kk-1 ... use f0 of row kk
+    double fw = hist[(long long)kk * HIST_COLS + 0];
+    if ((fw - fk) <= cfg.stop_window * cfg.stop_tol * fabs(fk)) {
+      s[S_DONE] = 1.0;
+      s[S_REASON] = 3.0;
+      return;
+    }
+  }
+  if (k + 1 >= cfg.max_iter) {
+    s[S_DONE] = 1.0;
+    s[S_REASON] = 4.0;
+    return;
+  }
+  double beta;
+  if (cfg.direction == 0) {
+    if (s[S_RHO_INIT] == 0.0) {
+      s[S_RHO_PREV] = rho;
+      s[S_RHO_INIT] = 1.0;
+    }
+    beta = rho / fmax(s[S_RHO_PREV], 1e-20);
+    s[S_RHO_PREV] = rho;
+  } else if (cfg.direction == 1) {
+    double num = rho - r[MAX_TERMS + 4];
+    double den = r[MAX_TERMS + 5];
+    beta = fmax(num / fmax(den, 1e-20), 0.0);
+  } else {
+    double num = rho;
+    double den = gdot - r[MAX_TERMS + 6];
+    beta = num / fmax(den, 1e-20);
+  }
+  s[S_BETA] = beta;
+}
+
+// Accept + direction update (one pass):
+//   x += t d ; gr += t gAd (if gr) ; then, unless done: d = beta d - g/D,
+//   g_prev = g (if g_prev), and Re<g, d_new> for the next slope at t = 0.
+__global__ void __launch_bounds__(RED_THREADS) ncg_update_kernel(long long n, float2* __restrict__ x,
+                                                                 float2* __restrict__ d,
+                                                                 const float2* __restrict__ g,
+                                                                 float2* __restrict__ gr,
+                                                                 const float2* __restrict__ gAd,
+                                                                 float2* __restrict__ g_prev,
+                                                                 const float* __restrict__ diag, long long ndiag,
+                                                                 const double* __restrict__ s,
+                                                                 double* __restrict__ partials) {
+  double acc[1] = {0.0};
+  const bool ok = s[S_LS_OK] != 0.0;
+  const bool upd_dir = ok && s[S_DONE] == 0.0;
+  const float t = (float)s[S_T];
+  const float beta = (float)s[S_BETA];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (ok) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+      float2 dv = d[i];
+      float2 xv = x[i];
+      // x.add_(d * t) (cg.py:205-207)
+      xv.x = __fadd_rn(xv.x, __fmul_rn(dv.x, t));
+      xv.y = __fadd_rn(xv.y, __fmul_rn(dv.y, t));
+      x[i] = xv;
+      if (gr) {
+        float2 a = gr[i], b = gAd[i];
+        a.x = fmaf(t, b.x, a.x);
+        a.y = fmaf(t, b.y, a.y);
+        gr[i] = a;
+      }
+      if (upd_dir) {
+        float2 gv = g[i];
+        float Dv = diag ? diag[i % ndiag] : 1.f;
+        // d.mul_(beta); d.addcdiv_(g, D, value=-1)  (directions.py:158-161)
+        float nx = __fadd_rn(__fmul_rn(dv.x, beta), -(gv.x / Dv));
+        float ny = __fadd_rn(__fmul_rn(dv.y, beta), -(gv.y / Dv));
+        d[i] = make_float2(nx, ny);
+        if (g_prev) g_prev[i] = gv;
+        acc[0] += (double)(gv.x * nx + gv.y * ny);
+      }
+    }
+  }
+  block_reduce_store<1>(acc, partials);
+}
+
+// d = -g/D (priming: cg.py:182-185) and Re<g,d>
+__global__ void __launch_bounds__(RED_THREADS) steepest_kernel(long long n, float2* __restrict__ d,
+                                                               const float2* __restrict__ g,
+                                                               float2* __restrict__ g_prev,
+                                                               const float* __restrict__ diag, long long ndiag,
+                                                               double* __restrict__ partials) {
+  double acc[1] = {0.0};
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    float2 gv = g[i];
+    float Dv = diag ? diag[i % ndiag] : 1.f;
+    float2 dv = make_float2(-(gv.x / Dv), -(gv.y / Dv));
+    d[i] = dv;
+    if (g_prev) g_prev[i] = gv;
+    acc[0] += (double)(gv.x * dv.x + gv.y * dv.y);
+  }
+  block_reduce_store<1>(acc, partials);
+}
+
+__global__ void copy_slot_kernel(double* s, int dst, int src) {
+  if (threadIdx.x == 0) s[dst] = s[src];
+}
+
+__global__ void set_steps_kernel(double* ts, int J, double beta) {
+  if (threadIdx.x == 0) {
+    ts[0] = 0.0;
+    double t = 1.0;
+    for (int j = 1; j < J; ++j) {
+      ts[j] = t;
+      t *= beta;
+    }
+  }
+}
+
+int build_plan(TVPlan& P, int nd, const int* S, int F, const mrb_tv_term* terms, int nterms) {
+  MRB_REQUIRE(nd >= 1 && nd <= 3, "spatial nd must be 1..3");
+  MRB_REQUIRE(F >= 1, "frames must be positive");
+  MRB_REQUIRE(nterms >= 0 && nterms <= MAX_TERMS, "at most %d TV terms", MAX_TERMS);
+  MRB_REQUIRE(nterms == 0 || terms != nullptr, "null terms");
+  memset(&P, 0, sizeof(P));
+  P.F = F;
+  // axis geometry of (F, 1, *S): axis 0 = frames, 2.. = spatial
+  long long astride[5] = {0, 0, 0, 0, 0};
+  int asize[5] = {F, 1, 1, 1, 1};
+  long long st = 1;
+  for (int a = 2 + nd - 1; a >= 2; --a) {
+    MRB_REQUIRE(S[a - 2] >= 1, "bad spatial size");
+    asize[a] = S[a - 2];
+    astride[a] = st;
+    st *= S[a - 2];
+  }
+  astride[0] = st;
+  long long n = st * F;
+  MRB_REQUIRE(n < (1LL << 31), "image too large for the TV kernels (%lld voxels)", n);
+  P.n = (unsigned)n;
+  int slot_of[5] = {-1, -1, -1, -1, -1};
+  int k = 0;
+  for (int i = 0; i < nterms; ++i) {
+    const mrb_tv_term& t = terms[i];
+    if (!t.enabled || t.weight == 0.f) continue;
+    MRB_REQUIRE(t.naxes >= 0 && t.naxes <= 4, "at most 4 axes per TV term");
+    int ax[4], na = 0;
+    float aw[4];
+    for (int q = 0; q < t.naxes; ++q) {
+      int a = t.axes[q];
+      MRB_REQUIRE(a >= 0 && a < 2 + nd, "TV axis %d out of range", a);
+      if (a == 1 || asize[a] == 1) continue;      // size-1 axis: forward difference is zero
+      if (slot_of[a] < 0) {
+        MRB_REQUIRE(P.ns < NSLOT, "too many distinct TV axes");
+        slot_of[a] = P.ns;
+        P.stride[P.ns] = (unsigned)astride[a];
+        P.size[P.ns] = asize[a];
+        P.ns++;
+      }
+      ax[na] = slot_of[a];
+      aw[na] = t.axis_weights[q];
+      ++na;
+    }
+    if (na == 0) continue;
+    if (t.isotropic) {
+      MRB_REQUIRE(P.nu < NUNIT, "too many TV units");
+      int u = P.nu++;
+      P.lam[u] = t.weight;
+      P.eps[u] = t.eps;
+      P.term_of[u] = k;
+      for (int q = 0; q < na; ++q) P.w[u][ax[q]] = aw[q];
+      for (int q = 0; q < na; ++q)
+        for (int q2 = 0; q2 < na; ++q2)
+          if (ax[q] != ax[q2]) P.diag_mask |= 1u << (ax[q] * NSLOT + ax[q2]);
+    } else {
+      for (int q = 0; q < na; ++q) {
+        MRB_REQUIRE(P.nu < NUNIT, "too many TV units");
+        int u = P.nu++;
+        P.lam[u] = t.weight;
+        P.eps[u] = t.eps;
+        P.term_of[u] = k;
+        P.w[u][ax[q]] = aw[q];
+      }
+    }
+    ++k;
+  }
+  return 0;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" int mrb_workspace_bytes(int64_t* bytes) {
+  MRB_REQUIRE(bytes != nullptr, "null pointer");
+  *bytes = (int64_t)RED_MAX_BLOCKS * RED_MAX_VALS * sizeof(double);
+  return 0;
+}
+
+extern "C" int mrb_ncg_slot_count(int64_t* slots, int64_t* hist_cols) {
+  MRB_REQUIRE(slots != nullptr && hist_cols != nullptr, "null pointer");
+  *slots = S_COUNT;
+  *hist_cols = HIST_COLS;
+  return 0;
+}
+
+extern "C" int mrb_dots_f64(int64_t n, int npairs, const void* const* a, const void* const* b,
+                            const float* const* diag, int64_t ndiag, double* out, void* ws, mrb_stream_t stream) {
+  MRB_REQUIRE(n >= 0 && npairs >= 1 && npairs <= 8, "npairs must be 1..8");
+  MRB_REQUIRE(a && b && out && ws, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  DotArgs d{};
+  for (int j = 0; j < npairs; ++j) {
+    MRB_REQUIRE(a[j] && b[j], "null operand %d", j);
+    d.a[j] = (const float2*)a[j];
+    d.b[j] = (const float2*)b[j];
+    d.diag[j] = diag ? diag[j] : nullptr;
+  }
+  d.ndiag = ndiag > 0 ? ndiag : 1;
+  d.n = n;
+  d.npairs = npairs;
+  int nb = red_blocks(n, 4);
+  double* part = (double*)ws;
+  switch (npairs) {
+    case 1: dots_kernel<1><<<nb, RED_THREADS, 0, st>>>(d, part); break;
+    case 2: dots_kernel<2><<<nb, RED_THREADS, 0, st>>>(d, part); break;
+    case 3: dots_kernel<3><<<nb, RED_THREADS, 0, st>>>(d, part); break;
+    case 4: dots_kernel<4><<<nb, RED_THREADS, 0, st>>>(d, part); break;
+    default: dots_kernel<8><<<nb, RED_THREADS, 0, st>>>(d, part); break;
+  }
+  MRB_LAUNCH_CHECK();
+  const int stride = npairs <= 4 ? npairs : 8;
+  return finalize(part, nb, stride, npairs, out, 0, nullptr, st);
+}
+
+extern "C" int mrb_kspace_pass(int mode, int64_t n, void* r, const void* Ad, const void* Ax, const void* y,
+                               const double* t_dev, double t_host, const double* skip, double* out, void* ws,
+                               mrb_stream_t stream) {
+  MRB_REQUIRE(mode >= 0 && mode <= 2, "bad k-space mode");
+  MRB_REQUIRE(r != nullptr && ws != nullptr, "null pointer");
+  MRB_REQUIRE(mode != 1 || (Ax && y), "mode 1 needs Ax and y");
+  MRB_REQUIRE(mode == 1 || Ad, "modes 0/2 need Ad");
+  MRB_REQUIRE(mode == 2 || out, "null output");
+  cudaStream_t st = (cudaStream_t)stream;
+  int nb = red_blocks(n, 4);
+  double* part = (double*)ws;
+  kspace_kernel<<<nb, RED_THREADS, 0, st>>>(mode, n, (float2*)r, (const float2*)Ad, (const float2*)Ax,
+                                            (const float2*)y, t_dev, t_host, skip, part);
+  MRB_LAUNCH_CHECK();
+  if (mode == 2) return 0;
+  return finalize(part, nb, mode == 0 ? 3 : 1, mode == 0 ? 3 : 1, out, 0, skip, st);
+}
+
+extern "C" int mrb_tv_grad(int nd, const int* S, int F, const mrb_tv_term* terms, int nterms, const void* x,
+                           const void* d, const double* t_dev, double t_host, const void* g_base, const void* g_dir,
+                           void* g_out, const float* diag, int64_t ndiag, const void* g_prev, const double* skip,
+                           int skip_if_zero, double* out, void* ws, mrb_stream_t stream) {
+  MRB_REQUIRE(x != nullptr && out != nullptr && ws != nullptr, "null pointer");
+  TVPlan P;
+  int rc = build_plan(P, nd, S, F, terms, nterms);
+  if (rc) return rc;
+  GradArgs a{};
+  a.x = (const float2*)x;
+  a.d = (const float2*)d;
+  a.t_dev = t_dev;
+  a.t_host = t_host;
+  a.g_base = (const float2*)g_base;
+  a.g_dir = (const float2*)g_dir;
+  a.g_out = (float2*)g_out;
+  a.diag = diag;
+  a.ndiag = ndiag > 0 ? ndiag : 1;
+  a.g_prev = (const float2*)g_prev;
+  a.skip = skip;
+  a.skip_if_zero = skip_if_zero;
+  cudaStream_t st = (cudaStream_t)stream;
+  int nb = red_blocks(P.n, 2);
+  double* part = (double*)ws;
+  grad_kernel<<<nb, RED_THREADS, 0, st>>>(a, P, part);
+  MRB_LAUNCH_CHECK();
+  return finalize(part, nb, GP_NV, GP_NV, out, 0, nullptr, st);
+}
+
+extern "C" int mrb_tv_multi(int nd, const int* S, int F, const mrb_tv_term* terms, int nterms, const void* x,
+                            const void* d, const double* ts, int J, const double* skip, double* out, void* ws,
+                            mrb_stream_t stream) {
+  MRB_REQUIRE(x != nullptr && d != nullptr && ts != nullptr && out != nullptr && ws != nullptr, "null pointer");
+  MRB_REQUIRE(J >= 1 && J <= MT_MAX_J, "J must be 1..%d", MT_MAX_J);
+  TVPlan P;
+  int rc = build_plan(P, nd, S, F, terms, nterms);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  int nb = red_blocks(P.n, 2);
+  double* part = (double*)ws;
+  tv_multi_kernel<<<nb, RED_THREADS, 0, st>>>((const float2*)x, (const float2*)d, ts, J, P, skip, part);
+  MRB_LAUNCH_CHECK();
+  return finalize(part, nb, MT_MAX_J, J, out, 0, skip, st);
+}
+
+extern "C" int mrb_ncg_armijo_select(double* slots, const double* cfg, mrb_stream_t stream) {
+  MRB_REQUIRE(slots != nullptr && cfg != nullptr, "null pointer");
+  armijo_select_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slots, cfg);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_ncg_control(double* slots, double* hist, const double* cfg, int nterms, int have_ft,
+                               mrb_stream_t stream) {
+  MRB_REQUIRE(slots != nullptr && hist != nullptr && cfg != nullptr, "null pointer");
+  ncg_control_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slots, hist, cfg, nterms, have_ft);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_ncg_update(int64_t n, void* x, void* d, const void* g, void* gr, const void* gAd, void* g_prev,
+                              const float* diag, int64_t ndiag, double* slots, void* ws, mrb_stream_t stream) {
+  MRB_REQUIRE(x && d && g && slots && ws, "null pointer");
+  MRB_REQUIRE(!gr || gAd, "gr needs gAd");
+  cudaStream_t st = (cudaStream_t)stream;
+  int nb = red_blocks(n, 2);
+  double* part = (double*)ws;
+  ncg_update_kernel<<<nb, RED_THREADS, 0, st>>>(n, (float2*)x, (float2*)d, (const float2*)g, (float2*)gr,
+                                                 (const float2*)gAd, (float2*)g_prev, diag, ndiag > 0 ? ndiag : 1,
+                                                 slots, part);
+  MRB_LAUNCH_CHECK();
+  // next slope at t = 0 -> S_G0D_NEXT, then S_G0D (skipped when not updated)
+  int rc = finalize(part, nb, 1, 1, slots + S_G0D_NEXT, 0, nullptr, st);
+  if (rc) return rc;
+  copy_slot_kernel<<<1, 32, 0, st>>>(slots, S_G0D, S_G0D_NEXT);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_ncg_steepest(int64_t n, void* d, const void* g, void* g_prev, const float* diag, int64_t ndiag,
+                                double* out, void* ws, mrb_stream_t stream) {
+  MRB_REQUIRE(d && g && out && ws, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  int nb = red_blocks(n, 2);
+  double* part = (double*)ws;
+  steepest_kernel<<<nb, RED_THREADS, 0, st>>>(n, (float2*)d, (const float2*)g, (float2*)g_prev, diag,
+                                               ndiag > 0 ? ndiag : 1, part);
+  MRB_LAUNCH_CHECK();
+  return finalize(part, nb, 1, 1, out, 0, nullptr, st);
+}
+
+extern "C" int mrb_ncg_set_steps(double* ts, int J, double beta, mrb_stream_t stream) {
+  MRB_REQUIRE(ts != nullptr && J >= 1 && J <= MT_MAX_J, "bad step table");
+  set_steps_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(ts, J, beta);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}

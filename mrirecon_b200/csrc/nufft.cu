@@ -65,6 +65,7 @@ struct mrb_plan {
   cufftHandle fft = 0;
   int fft_batch = 0;
   DevBuf tmp;         // scratch for set_points
+  size_t spread_smem_set = 0;   // dynamic smem opt-in already granted
 
   int64_t gtot() const {
     int64_t t = 1;
@@ -245,37 +246,36 @@ __global__ void dcf_weight_kernel(const float* __restrict__ dcf, float* __restri
 // ---------------------------------------------------------------------------
 // forward: SENSE * deapod * sign, zero-padded into the grid
 // ---------------------------------------------------------------------------
+// grid: x = pairs along the last dim, y = G0 (2D) or G1 (3D), z = volume
+// (2D: be*C + c; 3D: (be*C + c)*G0 + n0).  No 64-bit division.
 template <int ND>
-__global__ void pre_fft_kernel(const float2* __restrict__ x, const float2* __restrict__ maps,
-                               const float* __restrict__ invdeap, float4* __restrict__ grid, Geo g, int nb,
-                               int coil_images) {
-  // one thread per pair of cells along the last dim
+__global__ void __launch_bounds__(128) pre_fft_kernel(const float2* __restrict__ x, const float2* __restrict__ maps,
+                                                     const float* __restrict__ invdeap, float4* __restrict__ grid,
+                                                     Geo g, int nb, int coil_images) {
   const int Gl = g.G[ND - 1];
-  const int half = Gl >> 1;
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long pairs_per_vol = g.gtot >> 1;
-  long long total = pairs_per_vol * g.C * nb;
-  if (i >= total) return;
-  long long vol = i / pairs_per_vol;          // be*C + c
-  long long r = i - vol * pairs_per_vol;
-  int c = (int)(vol % g.C);
-  int be = (int)(vol / g.C);
-  int nl = (int)(r % half) * 2;
-  long long rest = r / half;
-  int n[3] = {0, 0, 0};
-  n[ND - 1] = nl;
+  const int pair = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pair >= (Gl >> 1)) return;
+  int n[3];
+  unsigned vol;
   if (ND == 2) {
-    n[0] = (int)rest;
+    n[0] = blockIdx.y;
+    vol = blockIdx.z;
   } else {
-    n[1] = (int)(rest % g.G[1]);
-    n[0] = (int)(rest / g.G[1]);
+    n[1] = blockIdx.y;
+    n[0] = blockIdx.z % g.G[0];
+    vol = blockIdx.z / g.G[0];
   }
-  float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+  const int c = vol % g.C;
+  const int be = vol / g.C;
+  const int nl = pair * 2;
+  long long row = (ND == 2) ? (long long)n[0] : (long long)n[0] * g.G[1] + n[1];
+  float4* out = grid + ((long long)vol * g.gtot + row * Gl + nl) / 2;
+  float4 o4 = make_float4(0.f, 0.f, 0.f, 0.f);
   bool inside = true;
   int ii[3];
   float dap = 1.f;
-  int dap_off = 0;
-  int parity = 0;
+  int dap_off = 0, parity = 0;
+#pragma unroll
   for (int d = 0; d < ND - 1; ++d) {
     ii[d] = n[d] - g.off[d];
     inside = inside && (unsigned)ii[d] < (unsigned)g.S[d];
@@ -284,8 +284,8 @@ __global__ void pre_fft_kernel(const float2* __restrict__ x, const float2* __res
     parity += n[d];
   }
   if (inside) {
-    long long base = 0;
-    for (int d = 0; d < ND - 1; ++d) base = base * g.S[d] + ii[d];
+    long long base = ii[0];
+    if (ND == 3) base = base * g.S[1] + ii[1];
     const int Sl = g.S[ND - 1];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -300,43 +300,50 @@ __global__ void pre_fft_kernel(const float2* __restrict__ x, const float2* __res
           xv = x[(long long)be * g.stot + pix];
           mv = maps[(long long)c * g.stot + pix];
         }
-        float s = dap * invdeap[dap_off + il] * (((parity + nl + h) & 1) ? -1.f : 1.f);
-        float re = (xv.x * mv.x - xv.y * mv.y) * s;
-        float im = (xv.x * mv.y + xv.y * mv.x) * s;
-        if (h == 0) { out.x = re; out.y = im; } else { out.z = re; out.w = im; }
+        float sc = dap * invdeap[dap_off + il] * (((parity + nl + h) & 1) ? -1.f : 1.f);
+        float re = (xv.x * mv.x - xv.y * mv.y) * sc;
+        float im = (xv.x * mv.y + xv.y * mv.x) * sc;
+        if (h == 0) { o4.x = re; o4.y = im; } else { o4.z = re; o4.w = im; }
       }
     }
   }
-  grid[i] = out;
+  *out = o4;
 }
 
 // ---------------------------------------------------------------------------
 // adjoint: crop * deapod * sign * conj(maps), summed over coils
+// grid: x = pixels along the last dim, y = S0 (2D) or S1 (3D), z = be (2D)
+// or be*S0 + i0 (3D).
 // ---------------------------------------------------------------------------
 template <int ND>
-__global__ void post_ifft_kernel(const float2* __restrict__ grid, const float2* __restrict__ maps,
-                                 const float* __restrict__ invdeap, float2* __restrict__ x, Geo g, int nb,
-                                 float scale) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long total = g.stot * nb;
-  if (i >= total) return;
-  int be = (int)(i / g.stot);
-  long long pix = i - (long long)be * g.stot;
+__global__ void __launch_bounds__(128) post_ifft_kernel(const float2* __restrict__ grid, const float2* __restrict__ maps,
+                                                       const float* __restrict__ invdeap, float2* __restrict__ x,
+                                                       Geo g, int nb, float scale) {
+  const int Sl = g.S[ND - 1];
+  const int il = blockIdx.x * blockDim.x + threadIdx.x;
+  if (il >= Sl) return;
   int ii[3];
-  long long rem = pix;
-  for (int d = ND - 1; d >= 0; --d) {
-    ii[d] = (int)(rem % g.S[d]);
-    rem /= g.S[d];
+  int be;
+  if (ND == 2) {
+    ii[0] = blockIdx.y;
+    be = blockIdx.z;
+  } else {
+    ii[1] = blockIdx.y;
+    ii[0] = blockIdx.z % g.S[0];
+    be = blockIdx.z / g.S[0];
   }
+  ii[ND - 1] = il;
   float dap = scale;
   int dap_off = 0, parity = 0;
-  long long cell = 0;
+  long long cell = 0, pix = 0;
+#pragma unroll
   for (int d = 0; d < ND; ++d) {
     dap *= invdeap[dap_off + ii[d]];
     dap_off += g.S[d];
     int n = ii[d] + g.off[d];
     parity += n;
     cell = cell * g.G[d] + n;
+    pix = pix * g.S[d] + ii[d];
   }
   if (parity & 1) dap = -dap;
   float re = 0.f, im = 0.f;
@@ -347,7 +354,7 @@ __global__ void post_ifft_kernel(const float2* __restrict__ grid, const float2* 
     re += m.x * v.x + m.y * v.y;
     im += m.x * v.y - m.y * v.x;
   }
-  x[i] = make_float2(re * dap, im * dap);
+  x[(long long)be * g.stot + pix] = make_float2(re * dap, im * dap);
 }
 
 // ---------------------------------------------------------------------------
@@ -432,11 +439,16 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly
 }
 
 // ---------------------------------------------------------------------------
-// adjoint spread (2D, W = 4): one warp owns one output tile of T x T cells for
-// a group of coils, walks the tile's sample list in order and accumulates in
-// shared memory without atomics (lane = 16 taps x 2 coil lanes; a __syncwarp
-// orders consecutive samples), then writes every cell of the tile once.
-// Deterministic; each grid cell is written by exactly one warp.
+// adjoint spread (W = 4).  One warp owns one output tile (T x T cells in 2D,
+// T^3 in 3D) for a group of coils and is the only writer of those cells:
+// it walks the tile's sample list (samples whose 4-node support meets the
+// tile, in sample order), accumulates into shared memory without atomics and
+// writes every cell of the tile once (zeros included).  Deterministic.
+// Samples are staged 32 at a time: lane i loads sample i's coordinates,
+// kernel weights and coil values (independent loads, one latency per batch),
+// then the warp applies them one by one from shared memory, lanes = taps x
+// coil lanes, with a __syncwarp between samples to order the read-modify-
+// writes of cells shared by consecutive samples.  Empty tiles only store zeros.
 // ---------------------------------------------------------------------------
 struct SpreadArgs {
   const float2* y;
@@ -452,142 +464,187 @@ struct SpreadArgs {
 };
 
 constexpr int SPREAD_WARPS = 4;
+constexpr int SPREAD_BATCH = 32;
 
-__global__ void __launch_bounds__(SPREAD_WARPS * 32) spread2d_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
-  extern __shared__ float2 sm[];
-  const int T = tg.T;
-  const int RS = T + 4;                 // padded row stride (bank spread for 4x4 taps)
+template <int ND, int T>
+struct SpreadSmem {
+  static constexpr int RS = ND == 2 ? T + 4 : T;                  // padded last-dim stride
+  static constexpr int CELLS = ND == 2 ? T * RS : T * T * T;      // per coil
+  static constexpr int NW = 4 * ND;                               // staged weights per sample
+  __host__ __device__ static size_t warp_bytes(int cpi) {
+    return (size_t)cpi * CELLS * sizeof(float2) + SPREAD_BATCH * (sizeof(int4) + NW * sizeof(float)) +
+           (size_t)SPREAD_BATCH * cpi * sizeof(float2);
+  }
+};
+
+template <int ND, int T>
+__global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
+  using SM = SpreadSmem<ND, T>;
+  constexpr int RS = SM::RS;
+  constexpr int CELLS = SM::CELLS;
+  constexpr int NW = SM::NW;
+  extern __shared__ float4 smem4[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   long long item = (long long)blockIdx.x * SPREAD_WARPS + warp;
   long long nitems = (long long)a.nb * tg.ntiles * a.ngroups;
   if (item >= nitems) return;
-  int grp = (int)(item % a.ngroups);
-  long long rest = item / a.ngroups;
-  int tile = (int)(rest % tg.ntiles);
-  int be = (int)(rest / tg.ntiles);
-  int b = frame_of(be, a.nb, g.B);
-  int c0 = grp * a.cpi;
-  int nc = min(a.cpi, g.C - c0);
-  int tx0 = (tile / tg.nt[1]) * T;
-  int ty0 = (tile % tg.nt[1]) * T;
-  float2* acc = sm + (long long)warp * a.cpi * T * RS;
-  const int ncell = nc * T * RS;
-  for (int i = lane; i < ncell; i += 32) acc[i] = make_float2(0.f, 0.f);
-  __syncwarp();
-
+  const int grp = (int)(item % a.ngroups);
+  const long long rest = item / a.ngroups;
+  const int tile = (int)(rest % tg.ntiles);
+  const int be = (int)(rest / tg.ntiles);
+  const int b = frame_of(be, a.nb, g.B);
+  const int c0 = grp * a.cpi;
+  const int nc = min(a.cpi, g.C - c0);
+  int o[3];
+  if (ND == 2) {
+    o[0] = (tile / tg.nt[1]) * T;
+    o[1] = (tile % tg.nt[1]) * T;
+    o[2] = 0;
+  } else {
+    o[2] = (tile % tg.nt[2]) * T;
+    o[1] = ((tile / tg.nt[2]) % tg.nt[1]) * T;
+    o[0] = (tile / (tg.nt[2] * tg.nt[1])) * T;
+  }
   const int key = b * tg.ntiles + tile;
   const int e0 = a.tile_start[key], e1 = a.tile_start[key + 1];
-  const int tap = lane & 15, csub = lane >> 4;
-  const int ox = tap >> 2, oy = tap & 3;
-  const float* gx0p = a.gx + (long long)b * 2 * g.K;
-  const float* gx1p = gx0p + g.K;
-  const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
-  for (int e = e0; e < e1; ++e) {
-    int k = a.entries[e];
-    float x0 = gx0p[k], x1 = gx1p[k];
-    int n0 = (int)floorf(x0) - 1 + ox;
-    int n1 = (int)floorf(x1) - 1 + oy;
-    int lx = mrb::wrap_i(n0, g.G[0]) - tx0;
-    int ly = mrb::wrap_i(n1, g.G[1]) - ty0;
-    bool in = (unsigned)lx < (unsigned)T && (unsigned)ly < (unsigned)T;
-    float w = mrb::kb_eval(kb, x0 - (float)n0) * mrb::kb_eval(kb, x1 - (float)n1) * a.gsign;
-    if ((n0 + n1) & 1) w = -w;
-    if (a.wadj) w *= a.wadj[(long long)b * g.K + k];
-    if (in) {
-      for (int cl = csub; cl < nc; cl += 2) {
-        float2 v = yb[(long long)cl * g.K + k];
-        float2* p = acc + ((long long)cl * T + lx) * RS + ly;
-        float2 t = *p;
-        t.x = fmaf(w, v.x, t.x);
-        t.y = fmaf(w, v.y, t.y);
-        *p = t;
-      }
-    }
-    __syncwarp();
-  }
-  // write the whole tile once (zeros included)
   float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
-  const int cells = nc * T * T;
-  for (int i = lane; i < cells; i += 32) {
-    int cl = i / (T * T);
-    int r = i - cl * T * T;
-    int lx = r / T, ly = r - lx * T;
-    int gx_ = tx0 + lx, gy_ = ty0 + ly;
-    if (gx_ < g.G[0] && gy_ < g.G[1])
-      gout[(long long)cl * g.gtot + (long long)gx_ * g.G[1] + gy_] = acc[((long long)cl * T + lx) * RS + ly];
-  }
-}
+  const int Gl = g.G[ND - 1];
 
-// ---------------------------------------------------------------------------
-// adjoint spread (3D, W = 4): same ownership scheme with T^3 tiles; lanes
-// cover 64 taps as 2 passes of 32, one coil at a time.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(SPREAD_WARPS * 32) spread3d_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
-  extern __shared__ float2 sm[];
-  const int T = tg.T;
-  const int T3 = T * T * T;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  long long item = (long long)blockIdx.x * SPREAD_WARPS + warp;
-  long long nitems = (long long)a.nb * tg.ntiles * a.ngroups;
-  if (item >= nitems) return;
-  int grp = (int)(item % a.ngroups);
-  long long rest = item / a.ngroups;
-  int tile = (int)(rest % tg.ntiles);
-  int be = (int)(rest / tg.ntiles);
-  int b = frame_of(be, a.nb, g.B);
-  int c0 = grp * a.cpi;
-  int nc = min(a.cpi, g.C - c0);
-  int t2 = tile % tg.nt[2];
-  int t1 = (tile / tg.nt[2]) % tg.nt[1];
-  int t0 = tile / (tg.nt[2] * tg.nt[1]);
-  int o0 = t0 * T, o1 = t1 * T, o2 = t2 * T;
-  float2* acc = sm + (long long)warp * a.cpi * T3;
-  const int ncell = nc * T3;
-  for (int i = lane; i < ncell; i += 32) acc[i] = make_float2(0.f, 0.f);
+  // cells of the tile as float4 pairs along the last dim
+  constexpr int PAIRS = (ND == 2 ? T * T : T * T * T) / 2;
+  auto cell_of_pair = [&](int r, int* n) -> long long {
+    int l = (r % (T / 2)) * 2;
+    int rr = r / (T / 2);
+    if (ND == 2) {
+      n[0] = o[0] + rr;
+      n[1] = o[1] + l;
+      return (long long)n[0] * Gl + n[1];
+    } else {
+      n[0] = o[0] + rr / T;
+      n[1] = o[1] + rr % T;
+      n[2] = o[2] + l;
+      return ((long long)n[0] * g.G[1] + n[1]) * Gl + n[2];
+    }
+  };
+  auto in_grid = [&](const int* n) {
+    bool ok = n[0] < g.G[0];
+    if (ND >= 2) ok = ok && n[1] < g.G[1];
+    if (ND == 3) ok = ok && n[2] < g.G[2];
+    return ok;
+  };
+
+  if (e0 == e1) {   // no sample touches this tile: zeros
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = lane; i < nc * PAIRS; i += 32) {
+      int cl = i / PAIRS, r = i - cl * PAIRS;
+      int n[3];
+      long long cell = cell_of_pair(r, n);
+      if (in_grid(n)) *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = z4;
+    }
+    return;
+  }
+
+  char* wbase = reinterpret_cast<char*>(smem4) + (size_t)warp * SM::warp_bytes(a.cpi);
+  float2* acc = reinterpret_cast<float2*>(wbase);
+  int4* sb = reinterpret_cast<int4*>(wbase + (size_t)a.cpi * CELLS * sizeof(float2));
+  float* sw = reinterpret_cast<float*>(sb + SPREAD_BATCH);
+  float2* sy = reinterpret_cast<float2*>(sw + SPREAD_BATCH * NW);
+
+  {
+    float4* acc4 = reinterpret_cast<float4*>(acc);
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = lane; i < nc * CELLS / 2; i += 32) acc4[i] = z4;
+  }
   __syncwarp();
-  const int key = b * tg.ntiles + tile;
-  const int e0 = a.tile_start[key], e1 = a.tile_start[key + 1];
-  const float* gxp = a.gx + (long long)b * 3 * g.K;
+
+  const float* gxp = a.gx + (long long)b * ND * g.K;
   const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
-  for (int e = e0; e < e1; ++e) {
-    int k = a.entries[e];
-    float x0 = gxp[k], x1 = gxp[g.K + k], x2 = gxp[2 * g.K + k];
-    int b0 = (int)floorf(x0) - 1, b1 = (int)floorf(x1) - 1, b2 = (int)floorf(x2) - 1;
-    float wadj = a.wadj ? a.wadj[(long long)b * g.K + k] : 1.f;
+  for (int e = e0; e < e1; e += SPREAD_BATCH) {
+    const int nbat = min(SPREAD_BATCH, e1 - e);
+    if (lane < nbat) {
+      const int k = a.entries[e + lane];
+      float ws = a.gsign;
+      if (a.wadj) ws *= a.wadj[(long long)b * g.K + k];
+      int base[3] = {0, 0, 0};
 #pragma unroll
-    for (int pass = 0; pass < 2; ++pass) {
-      int tap = lane + 32 * pass;
-      int a0 = tap >> 4, a1 = (tap >> 2) & 3, a2 = tap & 3;
-      int n0 = b0 + a0, n1 = b1 + a1, n2 = b2 + a2;
-      int l0 = mrb::wrap_i(n0, g.G[0]) - o0;
-      int l1 = mrb::wrap_i(n1, g.G[1]) - o1;
-      int l2 = mrb::wrap_i(n2, g.G[2]) - o2;
-      bool in = (unsigned)l0 < (unsigned)T && (unsigned)l1 < (unsigned)T && (unsigned)l2 < (unsigned)T;
-      if (in) {
-        float w = mrb::kb_eval(kb, x0 - (float)n0) * mrb::kb_eval(kb, x1 - (float)n1) *
-                  mrb::kb_eval(kb, x2 - (float)n2) * a.gsign * wadj;
-        if ((n0 + n1 + n2) & 1) w = -w;
-        int cell = (l0 * T + l1) * T + l2;
-        for (int cl = 0; cl < nc; ++cl) {
-          float2 v = yb[(long long)cl * g.K + k];
-          float2* p = acc + (long long)cl * T3 + cell;
-          float2 t = *p;
-          t.x = fmaf(w, v.x, t.x);
-          t.y = fmaf(w, v.y, t.y);
-          *p = t;
+      for (int d = 0; d < ND; ++d) {
+        const float x = gxp[(long long)d * g.K + k];
+        base[d] = (int)floorf(x) - 1;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int n = base[d] + q;
+          float w = mrb::kb_eval(kb, x - (float)n);
+          if (n & 1) w = -w;
+          if (d == 0) w *= ws;
+          sw[lane * NW + d * 4 + q] = w;
         }
       }
+      sb[lane] = make_int4(base[0], base[1], base[2], 0);
+      for (int cl = 0; cl < nc; ++cl) sy[lane * a.cpi + cl] = yb[(long long)cl * g.K + k];
     }
     __syncwarp();
+    for (int j = 0; j < nbat; ++j) {
+      const int4 bb = sb[j];
+      if (ND == 2) {
+        const int tap = lane & 15, csub = lane >> 4;
+        const int ox = tap >> 2, oy = tap & 3;
+        int n0 = bb.x + ox, n1 = bb.y + oy;
+        n0 += n0 < 0 ? g.G[0] : 0;
+        n0 -= n0 >= g.G[0] ? g.G[0] : 0;
+        n1 += n1 < 0 ? g.G[1] : 0;
+        n1 -= n1 >= g.G[1] ? g.G[1] : 0;
+        const int lx = n0 - o[0], ly = n1 - o[1];
+        if ((unsigned)lx < (unsigned)T && (unsigned)ly < (unsigned)T) {
+          const float w = sw[j * NW + ox] * sw[j * NW + 4 + oy];
+          for (int cl = csub; cl < nc; cl += 2) {
+            const float2 v = sy[j * a.cpi + cl];
+            float2* p = acc + ((long long)cl * T + lx) * RS + ly;
+            float2 t = *p;
+            t.x = fmaf(w, v.x, t.x);
+            t.y = fmaf(w, v.y, t.y);
+            *p = t;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int pass = 0; pass < 2; ++pass) {
+          const int tap = lane + 32 * pass;
+          const int a0 = tap >> 4, a1 = (tap >> 2) & 3, a2 = tap & 3;
+          int n0 = bb.x + a0, n1 = bb.y + a1, n2 = bb.z + a2;
+          n0 += n0 < 0 ? g.G[0] : 0;
+          n0 -= n0 >= g.G[0] ? g.G[0] : 0;
+          n1 += n1 < 0 ? g.G[1] : 0;
+          n1 -= n1 >= g.G[1] ? g.G[1] : 0;
+          n2 += n2 < 0 ? g.G[2] : 0;
+          n2 -= n2 >= g.G[2] ? g.G[2] : 0;
+          const int l0 = n0 - o[0], l1 = n1 - o[1], l2 = n2 - o[2];
+          if ((unsigned)l0 < (unsigned)T && (unsigned)l1 < (unsigned)T && (unsigned)l2 < (unsigned)T) {
+            const float w = sw[j * NW + a0] * sw[j * NW + 4 + a1] * sw[j * NW + 8 + a2];
+            const int cell = (l0 * T + l1) * T + l2;
+            for (int cl = 0; cl < nc; ++cl) {
+              const float2 v = sy[j * a.cpi + cl];
+              float2* p = acc + (long long)cl * CELLS + cell;
+              float2 t = *p;
+              t.x = fmaf(w, v.x, t.x);
+              t.y = fmaf(w, v.y, t.y);
+              *p = t;
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
   }
-  float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
-  for (int i = lane; i < ncell; i += 32) {
-    int cl = i / T3;
-    int r = i - cl * T3;
-    int l0 = r / (T * T), l1 = (r / T) % T, l2 = r % T;
-    int n0 = o0 + l0, n1 = o1 + l1, n2 = o2 + l2;
-    if (n0 < g.G[0] && n1 < g.G[1] && n2 < g.G[2])
-      gout[(long long)cl * g.gtot + ((long long)n0 * g.G[1] + n1) * g.G[2] + n2] = acc[i];
+  // write the whole tile once
+  for (int i = lane; i < nc * PAIRS; i += 32) {
+    int cl = i / PAIRS, r = i - cl * PAIRS;
+    int n[3];
+    long long cell = cell_of_pair(r, n);
+    if (!in_grid(n)) continue;
+    int l = (r % (T / 2)) * 2;
+    int rr = r / (T / 2);
+    const float2* src = ND == 2 ? acc + ((long long)cl * T + rr) * RS + l : acc + (long long)cl * CELLS + rr * T + l;
+    *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = *reinterpret_cast<const float4*>(src);
   }
 }
 
@@ -918,37 +975,120 @@ static int ensure_grid(mrb_plan* p, int nb) {
   return ensure_fft(p, nb);
 }
 
+// one stage of the forward/adjoint pipeline; x/y are the user image / samples
+static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cudaStream_t st, int coil_images) {
+  Geo g = make_geo(p);
+  if (stage == 0) {
+    const int Gl = p->G[p->nd - 1];
+    const long long nvol = (long long)nb * p->C;
+    dim3 blk(128);
+    dim3 grd((Gl / 2 + 127) / 128, p->nd == 2 ? p->G[0] : p->G[1],
+             (unsigned)(p->nd == 2 ? nvol : nvol * p->G[0]));
+    MRB_REQUIRE(grd.z <= 65535, "too many coil volumes in one call (%u)", grd.z);
+    if (p->nd == 2)
+      pre_fft_kernel<2><<<grd, blk, 0, st>>>(
+          (const float2*)x, p->maps.as<float2>(), p->invdeap.as<float>(), p->grid.as<float4>(), g, nb, coil_images);
+    else
+      pre_fft_kernel<3><<<grd, blk, 0, st>>>(
+          (const float2*)x, p->maps.as<float2>(), p->invdeap.as<float>(), p->grid.as<float4>(), g, nb, coil_images);
+    MRB_LAUNCH_CHECK();
+    return 0;
+  }
+  if (stage == 1 || stage == 4) {
+    cufftResult r = cufftSetStream(p->fft, st);
+    if (r == CUFFT_SUCCESS)
+      r = cufftExecC2C(p->fft, p->grid.as<cufftComplex>(), p->grid.as<cufftComplex>(),
+                       stage == 1 ? CUFFT_FORWARD : CUFFT_INVERSE);
+    if (r != CUFFT_SUCCESS) return mrb::fail(MRB_ECUFFT, "cufftExecC2C failed (%d)", (int)r);
+    return 0;
+  }
+  if (stage == 2) {
+    InterpArgs a{};
+    a.grid = p->grid.as<float2>();
+    a.gx = p->gx.as<float>();
+    a.wfwd = p->has_wfwd ? p->wfwd.as<float>() : nullptr;
+    a.order = nullptr;
+    a.y = (float2*)y;
+    a.nb = nb;
+    a.scale = p->scale;
+    a.gsign = p->gsign;
+    dim3 grid(grid_blocks(p->K, 256), nb);
+    if (p->nd == 2) interp_kernel<2><<<grid, 256, 0, st>>>(a, g, p->kb);
+    else interp_kernel<3><<<grid, 256, 0, st>>>(a, g, p->kb);
+    MRB_LAUNCH_CHECK();
+    return 0;
+  }
+  if (stage == 3) {
+    TileGeo tg{};
+    tg.T = p->tile;
+    tg.ntiles = p->ntiles;
+    for (int d = 0; d < 3; ++d) tg.nt[d] = p->ntile_d[d];
+    tg.lo_off = p->W / 2 - 1;
+    tg.hi_off = p->W / 2;
+    SpreadArgs a{};
+    a.y = (const float2*)y;
+    a.gx = p->gx.as<float>();
+    a.wadj = p->has_wadj ? p->wadj.as<float>() : nullptr;
+    a.entries = p->entries.as<int>();
+    a.tile_start = p->tile_start.as<int>();
+    a.grid = p->grid.as<float2>();
+    a.nb = nb;
+    a.cpi = p->coils_per_item;
+    a.ngroups = (p->C + a.cpi - 1) / a.cpi;
+    a.gsign = p->gsign;
+    long long items = (long long)nb * tg.ntiles * a.ngroups;
+    int blocks = grid_blocks(items, SPREAD_WARPS);
+    const void* fn = nullptr;
+    size_t smem = 0;
+#define MRB_SPREAD_CASE(ND_, T_)                                                             \
+  if (p->nd == ND_ && tg.T == T_) {                                                          \
+    fn = (const void*)spread_kernel<ND_, T_>;                                                \
+    smem = SPREAD_WARPS * SpreadSmem<ND_, T_>::warp_bytes(a.cpi);                            \
+  }
+    MRB_SPREAD_CASE(2, 4)
+    MRB_SPREAD_CASE(2, 8)
+    MRB_SPREAD_CASE(2, 16)
+    MRB_SPREAD_CASE(2, 32)
+    MRB_SPREAD_CASE(3, 4)
+    MRB_SPREAD_CASE(3, 8)
+#undef MRB_SPREAD_CASE
+    MRB_REQUIRE(fn != nullptr, "no spread kernel for nd=%d tile=%d", p->nd, tg.T);
+    MRB_REQUIRE(smem <= 227 * 1024, "spread tile needs %zu bytes of shared memory", smem);
+    if (smem > 48 * 1024 && smem > p->spread_smem_set) {
+      MRB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      p->spread_smem_set = smem;
+    }
+    void* args[] = {&a, &g, &tg, &p->kb};
+    MRB_CUDA_TRY(cudaLaunchKernel(fn, dim3(blocks), dim3(SPREAD_WARPS * 32), args, smem, st));
+    MRB_LAUNCH_CHECK();
+    return 0;
+  }
+  if (stage == 5) {
+    const int Sl = p->S[p->nd - 1];
+    dim3 blk(128);
+    dim3 grd((Sl + 127) / 128, p->nd == 2 ? p->S[0] : p->S[1],
+             (unsigned)(p->nd == 2 ? (long long)nb : (long long)nb * p->S[0]));
+    MRB_REQUIRE(grd.z <= 65535, "too many frames in one call");
+    if (p->nd == 2)
+      post_ifft_kernel<2><<<grd, blk, 0, st>>>(p->grid.as<float2>(), p->maps.as<float2>(), p->invdeap.as<float>(),
+                                               (float2*)x, g, nb, p->scale);
+    else
+      post_ifft_kernel<3><<<grd, blk, 0, st>>>(p->grid.as<float2>(), p->maps.as<float2>(), p->invdeap.as<float>(),
+                                               (float2*)x, g, nb, p->scale);
+    MRB_LAUNCH_CHECK();
+    return 0;
+  }
+  return mrb::fail(MRB_EINVAL, "unknown stage %d", stage);
+}
+
 static int forward_impl(mrb_plan* p, const void* x, void* y, int nb, cudaStream_t st, int coil_images) {
   int rc;
   if ((rc = check_ready(p))) return rc;
   if ((rc = check_nb(p, nb))) return rc;
   MRB_REQUIRE(x != nullptr && y != nullptr, "null x or y");
   if ((rc = ensure_grid(p, nb))) return rc;
-  Geo g = make_geo(p);
-  long long pairs = (long long)nb * p->C * (p->gtot() / 2);
-  if (p->nd == 2)
-    pre_fft_kernel<2><<<grid_blocks(pairs, 256), 256, 0, st>>>(
-        (const float2*)x, p->maps.as<float2>(), p->invdeap.as<float>(), p->grid.as<float4>(), g, nb, coil_images);
-  else
-    pre_fft_kernel<3><<<grid_blocks(pairs, 256), 256, 0, st>>>(
-        (const float2*)x, p->maps.as<float2>(), p->invdeap.as<float>(), p->grid.as<float4>(), g, nb, coil_images);
-  MRB_LAUNCH_CHECK();
-  cufftResult r = cufftSetStream(p->fft, st);
-  if (r == CUFFT_SUCCESS) r = cufftExecC2C(p->fft, p->grid.as<cufftComplex>(), p->grid.as<cufftComplex>(), CUFFT_FORWARD);
-  if (r != CUFFT_SUCCESS) return mrb::fail(MRB_ECUFFT, "cufftExecC2C forward failed (%d)", (int)r);
-  InterpArgs a{};
-  a.grid = p->grid.as<float2>();
-  a.gx = p->gx.as<float>();
-  a.wfwd = p->has_wfwd ? p->wfwd.as<float>() : nullptr;
-  a.order = nullptr;
-  a.y = (float2*)y;
-  a.nb = nb;
-  a.scale = p->scale;
-  a.gsign = p->gsign;
-  dim3 grid(grid_blocks(p->K, 256), nb);
-  if (p->nd == 2) interp_kernel<2><<<grid, 256, 0, st>>>(a, g, p->kb);
-  else interp_kernel<3><<<grid, 256, 0, st>>>(a, g, p->kb);
-  MRB_LAUNCH_CHECK();
+  for (int stage : {0, 1, 2})
+    if ((rc = run_stage(p, stage, x, y, nb, st, coil_images))) return rc;
   return 0;
 }
 
@@ -965,54 +1105,21 @@ extern "C" int mrb_nufft_adjoint(mrb_plan* p, const void* y, void* x, int nb, mr
   if ((rc = check_ready(p))) return rc;
   if ((rc = check_nb(p, nb))) return rc;
   MRB_REQUIRE(x != nullptr && y != nullptr, "null x or y");
-  cudaStream_t st = (cudaStream_t)stream;
   if ((rc = ensure_grid(p, nb))) return rc;
-  Geo g = make_geo(p);
-  TileGeo tg{};
-  tg.T = p->tile;
-  tg.ntiles = p->ntiles;
-  for (int d = 0; d < 3; ++d) tg.nt[d] = p->ntile_d[d];
-  tg.lo_off = p->W / 2 - 1;
-  tg.hi_off = p->W / 2;
-  SpreadArgs a{};
-  a.y = (const float2*)y;
-  a.gx = p->gx.as<float>();
-  a.wadj = p->has_wadj ? p->wadj.as<float>() : nullptr;
-  a.entries = p->entries.as<int>();
-  a.tile_start = p->tile_start.as<int>();
-  a.grid = p->grid.as<float2>();
-  a.nb = nb;
-  a.cpi = p->coils_per_item;
-  a.ngroups = (p->C + a.cpi - 1) / a.cpi;
-  a.gsign = p->gsign;
-  long long items = (long long)nb * tg.ntiles * a.ngroups;
-  int blocks = grid_blocks(items, SPREAD_WARPS);
-  if (p->nd == 2) {
-    size_t smem = (size_t)SPREAD_WARPS * a.cpi * tg.T * (tg.T + 4) * sizeof(float2);
-    if (smem > 48 * 1024)
-      MRB_CUDA_TRY(cudaFuncSetAttribute(spread2d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    MRB_REQUIRE(smem <= 227 * 1024, "spread tile needs %zu bytes of shared memory", smem);
-    spread2d_kernel<<<blocks, SPREAD_WARPS * 32, smem, st>>>(a, g, tg, p->kb);
-  } else {
-    size_t smem = (size_t)SPREAD_WARPS * a.cpi * tg.T * tg.T * tg.T * sizeof(float2);
-    if (smem > 48 * 1024)
-      MRB_CUDA_TRY(cudaFuncSetAttribute(spread3d_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    MRB_REQUIRE(smem <= 227 * 1024, "spread tile needs %zu bytes of shared memory", smem);
-    spread3d_kernel<<<blocks, SPREAD_WARPS * 32, smem, st>>>(a, g, tg, p->kb);
-  }
-  MRB_LAUNCH_CHECK();
-  cufftResult r = cufftSetStream(p->fft, st);
-  if (r == CUFFT_SUCCESS) r = cufftExecC2C(p->fft, p->grid.as<cufftComplex>(), p->grid.as<cufftComplex>(), CUFFT_INVERSE);
-  if (r != CUFFT_SUCCESS) return mrb::fail(MRB_ECUFFT, "cufftExecC2C inverse failed (%d)", (int)r);
-  long long total = p->stot() * nb;
-  if (p->nd == 2)
-    post_ifft_kernel<2><<<grid_blocks(total, 256), 256, 0, st>>>(p->grid.as<float2>(), p->maps.as<float2>(),
-                                                                 p->invdeap.as<float>(), (float2*)x, g, nb, p->scale);
-  else
-    post_ifft_kernel<3><<<grid_blocks(total, 256), 256, 0, st>>>(p->grid.as<float2>(), p->maps.as<float2>(),
-                                                                 p->invdeap.as<float>(), (float2*)x, g, nb, p->scale);
-  MRB_LAUNCH_CHECK();
+  for (int stage : {3, 4, 5})
+    if ((rc = run_stage(p, stage, x, (void*)y, nb, (cudaStream_t)stream, 0))) return rc;
   return 0;
+}
+
+extern "C" int mrb_nufft_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, mrb_stream_t stream) {
+  int rc;
+  if ((rc = check_ready(p))) return rc;
+  if ((rc = check_nb(p, nb))) return rc;
+  MRB_REQUIRE(stage >= 0 && stage <= 5, "stage must be 0..5");
+  MRB_REQUIRE((stage == 1 || stage == 4) || (stage == 0 || stage == 5 ? x != nullptr : y != nullptr),
+              "null x or y for stage %d", stage);
+  if ((rc = ensure_grid(p, nb))) return rc;
+  return run_stage(p, stage, x, y, nb, (cudaStream_t)stream, 0);
 }
 
 extern "C" int mrb_plan_info(mrb_plan* p, int64_t* out, int nout) {

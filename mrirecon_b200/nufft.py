@@ -101,6 +101,13 @@ class KBPlan:
         _lib.check(self.lib.mrb_nufft_adjoint(self.h, _lib.ptr(y), _lib.ptr(x), int(nb), _lib.stream_ptr(y.device)),
                    "nufft_adjoint")
 
+    STAGES = {"pre": 0, "fft": 1, "interp": 2, "spread": 3, "ifft": 4, "post": 5}
+
+    def stage(self, name: str, x: Optional[torch.Tensor], y: Optional[torch.Tensor], nb: int) -> None:
+        """Run one stage of the operators on the plan's grid (timing / tuning)."""
+        _lib.check(self.lib.mrb_nufft_stage(self.h, self.STAGES[name], _lib.ptr(x), _lib.ptr(y), int(nb),
+                                            _lib.stream_ptr(self.device)), "nufft_stage")
+
     def info(self) -> dict:
         out = (ct.c_int64 * 6)()
         _lib.check(self.lib.mrb_plan_info(self.h, out, 6), "plan_info")
@@ -232,6 +239,18 @@ class B200NUFFTAdapter:
 
     def k_per_frame(self) -> int:
         return int(self._K)
+
+    # operator conveniences so the adapter can drive the solver directly
+    @property
+    def roles_image(self) -> Roles:
+        return Roles(unlike=1, like=1, nufft=self.ndim)
+
+    @property
+    def roles_kspace(self) -> Roles:
+        return Roles(unlike=1, like=1, nufft=1)
+
+    def image_shape(self, y: torch.Tensor) -> Tuple[int, ...]:
+        return (int(y.shape[0]), 1) + tuple(self._im_shape[1:])
 
     @property
     def plan(self) -> KBPlan:

@@ -1,0 +1,285 @@
+"""TV, FP64 reductions and the NCG solver on the GPU vs the reference fixtures
+and the CPU oracle.
+
+Tolerances: TV energy/gradient rel <= 1e-5 (FP32 stencil vs the reference's
+FP32 torch chain); FP64 dots rel <= 1e-12 against FP64 torch on the same
+FP32 data; NCG objective history rel <= 1e-4 with identical accepted steps
+and final image rel-L2 <= 1e-3 against the reference CGSolver run on CPU.
+"""
+import ctypes as ct
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden, rel
+from oracle import kb as okb
+from oracle.tv import tv_energy_grad
+from oracle.ncg import NCGOracle, NCGConfig, TVSpec
+from mrirecon_b200 import _lib, phantoms
+from mrirecon_b200.nufft import B200NUFFTAdapter
+from mrirecon_b200.regularization import TVND, TVParams, RegContext, RegManager, workspace
+from mrirecon_b200.roles import Roles
+from mrirecon_b200.solver import CGSolver, CGConfig
+
+pytestmark = pytest.mark.gpu
+
+TV_CASES = dict(iso_sp=(1e-3, 1e-3, (2, 3), True, None), aniso_sp=(2e-3, 1e-2, (2, 3), False, None),
+                aw_sp=(1e-3, 1e-3, (2, 3), True, (2.0, 0.5)), temporal=(5e-3, 1e-3, "temporal", True, None),
+                iso_3ax=(3e-3, 1e-3, (0, 2, 3), True, None))
+
+
+@pytest.mark.parametrize("name", list(TV_CASES))
+def test_tv_vs_reference_fixture(cuda, name):
+    g = golden("tv.npz")
+    x = torch.from_numpy(g["x_c64"]).to(cuda)
+    w, eps, axes, iso, aw = TV_CASES[name]
+    reg = TVND(name, TVParams(weight=w, eps=eps, axes=axes, isotropic=iso, axis_weights=aw))
+    gbuf = torch.zeros_like(x)
+    roles = Roles(1, 1, 2)
+    ctx = RegContext(x=x, g=gbuf, diag=None, roles_image=roles, device=cuda, dtype_c=x.dtype, dtype_r=torch.float32)
+    E = reg.energy_grad_fixed_axes(ctx, roles.resolve_axes(axes))
+    Eref = float(g[f"{name}_c64_E"])
+    assert abs(float(E) - Eref) <= 1e-5 * abs(Eref)
+    assert rel(gbuf, torch.from_numpy(g[f"{name}_c64_g"])) < 1e-5
+    # accumulates into g (manager adds regs into the data gradient)
+    base = torch.randn_like(x)
+    g2 = base.clone()
+    reg.energy_grad_fixed_axes(RegContext(x=x, g=g2, diag=None, roles_image=roles, device=cuda, dtype_c=x.dtype,
+                                          dtype_r=torch.float32), roles.resolve_axes(axes))
+    assert rel(g2, base + gbuf) < 1e-6
+
+
+def test_tv_3d_volume(cuda):
+    x = phantoms.ellipsoid_phantom(20, 6, seed=3).view(1, 1, 20, 20, 20)
+    reg = TVND("s3", TVParams(weight=1e-3, eps=1e-3, axes="spatial"))
+    roles = Roles(1, 1, 3)
+    gbuf = torch.zeros_like(x).to(cuda)
+    E = reg.energy_grad_fixed_axes(RegContext(x=x.to(cuda), g=gbuf, diag=None, roles_image=roles, device=cuda,
+                                              dtype_c=x.dtype, dtype_r=torch.float32), (2, 3, 4))
+    Eo, go = tv_energy_grad(x.to(torch.complex128), (2, 3, 4), 1e-3, 1e-3)
+    assert abs(float(E) - float(Eo)) <= 1e-5 * abs(float(Eo))
+    assert rel(gbuf, go) < 1e-5
+
+
+def _terms(specs, roles):
+    regm = RegManager([TVND(f"r{i}", TVParams(weight=w, eps=e, axes=a, isotropic=iso))
+                       for i, (w, e, a, iso) in enumerate(specs)])
+    ts = regm.terms(roles)
+    return (_lib.TVTerm * len(ts))(*ts), len(ts)
+
+
+def test_tv_multi_and_grad_pass_vs_oracle(cuda):
+    """Energies at many step sizes in one pass, and the fused gradient pass at
+    z = x + t d with g = g_base + t g_dir - lam div p and its FP64 statistics."""
+    torch.manual_seed(0)
+    F, N = 6, 40
+    x = phantoms.dynamic_phantom(N, F, seed=2).unsqueeze(1)
+    d = 0.1 * torch.randn(x.shape, dtype=torch.complex64)
+    gb = torch.randn(x.shape, dtype=torch.complex64)
+    gd = torch.randn(x.shape, dtype=torch.complex64)
+    specs = [(1e-3, 1e-3, "spatial", True), (5e-3, 1e-3, "temporal", True)]
+    roles = Roles(1, 1, 2)
+    arr, nt = _terms(specs, roles)
+    S = (ct.c_int * 3)(N, N, 1)
+    lib = _lib.load()
+    ws = workspace(cuda)
+    xc, dc, gbc, gdc = (v.to(cuda) for v in (x, d, gb, gd))
+    ts = torch.tensor([0.0] + [0.5 ** j for j in range(12)], dtype=torch.float64, device=cuda)
+    out = torch.zeros(24, dtype=torch.float64, device=cuda)
+    _lib.check(lib.mrb_tv_multi(2, S, F, arr, nt, _lib.ptr(xc), _lib.ptr(dc), _lib.ptr(ts), 13, None,
+                                _lib.ptr(out), _lib.ptr(ws), _lib.stream_ptr()), "tv_multi")
+    x64, d64 = x.to(torch.complex128), d.to(torch.complex128)
+    for j, t in enumerate(ts.tolist()):
+        Eo = sum(float(tv_energy_grad(x64 + t * d64, (2, 3) if a == "spatial" else (0,), w, e)[0])
+                 for (w, e, a, _) in specs)
+        assert abs(float(out[j]) - Eo) <= 2e-5 * abs(Eo)
+    t = 0.37
+    gout = torch.empty_like(xc)
+    out2 = torch.zeros(24, dtype=torch.float64, device=cuda)
+    _lib.check(lib.mrb_tv_grad(2, S, F, arr, nt, _lib.ptr(xc), _lib.ptr(dc), None, t, _lib.ptr(gbc), _lib.ptr(gdc),
+                               _lib.ptr(gout), None, 0, None, None, 0, _lib.ptr(out2), _lib.ptr(ws),
+                               _lib.stream_ptr()), "tv_grad")
+    z = x64 + t * d64
+    E1, g1 = tv_energy_grad(z, (2, 3), 1e-3, 1e-3)
+    E2, g2 = tv_energy_grad(z, (0,), 5e-3, 1e-3)
+    gref = gb.to(torch.complex128) + t * gd.to(torch.complex128) + g1 + g2
+    assert rel(gout, gref) < 1e-5
+    o = out2.tolist()
+    assert abs(o[0] - float(E1)) <= 1e-5 * abs(float(E1)) and abs(o[1] - float(E2)) <= 1e-5 * abs(float(E2))
+    gg = gout.cpu().to(torch.complex128)
+    assert o[4] == pytest.approx(float(torch.vdot(gg.reshape(-1), d64.reshape(-1)).real), rel=1e-6)
+    assert o[5] == pytest.approx(float((gg.abs() ** 2).sum()), rel=1e-6)
+    assert o[7] == pytest.approx(float((d64.abs() ** 2).sum()), rel=1e-6)
+
+
+def test_dots_f64(cuda):
+    lib = _lib.load()
+    n = 3 * 1024 * 1024 + 17
+    a = torch.randn(n, dtype=torch.complex64, device=cuda)
+    b = torch.randn(n, dtype=torch.complex64, device=cuda)
+    D = torch.rand(n, dtype=torch.float32, device=cuda) + 0.5
+    out = torch.zeros(3, dtype=torch.float64, device=cuda)
+    A = (ct.c_void_p * 3)(a.data_ptr(), a.data_ptr(), b.data_ptr())
+    Bp = (ct.c_void_p * 3)(b.data_ptr(), a.data_ptr(), b.data_ptr())
+    Dp = (ct.c_void_p * 3)(0, D.data_ptr(), 0)
+    ws = workspace(cuda)
+    _lib.check(lib.mrb_dots_f64(n, 3, A, Bp, Dp, n, _lib.ptr(out), _lib.ptr(ws), _lib.stream_ptr()), "dots")
+    a64, b64, D64 = a.cpu().to(torch.complex128), b.cpu().to(torch.complex128), D.cpu().double()
+    ref = [float(torch.vdot(a64, b64).real), float((a64.abs() ** 2 / D64).sum()), float((b64.abs() ** 2).sum())]
+    for v, r in zip(out.tolist(), ref):
+        assert v == pytest.approx(r, rel=1e-6, abs=1e-6 * math.sqrt(n))
+    out2 = torch.zeros(3, dtype=torch.float64, device=cuda)
+    _lib.check(lib.mrb_dots_f64(n, 3, A, Bp, Dp, n, _lib.ptr(out2), _lib.ptr(ws), _lib.stream_ptr()), "dots")
+    assert torch.equal(out, out2)        # deterministic
+
+
+def _fixture_solver(run, schedule, **kw):
+    g = golden("ncg_small.npz")
+    dev = torch.device("cuda")
+    maps, traj, y = (torch.from_numpy(g[k]) for k in ("maps", "traj", "y"))
+    ad = B200NUFFTAdapter(ndim=2)
+    ad.prepare(tuple(maps.shape), traj.to(dev), None, maps.to(dev), torch.complex64, dev)
+    regm = RegManager([TVND("s", TVParams(weight=1e-3, eps=1e-3, axes=(2, 3))),
+                       TVND("t", TVParams(weight=5e-3, eps=1e-3, axes="temporal"))])
+    direction, ls = run.split("_")
+    cfg = CGConfig(direction=direction, ls_name=ls, max_iter=len(g[f"{run}_f"]), tol_g=0.0, tol_step=0.0,
+                   schedule=schedule, **kw)
+    return g, CGSolver(y.to(dev), ad, regm, cfg)
+
+
+@pytest.mark.parametrize("run", ["fr_armijo", "prplus_armijo", "dy_armijo", "fr_wolfe"])
+def test_reference_schedule_matches_reference_cgsolver(cuda, run):
+    g, s = _fixture_solver(run, "reference")
+    s.run()
+    h = s.history()
+    assert len(h) == len(g[f"{run}_f"])
+    np.testing.assert_array_equal([r["step"] for r in h], g[f"{run}_step"])
+    np.testing.assert_allclose([r["f"] for r in h], g[f"{run}_f"], rtol=1e-4)
+    np.testing.assert_allclose([r["xnorm"] for r in h], g[f"{run}_xnorm"], rtol=1e-4)
+    assert rel(s.result(), torch.from_numpy(g[f"{run}_x"])) < 1e-3
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_fast_schedule_matches_reference_cgsolver(cuda, graph):
+    g, s = _fixture_solver("fr_armijo", "fast", cuda_graph=graph, iters_per_graph=3)
+    s.run()
+    h = s.history()
+    run = "fr_armijo"
+    assert len(h) == len(g[f"{run}_f"])
+    np.testing.assert_array_equal([r["step"] for r in h], g[f"{run}_step"])
+    np.testing.assert_allclose([r["f"] for r in h], g[f"{run}_f"], rtol=1e-4)
+    assert rel(s.result(), torch.from_numpy(g[f"{run}_x"])) < 1e-3
+    # one forward and one adjoint NUFFT per iteration after priming
+    assert s.n_forward <= 2 + len(h) + 3 and s.n_adjoint <= 2 + len(h) + 3
+
+
+def test_fast_graph_equals_eager(cuda):
+    _, a = _fixture_solver("fr_armijo", "fast", cuda_graph=False)
+    _, b = _fixture_solver("fr_armijo", "fast", cuda_graph=True, iters_per_graph=4)
+    a.run()
+    b.run()
+    assert torch.equal(a.result(), b.result())
+    assert [r["f"] for r in a.history()] == [r["f"] for r in b.history()]
+
+
+def _grasp_problem(N=48, F=6, C=4, spf=9, nread=96, sigma=1e-3):
+    dev = torch.device("cuda")
+    maps = phantoms.coil_maps(N, C)
+    traj = phantoms.grasp_trajectory(F, spf, nread)
+    xt = phantoms.dynamic_phantom(N, F, seed=5).unsqueeze(1)
+    ad = B200NUFFTAdapter(ndim=2)
+    ad.prepare((C, N, N), traj.to(dev), None, maps.to(dev), torch.complex64, dev)
+    y = phantoms.add_noise(ad.A(xt.to(dev)), sigma, seed=1)
+    return ad, y, maps, traj
+
+
+def _regm():
+    return RegManager([TVND("s", TVParams(weight=1e-3, eps=1e-3, axes="spatial")),
+                       TVND("t", TVParams(weight=5e-3, eps=1e-3, axes="temporal"))])
+
+
+def test_fast_vs_reference_schedule_grasp(cuda):
+    ad, y, _, _ = _grasp_problem()
+    a = CGSolver(y, ad, _regm(), CGConfig(max_iter=40, tol_g=0.0, tol_step=0.0, schedule="reference"))
+    b = CGSolver(y, ad, _regm(), CGConfig(max_iter=40, tol_g=0.0, tol_step=0.0, schedule="fast"))
+    a.run()
+    b.run()
+    fa, fb = [r["f"] for r in a.history()], [r["f"] for r in b.history()]
+    assert len(fb) == len(fa)
+    np.testing.assert_allclose(fb, fa, rtol=1e-4)
+    assert rel(b.result(), a.result()) < 1e-3
+
+
+def test_fast_vs_oracle_ncg(cuda):
+    """The fast schedule against the CPU restatement of the reference schedule."""
+    ad, y, maps, traj = _grasp_problem(N=32, F=4, C=3, spf=7, nread=64)
+    k = okb.KBNufft(maps, traj, None, dtype=torch.complex64)
+    o = NCGOracle(lambda v: k.A(v).to(torch.complex64), lambda v: k.AH(v).to(torch.complex64), y.cpu(),
+                  torch.zeros((4, 1, 32, 32), dtype=torch.complex64), [TVSpec((2, 3), 1e-3), TVSpec((0,), 5e-3)],
+                  NCGConfig(max_iter=15, tol_g=0.0, tol_step=0.0))
+    o.run()
+    s = CGSolver(y, ad, _regm(), CGConfig(max_iter=15, tol_g=0.0, tol_step=0.0))
+    s.run()
+    np.testing.assert_allclose([r["f"] for r in s.history()], [h["f"] for h in o.hist], rtol=1e-4)
+    assert rel(s.result(), o.x) < 1e-3
+
+
+def test_stop_rule_windowed(cuda):
+    ad, y, _, _ = _grasp_problem()
+    s = CGSolver(y, ad, _regm(), CGConfig(max_iter=400, tol_g=0.0, tol_step=0.0, stop_window=10, stop_tol=1e-4))
+    s.run()
+    h = s.history()
+    assert s.stop_reason == "relative objective change"
+    fa = [h[0]["f"]] + [r["f_accepted"] for r in h]
+    W = 10
+    k = len(fa) - 1
+    assert (fa[k - W] - fa[k]) <= W * 1e-4 * abs(fa[k]) * (1 + 1e-9)
+    # it did not fire one iteration earlier
+    assert (fa[k - 1 - W] - fa[k - 1]) > W * 1e-4 * abs(fa[k - 1])
+
+
+def test_objective_decreases_and_matches_recomputed(cuda):
+    ad, y, _, _ = _grasp_problem()
+    s = CGSolver(y, ad, _regm(), CGConfig(max_iter=25, tol_g=0.0, tol_step=0.0))
+    s.run()
+    f = [r["f"] for r in s.history()]
+    assert all(b <= a for a, b in zip(f, f[1:]))
+    assert s.objective() == pytest.approx(s.history()[-1]["f_accepted"], rel=1e-5)
+
+
+class CartesianFFT:
+    """Unitary Cartesian FFT test operator (the reference's numerics-test fake,
+    graspcg/tests/test_numerics_ns.py:22-69), images (B, 1, H, W)."""
+    roles_image = Roles(1, 1, 2)
+
+    def A(self, x, out=None):
+        k = torch.fft.fftn(x, dim=(-2, -1), norm="ortho")
+        return k if out is None else out.copy_(k)
+
+    def AH(self, k, out=None):
+        x = torch.fft.ifftn(k, dim=(-2, -1), norm="ortho")
+        return x if out is None else out.copy_(x)
+
+    def image_shape(self, y):
+        return tuple(y.shape)
+
+
+@pytest.mark.parametrize("direction", ["fr", "prplus", "dy"])
+@pytest.mark.parametrize("schedule,ls", [("fast", "armijo"), ("reference", "armijo"), ("reference", "wolfe")])
+def test_known_answers_cartesian(cuda, direction, schedule, ls):
+    """With a unitary A, y = A x_true and no regulariser, the minimiser is
+    x_true; the first Armijo step from x = 0 accepts t = 1 exactly
+    (graspcg/tests/test_numerics_ns.py:175-194) and every direction is a descent
+    direction (:256-309)."""
+    torch.manual_seed(1)
+    xt = torch.randn((3, 1, 8, 8), dtype=torch.complex64, device=cuda)
+    op = CartesianFFT()
+    y = op.A(xt)
+    s = CGSolver(y, op, RegManager([]), CGConfig(direction=direction, ls_name=ls, max_iter=4, schedule=schedule,
+                                                 cuda_graph=False, tol_g=0.0, tol_step=0.0))
+    s.run()
+    h = s.history()
+    assert h[0]["step"] == 1.0 and h[0]["gdot"] < 0
+    assert rel(s.result(), xt) < 1e-5
