@@ -336,8 +336,10 @@ __global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P,
 }
 
 // Sum of all unit energies at z = x + t_j d for J <= MT_MAX_J step sizes, one
-// pass: per slot the differences A = D x, B = D d are loaded once and
-// D z(t_j) = A + t_j B is formed in registers for every t_j.
+// pass.  Per slot the differences A = D x and B = D d are loaded once; per unit
+// |D z(t)|^2 = sum_s w_s^2 |A_s + t B_s|^2 = alpha + 2 beta t + gamma t^2 is a
+// quadratic in t whose three coefficients are formed once per voxel, so each
+// trial step costs two FMAs and a square root per unit.
 constexpr int MT_MAX_J = 24;
 
 __global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __restrict__ x,
@@ -368,24 +370,29 @@ __global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __r
           }
         }
       }
+      float al[NUNIT], be2[NUNIT], ga[NUNIT];
+#pragma unroll
+      for (int u = 0; u < NUNIT; ++u) {
+        al[u] = be2[u] = ga[u] = 0.f;
+        if (u >= P.nu) continue;
+#pragma unroll
+        for (int s = 0; s < NSLOT; ++s) {
+          const float w2 = P.w[u][s] * P.w[u][s];
+          al[u] = fmaf(w2, A[s].x * A[s].x + A[s].y * A[s].y, al[u]);
+          be2[u] = fmaf(2.f * w2, A[s].x * B[s].x + A[s].y * B[s].y, be2[u]);
+          ga[u] = fmaf(w2, B[s].x * B[s].x + B[s].y * B[s].y, ga[u]);
+        }
+      }
 #pragma unroll
       for (int j = 0; j < MT_MAX_J; ++j) {
         if (j >= J) continue;
         const float t = tf[j];
-        float m[NSLOT];
-#pragma unroll
-        for (int s = 0; s < NSLOT; ++s) {
-          float ax = fmaf(t, B[s].x, A[s].x), ay = fmaf(t, B[s].y, A[s].y);
-          m[s] = ax * ax + ay * ay;
-        }
         float e = 0.f;
 #pragma unroll
         for (int u = 0; u < NUNIT; ++u) {
           if (u >= P.nu) continue;
-          float ss = 0.f;
-#pragma unroll
-          for (int s = 0; s < NSLOT; ++s) ss = fmaf(P.w[u][s] * P.w[u][s], m[s], ss);
-          e += P.lam[u] * (sqrtf(ss + P.eps[u] * P.eps[u]) - P.eps[u]);
+          const float ss = fmaxf(fmaf(t, fmaf(t, ga[u], be2[u]), al[u]), 0.f);
+          e = fmaf(P.lam[u], sqrtf(ss + P.eps[u] * P.eps[u]) - P.eps[u], e);
         }
         acc[j] += (double)e;
       }
