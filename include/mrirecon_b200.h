@@ -130,6 +130,22 @@ int mrb_workspace_bytes(int64_t* bytes);
 int mrb_dots_f64(int64_t n, int npairs, const void* const* a, const void* const* b,
                  const float* const* diag, int64_t ndiag, double* out, void* ws, mrb_stream_t stream);
 
+/* Same result as mrb_dots_f64 without a caller workspace and without any
+ * allocation: the block partials live in a fixed device array of 75,776 bytes
+ * (1184 blocks x 8 doubles) that every GPU loading this library keeps until
+ * the process exits.  For callers that cannot allocate device memory where
+ * they need the dots (inside a CUDA stream capture, in real-time loops where
+ * cudaMalloc/cudaFree would synchronise the device, or when another allocator
+ * owns all device memory).  npairs above 8 is rejected (MRB_ERANGE).  The
+ * first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All
+ * calls share the one array, so calls that overlap on the GPU (other streams,
+ * other host threads) race; serialise them.  No part of the array needs to
+ * start at zero: every call overwrites each partial it reads.
+ * This entry point has no counterpart in the reference. */
+int mrb_dots_f64_noalloc(int64_t n, int npairs, const void* const* a, const void* const* b,
+                         const float* const* diag, int64_t ndiag, double* out, mrb_stream_t stream);
+
 /* k-space passes over n complex64 samples (t from t_dev if non-NULL, else t_host;
  * the pass is skipped when skip != NULL and *skip != 0):
  *   mode 0: out[0..2] = |r|^2, Re<r,Ad>, |Ad|^2 (FP64)

@@ -60,6 +60,8 @@ _SIGS = {
     "mrb_workspace_bytes": (ct.c_int, [c_int64_p]),
     "mrb_dots_f64": (ct.c_int, [ct.c_int64, ct.c_int, ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_void_p),
                                 ct.POINTER(ct.c_void_p), ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mrb_dots_f64_noalloc": (ct.c_int, [ct.c_int64, ct.c_int, ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_void_p),
+                                        ct.POINTER(ct.c_void_p), ct.c_int64, ct.c_void_p, ct.c_void_p]),
     "mrb_kspace_pass": (ct.c_int, [ct.c_int, ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                    ct.c_void_p, ct.c_double, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mrb_tv_grad": (ct.c_int, [ct.c_int, c_int_p, ct.c_int, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p,

@@ -19,6 +19,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include "mrb_common.cuh"
 
@@ -875,4 +876,87 @@ extern "C" int mrb_ncg_set_steps(double* ts, int J, double beta, mrb_stream_t st
   set_steps_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(ts, J, beta);
   MRB_LAUNCH_CHECK();
   return 0;
+}
+
+// ===========================================================================
+// Allocation-free variant of mrb_dots_f64.
+//
+// Some callers cannot allocate device memory at the point where they need a
+// dot product: code running inside a CUDA stream capture (an allocation is not
+// a stream operation and invalidates a global-mode capture), real-time
+// reconstruction loops next to the scanner (cudaMalloc/cudaFree synchronise
+// the device and stall acquisition), and processes whose device memory is
+// handed out by another allocator up front (a stray cudaMalloc can fail).
+// This entry point keeps its block partials in a fixed file-scope device
+// array instead of a caller workspace, and calls no allocating routine.
+// ===========================================================================
+namespace {
+
+constexpr int NOALLOC_MAX_PAIRS = 8;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+// RED_MAX_BLOCKS x 8 doubles = 75,776 bytes; every GPU that loads this
+// library holds it until the process exits.
+static __device__ __align__(256) double g_noalloc_partials[RED_MAX_BLOCKS * NOALLOC_MAX_PAIRS];
+
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of the scratch array on the current device.  The host-side
+// name g_noalloc_partials is only a stand-in and must never be passed to a
+// kernel; the address is looked up once per device, with that device current.
+int noalloc_scratch(double** out) {
+  int dev = -1;
+  MRB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+    return mrb::fail(MRB_ERANGE, "device ordinal %d above the %d supported", dev, NOALLOC_MAX_DEVICES);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess || p == nullptr)
+      return mrb::fail(MRB_ECUDA, "cudaGetSymbolAddress(scratch) failed on device %d: %s", dev,
+                       cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = (double*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int mrb_dots_f64_noalloc(int64_t n, int npairs, const void* const* a, const void* const* b,
+                                    const float* const* diag, int64_t ndiag, double* out, mrb_stream_t stream) {
+  if (npairs < 1 || npairs > NOALLOC_MAX_PAIRS)
+    return mrb::fail(MRB_ERANGE, "mrb_dots_f64_noalloc: npairs = %d, the fixed scratch holds at most %d pairs",
+                     npairs, NOALLOC_MAX_PAIRS);
+  MRB_REQUIRE(n >= 0, "mrb_dots_f64_noalloc: negative length");
+  MRB_REQUIRE(a && b && out, "mrb_dots_f64_noalloc: null pointer");
+  double* part = nullptr;
+  int rc = noalloc_scratch(&part);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  DotArgs d{};
+  for (int j = 0; j < npairs; ++j) {
+    MRB_REQUIRE(a[j] && b[j], "mrb_dots_f64_noalloc: null operand %d", j);
+    d.a[j] = (const float2*)a[j];
+    d.b[j] = (const float2*)b[j];
+    d.diag[j] = diag ? diag[j] : nullptr;
+  }
+  d.ndiag = ndiag > 0 ? ndiag : 1;
+  d.n = n;
+  d.npairs = npairs;
+  // at most RED_MAX_BLOCKS blocks, each writing its `stride` partials before the
+  // final sum reads them: no part of the scratch has to start at zero
+  const int nb = red_blocks(n, 4);
+  switch (npairs) {
+    case 1: dots_kernel<1><<<nb, RED_THREADS, 0, st>>>(d, part); break;
+    case 2: dots_kernel<2><<<nb, RED_THREADS, 0, st>>>(d, part); break;
+    case 3: dots_kernel<3><<<nb, RED_THREADS, 0, st>>>(d, part); break;
+    case 4: dots_kernel<4><<<nb, RED_THREADS, 0, st>>>(d, part); break;
+    default: dots_kernel<8><<<nb, RED_THREADS, 0, st>>>(d, part); break;
+  }
+  MRB_LAUNCH_CHECK();
+  const int stride = npairs <= 4 ? npairs : 8;
+  return finalize(part, nb, stride, npairs, out, 0, nullptr, st);
 }
