@@ -1,0 +1,108 @@
+"""Spread tile / coil-group / chunk autotuner.
+
+For a prepared plan it times the adjoint spread stage (the kernel whose speed
+depends on the tiling; interp, pre/post and the FFT do not) for a list of
+(tile edge, coils per work item, samples per chunk) candidates on the plan's
+own trajectory, keeps the fastest and caches the choice per size class
+(nd, image shape, coils, frames, samples per frame) and GPU name in a JSON
+file (``$MRB_TUNE_CACHE`` or ``~/.cache/mrirecon_b200/spread_tune.json``).
+All candidates compute the same grid (deterministically, up to the order in
+which split tiles sum their partial tiles).
+"""
+from __future__ import annotations
+
+import json
+import os
+from typing import Dict, Iterable, Optional, Sequence, Tuple
+
+import torch
+
+CANDIDATES_2D: Tuple[Tuple[int, int, int], ...] = (
+    (16, 4, 128), (16, 4, 512), (16, 6, 128), (16, 2, 128), (8, 4, 64), (8, 6, 128), (16, 4, 32), (32, 2, 128))
+CANDIDATES_3D: Tuple[Tuple[int, int, int], ...] = (
+    (8, 2, 256), (8, 1, 256), (8, 4, 256), (8, 2, 64), (4, 4, 256), (4, 8, 256))
+
+
+def _cache_path() -> str:
+    p = os.environ.get("MRB_TUNE_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "mrirecon_b200", "spread_tune.json")
+
+
+def size_class(plan) -> str:
+    name = torch.cuda.get_device_name(plan.device)
+    return f"{name}|nd{plan.nd}|S{'x'.join(map(str, plan.S))}|C{plan.C}|B{plan.B}|K{plan.K}"
+
+
+def _load() -> Dict[str, dict]:
+    try:
+        with open(_cache_path()) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def _store(d: Dict[str, dict]) -> None:
+    path = _cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        with open(path, "w") as f:
+            json.dump(d, f, indent=1, sort_keys=True)
+    except Exception:
+        pass
+
+
+def time_spread(plan, y: torch.Tensor, nb: int, reps: int = 5) -> float:
+    for _ in range(2):
+        plan.stage("spread", None, y, nb)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(plan.device)
+    a.record()
+    for _ in range(reps):
+        plan.stage("spread", None, y, nb)
+    b.record()
+    torch.cuda.synchronize(plan.device)
+    return a.elapsed_time(b) / reps
+
+
+def apply(plan, traj: torch.Tensor, tile: int, cpi: int, chunk: int) -> None:
+    from .nufft import OPT_CHUNK, OPT_COILS_PER_ITEM, OPT_TILE
+    plan.set_option(OPT_TILE, tile)
+    plan.set_option(OPT_COILS_PER_ITEM, cpi)
+    plan.set_option(OPT_CHUNK, chunk)
+    plan.set_points(traj)
+
+
+def tune(plan, traj: torch.Tensor, candidates: Optional[Iterable[Tuple[int, int, int]]] = None,
+         reps: int = 5, use_cache: bool = True) -> dict:
+    """Pick (tile, coils per item, chunk) for `plan`; leaves the plan set to it."""
+    key = size_class(plan)
+    cache = _load() if use_cache else {}
+    if use_cache and key in cache:
+        c = cache[key]
+        apply(plan, traj, c["tile"], c["cpi"], c["chunk"])
+        return dict(c, cached=True)
+    if candidates is None:
+        candidates = CANDIDATES_2D if plan.nd == 2 else CANDIDATES_3D
+    g = torch.Generator(device=plan.device).manual_seed(0)
+    y = torch.randn((plan.B, plan.C, plan.K), dtype=torch.complex64, device=plan.device, generator=g)
+    results = []
+    for tile, cpi, chunk in candidates:
+        if tile < 4 or min(plan.G) < tile:
+            continue
+        try:
+            apply(plan, traj, tile, min(cpi, plan.C), chunk)
+            results.append((time_spread(plan, y, plan.B, reps), tile, min(cpi, plan.C), chunk))
+        except RuntimeError:
+            continue                     # e.g. shared memory above the per-block limit
+    if not results:
+        raise RuntimeError("no spread configuration could be timed")
+    ms, tile, cpi, chunk = min(results)
+    apply(plan, traj, tile, cpi, chunk)
+    best = {"tile": tile, "cpi": cpi, "chunk": chunk, "ms": ms,
+            "tried": [{"tile": t, "cpi": c, "chunk": h, "ms": m} for m, t, c, h in sorted(results)]}
+    if use_cache:
+        cache[key] = {k: best[k] for k in ("tile", "cpi", "chunk", "ms")}
+        _store(cache)
+    return best

@@ -19,6 +19,7 @@
 #include <cufft.h>
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -46,13 +47,19 @@ struct mrb_plan {
   int tile = 16;
   int coils_per_item = 4;
   int interp_mode = 0;
+  int chunk = 128;     // samples per spread work item (heavy tiles are split)
   // state
   bool have_points = false;
   bool have_maps = false;
   DevBuf gx;          // (B, nd, K) float
   DevBuf entries;     // (n_entries) int32 sample index, sorted by (frame, tile)
   DevBuf tile_start;  // (B * ntiles + 1) int32
-  DevBuf sorted_k;    // (B, K) int32 samples sorted by tile of their base node
+  DevBuf items;      // spread work items int4 (key, chunk, partial slot or -1, chunks of key), heaviest first
+  DevBuf multi;      // int4 (key, chunks, first partial slot, 0) for tiles split into several chunks
+  DevBuf partials;   // chunk partial tiles (rep, slot, C, T^nd) float2
+  int n_items = 0, n_multi = 0, n_slots = 0;
+  DevBuf empty_keys; // (frame, tile) keys with no sample: zero-filled by a store-only kernel
+  int n_empty = 0;
   int64_t n_entries = 0;
   int64_t touched = 0;
   int ntile_d[3] = {1, 1, 1};
@@ -396,30 +403,71 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly
   float s = a.scale * a.gsign;
   if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
   const float2* gb = a.grid + (long long)be * g.C * g.gtot;
-  for (int c = 0; c < g.C; ++c) {
-    const float2* gc = gb + (long long)c * g.gtot;
-    float re = 0.f, im = 0.f;
-    if (ND == 2) {
+  float2* yo = a.y + (long long)be * g.C * g.K + k;
+  if (ND == 2) {
+    // row offsets shared by all coils
+    long long roff[W];
 #pragma unroll
-      for (int i0 = 0; i0 < W; ++i0) {
-        const float2* row = gc + (long long)nidx[0][i0] * g.G[1];
-        float r2 = 0.f, i2 = 0.f;
+    for (int i0 = 0; i0 < W; ++i0) roff[i0] = (long long)nidx[0][i0] * g.G[1];
+    // two coils per pass: 32 independent loads in flight per thread
+    int c = 0;
+    for (; c + 1 < g.C; c += 2) {
+      const float2* g0 = gb + (long long)c * g.gtot;
+      const float2* g1 = g0 + g.gtot;
+      float2 v0[W][W], v1[W][W];
+#pragma unroll
+      for (int i0 = 0; i0 < W; ++i0)
 #pragma unroll
         for (int i1 = 0; i1 < W; ++i1) {
-          float2 v = __ldg(row + nidx[ND - 1][i1]);
-          r2 = fmaf(w[ND - 1][i1], v.x, r2);
-          i2 = fmaf(w[ND - 1][i1], v.y, i2);
+          v0[i0][i1] = __ldg(g0 + roff[i0] + nidx[1][i1]);
+          v1[i0][i1] = __ldg(g1 + roff[i0] + nidx[1][i1]);
         }
-        re = fmaf(w[0][i0], r2, re);
-        im = fmaf(w[0][i0], i2, im);
+      float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
+#pragma unroll
+      for (int i0 = 0; i0 < W; ++i0) {
+        float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
+#pragma unroll
+        for (int i1 = 0; i1 < W; ++i1) {
+          a0 = fmaf(w[1][i1], v0[i0][i1].x, a0);
+          b0 = fmaf(w[1][i1], v0[i0][i1].y, b0);
+          a1 = fmaf(w[1][i1], v1[i0][i1].x, a1);
+          b1 = fmaf(w[1][i1], v1[i0][i1].y, b1);
+        }
+        r0 = fmaf(w[0][i0], a0, r0);
+        m0 = fmaf(w[0][i0], b0, m0);
+        r1 = fmaf(w[0][i0], a1, r1);
+        m1 = fmaf(w[0][i0], b1, m1);
       }
-    } else {
+      yo[(long long)c * g.K] = make_float2(r0 * s, m0 * s);
+      yo[(long long)(c + 1) * g.K] = make_float2(r1 * s, m1 * s);
+    }
+    for (; c < g.C; ++c) {
+      const float2* g0 = gb + (long long)c * g.gtot;
+      float r0 = 0.f, m0 = 0.f;
+#pragma unroll
+      for (int i0 = 0; i0 < W; ++i0) {
+        float a0 = 0.f, b0 = 0.f;
+#pragma unroll
+        for (int i1 = 0; i1 < W; ++i1) {
+          float2 v = __ldg(g0 + roff[i0] + nidx[1][i1]);
+          a0 = fmaf(w[1][i1], v.x, a0);
+          b0 = fmaf(w[1][i1], v.y, b0);
+        }
+        r0 = fmaf(w[0][i0], a0, r0);
+        m0 = fmaf(w[0][i0], b0, m0);
+      }
+      yo[(long long)c * g.K] = make_float2(r0 * s, m0 * s);
+    }
+  } else {
+    for (int c = 0; c < g.C; ++c) {
+      const float2* gc = gb + (long long)c * g.gtot;
+      float re = 0.f, im = 0.f;
 #pragma unroll
       for (int i0 = 0; i0 < W; ++i0) {
         float r1 = 0.f, im1 = 0.f;
 #pragma unroll
         for (int i1 = 0; i1 < W; ++i1) {
-          const float2* row = gc + ((long long)nidx[0][i0] * g.G[1] + nidx[ND > 2 ? 1 : 0][i1]) * g.G[ND - 1];
+          const float2* row = gc + ((long long)nidx[0][i0] * g.G[1] + nidx[1][i1]) * g.G[ND - 1];
           float r2 = 0.f, i2 = 0.f;
 #pragma unroll
           for (int i2x = 0; i2x < W; ++i2x) {
@@ -427,14 +475,14 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly
             r2 = fmaf(w[ND - 1][i2x], v.x, r2);
             i2 = fmaf(w[ND - 1][i2x], v.y, i2);
           }
-          r1 = fmaf(w[ND > 2 ? 1 : 0][i1], r2, r1);
-          im1 = fmaf(w[ND > 2 ? 1 : 0][i1], i2, im1);
+          r1 = fmaf(w[1][i1], r2, r1);
+          im1 = fmaf(w[1][i1], i2, im1);
         }
         re = fmaf(w[0][i0], r1, re);
         im = fmaf(w[0][i0], im1, im);
       }
+      yo[(long long)c * g.K] = make_float2(re * s, im * s);
     }
-    a.y[((long long)be * g.C + c) * g.K + k] = make_float2(re * s, im * s);
   }
 }
 
@@ -456,6 +504,11 @@ struct SpreadArgs {
   const float* wadj;
   const int* entries;
   const int* tile_start;
+  const int4* items;   // (key, chunk, partial slot or -1, chunks), heaviest first
+  int n_items;
+  int chunk;
+  float2* partials;    // (rep, slot, C, T^nd) partial tiles of split keys
+  int n_slots;
   float2* grid;
   int nb;
   int cpi;     // coils per work item
@@ -486,13 +539,19 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
   extern __shared__ float4 smem4[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   long long item = (long long)blockIdx.x * SPREAD_WARPS + warp;
-  long long nitems = (long long)a.nb * tg.ntiles * a.ngroups;
+  const long long reps = g.B == 1 ? a.nb : a.nb / g.B;
+  const long long nitems = reps * a.n_items * a.ngroups;
   if (item >= nitems) return;
+  // work items run heaviest (frame, tile) first; every frame of a B_eff batch
+  // that shares the trajectory frame repeats the same item list
   const int grp = (int)(item % a.ngroups);
-  const long long rest = item / a.ngroups;
-  const int tile = (int)(rest % tg.ntiles);
-  const int be = (int)(rest / tg.ntiles);
-  const int b = frame_of(be, a.nb, g.B);
+  const long long oi = item / a.ngroups;
+  const int4 it = a.items[oi % a.n_items];
+  const int rep = (int)(oi / a.n_items);
+  const int okey = it.x;
+  const int b = okey / tg.ntiles;
+  const int tile = okey - b * tg.ntiles;
+  const int be = (g.B == 1) ? rep : b * (a.nb / g.B) + rep;
   const int c0 = grp * a.cpi;
   const int nc = min(a.cpi, g.C - c0);
   int o[3];
@@ -505,10 +564,14 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
     o[1] = ((tile / tg.nt[2]) % tg.nt[1]) * T;
     o[0] = (tile / (tg.nt[2] * tg.nt[1])) * T;
   }
-  const int key = b * tg.ntiles + tile;
-  const int e0 = a.tile_start[key], e1 = a.tile_start[key + 1];
+  const int key = okey;
+  const int k0 = a.tile_start[key], k1 = a.tile_start[key + 1];
+  const int e0 = min(k1, k0 + it.y * a.chunk), e1 = min(k1, e0 + a.chunk);
   float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
   const int Gl = g.G[ND - 1];
+  // split keys write their partial tile (unpadded T^nd per coil) to a slot
+  constexpr int TN = ND == 2 ? T * T : T * T * T;
+  float2* pout = it.z >= 0 ? a.partials + (((long long)rep * a.n_slots + it.z) * g.C + c0) * TN : nullptr;
 
   // cells of the tile as float4 pairs along the last dim
   constexpr int PAIRS = (ND == 2 ? T * T : T * T * T) / 2;
@@ -533,7 +596,7 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
     return ok;
   };
 
-  if (e0 == e1) {   // no sample touches this tile: zeros
+  if (e0 == e1 && !pout) {   // no sample touches this tile: zeros
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = lane; i < nc * PAIRS; i += 32) {
       int cl = i / PAIRS, r = i - cl * PAIRS;
@@ -635,16 +698,115 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
       __syncwarp();
     }
   }
-  // write the whole tile once
+  // write the whole tile once (or this chunk's partial tile)
   for (int i = lane; i < nc * PAIRS; i += 32) {
     int cl = i / PAIRS, r = i - cl * PAIRS;
-    int n[3];
-    long long cell = cell_of_pair(r, n);
-    if (!in_grid(n)) continue;
     int l = (r % (T / 2)) * 2;
     int rr = r / (T / 2);
     const float2* src = ND == 2 ? acc + ((long long)cl * T + rr) * RS + l : acc + (long long)cl * CELLS + rr * T + l;
-    *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = *reinterpret_cast<const float4*>(src);
+    const float4 v = *reinterpret_cast<const float4*>(src);
+    if (pout) {
+      *reinterpret_cast<float4*>(pout + (long long)cl * TN + rr * T + l) = v;
+      continue;
+    }
+    int n[3];
+    long long cell = cell_of_pair(r, n);
+    if (!in_grid(n)) continue;
+    *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = v;
+  }
+}
+
+// Zeros for the tiles no sample touches: a store-only grid-stride pass, one
+// float4 (two cells) per thread, consecutive threads along tile rows.
+template <int ND, int T>
+__global__ void __launch_bounds__(256) zero_tiles_kernel(const int* __restrict__ keys, int n_empty,
+                                                         float2* __restrict__ grid, Geo g, TileGeo tg, int nb) {
+  // block = one (rep, empty key); threads over (coil, cell pair)
+  constexpr int PAIRS = (ND == 2 ? T * T : T * T * T) / 2;
+  const int key = keys[blockIdx.x % n_empty];
+  const int rep = blockIdx.x / n_empty;
+  const int b = key / tg.ntiles;
+  const int tile = key - b * tg.ntiles;
+  const int be = (g.B == 1) ? rep : b * (nb / g.B) + rep;
+  int o0, o1, o2 = 0;
+  if (ND == 2) {
+    o0 = (tile / tg.nt[1]) * T;
+    o1 = (tile % tg.nt[1]) * T;
+  } else {
+    o2 = (tile % tg.nt[2]) * T;
+    o1 = ((tile / tg.nt[2]) % tg.nt[1]) * T;
+    o0 = (tile / (tg.nt[2] * tg.nt[1])) * T;
+  }
+  float2* base = grid + (long long)be * g.C * g.gtot;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = threadIdx.x; i < g.C * PAIRS; i += blockDim.x) {
+    const int c = i / PAIRS, r = i - c * PAIRS;
+    const int l = (r % (T / 2)) * 2;
+    const int rr = r / (T / 2);
+    int n0, n1, n2;
+    long long idx;
+    if (ND == 2) {
+      n0 = o0 + rr;
+      n1 = o1 + l;
+      if (n0 >= g.G[0] || n1 >= g.G[1]) continue;
+      idx = (long long)n0 * g.G[1] + n1;
+    } else {
+      n0 = o0 + rr / T;
+      n1 = o1 + rr % T;
+      n2 = o2 + l;
+      if (n0 >= g.G[0] || n1 >= g.G[1] || n2 >= g.G[2]) continue;
+      idx = ((long long)n0 * g.G[1] + n1) * g.G[2] + n2;
+    }
+    *reinterpret_cast<float4*>(base + (long long)c * g.gtot + idx) = z4;
+  }
+}
+
+// Sum of the chunk partial tiles of split keys, in chunk order, written once
+// into the grid.  Block = (rep, split key, coil); threads over the tile cells.
+template <int ND, int T>
+__global__ void __launch_bounds__(256) spread_reduce_kernel(const float2* __restrict__ partials,
+                                                            const int4* __restrict__ multi, int n_multi,
+                                                            int n_slots, float2* __restrict__ grid, Geo g,
+                                                            TileGeo tg, int nb) {
+  constexpr int TN = ND == 2 ? T * T : T * T * T;
+  const int c = blockIdx.y;
+  const int rep = blockIdx.z;
+  const int4 m = multi[blockIdx.x];
+  const int b = m.x / tg.ntiles;
+  const int tile = m.x - b * tg.ntiles;
+  const int be = (g.B == 1) ? rep : b * (nb / g.B) + rep;
+  int o[3];
+  if (ND == 2) {
+    o[0] = (tile / tg.nt[1]) * T;
+    o[1] = (tile % tg.nt[1]) * T;
+    o[2] = 0;
+  } else {
+    o[2] = (tile % tg.nt[2]) * T;
+    o[1] = ((tile / tg.nt[2]) % tg.nt[1]) * T;
+    o[0] = (tile / (tg.nt[2] * tg.nt[1])) * T;
+  }
+  for (int cell = threadIdx.x; cell < TN; cell += blockDim.x) {
+    float sx = 0.f, sy = 0.f;
+    for (int j = 0; j < m.y; ++j) {
+      float2 v = partials[(((long long)rep * n_slots + m.z + j) * g.C + c) * TN + cell];
+      sx += v.x;
+      sy += v.y;
+    }
+    int n0, n1, n2 = 0;
+    long long idx;
+    if (ND == 2) {
+      n0 = o[0] + cell / T;
+      n1 = o[1] + cell % T;
+      if (n0 >= g.G[0] || n1 >= g.G[1]) continue;
+      idx = (long long)n0 * g.G[1] + n1;
+    } else {
+      n0 = o[0] + cell / (T * T);
+      n1 = o[1] + (cell / T) % T;
+      n2 = o[2] + cell % T;
+      if (n0 >= g.G[0] || n1 >= g.G[1] || n2 >= g.G[2]) continue;
+      idx = ((long long)n0 * g.G[1] + n1) * g.G[2] + n2;
+    }
+    grid[((long long)be * g.C + c) * g.gtot + idx] = make_float2(sx, sy);
   }
 }
 
@@ -806,7 +968,7 @@ extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int 
 extern "C" int mrb_plan_destroy(mrb_plan* p) {
   if (!p) return 0;
   if (p->fft) cufftDestroy(p->fft);
-  for (DevBuf* b : {&p->gx, &p->entries, &p->tile_start, &p->sorted_k, &p->maps, &p->invdeap, &p->wfwd,
+  for (DevBuf* b : {&p->gx, &p->entries, &p->tile_start, &p->items, &p->multi, &p->partials, &p->empty_keys, &p->maps, &p->invdeap, &p->wfwd,
                     &p->wadj, &p->grid, &p->tmp})
     b->release();
   delete p;
@@ -829,6 +991,11 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
     case 2:
       MRB_REQUIRE(value == 0 || value == 1, "interp mode must be 0 or 1");
       p->interp_mode = (int)value;
+      return 0;
+    case 3:
+      MRB_REQUIRE(value >= 16 && value <= (1 << 20), "chunk must be 16 .. 2^20 samples");
+      p->chunk = (int)value;
+      p->have_points = false;   // the item table depends on it
       return 0;
     default:
       return mrb::fail(MRB_EINVAL, "unknown option %d", key);
@@ -902,6 +1069,55 @@ extern "C" int mrb_plan_set_points(mrb_plan* p, const float* traj, mrb_stream_t 
     fill_int_kernel<<<grid_blocks(nkeys + 1, 256), 256, 0, st>>>(p->tile_start.as<int>(), nkeys + 1, 0);
   }
   MRB_LAUNCH_CHECK();
+  // spread work items: (frame, tile) keys heaviest first, each split into
+  // chunks of at most p->chunk samples; a key with several chunks gets
+  // partial-tile slots that a second pass sums in chunk order
+  {
+    std::vector<int> ts((size_t)nkeys + 1);
+    MRB_CUDA_TRY(cudaMemcpyAsync(ts.data(), p->tile_start.p, ts.size() * sizeof(int), cudaMemcpyDeviceToHost, st));
+    MRB_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<int> order((size_t)nkeys);
+    for (int k = 0; k < nkeys; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return ts[a + 1] - ts[a] > ts[b + 1] - ts[b]; });
+    std::vector<int4> items, multi;
+    std::vector<int> empty;
+    items.reserve((size_t)nkeys);
+    int slots = 0;
+    for (int key : order) {
+      int cnt = ts[key + 1] - ts[key];
+      if (cnt == 0) {
+        empty.push_back(key);
+        continue;
+      }
+      int nch = (cnt + p->chunk - 1) / p->chunk;
+      int base = -1;
+      if (nch > 1) {
+        base = slots;
+        slots += nch;
+        multi.push_back(make_int4(key, nch, base, 0));
+      }
+      for (int c = 0; c < nch; ++c) items.push_back(make_int4(key, c, nch > 1 ? base + c : -1, nch));
+    }
+    MRB_REQUIRE(items.size() < (1u << 31), "too many spread work items");
+    std::sort(empty.begin(), empty.end());
+    p->n_empty = (int)empty.size();
+    if (!empty.empty()) {
+      if ((rc = p->empty_keys.ensure(empty.size() * sizeof(int)))) return rc;
+      MRB_CUDA_TRY(cudaMemcpy(p->empty_keys.p, empty.data(), empty.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    p->n_items = (int)items.size();
+    p->n_multi = (int)multi.size();
+    p->n_slots = slots;
+    if (!items.empty()) {
+      if ((rc = p->items.ensure(items.size() * sizeof(int4)))) return rc;
+      MRB_CUDA_TRY(cudaMemcpy(p->items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
+    if (!multi.empty()) {
+      if ((rc = p->multi.ensure(multi.size() * sizeof(int4)))) return rc;
+      MRB_CUDA_TRY(cudaMemcpy(p->multi.p, multi.data(), multi.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
+  }
 
   // touched cells (sum over frames), for the roofline bookkeeping
   {
@@ -1031,12 +1247,23 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     a.wadj = p->has_wadj ? p->wadj.as<float>() : nullptr;
     a.entries = p->entries.as<int>();
     a.tile_start = p->tile_start.as<int>();
+    a.items = p->items.as<int4>();
+    a.n_items = p->n_items;
+    a.chunk = p->chunk;
+    a.n_slots = p->n_slots;
     a.grid = p->grid.as<float2>();
+    const int reps = p->B == 1 ? nb : nb / p->B;
+    if (p->n_slots > 0) {
+      int rc2 = p->partials.ensure((size_t)reps * p->n_slots * p->C * (p->nd == 2 ? tg.T * tg.T : tg.T * tg.T * tg.T) *
+                                   sizeof(float2));
+      if (rc2) return rc2;
+    }
+    a.partials = p->partials.as<float2>();
     a.nb = nb;
     a.cpi = p->coils_per_item;
     a.ngroups = (p->C + a.cpi - 1) / a.cpi;
     a.gsign = p->gsign;
-    long long items = (long long)nb * tg.ntiles * a.ngroups;
+    long long items = (long long)reps * p->n_items * a.ngroups;
     int blocks = grid_blocks(items, SPREAD_WARPS);
     const void* fn = nullptr;
     size_t smem = 0;
@@ -1058,9 +1285,45 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       MRB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       p->spread_smem_set = smem;
     }
-    void* args[] = {&a, &g, &tg, &p->kb};
-    MRB_CUDA_TRY(cudaLaunchKernel(fn, dim3(blocks), dim3(SPREAD_WARPS * 32), args, smem, st));
-    MRB_LAUNCH_CHECK();
+    if (p->n_empty > 0) {
+      long long zbl = (long long)reps * p->n_empty;
+      MRB_REQUIRE(zbl < (1LL << 31), "too many empty tiles");
+      int zb = (int)zbl;
+      const int* ek = p->empty_keys.as<int>();
+      float2* gridp = p->grid.as<float2>();
+#define MRB_ZERO_CASE(ND_, T_)                                                                            \
+  if (p->nd == ND_ && tg.T == T_) zero_tiles_kernel<ND_, T_><<<zb, 256, 0, st>>>(ek, p->n_empty, gridp, g, tg, nb);
+      MRB_ZERO_CASE(2, 4)
+      MRB_ZERO_CASE(2, 8)
+      MRB_ZERO_CASE(2, 16)
+      MRB_ZERO_CASE(2, 32)
+      MRB_ZERO_CASE(3, 4)
+      MRB_ZERO_CASE(3, 8)
+#undef MRB_ZERO_CASE
+      MRB_LAUNCH_CHECK();
+    }
+    if (items > 0) {
+      void* args[] = {&a, &g, &tg, &p->kb};
+      MRB_CUDA_TRY(cudaLaunchKernel(fn, dim3(blocks), dim3(SPREAD_WARPS * 32), args, smem, st));
+      MRB_LAUNCH_CHECK();
+    }
+    if (p->n_multi > 0) {
+      MRB_REQUIRE(reps <= 65535 && p->C <= 65535, "too many frames for the split-tile reduction");
+      dim3 rg(p->n_multi, p->C, reps);
+      const float2* part = p->partials.as<float2>();
+      const int4* mt = p->multi.as<int4>();
+      float2* gridp = p->grid.as<float2>();
+      if (p->nd == 2) {
+        if (tg.T == 4) spread_reduce_kernel<2, 4><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
+        if (tg.T == 8) spread_reduce_kernel<2, 8><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
+        if (tg.T == 16) spread_reduce_kernel<2, 16><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
+        if (tg.T == 32) spread_reduce_kernel<2, 32><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
+      } else {
+        if (tg.T == 4) spread_reduce_kernel<3, 4><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
+        if (tg.T == 8) spread_reduce_kernel<3, 8><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
+      }
+      MRB_LAUNCH_CHECK();
+    }
     return 0;
   }
   if (stage == 5) {

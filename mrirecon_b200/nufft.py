@@ -31,7 +31,7 @@ from .layout import (AxisSpec, plan_image_layout, plan_kspace_layout, plan_image
                      plan_kspace_layout_from_sizes, user_image_shape, user_kspace_shape)
 from .roles import Roles
 
-OPT_TILE, OPT_COILS_PER_ITEM, OPT_INTERP_MODE = 0, 1, 2
+OPT_TILE, OPT_COILS_PER_ITEM, OPT_INTERP_MODE, OPT_CHUNK = 0, 1, 2, 3
 _DCF_MODES = {"none": 0, "balanced": 1, "standard": 2}
 
 
@@ -171,6 +171,9 @@ class B200NUFFTAdapter:
     norm: Literal["ortho", "none"] = "ortho"
     tile: Optional[int] = None
     coils_per_item: Optional[int] = None
+    chunk: Optional[int] = None
+    autotune: bool = False
+    tuned: Optional[dict] = None
 
     _im_shape: Optional[Tuple[int, ...]] = None
     _maps: Optional[torch.Tensor] = None
@@ -231,9 +234,14 @@ class B200NUFFTAdapter:
                 plan.set_option(OPT_TILE, self.tile)
             if self.coils_per_item is not None:
                 plan.set_option(OPT_COILS_PER_ITEM, self.coils_per_item)
+            if self.chunk is not None:
+                plan.set_option(OPT_CHUNK, self.chunk)
             plan.set_points(self._traj_BndK)
             plan.set_dcf(self._dcf_BK, self.dcf_mode, self.apply_dcf_in_fwd, self.apply_dcf_in_adj)
             plan.set_maps(self._maps)
+            if self.autotune:
+                from .autotune import tune
+                self.tuned = tune(plan, self._traj_BndK)
         self._plan = plan
         self._alpha_scalar = None
 
@@ -365,6 +373,7 @@ class NUFFTConfig:
     kwidth: int = 4
     osf: float = 2.0
     norm: Literal["ortho", "none"] = "ortho"
+    autotune: bool = False
 
 
 class NUFFT:
@@ -392,7 +401,7 @@ class NUFFT:
             self._dcf_BK = d.to(self.device, dtype=torch.float32).contiguous()
         be = B200NUFFTAdapter(ndim=ndim, traj_units=config.traj_units, dcf_mode=config.dcf_mode,
                               apply_dcf_in_fwd=config.apply_dcf_in_fwd, apply_dcf_in_adj=config.apply_dcf_in_adj,
-                              kwidth=config.kwidth, osf=config.osf, norm=config.norm)
+                              kwidth=config.kwidth, osf=config.osf, norm=config.norm, autotune=config.autotune)
         self._backend = be
         im_shape = (int(maps.shape[0]),) + tuple(int(s) for s in maps.shape[1:])
         be.prepare(im_shape, self._traj_BndK, self._dcf_BK, maps.to(self.device, dtype=dtype).contiguous(),

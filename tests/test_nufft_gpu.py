@@ -109,11 +109,19 @@ def test_dcf_modes(cuda, mode, fwd, adj):
     _check_pair(maps, traj, dcf, dcf_mode=mode, apply_dcf_in_fwd=fwd, apply_dcf_in_adj=adj)
 
 
-def test_beff_repeat_interleave(cuda):
+@pytest.mark.parametrize("chunk", [None, 16])
+def test_beff_repeat_interleave(cuda, chunk):
     """B_eff = 2*B uses trajectory frame be // 2 (torchkb _expand_omega)."""
     maps = _rand_c((2, 16, 16), 4, torch.complex64)
     traj = phantoms.random_traj(2, 2, 400, seed=4)
-    _check_pair(maps, traj, nb=4)
+    _check_pair(maps, traj, nb=4, chunk=chunk)
+
+
+def test_single_frame_expanded(cuda):
+    """B = 1 trajectory applied to B_eff = 3 images (the expand branch)."""
+    maps = _rand_c((2, 20, 20), 14, torch.complex64)
+    traj = phantoms.golden_angle_radial(24, 40).unsqueeze(0)
+    _check_pair(maps, traj, nb=3, chunk=16)
 
 
 def test_unnormalised(cuda):
@@ -122,25 +130,36 @@ def test_unnormalised(cuda):
     _check_pair(maps, traj, norm="none")
 
 
-@pytest.mark.parametrize("tile,cpi", [(8, 1), (16, 2), (32, 3), (4, 4)])
-def test_tiling_options_identical(cuda, tile, cpi):
-    """Every tile / coil-group choice gives the same (deterministic) grid."""
+@pytest.mark.parametrize("tile,cpi,chunk", [(8, 1, None), (16, 2, 16), (32, 3, 64), (4, 4, None), (16, 4, 100000)])
+def test_tiling_options_identical(cuda, tile, cpi, chunk):
+    """Every tile / coil-group / chunk choice gives the same grid (up to the
+    summation order of split tiles), deterministically."""
     maps = phantoms.coil_maps(64, 5).to(torch.complex64)
     traj = phantoms.grasp_trajectory(2, 13, 128)
     y = _rand_c((2, 5, traj.shape[-1]), 3, torch.complex64).to(cuda)
     ref = _adapter(maps, traj).AH(y)
-    ad = _adapter(maps, traj, tile=tile, coils_per_item=cpi)
+    ad = _adapter(maps, traj, tile=tile, coils_per_item=cpi, chunk=chunk)
     out = ad.AH(y)
     assert rel(out, ref) < 1e-6
     out2 = ad.AH(y)
     assert torch.equal(out, out2)
 
 
-def test_3d_vs_oracle(cuda):
+@pytest.mark.parametrize("chunk", [None, 16])
+def test_3d_vs_oracle(cuda, chunk):
     S = (12, 10, 8)
     maps = _rand_c((2,) + S, 12, torch.complex64)
     traj = phantoms.random_traj(2, 3, 700, seed=13)
-    _check_pair(maps, traj)
+    _check_pair(maps, traj, chunk=chunk)
+
+
+def test_3d_radial_koosh(cuda):
+    """Golden-means koosh-ball spokes: every spoke crosses the centre tile, which
+    is split into many chunks."""
+    S = (24, 24, 24)
+    maps = phantoms.coil_maps(24, 3, ndim=3).to(torch.complex64)
+    traj = phantoms.golden_means_koosh(300, 48).unsqueeze(0)
+    _check_pair(maps, traj, chunk=32)
 
 
 def test_vs_nudft_fixture(cuda):
@@ -212,3 +231,19 @@ def test_coil_images_forward(cuda):
     orc = okb.KBNufft(torch.ones((1,) + S, dtype=torch.complex128), traj, None)
     ya = torch.cat([orc.A(xc[:, c:c + 1]) for c in range(C)], dim=1)
     assert rel(y, ya) < TOL
+
+
+def test_autotuner_picks_a_timed_candidate(cuda, tmp_path, monkeypatch):
+    """The autotuner times the spread candidates on the plan's trajectory, keeps
+    the fastest, caches it per size class, and the tuned plan still matches the oracle."""
+    monkeypatch.setenv("MRB_TUNE_CACHE", str(tmp_path / "tune.json"))
+    maps = phantoms.coil_maps(48, 4).to(torch.complex64)
+    traj = phantoms.grasp_trajectory(3, 9, 96)
+    ad = _check_pair(maps, traj, autotune=True)
+    assert ad.tuned is not None and not ad.tuned.get("cached")
+    best = ad.tuned
+    assert best["ms"] == min(t["ms"] for t in best["tried"])
+    info = ad.plan.info()
+    assert (info["tile"], info["coils_per_item"]) == (best["tile"], best["cpi"])
+    ad2 = _check_pair(maps, traj, autotune=True)
+    assert ad2.tuned.get("cached") and ad2.tuned["tile"] == best["tile"]
