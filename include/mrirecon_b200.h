@@ -167,6 +167,8 @@ typedef struct mrb_tv_term {
   int naxes;             /* <= 4 */
   int axes[4];           /* axis ids of the (F, 1, *S) image: 0 = frame, 2.. = spatial */
   float axis_weights[4]; /* per-axis scale of the forward differences */
+  int frame_period;      /* > 0: the frame axis holds independent series of this many
+                            frames (no difference across series boundaries); 0: one series */
 } mrb_tv_term;
 
 /* At z = x + t*d (d may be NULL) for an image (F, 1, *S) complex64 with

@@ -34,6 +34,7 @@ class TVTerm(ct.Structure):
         ("naxes", ct.c_int),
         ("axes", ct.c_int * 4),
         ("axis_weights", ct.c_float * 4),
+        ("frame_period", ct.c_int),
     ]
 
 

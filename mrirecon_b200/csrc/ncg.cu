@@ -667,6 +667,15 @@ int build_plan(TVPlan& P, int nd, const int* S, int F, const mrb_tv_term* terms,
   MRB_REQUIRE(n < (1LL << 31), "image too large for the TV kernels (%lld voxels)", n);
   P.n = (unsigned)n;
   int slot_of[5] = {-1, -1, -1, -1, -1};
+  int period = 0;
+  for (int i = 0; i < nterms; ++i)
+    if (terms[i].enabled && terms[i].frame_period > 0) {
+      MRB_REQUIRE(period == 0 || period == terms[i].frame_period, "TV terms disagree on the frame period");
+      MRB_REQUIRE(F % terms[i].frame_period == 0, "frame period %d does not divide %d frames",
+                  terms[i].frame_period, F);
+      period = terms[i].frame_period;
+    }
+  if (period > 0) asize[0] = period;   // coordinates along frames are taken within a series
   int k = 0;
   for (int i = 0; i < nterms; ++i) {
     const mrb_tv_term& t = terms[i];

@@ -58,7 +58,7 @@ class RegContext:
     halo_map: Optional[dict] = None
 
 
-def tv_term_struct(params: TVParams, axes: Sequence[int]) -> _lib.TVTerm:
+def tv_term_struct(params: TVParams, axes: Sequence[int], frame_period: int = 0) -> _lib.TVTerm:
     if len(axes) > 4:
         raise ValueError("the fused TV kernel supports at most 4 axes per term")
     t = _lib.TVTerm()
@@ -73,6 +73,7 @@ def tv_term_struct(params: TVParams, axes: Sequence[int]) -> _lib.TVTerm:
     for i, (a, w) in enumerate(zip(axes, aw)):
         t.axes[i] = int(a)
         t.axis_weights[i] = float(w)
+    t.frame_period = int(frame_period)
     return t
 
 
@@ -152,13 +153,15 @@ class RegManager:
     def regs(self) -> List[TVND]:
         return self._regs
 
-    def terms(self, roles: Roles) -> List[_lib.TVTerm]:
+    def terms(self, roles: Roles, series_length: int = 0) -> List[_lib.TVTerm]:
+        """Kernel descriptors of the active TV terms.  series_length > 0 splits the
+        frame axis into independent series (several problems solved in one batch)."""
         out = []
         for r in self._regs:
             if not isinstance(r.params, TVParams):
                 raise TypeError(f"regulariser {r.name!r} is not a TV term")
             axes = roles.resolve_axes(r.params.axes)
-            t = tv_term_struct(r.params, axes)
+            t = tv_term_struct(r.params, axes, series_length)
             if t.enabled:
                 out.append(t)
         if len(out) > 4:

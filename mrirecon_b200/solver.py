@@ -71,6 +71,9 @@ class CGConfig:
     stop_tol: float = 1e-4
     cuda_graph: bool = True
     iters_per_graph: int = 8
+    # > 0: the frame axis holds independent series of this many frames (a batch of
+    # separate problems; temporal TV does not couple series)
+    series_length: int = 0
 
 
 class _Shard:
@@ -140,7 +143,7 @@ class CGSolver:
         self.nd = len(ishape) - 2
         self.S = tuple(int(s) for s in ishape[2:])
         self.F = int(ishape[0])
-        self.terms = regm.terms(roles) if regm is not None else []
+        self.terms = regm.terms(roles, c.series_length) if regm is not None else []
         self.nterms = len(self.terms)
         self._terms_arr = (_lib.TVTerm * max(1, self.nterms))(*self.terms)
         self._Sarr = (ct.c_int * 3)(*(list(self.S) + [1] * (3 - self.nd)))

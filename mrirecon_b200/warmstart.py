@@ -1,0 +1,431 @@
+"""Learned warm start for GRASP-style NCG: a BF16 2D+t residual CNN.
+
+The network (3 levels, 32 base channels, 3x3x3 convolutions over (t, y, x),
+U-Net skips, output = input + net(input)) maps a normalised adjoint
+reconstruction to an estimate of the converged NCG reconstruction.  It is
+trained on pairs (adjoint recon -> converged NCG recon) that the solver of
+this package generates on seeded synthetic phantoms, with the project's own
+CUDA kernels (``csrc/cnn.cu``): BF16 tensor-core implicit-GEMM convolution
+forward / data gradient / weight gradient, FP32 accumulation and FP32 master
+weights updated by Adam.  NCG always runs after it to the same objective
+tolerance, and it is only used when its objective is below the adjoint
+start's (``warm_start``).  The reference has no learned component.
+
+Layers (kernel channel counts; the input is padded to 32 channels, the last
+layer's 2 outputs to 32):
+  c1 2->32, c2 32->32 = B1; pool; c3 32->64, c4 64->64 = B2; pool; c5 64->128;
+  up; c6 [up(c5), B2] 192->64; up; c7 [up(c6), B1] 96->32; c8 32->2.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import math
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib
+
+# name, kernel cin (padded), real cin, coutp (padded), real cout, relu
+LAYERS: List[Tuple[str, int, int, int, int, bool]] = [
+    ("c1", 32, 2, 32, 32, True), ("c2", 32, 32, 32, 32, True), ("c3", 32, 32, 64, 64, True),
+    ("c4", 64, 64, 64, 64, True), ("c5", 64, 64, 128, 128, True), ("c6", 192, 192, 64, 64, True),
+    ("c7", 96, 96, 32, 32, True), ("c8", 32, 32, 32, 2, False)]
+XC = 32          # channels of the packed input tensor
+
+_SIGS = {
+    "mrb_cnn_conv3d_fwd": [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p,
+                           ct.c_int, ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_int, ct.c_int,
+                           ct.c_void_p, ct.c_void_p],
+    "mrb_cnn_conv3d_wgrad": [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_int, ct.c_int,
+                             ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_void_p],
+    "mrb_cnn_flip_weights": [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_void_p],
+    "mrb_cnn_relu_bwd": [ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_int64,
+                         ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p],
+    "mrb_cnn_pool2": [ct.c_int, ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int,
+                      ct.c_int, ct.c_void_p],
+    "mrb_cnn_up2": [ct.c_int, ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_int,
+                    ct.c_void_p],
+    "mrb_cnn_pack": [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p],
+    "mrb_cnn_unpack": [ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p],
+    "mrb_cnn_mse": [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                    ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_void_p],
+    "mrb_cnn_adam": [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_float, ct.c_float,
+                     ct.c_float, ct.c_float, ct.c_int, ct.c_void_p, ct.c_void_p],
+    "mrb_cnn_to_bf16": [ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_void_p],
+}
+
+
+def _lib_cnn():
+    lib = _lib.load()
+    if not getattr(lib, "_cnn_sigs", False):
+        for n, args in _SIGS.items():
+            f = getattr(lib, n)
+            f.restype = ct.c_int
+            f.argtypes = args
+        lib._cnn_sigs = True
+    return lib
+
+
+def _p(t):
+    return _lib.ptr(t)
+
+
+def _vol(Nb, D, H, W):
+    return (ct.c_int * 4)(Nb, D, H, W)
+
+
+class WarmStartCNN:
+    """Weights, Adam state and activation buffers of the warm-start network."""
+
+    def __init__(self, device="cuda", seed: int = 0):
+        self.device = torch.device(device)
+        self.lib = _lib_cnn()
+        g = torch.Generator().manual_seed(seed)
+        self.w32: Dict[str, torch.Tensor] = {}
+        self.b32: Dict[str, torch.Tensor] = {}
+        for name, cinp, cin, coutp, cout, relu in LAYERS:
+            w = torch.zeros((27, cinp, coutp), dtype=torch.float32)
+            std = math.sqrt(2.0 / (27 * cin)) * (0.1 if name == "c8" else 1.0)
+            w[:, :cin, :cout] = torch.randn((27, cin, cout), generator=g) * std
+            self.w32[name] = w.to(self.device)
+            self.b32[name] = torch.zeros(coutp, dtype=torch.float32, device=self.device)
+        self.step = 0
+        self.m = {k: torch.zeros_like(v) for k, v in self._params()}
+        self.v = {k: torch.zeros_like(v) for k, v in self._params()}
+        self._bufs: Dict[tuple, dict] = {}
+        self.refresh()
+
+    # -------------------------------------------------------------- parameters
+    def _params(self):
+        for name, *_ in LAYERS:
+            yield "w:" + name, self.w32[name]
+            yield "b:" + name, self.b32[name]
+
+    def refresh(self):
+        """BF16 weights for the forward pass and flipped BF16 weights for the data gradient."""
+        st = _lib.stream_ptr(self.device)
+        self.wb, self.wd = {}, {}
+        for name, cinp, cin, coutp, cout, relu in LAYERS:
+            wb = torch.empty((27, cinp, coutp), dtype=torch.bfloat16, device=self.device)
+            _lib.check(self.lib.mrb_cnn_to_bf16(_p(self.w32[name]), wb.numel(), _p(wb), st), "to_bf16")
+            self.wb[name] = wb
+            wd = torch.empty((27, coutp, cinp), dtype=torch.bfloat16, device=self.device)
+            _lib.check(self.lib.mrb_cnn_flip_weights(_p(wb), cinp, coutp, _p(wd), cinp, st), "flip")
+            self.wd[name] = wd
+
+    def state_dict(self):
+        return {k: v.detach().cpu().numpy() for k, v in self._params()}
+
+    def load_state_dict(self, d):
+        for name, *_ in LAYERS:
+            self.w32[name].copy_(torch.as_tensor(np.asarray(d["w:" + name])))
+            self.b32[name].copy_(torch.as_tensor(np.asarray(d["b:" + name])))
+        self.refresh()
+
+    def save(self, path):
+        np.savez_compressed(path, **self.state_dict())
+
+    def load(self, path):
+        self.load_state_dict(np.load(path))
+        return self
+
+    # ------------------------------------------------------------------ buffers
+    def _buffers(self, Nb, D, H, W, train: bool):
+        key = (Nb, D, H, W, train)
+        b = self._bufs.get(key)
+        if b is not None:
+            return b
+        if H % 4 or W % 4:
+            raise ValueError("the warm-start network needs H and W divisible by 4")
+        dev = self.device
+        bf = lambda *s: torch.zeros(s, dtype=torch.bfloat16, device=dev)
+        f32 = lambda *s: torch.zeros(s, dtype=torch.float32, device=dev)
+        V1, V2, V3 = Nb * D * H * W, Nb * D * (H // 2) * (W // 2), Nb * D * (H // 4) * (W // 4)
+        b = dict(X0=bf(V1, XC), A1=bf(V1, 32), CAT1=bf(V1, 96), P1=bf(V2, 32), A2=bf(V2, 64), CAT2=bf(V2, 192),
+                 P2=bf(V3, 64), A3=bf(V3, 128), C2=bf(V2, 64), C1=bf(V1, 32), O=f32(V1, 32),
+                 scale=f32(Nb), loss=torch.zeros(1, dtype=torch.float64, device=dev))
+        if train:
+            b.update(gO=f32(V1, 32), gC1=f32(V1, 32), gCAT1=f32(V1, 96), gC2=f32(V2, 64), gCAT2=f32(V2, 192),
+                     gA3=f32(V3, 128), gP2=f32(V3, 64), gA2=f32(V2, 64), gP1=f32(V2, 32), gA1=f32(V1, 32),
+                     gz32=bf(V1, 32), gz64=bf(V2, 64), gz128=bf(V3, 128), gz32h=bf(V2, 32),
+                     lpart=torch.zeros((V1 + 255) // 256, dtype=torch.float64, device=dev))
+            self.dw = {n: torch.zeros_like(self.w32[n]) for n, *_ in LAYERS}
+            self.db = {n: torch.zeros_like(self.b32[n]) for n, *_ in LAYERS}
+            wmax = max(27 * cinp * coutp for _, cinp, _, coutp, _, _ in LAYERS)
+            b["wpart"] = torch.zeros(wmax * 64, dtype=torch.float32, device=dev)
+        self._bufs[key] = b
+        return b
+
+    # ----------------------------------------------------------------- forward
+    def _conv(self, name, x, cx, xoff, vol, yb=None, cyb=0, ybo=0, yf=None, cyf=0, yfo=0, acc=0, weights=None,
+              cin=None, coutp=None, cout=None, relu=None, bias=True):
+        _, cinp, _, coutp_l, cout_l, relu_l = next(l for l in LAYERS if l[0] == name)
+        w = self.wb[name] if weights is None else weights
+        _lib.check(self.lib.mrb_cnn_conv3d_fwd(
+            _p(x), cx, xoff, cinp if cin is None else cin, _p(w), coutp_l if coutp is None else coutp,
+            cout_l if cout is None else cout, _p(self.b32[name]) if bias else None,
+            int(relu_l if relu is None else relu), _p(yb), cyb, ybo, _p(yf), cyf, yfo, acc, vol,
+            _lib.stream_ptr(self.device)), f"conv {name}")
+
+    def forward(self, z: torch.Tensor, train: bool = False) -> dict:
+        """z (Nb, D, H, W) complex64 (normalised by the per-series scale) -> buffers with O."""
+        Nb, D, H, W = (int(s) for s in z.shape)
+        b = self._buffers(Nb, D, H, W, train)
+        st = _lib.stream_ptr(self.device)
+        L = self.lib
+        v1, v2, v3 = _vol(Nb, D, H, W), _vol(Nb, D, H // 2, W // 2), _vol(Nb, D, H // 4, W // 4)
+        _lib.check(L.mrb_cnn_pack(_p(z), _p(b["scale"]), v1, _p(b["X0"]), XC, st), "pack")
+        self._conv("c1", b["X0"], XC, 0, v1, yb=b["A1"], cyb=32)
+        self._conv("c2", b["A1"], 32, 0, v1, yb=b["CAT1"], cyb=96, ybo=64)
+        _lib.check(L.mrb_cnn_pool2(0, _p(b["CAT1"]), 96, 64, 32, v1, _p(b["P1"]), 32, 0, st), "pool1")
+        self._conv("c3", b["P1"], 32, 0, v2, yb=b["A2"], cyb=64)
+        self._conv("c4", b["A2"], 64, 0, v2, yb=b["CAT2"], cyb=192, ybo=128)
+        _lib.check(L.mrb_cnn_pool2(0, _p(b["CAT2"]), 192, 128, 64, v2, _p(b["P2"]), 64, 0, st), "pool2")
+        self._conv("c5", b["P2"], 64, 0, v3, yb=b["A3"], cyb=128)
+        _lib.check(L.mrb_cnn_up2(0, _p(b["A3"]), 128, 0, 128, v3, _p(b["CAT2"]), 192, 0, st), "up2")
+        self._conv("c6", b["CAT2"], 192, 0, v2, yb=b["C2"], cyb=64)
+        _lib.check(L.mrb_cnn_up2(0, _p(b["C2"]), 64, 0, 64, v2, _p(b["CAT1"]), 96, 0, st), "up1")
+        self._conv("c7", b["CAT1"], 96, 0, v1, yb=b["C1"], cyb=32)
+        self._conv("c8", b["C1"], 32, 0, v1, yf=b["O"], cyf=32)
+        b["vols"] = (v1, v2, v3)
+        b["shape"] = (Nb, D, H, W)
+        return b
+
+    def set_scale(self, z: torch.Tensor) -> torch.Tensor:
+        """Per-series scale 1 / max|z| (written into the buffers used by forward)."""
+        Nb, D, H, W = (int(s) for s in z.shape)
+        s = 1.0 / z.reshape(Nb, -1).abs().amax(dim=1).clamp_min(1e-20)
+        for train in (False, True):
+            key = (Nb, D, H, W, train)
+            if key in self._bufs:
+                self._bufs[key]["scale"].copy_(s)
+        return s
+
+    @torch.no_grad()
+    def infer(self, z: torch.Tensor) -> torch.Tensor:
+        """Warm start for adjoint reconstructions z (Nb, D, H, W) complex64."""
+        z = z.to(torch.complex64).contiguous()
+        b = self._buffers(*(int(s) for s in z.shape), False)
+        self.set_scale(z)
+        self.forward(z, False)
+        out = torch.empty_like(z)
+        _lib.check(self.lib.mrb_cnn_unpack(_p(z), _p(b["O"]), 32, _p(b["scale"]), b["vols"][0], _p(out),
+                                           _lib.stream_ptr(self.device)), "unpack")
+        return out
+
+    # ---------------------------------------------------------------- training
+    def _wgrad(self, name, x, cx, xoff, gz, cg, goff, vol, b):
+        _, cinp, _, coutp, _, _ = next(l for l in LAYERS if l[0] == name)
+        _lib.check(self.lib.mrb_cnn_conv3d_wgrad(_p(x), cx, xoff, cinp, _p(gz), cg, goff, coutp, _p(self.dw[name]),
+                                                 _p(self.db[name]), _p(b["wpart"]), b["wpart"].numel(), vol,
+                                                 _lib.stream_ptr(self.device)), f"wgrad {name}")
+
+    def _dgrad(self, name, gz, cg, vol, gout, cgo, goff, acc=0):
+        _, cinp, _, coutp, _, _ = next(l for l in LAYERS if l[0] == name)
+        self._conv(name, gz, cg, 0, vol, yf=gout, cyf=cgo, yfo=goff, acc=acc, weights=self.wd[name],
+                   cin=coutp, coutp=cinp, cout=cinp, relu=False, bias=False)
+
+    def _relu_bwd(self, g, cgs, goff, act, cas, aoff, nch, V, gz, czs):
+        _lib.check(self.lib.mrb_cnn_relu_bwd(_p(g), cgs, goff, _p(act), cas, aoff, nch, V, _p(gz), czs, 0, czs,
+                                             _lib.stream_ptr(self.device)), "relu_bwd")
+
+    def loss_and_grad(self, z: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
+        """Forward + backward on one batch; leaves dW/db in self.dw/self.db; returns the loss (device)."""
+        Nb, D, H, W = (int(s) for s in z.shape)
+        b = self._buffers(Nb, D, H, W, True)
+        self.set_scale(z)
+        self.forward(z, True)
+        L, st = self.lib, _lib.stream_ptr(self.device)
+        v1, v2, v3 = b["vols"]
+        V1, V2, V3 = Nb * D * H * W, Nb * D * (H // 2) * (W // 2), Nb * D * (H // 4) * (W // 4)
+        _lib.check(L.mrb_cnn_mse(_p(z), _p(target), _p(b["O"]), 32, _p(b["scale"]), v1, _p(b["gO"]), _p(b["loss"]),
+                                 _p(b["lpart"]), b["lpart"].numel(), st), "mse")
+        # c8 (linear)
+        self._relu_bwd(b["gO"], 32, 0, None, 0, 0, 32, V1, b["gz32"], 32)
+        self._wgrad("c8", b["C1"], 32, 0, b["gz32"], 32, 0, v1, b)
+        self._dgrad("c8", b["gz32"], 32, v1, b["gC1"], 32, 0)
+        # c7
+        self._relu_bwd(b["gC1"], 32, 0, b["C1"], 32, 0, 32, V1, b["gz32"], 32)
+        self._wgrad("c7", b["CAT1"], 96, 0, b["gz32"], 32, 0, v1, b)
+        self._dgrad("c7", b["gz32"], 32, v1, b["gCAT1"], 96, 0)
+        # up1 -> C2, c6
+        _lib.check(L.mrb_cnn_up2(1, _p(b["gCAT1"]), 96, 0, 64, v2, _p(b["gC2"]), 64, 0, st), "up1 bwd")
+        self._relu_bwd(b["gC2"], 64, 0, b["C2"], 64, 0, 64, V2, b["gz64"], 64)
+        self._wgrad("c6", b["CAT2"], 192, 0, b["gz64"], 64, 0, v2, b)
+        self._dgrad("c6", b["gz64"], 64, v2, b["gCAT2"], 192, 0)
+        # up2 -> A3, c5
+        _lib.check(L.mrb_cnn_up2(1, _p(b["gCAT2"]), 192, 0, 128, v3, _p(b["gA3"]), 128, 0, st), "up2 bwd")
+        self._relu_bwd(b["gA3"], 128, 0, b["A3"], 128, 0, 128, V3, b["gz128"], 128)
+        self._wgrad("c5", b["P2"], 64, 0, b["gz128"], 128, 0, v3, b)
+        self._dgrad("c5", b["gz128"], 128, v3, b["gP2"], 64, 0)
+        # pool2 -> B2 (accumulate into the skip gradient), c4
+        _lib.check(L.mrb_cnn_pool2(1, _p(b["gP2"]), 64, 0, 64, v2, _p(b["gCAT2"]), 192, 128, st), "pool2 bwd")
+        self._relu_bwd(b["gCAT2"], 192, 128, b["CAT2"], 192, 128, 64, V2, b["gz64"], 64)
+        self._wgrad("c4", b["A2"], 64, 0, b["gz64"], 64, 0, v2, b)
+        self._dgrad("c4", b["gz64"], 64, v2, b["gA2"], 64, 0)
+        # c3
+        self._relu_bwd(b["gA2"], 64, 0, b["A2"], 64, 0, 64, V2, b["gz64"], 64)
+        self._wgrad("c3", b["P1"], 32, 0, b["gz64"], 64, 0, v2, b)
+        self._dgrad("c3", b["gz64"], 64, v2, b["gP1"], 32, 0)
+        # pool1 -> B1, c2
+        _lib.check(L.mrb_cnn_pool2(1, _p(b["gP1"]), 32, 0, 32, v1, _p(b["gCAT1"]), 96, 64, st), "pool1 bwd")
+        self._relu_bwd(b["gCAT1"], 96, 64, b["CAT1"], 96, 64, 32, V1, b["gz32"], 32)
+        self._wgrad("c2", b["A1"], 32, 0, b["gz32"], 32, 0, v1, b)
+        self._dgrad("c2", b["gz32"], 32, v1, b["gA1"], 32, 0)
+        # c1
+        self._relu_bwd(b["gA1"], 32, 0, b["A1"], 32, 0, 32, V1, b["gz32"], 32)
+        self._wgrad("c1", b["X0"], XC, 0, b["gz32"], 32, 0, v1, b)
+        return b["loss"]
+
+    def adam_step(self, lr: float = 1e-3, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8):
+        self.step += 1
+        st = _lib.stream_ptr(self.device)
+        for name, *_ in LAYERS:
+            for kind, p, gr in (("w:", self.w32[name], self.dw[name]), ("b:", self.b32[name], self.db[name])):
+                _lib.check(self.lib.mrb_cnn_adam(_p(p), _p(gr), _p(self.m[kind + name]), _p(self.v[kind + name]),
+                                                 p.numel(), lr, b1, b2, eps, self.step, None, st), "adam")
+        self.refresh()
+
+    def train(self, inputs: torch.Tensor, targets: torch.Tensor, epochs: int = 5, batch: int = 4,
+              lr: float = 1e-3, seed: int = 0, log=None) -> List[float]:
+        """inputs / targets (S, D, H, W) complex64 on the device; returns the mean loss per epoch."""
+        g = torch.Generator().manual_seed(seed)
+        S = int(inputs.shape[0])
+        hist = []
+        for ep in range(epochs):
+            perm = torch.randperm(S, generator=g)
+            tot = torch.zeros((), dtype=torch.float64, device=self.device)
+            nb = 0
+            for i in range(0, S - batch + 1, batch):
+                idx = perm[i:i + batch].to(self.device)
+                l = self.loss_and_grad(inputs[idx].contiguous(), targets[idx].contiguous())
+                tot += l[0]
+                nb += 1
+                self.adam_step(lr)
+            hist.append(float(tot) / max(1, nb))
+            if log:
+                log(f"epoch {ep}: loss {hist[-1]:.4e}")
+        return hist
+
+
+# ---------------------------------------------------------------------------
+# training pairs and the warm-start solve
+# ---------------------------------------------------------------------------
+@dataclass
+class PairSpec:
+    """Training series: the GRASP workload's acquisition (256^2, 12 coils, 21
+    golden-angle spokes x 512 samples per frame) over `frames` frames."""
+    N: int = 256
+    frames: int = 8
+    coils: int = 12
+    spokes: int = 21
+    nread: int = 512
+    lam_s: float = 1e-3
+    lam_t: float = 5e-3
+    eps: float = 1e-3
+    sigma: float = 1e-3
+    stop_tol: float = 5e-5
+    max_iter: int = 800
+
+
+def make_pairs(n_series: int, spec: PairSpec = PairSpec(), seed0: int = 1000, per_solve: int = 50,
+               device="cuda", log=None):
+    """(adjoint recon, converged NCG recon) pairs, (n_series, F, N, N) complex64 on the device.
+
+    Series s has phantom seed seed0 + s and golden-angle spokes that continue
+    across series; `per_solve` series are solved together in one NCG run whose
+    temporal TV does not couple series (the objective is separable, so each
+    series converges to its own minimiser)."""
+    from . import phantoms
+    from .nufft import B200NUFFTAdapter
+    from .regularization import RegManager, TVND, TVParams
+    from .solver import CGSolver, CGConfig
+    dev = torch.device(device)
+    F, N, C = spec.frames, spec.N, spec.coils
+    maps = phantoms.coil_maps(N, C).to(dev)
+    xs_adj, xs_ref = [], []
+    for s0 in range(0, n_series, per_solve):
+        P = min(per_solve, n_series - s0)
+        traj = torch.stack([phantoms.golden_angle_radial(spec.spokes, spec.nread, ((s0 + p) * F + f) * spec.spokes)
+                            for p in range(P) for f in range(F)]).to(dev)
+        xt = torch.cat([phantoms.dynamic_phantom(N, F, seed=seed0 + s0 + p) for p in range(P)]).unsqueeze(1)
+        ad = B200NUFFTAdapter(ndim=2)
+        ad.prepare((C, N, N), traj, None, maps, torch.complex64, dev)
+        y = ad.A(xt.to(dev))
+        if spec.sigma > 0:
+            y = phantoms.add_noise(y, spec.sigma, seed=seed0 + s0)
+        regm = RegManager([TVND("s", TVParams(weight=spec.lam_s, eps=spec.eps, axes="spatial")),
+                           TVND("t", TVParams(weight=spec.lam_t, eps=spec.eps, axes="temporal"))])
+        cfg = CGConfig(max_iter=spec.max_iter, stop_window=10, stop_tol=spec.stop_tol, series_length=F)
+        sol = CGSolver(y, ad, regm, cfg)
+        sol.run()
+        xs_ref.append(sol.result().reshape(P, F, N, N).clone())
+        xs_adj.append(ad.AH(y).reshape(P, F, N, N))
+        if log:
+            log(f"pairs {s0 + P}/{n_series}: {sol.iter} iterations ({sol.stop_reason})")
+    return torch.cat(xs_adj), torch.cat(xs_ref)
+
+
+def warm_start(solver, cnn: WarmStartCNN, adjoint: Optional[torch.Tensor] = None) -> dict:
+    """Initial image for `solver` from the network, with the fallback rule:
+    the network output is used only if its objective is below that of the
+    adjoint start (the adjoint recon scaled by its least-squares factor)."""
+    op = solver.op
+    y = solver.y
+    xa = op.AH(y) if adjoint is None else adjoint
+    Axa = op.A(xa)
+    den = float(torch.vdot(Axa.reshape(-1), Axa.reshape(-1)).real)
+    alpha = float(torch.vdot(Axa.reshape(-1), y.reshape(-1)).real) / max(den, 1e-30)
+    x_adj = (alpha * xa).to(torch.complex64)
+    F = int(xa.shape[0])
+    S = tuple(int(s) for s in xa.shape[2:])
+    # the network sees the raw adjoint, as in training (make_pairs); its output is
+    # then given its own least-squares data-consistency scale
+    x_net = cnn.infer(xa.to(torch.complex64).reshape((1, F) + S)).reshape(xa.shape)
+    Axn = op.A(x_net)
+    dn = float(torch.vdot(Axn.reshape(-1), Axn.reshape(-1)).real)
+    x_net = (float(torch.vdot(Axn.reshape(-1), y.reshape(-1)).real) / max(dn, 1e-30) * x_net).to(torch.complex64)
+    f_adj = _objective_at(solver, x_adj)
+    f_net = _objective_at(solver, x_net)
+    use = f_net < f_adj
+    solver.reset(x_net if use else x_adj)
+    return {"used_network": bool(use), "f_network": f_net, "f_adjoint": f_adj}
+
+
+def _objective_at(solver, x):
+    keep = solver.x.clone()
+    solver.x.copy_(x)
+    f = solver.objective()
+    solver.x.copy_(keep)
+    return f
+
+
+def main(argv=None):
+    """Generate training pairs, train, save:  python -m mrirecon_b200.warmstart --out w.npz"""
+    import argparse
+    import time
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--series", type=int, default=2000)
+    ap.add_argument("--per-solve", type=int, default=25)
+    ap.add_argument("--epochs", type=int, default=6)
+    ap.add_argument("--batch", type=int, default=2)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--frames", type=int, default=8)
+    a = ap.parse_args(argv)
+    t0 = time.time()
+    spec = PairSpec(frames=a.frames)
+    xa, xr = make_pairs(a.series, spec, per_solve=a.per_solve, log=lambda m: print(m, flush=True))
+    print(f"pairs: {time.time() - t0:.1f} s", flush=True)
+    net = WarmStartCNN("cuda", seed=0)
+    t1 = time.time()
+    hist = net.train(xa, xr, epochs=a.epochs, batch=a.batch, lr=a.lr, log=lambda m: print(m, flush=True))
+    print(f"training: {time.time() - t1:.1f} s, loss per epoch {hist}", flush=True)
+    net.save(a.out)
+
+
+if __name__ == "__main__":
+    main()
