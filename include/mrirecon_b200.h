@@ -62,7 +62,11 @@ int mrb_plan_destroy(mrb_plan* plan);
 
 /* Tuning knobs read by set_points / the operators (autotuner):
  * key 0 = spread tile edge (cells), key 1 = coils per spread work item,
- * key 2 = interp mode (0 acquisition order, 1 tile-sorted order). */
+ * key 2 = interp mode (0 acquisition order, 1 tile-sorted order),
+ * key 3 = samples per spread work item (heavy tiles are split),
+ * key 4 = FFT mode: 0 dense cuFFT transform with separate pad / crop kernels,
+ *         1 fused zero-pruned row / column passes (2D grids whose sides have
+ *         compiled kernels; the default wherever available). */
 int mrb_plan_set_option(mrb_plan* plan, int key, int64_t value);
 
 /* Trajectory (dev, (B, nd, K) float32 radians in [-pi, pi)): float32 grid
@@ -94,13 +98,17 @@ int mrb_nufft_adjoint(mrb_plan* plan, const void* y, void* x, int nb, mrb_stream
 /* One stage of the operators, for timing and tuning: stage 0 = pre-FFT
  * (SENSE, deapodisation, zero-pad; x -> grid), 1 = forward FFT, 2 = interp
  * (grid -> y), 3 = spread (y -> grid), 4 = inverse FFT, 5 = post-IFFT (crop,
- * deapodisation, conj-maps coil sum; grid -> x).  The grid is the plan's. */
+ * deapodisation, conj-maps coil sum; grid -> x).  The grid is the plan's.
+ * In FFT mode 1 stage 0 also runs the row transforms (x -> band buffer),
+ * 1 the column transforms (band -> grid), 4 the inverse column transforms
+ * (grid -> band) and 5 the inverse row transforms with crop and coil sum. */
 int mrb_nufft_stage(mrb_plan* plan, int stage, const void* x, void* y, int nb, mrb_stream_t stream);
 
 /* Plan facts for tests and the bench (host copies, synchronous):
  * out[0] = number of spread entries, out[1] = tiles per frame,
  * out[2] = touched grid cells summed over frames, out[3] = spread tile edge,
- * out[4] = coils per spread work item, out[5] = grid cells per frame. */
+ * out[4] = coils per spread work item, out[5] = grid cells per frame,
+ * out[6] = FFT mode (option key 4). */
 int mrb_plan_info(mrb_plan* plan, int64_t* out, int nout);
 
 /* floor of the float32 grid coordinates the plan computed, (B, nd, K) int32

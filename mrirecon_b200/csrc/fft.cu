@@ -1,0 +1,540 @@
+// Zero-pruned, fused oversampled 2D FFTs for the NUFFT (sm_100a).
+//
+// The oversampled grid of a coil-frame is zero outside the centred S0 x S1
+// image band, and the adjoint keeps only that band.  Instead of the dense
+// G0 x G1 transform (cuFFT: two read+write passes over the grid) plus separate
+// pad and crop kernels, the forward runs
+//   row pass    fused with SENSE x deapodisation x sign and the zero pad:
+//               S0 band rows of length G1 per coil-frame, image -> T (vol, S0, G1)
+//   column pass input-pruned (S0 of G0 inputs are non-zero): T -> grid
+// and the adjoint
+//   column pass output-pruned (only the S0 band rows are stored): grid -> T
+//   row pass    fused with crop, deapodisation, sign and the conj(S_c) coil sum:
+//               T -> image (nb, S0, S1)
+// HBM traffic per direction: grid once (write or read) + T twice, about 40% of
+// pad + cuFFT + crop.
+//
+// Each 1D transform is a Stockham autosort FFT over the radices 8, 4, 2, 3, 5
+// (twiddles e^{-2 pi i r k / (p R)} tabulated on the host in double precision),
+// computed in place in shared memory: a stage loads all of a thread's
+// R-point butterflies into registers, synchronises, and writes them back.  The
+// first stage loads straight from HBM and the last stage stores straight to
+// HBM, so a length-512 transform costs two shared-memory round trips.
+// Transform lengths are template parameters (the radix plan, twiddle offsets
+// and per-thread work unroll at compile time); fft2_supported() lists them.
+// Column kernels map consecutive threads to consecutive columns (128-byte
+// global segments, odd shared-memory row stride => no bank conflicts); row
+// kernels map consecutive threads along the row and pad shared memory by one
+// element per 8.  Sign conventions follow nufft.cu: (-1)^(n0+n1) on the image
+// side, the sample-side signs stay in the interp / spread weights.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "mrb_common.cuh"
+#include "fft.cuh"
+
+namespace {
+
+constexpr int ROW_NT = 256;   // threads per row-pass block
+constexpr int COL_NT = 512;   // threads per column-pass block
+
+// ---------------------------------------------------------------------------
+// compile-time radix plan: 8s first, then 4, 2, 3, 5
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int next_radix(int g) {
+  return g % 8 == 0 ? 8 : g % 4 == 0 ? 4 : g % 2 == 0 ? 2 : g % 3 == 0 ? 3 : g % 5 == 0 ? 5 : 0;
+}
+__host__ __device__ constexpr int n_stages(int G) {
+  int n = 0;
+  while (G > 1) {
+    const int r = next_radix(G);
+    if (r == 0) return -1;
+    G /= r;
+    ++n;
+  }
+  return n;
+}
+__host__ __device__ constexpr int radix_at(int G, int s) {
+  for (int i = 0; i < s; ++i) G /= next_radix(G);
+  return next_radix(G);
+}
+// product of the radices before stage s
+__host__ __device__ constexpr int span_at(int G, int s) {
+  int p = 1;
+  for (int i = 0; i < s; ++i) {
+    const int r = next_radix(G);
+    p *= r;
+    G /= r;
+  }
+  return p;
+}
+// offset of stage s in the twiddle table ([k][r-1] entries per stage)
+__host__ __device__ constexpr int tw_offset(int G, int s) {
+  int off = 0, p = 1;
+  for (int i = 0; i < s; ++i) {
+    const int r = next_radix(G);
+    off += p * (r - 1);
+    p *= r;
+    G /= r;
+  }
+  return off;
+}
+__host__ __device__ constexpr int clamp_rows(int r) { return r < 1 ? 1 : r > 16 ? 16 : r; }
+// transforms per block: about 8 (rows) / 16 (columns) complex values per thread
+__host__ __device__ constexpr int rows_per_block(int G) { return clamp_rows(8 * ROW_NT / G); }
+__host__ __device__ constexpr int cols_per_block(int G) { return clamp_rows(16 * COL_NT / G); }
+__host__ __device__ constexpr int padded_len(int G) { return G + (G >> 3) + 1; }
+
+std::vector<float2> host_twiddles(int G) {
+  std::vector<float2> t;
+  const int ns = n_stages(G);
+  for (int s = 0; s < ns; ++s) {
+    const int R = radix_at(G, s), p = span_at(G, s);
+    for (int k = 0; k < p; ++k)
+      for (int r = 1; r < R; ++r) {
+        const double a = -2.0 * M_PI * (double)r * (double)k / (double)(p * R);
+        t.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+      }
+  }
+  t.push_back(make_float2(1.f, 0.f));
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// small DFTs: X_k = sum_n u_n e^{DIR 2 pi i k n / R}, in place
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+template <int DIR>
+__device__ __forceinline__ float2 cmul_di(float2 a) {   // a * (DIR i)
+  return DIR > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+
+template <int R, int DIR>
+struct Dft;
+
+template <int DIR>
+struct Dft<2, DIR> {
+  __device__ __forceinline__ static void run(float2* u) {
+    const float2 a = u[0], b = u[1];
+    u[0] = cadd(a, b);
+    u[1] = csub(a, b);
+  }
+};
+
+template <int DIR>
+struct Dft<4, DIR> {
+  __device__ __forceinline__ static void run(float2* u) {
+    const float2 a0 = cadd(u[0], u[2]), a1 = csub(u[0], u[2]);
+    const float2 a2 = cadd(u[1], u[3]), a3 = cmul_di<DIR>(csub(u[1], u[3]));
+    u[0] = cadd(a0, a2);
+    u[2] = csub(a0, a2);
+    u[1] = cadd(a1, a3);
+    u[3] = csub(a1, a3);
+  }
+};
+
+template <int DIR>
+struct Dft<8, DIR> {
+  __device__ __forceinline__ static void run(float2* u) {
+    // radix-2 split into the 4-point DFTs of the even and odd samples
+    float2 e[4] = {u[0], u[2], u[4], u[6]};
+    float2 o[4] = {u[1], u[3], u[5], u[7]};
+    Dft<4, DIR>::run(e);
+    Dft<4, DIR>::run(o);
+    const float h = 0.707106781186547524f;
+    const float d = (float)DIR;
+    // o_k * e^{DIR i pi k / 4}
+    const float2 o1 = make_float2(h * (o[1].x - d * o[1].y), h * (o[1].y + d * o[1].x));
+    const float2 o2 = cmul_di<DIR>(o[2]);
+    const float2 o3 = make_float2(h * (-o[3].x - d * o[3].y), h * (-o[3].y + d * o[3].x));
+    u[0] = cadd(e[0], o[0]);
+    u[4] = csub(e[0], o[0]);
+    u[1] = cadd(e[1], o1);
+    u[5] = csub(e[1], o1);
+    u[2] = cadd(e[2], o2);
+    u[6] = csub(e[2], o2);
+    u[3] = cadd(e[3], o3);
+    u[7] = csub(e[3], o3);
+  }
+};
+
+template <int DIR>
+struct Dft<3, DIR> {
+  __device__ __forceinline__ static void run(float2* u) {
+    const float c1 = -0.5f, s1 = 0.866025403784438647f * (float)DIR;
+    const float2 t1 = cadd(u[1], u[2]), t2 = csub(u[1], u[2]);
+    const float2 m = make_float2(u[0].x + c1 * t1.x, u[0].y + c1 * t1.y);
+    const float2 r = make_float2(-s1 * t2.y, s1 * t2.x);
+    u[0] = cadd(u[0], t1);
+    u[1] = cadd(m, r);
+    u[2] = csub(m, r);
+  }
+};
+
+template <int DIR>
+struct Dft<5, DIR> {
+  __device__ __forceinline__ static void run(float2* u) {
+    // cos / sin of 2 pi k / 5
+    const float c1 = 0.309016994374947424f, c2 = -0.809016994374947424f;
+    const float s1 = 0.951056516295153572f * (float)DIR, s2 = 0.587785252292473129f * (float)DIR;
+    const float2 a1 = cadd(u[1], u[4]), b1 = csub(u[1], u[4]);
+    const float2 a2 = cadd(u[2], u[3]), b2 = csub(u[2], u[3]);
+    const float2 x0 = u[0];
+    const float2 m1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+    const float2 m2 = make_float2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+    const float2 n1 = make_float2(-(s1 * b1.y + s2 * b2.y), s1 * b1.x + s2 * b2.x);
+    const float2 n2 = make_float2(-(s2 * b1.y - s1 * b2.y), s2 * b1.x - s1 * b2.x);
+    u[0] = cadd(x0, cadd(a1, a2));
+    u[1] = cadd(m1, n1);
+    u[4] = csub(m1, n1);
+    u[2] = cadd(m2, n2);
+    u[3] = csub(m2, n2);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Stockham stages.  Item (q, i), i < T = G / R, of row q reads element
+// i + r T and writes element (i - k) R + k + r P, k = i mod P.  QFAST maps
+// consecutive threads to consecutive rows q (column kernels).
+// ---------------------------------------------------------------------------
+template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, class LD, class ST>
+__device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load, ST store) {
+  constexpr int R = radix_at(G, S);
+  constexpr int P = span_at(G, S);
+  constexpr int T = G / R;
+  constexpr int TOTAL = ROWS * T;
+  constexpr int NI = (TOTAL + NT - 1) / NT;
+  const float2* tws = tw + tw_offset(G, S);
+  float2 v[NI][R];
+#pragma unroll
+  for (int c = 0; c < NI; ++c) {
+    const int w = threadIdx.x + c * NT;
+    if (TOTAL % NT == 0 || w < TOTAL) {
+      const int q = QFAST ? w % ROWS : w / T;
+      const int i = QFAST ? w / ROWS : w % T;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[c][r] = load(q, i + r * T);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < NI; ++c) {
+    const int w = threadIdx.x + c * NT;
+    if (TOTAL % NT == 0 || w < TOTAL) {
+      const int q = QFAST ? w % ROWS : w / T;
+      const int i = QFAST ? w / ROWS : w % T;
+      const int k = i % P;
+      if (P > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          float2 t = __ldg(tws + k * (R - 1) + r - 1);
+          if (DIR > 0) t.y = -t.y;
+          v[c][r] = cmul(v[c][r], t);
+        }
+      }
+      Dft<R, DIR>::run(v[c]);
+      const int j = (i - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) store(q, j + r * P, v[c][r]);
+    }
+  }
+  __syncthreads();
+}
+
+// All stages of a length-G transform of ROWS rows: the first stage loads
+// through load0, the last stores through store_last, and intermediate results
+// live in buf (row q at q * LD, element e at e + e / 8 when PAD).
+template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool PAD, int LD, class LD0, class STL>
+__device__ __forceinline__ void fft_stages(float2* buf, const float2* tw, LD0 load0, STL store_last) {
+  constexpr int NS = n_stages(G);
+  if constexpr (S < NS) {
+    auto sload = [&](int q, int e) { return buf[q * LD + (PAD ? e + (e >> 3) : e)]; };
+    auto sstore = [&](int q, int e, float2 v) { buf[q * LD + (PAD ? e + (e >> 3) : e)] = v; };
+    if constexpr (S == 0 && S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST>(tw, load0, store_last);
+    else if constexpr (S == 0) fft_stage<G, S, ROWS, NT, DIR, QFAST>(tw, load0, sstore);
+    else if constexpr (S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST>(tw, sload, store_last);
+    else fft_stage<G, S, ROWS, NT, DIR, QFAST>(tw, sload, sstore);
+    fft_stages<G, S + 1, ROWS, NT, DIR, QFAST, PAD, LD>(buf, tw, load0, store_last);
+  }
+}
+
+struct Geo2 {
+  int S0, S1, G0, G1, off0, off1, C;
+  long long stot, gtot;
+};
+
+// forward row pass: T[row][:] = FFT_G1(pad(x[be][r][:] * S_c * deapod * sign)),
+// row = vol * S0 + r, ROWS consecutive rows per block
+template <int G1>
+__global__ void __launch_bounds__(ROW_NT) fwd_rows_kernel(const float2* __restrict__ x, const float2* __restrict__ maps,
+                                                          const float* __restrict__ invdeap, float2* __restrict__ Tb,
+                                                          const float2* __restrict__ tw, Geo2 g, long long nrows,
+                                                          int coil_images) {
+  constexpr int ROWS = rows_per_block(G1);
+  constexpr int LD = padded_len(G1);
+  extern __shared__ float2 sm[];
+  __shared__ long long s_xoff[ROWS], s_moff[ROWS];   // row starts in x and maps
+  __shared__ float s_d[ROWS];                        // row deapodisation x (-1)^(r + off0)
+  const long long row0 = (long long)blockIdx.x * ROWS;
+  const int nr = (int)min((long long)ROWS, nrows - row0);
+  if (threadIdx.x < nr) {
+    const long long row = row0 + threadIdx.x;
+    const long long vol = row / g.S0;
+    const int r = (int)(row - vol * g.S0);
+    const long long be = vol / g.C;
+    const int c = (int)(vol - be * g.C);
+    s_xoff[threadIdx.x] = (coil_images ? vol : be) * g.stot + (long long)r * g.S1;
+    s_moff[threadIdx.x] = (long long)c * g.stot + (long long)r * g.S1;
+    const float d = __ldg(invdeap + r);
+    s_d[threadIdx.x] = ((r + g.off0) & 1) ? -d : d;
+  }
+  __syncthreads();
+  auto load0 = [&](int q, int n1) -> float2 {
+    const int i1 = n1 - g.off1;
+    if (q >= nr || (unsigned)i1 >= (unsigned)g.S1) return make_float2(0.f, 0.f);
+    const float2 xv = x[s_xoff[q] + i1];
+    const float2 mv = coil_images ? make_float2(1.f, 0.f) : __ldg(maps + s_moff[q] + i1);
+    float s = s_d[q] * __ldg(invdeap + g.S0 + i1);
+    if (n1 & 1) s = -s;
+    return make_float2((xv.x * mv.x - xv.y * mv.y) * s, (xv.x * mv.y + xv.y * mv.x) * s);
+  };
+  auto store = [&](int q, int k1, float2 v) {
+    if (q < nr) Tb[(row0 + q) * G1 + k1] = v;
+  };
+  fft_stages<G1, 0, ROWS, ROW_NT, -1, false, true, LD>(sm, tw, load0, store);
+}
+
+// forward column pass: grid[vol][:][k1] = FFT_G0(band rows of T[vol][:][k1]),
+// COLS consecutive columns per block
+template <int G0>
+__global__ void __launch_bounds__(COL_NT) fwd_cols_kernel(const float2* __restrict__ Tb, float2* __restrict__ grid,
+                                                          const float2* __restrict__ tw, Geo2 g) {
+  constexpr int COLS = cols_per_block(G0);
+  constexpr int LD = G0 | 1;
+  extern __shared__ float2 sm[];
+  const int cblocks = (g.G1 + COLS - 1) / COLS;
+  const int vol = blockIdx.x / cblocks;
+  const int k0 = (blockIdx.x - vol * cblocks) * COLS;
+  const float2* tv = Tb + (long long)vol * g.S0 * g.G1;
+  float2* gv = grid + (long long)vol * g.gtot;
+  auto load0 = [&](int q, int n0) -> float2 {
+    const int r = n0 - g.off0;
+    if ((unsigned)r >= (unsigned)g.S0 || k0 + q >= g.G1) return make_float2(0.f, 0.f);
+    return tv[(long long)r * g.G1 + k0 + q];
+  };
+  auto store = [&](int q, int n0, float2 v) {
+    if (k0 + q < g.G1) gv[(long long)n0 * g.G1 + k0 + q] = v;
+  };
+  fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
+}
+
+// adjoint column pass: T[vol][r][k1] = IFFT_G0(grid[vol][:][k1])[r + off0]
+template <int G0>
+__global__ void __launch_bounds__(COL_NT) adj_cols_kernel(const float2* __restrict__ grid, float2* __restrict__ Tb,
+                                                          const float2* __restrict__ tw, Geo2 g) {
+  constexpr int COLS = cols_per_block(G0);
+  constexpr int LD = G0 | 1;
+  extern __shared__ float2 sm[];
+  const int cblocks = (g.G1 + COLS - 1) / COLS;
+  const int vol = blockIdx.x / cblocks;
+  const int k0 = (blockIdx.x - vol * cblocks) * COLS;
+  const float2* gv = grid + (long long)vol * g.gtot;
+  float2* tv = Tb + (long long)vol * g.S0 * g.G1;
+  auto load0 = [&](int q, int n0) -> float2 {
+    if (k0 + q >= g.G1) return make_float2(0.f, 0.f);
+    return gv[(long long)n0 * g.G1 + k0 + q];
+  };
+  auto store = [&](int q, int n0, float2 v) {
+    const int r = n0 - g.off0;
+    if ((unsigned)r < (unsigned)g.S0 && k0 + q < g.G1) tv[(long long)r * g.G1 + k0 + q] = v;
+  };
+  fft_stages<G0, 0, COLS, COL_NT, +1, true, false, LD>(sm, tw, load0, store);
+}
+
+// adjoint row pass: x[be][r][i1] = scale * deapod * sign *
+//   sum_c conj(S_c) IFFT_G1(T[(be, c)][r][:])[i1 + off1], one block per (be, r),
+// coils in passes of ROWS
+template <int G1>
+__global__ void __launch_bounds__(ROW_NT) adj_rows_kernel(const float2* __restrict__ Tb, const float2* __restrict__ maps,
+                                                          const float* __restrict__ invdeap, float2* __restrict__ x,
+                                                          const float2* __restrict__ tw, Geo2 g, float scale) {
+  constexpr int ROWS = rows_per_block(G1);
+  constexpr int LD = padded_len(G1);
+  extern __shared__ float2 sm[];
+  float2* acc = sm + ROWS * LD;   // S1 accumulators
+  const int row = blockIdx.x;
+  const int be = row / g.S0;
+  const int r = row - be * g.S0;
+  for (int i = threadIdx.x; i < g.S1; i += ROW_NT) acc[i] = make_float2(0.f, 0.f);
+  for (int c0 = 0; c0 < g.C; c0 += ROWS) {
+    const int ncl = min(ROWS, g.C - c0);
+    const float2* tb = Tb + (((long long)be * g.C + c0) * g.S0 + r) * G1;
+    const long long cstride = (long long)g.S0 * G1;
+    auto load0 = [&](int q, int n1) -> float2 {
+      if (q >= ncl) return make_float2(0.f, 0.f);
+      return tb[q * cstride + n1];
+    };
+    auto sstore = [&](int q, int e, float2 v) { sm[q * LD + e + (e >> 3)] = v; };
+    fft_stages<G1, 0, ROWS, ROW_NT, +1, false, true, LD>(sm, tw, load0, sstore);
+    for (int i = threadIdx.x; i < g.S1; i += ROW_NT) {
+      float2 s = acc[i];
+      const int e = i + g.off1;
+      const int pe = e + (e >> 3);
+      const float2* mp = maps + (long long)c0 * g.stot + (long long)r * g.S1 + i;
+      for (int q = 0; q < ncl; ++q) {
+        const float2 v = sm[q * LD + pe];
+        const float2 m = __ldg(mp + (long long)q * g.stot);
+        s.x += m.x * v.x + m.y * v.y;
+        s.y += m.x * v.y - m.y * v.x;
+      }
+      acc[i] = s;
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < g.S1; i += ROW_NT) {
+    float d = scale * __ldg(invdeap + r) * __ldg(invdeap + g.S0 + i);
+    if ((r + g.off0 + i + g.off1) & 1) d = -d;
+    const float2 s = acc[i];
+    x[((long long)be * g.S0 + r) * g.S1 + i] = make_float2(s.x * d, s.y * d);
+  }
+}
+
+Geo2 make_geo2(int S0, int S1, int G0, int G1, int C) {
+  return Geo2{S0, S1, G0, G1, G0 / 2 - S0 / 2, G1 / 2 - S1 / 2, C, (long long)S0 * S1, (long long)G0 * G1};
+}
+
+int set_smem(const void* fn, size_t bytes) {
+  MRB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return 0;
+}
+
+// the transform lengths with compiled kernels
+#define MRB_FFT_LENGTHS(X) \
+  X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256) X(320) X(384) X(512) X(640) X(768) X(1024)
+
+bool length_supported(int G) {
+  switch (G) {
+#define MRB_CASE(n) case n:
+    MRB_FFT_LENGTHS(MRB_CASE)
+#undef MRB_CASE
+    return true;
+    default:
+      return false;
+  }
+}
+
+template <int G1>
+int launch_fwd_rows(const void* x, const float2* maps, const float* invdeap, float2* Tb, const float2* tw,
+                    const Geo2& g, int nb, int coil_images, cudaStream_t st) {
+  constexpr int ROWS = rows_per_block(G1);
+  const size_t smem = (size_t)ROWS * padded_len(G1) * sizeof(float2);
+  int rc;
+  if ((rc = set_smem((const void*)fwd_rows_kernel<G1>, smem))) return rc;
+  const long long nrows = (long long)nb * g.C * g.S0;
+  const long long blocks = (nrows + ROWS - 1) / ROWS;
+  MRB_REQUIRE(blocks < (1LL << 31), "too many rows");
+  fwd_rows_kernel<G1><<<(unsigned)blocks, ROW_NT, smem, st>>>((const float2*)x, maps, invdeap, Tb, tw, g, nrows,
+                                                              coil_images);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+template <int G0>
+int launch_cols(bool forward, const float2* in, float2* out, const float2* tw, const Geo2& g, int nb, cudaStream_t st) {
+  constexpr int COLS = cols_per_block(G0);
+  const size_t smem = (size_t)COLS * (G0 | 1) * sizeof(float2);
+  const long long blocks = (long long)nb * g.C * ((g.G1 + COLS - 1) / COLS);
+  MRB_REQUIRE(blocks < (1LL << 31), "too many columns");
+  int rc;
+  if (forward) {
+    if ((rc = set_smem((const void*)fwd_cols_kernel<G0>, smem))) return rc;
+    fwd_cols_kernel<G0><<<(unsigned)blocks, COL_NT, smem, st>>>(in, out, tw, g);
+  } else {
+    if ((rc = set_smem((const void*)adj_cols_kernel<G0>, smem))) return rc;
+    adj_cols_kernel<G0><<<(unsigned)blocks, COL_NT, smem, st>>>(in, out, tw, g);
+  }
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+template <int G1>
+int launch_adj_rows(const float2* Tb, const float2* maps, const float* invdeap, void* x, const float2* tw,
+                    const Geo2& g, int nb, float scale, cudaStream_t st) {
+  constexpr int ROWS = rows_per_block(G1);
+  const size_t smem = ((size_t)ROWS * padded_len(G1) + g.S1) * sizeof(float2);
+  int rc;
+  if ((rc = set_smem((const void*)adj_rows_kernel<G1>, smem))) return rc;
+  const long long blocks = (long long)nb * g.S0;
+  MRB_REQUIRE(blocks < (1LL << 31), "too many rows");
+  adj_rows_kernel<G1><<<(unsigned)blocks, ROW_NT, smem, st>>>(Tb, maps, invdeap, (float2*)x, tw, g, scale);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+}  // namespace
+
+namespace mrb {
+
+bool fft2_supported(int S0, int S1, int G0, int G1) {
+  return length_supported(G0) && length_supported(G1) && S0 <= G0 && S1 <= G1;
+}
+
+size_t fft2_tmp_bytes(int S0, int G1, int C, int nb) { return (size_t)nb * C * S0 * G1 * sizeof(float2); }
+
+int fft2_twiddles(DevBuf& tw, int G, const float2** out) {
+  std::vector<float2> t = host_twiddles(G);
+  int rc = tw.ensure(t.size() * sizeof(float2));
+  if (rc) return rc;
+  MRB_CUDA_TRY(cudaMemcpy(tw.p, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  *out = tw.as<float2>();
+  return 0;
+}
+
+int fft2_forward_rows(const void* x, const float2* maps, const float* invdeap, float2* Tb, const float2* tw1, int S0,
+                      int S1, int G0, int G1, int C, int nb, int coil_images, cudaStream_t st) {
+  const Geo2 g = make_geo2(S0, S1, G0, G1, C);
+  switch (G1) {
+#define MRB_CASE(n) \
+  case n: return launch_fwd_rows<n>(x, maps, invdeap, Tb, tw1, g, nb, coil_images, st);
+    MRB_FFT_LENGTHS(MRB_CASE)
+#undef MRB_CASE
+    default:
+      return fail(MRB_EINVAL, "no fused FFT for length %d", G1);
+  }
+}
+
+int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, int S0, int S1, int G0, int G1, int C,
+                 int nb, cudaStream_t st) {
+  const Geo2 g = make_geo2(S0, S1, G0, G1, C);
+  switch (G0) {
+#define MRB_CASE(n) \
+  case n: return launch_cols<n>(forward != 0, in, out, tw0, g, nb, st);
+    MRB_FFT_LENGTHS(MRB_CASE)
+#undef MRB_CASE
+    default:
+      return fail(MRB_EINVAL, "no fused FFT for length %d", G0);
+  }
+}
+
+int fft2_adjoint_rows(const float2* Tb, const float2* maps, const float* invdeap, void* x, const float2* tw1, int S0,
+                      int S1, int G0, int G1, int C, int nb, float scale, cudaStream_t st) {
+  const Geo2 g = make_geo2(S0, S1, G0, G1, C);
+  switch (G1) {
+#define MRB_CASE(n) \
+  case n: return launch_adj_rows<n>(Tb, maps, invdeap, x, tw1, g, nb, scale, st);
+    MRB_FFT_LENGTHS(MRB_CASE)
+#undef MRB_CASE
+    default:
+      return fail(MRB_EINVAL, "no fused FFT for length %d", G1);
+  }
+}
+
+}  // namespace mrb

@@ -1,0 +1,29 @@
+// Fused, zero-pruned oversampled 2D FFT passes (fft.cu) used by the NUFFT plan.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "mrb_common.cuh"
+
+namespace mrb {
+
+// true when compiled kernels cover this 2D geometry (G0, G1 in the length list)
+bool fft2_supported(int S0, int S1, int G0, int G1);
+// bytes of the band buffer T (nb, C, S0, G1) complex
+size_t fft2_tmp_bytes(int S0, int G1, int C, int nb);
+// device twiddle table of a length-G transform
+int fft2_twiddles(DevBuf& tw, int G, const float2** out);
+
+// image (nb, S0, S1) [or coil images (nb, C, S0, S1)] -> T (nb, C, S0, G1)
+int fft2_forward_rows(const void* x, const float2* maps, const float* invdeap, float2* Tb, const float2* tw1, int S0,
+                      int S1, int G0, int G1, int C, int nb, int coil_images, cudaStream_t st);
+// forward != 0: T -> grid (nb, C, G0, G1); else grid -> T
+int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, int S0, int S1, int G0, int G1, int C,
+                 int nb, cudaStream_t st);
+// T -> image (nb, S0, S1), coil-combined with conj(maps), scaled
+int fft2_adjoint_rows(const float2* Tb, const float2* maps, const float* invdeap, void* x, const float2* tw1, int S0,
+                      int S1, int G0, int G1, int C, int nb, float scale, cudaStream_t st);
+
+}  // namespace mrb

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "mrb_common.cuh"
+#include "fft.cuh"
 
 using mrb::DevBuf;
 using mrb::KBPoly;
@@ -71,6 +72,11 @@ struct mrb_plan {
   DevBuf grid;        // (nb, C, *G) float2
   cufftHandle fft = 0;
   int fft_batch = 0;
+  int fft_mode = 0;   // 0 cuFFT dense transform + pad/crop kernels, 1 fused zero-pruned passes (fft.cu)
+  DevBuf band;        // fused mode: (nb, C, S0, G1) float2 row-transformed band
+  DevBuf tw0, tw1;    // fused mode: twiddle tables of G0 and G1
+  const float2* tw0p = nullptr;
+  const float2* tw1p = nullptr;
   DevBuf tmp;         // scratch for set_points
   size_t spread_smem_set = 0;   // dynamic smem opt-in already granted
 
@@ -957,6 +963,7 @@ extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int 
   int rc = p->invdeap.ensure(dap.size() * sizeof(float));
   if (!rc && cudaMemcpy(p->invdeap.p, dap.data(), dap.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
     rc = mrb::fail(MRB_ECUDA, "copying deapodisation failed");
+  if (!rc && nd == 2 && mrb::fft2_supported(p->S[0], p->S[1], p->G[0], p->G[1])) rc = mrb_plan_set_option(p, 4, 1);
   if (rc) {
     delete p;
     return rc;
@@ -969,7 +976,7 @@ extern "C" int mrb_plan_destroy(mrb_plan* p) {
   if (!p) return 0;
   if (p->fft) cufftDestroy(p->fft);
   for (DevBuf* b : {&p->gx, &p->entries, &p->tile_start, &p->items, &p->multi, &p->partials, &p->empty_keys, &p->maps, &p->invdeap, &p->wfwd,
-                    &p->wadj, &p->grid, &p->tmp})
+                    &p->wadj, &p->grid, &p->tmp, &p->band, &p->tw0, &p->tw1})
     b->release();
   delete p;
   return 0;
@@ -996,6 +1003,19 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
       MRB_REQUIRE(value >= 16 && value <= (1 << 20), "chunk must be 16 .. 2^20 samples");
       p->chunk = (int)value;
       p->have_points = false;   // the item table depends on it
+      return 0;
+    case 4:
+      MRB_REQUIRE(value == 0 || value == 1, "fft mode must be 0 (cuFFT) or 1 (fused)");
+      if (value == 1) {
+        MRB_REQUIRE(p->nd == 2 && mrb::fft2_supported(p->S[0], p->S[1], p->G[0], p->G[1]),
+                    "no fused FFT kernels for this grid (%d x %d)", p->G[0], p->G[1]);
+        if (!p->tw0p) {
+          int rc;
+          if ((rc = mrb::fft2_twiddles(p->tw0, p->G[0], &p->tw0p))) return rc;
+          if ((rc = mrb::fft2_twiddles(p->tw1, p->G[1], &p->tw1p))) return rc;
+        }
+      }
+      p->fft_mode = (int)value;
       return 0;
     default:
       return mrb::fail(MRB_EINVAL, "unknown option %d", key);
@@ -1188,12 +1208,29 @@ static int ensure_grid(mrb_plan* p, int nb) {
   size_t bytes = (size_t)nb * p->C * p->gtot() * sizeof(float2);
   int rc = p->grid.ensure(bytes);
   if (rc) return rc;
+  if (p->fft_mode == 1) return p->band.ensure(mrb::fft2_tmp_bytes(p->S[0], p->G[1], p->C, nb));
   return ensure_fft(p, nb);
 }
 
 // one stage of the forward/adjoint pipeline; x/y are the user image / samples
 static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cudaStream_t st, int coil_images) {
   Geo g = make_geo(p);
+  if (p->fft_mode == 1) {
+    // fused passes: 0 = SENSE/deapod/pad + row FFTs, 1 = column FFTs,
+    // 4 = inverse column FFTs, 5 = inverse row FFTs + crop/deapod/coil sum
+    if (stage == 0)
+      return mrb::fft2_forward_rows(x, p->maps.as<float2>(), p->invdeap.as<float>(), p->band.as<float2>(), p->tw1p,
+                                    p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb, coil_images, st);
+    if (stage == 1)
+      return mrb::fft2_columns(1, p->band.as<float2>(), p->grid.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
+                               p->G[1], p->C, nb, st);
+    if (stage == 4)
+      return mrb::fft2_columns(0, p->grid.as<float2>(), p->band.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
+                               p->G[1], p->C, nb, st);
+    if (stage == 5)
+      return mrb::fft2_adjoint_rows(p->band.as<float2>(), p->maps.as<float2>(), p->invdeap.as<float>(), (void*)x,
+                                    p->tw1p, p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb, p->scale, st);
+  }
   if (stage == 0) {
     const int Gl = p->G[p->nd - 1];
     const long long nvol = (long long)nb * p->C;
@@ -1387,8 +1424,8 @@ extern "C" int mrb_nufft_stage(mrb_plan* p, int stage, const void* x, void* y, i
 
 extern "C" int mrb_plan_info(mrb_plan* p, int64_t* out, int nout) {
   MRB_REQUIRE(p != nullptr && out != nullptr, "null plan or output");
-  int64_t v[6] = {p->n_entries, p->ntiles, p->touched, p->tile, p->coils_per_item, p->gtot()};
-  for (int i = 0; i < nout && i < 6; ++i) out[i] = v[i];
+  int64_t v[7] = {p->n_entries, p->ntiles, p->touched, p->tile, p->coils_per_item, p->gtot(), p->fft_mode};
+  for (int i = 0; i < nout && i < 7; ++i) out[i] = v[i];
   return 0;
 }
 

@@ -31,7 +31,8 @@ from .layout import (AxisSpec, plan_image_layout, plan_kspace_layout, plan_image
                      plan_kspace_layout_from_sizes, user_image_shape, user_kspace_shape)
 from .roles import Roles
 
-OPT_TILE, OPT_COILS_PER_ITEM, OPT_INTERP_MODE, OPT_CHUNK = 0, 1, 2, 3
+OPT_TILE, OPT_COILS_PER_ITEM, OPT_INTERP_MODE, OPT_CHUNK, OPT_FFT_MODE = 0, 1, 2, 3, 4
+FFT_CUFFT, FFT_FUSED = 0, 1
 _DCF_MODES = {"none": 0, "balanced": 1, "standard": 2}
 
 
@@ -109,9 +110,9 @@ class KBPlan:
                                             _lib.stream_ptr(self.device)), "nufft_stage")
 
     def info(self) -> dict:
-        out = (ct.c_int64 * 6)()
-        _lib.check(self.lib.mrb_plan_info(self.h, out, 6), "plan_info")
-        keys = ("entries", "tiles_per_frame", "touched_cells", "tile", "coils_per_item", "grid_cells")
+        out = (ct.c_int64 * 7)()
+        _lib.check(self.lib.mrb_plan_info(self.h, out, 7), "plan_info")
+        keys = ("entries", "tiles_per_frame", "touched_cells", "tile", "coils_per_item", "grid_cells", "fft_mode")
         return {k: int(v) for k, v in zip(keys, out)}
 
     def cell_base(self) -> torch.Tensor:
@@ -172,6 +173,7 @@ class B200NUFFTAdapter:
     tile: Optional[int] = None
     coils_per_item: Optional[int] = None
     chunk: Optional[int] = None
+    fft_mode: Optional[int] = None
     autotune: bool = False
     tuned: Optional[dict] = None
 
@@ -236,6 +238,8 @@ class B200NUFFTAdapter:
                 plan.set_option(OPT_COILS_PER_ITEM, self.coils_per_item)
             if self.chunk is not None:
                 plan.set_option(OPT_CHUNK, self.chunk)
+            if self.fft_mode is not None:
+                plan.set_option(OPT_FFT_MODE, self.fft_mode)
             plan.set_points(self._traj_BndK)
             plan.set_dcf(self._dcf_BK, self.dcf_mode, self.apply_dcf_in_fwd, self.apply_dcf_in_adj)
             plan.set_maps(self._maps)

@@ -247,3 +247,45 @@ def test_autotuner_picks_a_timed_candidate(cuda, tmp_path, monkeypatch):
     assert (info["tile"], info["coils_per_item"]) == (best["tile"], best["cpi"])
     ad2 = _check_pair(maps, traj, autotune=True)
     assert ad2.tuned.get("cached") and ad2.tuned["tile"] == best["tile"]
+
+
+@pytest.mark.parametrize("S,C,nb", [((128, 128), 12, 3), ((96, 80), 4, 2), ((160, 192), 3, 2), ((20, 20), 5, 2)])
+def test_fused_fft_matches_cufft(cuda, S, C, nb):
+    """The fused zero-pruned row/column FFT passes (default for 2D grids with
+    compiled lengths, radices 8/4/2/3/5) agree with the dense cuFFT path."""
+    maps = _rand_c((C,) + S, 41, torch.complex64)
+    traj = phantoms.random_traj(nb, 2, 900, seed=42)
+    fused = _adapter(maps, traj)
+    dense = _adapter(maps, traj, fft_mode=0)
+    assert fused.plan.info()["fft_mode"] == 1 and dense.plan.info()["fft_mode"] == 0
+    x = _rand_c((nb, 1) + S, 43, torch.complex64).to(cuda)
+    y = _rand_c((nb, C, 900), 44, torch.complex64).to(cuda)
+    assert rel(fused.A(x), dense.A(x)) < 2e-6
+    assert rel(fused.AH(y), dense.AH(y)) < 2e-6
+    xc = _rand_c((nb, C) + S, 45, torch.complex64).to(cuda)
+    yf = torch.empty_like(y)
+    yd = torch.empty_like(y)
+    _lib_forward_coils(fused, xc, yf, nb)
+    _lib_forward_coils(dense, xc, yd, nb)
+    assert rel(yf, yd) < 2e-6
+
+
+def _lib_forward_coils(ad, xc, y, nb):
+    from mrirecon_b200 import _lib
+    _lib.check(_lib.load().mrb_nufft_forward_coils(ad.plan.h, _lib.ptr(xc), _lib.ptr(y), nb,
+                                                   _lib.stream_ptr(xc.device)), "forward_coils")
+
+
+def test_fft_mode_selection(cuda):
+    """Fused FFT by default where kernels exist; cuFFT for other 2D sizes and 3D;
+    asking for the fused mode where it does not exist is an error."""
+    traj2 = phantoms.random_traj(1, 2, 100, seed=1)
+    assert _adapter(_rand_c((2, 32, 40), 1, torch.complex64), traj2).plan.info()["fft_mode"] == 1
+    assert _adapter(_rand_c((2, 31, 33), 1, torch.complex64), traj2).plan.info()["fft_mode"] == 0
+    traj3 = phantoms.random_traj(1, 3, 100, seed=1)
+    ad3 = _adapter(_rand_c((2, 8, 8, 8), 1, torch.complex64), traj3)
+    assert ad3.plan.info()["fft_mode"] == 0
+    with pytest.raises(RuntimeError):
+        _adapter(_rand_c((2, 8, 8, 8), 1, torch.complex64), traj3, fft_mode=1)
+    with pytest.raises(RuntimeError):
+        _adapter(_rand_c((2, 31, 33), 1, torch.complex64), traj2, fft_mode=1)
