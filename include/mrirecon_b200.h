@@ -111,6 +111,27 @@ int mrb_nufft_stage(mrb_plan* plan, int stage, const void* x, void* y, int nb, m
  * out[6] = FFT mode (option key 4). */
 int mrb_plan_info(mrb_plan* plan, int64_t* out, int nout);
 
+/* Toeplitz normal operator (no counterpart in the reference; its item
+ * "Toeplitz A^H A embedding").  With t_b(D) = sum_k w_k exp(i w_k . D) the
+ * sampling point-spread function of frame b (w the product of the forward and
+ * adjoint DCF weights), A^H A x = s^2 sum_n x_n t_b(r_m - r_n) is a circular
+ * convolution on the 2x grid.  psf (dev, (B, G0, G1) float32) is its real
+ * transfer function FFT(circular t_b) * s^2 / (G0 G1), rolled by (G0/2, G1/2);
+ * copied into the plan.  Needs FFT mode 1. */
+int mrb_plan_set_toeplitz(mrb_plan* plan, const float* psf, mrb_stream_t stream);
+/* out (dev, (nb, 1, *S)) = A^H A x through the Toeplitz transfer function:
+ * SENSE + row FFTs, column FFT x P x inverse column FFT in shared memory,
+ * inverse row FFTs + conj(S_c) coil sum.  No gridding. */
+int mrb_nufft_normal(mrb_plan* plan, const void* x, void* out, int nb, mrb_stream_t stream);
+
+/* Device flag (dev, one double, or NULL to clear) read by every operator
+ * kernel launched from now on: when it is non-zero at run time the kernel
+ * returns without work.  A solver points it at its own "done" flag so that
+ * graph replays past convergence (and finished instances of a batch) cost no
+ * gridding or FFT work; the dense cuFFT transform (FFT mode 0) still runs.
+ * No counterpart in the reference (its loop stops on the host). */
+int mrb_plan_set_skip_flag(mrb_plan* plan, const double* flag);
+
 /* floor of the float32 grid coordinates the plan computed, (B, nd, K) int32
  * (dev out).  Bit-exact key of the production binning. */
 int mrb_plan_cell_base(mrb_plan* plan, int32_t* out, mrb_stream_t stream);
@@ -222,6 +243,60 @@ int mrb_ncg_update(int64_t n, void* x, void* d, const void* g, void* gr, const v
                    const float* diag, int64_t ndiag, double* slots, void* ws, mrb_stream_t stream);
 int mrb_ncg_steepest(int64_t n, void* d, const void* g, void* g_prev, const float* diag, int64_t ndiag,
                      double* out, void* ws, mrb_stream_t stream);
+/* Residual energy after the accepted step when the k-space residual is not
+ * kept (Toeplitz schedule): slot err += 2 t erd + t^2 edd (no reference
+ * counterpart; the reference recomputes A x every iteration). */
+int mrb_ncg_err_step(double* slots, mrb_stream_t stream);
+/* Optional restart after mrb_ncg_update (no counterpart in the reference,
+ * whose loop stops when the new direction is not a descent direction): if
+ * Re<g, d> >= 0, d = -g/D, the slope slot becomes -<g, g/D> and slot 19
+ * counts the restarts.  Returns at once on the device when no restart is due. */
+int mrb_ncg_restart(int64_t n, void* d, const void* g, const float* diag, int64_t ndiag, double* slots,
+                    mrb_stream_t stream);
+
+/* ------------------------------------------------------------------------
+ * Learned warm start (no counterpart in the reference).  Activations are
+ * channels-last BF16 volumes (Nb, D, H, W, channels) with a channel stride
+ * and a channel offset (concatenation is a channel offset); `vol` is a DEVICE
+ * int[4] {Nb, D, H, W}.  Weights are BF16 [27][cin][coutp], tap = kd*9+kh*3+kw
+ * over (t, y, x); coutp and channel counts are multiples of 32.
+ * ---------------------------------------------------------------------- */
+/* 3x3x3 zero-padded convolution on tensor cores (BF16 in, FP32 accumulate),
+ * + bias, optional ReLU; writes BF16 (yb) and/or FP32 (yf, accumulated when
+ * yf_acc).  The data gradient is this call with mrb_cnn_flip_weights. */
+int mrb_cnn_conv3d_fwd(const void* x, int cx, int ci_off, int cin, const void* w, int coutp, int cout,
+                       const float* bias, int relu, void* yb, int cyb, int yb_off, float* yf, int cyf,
+                       int yf_off, int yf_acc, const int* vol, mrb_stream_t stream);
+/* Weight (and bias) gradient: dw[27][cin][coutp] = sum over voxels of
+ * x(shifted) * gz, split-K partials in `part` summed in a fixed order. */
+int mrb_cnn_conv3d_wgrad(const void* x, int cx, int ci_off, int cin, const void* gz, int cg, int cg_off,
+                         int coutp, float* dw, float* dbias, float* part, int64_t part_floats,
+                         const int* vol, mrb_stream_t stream);
+/* Spatially flipped, transposed weights [27][coutp][cinp] for the data gradient. */
+int mrb_cnn_flip_weights(const void* w, int cin, int coutp, void* wd, int cinp, mrb_stream_t stream);
+/* gz = g * (act > 0) over nch channels (BF16 out, padded to nchp). */
+int mrb_cnn_relu_bwd(const float* g, int cgs, int g_off, const void* act, int cas, int a_off, int nch,
+                     int64_t voxels, void* gz, int czs, int z_off, int nchp, mrb_stream_t stream);
+/* 2x2 mean pooling over (y, x) (dir 0) or its adjoint (dir 1). */
+int mrb_cnn_pool2(int dir, const void* in, int cin_s, int in_off, int nch, const int* fine_vol, void* out,
+                  int cout_s, int out_off, mrb_stream_t stream);
+/* Nearest 2x upsampling over (y, x) (dir 0) or its adjoint (dir 1). */
+int mrb_cnn_up2(int dir, const void* in, int cin_s, int in_off, int nch, const int* coarse_vol, void* out,
+                int cout_s, int out_off, mrb_stream_t stream);
+/* complex image series z (Nb, D, H, W) * scale[Nb] -> 2 real channels of x. */
+int mrb_cnn_pack(const void* z, const float* scale, const int* vol, void* x, int cx, mrb_stream_t stream);
+/* zout = zin + net[channels 0, 1] / scale (residual output). */
+int mrb_cnn_unpack(const void* zin, const float* net, int cy, const float* scale, const int* vol, void* zout,
+                   mrb_stream_t stream);
+/* Mean squared error of the residual output against target, FP64 loss, FP32
+ * gradient with respect to the network output. */
+int mrb_cnn_mse(const void* zin, const void* target, const float* net, int cy, const float* scale,
+                const int* vol, float* grad, double* loss, double* part, int64_t part_len,
+                mrb_stream_t stream);
+/* Adam on FP32 master weights; refreshes the BF16 copy wb when non-null. */
+int mrb_cnn_adam(float* w, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2,
+                 float eps, int step, void* wb, mrb_stream_t stream);
+int mrb_cnn_to_bf16(const float* a, int64_t n, void* b, mrb_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -55,6 +55,9 @@ _SIGS = {
     "mrb_nufft_forward_coils": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p]),
     "mrb_nufft_adjoint": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p]),
     "mrb_plan_info": (ct.c_int, [ct.c_void_p, c_int64_p, ct.c_int]),
+    "mrb_plan_set_skip_flag": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
+    "mrb_plan_set_toeplitz": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mrb_nufft_normal": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p]),
     "mrb_plan_cell_base": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mrb_grid_indices": (ct.c_int, [ct.c_void_p, ct.c_int, c_int_p, ct.c_int64, ct.c_int, ct.c_int, ct.c_void_p,
                                     ct.c_void_p]),
@@ -79,6 +82,9 @@ _SIGS = {
                                   ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "mrb_ncg_steepest": (ct.c_int, [ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64,
                                     ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mrb_ncg_err_step": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
+    "mrb_ncg_restart": (ct.c_int, [ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_void_p,
+                                   ct.c_void_p]),
 }
 
 

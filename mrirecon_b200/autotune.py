@@ -4,7 +4,7 @@ For a prepared plan it times the adjoint spread stage (the kernel whose speed
 depends on the tiling; interp, pre/post and the FFT do not) for a list of
 (tile edge, coils per work item, samples per chunk) candidates on the plan's
 own trajectory, keeps the fastest and caches the choice per size class
-(nd, image shape, coils, frames, samples per frame) and GPU name in a JSON
+(nd, image shape, frames, coils and samples per frame bucketed) and GPU name in a JSON
 file (``$MRB_TUNE_CACHE`` or ``~/.cache/mrirecon_b200/spread_tune.json``).
 All candidates compute the same grid (deterministically, up to the order in
 which split tiles sum their partial tiles).
@@ -12,6 +12,7 @@ which split tiles sum their partial tiles).
 from __future__ import annotations
 
 import json
+import math
 import os
 from typing import Dict, Iterable, Optional, Sequence, Tuple
 
@@ -31,8 +32,12 @@ def _cache_path() -> str:
 
 
 def size_class(plan) -> str:
+    """Tuning key: GPU, image shape, frames, coils rounded up to a multiple of 4
+    and samples per frame in half-octave buckets (plans in one class share a choice)."""
     name = torch.cuda.get_device_name(plan.device)
-    return f"{name}|nd{plan.nd}|S{'x'.join(map(str, plan.S))}|C{plan.C}|B{plan.B}|K{plan.K}"
+    cq = -(-int(plan.C) // 4) * 4
+    kq = round(2.0 * math.log2(max(1, int(plan.K)))) / 2.0
+    return f"{name}|nd{plan.nd}|S{'x'.join(map(str, plan.S))}|C{cq}|B{plan.B}|K2^{kq:g}"
 
 
 def _load() -> Dict[str, dict]:

@@ -269,6 +269,7 @@ __device__ __forceinline__ void fft_stages(float2* buf, const float2* tw, LD0 lo
 struct Geo2 {
   int S0, S1, G0, G1, off0, off1, C;
   long long stot, gtot;
+  const double* skip;   // when non-null and non-zero the kernels return at once
 };
 
 // forward row pass: T[row][:] = FFT_G1(pad(x[be][r][:] * S_c * deapod * sign)),
@@ -281,6 +282,7 @@ __global__ void __launch_bounds__(ROW_NT) fwd_rows_kernel(const float2* __restri
   constexpr int ROWS = rows_per_block(G1);
   constexpr int LD = padded_len(G1);
   extern __shared__ float2 sm[];
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   __shared__ long long s_xoff[ROWS], s_moff[ROWS];   // row starts in x and maps
   __shared__ float s_d[ROWS];                        // row deapodisation x (-1)^(r + off0)
   const long long row0 = (long long)blockIdx.x * ROWS;
@@ -320,6 +322,7 @@ __global__ void __launch_bounds__(COL_NT) fwd_cols_kernel(const float2* __restri
   constexpr int COLS = cols_per_block(G0);
   constexpr int LD = G0 | 1;
   extern __shared__ float2 sm[];
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   const int cblocks = (g.G1 + COLS - 1) / COLS;
   const int vol = blockIdx.x / cblocks;
   const int k0 = (blockIdx.x - vol * cblocks) * COLS;
@@ -343,6 +346,7 @@ __global__ void __launch_bounds__(COL_NT) adj_cols_kernel(const float2* __restri
   constexpr int COLS = cols_per_block(G0);
   constexpr int LD = G0 | 1;
   extern __shared__ float2 sm[];
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   const int cblocks = (g.G1 + COLS - 1) / COLS;
   const int vol = blockIdx.x / cblocks;
   const int k0 = (blockIdx.x - vol * cblocks) * COLS;
@@ -359,6 +363,49 @@ __global__ void __launch_bounds__(COL_NT) adj_cols_kernel(const float2* __restri
   fft_stages<G0, 0, COLS, COL_NT, +1, true, false, LD>(sm, tw, load0, store);
 }
 
+// Toeplitz column pass (normal operator A^H A by circular convolution on the
+// 2x grid): for each column of the band, T <- IFFT_G0(P[frame] * FFT_G0(T)),
+// band rows in, band rows out, the column never leaves shared memory.
+// P (B, G0, G1) float is the real transfer function, already rolled by G/2 in
+// both dims (the row passes' (-1)^n signs) and scaled.
+template <int G0>
+__global__ void __launch_bounds__(COL_NT) toeplitz_cols_kernel(float2* __restrict__ Tb,
+                                                               const float* __restrict__ P,
+                                                               const float2* __restrict__ tw, Geo2 g, int nb,
+                                                               int B) {
+  constexpr int COLS = cols_per_block(G0);
+  constexpr int LD = G0 | 1;
+  extern __shared__ float2 sm[];
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+  const int cblocks = (g.G1 + COLS - 1) / COLS;
+  const int vol = blockIdx.x / cblocks;
+  const int k0 = (blockIdx.x - vol * cblocks) * COLS;
+  const int be = vol / g.C;
+  const int b = (B == 1) ? 0 : be / (nb / B);
+  float2* tv = Tb + (long long)vol * g.S0 * g.G1;
+  const float* pb = P + (long long)b * g.gtot;
+  auto load0 = [&](int q, int n0) -> float2 {
+    const int r = n0 - g.off0;
+    if ((unsigned)r >= (unsigned)g.S0 || k0 + q >= g.G1) return make_float2(0.f, 0.f);
+    return tv[(long long)r * g.G1 + k0 + q];
+  };
+  auto sload = [&](int q, int e) { return sm[q * LD + e]; };
+  auto sstore = [&](int q, int e, float2 v) { sm[q * LD + e] = v; };
+  fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, sstore);
+  for (int e = threadIdx.x; e < COLS * G0; e += COL_NT) {
+    const int q = e % COLS, kr = e / COLS;
+    const float p = k0 + q < g.G1 ? __ldg(pb + (long long)kr * g.G1 + k0 + q) : 0.f;
+    float2 v = sm[q * LD + kr];
+    sm[q * LD + kr] = make_float2(v.x * p, v.y * p);
+  }
+  __syncthreads();
+  auto store = [&](int q, int n0, float2 v) {
+    const int r = n0 - g.off0;
+    if ((unsigned)r < (unsigned)g.S0 && k0 + q < g.G1) tv[(long long)r * g.G1 + k0 + q] = v;
+  };
+  fft_stages<G0, 0, COLS, COL_NT, +1, true, false, LD>(sm, tw, sload, store);
+}
+
 // adjoint row pass: x[be][r][i1] = scale * deapod * sign *
 //   sum_c conj(S_c) IFFT_G1(T[(be, c)][r][:])[i1 + off1], one block per (be, r),
 // coils in passes of ROWS
@@ -369,6 +416,7 @@ __global__ void __launch_bounds__(ROW_NT) adj_rows_kernel(const float2* __restri
   constexpr int ROWS = rows_per_block(G1);
   constexpr int LD = padded_len(G1);
   extern __shared__ float2 sm[];
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   float2* acc = sm + ROWS * LD;   // S1 accumulators
   const int row = blockIdx.x;
   const int be = row / g.S0;
@@ -407,8 +455,8 @@ __global__ void __launch_bounds__(ROW_NT) adj_rows_kernel(const float2* __restri
   }
 }
 
-Geo2 make_geo2(int S0, int S1, int G0, int G1, int C) {
-  return Geo2{S0, S1, G0, G1, G0 / 2 - S0 / 2, G1 / 2 - S1 / 2, C, (long long)S0 * S1, (long long)G0 * G1};
+Geo2 make_geo2(int S0, int S1, int G0, int G1, int C, const double* skip) {
+  return Geo2{S0, S1, G0, G1, G0 / 2 - S0 / 2, G1 / 2 - S1 / 2, C, (long long)S0 * S1, (long long)G0 * G1, skip};
 }
 
 int set_smem(const void* fn, size_t bytes) {
@@ -465,6 +513,20 @@ int launch_cols(bool forward, const float2* in, float2* out, const float2* tw, c
   return 0;
 }
 
+template <int G0>
+int launch_toeplitz_cols(float2* Tb, const float* P, const float2* tw, const Geo2& g, int nb, int B,
+                         cudaStream_t st) {
+  constexpr int COLS = cols_per_block(G0);
+  const size_t smem = (size_t)COLS * (G0 | 1) * sizeof(float2);
+  const long long blocks = (long long)nb * g.C * ((g.G1 + COLS - 1) / COLS);
+  MRB_REQUIRE(blocks < (1LL << 31), "too many columns");
+  int rc;
+  if ((rc = set_smem((const void*)toeplitz_cols_kernel<G0>, smem))) return rc;
+  toeplitz_cols_kernel<G0><<<(unsigned)blocks, COL_NT, smem, st>>>(Tb, P, tw, g, nb, B);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
 template <int G1>
 int launch_adj_rows(const float2* Tb, const float2* maps, const float* invdeap, void* x, const float2* tw,
                     const Geo2& g, int nb, float scale, cudaStream_t st) {
@@ -499,8 +561,9 @@ int fft2_twiddles(DevBuf& tw, int G, const float2** out) {
 }
 
 int fft2_forward_rows(const void* x, const float2* maps, const float* invdeap, float2* Tb, const float2* tw1, int S0,
-                      int S1, int G0, int G1, int C, int nb, int coil_images, cudaStream_t st) {
-  const Geo2 g = make_geo2(S0, S1, G0, G1, C);
+                      int S1, int G0, int G1, int C, int nb, int coil_images, const double* skip,
+                      cudaStream_t st) {
+  const Geo2 g = make_geo2(S0, S1, G0, G1, C, skip);
   switch (G1) {
 #define MRB_CASE(n) \
   case n: return launch_fwd_rows<n>(x, maps, invdeap, Tb, tw1, g, nb, coil_images, st);
@@ -512,8 +575,8 @@ int fft2_forward_rows(const void* x, const float2* maps, const float* invdeap, f
 }
 
 int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, int S0, int S1, int G0, int G1, int C,
-                 int nb, cudaStream_t st) {
-  const Geo2 g = make_geo2(S0, S1, G0, G1, C);
+                 int nb, const double* skip, cudaStream_t st) {
+  const Geo2 g = make_geo2(S0, S1, G0, G1, C, skip);
   switch (G0) {
 #define MRB_CASE(n) \
   case n: return launch_cols<n>(forward != 0, in, out, tw0, g, nb, st);
@@ -524,9 +587,23 @@ int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, 
   }
 }
 
+int fft2_toeplitz_columns(float2* Tb, const float* P, const float2* tw0, int S0, int S1, int G0, int G1, int C, int nb,
+                          int B, const double* skip, cudaStream_t st) {
+  const Geo2 g = make_geo2(S0, S1, G0, G1, C, skip);
+  switch (G0) {
+#define MRB_CASE(n) \
+  case n: return launch_toeplitz_cols<n>(Tb, P, tw0, g, nb, B, st);
+    MRB_FFT_LENGTHS(MRB_CASE)
+#undef MRB_CASE
+    default:
+      return fail(MRB_EINVAL, "no fused FFT for length %d", G0);
+  }
+}
+
 int fft2_adjoint_rows(const float2* Tb, const float2* maps, const float* invdeap, void* x, const float2* tw1, int S0,
-                      int S1, int G0, int G1, int C, int nb, float scale, cudaStream_t st) {
-  const Geo2 g = make_geo2(S0, S1, G0, G1, C);
+                      int S1, int G0, int G1, int C, int nb, float scale, const double* skip,
+                      cudaStream_t st) {
+  const Geo2 g = make_geo2(S0, S1, G0, G1, C, skip);
   switch (G1) {
 #define MRB_CASE(n) \
   case n: return launch_adj_rows<n>(Tb, maps, invdeap, x, tw1, g, nb, scale, st);

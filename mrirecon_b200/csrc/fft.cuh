@@ -16,14 +16,21 @@ size_t fft2_tmp_bytes(int S0, int G1, int C, int nb);
 // device twiddle table of a length-G transform
 int fft2_twiddles(DevBuf& tw, int G, const float2** out);
 
+// skip: device flag, the kernels return at once when it is non-zero (may be null)
 // image (nb, S0, S1) [or coil images (nb, C, S0, S1)] -> T (nb, C, S0, G1)
 int fft2_forward_rows(const void* x, const float2* maps, const float* invdeap, float2* Tb, const float2* tw1, int S0,
-                      int S1, int G0, int G1, int C, int nb, int coil_images, cudaStream_t st);
+                      int S1, int G0, int G1, int C, int nb, int coil_images, const double* skip,
+                      cudaStream_t st);
 // forward != 0: T -> grid (nb, C, G0, G1); else grid -> T
 int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, int S0, int S1, int G0, int G1, int C,
-                 int nb, cudaStream_t st);
+                 int nb, const double* skip, cudaStream_t st);
+// Toeplitz normal operator on the band, in place: T <- IFFT_G0(P[frame] * FFT_G0(T)) per
+// column; P (B, G0, G1) real, frame = be / (nb / B) (0 when B == 1)
+int fft2_toeplitz_columns(float2* Tb, const float* P, const float2* tw0, int S0, int S1, int G0, int G1, int C, int nb,
+                          int B, const double* skip, cudaStream_t st);
 // T -> image (nb, S0, S1), coil-combined with conj(maps), scaled
 int fft2_adjoint_rows(const float2* Tb, const float2* maps, const float* invdeap, void* x, const float2* tw1, int S0,
-                      int S1, int G0, int G1, int C, int nb, float scale, cudaStream_t st);
+                      int S1, int G0, int G1, int C, int nb, float scale, const double* skip,
+                      cudaStream_t st);
 
 }  // namespace mrb

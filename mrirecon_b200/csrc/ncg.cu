@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __r
 enum Slot {
   S_T = 0, S_LS_OK, S_DONE, S_REASON, S_ITER, S_F0, S_G0D, S_FT, S_GDT,
   S_ERR, S_ERD, S_EDD, S_RHO_PREV, S_RHO_INIT, S_BETA,
-  S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL,
+  S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL, S_NRESTART,
   S_RED = 24,            // reduction outputs of the gradient pass (GP_NV values)
   S_EJ = 48,             // multi-t energies (MT_MAX_J values)
   S_G0D_NEXT = 80,
@@ -628,6 +628,43 @@ __global__ void __launch_bounds__(RED_THREADS) steepest_kernel(long long n, floa
     acc[0] += (double)(gv.x * dv.x + gv.y * dv.y);
   }
   block_reduce_store<1>(acc, partials);
+}
+
+// Optional restart (not in the reference): when the updated direction is not a
+// descent direction (Re<g, d> >= 0 or not finite) it becomes steepest descent
+// -g/D.  The direction pass leaves the slots alone so that every block sees the
+// same decision; restart_slot_kernel then sets the slope to -<g, g/D> (the rho
+// of the gradient pass) and counts the restart.
+__device__ __forceinline__ bool needs_restart(const double* s) {
+  return s[S_LS_OK] != 0.0 && s[S_DONE] == 0.0 && !(s[S_G0D] < 0.0);
+}
+
+__global__ void __launch_bounds__(RED_THREADS) restart_dir_kernel(long long n, float2* __restrict__ d,
+                                                                  const float2* __restrict__ g,
+                                                                  const float* __restrict__ diag, long long ndiag,
+                                                                  const double* __restrict__ s) {
+  if (!needs_restart(s)) return;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const float2 gv = g[i];
+    const float Dv = diag ? diag[i % ndiag] : 1.f;
+    d[i] = make_float2(-(gv.x / Dv), -(gv.y / Dv));
+  }
+}
+
+__global__ void restart_slot_kernel(double* s) {
+  if (threadIdx.x != 0 || !needs_restart(s)) return;
+  s[S_G0D] = -s[S_RED + MAX_TERMS + 1];
+  s[S_G0D_NEXT] = s[S_G0D];
+  s[S_NRESTART] += 1.0;
+}
+
+// ||r||^2 after an accepted step when r is not kept (Toeplitz schedule):
+// ||r + t Ad||^2 = err + 2 t Re<r, Ad> + t^2 ||Ad||^2.
+__global__ void err_step_kernel(double* s) {
+  if (threadIdx.x != 0 || s[S_LS_OK] == 0.0) return;
+  const double t = s[S_T];
+  s[S_ERR] += 2.0 * t * s[S_ERD] + t * t * s[S_EDD];
 }
 
 __global__ void copy_slot_kernel(double* s, int dst, int src) {
@@ -864,6 +901,25 @@ extern "C" int mrb_ncg_update(int64_t n, void* x, void* d, const void* g, void* 
   int rc = finalize(part, nb, 1, 1, slots + S_G0D_NEXT, 0, nullptr, st);
   if (rc) return rc;
   copy_slot_kernel<<<1, 32, 0, st>>>(slots, S_G0D, S_G0D_NEXT);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_ncg_err_step(double* slots, mrb_stream_t stream) {
+  MRB_REQUIRE(slots != nullptr, "null slots");
+  err_step_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slots);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_ncg_restart(int64_t n, void* d, const void* g, const float* diag, int64_t ndiag, double* slots,
+                               mrb_stream_t stream) {
+  MRB_REQUIRE(d && g && slots, "null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  restart_dir_kernel<<<red_blocks(n, 2), RED_THREADS, 0, st>>>(n, (float2*)d, (const float2*)g, diag,
+                                                               ndiag > 0 ? ndiag : 1, slots);
+  MRB_LAUNCH_CHECK();
+  restart_slot_kernel<<<1, 32, 0, st>>>(slots);
   MRB_LAUNCH_CHECK();
   return 0;
 }

@@ -77,6 +77,10 @@ struct mrb_plan {
   DevBuf tw0, tw1;    // fused mode: twiddle tables of G0 and G1
   const float2* tw0p = nullptr;
   const float2* tw1p = nullptr;
+  const double* skip = nullptr;   // device flag: operator kernels return when it is non-zero
+  DevBuf psf;         // Toeplitz transfer functions (B, G0, G1) float (mrb_plan_set_toeplitz)
+  DevBuf ones;        // S0 + S1 ones: the row passes without deapodisation
+  bool have_psf = false;
   DevBuf tmp;         // scratch for set_points
   size_t spread_smem_set = 0;   // dynamic smem opt-in already granted
 
@@ -106,6 +110,7 @@ struct Geo {
   long long K;
   long long gtot;
   long long stot;
+  const double* skip;   // when non-null and non-zero the operator kernels return at once
 };
 
 Geo make_geo(const mrb_plan* p) {
@@ -123,6 +128,7 @@ Geo make_geo(const mrb_plan* p) {
   g.K = p->K;
   g.gtot = p->gtot();
   g.stot = p->stot();
+  g.skip = p->skip;
   return g;
 }
 
@@ -265,6 +271,7 @@ template <int ND>
 __global__ void __launch_bounds__(128) pre_fft_kernel(const float2* __restrict__ x, const float2* __restrict__ maps,
                                                      const float* __restrict__ invdeap, float4* __restrict__ grid,
                                                      Geo g, int nb, int coil_images) {
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   const int Gl = g.G[ND - 1];
   const int pair = blockIdx.x * blockDim.x + threadIdx.x;
   if (pair >= (Gl >> 1)) return;
@@ -332,6 +339,7 @@ template <int ND>
 __global__ void __launch_bounds__(128) post_ifft_kernel(const float2* __restrict__ grid, const float2* __restrict__ maps,
                                                        const float* __restrict__ invdeap, float2* __restrict__ x,
                                                        Geo g, int nb, float scale) {
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   const int Sl = g.S[ND - 1];
   const int il = blockIdx.x * blockDim.x + threadIdx.x;
   if (il >= Sl) return;
@@ -387,6 +395,7 @@ struct InterpArgs {
 template <int ND>
 __global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly kb) {
   constexpr int W = 4;
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   long long kk = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   int be = blockIdx.y;
   if (kk >= g.K) return;
@@ -538,6 +547,7 @@ struct SpreadSmem {
 
 template <int ND, int T>
 __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   using SM = SpreadSmem<ND, T>;
   constexpr int RS = SM::RS;
   constexpr int CELLS = SM::CELLS;
@@ -727,6 +737,7 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
 template <int ND, int T>
 __global__ void __launch_bounds__(256) zero_tiles_kernel(const int* __restrict__ keys, int n_empty,
                                                          float2* __restrict__ grid, Geo g, TileGeo tg, int nb) {
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   // block = one (rep, empty key); threads over (coil, cell pair)
   constexpr int PAIRS = (ND == 2 ? T * T : T * T * T) / 2;
   const int key = keys[blockIdx.x % n_empty];
@@ -774,6 +785,7 @@ __global__ void __launch_bounds__(256) spread_reduce_kernel(const float2* __rest
                                                             const int4* __restrict__ multi, int n_multi,
                                                             int n_slots, float2* __restrict__ grid, Geo g,
                                                             TileGeo tg, int nb) {
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   constexpr int TN = ND == 2 ? T * T : T * T * T;
   const int c = blockIdx.y;
   const int rep = blockIdx.z;
@@ -976,7 +988,7 @@ extern "C" int mrb_plan_destroy(mrb_plan* p) {
   if (!p) return 0;
   if (p->fft) cufftDestroy(p->fft);
   for (DevBuf* b : {&p->gx, &p->entries, &p->tile_start, &p->items, &p->multi, &p->partials, &p->empty_keys, &p->maps, &p->invdeap, &p->wfwd,
-                    &p->wadj, &p->grid, &p->tmp, &p->band, &p->tw0, &p->tw1})
+                    &p->wadj, &p->grid, &p->tmp, &p->band, &p->tw0, &p->tw1, &p->psf, &p->ones})
     b->release();
   delete p;
   return 0;
@@ -1220,16 +1232,16 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     // 4 = inverse column FFTs, 5 = inverse row FFTs + crop/deapod/coil sum
     if (stage == 0)
       return mrb::fft2_forward_rows(x, p->maps.as<float2>(), p->invdeap.as<float>(), p->band.as<float2>(), p->tw1p,
-                                    p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb, coil_images, st);
+                                    p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb, coil_images, p->skip, st);
     if (stage == 1)
       return mrb::fft2_columns(1, p->band.as<float2>(), p->grid.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
-                               p->G[1], p->C, nb, st);
+                               p->G[1], p->C, nb, p->skip, st);
     if (stage == 4)
       return mrb::fft2_columns(0, p->grid.as<float2>(), p->band.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
-                               p->G[1], p->C, nb, st);
+                               p->G[1], p->C, nb, p->skip, st);
     if (stage == 5)
       return mrb::fft2_adjoint_rows(p->band.as<float2>(), p->maps.as<float2>(), p->invdeap.as<float>(), (void*)x,
-                                    p->tw1p, p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb, p->scale, st);
+                                    p->tw1p, p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb, p->scale, p->skip, st);
   }
   if (stage == 0) {
     const int Gl = p->G[p->nd - 1];
@@ -1426,6 +1438,48 @@ extern "C" int mrb_plan_info(mrb_plan* p, int64_t* out, int nout) {
   MRB_REQUIRE(p != nullptr && out != nullptr, "null plan or output");
   int64_t v[7] = {p->n_entries, p->ntiles, p->touched, p->tile, p->coils_per_item, p->gtot(), p->fft_mode};
   for (int i = 0; i < nout && i < 7; ++i) out[i] = v[i];
+  return 0;
+}
+
+extern "C" int mrb_plan_set_toeplitz(mrb_plan* p, const float* psf, mrb_stream_t stream) {
+  MRB_REQUIRE(p != nullptr && psf != nullptr, "null plan or transfer function");
+  MRB_REQUIRE(p->fft_mode == 1, "the Toeplitz normal operator needs the fused FFT mode (2D, compiled grid sizes)");
+  const size_t bytes = (size_t)p->B * p->gtot() * sizeof(float);
+  int rc;
+  if ((rc = p->psf.ensure(bytes))) return rc;
+  MRB_CUDA_TRY(cudaMemcpyAsync(p->psf.p, psf, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  if (!p->ones.p) {
+    std::vector<float> one((size_t)p->S[0] + p->S[1], 1.f);
+    if ((rc = p->ones.ensure(one.size() * sizeof(float)))) return rc;
+    MRB_CUDA_TRY(cudaMemcpy(p->ones.p, one.data(), one.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  p->have_psf = true;
+  return 0;
+}
+
+extern "C" int mrb_nufft_normal(mrb_plan* p, const void* x, void* out, int nb, mrb_stream_t stream) {
+  int rc;
+  if ((rc = check_ready(p))) return rc;
+  if ((rc = check_nb(p, nb))) return rc;
+  MRB_REQUIRE(x != nullptr && out != nullptr, "null x or out");
+  if (!p->have_psf) return mrb::fail(MRB_ESTATE, "plan has no Toeplitz transfer function (mrb_plan_set_toeplitz)");
+  if ((rc = ensure_grid(p, nb))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const float* one = p->ones.as<float>();
+  float2* band = p->band.as<float2>();
+  if ((rc = mrb::fft2_forward_rows(x, p->maps.as<float2>(), one, band, p->tw1p, p->S[0], p->S[1], p->G[0], p->G[1],
+                                   p->C, nb, 0, p->skip, st)))
+    return rc;
+  if ((rc = mrb::fft2_toeplitz_columns(band, p->psf.as<float>(), p->tw0p, p->S[0], p->S[1], p->G[0], p->G[1], p->C,
+                                       nb, p->B, p->skip, st)))
+    return rc;
+  return mrb::fft2_adjoint_rows(band, p->maps.as<float2>(), one, out, p->tw1p, p->S[0], p->S[1], p->G[0], p->G[1],
+                                p->C, nb, 1.f, p->skip, st);
+}
+
+extern "C" int mrb_plan_set_skip_flag(mrb_plan* p, const double* flag) {
+  MRB_REQUIRE(p != nullptr, "null plan");
+  p->skip = flag;
   return 0;
 }
 

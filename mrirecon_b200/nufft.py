@@ -109,6 +109,24 @@ class KBPlan:
         _lib.check(self.lib.mrb_nufft_stage(self.h, self.STAGES[name], _lib.ptr(x), _lib.ptr(y), int(nb),
                                             _lib.stream_ptr(self.device)), "nufft_stage")
 
+    def set_toeplitz(self, psf: torch.Tensor) -> None:
+        """Transfer function (B, G0, G1) float32 of the Toeplitz normal operator (copied)."""
+        _lib.require_cuda(psf, "psf")
+        if psf.dtype != torch.float32 or not psf.is_contiguous():
+            raise ValueError("psf must be contiguous float32")
+        _lib.check(self.lib.mrb_plan_set_toeplitz(self.h, _lib.ptr(psf), _lib.stream_ptr(self.device)),
+                   "plan_set_toeplitz")
+
+    def normal(self, x: torch.Tensor, out: torch.Tensor, nb: int) -> None:
+        """out = A^H A x through the Toeplitz transfer function (no gridding)."""
+        _lib.check(self.lib.mrb_nufft_normal(self.h, _lib.ptr(x), _lib.ptr(out), int(nb),
+                                             _lib.stream_ptr(self.device)), "nufft_normal")
+
+    def set_skip_flag(self, ptr: Optional[int]) -> None:
+        """Device address of a double that, when non-zero, makes the operator
+        kernels launched from now on return at once (None clears it)."""
+        _lib.check(self.lib.mrb_plan_set_skip_flag(self.h, ptr), "plan_set_skip_flag")
+
     def info(self) -> dict:
         out = (ct.c_int64 * 7)()
         _lib.check(self.lib.mrb_plan_info(self.h, out, 7), "plan_info")
@@ -251,6 +269,79 @@ class B200NUFFTAdapter:
 
     def k_per_frame(self) -> int:
         return int(self._K)
+
+    # -- Toeplitz normal operator ----------------------------------------------
+    @torch.no_grad()
+    def prepare_toeplitz(self, psf: str = "exact") -> torch.Tensor:
+        """Compute and install the Toeplitz transfer function of A^H A.
+
+        t_b(D) = sum_k w_k exp(i w_k . D) (w = forward x adjoint DCF weights) on
+        the lags D = i - G/2 of a G0 x G1 image.  psf="exact": the exponential
+        separates, t_b = E0^T diag(w) E1 with E_d[k, i] = exp(i w_dk (i - G_d/2)),
+        one FP64 matrix product per frame (exact to rounding, so the Toeplitz
+        A^H A is the NUDFT normal operator and positive semi-definite);
+        psf="kb": the adjoint NUFFT of w onto the G0 x G1 image (a second,
+        unnormalised plan, its own KB gridding).  Placed circularly (lag -G/2 set
+        to zero, never used by the linear convolution of an S image), its FFT is
+        real.  Scaled by s^2 / (G0 G1) (s the ortho factor) and rolled by G/2 for
+        the row passes' (-1)^n signs.  Needs a 2D plan in the fused FFT mode with
+        G >= 2 S - 1 (osf >= 2).  Returns the transfer function."""
+        if self.ndim != 2:
+            raise ValueError("the Toeplitz normal operator is 2D")
+        plan = self._plan
+        if plan.info()["fft_mode"] != FFT_FUSED:
+            raise RuntimeError("the Toeplitz normal operator needs the fused FFT mode")
+        S = self._im_shape[1:]
+        G = tuple(int(math.ceil(self.osf * s)) for s in S)
+        if any(g < 2 * s - 1 for g, s in zip(G, S)):
+            raise ValueError("the Toeplitz embedding needs a grid of at least 2S-1 (osf >= 2)")
+        B, K = int(self._traj_BndK.shape[0]), int(self._K)
+        dev = self._dev
+        w = torch.ones((B, K), dtype=torch.float32, device=dev)
+        if self._dcf_BK is not None and self.dcf_mode != "none":
+            d = self._dcf_BK
+            if self.dcf_mode == "balanced":
+                w = d.clamp_min(0)
+            else:
+                w = d ** (int(self.apply_dcf_in_fwd) + int(self.apply_dcf_in_adj))
+        if psf == "exact":
+            t = torch.empty((B,) + G, dtype=torch.complex128, device=dev)
+            lag = [torch.arange(g, dtype=torch.float64, device=dev) - g // 2 for g in G]
+            for b in range(B):
+                om = self._traj_BndK[b].to(torch.float64)                      # (2, K)
+                e0 = torch.polar(torch.ones(1, dtype=torch.float64, device=dev), om[0][:, None] * lag[0][None, :])
+                e1 = torch.polar(torch.ones(1, dtype=torch.float64, device=dev), om[1][:, None] * lag[1][None, :])
+                t[b] = e0.transpose(0, 1) @ (w[b].to(torch.float64)[:, None] * e1)
+        elif psf == "kb":
+            psf_op = B200NUFFTAdapter(ndim=2, dcf_mode="none", kwidth=self.kwidth, osf=self.osf, norm="none")
+            psf_op.prepare((1,) + G, self._traj_BndK, None, torch.ones((1,) + G, dtype=torch.complex64, device=dev),
+                           torch.complex64, dev)
+            t = psf_op.AH(w.to(torch.complex64).reshape(B, 1, K)).reshape(B, *G)
+            del psf_op
+        else:
+            raise ValueError("psf must be 'exact' or 'kb'")
+        c = torch.roll(t, shifts=(G[0] // 2, G[1] // 2), dims=(1, 2))
+        c[:, G[0] // 2, :] = 0
+        c[:, :, G[1] // 2] = 0
+        P = torch.fft.fft2(c.to(torch.complex128)).real
+        s2 = 1.0 / (G[0] * G[1]) if self.norm == "ortho" else 1.0
+        P = torch.roll(P * (s2 / (G[0] * G[1])), shifts=(G[0] // 2, G[1] // 2), dims=(1, 2))
+        P = P.to(torch.float32).contiguous()
+        plan.set_toeplitz(P)
+        self._toeplitz = True
+        return P
+
+    def AHA(self, x: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """A^H A x by the Toeplitz transfer function (prepare_toeplitz first)."""
+        if not getattr(self, "_toeplitz", False):
+            raise RuntimeError("call prepare_toeplitz() first")
+        if x.dtype != torch.complex64 or not x.is_contiguous():
+            raise ValueError("x must be contiguous complex64")
+        nb = int(x.shape[0])
+        if out is None:
+            out = torch.empty_like(x)
+        self._plan.normal(x, out, nb)
+        return out
 
     # operator conveniences so the adapter can drive the solver directly
     @property

@@ -20,6 +20,15 @@ Two schedules compute the same iterates (up to floating-point rounding):
     gradient/statistics pass at the accepted t and one fused update pass.
     Iterations are captured in a CUDA graph and replayed.
 
+``schedule="toeplitz"`` (Armijo)  the fast schedule with the normal operator
+    A^H A applied through its Toeplitz transfer function on the 2x grid
+    (``B200NUFFTAdapter.prepare_toeplitz``): A^H r and A^H A d live in image
+    space (A^H r = A^H A x - A^H y, A^H y computed once by the gridded
+    adjoint), Re<r, Ad> = Re<A^H r, d>, ||Ad||^2 = Re<A^H A d, d>, and ||r||^2
+    follows its quadratic recurrence.  One iteration is one fused FFT pass and
+    no gridding; the operator differs from the gridded A^H A by the KB
+    approximation of the point-spread function (stated in the tests).
+
 FP64 holds every objective value, dot product and line-search decision.
 ``stop_window`` > 0 adds the windowed relative-objective stop rule
 (f_{k-W} - f_k) <= W * stop_tol * |f_k| on the accepted objectives.
@@ -40,7 +49,7 @@ from .roles import Roles
 # slot indices (must match csrc/ncg.cu)
 S_T, S_LS_OK, S_DONE, S_REASON, S_ITER, S_F0, S_G0D, S_FT, S_GDT = range(9)
 S_ERR, S_ERD, S_EDD, S_RHO_PREV, S_RHO_INIT, S_BETA = range(9, 15)
-S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL = range(15, 19)
+S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL, S_NRESTART = range(15, 20)
 S_RED, S_EJ, S_G0D_NEXT = 24, 48, 80
 MAX_TERMS = 4
 REASONS = {0: "running", 1: "line-search failed", 2: "converged (tol_g/tol_step)",
@@ -71,6 +80,9 @@ class CGConfig:
     stop_tol: float = 1e-4
     cuda_graph: bool = True
     iters_per_graph: int = 8
+    # replace a non-descent direction by steepest descent instead of stopping
+    # (not in the reference, whose loop ends on the line-search failure; fast schedule)
+    restart: bool = False
     # > 0: the frame axis holds independent series of this many frames (a batch of
     # separate problems; temporal TV does not couple series)
     series_length: int = 0
@@ -122,11 +134,11 @@ class CGSolver:
             raise ValueError(f"direction must be one of {list(DIRS)}")
         if c.ls_name not in ("armijo", "wolfe"):
             raise ValueError("ls_name must be 'armijo' or 'wolfe'")
-        if c.schedule not in ("fast", "reference"):
-            raise ValueError("schedule must be 'fast' or 'reference'")
-        if c.schedule == "fast" and c.ls_name != "armijo":
-            raise ValueError("the fast schedule implements Armijo; use schedule='reference' for Wolfe")
-        if c.schedule == "fast" and not (1 <= c.ls_max_iter <= 23):
+        if c.schedule not in ("fast", "reference", "toeplitz"):
+            raise ValueError("schedule must be 'fast', 'toeplitz' or 'reference'")
+        if c.schedule != "reference" and c.ls_name != "armijo":
+            raise ValueError("the fast schedules implement Armijo; use schedule='reference' for Wolfe")
+        if c.schedule != "reference" and not (1 <= c.ls_max_iter <= 23):
             raise ValueError("the fast schedule evaluates at most 23 trial steps per pass")
         _lib.require_cuda(y, "y")
         self.lib = _lib.load()
@@ -164,6 +176,18 @@ class CGSolver:
         self.cfg_dev = torch.tensor([c.c1, c.ls_beta, c.ls_max_iter, c.max_iter, c.tol_g, c.tol_step,
                                      c.stop_window, c.stop_tol, DIRS[c.direction.lower()], c.max_iter],
                                     dtype=torch.float64, device=dev)
+        self._toep = None
+        if c.schedule == "toeplitz":
+            backend = getattr(nufft_op, "backend", nufft_op)
+            if not hasattr(backend, "AHA"):
+                raise ValueError("the toeplitz schedule needs the B200 NUFFT backend")
+            if not getattr(backend, "_toeplitz", False):
+                backend.prepare_toeplitz()
+            self._toep = backend
+            self.ahy = z(ishape)
+            self._dot_a = (ct.c_void_p * 2)(_lib.ptr(self.gr), _lib.ptr(self.gAd))
+            self._dot_b = (ct.c_void_p * 2)(_lib.ptr(self.d), _lib.ptr(self.d))
+            self._dot_w = (ct.c_void_p * 2)(None, None)
         self.ws = SolverWorkspace({"var": self.x, "grad": self.g, "dir": self.d, "data": self.y,
                                    "fwd_dir_sh": self.Ad, "resid_sh": self.r}, roles, dev)
         self.iter = 0
@@ -215,7 +239,13 @@ class CGSolver:
         _lib.check(self.lib.mrb_kspace_pass(1, self.n_k, _lib.ptr(self.r), None, _lib.ptr(self.Ad),
                                             _lib.ptr(self.y), None, 0.0, None, self._slot(S_ERR),
                                             _lib.ptr(self.ws_buf), st), "kspace_pass")
-        self._AH(self.r, self.gr)
+        if self._toep is not None:
+            # A^H r = A^H A x - A^H y (Toeplitz normal operator, gridded A^H y)
+            self._AH(self.y, self.ahy)
+            self._toep.AHA(self.x, out=self.gr)
+            self.gr.sub_(self.ahy)
+        else:
+            self._AH(self.r, self.gr)
         self._tv_grad(None, None, 0.0, self.gr, None, self.g, self._slot(S_RED))
         _lib.check(self.lib.mrb_ncg_steepest(self.n_img, _lib.ptr(self.d), _lib.ptr(self.g), _lib.ptr(self.g_prev),
                                              None, 0, self._slot(S_G0D), _lib.ptr(self.ws_buf), st), "steepest")
@@ -229,10 +259,15 @@ class CGSolver:
         st = self._st()
         lib, ws = self.lib, _lib.ptr(self.ws_buf)
         J = self.cfg.ls_max_iter + 1
-        self._A(self.d, self.Ad)
-        _lib.check(lib.mrb_kspace_pass(0, self.n_k, _lib.ptr(self.r), _lib.ptr(self.Ad), None, None, None, 0.0,
-                                       self._slot(S_DONE), self._slot(S_ERR), ws, st), "kspace_pass")
-        self._AH(self.Ad, self.gAd)
+        if self._toep is not None:
+            self._toep.AHA(self.d, out=self.gAd)
+            _lib.check(lib.mrb_dots_f64(self.n_img, 2, self._dot_a, self._dot_b, self._dot_w, 0,
+                                        self._slot(S_ERD), ws, st), "dots")
+        else:
+            self._A(self.d, self.Ad)
+            _lib.check(lib.mrb_kspace_pass(0, self.n_k, _lib.ptr(self.r), _lib.ptr(self.Ad), None, None, None,
+                                           0.0, self._slot(S_DONE), self._slot(S_ERR), ws, st), "kspace_pass")
+            self._AH(self.Ad, self.gAd)
         _lib.check(lib.mrb_tv_multi(self.nd, self._Sarr, self.F, self._terms_arr, self.nterms, _lib.ptr(self.x),
                                     _lib.ptr(self.d), _lib.ptr(self.ts), J, self._slot(S_DONE), self._slot(S_EJ),
                                     ws, st), "tv_multi")
@@ -244,18 +279,49 @@ class CGSolver:
         _lib.check(lib.mrb_ncg_update(self.n_img, _lib.ptr(self.x), _lib.ptr(self.d), _lib.ptr(self.g),
                                       _lib.ptr(self.gr), _lib.ptr(self.gAd), _lib.ptr(self.g_prev), None, 0,
                                       _lib.ptr(self.s), ws, st), "ncg_update")
-        _lib.check(lib.mrb_kspace_pass(2, self.n_k, _lib.ptr(self.r), _lib.ptr(self.Ad), None, None,
-                                       self._slot(S_T), 0.0, self._slot(S_DONE), None, ws, st), "kspace_pass")
+        if self.cfg.restart:
+            _lib.check(lib.mrb_ncg_restart(self.n_img, _lib.ptr(self.d), _lib.ptr(self.g), None, 0,
+                                           _lib.ptr(self.s), st), "ncg_restart")
+        if self._toep is not None:
+            _lib.check(lib.mrb_ncg_err_step(_lib.ptr(self.s), st), "err_step")
+        else:
+            _lib.check(lib.mrb_kspace_pass(2, self.n_k, _lib.ptr(self.r), _lib.ptr(self.Ad), None, None,
+                                           self._slot(S_T), 0.0, self._slot(S_DONE), None, ws, st), "kspace_pass")
+
+    def _plan(self):
+        """The B200 NUFFT plan behind the operator (front-end or adapter), if any."""
+        backend = getattr(self.op, "backend", self.op)
+        return getattr(backend, "plan", None)
+
+    def _skip_on_done(self, on: bool):
+        plan = self._plan()
+        if plan is not None and hasattr(plan, "set_skip_flag"):
+            plan.set_skip_flag(self._slot(S_DONE) if on else None)
 
     def _run_fast(self, max_iter):
-        c = self.cfg
+        try:
+            self._run_fast_body(max_iter)
+        finally:
+            self._skip_on_done(False)
+
+    def _fast_setup(self, max_iter) -> bool:
+        """Size the history for max_iter; True when a captured graph is still valid."""
         self.cfg_dev[3] = float(max_iter)
+        ok = True
         if self.hist.shape[0] < max_iter:
             self.hist = torch.zeros((max_iter, self.hist_cols), dtype=torch.float64, device=self.device)
             self._graph = None                      # the captured graph wrote the old history buffer
+            ok = False
         self.cfg_dev[9] = float(self.hist.shape[0])
+        return ok
+
+    def _run_fast_body(self, max_iter):
+        c = self.cfg
+        self._fast_setup(max_iter)
         n0 = _lib.launch_count()
         self._prime_fast()
+        # iterations past the stop (graph replays) skip the operator kernels
+        self._skip_on_done(True)
         self._iteration_fast()                                # eager: warms every lazy allocation
         self.launch_stats["eager"] += _lib.launch_count() - n0
         done = lambda: bool(self.s[S_DONE].item())
@@ -440,13 +506,18 @@ class CGSolver:
         self.cfg_dev[5] = float(c.tol_step)
         max_iter = int(max_iter or c.max_iter)
         with torch.cuda.device(self.device):
-            if c.schedule == "fast":
+            if c.schedule in ("fast", "toeplitz"):
                 self._run_fast(max_iter)
                 self.iter = int(self.s[S_ITER].item())
                 self.stop_reason = REASONS[int(self.s[S_REASON].item())]
             else:
                 self._run_reference(max_iter)
         return self
+
+    @property
+    def restarts(self) -> int:
+        """Directions replaced by steepest descent in the last run (CGConfig.restart)."""
+        return int(self.s[S_NRESTART].item())
 
     def launches(self) -> int:
         """Library kernel launches executed so far by this solver."""

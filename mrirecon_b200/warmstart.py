@@ -2,7 +2,9 @@
 
 The network (3 levels, 32 base channels, 3x3x3 convolutions over (t, y, x),
 U-Net skips, output = input + net(input)) maps a normalised adjoint
-reconstruction to an estimate of the converged NCG reconstruction.  It is
+reconstruction -- the density-compensated adjoint A^H(w y) with the radial
+ramp w ~ |k| (``ramp_adjoint``), whose point-spread function is far narrower
+than that of A^H y -- to an estimate of the converged NCG reconstruction.  It is
 trained on pairs (adjoint recon -> converged NCG recon) that the solver of
 this package generates on seeded synthetic phantoms, with the project's own
 CUDA kernels (``csrc/cnn.cu``): BF16 tensor-core implicit-GEMM convolution
@@ -20,6 +22,7 @@ from __future__ import annotations
 
 import ctypes as ct
 import math
+import os
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Tuple
 
@@ -34,6 +37,13 @@ LAYERS: List[Tuple[str, int, int, int, int, bool]] = [
     ("c4", 64, 64, 64, 64, True), ("c5", 64, 64, 128, 128, True), ("c6", 192, 192, 64, 64, True),
     ("c7", 96, 96, 32, 32, True), ("c8", 32, 32, 32, 2, False)]
 XC = 32          # channels of the packed input tensor
+
+# Weights trained for the GRASP acquisition (256^2, 12 coils, 21 golden-angle
+# spokes x 512 samples per frame) by
+#   python -m mrirecon_b200.warmstart --out mrirecon_b200/weights/warmstart_grasp256.npz \
+#       --series 2000 --per-solve 25 --epochs 12
+# (2,000 seeded 8-frame series, pairs from this package's NCG, ~13 GPU-minutes on one B200).
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "warmstart_grasp256.npz")
 
 _SIGS = {
     "mrb_cnn_conv3d_fwd": [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p,
@@ -131,6 +141,11 @@ class WarmStartCNN:
     def load(self, path):
         self.load_state_dict(np.load(path))
         return self
+
+    @classmethod
+    def pretrained(cls, device="cuda", path: str = DEFAULT_WEIGHTS) -> "WarmStartCNN":
+        """The network with the packaged GRASP weights."""
+        return cls(device).load(path)
 
     # ------------------------------------------------------------------ buffers
     def _buffers(self, Nb, D, H, W, train: bool):
@@ -363,31 +378,59 @@ def make_pairs(n_series: int, spec: PairSpec = PairSpec(), seed0: int = 1000, pe
         sol = CGSolver(y, ad, regm, cfg)
         sol.run()
         xs_ref.append(sol.result().reshape(P, F, N, N).clone())
-        xs_adj.append(ad.AH(y).reshape(P, F, N, N))
+        xs_adj.append(ramp_adjoint(ad, y).reshape(P, F, N, N))
+        del ad._ramp_adapter
         if log:
             log(f"pairs {s0 + P}/{n_series}: {sol.iter} iterations ({sol.stop_reason})")
     return torch.cat(xs_adj), torch.cat(xs_ref)
 
 
-def warm_start(solver, cnn: WarmStartCNN, adjoint: Optional[torch.Tensor] = None) -> dict:
+def ramp_adjoint(op, y: torch.Tensor) -> torch.Tensor:
+    """The network input: the density-compensated adjoint A^H(w * y) (gridding
+    reconstruction) with the radial ramp w = max(|k|, pi / (2 max S)) / pi.
+    `op` is a B200 NUFFT front-end or adapter and y is in its canonical
+    (B, C, K) layout; the ramp operator is built once and cached on the adapter."""
+    from .nufft import B200NUFFTAdapter
+    ad = getattr(op, "backend", op)
+    r = getattr(ad, "_ramp_adapter", None)
+    if r is None:
+        traj = ad._traj_BndK
+        S = ad._im_shape[1:]
+        kr = torch.linalg.vector_norm(traj, dim=1)
+        w = kr.clamp_min(math.pi / (2.0 * max(S))) / math.pi
+        r = B200NUFFTAdapter(ndim=ad.ndim, dcf_mode="standard", apply_dcf_in_fwd=False, apply_dcf_in_adj=True,
+                             kwidth=ad.kwidth, osf=ad.osf, norm=ad.norm)
+        r.prepare(ad._im_shape, traj, w, ad._maps, torch.complex64, ad._dev)
+        ad._ramp_adapter = r
+    C, K = int(ad._im_shape[0]), int(ad._K)
+    return r.AH(y.reshape(-1, C, K))
+
+
+def _ls_scaled(op, y, x):
+    """x times its least-squares data-consistency factor argmin_a ||a A x - y||."""
+    Ax = op.A(x)
+    den = float(torch.vdot(Ax.reshape(-1), Ax.reshape(-1)).real)
+    a = float(torch.vdot(Ax.reshape(-1), y.reshape(-1)).real) / max(den, 1e-30)
+    return (a * x).to(torch.complex64)
+
+
+def network_start(op, y, cnn: WarmStartCNN, image_shape) -> torch.Tensor:
+    """The network's image for data y (LS-scaled), shaped like the solver's image."""
+    z = ramp_adjoint(op, y)
+    F = int(z.shape[0])
+    S = tuple(int(s) for s in z.shape[2:])
+    x = cnn.infer(z.to(torch.complex64).reshape((1, F) + S)).reshape(image_shape)
+    return _ls_scaled(op, y, x)
+
+
+def warm_start(solver, cnn: WarmStartCNN) -> dict:
     """Initial image for `solver` from the network, with the fallback rule:
     the network output is used only if its objective is below that of the
-    adjoint start (the adjoint recon scaled by its least-squares factor)."""
+    adjoint start (the adjoint recon A^H y scaled by its least-squares factor)."""
     op = solver.op
     y = solver.y
-    xa = op.AH(y) if adjoint is None else adjoint
-    Axa = op.A(xa)
-    den = float(torch.vdot(Axa.reshape(-1), Axa.reshape(-1)).real)
-    alpha = float(torch.vdot(Axa.reshape(-1), y.reshape(-1)).real) / max(den, 1e-30)
-    x_adj = (alpha * xa).to(torch.complex64)
-    F = int(xa.shape[0])
-    S = tuple(int(s) for s in xa.shape[2:])
-    # the network sees the raw adjoint, as in training (make_pairs); its output is
-    # then given its own least-squares data-consistency scale
-    x_net = cnn.infer(xa.to(torch.complex64).reshape((1, F) + S)).reshape(xa.shape)
-    Axn = op.A(x_net)
-    dn = float(torch.vdot(Axn.reshape(-1), Axn.reshape(-1)).real)
-    x_net = (float(torch.vdot(Axn.reshape(-1), y.reshape(-1)).real) / max(dn, 1e-30) * x_net).to(torch.complex64)
+    x_adj = _ls_scaled(op, y, op.AH(y))
+    x_net = network_start(op, y, cnn, x_adj.shape)
     f_adj = _objective_at(solver, x_adj)
     f_net = _objective_at(solver, x_net)
     use = f_net < f_adj
@@ -403,19 +446,75 @@ def _objective_at(solver, x):
     return f
 
 
+def evaluate(cnn: "WarmStartCNN", workload: str = "grasp", device="cuda", reps: int = 1) -> dict:
+    """Warm-start + NCG against plain NCG (from x = 0) on a seeded workload, both to
+    the same windowed objective tolerance on the same GPU.  Times are device
+    seconds per solve (CUDA events); the warm-started time includes the adjoint,
+    the network, its least-squares scaling and the fallback test."""
+    from .solver import CGSolver
+    from .workloads import WORKLOADS, build, regs, solver_cfg
+    w = WORKLOADS[workload]
+    dev = torch.device(device)
+    op, y, x_true, _, _ = build(w, dev)
+    solver = CGSolver(y, op, regs(w), solver_cfg())
+    solver.reset().run()
+    warm_start(solver, cnn)
+    solver.run()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    a, b = ev(), ev()
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(reps):
+        solver.reset().run()
+    b.record()
+    torch.cuda.synchronize()
+    t_plain = a.elapsed_time(b) / 1e3 / reps
+    it_plain = solver.iter
+    x_plain = solver.result().clone()
+    f_plain = solver.objective()
+    a, b = ev(), ev()
+    a.record()
+    for _ in range(reps):
+        info = warm_start(solver, cnn)
+        solver.run()
+    b.record()
+    torch.cuda.synchronize()
+    t_warm = a.elapsed_time(b) / 1e3 / reps
+    x_warm = solver.result()
+    xt = x_true.to(dev).reshape(x_plain.shape)
+    rel = lambda u, v: float(torch.linalg.vector_norm(u - v) / torch.linalg.vector_norm(v))
+    x_net = network_start(op, y, cnn, x_plain.shape)
+    x_adj = _ls_scaled(op, y, op.AH(y))
+    return {"workload": w["name"], "plain_s": t_plain, "plain_iters": it_plain, "f_plain": f_plain,
+            "warm_s": t_warm, "warm_iters": solver.iter, "f_warm": solver.objective(),
+            "err_vs_plain": rel(x_warm, x_plain), "plain_err_vs_truth": rel(x_plain, xt),
+            "warm_err_vs_truth": rel(x_warm, xt), "network_start_err_vs_plain": rel(x_net, x_plain),
+            "adjoint_start_err_vs_plain": rel(x_adj, x_plain), **info}
+
+
 def main(argv=None):
-    """Generate training pairs, train, save:  python -m mrirecon_b200.warmstart --out w.npz"""
+    """Generate training pairs, train, save:  python -m mrirecon_b200.warmstart --out w.npz
+    Evaluate saved weights on the GRASP workload:  python -m mrirecon_b200.warmstart --eval w.npz"""
     import argparse
+    import json
     import time
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", required=True)
+    ap.add_argument("--eval", default=None)
+    ap.add_argument("--out", default=None)
     ap.add_argument("--series", type=int, default=2000)
     ap.add_argument("--per-solve", type=int, default=25)
-    ap.add_argument("--epochs", type=int, default=6)
+    ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--batch", type=int, default=2)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--frames", type=int, default=8)
     a = ap.parse_args(argv)
+    if a.eval:
+        net = WarmStartCNN("cuda", seed=0)
+        net.load(a.eval)
+        print(json.dumps(evaluate(net)), flush=True)
+        return
+    if not a.out:
+        ap.error("--out or --eval is required")
     t0 = time.time()
     spec = PairSpec(frames=a.frames)
     xa, xr = make_pairs(a.series, spec, per_solve=a.per_solve, log=lambda m: print(m, flush=True))
@@ -425,6 +524,7 @@ def main(argv=None):
     hist = net.train(xa, xr, epochs=a.epochs, batch=a.batch, lr=a.lr, log=lambda m: print(m, flush=True))
     print(f"training: {time.time() - t1:.1f} s, loss per epoch {hist}", flush=True)
     net.save(a.out)
+    print(json.dumps(evaluate(net)), flush=True)
 
 
 if __name__ == "__main__":

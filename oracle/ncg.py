@@ -13,6 +13,8 @@ no-op.  Follows:
      FR beta is 1: directions.py:146-156)
 * Objective.f_g_tensor         graspcg/ops/objective.py:184-291
     r = Ax + t Ad - y; f = 0.5||r||^2 + R(x + t d); g = A^H r + grad R
+* optional restart (NCGConfig.restart, not in the reference): a direction
+    with Re<g, d> >= 0 after the update becomes -g/D
 * converged                    graspcg/solvers/utils.py:40-43
 * history                      graspcg/solvers/utils.py:64-87; the reference
     adds xnorm/gnorm/stepnorm into live StatsBoard slots that are never reset,
@@ -49,6 +51,7 @@ class NCGConfig:
     max_iter: int = 50
     tol_g: float = 1e-4
     tol_step: float = 1e-9
+    restart: bool = False   # not in the reference: non-descent direction -> -g/D
 
 
 def _rdot(a, b):
@@ -75,6 +78,7 @@ class NCGOracle:
         self.hist: List[Dict[str, float]] = []
         self.n_A = 0
         self.n_AH = 0
+        self.n_restart = 0
         self._cum = {"xnorm": 0.0, "gnorm": 0.0, "stepnorm": 0.0}
 
     # --- objective -----------------------------------------------------------
@@ -178,6 +182,9 @@ class NCGOracle:
         else:
             raise ValueError(name)
         self.d = self.d * beta - self.g / self.D
+        if self.cfg.restart and not (float(_rdot(self.g, self.d)) < 0.0):
+            self.d = -(self.g / self.D)
+            self.n_restart += 1
         if name in ("prplus", "dy"):
             self.g_prev = self.g.clone()
         return beta

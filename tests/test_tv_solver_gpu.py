@@ -298,3 +298,47 @@ def test_known_answers_cartesian(cuda, direction, schedule, ls):
     h = s.history()
     assert h[0]["step"] == 1.0 and h[0]["gdot"] < 0
     assert rel(s.result(), xt) < 1e-5
+
+
+def test_restart_on_non_descent_matches_oracle(cuda):
+    """Densely sampled radial data: FR + Armijo (reference semantics) stops on a
+    non-descent direction after one step, as the CPU oracle does; with
+    CGConfig.restart the direction falls back to -g and the solve continues,
+    again step for step with the oracle (objective history rel <= 1e-4)."""
+    import math
+    from oracle import kb as okb
+    from oracle.ncg import NCGOracle, NCGConfig, TVSpec
+    from mrirecon_b200 import phantoms
+    from mrirecon_b200.nufft import NUFFT, NUFFTConfig
+    from mrirecon_b200.regularization import RegManager, TVND, TVParams
+    from mrirecon_b200.solver import CGConfig, CGSolver
+    from mrirecon_b200.workloads import axis_spec
+    N, C, sp = 64, 6, 150
+    x = phantoms.ellipse_phantom(N, seed=7000).reshape(1, 1, N, N)
+    maps = phantoms.coil_maps(N, C)
+    traj = phantoms.golden_angle_radial(sp, 2 * N).unsqueeze(0)
+    k = okb.KBNufft(maps, traj, None, dtype=torch.complex64, norm="ortho")
+    y = k.A(x).to(torch.complex64)
+    A = lambda v: k.A(v).to(torch.complex64)
+    AH = lambda v: k.AH(v).to(torch.complex64)
+    op = NUFFT(maps.to(cuda), traj.to(cuda), None, axis=axis_spec(), config=NUFFTConfig(ndim=2, traj_units="rad"),
+               device=cuda)
+    regm = RegManager([TVND("s", TVParams(weight=1e-3, eps=1e-3, axes="spatial"))])
+    n_it = 12
+    runs = {}
+    for restart in (False, True):
+        o = NCGOracle(A, AH, y, torch.zeros_like(x), [TVSpec((2, 3), 1e-3, 1e-3)],
+                      NCGConfig(max_iter=n_it, restart=restart)).run()
+        s = CGSolver(y.to(cuda), op, regm, CGConfig(max_iter=n_it, stop_window=0, restart=restart)).run()
+        runs[restart] = (o, s)
+    o, s = runs[False]
+    assert len(o.hist) < 3, "the densely sampled case should stop early without restart"
+    assert s.iter == len(o.hist)
+    o, s = runs[True]
+    assert len(o.hist) == n_it and s.iter == n_it
+    assert o.n_restart >= 1 and s.restarts == o.n_restart
+    fo = [h["f"] for h in o.hist]
+    fs = [h["f"] for h in s.history()]
+    for a, b in zip(fo, fs):
+        assert abs(a - b) <= 1e-4 * abs(a)
+    assert all(b <= a * (1 + 1e-6) for a, b in zip(fs, fs[1:]))

@@ -1,0 +1,50 @@
+"""What the trained warm-start network gains over the method without it, and
+the fallback rule (GRASP workload: 256^2, 34 frames, 12 coils, 21 spokes)."""
+import pytest
+import torch
+
+from mrirecon_b200 import phantoms
+from mrirecon_b200.nufft import B200NUFFTAdapter
+from mrirecon_b200.regularization import RegManager, TVND, TVParams
+from mrirecon_b200.solver import CGConfig, CGSolver
+from mrirecon_b200.warmstart import WarmStartCNN, evaluate, warm_start, _ls_scaled
+
+pytestmark = pytest.mark.gpu
+
+
+def test_trained_network_gains_on_grasp(cuda):
+    """Packaged weights: the network start has a far lower objective than the
+    scaled adjoint, NCG then needs far fewer iterations and less time to the same
+    windowed tolerance, and ends at an objective no higher than plain NCG's."""
+    r = evaluate(WarmStartCNN.pretrained(cuda))
+    assert r["used_network"]
+    assert r["f_network"] < 0.1 * r["f_adjoint"]
+    assert r["network_start_err_vs_plain"] < 0.5 * r["adjoint_start_err_vs_plain"]
+    assert r["warm_iters"] < 0.7 * r["plain_iters"]
+    assert r["warm_s"] < r["plain_s"]
+    assert r["f_warm"] <= r["f_plain"] * (1 + 1e-3)
+    # same tolerance, different start: the two results differ by what the
+    # windowed 1e-4 stop rule leaves unconverged
+    assert r["err_vs_plain"] < 2e-2
+
+
+def test_fallback_to_adjoint_start(cuda):
+    """A network whose output has a higher objective than the scaled adjoint is
+    not used: the solve starts from the scaled adjoint and still converges."""
+    N, C, F = 64, 4, 4
+    x = phantoms.dynamic_phantom(N, F, seed=4).unsqueeze(1)
+    maps = phantoms.coil_maps(N, C)
+    traj = phantoms.grasp_trajectory(F, 13, 2 * N)
+    ad = B200NUFFTAdapter(ndim=2)
+    ad.prepare((C, N, N), traj.to(cuda), None, maps.to(cuda), torch.complex64, cuda)
+    y = ad.A(x.to(cuda))
+    regm = RegManager([TVND("s", TVParams(weight=1e-3, eps=1e-3, axes="spatial")),
+                       TVND("t", TVParams(weight=5e-3, eps=1e-3, axes="temporal"))])
+    s = CGSolver(y, ad, regm, CGConfig(max_iter=400, stop_window=10, stop_tol=1e-4))
+    bad = WarmStartCNN.pretrained(cuda)
+    bad.b32["c8"][:2] = 1e3            # a constant offset far from any image
+    info = warm_start(s, bad)
+    assert not info["used_network"] and info["f_network"] > info["f_adjoint"]
+    assert torch.equal(s.x, _ls_scaled(ad, y, ad.AH(y)))
+    s.run()
+    assert s.stop_reason.startswith("relative")
