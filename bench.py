@@ -63,6 +63,14 @@ from mrirecon_b200.workloads import (WORKLOADS, STOP_WINDOW, STOP_TOL, make_inpu
 ITERS_TO_TOL = {"grasp": 252, "radial128": None}
 
 
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of each
+# stage's kernels on the grasp workload, from one `ncu --set full` capture per
+# kernel of `python bench.py --nufft-only` (spread stage = spread_kernel +
+# zero_tiles_kernel; the small split-tile reduction is not included)
+NCU_TRAFFIC = {"grasp": {"pre": 396.30e6, "fft": 1228.03e6, "interp": 433.49e6, "spread": 816.50e6,
+                         "ifft": 1256.29e6, "post": 454.12e6}}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -544,7 +552,8 @@ def run_b200(args, w, ws, rank, local):
     if info.get("fft_mode", 0) != 1:
         kname.update(pre="pre_fft_kernel", post="post_ifft_kernel")
     roof = {"kernel": kname[dom], "stage": dom, "bound": "hbm", "achieved": gbs[dom], "peak": hbm, "unit": "GB/s",
-            "frac": gbs[dom] / hbm, "peak_source": peak_src, "traffic": None,
+            "frac": gbs[dom] / hbm, "peak_source": peak_src,
+            "traffic": NCU_TRAFFIC.get(args.workload, {}).get(dom) if info.get("fft_mode", 0) == 1 else None,
             "algorithmic_bytes_per_launch": ab[dom], "launch_ms": stages[dom]}
     line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
