@@ -189,7 +189,31 @@ struct TVPlan {
   float eps[NUNIT];
   int term_of[NUNIT];            // user term each unit belongs to
   unsigned diag_mask;            // bit (s*NSLOT+s2): some unit couples slots s and s2
+  // v / stride and q % size by multiply-shift (numerators < 2^31): magic, shift
+  unsigned st_m[NSLOT], sz_m[NSLOT];
+  int st_s[NSLOT], sz_s[NSLOT];
 };
+
+// q = v / d for v < 2^31 with m = ceil(2^(31+l) / d), l = ceil(log2 d), shift = l - 1
+// (m = 0 encodes d = 1): Granlund-Montgomery division by an invariant integer.
+__device__ __forceinline__ unsigned magic_div(unsigned v, unsigned m, int sh) {
+  return m ? (__umulhi(v, m) >> sh) : v;
+}
+
+// coordinate of voxel v along slot s: (v / stride) % size
+__device__ __forceinline__ int slot_coord(const TVPlan& P, int s, unsigned v) {
+  const unsigned q = magic_div(v, P.st_m[s], P.st_s[s]);
+  return (int)(q - magic_div(q, P.sz_m[s], P.sz_s[s]) * (unsigned)P.size[s]);
+}
+
+// sqrt(q + e^2) - e = q / (sqrt(q + e^2) + e), without cancellation for q << e^2;
+// *inv receives 1 / sqrt(q + e^2)
+__device__ __forceinline__ float huber_excess(float q, float e, float* inv) {
+  const float s2 = q + e * e;
+  const float r = rsqrtf(s2);
+  if (inv) *inv = r;
+  return __fdividef(q, fmaf(s2, r, e));
+}
 
 __device__ __forceinline__ float2 zload(const float2* __restrict__ x, const float2* __restrict__ d, float t,
                                         unsigned i) {
@@ -224,27 +248,33 @@ struct GradArgs {
   int skip_if_zero;
 };
 
+template <int NS, int NU>
 __global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P, double* __restrict__ partials) {
+  // dot products (which may cancel) accumulate in FP64 per thread; the TV
+  // energies (non-negative terms) in FP32 per thread; reductions in FP64
   double acc[GP_NV];
 #pragma unroll
   for (int j = 0; j < GP_NV; ++j) acc[j] = 0.0;
+  float eacc[MAX_TERMS];
+#pragma unroll
+  for (int j = 0; j < MAX_TERMS; ++j) eacc[j] = 0.f;
   bool sk = false;
   if (a.skip) sk = a.skip_if_zero ? (*a.skip == 0.0) : (*a.skip != 0.0);
   const float t = (float)(a.t_dev ? *a.t_dev : a.t_host);
   const unsigned stride_all = gridDim.x * blockDim.x;
   if (!sk) {
     for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < P.n; v += stride_all) {
-      int c[NSLOT];
-      bool hn[NSLOT], hp[NSLOT];
-      float2 zn[NSLOT], zp[NSLOT];
+      int c[NS];
+      bool hn[NS], hp[NS];
+      float2 zn[NS], zp[NS];
       const float2 zv = zload(a.x, a.d, t, v);
 #pragma unroll
-      for (int s = 0; s < NSLOT; ++s) {
+      for (int s = 0; s < NS; ++s) {
         c[s] = 0;
         hn[s] = hp[s] = false;
         zn[s] = zp[s] = make_float2(0.f, 0.f);
         if (s < P.ns) {
-          c[s] = (int)((v / P.stride[s]) % (unsigned)P.size[s]);
+          c[s] = slot_coord(P, s, v);
           hn[s] = c[s] + 1 < P.size[s];
           hp[s] = c[s] > 0;
           if (hn[s]) zn[s] = zload(a.x, a.d, t, v + P.stride[s]);
@@ -252,16 +282,16 @@ __global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P,
         }
       }
       // forward differences at v
-      float2 D[NSLOT];
+      float2 D[NS];
 #pragma unroll
-      for (int s = 0; s < NSLOT; ++s)
+      for (int s = 0; s < NS; ++s)
         D[s] = hn[s] ? make_float2(zn[s].x - zv.x, zn[s].y - zv.y) : make_float2(0.f, 0.f);
       // forward differences at v - e_s, along every slot s2: Dp[s][s2]
-      float2 Dp[NSLOT][NSLOT];
+      float2 Dp[NS][NS];
 #pragma unroll
-      for (int s = 0; s < NSLOT; ++s) {
+      for (int s = 0; s < NS; ++s) {
 #pragma unroll
-        for (int s2 = 0; s2 < NSLOT; ++s2) {
+        for (int s2 = 0; s2 < NS; ++s2) {
           Dp[s][s2] = make_float2(0.f, 0.f);
           if (!hp[s]) continue;
           if (s2 == s) {
@@ -278,25 +308,25 @@ __global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P,
       if (a.g_base) { float2 b = a.g_base[v]; gx = b.x; gy = b.y; }
       if (a.g_dir) { float2 b = a.g_dir[v]; gx = fmaf(t, b.x, gx); gy = fmaf(t, b.y, gy); }
 #pragma unroll
-      for (int u = 0; u < NUNIT; ++u) {
+      for (int u = 0; u < NU; ++u) {
         if (u >= P.nu) continue;
         const float e2 = P.eps[u] * P.eps[u];
         float ss = 0.f;
 #pragma unroll
-        for (int s = 0; s < NSLOT; ++s) {
+        for (int s = 0; s < NS; ++s) {
           const float w = P.w[u][s];
           float2 q = make_float2(w * D[s].x, w * D[s].y);
           ss += q.x * q.x + q.y * q.y;
         }
-        const float den = sqrtf(ss + e2);
-        const float inv = 1.f / fmaxf(den, 1e-12f);
+        float inv;
+        const float ex = huber_excess(ss, P.eps[u], &inv);
         const int ti = P.term_of[u];
 #pragma unroll
         for (int tt = 0; tt < MAX_TERMS; ++tt)
-          if (tt == ti) acc[tt] += (double)(P.lam[u] * (den - P.eps[u]));
+          if (tt == ti) eacc[tt] = fmaf(P.lam[u], ex, eacc[tt]);
         float dx = 0.f, dy = 0.f;
 #pragma unroll
-        for (int s = 0; s < NSLOT; ++s) {
+        for (int s = 0; s < NS; ++s) {
           const float w = P.w[u][s];
           if (w == 0.f) continue;
           dx += w * D[s].x * inv;
@@ -304,12 +334,12 @@ __global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P,
           if (hp[s]) {
             float ssp = 0.f;
 #pragma unroll
-            for (int s2 = 0; s2 < NSLOT; ++s2) {
+            for (int s2 = 0; s2 < NS; ++s2) {
               const float w2 = P.w[u][s2];
               float2 q = make_float2(w2 * Dp[s][s2].x, w2 * Dp[s][s2].y);
               ssp += q.x * q.x + q.y * q.y;
             }
-            const float invp = 1.f / fmaxf(sqrtf(ssp + e2), 1e-12f);
+            const float invp = rsqrtf(ssp + e2);
             dx -= w * Dp[s][s].x * invp;
             dy -= w * Dp[s][s].y * invp;
           }
@@ -333,6 +363,8 @@ __global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P,
       }
     }
   }
+#pragma unroll
+  for (int j = 0; j < MAX_TERMS; ++j) acc[j] = (double)eacc[j];
   block_reduce_store<GP_NV>(acc, partials);
 }
 
@@ -343,41 +375,41 @@ __global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P,
 // trial step costs two FMAs and a square root per unit.
 constexpr int MT_MAX_J = 24;
 
+template <int NS, int NU>
 __global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __restrict__ x,
                                                                const float2* __restrict__ d,
                                                                const double* __restrict__ ts, int J, TVPlan P,
                                                                const double* skip, double* __restrict__ partials) {
-  double acc[MT_MAX_J];
+  // energies are sums of non-negative terms: a thread sums its ~n / (blocks x threads)
+  // voxels in FP32, the block and grid reductions run in FP64
+  float facc[MT_MAX_J];
 #pragma unroll
-  for (int j = 0; j < MT_MAX_J; ++j) acc[j] = 0.0;
+  for (int j = 0; j < MT_MAX_J; ++j) facc[j] = 0.f;
   const bool sk = skipped(skip) != 0.0;
-  float tf[MT_MAX_J];
-#pragma unroll
-  for (int j = 0; j < MT_MAX_J; ++j) tf[j] = j < J ? (float)ts[j] : 0.f;
+  __shared__ float tf[MT_MAX_J];   // trial steps, broadcast from shared memory
+  if (threadIdx.x < MT_MAX_J) tf[threadIdx.x] = threadIdx.x < J ? (float)ts[threadIdx.x] : 0.f;
+  __syncthreads();
   const unsigned stride_all = gridDim.x * blockDim.x;
   if (!sk) {
     for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < P.n; v += stride_all) {
       const float2 xv = x[v], dv = d[v];
-      float2 A[NSLOT], B[NSLOT];
+      float2 A[NS], B[NS];
 #pragma unroll
-      for (int s = 0; s < NSLOT; ++s) {
+      for (int s = 0; s < NS; ++s) {
         A[s] = B[s] = make_float2(0.f, 0.f);
-        if (s < P.ns) {
-          int c = (int)((v / P.stride[s]) % (unsigned)P.size[s]);
-          if (c + 1 < P.size[s]) {
-            float2 xn = x[v + P.stride[s]], dn = d[v + P.stride[s]];
-            A[s] = make_float2(xn.x - xv.x, xn.y - xv.y);
-            B[s] = make_float2(dn.x - dv.x, dn.y - dv.y);
-          }
+        if (s < P.ns && slot_coord(P, s, v) + 1 < P.size[s]) {
+          const float2 xn = x[v + P.stride[s]], dn = d[v + P.stride[s]];
+          A[s] = make_float2(xn.x - xv.x, xn.y - xv.y);
+          B[s] = make_float2(dn.x - dv.x, dn.y - dv.y);
         }
       }
-      float al[NUNIT], be2[NUNIT], ga[NUNIT];
+      float al[NU], be2[NU], ga[NU];
 #pragma unroll
-      for (int u = 0; u < NUNIT; ++u) {
+      for (int u = 0; u < NU; ++u) {
         al[u] = be2[u] = ga[u] = 0.f;
         if (u >= P.nu) continue;
 #pragma unroll
-        for (int s = 0; s < NSLOT; ++s) {
+        for (int s = 0; s < NS; ++s) {
           const float w2 = P.w[u][s] * P.w[u][s];
           al[u] = fmaf(w2, A[s].x * A[s].x + A[s].y * A[s].y, al[u]);
           be2[u] = fmaf(2.f * w2, A[s].x * B[s].x + A[s].y * B[s].y, be2[u]);
@@ -390,15 +422,18 @@ __global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __r
         const float t = tf[j];
         float e = 0.f;
 #pragma unroll
-        for (int u = 0; u < NUNIT; ++u) {
+        for (int u = 0; u < NU; ++u) {
           if (u >= P.nu) continue;
-          const float ss = fmaxf(fmaf(t, fmaf(t, ga[u], be2[u]), al[u]), 0.f);
-          e = fmaf(P.lam[u], sqrtf(ss + P.eps[u] * P.eps[u]) - P.eps[u], e);
+          const float q = fmaxf(fmaf(t, fmaf(t, ga[u], be2[u]), al[u]), 0.f);
+          e = fmaf(P.lam[u], huber_excess(q, P.eps[u], nullptr), e);
         }
-        acc[j] += (double)e;
+        facc[j] += e;
       }
     }
   }
+  double acc[MT_MAX_J];
+#pragma unroll
+  for (int j = 0; j < MT_MAX_J; ++j) acc[j] = (double)facc[j];
   block_reduce_store<MT_MAX_J>(acc, partials);
 }
 
@@ -682,6 +717,33 @@ __global__ void set_steps_kernel(double* ts, int J, double beta) {
   }
 }
 
+// Kernel instance for the plan's slot / unit counts (rounded up), so the
+// unrolled per-voxel loops keep only the accumulators in use.
+struct GradLaunch {
+  template <int NS, int NU, class... A>
+  static void go(int nb, cudaStream_t st, A... args) { grad_kernel<NS, NU><<<nb, RED_THREADS, 0, st>>>(args...); }
+};
+struct MultiLaunch {
+  template <int NS, int NU, class... A>
+  static void go(int nb, cudaStream_t st, A... args) { tv_multi_kernel<NS, NU><<<nb, RED_THREADS, 0, st>>>(args...); }
+};
+
+template <class L, int NS, class... A>
+void launch_tv_nu(const TVPlan& P, int nb, cudaStream_t st, A... args) {
+  if (P.nu <= 1) L::template go<NS, 1>(nb, st, args...);
+  else if (P.nu <= 2) L::template go<NS, 2>(nb, st, args...);
+  else if (P.nu <= 4) L::template go<NS, 4>(nb, st, args...);
+  else L::template go<NS, NUNIT>(nb, st, args...);
+}
+
+template <class L, class... A>
+void launch_tv(const TVPlan& P, int nb, cudaStream_t st, A... args) {
+  if (P.ns <= 1) launch_tv_nu<L, 1>(P, nb, st, args...);
+  else if (P.ns <= 2) launch_tv_nu<L, 2>(P, nb, st, args...);
+  else if (P.ns <= 3) launch_tv_nu<L, 3>(P, nb, st, args...);
+  else launch_tv_nu<L, NSLOT>(P, nb, st, args...);
+}
+
 int build_plan(TVPlan& P, int nd, const int* S, int F, const mrb_tv_term* terms, int nterms) {
   MRB_REQUIRE(nd >= 1 && nd <= 3, "spatial nd must be 1..3");
   MRB_REQUIRE(F >= 1, "frames must be positive");
@@ -757,6 +819,22 @@ int build_plan(TVPlan& P, int nd, const int* S, int F, const mrb_tv_term* terms,
       }
     }
     ++k;
+  }
+  auto magic = [](unsigned dv, unsigned* m, int* sh) {
+    if (dv <= 1) {
+      *m = 0;
+      *sh = 0;
+      return;
+    }
+    int l = 0;
+    while ((1ull << l) < dv) ++l;                                  // ceil(log2 dv)
+    const unsigned long long p2 = 1ull << (31 + l);
+    *m = (unsigned)((p2 + dv - 1) / dv);
+    *sh = l - 1;
+  };
+  for (int q = 0; q < P.ns; ++q) {
+    magic(P.stride[q], &P.st_m[q], &P.st_s[q]);
+    magic((unsigned)P.size[q], &P.sz_m[q], &P.sz_s[q]);
   }
   return 0;
 }
@@ -850,7 +928,7 @@ extern "C" int mrb_tv_grad(int nd, const int* S, int F, const mrb_tv_term* terms
   cudaStream_t st = (cudaStream_t)stream;
   int nb = red_blocks(P.n, 2);
   double* part = (double*)ws;
-  grad_kernel<<<nb, RED_THREADS, 0, st>>>(a, P, part);
+  launch_tv<GradLaunch>(P, nb, st, a, P, part);
   MRB_LAUNCH_CHECK();
   return finalize(part, nb, GP_NV, GP_NV, out, 0, nullptr, st);
 }
@@ -866,7 +944,7 @@ extern "C" int mrb_tv_multi(int nd, const int* S, int F, const mrb_tv_term* term
   cudaStream_t st = (cudaStream_t)stream;
   int nb = red_blocks(P.n, 2);
   double* part = (double*)ws;
-  tv_multi_kernel<<<nb, RED_THREADS, 0, st>>>((const float2*)x, (const float2*)d, ts, J, P, skip, part);
+  launch_tv<MultiLaunch>(P, nb, st, (const float2*)x, (const float2*)d, ts, J, P, skip, part);
   MRB_LAUNCH_CHECK();
   return finalize(part, nb, MT_MAX_J, J, out, 0, skip, st);
 }
