@@ -536,12 +536,15 @@ constexpr int SPREAD_BATCH = 32;
 
 template <int ND, int T>
 struct SpreadSmem {
-  static constexpr int RS = ND == 2 ? T + 4 : T;                  // padded last-dim stride
-  static constexpr int CELLS = ND == 2 ? T * RS : T * T * T;      // per coil
+  static constexpr int CELLS = ND == 2 ? T * T : T * T * T;
   static constexpr int NW = 4 * ND;                               // staged weights per sample
+  static constexpr int NTAP = ND == 2 ? 16 : 64;
+  // the shared tile is coil-interleaved, [cell][coil] with an even coil stride, so
+  // one lane updates a pair of coils with one 128-bit read-modify-write
+  __host__ __device__ static int cstride(int cpi) { return (cpi + 1) & ~1; }
   __host__ __device__ static size_t warp_bytes(int cpi) {
-    return (size_t)cpi * CELLS * sizeof(float2) + SPREAD_BATCH * (sizeof(int4) + NW * sizeof(float)) +
-           (size_t)SPREAD_BATCH * cpi * sizeof(float2);
+    return (size_t)cstride(cpi) * CELLS * sizeof(float2) + SPREAD_BATCH * (sizeof(int4) + NW * sizeof(float)) +
+           (size_t)SPREAD_BATCH * cstride(cpi) * sizeof(float2);
   }
 };
 
@@ -549,9 +552,9 @@ template <int ND, int T>
 __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
   if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   using SM = SpreadSmem<ND, T>;
-  constexpr int RS = SM::RS;
   constexpr int CELLS = SM::CELLS;
   constexpr int NW = SM::NW;
+  constexpr int NTAP = SM::NTAP;
   extern __shared__ float4 smem4[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   long long item = (long long)blockIdx.x * SPREAD_WARPS + warp;
@@ -623,21 +626,24 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
     return;
   }
 
+  const int cps = SM::cstride(a.cpi);   // coils per shared cell (even)
+  const int npair = cps >> 1;
   char* wbase = reinterpret_cast<char*>(smem4) + (size_t)warp * SM::warp_bytes(a.cpi);
   float2* acc = reinterpret_cast<float2*>(wbase);
-  int4* sb = reinterpret_cast<int4*>(wbase + (size_t)a.cpi * CELLS * sizeof(float2));
+  int4* sb = reinterpret_cast<int4*>(wbase + (size_t)cps * CELLS * sizeof(float2));
   float* sw = reinterpret_cast<float*>(sb + SPREAD_BATCH);
   float2* sy = reinterpret_cast<float2*>(sw + SPREAD_BATCH * NW);
 
   {
     float4* acc4 = reinterpret_cast<float4*>(acc);
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = lane; i < nc * CELLS / 2; i += 32) acc4[i] = z4;
+    for (int i = lane; i < cps * CELLS / 2; i += 32) acc4[i] = z4;
   }
   __syncwarp();
 
   const float* gxp = a.gx + (long long)b * ND * g.K;
   const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
+  const int ntask = NTAP * npair;
   for (int e = e0; e < e1; e += SPREAD_BATCH) {
     const int nbat = min(SPREAD_BATCH, e1 - e);
     if (lane < nbat) {
@@ -659,35 +665,32 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
         }
       }
       sb[lane] = make_int4(base[0], base[1], base[2], 0);
-      for (int cl = 0; cl < nc; ++cl) sy[lane * a.cpi + cl] = yb[(long long)cl * g.K + k];
+      for (int cl = 0; cl < cps; ++cl)
+        sy[lane * cps + cl] = cl < nc ? yb[(long long)cl * g.K + k] : make_float2(0.f, 0.f);
     }
     __syncwarp();
     for (int j = 0; j < nbat; ++j) {
       const int4 bb = sb[j];
-      if (ND == 2) {
-        const int tap = lane & 15, csub = lane >> 4;
-        const int ox = tap >> 2, oy = tap & 3;
-        int n0 = bb.x + ox, n1 = bb.y + oy;
-        n0 += n0 < 0 ? g.G[0] : 0;
-        n0 -= n0 >= g.G[0] ? g.G[0] : 0;
-        n1 += n1 < 0 ? g.G[1] : 0;
-        n1 -= n1 >= g.G[1] ? g.G[1] : 0;
-        const int lx = n0 - o[0], ly = n1 - o[1];
-        if ((unsigned)lx < (unsigned)T && (unsigned)ly < (unsigned)T) {
-          const float w = sw[j * NW + ox] * sw[j * NW + 4 + oy];
-          for (int cl = csub; cl < nc; cl += 2) {
-            const float2 v = sy[j * a.cpi + cl];
-            float2* p = acc + ((long long)cl * T + lx) * RS + ly;
-            float2 t = *p;
-            t.x = fmaf(w, v.x, t.x);
-            t.y = fmaf(w, v.y, t.y);
-            *p = t;
-          }
-        }
-      } else {
-#pragma unroll
-        for (int pass = 0; pass < 2; ++pass) {
-          const int tap = lane + 32 * pass;
+      const float* wj = sw + j * NW;
+      const float4* yj = reinterpret_cast<const float4*>(sy + j * cps);
+      // lane tasks: (tap, coil pair), every task of a sample touches a distinct float4
+      for (int tk = lane; tk < ntask; tk += 32) {
+        const int tap = tk & (NTAP - 1), pr = tk / NTAP;
+        int cell;
+        float w;
+        bool inside;
+        if (ND == 2) {
+          const int ox = tap >> 2, oy = tap & 3;
+          int n0 = bb.x + ox, n1 = bb.y + oy;
+          n0 += n0 < 0 ? g.G[0] : 0;
+          n0 -= n0 >= g.G[0] ? g.G[0] : 0;
+          n1 += n1 < 0 ? g.G[1] : 0;
+          n1 -= n1 >= g.G[1] ? g.G[1] : 0;
+          const int lx = n0 - o[0], ly = n1 - o[1];
+          inside = (unsigned)lx < (unsigned)T && (unsigned)ly < (unsigned)T;
+          cell = lx * T + ly;
+          w = inside ? wj[ox] * wj[4 + oy] : 0.f;
+        } else {
           const int a0 = tap >> 4, a1 = (tap >> 2) & 3, a2 = tap & 3;
           int n0 = bb.x + a0, n1 = bb.y + a1, n2 = bb.z + a2;
           n0 += n0 < 0 ? g.G[0] : 0;
@@ -697,38 +700,48 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
           n2 += n2 < 0 ? g.G[2] : 0;
           n2 -= n2 >= g.G[2] ? g.G[2] : 0;
           const int l0 = n0 - o[0], l1 = n1 - o[1], l2 = n2 - o[2];
-          if ((unsigned)l0 < (unsigned)T && (unsigned)l1 < (unsigned)T && (unsigned)l2 < (unsigned)T) {
-            const float w = sw[j * NW + a0] * sw[j * NW + 4 + a1] * sw[j * NW + 8 + a2];
-            const int cell = (l0 * T + l1) * T + l2;
-            for (int cl = 0; cl < nc; ++cl) {
-              const float2 v = sy[j * a.cpi + cl];
-              float2* p = acc + (long long)cl * CELLS + cell;
-              float2 t = *p;
-              t.x = fmaf(w, v.x, t.x);
-              t.y = fmaf(w, v.y, t.y);
-              *p = t;
-            }
-          }
+          inside = (unsigned)l0 < (unsigned)T && (unsigned)l1 < (unsigned)T && (unsigned)l2 < (unsigned)T;
+          cell = (l0 * T + l1) * T + l2;
+          w = inside ? wj[a0] * wj[4 + a1] * wj[8 + a2] : 0.f;
+        }
+        if (inside) {
+          const float4 v = yj[pr];
+          float4* p = reinterpret_cast<float4*>(acc + cell * cps) + pr;
+          float4 t = *p;
+          t.x = fmaf(w, v.x, t.x);
+          t.y = fmaf(w, v.y, t.y);
+          t.z = fmaf(w, v.z, t.z);
+          t.w = fmaf(w, v.w, t.w);
+          *p = t;
         }
       }
       __syncwarp();
     }
   }
-  // write the whole tile once (or this chunk's partial tile)
-  for (int i = lane; i < nc * PAIRS; i += 32) {
-    int cl = i / PAIRS, r = i - cl * PAIRS;
-    int l = (r % (T / 2)) * 2;
-    int rr = r / (T / 2);
-    const float2* src = ND == 2 ? acc + ((long long)cl * T + rr) * RS + l : acc + (long long)cl * CELLS + rr * T + l;
-    const float4 v = *reinterpret_cast<const float4*>(src);
-    if (pout) {
-      *reinterpret_cast<float4*>(pout + (long long)cl * TN + rr * T + l) = v;
-      continue;
-    }
+  // write the whole tile once (or this chunk's partial tile): lane task = (cell
+  // pair along the last dim, coil pair); two 128-bit shared loads, one 128-bit
+  // global store per coil
+  for (int i = lane; i < PAIRS * npair; i += 32) {
+    const int pr = i % npair, r = i / npair;
+    const int l = (r % (T / 2)) * 2;
+    const int rr = r / (T / 2);
+    const int cl0 = rr * T + l;
+    const float4 a0 = reinterpret_cast<const float4*>(acc + cl0 * cps)[pr];
+    const float4 a1 = reinterpret_cast<const float4*>(acc + (cl0 + 1) * cps)[pr];
     int n[3];
-    long long cell = cell_of_pair(r, n);
-    if (!in_grid(n)) continue;
-    *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = v;
+    const long long cell = cell_of_pair(r, n);
+    const bool ok = in_grid(n);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int cl = 2 * pr + h;
+      if (cl >= nc) continue;
+      const float4 v = h == 0 ? make_float4(a0.x, a0.y, a1.x, a1.y) : make_float4(a0.z, a0.w, a1.z, a1.w);
+      if (pout) {
+        *reinterpret_cast<float4*>(pout + (long long)cl * TN + rr * T + l) = v;
+      } else if (ok) {
+        *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = v;
+      }
+    }
   }
 }
 
