@@ -257,7 +257,7 @@ int mrb_ncg_restart(int64_t n, void* d, const void* g, const float* diag, int64_
 /* ------------------------------------------------------------------------
  * Learned warm start (no counterpart in the reference).  Activations are
  * channels-last BF16 volumes (Nb, D, H, W, channels) with a channel stride
- * and a channel offset (concatenation is a channel offset); `vol` is a DEVICE
+ * and a channel offset (concatenation is a channel offset); `vol` is a host
  * int[4] {Nb, D, H, W}.  Weights are BF16 [27][cin][coutp], tap = kd*9+kh*3+kw
  * over (t, y, x); coutp and channel counts are multiples of 32.
  * ---------------------------------------------------------------------- */
@@ -297,6 +297,21 @@ int mrb_cnn_mse(const void* zin, const void* target, const float* net, int cy, c
 int mrb_cnn_adam(float* w, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2,
                  float eps, int step, void* wb, mrb_stream_t stream);
 int mrb_cnn_to_bf16(const float* a, int64_t n, void* b, mrb_stream_t stream);
+/* The same 3x3x3 convolution on the 5th-generation tensor cores: tcgen05.mma
+ * with the FP32 accumulator in tensor memory, operands staged by TMA (the 27
+ * taps are coordinate offsets of one 5-D tensor map; out-of-volume reads are
+ * the zero padding).  Weights K-major, wk [27][N][cin]; flip != 0 reads tap
+ * 26 - t (data gradient with the forward weights [27][cin][cout] read as
+ * [27][N = cin][K = cout]).  Needs cin % 32 == 0, N % 16 == 0, N <= 256, and a
+ * 128-voxel (H, W) patch: W % 128 == 0, or W dividing 128 with H a multiple of
+ * 128 / W (mrb_cnn_tc_supported).  Dims are host values. */
+int mrb_cnn_tc_supported(int cin, int ci_off, int cx, int N, int W, int H);
+int mrb_cnn_conv3d_tc(const void* x, int cx, int ci_off, int cin, const void* wk, int flip, int N, int cout,
+                      const float* bias, int relu, void* yb, int cyb, int yb_off, float* yf, int cyf, int yf_off,
+                      int yf_acc, int Nb, int D, int H, int W, mrb_stream_t stream);
+/* Reads and clears the timeout flag of the tensor-core convolution
+ * (synchronous; 0 = every barrier wait completed). */
+int mrb_cnn_tc_error(int* out);
 
 #ifdef __cplusplus
 }

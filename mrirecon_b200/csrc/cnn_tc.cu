@@ -1,0 +1,384 @@
+// Warm-start network convolution on the 5th-generation tensor cores (sm_100a):
+// tcgen05.mma with the accumulator in tensor memory, operands staged in shared
+// memory by TMA.
+//
+// 3x3x3 convolution (stride 1, zero padding 1) on channels-last BF16 volumes
+// (Nb, D, H, W, C) as an implicit GEMM: M = 128 output voxels per CTA (a
+// BH x BW patch of one (n, d) plane), N = output channels (16 .. 256), K = 27
+// taps x input channels in chunks of 32.  For tap (dz, dy, dx) the A tile is the
+// input patch shifted by the tap: one 5-D TMA box {32 channels, BW, BH, 1, 1} at
+// coordinates (c, w0 + dx, h0 + dy, d + dz, n); coordinates outside the volume
+// read as zero, which is the zero padding.  B is the weight slice [tap][N][32]
+// (K-major).  Both land in 64-byte-swizzled shared tiles that the MMA reads
+// through shared-memory descriptors.  A 4-stage ring: one thread issues TMA
+// loads (mbarrier transaction counts), one thread issues the MMAs (K = 16 per
+// instruction, FP32 accumulation in TMEM) and commits each stage back to the
+// producer; the epilogue reads TMEM with tcgen05.ld (warp w owns lanes
+// 32w .. 32w+31 = voxels), adds the bias, applies ReLU and stores BF16 and/or
+// FP32 (optionally accumulating).  Every mbarrier wait is bounded: on timeout
+// the kernel records an error flag, skips the remaining work, releases its
+// TMEM and returns.
+// No reference counterpart: the reference has no learned component.
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "mrb_common.cuh"
+
+namespace {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int TC_BM = 128;      // voxels per CTA (UMMA M)
+constexpr int TC_BK = 32;       // K per stage (channels): one 64-byte swizzle row
+constexpr int TC_STAGES = 4;
+constexpr int TC_THREADS = 128;
+constexpr long long TC_WAIT_LIMIT = 1LL << 22;   // polls of a barrier phase before giving up
+
+__device__ int g_tc_error = 0;   // set when a barrier wait times out
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait for the phase with the given parity; false on timeout or when
+// another thread of the CTA already gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  for (long long i = 0; i < TC_WAIT_LIMIT; ++i) {
+    if (mbar_test(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if ((i & 1023) == 1023 && *(volatile int*)&g_tc_error) {   // another CTA gave up: stop too
+      *abort_flag = 1;
+      return false;
+    }
+    if (i > 64) __nanosleep(64);
+  }
+  *abort_flag = 1;
+  atomicExch(&g_tc_error, 1);
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2,
+                                            int c3, int c4) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6, "
+      "%7}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
+                                            int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+      "[%2];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major tile of rows of 64 bytes, 64-byte
+// swizzle, 8-row groups 512 bytes apart (start and offsets in 16-byte units;
+// descriptor version 1; layout code 4 = 64-byte swizzle).
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(512 >> 4) << 32;        // stride byte offset: 8 rows x 64 B
+  d |= (uint64_t)1 << 46;                 // version
+  d |= (uint64_t)4 << 61;                 // 64-byte swizzle
+  return d;
+}
+
+// Instruction descriptor, kind::f16: D FP32, A and B BF16, both K-major, N, M.
+__host__ __device__ constexpr uint32_t f16_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+struct TcArgs {
+  int cin;           // K channels (multiple of 32), read at channel offset ci_off
+  int ci_off;
+  int N;             // output channels computed (multiple of 16, <= 256)
+  int cout;          // output channels written
+  int flip;          // weight tap = 26 - tap (data gradient)
+  const float* bias;
+  int relu;
+  bf16* yb;
+  int cyb, yb_off;
+  float* yf;
+  int cyf, yf_off, yf_acc;
+  int Nb, D, H, W;
+  int BW, BH;        // voxel patch of one CTA (BW * BH = 128)
+  int ncols;         // TMEM columns allocated (power of two >= 32, >= N)
+};
+
+__global__ void __launch_bounds__(TC_THREADS) conv3d_tc_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                               const __grid_constant__ CUtensorMap wmap, TcArgs a) {
+  extern __shared__ __align__(1024) uint8_t dsm[];
+  __shared__ __align__(8) uint64_t full_bar[TC_STAGES], empty_bar[TC_STAGES], done_bar;
+  __shared__ uint32_t tmem_base;
+  __shared__ volatile int abort_flag;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // stage buffers, 1024-byte aligned (swizzle atoms)
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(dsm) + 1023) & ~uintptr_t(1023));
+  const uint32_t a_bytes = TC_BM * TC_BK * 2;             // 8 KB
+  const uint32_t b_bytes = (uint32_t)a.N * TC_BK * 2;      // N x 64 B
+  const uint32_t stage_bytes = (a_bytes + b_bytes + 1023) & ~1023u;
+
+  // tile -> (n, d, h0, w0)
+  const int tw = a.W / a.BW, th = a.H / a.BH;
+  long long t = blockIdx.x;
+  const int w0 = (int)(t % tw) * a.BW;
+  t /= tw;
+  const int h0 = (int)(t % th) * a.BH;
+  t /= th;
+  const int dd = (int)(t % a.D);
+  const int nn = (int)(t / a.D);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TC_STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    mbar_init(&done_bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(a.ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem_d = tmem_base;
+
+  const int kch = a.cin / TC_BK;
+  const int nk = 27 * kch;
+
+  if (warp == 0 && lane == 0) {
+    // producer: TMA loads of A (shifted input patch) and B (weight slice)
+    for (int ks = 0; ks < nk; ++ks) {
+      const int s = ks % TC_STAGES;
+      if (ks >= TC_STAGES && !mbar_wait(&empty_bar[s], ((ks / TC_STAGES) - 1) & 1, &abort_flag)) break;
+      const int tap = ks / kch, kc = ks - tap * kch;
+      const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+      const int wtap = a.flip ? 26 - tap : tap;
+      uint8_t* sa = base + (size_t)s * stage_bytes;
+      uint8_t* sb = sa + a_bytes;
+      mbar_expect_tx(&full_bar[s], a_bytes + b_bytes);
+      tma_load_5d(sa, &xmap, &full_bar[s], a.ci_off + kc * TC_BK, w0 + dx, h0 + dy, dd + dz, nn);
+      tma_load_3d(sb, &wmap, &full_bar[s], kc * TC_BK, 0, wtap);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer
+    const uint32_t idesc = f16_idesc(TC_BM, a.N);
+    for (int ks = 0; ks < nk; ++ks) {
+      const int s = ks % TC_STAGES;
+      if (!mbar_wait(&full_bar[s], (ks / TC_STAGES) & 1, &abort_flag)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t sa = smem_u32(base + (size_t)s * stage_bytes);
+      const uint32_t sb = sa + a_bytes;
+#pragma unroll
+      for (int kk = 0; kk < TC_BK / 16; ++kk) {
+        const uint64_t adesc = sw64_desc(sa + kk * 32);
+        const uint64_t bdesc = sw64_desc(sb + kk * 32);
+        const uint32_t accum = (ks > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&empty_bar[s]))
+                   : "memory");
+    }
+    // arrives once every MMA issued above has completed (also after an abort)
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(&done_bar))
+                 : "memory");
+  }
+  __syncwarp();
+
+  // epilogue: wait for the accumulator, TMEM -> registers -> global
+  bool have = mbar_wait(&done_bar, 0, &abort_flag) && !abort_flag;
+  have = __all_sync(0xffffffffu, have);   // tcgen05.ld is warp-collective
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (have) {
+    const int row = warp * 32 + lane;   // TMEM lane = voxel of the patch
+    const int hl = row / a.BW, wl = row - hl * a.BW;
+    const long long vox = (((long long)nn * a.D + dd) * a.H + (h0 + hl)) * a.W + (w0 + wl);
+    for (int c0 = 0; c0 < a.N; c0 += 16) {
+      uint32_t r[16];
+      const uint32_t taddr = tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+          "%15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (c0 >= a.cout) continue;
+      float v[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        float x = __uint_as_float(r[j]);
+        if (a.bias) x += __ldg(a.bias + c0 + j);
+        if (a.relu) x = fmaxf(x, 0.f);
+        v[j] = x;
+      }
+      const int nw = min(16, a.cout - c0);
+      if (a.yb) {
+        bf16* p = a.yb + vox * a.cyb + a.yb_off + c0;
+        if (nw == 16) {
+          uint32_t pk[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            __nv_bfloat162 h2 = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+            pk[j] = *reinterpret_cast<uint32_t*>(&h2);
+          }
+          reinterpret_cast<uint4*>(p)[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          reinterpret_cast<uint4*>(p)[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        } else {
+          for (int j = 0; j < nw; ++j) p[j] = __float2bfloat16_rn(v[j]);
+        }
+      }
+      if (a.yf) {
+        float* p = a.yf + vox * a.cyf + a.yf_off + c0;
+        for (int j = 0; j < nw; ++j) p[j] = a.yf_acc ? p[j] + v[j] : v[j];
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(a.ncols) : "memory");
+  }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" int mrb_cnn_tc_supported(int cin, int ci_off, int cx, int N, int W, int H) {
+  if (cin <= 0 || cin % TC_BK != 0 || ci_off % 8 != 0 || cx % 8 != 0) return 0;
+  if (N < 16 || N > 256 || N % 16 != 0) return 0;
+  const int BW = W >= TC_BM ? TC_BM : W;
+  if (BW <= 0 || TC_BM % BW != 0 || W % BW != 0) return 0;
+  const int BH = TC_BM / BW;
+  if (H % BH != 0 || BH > 256) return 0;
+  return 1;
+}
+
+extern "C" int mrb_cnn_conv3d_tc(const void* x, int cx, int ci_off, int cin, const void* wk, int flip, int N, int cout,
+                                 const float* bias, int relu, void* yb, int cyb, int yb_off, float* yf, int cyf,
+                                 int yf_off, int yf_acc, int Nb, int D, int H, int W, mrb_stream_t stream) {
+  MRB_REQUIRE(x && wk && (yb || yf), "null pointer");
+  MRB_REQUIRE(Nb >= 1 && D >= 1 && H >= 1 && W >= 1, "bad volume");
+  MRB_REQUIRE(mrb_cnn_tc_supported(cin, ci_off, cx, N, W, H), "shape not supported by the tensor-core conv");
+  MRB_REQUIRE(cout <= N, "cout > N");
+  MRB_REQUIRE(ci_off + cin <= cx, "channel range outside the input");
+  MRB_REQUIRE(((uintptr_t)x & 15) == 0 && ((uintptr_t)wk & 15) == 0, "operands must be 16-byte aligned");
+  MRB_REQUIRE(!yb || (cyb % 8 == 0 && yb_off % 8 == 0 && ((uintptr_t)yb & 15) == 0), "BF16 output misaligned");
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return mrb::fail(MRB_ECUDA, "cuTensorMapEncodeTiled unavailable");
+  TcArgs a{};
+  a.cin = cin;
+  a.ci_off = ci_off;
+  a.N = N;
+  a.cout = cout;
+  a.flip = flip;
+  a.bias = bias;
+  a.relu = relu;
+  a.yb = (bf16*)yb;
+  a.cyb = cyb;
+  a.yb_off = yb_off;
+  a.yf = yf;
+  a.cyf = cyf;
+  a.yf_off = yf_off;
+  a.yf_acc = yf_acc;
+  a.Nb = Nb;
+  a.D = D;
+  a.H = H;
+  a.W = W;
+  a.BW = W >= TC_BM ? TC_BM : W;
+  a.BH = TC_BM / a.BW;
+  a.ncols = 32;
+  while (a.ncols < N) a.ncols <<= 1;
+  // activations: (Nb, D, H, W, cx) bf16, box {32, BW, BH, 1, 1}
+  CUtensorMap xmap, wmap;
+  cuuint64_t xd[5] = {(cuuint64_t)cx, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D, (cuuint64_t)Nb};
+  cuuint64_t xs[4] = {(cuuint64_t)cx * 2, (cuuint64_t)cx * 2 * W, (cuuint64_t)cx * 2 * W * H,
+                      (cuuint64_t)cx * 2 * W * H * D};
+  cuuint32_t xb[5] = {(cuuint32_t)TC_BK, (cuuint32_t)a.BW, (cuuint32_t)a.BH, 1, 1};
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  CUresult r = enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(x), xd, xs, xb, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return mrb::fail(MRB_ECUDA, "activation tensor map failed (%d)", (int)r);
+  // weights: [27][N][cin] bf16 (K-major), box {32, N, 1}
+  cuuint64_t wd[3] = {(cuuint64_t)cin, (cuuint64_t)N, 27};
+  cuuint64_t ws[2] = {(cuuint64_t)cin * 2, (cuuint64_t)cin * 2 * N};
+  cuuint32_t wb[3] = {(cuuint32_t)TC_BK, (cuuint32_t)N, 1};
+  r = enc(&wmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(wk), wd, ws, wb, es,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return mrb::fail(MRB_ECUDA, "weight tensor map failed (%d)", (int)r);
+  const size_t stage = ((size_t)TC_BM * TC_BK * 2 + (size_t)N * TC_BK * 2 + 1023) & ~(size_t)1023;
+  const size_t smem = TC_STAGES * stage + 1024;
+  MRB_CUDA_TRY(cudaFuncSetAttribute(conv3d_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long tiles = (long long)Nb * D * (H / a.BH) * (W / a.BW);
+  MRB_REQUIRE(tiles < (1LL << 31), "volume too large");
+  conv3d_tc_kernel<<<(unsigned)tiles, TC_THREADS, smem, (cudaStream_t)stream>>>(xmap, wmap, a);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+// Reads and clears the timeout flag of the tensor-core conv (synchronous).
+extern "C" int mrb_cnn_tc_error(int* out) {
+  MRB_REQUIRE(out != nullptr, "null pointer");
+  int zero = 0;
+  MRB_CUDA_TRY(cudaMemcpyFromSymbol(out, g_tc_error, sizeof(int)));
+  MRB_CUDA_TRY(cudaMemcpyToSymbol(g_tc_error, &zero, sizeof(int)));
+  return 0;
+}

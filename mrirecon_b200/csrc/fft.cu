@@ -205,18 +205,28 @@ struct Dft<5, DIR> {
 // i + r T and writes element (i - k) R + k + r P, k = i mod P.  QFAST maps
 // consecutive threads to consecutive rows q (column kernels).
 // ---------------------------------------------------------------------------
-template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, class LD, class ST>
+// WARP: the transform belongs to one warp (NT = 32, ROWS = 1) and the exchanges
+// synchronise the warp only.
+template <bool WARP>
+__device__ __forceinline__ void stage_sync() {
+  if (WARP) __syncwarp();
+  else __syncthreads();
+}
+
+template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool WARP, class LD, class ST>
 __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load, ST store) {
   constexpr int R = radix_at(G, S);
   constexpr int P = span_at(G, S);
   constexpr int T = G / R;
   constexpr int TOTAL = ROWS * T;
   constexpr int NI = (TOTAL + NT - 1) / NT;
+  static_assert(!WARP || (NT == 32 && ROWS == 1), "warp transforms are one row of 32 lanes");
+  const int tid = WARP ? (int)(threadIdx.x & 31) : (int)threadIdx.x;
   const float2* tws = tw + tw_offset(G, S);
   float2 v[NI][R];
 #pragma unroll
   for (int c = 0; c < NI; ++c) {
-    const int w = threadIdx.x + c * NT;
+    const int w = tid + c * NT;
     if (TOTAL % NT == 0 || w < TOTAL) {
       const int q = QFAST ? w % ROWS : w / T;
       const int i = QFAST ? w / ROWS : w % T;
@@ -224,10 +234,10 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load
       for (int r = 0; r < R; ++r) v[c][r] = load(q, i + r * T);
     }
   }
-  __syncthreads();
+  stage_sync<WARP>();
 #pragma unroll
   for (int c = 0; c < NI; ++c) {
-    const int w = threadIdx.x + c * NT;
+    const int w = tid + c * NT;
     if (TOTAL % NT == 0 || w < TOTAL) {
       const int q = QFAST ? w % ROWS : w / T;
       const int i = QFAST ? w / ROWS : w % T;
@@ -246,23 +256,24 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load
       for (int r = 0; r < R; ++r) store(q, j + r * P, v[c][r]);
     }
   }
-  __syncthreads();
+  stage_sync<WARP>();
 }
 
 // All stages of a length-G transform of ROWS rows: the first stage loads
 // through load0, the last stores through store_last, and intermediate results
 // live in buf (row q at q * LD, element e at e + e / 8 when PAD).
-template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool PAD, int LD, class LD0, class STL>
+template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool PAD, int LD, bool WARP = false, class LD0,
+          class STL>
 __device__ __forceinline__ void fft_stages(float2* buf, const float2* tw, LD0 load0, STL store_last) {
   constexpr int NS = n_stages(G);
   if constexpr (S < NS) {
     auto sload = [&](int q, int e) { return buf[q * LD + (PAD ? e + (e >> 3) : e)]; };
     auto sstore = [&](int q, int e, float2 v) { buf[q * LD + (PAD ? e + (e >> 3) : e)] = v; };
-    if constexpr (S == 0 && S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST>(tw, load0, store_last);
-    else if constexpr (S == 0) fft_stage<G, S, ROWS, NT, DIR, QFAST>(tw, load0, sstore);
-    else if constexpr (S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST>(tw, sload, store_last);
-    else fft_stage<G, S, ROWS, NT, DIR, QFAST>(tw, sload, sstore);
-    fft_stages<G, S + 1, ROWS, NT, DIR, QFAST, PAD, LD>(buf, tw, load0, store_last);
+    if constexpr (S == 0 && S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP>(tw, load0, store_last);
+    else if constexpr (S == 0) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP>(tw, load0, sstore);
+    else if constexpr (S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP>(tw, sload, store_last);
+    else fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP>(tw, sload, sstore);
+    fft_stages<G, S + 1, ROWS, NT, DIR, QFAST, PAD, LD, WARP>(buf, tw, load0, store_last);
   }
 }
 
@@ -273,45 +284,40 @@ struct Geo2 {
 };
 
 // forward row pass: T[row][:] = FFT_G1(pad(x[be][r][:] * S_c * deapod * sign)),
-// row = vol * S0 + r, ROWS consecutive rows per block
+// row = vol * S0 + r; one warp per row (warp-scope exchanges), ROW_WARPS rows per block
+constexpr int ROW_WARPS = ROW_NT / 32;
+
 template <int G1>
 __global__ void __launch_bounds__(ROW_NT) fwd_rows_kernel(const float2* __restrict__ x, const float2* __restrict__ maps,
                                                           const float* __restrict__ invdeap, float2* __restrict__ Tb,
                                                           const float2* __restrict__ tw, Geo2 g, long long nrows,
                                                           int coil_images) {
-  constexpr int ROWS = rows_per_block(G1);
   constexpr int LD = padded_len(G1);
   extern __shared__ float2 sm[];
   if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  __shared__ long long s_xoff[ROWS], s_moff[ROWS];   // row starts in x and maps
-  __shared__ float s_d[ROWS];                        // row deapodisation x (-1)^(r + off0)
-  const long long row0 = (long long)blockIdx.x * ROWS;
-  const int nr = (int)min((long long)ROWS, nrows - row0);
-  if (threadIdx.x < nr) {
-    const long long row = row0 + threadIdx.x;
-    const long long vol = row / g.S0;
-    const int r = (int)(row - vol * g.S0);
-    const long long be = vol / g.C;
-    const int c = (int)(vol - be * g.C);
-    s_xoff[threadIdx.x] = (coil_images ? vol : be) * g.stot + (long long)r * g.S1;
-    s_moff[threadIdx.x] = (long long)c * g.stot + (long long)r * g.S1;
-    const float d = __ldg(invdeap + r);
-    s_d[threadIdx.x] = ((r + g.off0) & 1) ? -d : d;
-  }
-  __syncthreads();
-  auto load0 = [&](int q, int n1) -> float2 {
+  const int warp = threadIdx.x >> 5;
+  const long long row = (long long)blockIdx.x * ROW_WARPS + warp;
+  if (row >= nrows) return;                          // no block-wide barrier below
+  float2* buf = sm + warp * LD;
+  const long long vol = row / g.S0;
+  const int r = (int)(row - vol * g.S0);
+  const long long be = vol / g.C;
+  const int c = (int)(vol - be * g.C);
+  const float2* xr = x + (coil_images ? vol : be) * g.stot + (long long)r * g.S1;
+  const float2* mr = maps + (long long)c * g.stot + (long long)r * g.S1;
+  const float dr = ((r + g.off0) & 1) ? -__ldg(invdeap + r) : __ldg(invdeap + r);
+  float2* out = Tb + row * G1;
+  auto load0 = [&](int, int n1) -> float2 {
     const int i1 = n1 - g.off1;
-    if (q >= nr || (unsigned)i1 >= (unsigned)g.S1) return make_float2(0.f, 0.f);
-    const float2 xv = x[s_xoff[q] + i1];
-    const float2 mv = coil_images ? make_float2(1.f, 0.f) : __ldg(maps + s_moff[q] + i1);
-    float s = s_d[q] * __ldg(invdeap + g.S0 + i1);
+    if ((unsigned)i1 >= (unsigned)g.S1) return make_float2(0.f, 0.f);
+    const float2 xv = xr[i1];
+    const float2 mv = coil_images ? make_float2(1.f, 0.f) : __ldg(mr + i1);
+    float s = dr * __ldg(invdeap + g.S0 + i1);
     if (n1 & 1) s = -s;
     return make_float2((xv.x * mv.x - xv.y * mv.y) * s, (xv.x * mv.y + xv.y * mv.x) * s);
   };
-  auto store = [&](int q, int k1, float2 v) {
-    if (q < nr) Tb[(row0 + q) * G1 + k1] = v;
-  };
-  fft_stages<G1, 0, ROWS, ROW_NT, -1, false, true, LD>(sm, tw, load0, store);
+  auto store = [&](int, int k1, float2 v) { out[k1] = v; };
+  fft_stages<G1, 0, 1, 32, -1, false, true, LD, true>(buf, tw, load0, store);
 }
 
 // forward column pass: grid[vol][:][k1] = FFT_G0(band rows of T[vol][:][k1]),
@@ -482,12 +488,11 @@ bool length_supported(int G) {
 template <int G1>
 int launch_fwd_rows(const void* x, const float2* maps, const float* invdeap, float2* Tb, const float2* tw,
                     const Geo2& g, int nb, int coil_images, cudaStream_t st) {
-  constexpr int ROWS = rows_per_block(G1);
-  const size_t smem = (size_t)ROWS * padded_len(G1) * sizeof(float2);
+  const size_t smem = (size_t)ROW_WARPS * padded_len(G1) * sizeof(float2);
   int rc;
   if ((rc = set_smem((const void*)fwd_rows_kernel<G1>, smem))) return rc;
   const long long nrows = (long long)nb * g.C * g.S0;
-  const long long blocks = (nrows + ROWS - 1) / ROWS;
+  const long long blocks = (nrows + ROW_WARPS - 1) / ROW_WARPS;
   MRB_REQUIRE(blocks < (1LL << 31), "too many rows");
   fwd_rows_kernel<G1><<<(unsigned)blocks, ROW_NT, smem, st>>>((const float2*)x, maps, invdeap, Tb, tw, g, nrows,
                                                               coil_images);

@@ -65,6 +65,11 @@ _SIGS = {
     "mrb_cnn_adam": [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_float, ct.c_float,
                      ct.c_float, ct.c_float, ct.c_int, ct.c_void_p, ct.c_void_p],
     "mrb_cnn_to_bf16": [ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_void_p],
+    "mrb_cnn_tc_supported": [ct.c_int] * 6,
+    "mrb_cnn_conv3d_tc": [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_int, ct.c_int,
+                          ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_int,
+                          ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p],
+    "mrb_cnn_tc_error": [ct.c_void_p],
 }
 
 
@@ -106,6 +111,9 @@ class WarmStartCNN:
         self.m = {k: torch.zeros_like(v) for k, v in self._params()}
         self.v = {k: torch.zeros_like(v) for k, v in self._params()}
         self._bufs: Dict[tuple, dict] = {}
+        # convolutions run on tcgen05 (tensor memory) where the shape allows,
+        # on the warp-level mma.sync kernel otherwise
+        self.use_tc = True
         self.refresh()
 
     # -------------------------------------------------------------- parameters
@@ -115,13 +123,15 @@ class WarmStartCNN:
             yield "b:" + name, self.b32[name]
 
     def refresh(self):
-        """BF16 weights for the forward pass and flipped BF16 weights for the data gradient."""
+        """BF16 weights for the forward pass, their K-major copy for the tensor-core
+        convolution and flipped BF16 weights for the data gradient."""
         st = _lib.stream_ptr(self.device)
-        self.wb, self.wd = {}, {}
+        self.wb, self.wd, self.wk = {}, {}, {}
         for name, cinp, cin, coutp, cout, relu in LAYERS:
             wb = torch.empty((27, cinp, coutp), dtype=torch.bfloat16, device=self.device)
             _lib.check(self.lib.mrb_cnn_to_bf16(_p(self.w32[name]), wb.numel(), _p(wb), st), "to_bf16")
             self.wb[name] = wb
+            self.wk[name] = wb.permute(0, 2, 1).contiguous()
             wd = torch.empty((27, coutp, cinp), dtype=torch.bfloat16, device=self.device)
             _lib.check(self.lib.mrb_cnn_flip_weights(_p(wb), cinp, coutp, _p(wd), cinp, st), "flip")
             self.wd[name] = wd
@@ -176,8 +186,21 @@ class WarmStartCNN:
 
     # ----------------------------------------------------------------- forward
     def _conv(self, name, x, cx, xoff, vol, yb=None, cyb=0, ybo=0, yf=None, cyf=0, yfo=0, acc=0, weights=None,
-              cin=None, coutp=None, cout=None, relu=None, bias=True):
+              cin=None, coutp=None, cout=None, relu=None, bias=True, dgrad=False):
         _, cinp, _, coutp_l, cout_l, relu_l = next(l for l in LAYERS if l[0] == name)
+        k = cinp if cin is None else cin
+        n = coutp_l if coutp is None else coutp
+        co = cout_l if cout is None else cout
+        Nb, D, H, W = (int(v) for v in vol)
+        if self.use_tc and self.lib.mrb_cnn_tc_supported(k, xoff, cx, n, W, H) and (yb is None or (cyb % 8 == 0 and ybo % 8 == 0)):
+            # K-major weights: forward [27][N = cout][K = cin]; data gradient: the
+            # forward weights [27][cin][cout] read as [27][N = cin][K = cout], taps flipped
+            wk = self.wb[name] if dgrad else self.wk[name]
+            _lib.check(self.lib.mrb_cnn_conv3d_tc(
+                _p(x), cx, xoff, k, _p(wk), 1 if dgrad else 0, n, co, _p(self.b32[name]) if bias else None,
+                int(relu_l if relu is None else relu), _p(yb), cyb, ybo, _p(yf), cyf, yfo, acc, Nb, D, H, W,
+                _lib.stream_ptr(self.device)), f"conv {name}")
+            return
         w = self.wb[name] if weights is None else weights
         _lib.check(self.lib.mrb_cnn_conv3d_fwd(
             _p(x), cx, xoff, cinp if cin is None else cin, _p(w), coutp_l if coutp is None else coutp,
@@ -241,7 +264,7 @@ class WarmStartCNN:
     def _dgrad(self, name, gz, cg, vol, gout, cgo, goff, acc=0):
         _, cinp, _, coutp, _, _ = next(l for l in LAYERS if l[0] == name)
         self._conv(name, gz, cg, 0, vol, yf=gout, cyf=cgo, yfo=goff, acc=acc, weights=self.wd[name],
-                   cin=coutp, coutp=cinp, cout=cinp, relu=False, bias=False)
+                   cin=coutp, coutp=cinp, cout=cinp, relu=False, bias=False, dgrad=True)
 
     def _relu_bwd(self, g, cgs, goff, act, cas, aoff, nch, V, gz, czs):
         _lib.check(self.lib.mrb_cnn_relu_bwd(_p(g), cgs, goff, _p(act), cas, aoff, nch, V, _p(gz), czs, 0, czs,

@@ -110,3 +110,72 @@ def test_training_reduces_loss(cuda):
     net = WarmStartCNN(cuda, seed=1)
     hist = net.train(inp.to(cuda), tgt.to(cuda), epochs=12, batch=2, lr=2e-3)
     assert hist[-1] < 0.6 * hist[0]
+
+
+@pytest.mark.parametrize("cin,cout,vol,ci_off", [(32, 32, (1, 3, 4, 32), 0), (64, 128, (2, 2, 2, 64), 32),
+                                                 (192, 64, (1, 2, 1, 128), 0), (96, 32, (1, 3, 2, 64), 32)])
+def test_conv_tcgen05_fwd_dgrad_exact(cuda, cin, cout, vol, ci_off):
+    """tcgen05 / TMEM convolution (TMA-staged, zero padding by out-of-volume
+    coordinates) against the FP64 reference on BF16 values: forward (FP32 and
+    BF16-at-offset outputs) and the data gradient through the flipped-tap read
+    of the forward weights; the barrier-timeout flag stays clear."""
+    from mrirecon_b200 import _lib
+    from mrirecon_b200.warmstart import _lib_cnn
+    L = _lib_cnn()
+    st = _lib.stream_ptr()
+    Nb, D, H, W = vol
+    assert L.mrb_cnn_tc_supported(cin, ci_off, cin + ci_off, cout, W, H)
+    g = torch.Generator().manual_seed(7 * cin + cout)
+    V = Nb * D * H * W
+    cx = cin + ci_off
+    xfull = _bf(torch.randn((V, cx), generator=g))
+    x = xfull[:, ci_off:]
+    w = _bf(torch.randn((27, cin, cout), generator=g) * 0.1)
+    bias = torch.randn(cout, generator=g)
+    gy = _bf(torch.randn((V, cout), generator=g))
+    xc, bc, gyc = xfull.to(cuda), bias.to(cuda), gy.to(cuda)
+    wk = w.permute(0, 2, 1).contiguous().to(cuda)          # [27][cout][cin], K-major
+    y = torch.zeros((V, cout), dtype=torch.float32, device=cuda)
+    yb = torch.zeros((V, cout + 32), dtype=torch.bfloat16, device=cuda)
+    _lib.check(L.mrb_cnn_conv3d_tc(xc.data_ptr(), cx, ci_off, cin, wk.data_ptr(), 0, cout, cout, bc.data_ptr(), 0,
+                                   yb.data_ptr(), cout + 32, 32, y.data_ptr(), cout, 0, 0, Nb, D, H, W, st), "tc fwd")
+    x5 = x.double().reshape(Nb, D, H, W, cin).permute(0, 4, 1, 2, 3).requires_grad_(True)
+    w5 = _torch_w(w.double())
+    y5 = Fn.conv3d(x5, w5, bias.double(), padding=1)
+    yref = y5.permute(0, 2, 3, 4, 1).reshape(V, cout)
+    assert rel(y, yref) < 1e-5
+    assert rel(yb[:, 32:].float(), yref) < 1e-2          # BF16 rounding of the output
+    assert float(yb[:, :32].float().abs().max()) == 0.0   # channels before the offset untouched
+    y5.backward(gy.double().reshape(Nb, D, H, W, cout).permute(0, 4, 1, 2, 3))
+    wc = w.to(cuda)                                       # [27][cin][cout] read as [27][N = cin][K = cout]
+    dx = torch.zeros((V, cin), dtype=torch.float32, device=cuda)
+    _lib.check(L.mrb_cnn_conv3d_tc(gyc.data_ptr(), cout, 0, cout, wc.data_ptr(), 1, cin, cin, None, 0, None, 0, 0,
+                                   dx.data_ptr(), cin, 0, 0, Nb, D, H, W, st), "tc dgrad")
+    assert rel(dx, x5.grad.permute(0, 2, 3, 4, 1).reshape(V, cin)) < 1e-5
+    err = ct.c_int(-1)
+    _lib.check(L.mrb_cnn_tc_error(ct.byref(err)), "tc error flag")
+    assert err.value == 0
+
+
+def test_network_tcgen05_equals_mma_sync_path(cuda):
+    """The network's inference and gradients agree on the tcgen05 and the
+    mma.sync convolution paths (same BF16 operands, FP32 accumulation order
+    differs)."""
+    from mrirecon_b200.warmstart import WarmStartCNN
+    net = WarmStartCNN(cuda, seed=5)
+    net.w32["c8"].mul_(10.0)
+    net.refresh()
+    g = torch.Generator().manual_seed(2)
+    z = (torch.randn((1, 4, 64, 64), generator=g) + 1j * torch.randn((1, 4, 64, 64), generator=g)).to(
+        torch.complex64).to(cuda)
+    tgt = (z * 0.5).contiguous()
+    outs, losses, grads = [], [], []
+    for tc in (True, False):
+        net.use_tc = tc
+        outs.append(net.infer(z).clone())
+        losses.append(float(net.loss_and_grad(z, tgt)[0]))
+        grads.append({k: v.clone() for k, v in net.dw.items()})
+    assert rel(outs[0], outs[1]) < 1e-3
+    assert abs(losses[0] - losses[1]) <= 1e-3 * abs(losses[1])
+    for k in grads[0]:
+        assert rel(grads[0][k], grads[1][k]) < 2e-2, k
