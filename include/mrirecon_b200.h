@@ -148,7 +148,10 @@ int mrb_grid_indices(const float* traj, int nd, const int* G, int64_t K, int W, 
 /* ------------------------------------------------------------------------
  * Scratch for the FP64 reductions.  Every reducing entry point below takes
  * a caller-owned device workspace `ws` of at least mrb_workspace_bytes()
- * bytes (block partials); calls on one stream may share it.
+ * bytes (block partials and a completion counter), ZERO-FILLED before its
+ * first use (the library leaves the counter at zero after every call); calls
+ * on one stream may share it, calls that may overlap on the GPU need their
+ * own.
  * ---------------------------------------------------------------------- */
 int mrb_workspace_bytes(int64_t* bytes);
 
@@ -237,6 +240,11 @@ int mrb_tv_multi(int nd, const int* S, int F, const mrb_tv_term* terms, int nter
 int mrb_ncg_slot_count(int64_t* slots, int64_t* hist_cols);
 int mrb_ncg_set_steps(double* ts, int J, double beta, mrb_stream_t stream);
 int mrb_ncg_armijo_select(double* slots, const double* cfg, mrb_stream_t stream);
+/* The same backtracking choice in two phases (no reference counterpart): phase
+ * 1 tries steps j = 1 .. J1-1 from a tv_multi pass over J1 steps; phase 2 (after
+ * a tv_multi pass over the remaining steps, skipped through slot 20 when phase
+ * 1 decided) continues at j = J1.  Same accepted step as the single pass. */
+int mrb_ncg_armijo_phase(double* slots, const double* cfg, int J1, int phase, mrb_stream_t stream);
 int mrb_ncg_control(double* slots, double* hist, const double* cfg, int nterms, int have_ft,
                     mrb_stream_t stream);
 int mrb_ncg_update(int64_t n, void* x, void* d, const void* g, void* gr, const void* gAd, void* g_prev,

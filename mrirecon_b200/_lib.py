@@ -77,6 +77,7 @@ _SIGS = {
     "mrb_ncg_slot_count": (ct.c_int, [c_int64_p, c_int64_p]),
     "mrb_ncg_set_steps": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_double, ct.c_void_p]),
     "mrb_ncg_armijo_select": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mrb_ncg_armijo_phase": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p]),
     "mrb_ncg_control": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p]),
     "mrb_ncg_update": (ct.c_int, [ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                   ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p]),

@@ -37,7 +37,7 @@ class BatchedSolver:
         for y, op, regm in problems:
             s = CGSolver(y, op, regm, CGConfig(**vars(self.cfg)))
             # private reduction scratch: instances run concurrently
-            s.ws_buf = torch.empty(_lib.workspace_bytes(), dtype=torch.uint8, device=s.device)
+            s.ws_buf = torch.zeros(_lib.workspace_bytes(), dtype=torch.uint8, device=s.device)
             self.solvers.append(s)
         self.device = self.solvers[0].device
         if any(s.device != self.device for s in self.solvers):

@@ -36,7 +36,7 @@ constexpr int TC_BM = 128;      // voxels per CTA (UMMA M)
 constexpr int TC_BK = 32;       // K per stage (channels): one 64-byte swizzle row
 constexpr int TC_STAGES = 4;
 constexpr int TC_THREADS = 128;
-constexpr long long TC_WAIT_LIMIT = 1LL << 22;   // polls of a barrier phase before giving up
+constexpr long long TC_WAIT_LIMIT = 1LL << 20;   // bounded try_wait rounds of a barrier phase before giving up
 
 __device__ int g_tc_error = 0;   // set when a barrier wait times out
 
@@ -50,10 +50,12 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 
+// try_wait suspends the thread in hardware for a bounded, system-dependent time
+// while the phase is incomplete (no busy polling of the issue slots)
 __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
       : "r"(smem_u32(bar)), "r"(parity)
       : "memory");
@@ -70,7 +72,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volati
       *abort_flag = 1;
       return false;
     }
-    if (i > 64) __nanosleep(64);
   }
   *abort_flag = 1;
   atomicExch(&g_tc_error, 1);

@@ -17,6 +17,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -83,6 +85,80 @@ int finalize(const double* partials, int nblocks, int stride, int nv, double* ou
 
 __device__ __forceinline__ double skipped(const double* flag) { return flag ? *flag : 0.0; }
 
+// Where a reducing kernel leaves its result: the block partials are summed by
+// the last block to finish (a completion counter in the caller's workspace,
+// zero between launches), in the same fixed order as finalize_kernel, so the
+// separate finalize launch disappears and the result is bit-identical.
+struct RedOut {
+  double* out;          // nv results
+  int nv;
+  int accumulate;       // out[j] += sum
+  const double* skip;   // out untouched when *skip != 0
+  double* copy0;        // optional second destination of out[0]
+  unsigned* counter;    // completion counter (zero between launches)
+};
+
+template <int NV>
+__device__ __forceinline__ void block_reduce_finish(double (&v)[NV], double* __restrict__ partials,
+                                                    const RedOut& r) {
+  block_reduce_store<NV>(v, partials);
+  __shared__ unsigned s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(r.counter, 1u) == gridDim.x - 1 ? 1u : 0u;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // the last block: every thread sums a fixed, strided set of block partials
+  // (independent loads, values in groups of 8), then one fixed-order block tree
+  __shared__ double fin[RED_THREADS / 32][NV];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int GRP = NV < 8 ? NV : 8;
+#pragma unroll 1
+  for (int j0 = 0; j0 < NV; j0 += GRP) {
+    double acc[GRP];
+#pragma unroll
+    for (int q = 0; q < GRP; ++q) acc[q] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+      for (int q = 0; q < GRP; ++q)
+        if (j0 + q < NV) acc[q] += __ldcg(partials + (long long)b * NV + j0 + q);
+    }
+#pragma unroll
+    for (int q = 0; q < GRP; ++q) {
+      double sv = acc[q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sv += __shfl_down_sync(0xffffffffu, sv, o);
+      if (lane == 0 && j0 + q < NV) fin[warp][j0 + q] = sv;
+    }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const bool skip = r.skip && *r.skip != 0.0;
+    for (int j = 0; j < r.nv; ++j) {
+      double sv = lane < RED_THREADS / 32 ? fin[lane][j] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) sv += __shfl_down_sync(0xffffffffu, sv, o);
+      if (lane == 0 && !skip) {
+        const double val = r.accumulate ? r.out[j] + sv : sv;
+        r.out[j] = val;
+        if (j == 0 && r.copy0) *r.copy0 = val;
+      }
+    }
+    if (lane == 0) *r.counter = 0u;
+  }
+}
+
+constexpr size_t RED_PART_BYTES = (size_t)RED_MAX_BLOCKS * RED_MAX_VALS * sizeof(double);
+
+__host__ __device__ inline unsigned* ws_counter(void* ws) {
+  return reinterpret_cast<unsigned*>(reinterpret_cast<char*>(ws) + RED_PART_BYTES);
+}
+
+inline RedOut red_out(void* ws, double* out, int nv, int accumulate, const double* skip, double* copy0 = nullptr) {
+  return RedOut{out, nv, accumulate, skip, copy0, ws_counter(ws)};
+}
+
 // ---------------------------------------------------------------------------
 // generic dots: out[j] = sum Re(conj(a_j) b_j) / diag_j
 // ---------------------------------------------------------------------------
@@ -124,9 +200,10 @@ __global__ void __launch_bounds__(RED_THREADS) kspace_kernel(int mode, long long
                                                              const float2* __restrict__ Ax,
                                                              const float2* __restrict__ y, const double* t_dev,
                                                              double t_host, const double* skip,
-                                                             double* __restrict__ partials) {
+                                                             double* __restrict__ partials, RedOut ro) {
   double acc[3] = {0.0, 0.0, 0.0};
-  bool sk = skipped(skip) != 0.0;
+  if (skipped(skip) != 0.0) return;   // uniform over the grid: no partials, no counter
+  const bool sk = false;
   float t = (float)(t_dev ? *t_dev : t_host);
   const long long stride = (long long)gridDim.x * blockDim.x;
   if (!sk) {
@@ -155,9 +232,9 @@ __global__ void __launch_bounds__(RED_THREADS) kspace_kernel(int mode, long long
   if (mode == 2) return;
   if (mode == 1) {
     double v1[1] = {acc[0]};
-    block_reduce_store<1>(v1, partials);
+    block_reduce_finish<1>(v1, partials, ro);
   } else {
-    block_reduce_store<3>(acc, partials);
+    block_reduce_finish<3>(acc, partials, ro);
   }
 }
 
@@ -249,7 +326,8 @@ struct GradArgs {
 };
 
 template <int NS, int NU>
-__global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P, double* __restrict__ partials) {
+__global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P, double* __restrict__ partials,
+                                                           RedOut ro) {
   // dot products (which may cancel) accumulate in FP64 per thread; the TV
   // energies (non-negative terms) in FP32 per thread; reductions in FP64
   double acc[GP_NV];
@@ -258,8 +336,8 @@ __global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P,
   float eacc[MAX_TERMS];
 #pragma unroll
   for (int j = 0; j < MAX_TERMS; ++j) eacc[j] = 0.f;
-  bool sk = false;
-  if (a.skip) sk = a.skip_if_zero ? (*a.skip == 0.0) : (*a.skip != 0.0);
+  if (a.skip && (a.skip_if_zero ? (*a.skip == 0.0) : (*a.skip != 0.0))) return;   // uniform: out untouched
+  const bool sk = false;
   const float t = (float)(a.t_dev ? *a.t_dev : a.t_host);
   const unsigned stride_all = gridDim.x * blockDim.x;
   if (!sk) {
@@ -365,7 +443,7 @@ __global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P,
   }
 #pragma unroll
   for (int j = 0; j < MAX_TERMS; ++j) acc[j] = (double)eacc[j];
-  block_reduce_store<GP_NV>(acc, partials);
+  block_reduce_finish<GP_NV>(acc, partials, ro);
 }
 
 // Sum of all unit energies at z = x + t_j d for J <= MT_MAX_J step sizes, one
@@ -379,13 +457,15 @@ template <int NS, int NU>
 __global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __restrict__ x,
                                                                const float2* __restrict__ d,
                                                                const double* __restrict__ ts, int J, TVPlan P,
-                                                               const double* skip, double* __restrict__ partials) {
+                                                               const double* skip, double* __restrict__ partials,
+                                                               RedOut ro) {
   // energies are sums of non-negative terms: a thread sums its ~n / (blocks x threads)
   // voxels in FP32, the block and grid reductions run in FP64
   float facc[MT_MAX_J];
 #pragma unroll
   for (int j = 0; j < MT_MAX_J; ++j) facc[j] = 0.f;
-  const bool sk = skipped(skip) != 0.0;
+  if (skipped(skip) != 0.0) return;   // uniform over the grid: no partials, no counter
+  const bool sk = false;
   __shared__ float tf[MT_MAX_J];   // trial steps, broadcast from shared memory
   if (threadIdx.x < MT_MAX_J) tf[threadIdx.x] = threadIdx.x < J ? (float)ts[threadIdx.x] : 0.f;
   __syncthreads();
@@ -434,7 +514,7 @@ __global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __r
   double acc[MT_MAX_J];
 #pragma unroll
   for (int j = 0; j < MT_MAX_J; ++j) acc[j] = (double)facc[j];
-  block_reduce_store<MT_MAX_J>(acc, partials);
+  block_reduce_finish<MT_MAX_J>(acc, partials, ro);
 }
 
 // ---------------------------------------------------------------------------
@@ -443,7 +523,7 @@ __global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __r
 enum Slot {
   S_T = 0, S_LS_OK, S_DONE, S_REASON, S_ITER, S_F0, S_G0D, S_FT, S_GDT,
   S_ERR, S_ERD, S_EDD, S_RHO_PREV, S_RHO_INIT, S_BETA,
-  S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL, S_NRESTART,
+  S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL, S_NRESTART, S_NOMORE,
   S_RED = 24,            // reduction outputs of the gradient pass (GP_NV values)
   S_EJ = 48,             // multi-t energies (MT_MAX_J values)
   S_G0D_NEXT = 80,
@@ -516,6 +596,66 @@ __global__ void armijo_select_kernel(double* s, const double* cfg_dev) {
   }
   s[S_T] = t;
   s[S_LS_OK] = 0.0;
+  s[S_DONE] = 1.0;
+  s[S_REASON] = 1.0;
+}
+
+// Two-phase Armijo selection over the same backtracking sequence: phase 1
+// tries j = 1 .. J1-1 on the energies of a first tv_multi pass over J1 steps;
+// when none satisfies f(t) <= f(0) + c1 t f'(0) it clears S_NOMORE and phase 2,
+// after a second tv_multi pass over the remaining steps, continues at j = J1.
+// S_NOMORE = 1 whenever the second pass and phase 2 have nothing to do.
+__global__ void armijo_phase_kernel(double* s, const double* cfg_dev, int J1, int phase) {
+  if (threadIdx.x != 0) return;
+  const NCGCfg cfg = load_cfg(cfg_dev);
+  const int jmax = cfg.ls_max_iter < MT_MAX_J - 1 ? cfg.ls_max_iter : MT_MAX_J - 1;
+  const double err = s[S_ERR], erd = s[S_ERD], edd = s[S_EDD];
+  double t;
+  int j0, j1;
+  if (phase == 1) {
+    s[S_NOMORE] = 1.0;
+    if (s[S_DONE] != 0.0) {
+      s[S_LS_OK] = 0.0;
+      return;
+    }
+    const double f0 = 0.5 * err + s[S_EJ + 0];
+    const double g0d = s[S_G0D];
+    s[S_F0] = f0;
+    if (!(g0d < 0.0) || isnan(g0d) || isinf(g0d)) {
+      s[S_LS_OK] = 0.0;
+      s[S_DONE] = 1.0;
+      s[S_REASON] = 1.0;
+      s[S_T] = 0.0;
+      return;
+    }
+    t = 1.0;
+    j0 = 1;
+    j1 = J1 - 1 < jmax ? J1 - 1 : jmax;
+  } else {
+    if (s[S_NOMORE] != 0.0) return;
+    s[S_NOMORE] = 1.0;
+    t = s[S_T];
+    j0 = J1;
+    j1 = jmax;
+  }
+  const double f0 = s[S_F0], g0d = s[S_G0D];
+  for (int j = j0; j <= j1; ++j) {
+    double ft = 0.5 * (err + 2.0 * t * erd + t * t * edd) + s[S_EJ + j];
+    if (ft <= f0 + cfg.c1 * t * g0d) {
+      s[S_T] = t;
+      s[S_FT] = ft;
+      s[S_LS_OK] = 1.0;
+      s[S_NTRIAL] = (double)j;
+      return;
+    }
+    t *= cfg.ls_beta;
+  }
+  s[S_T] = t;
+  s[S_LS_OK] = 0.0;
+  if (phase == 1 && j1 < jmax) {
+    s[S_NOMORE] = 0.0;   // the remaining steps decide
+    return;
+  }
   s[S_DONE] = 1.0;
   s[S_REASON] = 1.0;
 }
@@ -610,7 +750,7 @@ __global__ void __launch_bounds__(RED_THREADS) ncg_update_kernel(long long n, fl
                                                                  float2* __restrict__ g_prev,
                                                                  const float* __restrict__ diag, long long ndiag,
                                                                  const double* __restrict__ s,
-                                                                 double* __restrict__ partials) {
+                                                                 double* __restrict__ partials, RedOut ro) {
   double acc[1] = {0.0};
   const bool ok = s[S_LS_OK] != 0.0;
   const bool upd_dir = ok && s[S_DONE] == 0.0;
@@ -643,7 +783,7 @@ __global__ void __launch_bounds__(RED_THREADS) ncg_update_kernel(long long n, fl
       }
     }
   }
-  block_reduce_store<1>(acc, partials);
+  block_reduce_finish<1>(acc, partials, ro);
 }
 
 // d = -g/D (priming: cg.py:182-185) and Re<g,d>
@@ -651,7 +791,7 @@ __global__ void __launch_bounds__(RED_THREADS) steepest_kernel(long long n, floa
                                                                const float2* __restrict__ g,
                                                                float2* __restrict__ g_prev,
                                                                const float* __restrict__ diag, long long ndiag,
-                                                               double* __restrict__ partials) {
+                                                               double* __restrict__ partials, RedOut ro) {
   double acc[1] = {0.0};
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -662,7 +802,7 @@ __global__ void __launch_bounds__(RED_THREADS) steepest_kernel(long long n, floa
     if (g_prev) g_prev[i] = gv;
     acc[0] += (double)(gv.x * dv.x + gv.y * dv.y);
   }
-  block_reduce_store<1>(acc, partials);
+  block_reduce_finish<1>(acc, partials, ro);
 }
 
 // Optional restart (not in the reference): when the updated direction is not a
@@ -742,6 +882,17 @@ void launch_tv(const TVPlan& P, int nb, cudaStream_t st, A... args) {
   else if (P.ns <= 2) launch_tv_nu<L, 2>(P, nb, st, args...);
   else if (P.ns <= 3) launch_tv_nu<L, 3>(P, nb, st, args...);
   else launch_tv_nu<L, NSLOT>(P, nb, st, args...);
+}
+
+// grid of the TV passes: one wave of 3 resident 256-thread blocks per SM
+int tv_grid() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    n = std::max(1, std::min(RED_MAX_BLOCKS, 3 * sms));
+  }
+  return n;
 }
 
 int build_plan(TVPlan& P, int nd, const int* S, int F, const mrb_tv_term* terms, int nterms) {
@@ -846,7 +997,7 @@ int build_plan(TVPlan& P, int nd, const int* S, int F, const mrb_tv_term* terms,
 // ===========================================================================
 extern "C" int mrb_workspace_bytes(int64_t* bytes) {
   MRB_REQUIRE(bytes != nullptr, "null pointer");
-  *bytes = (int64_t)RED_MAX_BLOCKS * RED_MAX_VALS * sizeof(double);
+  *bytes = (int64_t)RED_PART_BYTES + 256;   // block partials + completion counter
   return 0;
 }
 
@@ -898,10 +1049,10 @@ extern "C" int mrb_kspace_pass(int mode, int64_t n, void* r, const void* Ad, con
   int nb = red_blocks(n, 4);
   double* part = (double*)ws;
   kspace_kernel<<<nb, RED_THREADS, 0, st>>>(mode, n, (float2*)r, (const float2*)Ad, (const float2*)Ax,
-                                            (const float2*)y, t_dev, t_host, skip, part);
+                                            (const float2*)y, t_dev, t_host, skip, part,
+                                            red_out(ws, out, mode == 0 ? 3 : 1, 0, skip));
   MRB_LAUNCH_CHECK();
-  if (mode == 2) return 0;
-  return finalize(part, nb, mode == 0 ? 3 : 1, mode == 0 ? 3 : 1, out, 0, skip, st);
+  return 0;
 }
 
 extern "C" int mrb_tv_grad(int nd, const int* S, int F, const mrb_tv_term* terms, int nterms, const void* x,
@@ -926,11 +1077,11 @@ extern "C" int mrb_tv_grad(int nd, const int* S, int F, const mrb_tv_term* terms
   a.skip = skip;
   a.skip_if_zero = skip_if_zero;
   cudaStream_t st = (cudaStream_t)stream;
-  int nb = red_blocks(P.n, 2);
+  int nb = std::min(red_blocks(P.n, 2), tv_grid());
   double* part = (double*)ws;
-  launch_tv<GradLaunch>(P, nb, st, a, P, part);
+  launch_tv<GradLaunch>(P, nb, st, a, P, part, red_out(ws, out, GP_NV, 0, nullptr));
   MRB_LAUNCH_CHECK();
-  return finalize(part, nb, GP_NV, GP_NV, out, 0, nullptr, st);
+  return 0;
 }
 
 extern "C" int mrb_tv_multi(int nd, const int* S, int F, const mrb_tv_term* terms, int nterms, const void* x,
@@ -942,16 +1093,26 @@ extern "C" int mrb_tv_multi(int nd, const int* S, int F, const mrb_tv_term* term
   int rc = build_plan(P, nd, S, F, terms, nterms);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  int nb = red_blocks(P.n, 2);
+  int nb = std::min(red_blocks(P.n, 2), tv_grid());
   double* part = (double*)ws;
-  launch_tv<MultiLaunch>(P, nb, st, (const float2*)x, (const float2*)d, ts, J, P, skip, part);
+  launch_tv<MultiLaunch>(P, nb, st, (const float2*)x, (const float2*)d, ts, J, P, skip, part,
+                         red_out(ws, out, J, 0, skip));
   MRB_LAUNCH_CHECK();
-  return finalize(part, nb, MT_MAX_J, J, out, 0, skip, st);
+  return 0;
 }
 
 extern "C" int mrb_ncg_armijo_select(double* slots, const double* cfg, mrb_stream_t stream) {
   MRB_REQUIRE(slots != nullptr && cfg != nullptr, "null pointer");
   armijo_select_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slots, cfg);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_ncg_armijo_phase(double* slots, const double* cfg, int J1, int phase, mrb_stream_t stream) {
+  MRB_REQUIRE(slots != nullptr && cfg != nullptr, "null pointer");
+  MRB_REQUIRE(phase == 1 || phase == 2, "phase must be 1 or 2");
+  MRB_REQUIRE(J1 >= 2 && J1 <= MT_MAX_J, "J1 out of range");
+  armijo_phase_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slots, cfg, J1, phase);
   MRB_LAUNCH_CHECK();
   return 0;
 }
@@ -971,14 +1132,11 @@ extern "C" int mrb_ncg_update(int64_t n, void* x, void* d, const void* g, void* 
   cudaStream_t st = (cudaStream_t)stream;
   int nb = red_blocks(n, 2);
   double* part = (double*)ws;
+  // next slope at t = 0 -> S_G0D_NEXT and S_G0D
   ncg_update_kernel<<<nb, RED_THREADS, 0, st>>>(n, (float2*)x, (float2*)d, (const float2*)g, (float2*)gr,
                                                  (const float2*)gAd, (float2*)g_prev, diag, ndiag > 0 ? ndiag : 1,
-                                                 slots, part);
-  MRB_LAUNCH_CHECK();
-  // next slope at t = 0 -> S_G0D_NEXT, then S_G0D (skipped when not updated)
-  int rc = finalize(part, nb, 1, 1, slots + S_G0D_NEXT, 0, nullptr, st);
-  if (rc) return rc;
-  copy_slot_kernel<<<1, 32, 0, st>>>(slots, S_G0D, S_G0D_NEXT);
+                                                 slots, part,
+                                                 red_out(ws, slots + S_G0D_NEXT, 1, 0, nullptr, slots + S_G0D));
   MRB_LAUNCH_CHECK();
   return 0;
 }
@@ -1009,9 +1167,9 @@ extern "C" int mrb_ncg_steepest(int64_t n, void* d, const void* g, void* g_prev,
   int nb = red_blocks(n, 2);
   double* part = (double*)ws;
   steepest_kernel<<<nb, RED_THREADS, 0, st>>>(n, (float2*)d, (const float2*)g, (float2*)g_prev, diag,
-                                               ndiag > 0 ? ndiag : 1, part);
+                                               ndiag > 0 ? ndiag : 1, part, red_out(ws, out, 1, 0, nullptr));
   MRB_LAUNCH_CHECK();
-  return finalize(part, nb, 1, 1, out, 0, nullptr, st);
+  return 0;
 }
 
 extern "C" int mrb_ncg_set_steps(double* ts, int J, double beta, mrb_stream_t stream) {

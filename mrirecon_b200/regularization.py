@@ -138,7 +138,7 @@ def workspace(device) -> torch.Tensor:
     key = (device.type, device.index)
     ws = _WS.get(key)
     if ws is None:
-        ws = torch.empty(_lib.workspace_bytes(), dtype=torch.uint8, device=device)
+        ws = torch.zeros(_lib.workspace_bytes(), dtype=torch.uint8, device=device)   # counter starts at zero
         _WS[key] = ws
     return ws
 

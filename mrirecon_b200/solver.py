@@ -49,7 +49,8 @@ from .roles import Roles
 # slot indices (must match csrc/ncg.cu)
 S_T, S_LS_OK, S_DONE, S_REASON, S_ITER, S_F0, S_G0D, S_FT, S_GDT = range(9)
 S_ERR, S_ERD, S_EDD, S_RHO_PREV, S_RHO_INIT, S_BETA = range(9, 15)
-S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL, S_NRESTART = range(15, 20)
+S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL, S_NRESTART, S_NOMORE = range(15, 21)
+ARMIJO_J1 = 6   # trial steps of the first energy pass (t = 0, 1, 1/2, ..., 1/16)
 S_RED, S_EJ, S_G0D_NEXT = 24, 48, 80
 MAX_TERMS = 4
 REASONS = {0: "running", 1: "line-search failed", 2: "converged (tol_g/tol_step)",
@@ -268,10 +269,18 @@ class CGSolver:
             _lib.check(lib.mrb_kspace_pass(0, self.n_k, _lib.ptr(self.r), _lib.ptr(self.Ad), None, None, None,
                                            0.0, self._slot(S_DONE), self._slot(S_ERR), ws, st), "kspace_pass")
             self._AH(self.Ad, self.gAd)
+        # Armijo in two phases: the TV energies of the first ARMIJO_J1 trial steps,
+        # the rest only when none of those is accepted (device-side skip)
+        J1 = min(J, ARMIJO_J1)
         _lib.check(lib.mrb_tv_multi(self.nd, self._Sarr, self.F, self._terms_arr, self.nterms, _lib.ptr(self.x),
-                                    _lib.ptr(self.d), _lib.ptr(self.ts), J, self._slot(S_DONE), self._slot(S_EJ),
+                                    _lib.ptr(self.d), _lib.ptr(self.ts), J1, self._slot(S_DONE), self._slot(S_EJ),
                                     ws, st), "tv_multi")
-        _lib.check(lib.mrb_ncg_armijo_select(_lib.ptr(self.s), _lib.ptr(self.cfg_dev), st), "armijo_select")
+        _lib.check(lib.mrb_ncg_armijo_phase(_lib.ptr(self.s), _lib.ptr(self.cfg_dev), J1, 1, st), "armijo 1")
+        if J > J1:
+            _lib.check(lib.mrb_tv_multi(self.nd, self._Sarr, self.F, self._terms_arr, self.nterms,
+                                        _lib.ptr(self.x), _lib.ptr(self.d), _lib.ptr(self.ts) + 8 * J1, J - J1,
+                                        self._slot(S_NOMORE), self._slot(S_EJ + J1), ws, st), "tv_multi 2")
+            _lib.check(lib.mrb_ncg_armijo_phase(_lib.ptr(self.s), _lib.ptr(self.cfg_dev), J1, 2, st), "armijo 2")
         self._tv_grad(self.d, self._slot(S_T), 0.0, self.gr, self.gAd, self.g, self._slot(S_RED),
                       skip=self._slot(S_LS_OK), skip_if_zero=1)
         _lib.check(lib.mrb_ncg_control(_lib.ptr(self.s), _lib.ptr(self.hist), _lib.ptr(self.cfg_dev),
