@@ -174,6 +174,10 @@ class CGSolver:
         self.hist = torch.zeros((max(1, c.max_iter), self.hist_cols), dtype=torch.float64, device=dev)
         self.ts = torch.zeros(24, dtype=torch.float64, device=dev)
         self.ws_buf = workspace(dev)
+        # the first TV energy pass of each iteration needs only x and d: it runs on a
+        # side stream (own reduction scratch) while the NUFFT chain runs
+        self._side = torch.cuda.Stream(dev)
+        self.ws_side = torch.zeros(_lib.workspace_bytes(), dtype=torch.uint8, device=dev)
         self.cfg_dev = torch.tensor([c.c1, c.ls_beta, c.ls_max_iter, c.max_iter, c.tol_g, c.tol_step,
                                      c.stop_window, c.stop_tol, DIRS[c.direction.lower()], c.max_iter],
                                     dtype=torch.float64, device=dev)
@@ -260,6 +264,14 @@ class CGSolver:
         st = self._st()
         lib, ws = self.lib, _lib.ptr(self.ws_buf)
         J = self.cfg.ls_max_iter + 1
+        J1 = min(J, ARMIJO_J1)
+        main = torch.cuda.current_stream(self.device)
+        self._side.wait_stream(main)
+        with torch.cuda.stream(self._side):
+            _lib.check(lib.mrb_tv_multi(self.nd, self._Sarr, self.F, self._terms_arr, self.nterms,
+                                        _lib.ptr(self.x), _lib.ptr(self.d), _lib.ptr(self.ts), J1,
+                                        self._slot(S_DONE), self._slot(S_EJ), _lib.ptr(self.ws_side),
+                                        _lib.stream_ptr(self.device)), "tv_multi")
         if self._toep is not None:
             self._toep.AHA(self.d, out=self.gAd)
             _lib.check(lib.mrb_dots_f64(self.n_img, 2, self._dot_a, self._dot_b, self._dot_w, 0,
@@ -269,12 +281,9 @@ class CGSolver:
             _lib.check(lib.mrb_kspace_pass(0, self.n_k, _lib.ptr(self.r), _lib.ptr(self.Ad), None, None, None,
                                            0.0, self._slot(S_DONE), self._slot(S_ERR), ws, st), "kspace_pass")
             self._AH(self.Ad, self.gAd)
-        # Armijo in two phases: the TV energies of the first ARMIJO_J1 trial steps,
-        # the rest only when none of those is accepted (device-side skip)
-        J1 = min(J, ARMIJO_J1)
-        _lib.check(lib.mrb_tv_multi(self.nd, self._Sarr, self.F, self._terms_arr, self.nterms, _lib.ptr(self.x),
-                                    _lib.ptr(self.d), _lib.ptr(self.ts), J1, self._slot(S_DONE), self._slot(S_EJ),
-                                    ws, st), "tv_multi")
+        # Armijo in two phases: the TV energies of the first ARMIJO_J1 trial steps
+        # (side stream, above), the rest only when none of those is accepted
+        main.wait_stream(self._side)
         _lib.check(lib.mrb_ncg_armijo_phase(_lib.ptr(self.s), _lib.ptr(self.cfg_dev), J1, 1, st), "armijo 1")
         if J > J1:
             _lib.check(lib.mrb_tv_multi(self.nd, self._Sarr, self.F, self._terms_arr, self.nterms,
