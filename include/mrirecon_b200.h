@@ -66,7 +66,10 @@ int mrb_plan_destroy(mrb_plan* plan);
  * key 3 = samples per spread work item (heavy tiles are split),
  * key 4 = FFT mode: 0 dense cuFFT transform with separate pad / crop kernels,
  *         1 fused zero-pruned row / column passes (2D grids whose sides have
- *         compiled kernels; the default wherever available). */
+ *         compiled kernels; the default wherever available),
+ * key 5 = 3D forward interp on a coil-interleaved copy of the grid (1, the 3D
+ *         default: a tiled transpose then 128-bit gathers of all coils of a
+ *         cell; costs one more grid-sized buffer) or on the planar grid (0). */
 int mrb_plan_set_option(mrb_plan* plan, int key, int64_t value);
 
 /* Trajectory (dev, (B, nd, K) float32 radians in [-pi, pi)): float32 grid

@@ -78,6 +78,8 @@ struct mrb_plan {
   const float2* tw0p = nullptr;
   const float2* tw1p = nullptr;
   const double* skip = nullptr;   // device flag: operator kernels return when it is non-zero
+  int il = 0;         // 1: forward interp reads a coil-interleaved copy of the grid (3D, cuFFT mode)
+  DevBuf grid_il;     // (nb, gtot, C) float2, written by the transpose at the start of the interp stage
   DevBuf psf;         // Toeplitz transfer functions (B, G0, G1) float (mrb_plan_set_toeplitz)
   DevBuf ones;        // S0 + S1 ones: the row passes without deapodisation
   bool have_psf = false;
@@ -499,6 +501,118 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly
       yo[(long long)c * g.K] = make_float2(re * s, im * s);
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// 3D forward interp on a coil-interleaved grid.  The dense cuFFT leaves the
+// oversampled grid planar, (be, coil, cell); a 64-tap gather from it touches
+// 64 x C scattered 8-byte values per sample, a quarter of every 32-byte sector.
+// The interp stage first rewrites the grid as (be, cell, coil) with a
+// shared-memory tiled transpose (one read and one write of the grid, both
+// coalesced), then gathers with one thread per (sample, coil pair): the
+// threads of a sample read the C coils of a cell as one contiguous run
+// (C = 16: one 128-byte line per tap), 128-bit loads when C is even.
+// ---------------------------------------------------------------------------
+constexpr int TR_CELLS = 64;    // cells per transpose block
+constexpr int TR_COILS = 16;    // coils per shared tile pass
+
+__global__ void __launch_bounds__(256) coil_interleave_kernel(const float2* __restrict__ in, float2* __restrict__ out,
+                                                              long long gtot, int C, const double* skip) {
+  if (skip != nullptr && *skip != 0.0) return;   // solve already finished
+  __shared__ float2 tile[TR_COILS][TR_CELLS + 1];
+  const long long cell0 = (long long)blockIdx.x * TR_CELLS;
+  const long long be = blockIdx.y;
+  const float2* src = in + be * C * gtot;
+  float2* dst = out + be * C * gtot;
+  const int ncell = (int)min((long long)TR_CELLS, gtot - cell0);
+  for (int c0 = 0; c0 < C; c0 += TR_COILS) {
+    const int cc = min(TR_COILS, C - c0);
+    for (int e = threadIdx.x; e < cc * TR_CELLS; e += blockDim.x) {
+      const int c = e / TR_CELLS, l = e - c * TR_CELLS;
+      if (l < ncell) tile[c][l] = src[(long long)(c0 + c) * gtot + cell0 + l];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < cc * TR_CELLS; e += blockDim.x) {
+      const int l = e / cc, c = e - l * cc;
+      if (l < ncell) dst[(cell0 + l) * C + c0 + c] = tile[c][l];
+    }
+    __syncthreads();
+  }
+}
+
+template <bool V4>
+__global__ void __launch_bounds__(256) interp3_il_kernel(InterpArgs a, Geo g, KBPoly kb) {
+  constexpr int W = 4;
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+  const int P = (g.C + 1) >> 1;   // coil pairs
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int be = blockIdx.y;
+  if (t >= g.K * P) return;
+  const long long k = t / P;
+  const int pr = (int)(t - k * P);
+  const int b = frame_of(be, a.nb, g.B);
+  float w[3][W];
+  int nidx[3][W];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const float x = a.gx[((long long)b * 3 + d) * g.K + k];
+    const int base = (int)floorf(x);
+#pragma unroll
+    for (int o = 0; o < W; ++o) {
+      const int n = base - (W / 2 - 1) + o;
+      const float wd = mrb::kb_eval(kb, x - (float)n);
+      w[d][o] = (n & 1) ? -wd : wd;
+      nidx[d][o] = mrb::wrap_i(n, g.G[d]);
+    }
+  }
+  float s = a.scale * a.gsign;
+  if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
+  const int c0 = 2 * pr;
+  const bool two = c0 + 1 < g.C;
+  const float2* gb = a.grid + (long long)be * g.C * g.gtot + c0;
+  float re0 = 0.f, im0 = 0.f, re1 = 0.f, im1 = 0.f;
+#pragma unroll
+  for (int i0 = 0; i0 < W; ++i0) {
+    float4 v[W][W];
+#pragma unroll
+    for (int i1 = 0; i1 < W; ++i1) {
+      const long long row = ((long long)nidx[0][i0] * g.G[1] + nidx[1][i1]) * g.G[2];
+#pragma unroll
+      for (int i2 = 0; i2 < W; ++i2) {
+        const float2* q = gb + (row + nidx[2][i2]) * g.C;
+        if (V4) {
+          v[i1][i2] = __ldg(reinterpret_cast<const float4*>(q));
+        } else {
+          const float2 u0 = __ldg(q);
+          const float2 u1 = two ? __ldg(q + 1) : make_float2(0.f, 0.f);
+          v[i1][i2] = make_float4(u0.x, u0.y, u1.x, u1.y);
+        }
+      }
+    }
+    float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
+#pragma unroll
+    for (int i1 = 0; i1 < W; ++i1) {
+      float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
+#pragma unroll
+      for (int i2 = 0; i2 < W; ++i2) {
+        a0 = fmaf(w[2][i2], v[i1][i2].x, a0);
+        b0 = fmaf(w[2][i2], v[i1][i2].y, b0);
+        a1 = fmaf(w[2][i2], v[i1][i2].z, a1);
+        b1 = fmaf(w[2][i2], v[i1][i2].w, b1);
+      }
+      r0 = fmaf(w[1][i1], a0, r0);
+      m0 = fmaf(w[1][i1], b0, m0);
+      r1 = fmaf(w[1][i1], a1, r1);
+      m1 = fmaf(w[1][i1], b1, m1);
+    }
+    re0 = fmaf(w[0][i0], r0, re0);
+    im0 = fmaf(w[0][i0], m0, im0);
+    re1 = fmaf(w[0][i0], r1, re1);
+    im1 = fmaf(w[0][i0], m1, im1);
+  }
+  float2* yo = a.y + ((long long)be * g.C + c0) * g.K + k;
+  yo[0] = make_float2(re0 * s, im0 * s);
+  if (two) yo[g.K] = make_float2(re1 * s, im1 * s);
 }
 
 // ---------------------------------------------------------------------------
@@ -989,6 +1103,7 @@ extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int 
   if (!rc && cudaMemcpy(p->invdeap.p, dap.data(), dap.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
     rc = mrb::fail(MRB_ECUDA, "copying deapodisation failed");
   if (!rc && nd == 2 && mrb::fft2_supported(p->S[0], p->S[1], p->G[0], p->G[1])) rc = mrb_plan_set_option(p, 4, 1);
+  if (!rc && nd == 3) p->il = 1;
   if (rc) {
     delete p;
     return rc;
@@ -1001,7 +1116,7 @@ extern "C" int mrb_plan_destroy(mrb_plan* p) {
   if (!p) return 0;
   if (p->fft) cufftDestroy(p->fft);
   for (DevBuf* b : {&p->gx, &p->entries, &p->tile_start, &p->items, &p->multi, &p->partials, &p->empty_keys, &p->maps, &p->invdeap, &p->wfwd,
-                    &p->wadj, &p->grid, &p->tmp, &p->band, &p->tw0, &p->tw1, &p->psf, &p->ones})
+                    &p->wadj, &p->grid, &p->tmp, &p->band, &p->tw0, &p->tw1, &p->psf, &p->ones, &p->grid_il})
     b->release();
   delete p;
   return 0;
@@ -1041,6 +1156,11 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
         }
       }
       p->fft_mode = (int)value;
+      return 0;
+    case 5:
+      MRB_REQUIRE(value == 0 || value == 1, "interleaved interp must be 0 or 1");
+      MRB_REQUIRE(value == 0 || p->nd == 3, "the interleaved interp is 3D only");
+      p->il = (int)value;
       return 0;
     default:
       return mrb::fail(MRB_EINVAL, "unknown option %d", key);
@@ -1234,6 +1354,7 @@ static int ensure_grid(mrb_plan* p, int nb) {
   int rc = p->grid.ensure(bytes);
   if (rc) return rc;
   if (p->fft_mode == 1) return p->band.ensure(mrb::fft2_tmp_bytes(p->S[0], p->G[1], p->C, nb));
+  if (p->il && (rc = p->grid_il.ensure(bytes))) return rc;
   return ensure_fft(p, nb);
 }
 
@@ -1290,6 +1411,22 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     a.nb = nb;
     a.scale = p->scale;
     a.gsign = p->gsign;
+    if (p->il && p->nd == 3) {
+      MRB_REQUIRE(nb <= 65535, "too many frames in one call");
+      const long long tb = (p->gtot() + TR_CELLS - 1) / TR_CELLS;
+      MRB_REQUIRE(tb < (1LL << 31), "grid too large for the coil transpose");
+      coil_interleave_kernel<<<dim3((unsigned)tb, nb), 256, 0, st>>>(p->grid.as<float2>(), p->grid_il.as<float2>(),
+                                                                     p->gtot(), p->C, p->skip);
+      MRB_LAUNCH_CHECK();
+      a.grid = p->grid_il.as<float2>();
+      const long long nt = p->K * ((p->C + 1) / 2);
+      MRB_REQUIRE((nt + 255) / 256 < (1LL << 31), "too many samples for the interleaved interp");
+      dim3 grid(grid_blocks(nt, 256), nb);
+      if (p->C % 2 == 0) interp3_il_kernel<true><<<grid, 256, 0, st>>>(a, g, p->kb);
+      else interp3_il_kernel<false><<<grid, 256, 0, st>>>(a, g, p->kb);
+      MRB_LAUNCH_CHECK();
+      return 0;
+    }
     dim3 grid(grid_blocks(p->K, 256), nb);
     if (p->nd == 2) interp_kernel<2><<<grid, 256, 0, st>>>(a, g, p->kb);
     else interp_kernel<3><<<grid, 256, 0, st>>>(a, g, p->kb);

@@ -31,7 +31,7 @@ from .layout import (AxisSpec, plan_image_layout, plan_kspace_layout, plan_image
                      plan_kspace_layout_from_sizes, user_image_shape, user_kspace_shape)
 from .roles import Roles
 
-OPT_TILE, OPT_COILS_PER_ITEM, OPT_INTERP_MODE, OPT_CHUNK, OPT_FFT_MODE = 0, 1, 2, 3, 4
+OPT_TILE, OPT_COILS_PER_ITEM, OPT_INTERP_MODE, OPT_CHUNK, OPT_FFT_MODE, OPT_INTERLEAVE = 0, 1, 2, 3, 4, 5
 FFT_CUFFT, FFT_FUSED = 0, 1
 _DCF_MODES = {"none": 0, "balanced": 1, "standard": 2}
 
@@ -192,6 +192,7 @@ class B200NUFFTAdapter:
     coils_per_item: Optional[int] = None
     chunk: Optional[int] = None
     fft_mode: Optional[int] = None
+    interleave: Optional[int] = None   # 3D: interp on a coil-interleaved grid copy (default 1)
     autotune: bool = False
     tuned: Optional[dict] = None
 
@@ -258,6 +259,8 @@ class B200NUFFTAdapter:
                 plan.set_option(OPT_CHUNK, self.chunk)
             if self.fft_mode is not None:
                 plan.set_option(OPT_FFT_MODE, self.fft_mode)
+            if self.interleave is not None:
+                plan.set_option(OPT_INTERLEAVE, self.interleave)
             plan.set_points(self._traj_BndK)
             plan.set_dcf(self._dcf_BK, self.dcf_mode, self.apply_dcf_in_fwd, self.apply_dcf_in_adj)
             plan.set_maps(self._maps)
