@@ -20,8 +20,10 @@ import torch
 
 CANDIDATES_2D: Tuple[Tuple[int, int, int], ...] = (
     (16, 4, 128), (16, 4, 512), (16, 6, 128), (16, 2, 128), (8, 4, 64), (8, 6, 128), (16, 4, 32), (32, 2, 128))
+# 3D tile 8 runs the block-per-tile kernel (coils per block fixed at 16): only
+# the chunk matters there; tile 4 runs the per-warp kernel
 CANDIDATES_3D: Tuple[Tuple[int, int, int], ...] = (
-    (8, 2, 256), (8, 1, 256), (8, 4, 256), (8, 2, 64), (4, 4, 256), (4, 8, 256))
+    (8, 16, 4096), (8, 16, 1024), (8, 16, 16384), (8, 16, 256), (4, 4, 256), (4, 8, 256))
 
 
 def _cache_path() -> str:

@@ -84,7 +84,6 @@ struct mrb_plan {
   DevBuf ones;        // S0 + S1 ones: the row passes without deapodisation
   bool have_psf = false;
   DevBuf tmp;         // scratch for set_points
-  size_t spread_smem_set = 0;   // dynamic smem opt-in already granted
 
   int64_t gtot() const {
     int64_t t = 1;
@@ -859,6 +858,168 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
   }
 }
 
+// 3D adjoint spread, one block per work item (8^3 tile, chunk of its sample
+// list, group of up to 16 coils).  The per-warp kernel above repeats the tap
+// arithmetic once per coil group and walks all 64 taps of every sample visit;
+// in 3D that is most of its time.  Here the coils of a group share one
+// shared-memory tile [cell][coil pair] and the sample staging: each batch of
+// samples is loaded once per block (weights computed once, 64 x (dim) kernel
+// evaluations per batch, coil values read coalesced along the sample list).
+// Warp w owns the tile plane l0 = w, so warps never write the same cell and
+// need no atomics: for a sample whose support meets plane w, lanes are
+// (coil pair p, tap a2) and the loop runs over a1 (a warp-uniform row test
+// skips rows outside the tile).  A quarter warp updates the PPL coil pairs of
+// one cell: 16 * PPL contiguous bytes, free of bank conflicts.  The staged
+// coil values are XOR-swizzled by sample so that the staging stores conflict
+// at most 4-way.  Summation order per (cell, coil) is the sample-list order,
+// as in the per-warp kernel: both give identical grids.
+// ---------------------------------------------------------------------------
+constexpr int S3_T = 8;         // tile edge (cells)
+constexpr int S3_WARPS = 8;     // one warp per tile plane
+constexpr int S3_BATCH = 32;    // samples staged per pass (3 blocks of 70 KB per SM)
+constexpr int S3_CPB = 16;      // coils per block (group)
+
+template <int PPL>
+struct Spread3Smem {
+  static constexpr int CELLS = S3_T * S3_T * S3_T;
+  static constexpr int CPS = 2 * PPL;   // float2 per cell
+  static constexpr size_t ACC = (size_t)CELLS * CPS * sizeof(float2);
+  static constexpr size_t BYTES = ACC + S3_BATCH * (sizeof(int4) + 12 * sizeof(float)) +
+                                  (size_t)S3_BATCH * CPS * sizeof(float2);
+};
+
+template <int PPL>
+__global__ void __launch_bounds__(S3_WARPS * 32) spread3_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+  using SM = Spread3Smem<PPL>;
+  constexpr int T = S3_T;
+  constexpr int CPS = SM::CPS;
+  constexpr int TPI = 32 / PPL;        // taps (a1, a2) per lane pass
+  constexpr int ROWS = TPI / 4;        // a1 rows per lane pass
+  extern __shared__ float4 smem4[];
+  float4* acc4 = smem4;                                             // [cell][pair]
+  int4* sb = reinterpret_cast<int4*>(reinterpret_cast<char*>(smem4) + SM::ACC);
+  float* sw = reinterpret_cast<float*>(sb + S3_BATCH);
+  float4* sy4 = reinterpret_cast<float4*>(sw + S3_BATCH * 12);     // [sample][pair slot]
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long item = blockIdx.x;
+  const int grp = (int)(item % a.ngroups);
+  const long long oi = item / a.ngroups;
+  const int4 it = a.items[oi % a.n_items];
+  const int rep = (int)(oi / a.n_items);
+  const int b = it.x / tg.ntiles;
+  const int tile = it.x - b * tg.ntiles;
+  const int be = (g.B == 1) ? rep : b * (a.nb / g.B) + rep;
+  const int c0 = grp * a.cpi;
+  const int nc = min(a.cpi, g.C - c0);
+  const int o2 = (tile % tg.nt[2]) * T;
+  const int o1 = ((tile / tg.nt[2]) % tg.nt[1]) * T;
+  const int o0 = (tile / (tg.nt[2] * tg.nt[1])) * T;
+  const int k0 = a.tile_start[it.x], k1 = a.tile_start[it.x + 1];
+  const int e0 = min(k1, k0 + it.y * a.chunk), e1 = min(k1, e0 + a.chunk);
+  constexpr int TN = T * T * T;
+  float2* pout = it.z >= 0 ? a.partials + (((long long)rep * a.n_slots + it.z) * g.C + c0) * TN : nullptr;
+
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = threadIdx.x; i < SM::CELLS * PPL; i += blockDim.x) acc4[i] = z4;
+
+  // this warp's plane; lanes (pair p, tap sub q)
+  const int P0 = o0 + warp;
+  const int p = lane % PPL, q = lane / PPL;
+  const int a2 = q & 3, arow = q >> 2;
+  const float* gxp = a.gx + (long long)b * 3 * g.K;
+  const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
+
+  for (int e = e0; e < e1; e += S3_BATCH) {
+    const int nbat = min(S3_BATCH, e1 - e);
+    __syncthreads();   // previous batch consumed (and the zero fill done)
+    // stage: (sample, dim) weights, then coil values
+    for (int i = threadIdx.x; i < nbat * 3; i += blockDim.x) {
+      const int j = i / 3, d = i - 3 * j;
+      const int k = a.entries[e + j];
+      const float x = gxp[(long long)d * g.K + k];
+      const int base = (int)floorf(x) - 1;
+      float ws = 1.f;
+      if (d == 0) {
+        ws = a.gsign;
+        if (a.wadj) ws *= a.wadj[(long long)b * g.K + k];
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int n = base + t;
+        float w = mrb::kb_eval(kb, x - (float)n);
+        if (n & 1) w = -w;
+        sw[j * 12 + d * 4 + t] = w * ws;
+      }
+      reinterpret_cast<int*>(sb + j)[d] = base;
+    }
+    for (int i = threadIdx.x; i < S3_BATCH * CPS; i += blockDim.x) {
+      const int j = i % S3_BATCH, c = i / S3_BATCH;   // lanes along the sample list
+      float2 v = make_float2(0.f, 0.f);
+      if (j < nbat && c < nc) v = yb[(long long)c * g.K + a.entries[e + j]];
+      const int slot = (c >> 1) ^ (j & (PPL - 1));
+      reinterpret_cast<float2*>(sy4 + j * PPL + slot)[c & 1] = v;
+    }
+    __syncthreads();
+    if (P0 >= g.G[0]) continue;   // plane beyond a partial last tile: nothing lands here
+    for (int j = 0; j < nbat; ++j) {
+      const int4 bb = sb[j];
+      int d0 = P0 - bb.x;
+      d0 += d0 < 0 ? g.G[0] : 0;
+      d0 -= d0 >= g.G[0] ? g.G[0] : 0;
+      if (d0 >= 4) continue;   // warp-uniform: the sample's support misses this plane
+      int n2 = bb.z + a2;
+      n2 += n2 < 0 ? g.G[2] : 0;
+      n2 -= n2 >= g.G[2] ? g.G[2] : 0;
+      const int l2 = n2 - o2;
+      const bool in2 = (unsigned)l2 < (unsigned)T && p < (nc + 1) / 2;
+      const float* wj = sw + j * 12;
+      const float w0 = wj[d0], w2 = wj[8 + a2];
+      const float4 v = sy4[j * PPL + (p ^ (j & (PPL - 1)))];
+#pragma unroll
+      for (int r = 0; r < 4 / ROWS; ++r) {
+        const int a1 = r * ROWS + arow;
+        int n1 = bb.y + a1;
+        n1 += n1 < 0 ? g.G[1] : 0;
+        n1 -= n1 >= g.G[1] ? g.G[1] : 0;
+        const int l1 = n1 - o1;
+        if (in2 && (unsigned)l1 < (unsigned)T) {
+          const float w = w0 * wj[4 + a1] * w2;   // the per-warp kernel's product order
+          float4* c4 = acc4 + ((warp * T + l1) * T + l2) * PPL + p;
+          float4 t = *c4;
+          t.x = fmaf(w, v.x, t.x);
+          t.y = fmaf(w, v.y, t.y);
+          t.z = fmaf(w, v.z, t.z);
+          t.w = fmaf(w, v.w, t.w);
+          *c4 = t;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // write-out: lanes (coil, cell pair along l2) read whole cells from shared
+  // memory; each coil row gets 32-byte pieces
+  const float2* acc = reinterpret_cast<const float2*>(acc4);
+  float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
+  for (int i = threadIdx.x; i < (TN / 2) * CPS; i += blockDim.x) {
+    const int c = i % CPS, r = i / CPS;   // r: cell pair
+    if (c >= nc) continue;
+    const int cl = 2 * r;                  // local cell (l0, l1, l2 even)
+    const float2 u0 = acc[cl * CPS + c], u1 = acc[(cl + 1) * CPS + c];
+    const float4 v = make_float4(u0.x, u0.y, u1.x, u1.y);
+    if (pout) {
+      *reinterpret_cast<float4*>(pout + (long long)c * TN + cl) = v;
+    } else {
+      const int l0 = cl / (T * T), l1 = (cl / T) % T, l2 = cl % T;
+      const int n0 = o0 + l0, n1 = o1 + l1, n2 = o2 + l2;
+      if (n0 < g.G[0] && n1 < g.G[1] && n2 < g.G[2])
+        *reinterpret_cast<float4*>(gout + (long long)c * g.gtot + ((long long)n0 * g.G[1] + n1) * g.G[2] + n2) = v;
+    }
+  }
+}
+
 // Zeros for the tiles no sample touches: a store-only grid-stride pass, one
 // float4 (two cells) per thread, consecutive threads along tile rows.
 template <int ND, int T>
@@ -1074,6 +1235,7 @@ extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int 
   p->beta = M_PI * std::sqrt(std::pow((W / osf) * (osf - 0.5), 2) - 0.8);   // ptnufft.py:125
   mrb::kb_poly_init(p->kb, W, p->beta);
   p->tile = nd == 2 ? 16 : 8;
+  p->chunk = nd == 2 ? 128 : 4096;   // 3D: a block per item, only the centre tiles need splitting
   p->coils_per_item = nd == 2 ? std::min(C, 4) : std::min(C, 2);
   // deapodisation: closed-form FT of the truncated KB window
   std::vector<float> dap;
@@ -1358,6 +1520,21 @@ static int ensure_grid(mrb_plan* p, int nb) {
   return ensure_fft(p, nb);
 }
 
+// raise a kernel's dynamic shared-memory limit once per (kernel, size)
+static int ensure_smem(const void* fn, size_t smem) {
+  static const void* fns[32];
+  static size_t set[32];
+  static int n = 0;
+  if (smem <= 48 * 1024) return 0;
+  int i = 0;
+  while (i < n && fns[i] != fn) ++i;
+  if (i < n && set[i] >= smem) return 0;
+  MRB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (i == n && n < 32) fns[n++] = fn;
+  if (i < n) set[i] = smem;
+  return 0;
+}
+
 // one stage of the forward/adjoint pipeline; x/y are the user image / samples
 static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cudaStream_t st, int coil_images) {
   Geo g = make_geo(p);
@@ -1459,15 +1636,32 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     }
     a.partials = p->partials.as<float2>();
     a.nb = nb;
-    a.cpi = p->coils_per_item;
+    const bool blk3 = p->nd == 3 && tg.T == S3_T;   // block-per-tile 3D kernel
+    a.cpi = blk3 ? std::min(p->C, S3_CPB) : p->coils_per_item;
     a.ngroups = (p->C + a.cpi - 1) / a.cpi;
     a.gsign = p->gsign;
     long long items = (long long)reps * p->n_items * a.ngroups;
-    int blocks = grid_blocks(items, SPREAD_WARPS);
+    MRB_REQUIRE(items < (1LL << 31), "too many spread work items");
+    int blocks = blk3 ? (int)items : grid_blocks(items, SPREAD_WARPS);
     const void* fn = nullptr;
     size_t smem = 0;
+    int threads = SPREAD_WARPS * 32;
+    if (blk3) {
+      const int pairs = (a.cpi + 1) / 2;
+      threads = S3_WARPS * 32;
+      if (pairs <= 2) {
+        fn = (const void*)spread3_kernel<2>;
+        smem = Spread3Smem<2>::BYTES;
+      } else if (pairs <= 4) {
+        fn = (const void*)spread3_kernel<4>;
+        smem = Spread3Smem<4>::BYTES;
+      } else {
+        fn = (const void*)spread3_kernel<8>;
+        smem = Spread3Smem<8>::BYTES;
+      }
+    }
 #define MRB_SPREAD_CASE(ND_, T_)                                                             \
-  if (p->nd == ND_ && tg.T == T_) {                                                          \
+  if (!fn && p->nd == ND_ && tg.T == T_) {                                                   \
     fn = (const void*)spread_kernel<ND_, T_>;                                                \
     smem = SPREAD_WARPS * SpreadSmem<ND_, T_>::warp_bytes(a.cpi);                            \
   }
@@ -1480,10 +1674,7 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
 #undef MRB_SPREAD_CASE
     MRB_REQUIRE(fn != nullptr, "no spread kernel for nd=%d tile=%d", p->nd, tg.T);
     MRB_REQUIRE(smem <= 227 * 1024, "spread tile needs %zu bytes of shared memory", smem);
-    if (smem > 48 * 1024 && smem > p->spread_smem_set) {
-      MRB_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      p->spread_smem_set = smem;
-    }
+    if (int rc3 = ensure_smem(fn, smem)) return rc3;
     if (p->n_empty > 0) {
       long long zbl = (long long)reps * p->n_empty;
       MRB_REQUIRE(zbl < (1LL << 31), "too many empty tiles");
@@ -1503,7 +1694,7 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     }
     if (items > 0) {
       void* args[] = {&a, &g, &tg, &p->kb};
-      MRB_CUDA_TRY(cudaLaunchKernel(fn, dim3(blocks), dim3(SPREAD_WARPS * 32), args, smem, st));
+      MRB_CUDA_TRY(cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smem, st));
       MRB_LAUNCH_CHECK();
     }
     if (p->n_multi > 0) {

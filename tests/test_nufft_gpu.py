@@ -303,3 +303,27 @@ def test_3d_interleaved_interp_identical(cuda, C, nb):
     y1 = _adapter(maps, traj, interleave=1).A(x)
     y0 = _adapter(maps, traj, interleave=0).A(x)
     assert torch.equal(y0, y1)
+
+
+@pytest.mark.parametrize("C,chunk", [(20, None), (5, 16), (1, 64)])
+def test_3d_block_spread_vs_oracle(cuda, C, chunk):
+    """The block-per-tile 3D spread (tile 8) with two coil groups (C = 20:
+    16 + 4), an odd coil count and a single coil, with and without split tiles."""
+    S = (12, 10, 8)
+    maps = _rand_c((C,) + S, 31, torch.complex64)
+    traj = phantoms.random_traj(2, 3, 700, seed=19)
+    _check_pair(maps, traj, chunk=chunk)
+
+
+def test_3d_block_spread_matches_warp_kernel(cuda):
+    """Tile 8 (block kernel) and tile 4 (per-warp kernel) give the same grid up
+    to the summation order of split tiles; the block kernel is deterministic."""
+    S = (24, 24, 24)
+    maps = phantoms.coil_maps(24, 6, ndim=3).to(torch.complex64)
+    traj = phantoms.golden_means_koosh(200, 48).unsqueeze(0)
+    y = _rand_c((1, 6, traj.shape[-1]), 3, torch.complex64).to(cuda)
+    ref = _adapter(maps, traj, tile=4, coils_per_item=2).AH(y)
+    ad = _adapter(maps, traj, tile=8, chunk=100000)
+    out = ad.AH(y)
+    assert rel(out, ref) < 1e-6
+    assert torch.equal(out, ad.AH(y))
