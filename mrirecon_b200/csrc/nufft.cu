@@ -60,6 +60,8 @@ struct mrb_plan {
   DevBuf partials;   // chunk partial tiles (rep, slot, C, T^nd) float2
   int n_items = 0, n_multi = 0, n_slots = 0;
   DevBuf empty_keys; // (frame, tile) keys with no sample: zero-filled by a store-only kernel
+  DevBuf seg_order;  // 3D interp: (B, nseg) segments of IL_SEG consecutive samples in Morton order
+  long long nseg = 0;
   int n_empty = 0;
   int64_t n_entries = 0;
   int64_t touched = 0;
@@ -391,6 +393,8 @@ struct InterpArgs {
   int nb;
   float scale;
   float gsign;
+  const int* seg;      // 3D interleaved interp: segment visiting order (B, nseg) or null
+  long long nseg;
 };
 
 template <int ND>
@@ -513,6 +517,26 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly
 // (C = 16: one 128-byte line per tap), 128-bit loads when C is even.
 // ---------------------------------------------------------------------------
 constexpr int TR_CELLS = 64;    // cells per transpose block
+constexpr int IL_SEG = 8;       // samples per interp visiting segment
+
+// 3D visiting-order key of a segment: frame, then the Morton code of the
+// 8-cell tile holding its middle sample
+__global__ void seg_key_kernel(const float* __restrict__ gx, unsigned long long* __restrict__ keys,
+                               int* __restrict__ vals, Geo g, long long nseg, int bits) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)g.B * nseg) return;
+  const int b = (int)(i / nseg);
+  const long long s = i - (long long)b * nseg;
+  const long long k = min(s * IL_SEG + IL_SEG / 2, g.K - 1);
+  unsigned long long m = 0;
+  for (int d = 0; d < 3; ++d) {
+    int c = (int)floorf(gx[((long long)b * 3 + d) * g.K + k]);
+    c = min(max(c, 0), g.G[d] - 1) >> 3;
+    for (int q = 0; q < bits; ++q) m |= (unsigned long long)((c >> q) & 1) << (3 * q + (2 - d));
+  }
+  keys[i] = ((unsigned long long)b << (3 * bits)) | m;
+  vals[i] = (int)s;
+}
 constexpr int TR_COILS = 16;    // coils per shared tile pass
 
 __global__ void __launch_bounds__(256) coil_interleave_kernel(const float2* __restrict__ in, float2* __restrict__ out,
@@ -546,10 +570,17 @@ __global__ void __launch_bounds__(256) interp3_il_kernel(InterpArgs a, Geo g, KB
   const int P = (g.C + 1) >> 1;   // coil pairs
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int be = blockIdx.y;
-  if (t >= g.K * P) return;
-  const long long k = t / P;
-  const int pr = (int)(t - k * P);
   const int b = frame_of(be, a.nb, g.B);
+  long long k = t / P;
+  const int pr = (int)(t - k * P);
+  if (a.seg) {
+    // segments of IL_SEG consecutive samples (whole 32-byte pieces of every
+    // coil row of y) visited in the Morton order of their middle sample's tile
+    const long long ss = k / IL_SEG;
+    if (ss >= a.nseg) return;
+    k = (long long)a.seg[(long long)b * a.nseg + ss] * IL_SEG + (k - ss * IL_SEG);
+  }
+  if (k >= g.K) return;
   float w[3][W];
   int nidx[3][W];
 #pragma unroll
@@ -1236,6 +1267,7 @@ extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int 
   mrb::kb_poly_init(p->kb, W, p->beta);
   p->tile = nd == 2 ? 16 : 8;
   p->chunk = nd == 2 ? 128 : 4096;   // 3D: a block per item, only the centre tiles need splitting
+  p->interp_mode = nd == 3 ? 1 : 0;
   p->coils_per_item = nd == 2 ? std::min(C, 4) : std::min(C, 2);
   // deapodisation: closed-form FT of the truncated KB window
   std::vector<float> dap;
@@ -1278,7 +1310,8 @@ extern "C" int mrb_plan_destroy(mrb_plan* p) {
   if (!p) return 0;
   if (p->fft) cufftDestroy(p->fft);
   for (DevBuf* b : {&p->gx, &p->entries, &p->tile_start, &p->items, &p->multi, &p->partials, &p->empty_keys, &p->maps, &p->invdeap, &p->wfwd,
-                    &p->wadj, &p->grid, &p->tmp, &p->band, &p->tw0, &p->tw1, &p->psf, &p->ones, &p->grid_il})
+                    &p->wadj, &p->grid, &p->tmp, &p->band, &p->tw0, &p->tw1, &p->psf, &p->ones, &p->grid_il,
+                    &p->seg_order})
     b->release();
   delete p;
   return 0;
@@ -1446,6 +1479,40 @@ extern "C" int mrb_plan_set_points(mrb_plan* p, const float* traj, mrb_stream_t 
     }
   }
 
+  // 3D interp visiting order: segments of IL_SEG samples sorted by (frame,
+  // Morton code of the middle sample's tile), so that concurrently running
+  // blocks gather from neighbouring cells instead of re-reading each spoke's
+  // whole tube of the grid from HBM
+  p->nseg = 0;
+  if (p->nd == 3) {
+    const long long nseg = (p->K + IL_SEG - 1) / IL_SEG;
+    const long long n = (long long)p->B * nseg;
+    MRB_REQUIRE(n < (1LL << 31) && nseg < (1LL << 31), "too many interp segments");
+    int bits = 1;
+    while ((1 << bits) < (std::max(p->G[0], std::max(p->G[1], p->G[2])) + 7) / 8) ++bits;
+    int bbits = 1;
+    while ((1LL << bbits) < p->B) ++bbits;
+    const int end_bit2 = 3 * bits + bbits;
+    MRB_REQUIRE(end_bit2 <= 64, "interp order key too wide");
+    DevBuf k_in, k_out, v_in;
+    if ((rc = k_in.ensure(n * sizeof(unsigned long long)))) return rc;
+    if ((rc = k_out.ensure(n * sizeof(unsigned long long)))) return rc;
+    if ((rc = v_in.ensure(n * sizeof(int)))) return rc;
+    if ((rc = p->seg_order.ensure(n * sizeof(int)))) return rc;
+    seg_key_kernel<<<grid_blocks(n, 256), 256, 0, st>>>(p->gx.as<float>(), k_in.as<unsigned long long>(),
+                                                         v_in.as<int>(), g, nseg, bits);
+    MRB_LAUNCH_CHECK();
+    size_t tb2 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb2, k_in.as<unsigned long long>(), k_out.as<unsigned long long>(),
+                                    v_in.as<int>(), p->seg_order.as<int>(), (int)n, 0, end_bit2, st);
+    if ((rc = p->tmp.ensure(tb2))) return rc;
+    cub::DeviceRadixSort::SortPairs(p->tmp.p, tb2, k_in.as<unsigned long long>(), k_out.as<unsigned long long>(),
+                                    v_in.as<int>(), p->seg_order.as<int>(), (int)n, 0, end_bit2, st);
+    MRB_LAUNCH_CHECK();
+    MRB_CUDA_TRY(cudaStreamSynchronize(st));   // the temporaries are freed on return
+    p->nseg = nseg;
+  }
+
   // touched cells (sum over frames), for the roofline bookkeeping
   {
     long long nwords = (p->gtot() + 31) / 32;
@@ -1596,7 +1663,9 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
                                                                      p->gtot(), p->C, p->skip);
       MRB_LAUNCH_CHECK();
       a.grid = p->grid_il.as<float2>();
-      const long long nt = p->K * ((p->C + 1) / 2);
+      a.seg = p->nseg > 0 && p->interp_mode == 1 ? p->seg_order.as<int>() : nullptr;
+      a.nseg = p->nseg;
+      const long long nt = (a.seg ? p->nseg * IL_SEG : p->K) * ((p->C + 1) / 2);
       MRB_REQUIRE((nt + 255) / 256 < (1LL << 31), "too many samples for the interleaved interp");
       dim3 grid(grid_blocks(nt, 256), nb);
       if (p->C % 2 == 0) interp3_il_kernel<true><<<grid, 256, 0, st>>>(a, g, p->kb);

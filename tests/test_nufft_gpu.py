@@ -303,6 +303,10 @@ def test_3d_interleaved_interp_identical(cuda, C, nb):
     y1 = _adapter(maps, traj, interleave=1).A(x)
     y0 = _adapter(maps, traj, interleave=0).A(x)
     assert torch.equal(y0, y1)
+    # acquisition visiting order instead of the Morton segment order
+    ad = _adapter(maps, traj, interleave=1)
+    ad.plan.set_option(2, 0)
+    assert torch.equal(ad.A(x), y1)
 
 
 @pytest.mark.parametrize("C,chunk", [(20, None), (5, 16), (1, 64)])
