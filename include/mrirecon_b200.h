@@ -69,6 +69,14 @@ int mrb_plan_destroy(mrb_plan* plan);
  * key 4 = FFT mode: 0 dense cuFFT transform with separate pad / crop kernels,
  *         1 fused zero-pruned row / column passes (2D grids whose sides have
  *         compiled kernels; the default wherever available),
+ * key 6 = spread kernel: 1 one block per work item, all coils of a group
+ *         sharing the staged samples (2D tile 16, 3D tile 8; other tiles fall
+ *         back to 0; the 3D default), 0 one warp per work item and coil group
+ *         (the 2D default),
+ * key 7 = grid mask (fused FFT mode): 1 (default) the forward column pass
+ *         stores, and the adjoint column pass loads, only the grid cells inside
+ *         some sample's support (per-frame bitmaps built by set_points), and the
+ *         spread stores no zeros outside them; 0 full grid passes,
  * key 5 = 3D forward interp on a coil-interleaved copy of the grid (1, the 3D
  *         default: a tiled transpose then 128-bit gathers of all coils of a
  *         cell; costs one more grid-sized buffer) or on the planar grid (0). */
@@ -113,7 +121,8 @@ int mrb_nufft_stage(mrb_plan* plan, int stage, const void* x, void* y, int nb, m
  * out[0] = number of spread entries, out[1] = tiles per frame,
  * out[2] = touched grid cells summed over frames, out[3] = spread tile edge,
  * out[4] = coils per spread work item, out[5] = grid cells per frame,
- * out[6] = FFT mode (option key 4). */
+ * out[6] = FFT mode (option key 4), out[7] = 1 when the spread runs the
+ * block-per-tile kernel (option key 6). */
 int mrb_plan_info(mrb_plan* plan, int64_t* out, int nout);
 
 /* Toeplitz normal operator (no counterpart in the reference; its item

@@ -1,8 +1,8 @@
-"""Spread tile / coil-group / chunk autotuner.
+"""Spread tile / coil-group / chunk / kernel autotuner.
 
 For a prepared plan it times the adjoint spread stage (the kernel whose speed
 depends on the tiling; interp, pre/post and the FFT do not) for a list of
-(tile edge, coils per work item, samples per chunk) candidates on the plan's
+(tile edge, coils per work item, samples per chunk, kernel) candidates on the plan's
 own trajectory, keeps the fastest and caches the choice per size class
 (nd, image shape, frames, coils and samples per frame bucketed) and GPU name in a JSON
 file (``$MRB_TUNE_CACHE`` or ``~/.cache/mrirecon_b200/spread_tune.json``).
@@ -18,12 +18,14 @@ from typing import Dict, Iterable, Optional, Sequence, Tuple
 
 import torch
 
-CANDIDATES_2D: Tuple[Tuple[int, int, int], ...] = (
-    (16, 4, 128), (16, 4, 512), (16, 6, 128), (16, 2, 128), (8, 4, 64), (8, 6, 128), (16, 4, 32), (32, 2, 128))
-# 3D tile 8 runs the block-per-tile kernel (coils per block fixed at 16): only
-# the chunk matters there; tile 4 runs the per-warp kernel
-CANDIDATES_3D: Tuple[Tuple[int, int, int], ...] = (
-    (8, 16, 4096), (8, 16, 1024), (8, 16, 16384), (8, 16, 256), (4, 4, 256), (4, 8, 256))
+# (tile edge, coils per work item, samples per chunk, kernel): kernel 1 is the
+# block-per-tile spread (2D tile 16, 3D tile 8; up to 16 coils per block, the
+# coils-per-item entry is then unused), kernel 0 the per-warp spread
+CANDIDATES_2D: Tuple[Tuple[int, int, int, int], ...] = (
+    (16, 16, 128, 1), (16, 16, 256, 1), (16, 16, 512, 1), (16, 16, 64, 1),
+    (16, 4, 128, 0), (16, 6, 128, 0), (8, 4, 64, 0), (32, 2, 128, 0))
+CANDIDATES_3D: Tuple[Tuple[int, int, int, int], ...] = (
+    (8, 16, 4096, 1), (8, 16, 1024, 1), (8, 16, 16384, 1), (8, 16, 256, 1), (4, 4, 256, 0), (4, 8, 256, 0))
 
 
 def _cache_path() -> str:
@@ -73,43 +75,46 @@ def time_spread(plan, y: torch.Tensor, nb: int, reps: int = 5) -> float:
     return a.elapsed_time(b) / reps
 
 
-def apply(plan, traj: torch.Tensor, tile: int, cpi: int, chunk: int) -> None:
-    from .nufft import OPT_CHUNK, OPT_COILS_PER_ITEM, OPT_TILE
+def apply(plan, traj: torch.Tensor, tile: int, cpi: int, chunk: int, kernel: int = 1) -> None:
+    from .nufft import OPT_CHUNK, OPT_COILS_PER_ITEM, OPT_SPREAD_KERNEL, OPT_TILE
     plan.set_option(OPT_TILE, tile)
     plan.set_option(OPT_COILS_PER_ITEM, cpi)
     plan.set_option(OPT_CHUNK, chunk)
+    plan.set_option(OPT_SPREAD_KERNEL, kernel)
     plan.set_points(traj)
 
 
-def tune(plan, traj: torch.Tensor, candidates: Optional[Iterable[Tuple[int, int, int]]] = None,
+def tune(plan, traj: torch.Tensor, candidates: Optional[Iterable[Tuple[int, ...]]] = None,
          reps: int = 5, use_cache: bool = True) -> dict:
-    """Pick (tile, coils per item, chunk) for `plan`; leaves the plan set to it."""
+    """Pick (tile, coils per item, chunk, kernel) for `plan`; leaves the plan set to it."""
     key = size_class(plan)
     cache = _load() if use_cache else {}
-    if use_cache and key in cache:
+    if use_cache and key in cache and "kernel" in cache[key]:
         c = cache[key]
-        apply(plan, traj, c["tile"], c["cpi"], c["chunk"])
+        apply(plan, traj, c["tile"], c["cpi"], c["chunk"], c["kernel"])
         return dict(c, cached=True)
     if candidates is None:
         candidates = CANDIDATES_2D if plan.nd == 2 else CANDIDATES_3D
     g = torch.Generator(device=plan.device).manual_seed(0)
     y = torch.randn((plan.B, plan.C, plan.K), dtype=torch.complex64, device=plan.device, generator=g)
     results = []
-    for tile, cpi, chunk in candidates:
+    for cand in candidates:
+        tile, cpi, chunk = cand[:3]
+        kernel = cand[3] if len(cand) > 3 else 0
         if tile < 4 or min(plan.G) < tile:
             continue
         try:
-            apply(plan, traj, tile, min(cpi, plan.C), chunk)
-            results.append((time_spread(plan, y, plan.B, reps), tile, min(cpi, plan.C), chunk))
+            apply(plan, traj, tile, min(cpi, plan.C), chunk, kernel)
+            results.append((time_spread(plan, y, plan.B, reps), tile, min(cpi, plan.C), chunk, kernel))
         except RuntimeError:
             continue                     # e.g. shared memory above the per-block limit
     if not results:
         raise RuntimeError("no spread configuration could be timed")
-    ms, tile, cpi, chunk = min(results)
-    apply(plan, traj, tile, cpi, chunk)
-    best = {"tile": tile, "cpi": cpi, "chunk": chunk, "ms": ms,
-            "tried": [{"tile": t, "cpi": c, "chunk": h, "ms": m} for m, t, c, h in sorted(results)]}
+    ms, tile, cpi, chunk, kernel = min(results)
+    apply(plan, traj, tile, cpi, chunk, kernel)
+    best = {"tile": tile, "cpi": cpi, "chunk": chunk, "kernel": kernel, "ms": ms,
+            "tried": [{"tile": t, "cpi": c, "chunk": h, "kernel": kk, "ms": m} for m, t, c, h, kk in sorted(results)]}
     if use_cache:
-        cache[key] = {k: best[k] for k in ("tile", "cpi", "chunk", "ms")}
+        cache[key] = {k: best[k] for k in ("tile", "cpi", "chunk", "kernel", "ms")}
         _store(cache)
     return best

@@ -48,6 +48,13 @@ struct mrb_plan {
   int tile = 16;
   int coils_per_item = 4;
   int interp_mode = 0;
+  int spread_kernel = 1;   // 1: block-per-tile kernels (2D tile 16, 3D tile 8) where they apply (3D default)
+  int grid_mask = 1;       // fused FFT mode: the spread stores only cell pairs inside some support
+  DevBuf touch;            // (B, twords) bitmaps of the cells inside some sample's support
+  long long twords = 0;
+  DevBuf grid_adj;         // fused mode with the mask: the spread's own grid, zero outside the supports
+  bool adj_zero = false;   // grid_adj holds zeros outside the current supports
+  int adj_nb = 0;          // ... for this batch (the frame of slot be depends on it)
   int chunk = 128;     // samples per spread work item (heavy tiles are split)
   // state
   bool have_points = false;
@@ -673,7 +680,15 @@ struct SpreadArgs {
   int cpi;     // coils per work item
   int ngroups; // ceil(C / cpi)
   float gsign;
+  const unsigned* touch;   // per-frame touched-cell bitmaps: grid cells outside them are not stored
+  long long twords;
 };
+
+// a tile's cell pair (cell, cell + 1; cell even) holds a touched cell, or no bitmap is in use
+__device__ __forceinline__ bool pair_touched(const SpreadArgs& a, int b, long long cell) {
+  if (a.touch == nullptr) return true;
+  return (__ldg(a.touch + (long long)b * a.twords + (cell >> 5)) >> (cell & 31)) & 3u;
+}
 
 constexpr int SPREAD_WARPS = 4;
 constexpr int SPREAD_BATCH = 32;
@@ -760,6 +775,7 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
   };
 
   if (e0 == e1 && !pout) {   // no sample touches this tile: zeros
+    if (a.touch) return;     // its cells are outside every support and never read
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int i = lane; i < nc * PAIRS; i += 32) {
       int cl = i / PAIRS, r = i - cl * PAIRS;
@@ -874,7 +890,7 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
     const float4 a1 = reinterpret_cast<const float4*>(acc + (cl0 + 1) * cps)[pr];
     int n[3];
     const long long cell = cell_of_pair(r, n);
-    const bool ok = in_grid(n);
+    const bool ok = in_grid(n) && (pout || pair_touched(a, b, cell));
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int cl = 2 * pr + h;
@@ -994,12 +1010,20 @@ __global__ void __launch_bounds__(S3_WARPS * 32) spread3_kernel(SpreadArgs a, Ge
     }
     __syncthreads();
     if (P0 >= g.G[0]) continue;   // plane beyond a partial last tile: nothing lands here
-    for (int j = 0; j < nbat; ++j) {
+    // lane j tests sample j against this warp's plane; the warp then visits
+    // only the samples whose support meets it
+    int myd0 = 4;
+    if (lane < nbat) {
+      myd0 = P0 - sb[lane].x;
+      myd0 += myd0 < 0 ? g.G[0] : 0;
+      myd0 -= myd0 >= g.G[0] ? g.G[0] : 0;
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, myd0 < 4);
+    while (todo) {
+      const int j = __ffs(todo) - 1;
+      todo &= todo - 1;
       const int4 bb = sb[j];
-      int d0 = P0 - bb.x;
-      d0 += d0 < 0 ? g.G[0] : 0;
-      d0 -= d0 >= g.G[0] ? g.G[0] : 0;
-      if (d0 >= 4) continue;   // warp-uniform: the sample's support misses this plane
+      const int d0 = __shfl_sync(0xffffffffu, myd0, j);
       int n2 = bb.z + a2;
       n2 += n2 < 0 ? g.G[2] : 0;
       n2 -= n2 >= g.G[2] ? g.G[2] : 0;
@@ -1047,6 +1071,165 @@ __global__ void __launch_bounds__(S3_WARPS * 32) spread3_kernel(SpreadArgs a, Ge
       const int n0 = o0 + l0, n1 = o1 + l1, n2 = o2 + l2;
       if (n0 < g.G[0] && n1 < g.G[1] && n2 < g.G[2])
         *reinterpret_cast<float4*>(gout + (long long)c * g.gtot + ((long long)n0 * g.G[1] + n1) * g.G[2] + n2) = v;
+    }
+  }
+}
+
+// 2D adjoint spread, one block per work item (16x16 tile, chunk of its sample
+// list, group of up to 16 coils): the 2D counterpart of spread3_kernel.  Warp
+// w owns tile rows 2w and 2w+1; lanes are (coil pair p, tap column a1) and a
+// lane pass covers 8 / PPL tap rows.  Staging (coordinates, 8 kernel weights,
+// coil values) is done once per block for all coils of the group.  Per
+// (cell, coil) the samples are summed in sample-list order with the per-warp
+// kernel's weight product, so both kernels give identical grids.
+// ---------------------------------------------------------------------------
+constexpr int S2_T = 16;
+constexpr int S2_WARPS = 8;
+constexpr int S2_RPW = S2_T / S2_WARPS;   // tile rows per warp
+constexpr int S2_BATCH = 32;
+
+template <int PPL>
+struct Spread2Smem {
+  static constexpr int CELLS = S2_T * S2_T;
+  static constexpr int CPS = 2 * PPL;
+  static constexpr size_t ACC = (size_t)CELLS * CPS * sizeof(float2);
+  static constexpr size_t BYTES = ACC + S2_BATCH * (sizeof(int4) + 8 * sizeof(float)) +
+                                  (size_t)S2_BATCH * CPS * sizeof(float2);
+};
+
+template <int PPL>
+__global__ void __launch_bounds__(S2_WARPS * 32) spread2_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+  using SM = Spread2Smem<PPL>;
+  constexpr int T = S2_T;
+  constexpr int CPS = SM::CPS;
+  constexpr int RI = 8 / PPL;   // tap rows per lane pass
+  extern __shared__ float4 smem4[];
+  float4* acc4 = smem4;                                             // [cell][pair]
+  int4* sb = reinterpret_cast<int4*>(reinterpret_cast<char*>(smem4) + SM::ACC);
+  float* sw = reinterpret_cast<float*>(sb + S2_BATCH);
+  float4* sy4 = reinterpret_cast<float4*>(sw + S2_BATCH * 8);      // [sample][pair slot]
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long item = blockIdx.x;
+  const int grp = (int)(item % a.ngroups);
+  const long long oi = item / a.ngroups;
+  const int4 it = a.items[oi % a.n_items];
+  const int rep = (int)(oi / a.n_items);
+  const int b = it.x / tg.ntiles;
+  const int tile = it.x - b * tg.ntiles;
+  const int be = (g.B == 1) ? rep : b * (a.nb / g.B) + rep;
+  const int c0 = grp * a.cpi;
+  const int nc = min(a.cpi, g.C - c0);
+  const int o0 = (tile / tg.nt[1]) * T;
+  const int o1 = (tile % tg.nt[1]) * T;
+  const int k0 = a.tile_start[it.x], k1 = a.tile_start[it.x + 1];
+  const int e0 = min(k1, k0 + it.y * a.chunk), e1 = min(k1, e0 + a.chunk);
+  constexpr int TN = T * T;
+  float2* pout = it.z >= 0 ? a.partials + (((long long)rep * a.n_slots + it.z) * g.C + c0) * TN : nullptr;
+
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = threadIdx.x; i < SM::CELLS * PPL; i += blockDim.x) acc4[i] = z4;
+
+  const int R0 = o0 + warp * S2_RPW;   // the warp's first grid row
+  const int p = lane % PPL, q = lane / PPL;
+  const int a1 = q & 3, rsub = q >> 2;
+  const bool pair_ok = p < (nc + 1) / 2;
+  const float* gxp = a.gx + (long long)b * 2 * g.K;
+  const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
+
+  for (int e = e0; e < e1; e += S2_BATCH) {
+    const int nbat = min(S2_BATCH, e1 - e);
+    __syncthreads();   // previous batch consumed (and the zero fill done)
+    for (int i = threadIdx.x; i < nbat * 2; i += blockDim.x) {
+      const int j = i >> 1, d = i & 1;
+      const int k = a.entries[e + j];
+      const float x = gxp[(long long)d * g.K + k];
+      const int base = (int)floorf(x) - 1;
+      float ws = 1.f;
+      if (d == 0) {
+        ws = a.gsign;
+        if (a.wadj) ws *= a.wadj[(long long)b * g.K + k];
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int n = base + t;
+        float w = mrb::kb_eval(kb, x - (float)n);
+        if (n & 1) w = -w;
+        sw[j * 8 + d * 4 + t] = w * ws;
+      }
+      reinterpret_cast<int*>(sb + j)[d] = base;
+    }
+    for (int i = threadIdx.x; i < S2_BATCH * CPS; i += blockDim.x) {
+      const int j = i % S2_BATCH, c = i / S2_BATCH;   // lanes along the sample list
+      float2 v = make_float2(0.f, 0.f);
+      if (j < nbat && c < nc) v = yb[(long long)c * g.K + a.entries[e + j]];
+      const int slot = (c >> 1) ^ (j & (PPL - 1));
+      reinterpret_cast<float2*>(sy4 + j * PPL + slot)[c & 1] = v;
+    }
+    __syncthreads();
+    if (R0 >= g.G[0]) continue;   // rows beyond a partial last tile: nothing lands here
+    // lane j tests sample j against this warp's rows; the warp then visits
+    // only the samples whose support meets them
+    int myd0 = 4;
+    bool hit = false;
+    if (lane < nbat) {
+      myd0 = R0 - sb[lane].x;
+      myd0 += myd0 < 0 ? g.G[0] : 0;
+      myd0 -= myd0 >= g.G[0] ? g.G[0] : 0;
+      hit = myd0 < 4 || myd0 + S2_RPW - 1 >= g.G[0];
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, hit);
+    while (todo) {
+      const int j = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int4 bb = sb[j];
+      const int d0 = __shfl_sync(0xffffffffu, myd0, j);
+      int n1 = bb.y + a1;
+      n1 += n1 < 0 ? g.G[1] : 0;
+      n1 -= n1 >= g.G[1] ? g.G[1] : 0;
+      const int l1 = n1 - o1;
+      const bool in1 = pair_ok && (unsigned)l1 < (unsigned)T;
+      const float* wj = sw + j * 8;
+      const float w1 = wj[4 + a1];
+      const float4 v = sy4[j * PPL + (p ^ (j & (PPL - 1)))];
+#pragma unroll
+      for (int r0 = 0; r0 < S2_RPW; r0 += RI) {
+        const int r = r0 + rsub;
+        int a0 = d0 + r;
+        a0 -= a0 >= g.G[0] ? g.G[0] : 0;
+        if (in1 && r < S2_RPW && a0 < 4 && R0 + r < g.G[0]) {
+          const float w = wj[a0] * w1;   // the per-warp kernel's product order
+          float4* c4 = acc4 + ((warp * S2_RPW + r) * T + l1) * PPL + p;
+          float4 t = *c4;
+          t.x = fmaf(w, v.x, t.x);
+          t.y = fmaf(w, v.y, t.y);
+          t.z = fmaf(w, v.z, t.z);
+          t.w = fmaf(w, v.w, t.w);
+          *c4 = t;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // write-out: lanes (coil, cell pair along the row) read whole cells from
+  // shared memory; each coil row gets 32-byte pieces
+  const float2* acc = reinterpret_cast<const float2*>(acc4);
+  float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
+  for (int i = threadIdx.x; i < (TN / 2) * CPS; i += blockDim.x) {
+    const int c = i % CPS, r = i / CPS;
+    if (c >= nc) continue;
+    const int cl = 2 * r;
+    const float2 u0 = acc[cl * CPS + c], u1 = acc[(cl + 1) * CPS + c];
+    const float4 v = make_float4(u0.x, u0.y, u1.x, u1.y);
+    if (pout) {
+      *reinterpret_cast<float4*>(pout + (long long)c * TN + cl) = v;
+    } else {
+      const int n0 = o0 + cl / T, n1 = o1 + cl % T;
+      const long long cell = (long long)n0 * g.G[1] + n1;
+      if (n0 < g.G[0] && n1 < g.G[1] && pair_touched(a, b, cell))
+        *reinterpret_cast<float4*>(gout + (long long)c * g.gtot + cell) = v;
     }
   }
 }
@@ -1268,6 +1451,7 @@ extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int 
   p->tile = nd == 2 ? 16 : 8;
   p->chunk = nd == 2 ? 128 : 4096;   // 3D: a block per item, only the centre tiles need splitting
   p->interp_mode = nd == 3 ? 1 : 0;
+  p->spread_kernel = nd == 3 ? 1 : 0;   // 2D: the per-warp kernel is faster at typical coil counts
   p->coils_per_item = nd == 2 ? std::min(C, 4) : std::min(C, 2);
   // deapodisation: closed-form FT of the truncated KB window
   std::vector<float> dap;
@@ -1311,7 +1495,7 @@ extern "C" int mrb_plan_destroy(mrb_plan* p) {
   if (p->fft) cufftDestroy(p->fft);
   for (DevBuf* b : {&p->gx, &p->entries, &p->tile_start, &p->items, &p->multi, &p->partials, &p->empty_keys, &p->maps, &p->invdeap, &p->wfwd,
                     &p->wadj, &p->grid, &p->tmp, &p->band, &p->tw0, &p->tw1, &p->psf, &p->ones, &p->grid_il,
-                    &p->seg_order})
+                    &p->seg_order, &p->touch, &p->grid_adj})
     b->release();
   delete p;
   return 0;
@@ -1351,6 +1535,15 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
         }
       }
       p->fft_mode = (int)value;
+      return 0;
+    case 6:
+      MRB_REQUIRE(value == 0 || value == 1, "spread kernel must be 0 (per-warp) or 1 (block per tile)");
+      p->spread_kernel = (int)value;
+      return 0;
+    case 7:
+      MRB_REQUIRE(value == 0 || value == 1, "grid mask must be 0 or 1");
+      if (value != p->grid_mask) p->adj_zero = false;
+      p->grid_mask = (int)value;
       return 0;
     case 5:
       MRB_REQUIRE(value == 0 || value == 1, "interleaved interp must be 0 or 1");
@@ -1515,17 +1708,20 @@ extern "C" int mrb_plan_set_points(mrb_plan* p, const float* traj, mrb_stream_t 
 
   // touched cells (sum over frames), for the roofline bookkeeping
   {
+    // kept per frame: the fused column passes and the spread write-out use them
     long long nwords = (p->gtot() + 31) / 32;
-    DevBuf bits, cntd;
-    if ((rc = bits.ensure(nwords * sizeof(unsigned)))) return rc;
+    DevBuf cntd;
+    if ((rc = p->touch.ensure((size_t)p->B * nwords * sizeof(unsigned)))) return rc;
     if ((rc = cntd.ensure(sizeof(unsigned long long)))) return rc;
     MRB_CUDA_TRY(cudaMemsetAsync(cntd.p, 0, sizeof(unsigned long long), st));
+    MRB_CUDA_TRY(cudaMemsetAsync(p->touch.p, 0, (size_t)p->B * nwords * sizeof(unsigned), st));
     for (int b = 0; b < p->B; ++b) {
-      MRB_CUDA_TRY(cudaMemsetAsync(bits.p, 0, nwords * sizeof(unsigned), st));
-      touch_kernel<<<grid_blocks(p->K, 256), 256, 0, st>>>(p->gx.as<float>(), bits.as<unsigned>(), g, p->W, b);
-      popc_kernel<<<grid_blocks(nwords, 256), 256, 0, st>>>(bits.as<unsigned>(), nwords,
-                                                            cntd.as<unsigned long long>());
+      unsigned* bits = p->touch.as<unsigned>() + (long long)b * nwords;
+      touch_kernel<<<grid_blocks(p->K, 256), 256, 0, st>>>(p->gx.as<float>(), bits, g, p->W, b);
+      popc_kernel<<<grid_blocks(nwords, 256), 256, 0, st>>>(bits, nwords, cntd.as<unsigned long long>());
     }
+    p->twords = nwords;
+    p->adj_zero = false;   // the supports changed: the spread grid is zeroed again before its next use
     MRB_LAUNCH_CHECK();
     unsigned long long touched = 0;
     MRB_CUDA_TRY(cudaMemcpyAsync(&touched, cntd.p, sizeof(touched), cudaMemcpyDeviceToHost, st));
@@ -1578,14 +1774,39 @@ extern "C" int mrb_plan_set_maps(mrb_plan* p, const void* maps, mrb_stream_t str
   return 0;
 }
 
-static int ensure_grid(mrb_plan* p, int nb) {
+static int ensure_grid(mrb_plan* p, int nb, cudaStream_t st) {
   size_t bytes = (size_t)nb * p->C * p->gtot() * sizeof(float2);
   int rc = p->grid.ensure(bytes);
   if (rc) return rc;
+  if (p->fft_mode == 1 && p->grid_mask == 1) {
+    if (p->grid_adj.bytes < bytes) {
+      if ((rc = p->grid_adj.ensure(bytes))) return rc;
+      p->adj_zero = false;
+    }
+    if (p->adj_nb != nb) p->adj_zero = false;
+    p->adj_nb = nb;
+    if (!p->adj_zero) {
+      // once per trajectory and size, in stream order: afterwards the spread
+      // only ever writes cell pairs inside the supports.  Inside a stream
+      // capture the fill becomes part of the graph (run on every replay).
+      MRB_CUDA_TRY(cudaMemsetAsync(p->grid_adj.p, 0, p->grid_adj.bytes, st));
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      MRB_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+      if (cs == cudaStreamCaptureStatusNone) p->adj_zero = true;
+    }
+  }
   if (p->fft_mode == 1) return p->band.ensure(mrb::fft2_tmp_bytes(p->S[0], p->G[1], p->C, nb));
   if (p->il && (rc = p->grid_il.ensure(bytes))) return rc;
   return ensure_fft(p, nb);
 }
+
+// the spread writes only touched cell pairs into a grid of its own (fused FFT mode)
+static bool spread_masked(const mrb_plan* p) {
+  return p->fft_mode == 1 && p->grid_mask == 1 && p->touch.p != nullptr && p->adj_zero;
+}
+
+// the grid the spread writes and the adjoint column pass reads
+static float2* adj_grid(mrb_plan* p) { return spread_masked(p) ? p->grid_adj.as<float2>() : p->grid.as<float2>(); }
 
 // raise a kernel's dynamic shared-memory limit once per (kernel, size)
 static int ensure_smem(const void* fn, size_t smem) {
@@ -1615,7 +1836,7 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       return mrb::fft2_columns(1, p->band.as<float2>(), p->grid.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
                                p->G[1], p->C, nb, p->skip, st);
     if (stage == 4)
-      return mrb::fft2_columns(0, p->grid.as<float2>(), p->band.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
+      return mrb::fft2_columns(0, adj_grid(p), p->band.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
                                p->G[1], p->C, nb, p->skip, st);
     if (stage == 5)
       return mrb::fft2_adjoint_rows(p->band.as<float2>(), p->maps.as<float2>(), p->invdeap.as<float>(), (void*)x,
@@ -1705,13 +1926,21 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     }
     a.partials = p->partials.as<float2>();
     a.nb = nb;
-    const bool blk3 = p->nd == 3 && tg.T == S3_T;   // block-per-tile 3D kernel
-    a.cpi = blk3 ? std::min(p->C, S3_CPB) : p->coils_per_item;
+    // fused mode with the bitmaps: the spread has a grid of its own whose
+    // cells outside every support were zeroed once; it stores only the cell
+    // pairs that hold a touched cell and no zero tiles
+    const bool masked = spread_masked(p);
+    a.touch = masked ? p->touch.as<unsigned>() : nullptr;
+    a.twords = p->twords;
+    a.grid = adj_grid(p);
+    const bool blk3 = p->spread_kernel == 1 && p->nd == 3 && tg.T == S3_T;   // block-per-tile kernels
+    const bool blk2 = p->spread_kernel == 1 && p->nd == 2 && tg.T == S2_T;
+    a.cpi = blk3 || blk2 ? std::min(p->C, S3_CPB) : p->coils_per_item;
     a.ngroups = (p->C + a.cpi - 1) / a.cpi;
     a.gsign = p->gsign;
     long long items = (long long)reps * p->n_items * a.ngroups;
     MRB_REQUIRE(items < (1LL << 31), "too many spread work items");
-    int blocks = blk3 ? (int)items : grid_blocks(items, SPREAD_WARPS);
+    int blocks = blk3 || blk2 ? (int)items : grid_blocks(items, SPREAD_WARPS);
     const void* fn = nullptr;
     size_t smem = 0;
     int threads = SPREAD_WARPS * 32;
@@ -1729,6 +1958,20 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
         smem = Spread3Smem<8>::BYTES;
       }
     }
+    if (blk2) {
+      const int pairs = (a.cpi + 1) / 2;
+      threads = S2_WARPS * 32;
+      if (pairs <= 2) {
+        fn = (const void*)spread2_kernel<2>;
+        smem = Spread2Smem<2>::BYTES;
+      } else if (pairs <= 4) {
+        fn = (const void*)spread2_kernel<4>;
+        smem = Spread2Smem<4>::BYTES;
+      } else {
+        fn = (const void*)spread2_kernel<8>;
+        smem = Spread2Smem<8>::BYTES;
+      }
+    }
 #define MRB_SPREAD_CASE(ND_, T_)                                                             \
   if (!fn && p->nd == ND_ && tg.T == T_) {                                                   \
     fn = (const void*)spread_kernel<ND_, T_>;                                                \
@@ -1744,12 +1987,12 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     MRB_REQUIRE(fn != nullptr, "no spread kernel for nd=%d tile=%d", p->nd, tg.T);
     MRB_REQUIRE(smem <= 227 * 1024, "spread tile needs %zu bytes of shared memory", smem);
     if (int rc3 = ensure_smem(fn, smem)) return rc3;
-    if (p->n_empty > 0) {
+    if (p->n_empty > 0 && !masked) {
       long long zbl = (long long)reps * p->n_empty;
       MRB_REQUIRE(zbl < (1LL << 31), "too many empty tiles");
       int zb = (int)zbl;
       const int* ek = p->empty_keys.as<int>();
-      float2* gridp = p->grid.as<float2>();
+      float2* gridp = a.grid;
 #define MRB_ZERO_CASE(ND_, T_)                                                                            \
   if (p->nd == ND_ && tg.T == T_) zero_tiles_kernel<ND_, T_><<<zb, 256, 0, st>>>(ek, p->n_empty, gridp, g, tg, nb);
       MRB_ZERO_CASE(2, 4)
@@ -1771,7 +2014,7 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       dim3 rg(p->n_multi, p->C, reps);
       const float2* part = p->partials.as<float2>();
       const int4* mt = p->multi.as<int4>();
-      float2* gridp = p->grid.as<float2>();
+      float2* gridp = a.grid;
       if (p->nd == 2) {
         if (tg.T == 4) spread_reduce_kernel<2, 4><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
         if (tg.T == 8) spread_reduce_kernel<2, 8><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
@@ -1808,7 +2051,7 @@ static int forward_impl(mrb_plan* p, const void* x, void* y, int nb, cudaStream_
   if ((rc = check_ready(p))) return rc;
   if ((rc = check_nb(p, nb))) return rc;
   MRB_REQUIRE(x != nullptr && y != nullptr, "null x or y");
-  if ((rc = ensure_grid(p, nb))) return rc;
+  if ((rc = ensure_grid(p, nb, st))) return rc;
   for (int stage : {0, 1, 2})
     if ((rc = run_stage(p, stage, x, y, nb, st, coil_images))) return rc;
   return 0;
@@ -1827,7 +2070,7 @@ extern "C" int mrb_nufft_adjoint(mrb_plan* p, const void* y, void* x, int nb, mr
   if ((rc = check_ready(p))) return rc;
   if ((rc = check_nb(p, nb))) return rc;
   MRB_REQUIRE(x != nullptr && y != nullptr, "null x or y");
-  if ((rc = ensure_grid(p, nb))) return rc;
+  if ((rc = ensure_grid(p, nb, (cudaStream_t)stream))) return rc;
   for (int stage : {3, 4, 5})
     if ((rc = run_stage(p, stage, x, (void*)y, nb, (cudaStream_t)stream, 0))) return rc;
   return 0;
@@ -1840,14 +2083,15 @@ extern "C" int mrb_nufft_stage(mrb_plan* p, int stage, const void* x, void* y, i
   MRB_REQUIRE(stage >= 0 && stage <= 5, "stage must be 0..5");
   MRB_REQUIRE((stage == 1 || stage == 4) || (stage == 0 || stage == 5 ? x != nullptr : y != nullptr),
               "null x or y for stage %d", stage);
-  if ((rc = ensure_grid(p, nb))) return rc;
+  if ((rc = ensure_grid(p, nb, (cudaStream_t)stream))) return rc;
   return run_stage(p, stage, x, y, nb, (cudaStream_t)stream, 0);
 }
 
 extern "C" int mrb_plan_info(mrb_plan* p, int64_t* out, int nout) {
   MRB_REQUIRE(p != nullptr && out != nullptr, "null plan or output");
-  int64_t v[7] = {p->n_entries, p->ntiles, p->touched, p->tile, p->coils_per_item, p->gtot(), p->fft_mode};
-  for (int i = 0; i < nout && i < 7; ++i) out[i] = v[i];
+  const int blk = p->spread_kernel == 1 && ((p->nd == 2 && p->tile == S2_T) || (p->nd == 3 && p->tile == S3_T));
+  int64_t v[8] = {p->n_entries, p->ntiles, p->touched, p->tile, p->coils_per_item, p->gtot(), p->fft_mode, blk};
+  for (int i = 0; i < nout && i < 8; ++i) out[i] = v[i];
   return 0;
 }
 
@@ -1873,7 +2117,7 @@ extern "C" int mrb_nufft_normal(mrb_plan* p, const void* x, void* out, int nb, m
   if ((rc = check_nb(p, nb))) return rc;
   MRB_REQUIRE(x != nullptr && out != nullptr, "null x or out");
   if (!p->have_psf) return mrb::fail(MRB_ESTATE, "plan has no Toeplitz transfer function (mrb_plan_set_toeplitz)");
-  if ((rc = ensure_grid(p, nb))) return rc;
+  if ((rc = ensure_grid(p, nb, (cudaStream_t)stream))) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   const float* one = p->ones.as<float>();
   float2* band = p->band.as<float2>();

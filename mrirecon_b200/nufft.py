@@ -31,7 +31,8 @@ from .layout import (AxisSpec, plan_image_layout, plan_kspace_layout, plan_image
                      plan_kspace_layout_from_sizes, user_image_shape, user_kspace_shape)
 from .roles import Roles
 
-OPT_TILE, OPT_COILS_PER_ITEM, OPT_INTERP_MODE, OPT_CHUNK, OPT_FFT_MODE, OPT_INTERLEAVE = 0, 1, 2, 3, 4, 5
+OPT_TILE, OPT_COILS_PER_ITEM, OPT_INTERP_MODE, OPT_CHUNK, OPT_FFT_MODE, OPT_INTERLEAVE, OPT_SPREAD_KERNEL, \
+    OPT_GRID_MASK = 0, 1, 2, 3, 4, 5, 6, 7
 FFT_CUFFT, FFT_FUSED = 0, 1
 _DCF_MODES = {"none": 0, "balanced": 1, "standard": 2}
 
@@ -128,9 +129,10 @@ class KBPlan:
         _lib.check(self.lib.mrb_plan_set_skip_flag(self.h, ptr), "plan_set_skip_flag")
 
     def info(self) -> dict:
-        out = (ct.c_int64 * 7)()
-        _lib.check(self.lib.mrb_plan_info(self.h, out, 7), "plan_info")
-        keys = ("entries", "tiles_per_frame", "touched_cells", "tile", "coils_per_item", "grid_cells", "fft_mode")
+        out = (ct.c_int64 * 8)()
+        _lib.check(self.lib.mrb_plan_info(self.h, out, 8), "plan_info")
+        keys = ("entries", "tiles_per_frame", "touched_cells", "tile", "coils_per_item", "grid_cells", "fft_mode",
+                "block_spread")
         return {k: int(v) for k, v in zip(keys, out)}
 
     def cell_base(self) -> torch.Tensor:
@@ -193,6 +195,7 @@ class B200NUFFTAdapter:
     chunk: Optional[int] = None
     fft_mode: Optional[int] = None
     interleave: Optional[int] = None   # 3D: interp on a coil-interleaved grid copy (default 1)
+    spread_kernel: Optional[int] = None  # 1 block per tile (default), 0 warp per tile and coil group
     autotune: bool = False
     tuned: Optional[dict] = None
 
@@ -261,6 +264,8 @@ class B200NUFFTAdapter:
                 plan.set_option(OPT_FFT_MODE, self.fft_mode)
             if self.interleave is not None:
                 plan.set_option(OPT_INTERLEAVE, self.interleave)
+            if self.spread_kernel is not None:
+                plan.set_option(OPT_SPREAD_KERNEL, self.spread_kernel)
             plan.set_points(self._traj_BndK)
             plan.set_dcf(self._dcf_BK, self.dcf_mode, self.apply_dcf_in_fwd, self.apply_dcf_in_adj)
             plan.set_maps(self._maps)

@@ -331,3 +331,45 @@ def test_3d_block_spread_matches_warp_kernel(cuda):
     out = ad.AH(y)
     assert rel(out, ref) < 1e-6
     assert torch.equal(out, ad.AH(y))
+
+
+@pytest.mark.parametrize("C,chunk,nb", [(12, None, 2), (12, 16, 2), (3, 32, 1), (7, None, 2), (20, 64, 2)])
+def test_2d_block_spread_identical_to_warp_kernel(cuda, C, chunk, nb):
+    """The block-per-tile 2D spread (tile 16: 2, 4 or 8 coil pairs per lane
+    group, two coil groups at C = 20) sums every (cell, coil) in the per-warp
+    kernel's order: same grid bit for bit, split tiles included."""
+    maps = _rand_c((C, 40, 36), 51, torch.complex64)
+    traj = phantoms.grasp_trajectory(nb, 11, 96)
+    y = _rand_c((nb, C, traj.shape[-1]), 52, torch.complex64).to(cuda)
+    blk = _adapter(maps, traj, tile=16, chunk=chunk, spread_kernel=1)
+    warp = _adapter(maps, traj, tile=16, chunk=chunk, spread_kernel=0)
+    assert blk.plan.info()["block_spread"] == 1 and warp.plan.info()["block_spread"] == 0
+    assert torch.equal(blk.AH(y), warp.AH(y))
+
+
+@pytest.mark.parametrize("S,C,nb,B", [((64, 64), 5, 2, 2), ((48, 40), 3, 4, 2), ((40, 40), 4, 3, 1)])
+def test_grid_mask_identical(cuda, S, C, nb, B):
+    """Fused FFT mode: restricting the column passes and the spread write-out to
+    the touched cells (per-frame bitmaps, frame = be // (nb // B)) gives the same
+    forward and adjoint results bit for bit, including after the unmasked
+    passes have left other values in the grid."""
+    maps = _rand_c((C,) + S, 61, torch.complex64)
+    traj = phantoms.grasp_trajectory(B, 7, 2 * S[0])
+    K = traj.shape[-1]
+    x = _rand_c((nb, 1) + S, 62, torch.complex64).to(cuda)
+    y = _rand_c((nb, C, K), 63, torch.complex64).to(cuda)
+    ad = _adapter(maps, traj)
+    assert ad.plan.info()["fft_mode"] == 1
+    ad.plan.set_option(7, 0)
+    ya, xa = ad.A(x), ad.AH(y)
+    ad.plan.set_option(7, 1)
+    assert torch.equal(ad.A(x), ya) and torch.equal(ad.AH(y), xa)
+    ad.plan.set_option(7, 0)
+    assert torch.equal(ad.A(x), ya) and torch.equal(ad.AH(y), xa)
+    if B > 1 and nb > B:
+        # a smaller batch maps the grid slots to other trajectory frames
+        ad.plan.set_option(7, 0)
+        xb = ad.AH(y[:B])
+        ad.plan.set_option(7, 1)
+        ad.AH(y)
+        assert torch.equal(ad.AH(y[:B]), xb)
