@@ -85,6 +85,9 @@ def parse():
     ap.add_argument("--no-toeplitz", action="store_true", help="skip the Toeplitz-schedule solve block")
     ap.add_argument("--nufft-only", action="store_true",
                     help="profiling case: prepare the workload's operator and run 3 forward/adjoint pairs")
+    ap.add_argument("--koosh-only", type=int, default=0, metavar="N",
+                    help="profiling case: the 3D koosh-ball operator scaled to an N^3 image (spokes x (N/160)^2, "
+                         "samples per spoke x N/160, 16 coils), 3 forward/adjoint pairs")
     return ap.parse_args()
 
 
@@ -309,21 +312,45 @@ def run_nufft_only(w, local):
 KOOSH = dict(name="koosh3d_160cube_16coil_20000spk_256ro", N=160, C=16, spokes=20000, nread=256)
 
 
-def koosh3d_throughput(dev, reps=10):
-    """3D radial koosh-ball NUFFT (160^3, 16 coils, 20,000 golden-means spokes x 256
-    samples, grid 320^3): per-stage device times, algorithmic GB/s and fraction of
-    the measured HBM peak, A / A^H times."""
+def koosh_operator(dev, N=160):
+    """The koosh-ball operator, image, maps and trajectory; N < 160 scales the
+    case down at the same angular and radial sample density."""
     from mrirecon_b200 import phantoms
     from mrirecon_b200.layout import AxisSpec
     from mrirecon_b200.nufft import NUFFT, NUFFTConfig
     k = KOOSH
-    N, C = k["N"], k["C"]
+    C = k["C"]
+    spokes = int(round(k["spokes"] * (N / k["N"]) ** 2))
+    nread = 2 * int(round(k["nread"] * N / k["N"] / 2))
     x = phantoms.ellipsoid_phantom(N, seed=0).reshape(1, 1, N, N, N).to(dev, torch.complex64)
     maps = phantoms.coil_maps(N, C, ndim=3).to(dev)
-    traj = phantoms.golden_means_koosh(k["spokes"], k["nread"]).unsqueeze(0).to(dev)
+    traj = phantoms.golden_means_koosh(spokes, nread).unsqueeze(0).to(dev)
     axis = AxisSpec(image_labels=("B", "coil", "X", "Y", "Z"), kspace_labels=("B", "coil", "K"),
                     image_fft_labels=("X", "Y", "Z"), coil_label="coil")
     op = NUFFT(maps, traj, None, axis=axis, config=NUFFTConfig(ndim=3, traj_units="rad"), device=dev)
+    return op, x, maps, traj
+
+
+def run_koosh_only(N, local):
+    """Profiling case: the (scaled) koosh-ball operator, three A/A^H pairs."""
+    dev = torch.device("cuda", local)
+    op, x, maps, traj = koosh_operator(dev, N)
+    y = op.A(x)
+    for _ in range(3):
+        op.A(x, out=y)
+        op.AH(y, out=x)
+    torch.cuda.synchronize()
+    print(json.dumps({"koosh_only": N, "samples": int(traj.shape[-1]), "plan": op.backend.plan.info()}))
+    return 0
+
+
+def koosh3d_throughput(dev, reps=10):
+    """3D radial koosh-ball NUFFT (160^3, 16 coils, 20,000 golden-means spokes x 256
+    samples, grid 320^3): per-stage device times, algorithmic GB/s and fraction of
+    the measured HBM peak, A / A^H times."""
+    k = KOOSH
+    N, C = k["N"], k["C"]
+    op, x, maps, traj = koosh_operator(dev, N)
     y = op.A(x)
     st = time_stages(op, x.clone(), torch.empty_like(y), 1, reps=reps)
     info = op.backend.plan.info()
@@ -603,6 +630,8 @@ def main():
             return run_reference(args, w, ws, rank)
         if args.nufft_only:
             return run_nufft_only(w, local)
+        if args.koosh_only:
+            return run_koosh_only(args.koosh_only, local)
         return run_b200(args, w, ws, rank, local)
     finally:
         if ws > 1:

@@ -19,13 +19,14 @@ from typing import Dict, Iterable, Optional, Sequence, Tuple
 import torch
 
 # (tile edge, coils per work item, samples per chunk, kernel): kernel 1 is the
-# block-per-tile spread (2D tile 16, 3D tile 8; up to 16 coils per block, the
-# coils-per-item entry is then unused), kernel 0 the per-warp spread
+# block-per-tile spread (2D tile 16, 3D tile 8; coils per block = min(coils per
+# item, 16)), kernel 0 the per-warp spread
 CANDIDATES_2D: Tuple[Tuple[int, int, int, int], ...] = (
     (16, 16, 128, 1), (16, 16, 256, 1), (16, 16, 512, 1), (16, 16, 64, 1),
     (16, 4, 128, 0), (16, 6, 128, 0), (8, 4, 64, 0), (32, 2, 128, 0))
 CANDIDATES_3D: Tuple[Tuple[int, int, int, int], ...] = (
-    (8, 16, 4096, 1), (8, 16, 1024, 1), (8, 16, 16384, 1), (8, 16, 256, 1), (4, 4, 256, 0), (4, 8, 256, 0))
+    (8, 16, 4096, 1), (8, 8, 4096, 1), (8, 16, 1024, 1), (8, 8, 1024, 1), (8, 16, 16384, 1), (4, 4, 256, 0),
+    (4, 8, 256, 0))
 
 
 def _cache_path() -> str:

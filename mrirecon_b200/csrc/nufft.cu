@@ -571,7 +571,7 @@ __global__ void __launch_bounds__(256) coil_interleave_kernel(const float2* __re
 }
 
 template <bool V4>
-__global__ void __launch_bounds__(256) interp3_il_kernel(InterpArgs a, Geo g, KBPoly kb) {
+__global__ void __launch_bounds__(256, 4) interp3_il_kernel(InterpArgs a, Geo g, KBPoly kb) {
   constexpr int W = 4;
   if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   const int P = (g.C + 1) >> 1;   // coil pairs
@@ -607,16 +607,20 @@ __global__ void __launch_bounds__(256) interp3_il_kernel(InterpArgs a, Geo g, KB
   const int c0 = 2 * pr;
   const bool two = c0 + 1 < g.C;
   const float2* gb = a.grid + (long long)be * g.C * g.gtot + c0;
+  // 32-bit element offsets within a frame (gtot * C < 2^31, checked on the host)
+  int off2[W];
+#pragma unroll
+  for (int i2 = 0; i2 < W; ++i2) off2[i2] = nidx[2][i2] * g.C;
   float re0 = 0.f, im0 = 0.f, re1 = 0.f, im1 = 0.f;
 #pragma unroll
   for (int i0 = 0; i0 < W; ++i0) {
     float4 v[W][W];
 #pragma unroll
     for (int i1 = 0; i1 < W; ++i1) {
-      const long long row = ((long long)nidx[0][i0] * g.G[1] + nidx[1][i1]) * g.G[2];
+      const int row = (nidx[0][i0] * g.G[1] + nidx[1][i1]) * g.G[2] * g.C;
 #pragma unroll
       for (int i2 = 0; i2 < W; ++i2) {
-        const float2* q = gb + (row + nidx[2][i2]) * g.C;
+        const float2* q = gb + (row + off2[i2]);
         if (V4) {
           v[i1][i2] = __ldg(reinterpret_cast<const float4*>(q));
         } else {
@@ -1452,7 +1456,7 @@ extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int 
   p->chunk = nd == 2 ? 128 : 4096;   // 3D: a block per item, only the centre tiles need splitting
   p->interp_mode = nd == 3 ? 1 : 0;
   p->spread_kernel = nd == 3 ? 1 : 0;   // 2D: the per-warp kernel is faster at typical coil counts
-  p->coils_per_item = nd == 2 ? std::min(C, 4) : std::min(C, 2);
+  p->coils_per_item = nd == 2 ? std::min(C, 4) : std::min(C, 8);
   // deapodisation: closed-form FT of the truncated KB window
   std::vector<float> dap;
   double i0b = 0.0;
@@ -1878,6 +1882,7 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     a.gsign = p->gsign;
     if (p->il && p->nd == 3) {
       MRB_REQUIRE(nb <= 65535, "too many frames in one call");
+      MRB_REQUIRE(p->gtot() * p->C < (1LL << 31), "interleaved grid of one frame exceeds 2^31 elements");
       const long long tb = (p->gtot() + TR_CELLS - 1) / TR_CELLS;
       MRB_REQUIRE(tb < (1LL << 31), "grid too large for the coil transpose");
       coil_interleave_kernel<<<dim3((unsigned)tb, nb), 256, 0, st>>>(p->grid.as<float2>(), p->grid_il.as<float2>(),
@@ -1935,7 +1940,7 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     a.grid = adj_grid(p);
     const bool blk3 = p->spread_kernel == 1 && p->nd == 3 && tg.T == S3_T;   // block-per-tile kernels
     const bool blk2 = p->spread_kernel == 1 && p->nd == 2 && tg.T == S2_T;
-    a.cpi = blk3 || blk2 ? std::min(p->C, S3_CPB) : p->coils_per_item;
+    a.cpi = blk3 || blk2 ? std::min(std::min(p->C, S3_CPB), p->coils_per_item) : p->coils_per_item;
     a.ngroups = (p->C + a.cpi - 1) / a.cpi;
     a.gsign = p->gsign;
     long long items = (long long)reps * p->n_items * a.ngroups;

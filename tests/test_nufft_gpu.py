@@ -341,7 +341,7 @@ def test_2d_block_spread_identical_to_warp_kernel(cuda, C, chunk, nb):
     maps = _rand_c((C, 40, 36), 51, torch.complex64)
     traj = phantoms.grasp_trajectory(nb, 11, 96)
     y = _rand_c((nb, C, traj.shape[-1]), 52, torch.complex64).to(cuda)
-    blk = _adapter(maps, traj, tile=16, chunk=chunk, spread_kernel=1)
+    blk = _adapter(maps, traj, tile=16, chunk=chunk, spread_kernel=1, coils_per_item=16)
     warp = _adapter(maps, traj, tile=16, chunk=chunk, spread_kernel=0)
     assert blk.plan.info()["block_spread"] == 1 and warp.plan.info()["block_spread"] == 0
     assert torch.equal(blk.AH(y), warp.AH(y))
