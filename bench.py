@@ -65,9 +65,10 @@ ITERS_TO_TOL = {"grasp": 252, "radial128": None}
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of each
 # stage's kernels on the grasp workload, from one `ncu --set full` capture per
-# kernel of `python bench.py --nufft-only` (spread stage = spread_kernel +
-# zero_tiles_kernel; the small split-tile reduction is not included)
-NCU_TRAFFIC = {"grasp": {"pre": 396.30e6, "fft": 1228.03e6, "interp": 433.49e6, "spread": 816.50e6,
+# kernel of `python bench.py --nufft-only` (spread stage = spread_kernel, which
+# stores only the cell pairs inside some support into a grid whose other cells
+# stay zero from a one-time fill; the small split-tile reduction is not included)
+NCU_TRAFFIC = {"grasp": {"pre": 396.30e6, "fft": 1228.03e6, "interp": 433.49e6, "spread": 338.06e6,
                          "ifft": 1256.29e6, "post": 454.12e6}}
 
 
