@@ -62,9 +62,11 @@ int mrb_plan_destroy(mrb_plan* plan);
 
 /* Tuning knobs read by set_points / the operators (autotuner):
  * key 0 = spread tile edge (cells), key 1 = coils per spread work item,
- * key 2 = interp mode: 0 acquisition order; 1 (3D default) segments of 8
- *         consecutive samples visited in the Morton order of their tile (the
- *         samples and results stay in acquisition order),
+ * key 2 = interp mode: 0 one thread per sample for all coils, in acquisition
+ *         order; 1 (default) 2D: one thread per (sample, coil pair); 3D (coil-
+ *         interleaved grid): segments of 8 consecutive samples visited in the
+ *         Morton order of their tile (samples and results stay in acquisition
+ *         order); both give the same results as mode 0,
  * key 3 = samples per spread work item (heavy tiles are split),
  * key 4 = FFT mode: 0 dense cuFFT transform with separate pad / crop kernels,
  *         1 fused zero-pruned row / column passes (2D grids whose sides have

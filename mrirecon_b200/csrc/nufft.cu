@@ -513,6 +513,72 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly
   }
 }
 
+// 2D forward interp, one thread per (sample, coil pair): the 16 taps of both
+// coils (32 independent 8-byte loads) in flight at once, and a grid of
+// C/2 times more threads than samples, so the latency of the scattered reads
+// is hidden by parallelism rather than by a per-thread loop over the coils.
+// Blocks cover 256 consecutive samples of one coil pair (coalesced sample
+// reads and result writes).  Same summation order as interp_kernel<2>.
+__global__ void __launch_bounds__(256) interp2p_kernel(InterpArgs a, Geo g, KBPoly kb) {
+  constexpr int W = 4;
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+  const int kblocks = (int)((g.K + 255) / 256);
+  const int pr = blockIdx.x / kblocks;
+  const long long k = (long long)(blockIdx.x - pr * kblocks) * 256 + threadIdx.x;
+  const int be = blockIdx.y;
+  if (k >= g.K) return;
+  const int b = frame_of(be, a.nb, g.B);
+  float w[2][W];
+  int nidx[2][W];
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    const float x = a.gx[((long long)b * 2 + d) * g.K + k];
+    const int base = (int)floorf(x);
+#pragma unroll
+    for (int o = 0; o < W; ++o) {
+      const int n = base - (W / 2 - 1) + o;
+      const float wd = mrb::kb_eval(kb, x - (float)n);
+      w[d][o] = (n & 1) ? -wd : wd;
+      nidx[d][o] = mrb::wrap_i(n, g.G[d]);
+    }
+  }
+  float s = a.scale * a.gsign;
+  if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
+  const int c = 2 * pr;
+  const bool two = c + 1 < g.C;
+  const float2* g0 = a.grid + ((long long)be * g.C + c) * g.gtot;
+  const float2* g1 = two ? g0 + g.gtot : g0;
+  float2 v0[W][W], v1[W][W];
+#pragma unroll
+  for (int i0 = 0; i0 < W; ++i0) {
+    const int roff = nidx[0][i0] * g.G[1];
+#pragma unroll
+    for (int i1 = 0; i1 < W; ++i1) {
+      v0[i0][i1] = __ldg(g0 + roff + nidx[1][i1]);
+      v1[i0][i1] = two ? __ldg(g1 + roff + nidx[1][i1]) : make_float2(0.f, 0.f);
+    }
+  }
+  float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
+#pragma unroll
+  for (int i0 = 0; i0 < W; ++i0) {
+    float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
+#pragma unroll
+    for (int i1 = 0; i1 < W; ++i1) {
+      a0 = fmaf(w[1][i1], v0[i0][i1].x, a0);
+      b0 = fmaf(w[1][i1], v0[i0][i1].y, b0);
+      a1 = fmaf(w[1][i1], v1[i0][i1].x, a1);
+      b1 = fmaf(w[1][i1], v1[i0][i1].y, b1);
+    }
+    r0 = fmaf(w[0][i0], a0, r0);
+    m0 = fmaf(w[0][i0], b0, m0);
+    r1 = fmaf(w[0][i0], a1, r1);
+    m1 = fmaf(w[0][i0], b1, m1);
+  }
+  float2* yo = a.y + ((long long)be * g.C + c) * g.K + k;
+  yo[0] = make_float2(r0 * s, m0 * s);
+  if (two) yo[g.K] = make_float2(r1 * s, m1 * s);
+}
+
 // ---------------------------------------------------------------------------
 // 3D forward interp on a coil-interleaved grid.  The dense cuFFT leaves the
 // oversampled grid planar, (be, coil, cell); a 64-tap gather from it touches
@@ -1454,7 +1520,7 @@ extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int 
   mrb::kb_poly_init(p->kb, W, p->beta);
   p->tile = nd == 2 ? 16 : 8;
   p->chunk = nd == 2 ? 128 : 4096;   // 3D: a block per item, only the centre tiles need splitting
-  p->interp_mode = nd == 3 ? 1 : 0;
+  p->interp_mode = 1;
   p->spread_kernel = nd == 3 ? 1 : 0;   // 2D: the per-warp kernel is faster at typical coil counts
   p->coils_per_item = nd == 2 ? std::min(C, 4) : std::min(C, 8);
   // deapodisation: closed-form FT of the truncated KB window
@@ -1896,6 +1962,13 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       dim3 grid(grid_blocks(nt, 256), nb);
       if (p->C % 2 == 0) interp3_il_kernel<true><<<grid, 256, 0, st>>>(a, g, p->kb);
       else interp3_il_kernel<false><<<grid, 256, 0, st>>>(a, g, p->kb);
+      MRB_LAUNCH_CHECK();
+      return 0;
+    }
+    if (p->nd == 2 && p->interp_mode == 1) {
+      const long long nbx = (long long)grid_blocks(p->K, 256) * ((p->C + 1) / 2);
+      MRB_REQUIRE(nbx < (1LL << 31) && nb <= 65535, "too many samples for the interp");
+      interp2p_kernel<<<dim3((unsigned)nbx, nb), 256, 0, st>>>(a, g, p->kb);
       MRB_LAUNCH_CHECK();
       return 0;
     }

@@ -373,3 +373,17 @@ def test_grid_mask_identical(cuda, S, C, nb, B):
         ad.plan.set_option(7, 1)
         ad.AH(y)
         assert torch.equal(ad.AH(y[:B]), xb)
+
+
+@pytest.mark.parametrize("C,nb,B", [(12, 2, 2), (5, 4, 2), (1, 1, 1), (3, 3, 1)])
+def test_2d_pair_parallel_interp_identical(cuda, C, nb, B):
+    """2D interp with one thread per (sample, coil pair) (mode 1, the default) sums
+    in the per-sample kernel's order: identical samples, odd coil counts included."""
+    maps = _rand_c((C, 40, 48), 71, torch.complex64)
+    traj = phantoms.random_traj(B, 2, 1000, seed=72)
+    x = _rand_c((nb, 1, 40, 48), 73, torch.complex64).to(cuda)
+    for fft_mode in (1, 0):
+        ad = _adapter(maps, traj, fft_mode=fft_mode)
+        y1 = ad.A(x)
+        ad.plan.set_option(2, 0)
+        assert torch.equal(ad.A(x), y1)
