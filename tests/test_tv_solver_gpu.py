@@ -342,3 +342,32 @@ def test_restart_on_non_descent_matches_oracle(cuda):
     for a, b in zip(fo, fs):
         assert abs(a - b) <= 1e-4 * abs(a)
     assert all(b <= a * (1 + 1e-6) for a, b in zip(fs, fs[1:]))
+
+
+def test_directional_derivative_matches_finite_difference(cuda):
+    """phi'(0) = Re<g, d> from the objective pass (NUFFT data term + spatial and
+    temporal TV, FP64 sums) agrees with a Richardson central difference of phi
+    along a fixed random d, as graspcg/tests/test_cg_descend_compile_ns.py:180-229
+    checks; same bar: |g_fd - phi'(0)| <= max(1e-6, 1e-2 max(1, |phi'(0)|))."""
+    ad, y, _, _ = _grasp_problem()
+    s = CGSolver(y, ad, _regm(), CGConfig(schedule="reference", max_iter=1, cuda_graph=False))
+    g = torch.Generator().manual_seed(555)
+    shape = tuple(s.x.shape)
+    rnd = lambda: (torch.randn(shape, generator=g) + 1j * torch.randn(shape, generator=g)).to(torch.complex64)
+    s.x.copy_(0.05 * rnd().to(cuda))
+    s.d.copy_(0.05 * rnd().to(cuda))
+    s.Ax = torch.empty_like(s.y)
+    s._A(s.x, s.Ax)
+    s._A(s.d, s.Ad)
+    out = torch.zeros(24, dtype=torch.float64, device=cuda)
+    _, g0d, _ = s._fg(0.0, out)
+
+    def fd(h):
+        fp = s._fg(h, out)[0]
+        fm = s._fg(-h, out)[0]
+        return (fp - fm) / (2 * h)
+
+    h = 1e-3
+    g_fd = (4 * fd(h) - fd(2 * h)) / 3.0
+    assert math.isfinite(g_fd) and math.isfinite(g0d)
+    assert abs(g_fd - g0d) <= max(1e-6, 1e-2 * max(1.0, abs(g0d))), (g_fd, g0d)
