@@ -359,13 +359,23 @@ def koosh3d_throughput(dev, reps=10):
     Gc = (2 * N) ** 3
     T = info["touched_cells"]
     N3 = N ** 3
-    ab = {"interp": C * (8 * T + 8 * K) + 12 * K, "spread": C * (8 * K + 8 * Gc) + 12 * K,
-          "pre": 8 * N3 + C * 8 * N3 + C * 8 * Gc, "post": C * 8 * N3 + C * 8 * N3 + 8 * N3}
+    ab = {"interp": C * (8 * T + 8 * K) + 12 * K, "spread": C * (8 * K + 8 * Gc) + 12 * K}
+    if info.get("fft_mode", 0) == 1:
+        # zero-pruned passes: z rows -> band1 (C, N, N, 2N), y columns -> band2
+        # (C, N, 2N, 2N), x columns -> grid; the adjoint in reverse
+        b1, b2 = C * 8 * N * N * 2 * N, C * 8 * N * 4 * N * N
+        ab.update(pre=8 * N3 + C * 8 * N3 + b1, fft=b1 + 2 * b2 + C * 8 * Gc, ifft=C * 8 * Gc + 2 * b2 + b1,
+                  post=b1 + C * 8 * N3 + 8 * N3)
+        fft = "fused zero-pruned z / y / x passes (320^3 grid, 16 coils)"
+    else:
+        ab.update(pre=8 * N3 + C * 8 * N3 + C * 8 * Gc, fft=C * 16 * Gc, ifft=C * 16 * Gc,
+                  post=C * 8 * N3 + C * 8 * N3 + 8 * N3)
+        fft = "cuFFT dense 320^3 (C2C, batch 16)"
     gbs = {n: ab[n] / (st[n] * 1e-3) / 1e9 for n in ab}
     del op, y, maps, traj, x
     torch.cuda.empty_cache()
     return {"workload": k["name"], "nufft_ms": st, "nufft_gbs": gbs, "touched_cells": T,
-            "samples": K, "grid_cells": Gc, "fft": "cuFFT dense 320^3 (C2C, batch 16)"}
+            "samples": K, "grid_cells": Gc, "fft": fft}
 
 
 def batched_throughput(dev, steps=3):

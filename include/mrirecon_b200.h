@@ -69,8 +69,9 @@ int mrb_plan_destroy(mrb_plan* plan);
  *         order); both give the same results as mode 0,
  * key 3 = samples per spread work item (heavy tiles are split),
  * key 4 = FFT mode: 0 dense cuFFT transform with separate pad / crop kernels,
- *         1 fused zero-pruned row / column passes (2D grids whose sides have
- *         compiled kernels; the default wherever available),
+ *         1 fused zero-pruned passes (2D: rows then columns; 3D: z rows, then
+ *         y and x columns; grids whose sides all have compiled kernels; the
+ *         default wherever available),
  * key 6 = spread kernel: 1 one block per work item, all coils of a group
  *         sharing the staged samples (2D tile 16, 3D tile 8; other tiles fall
  *         back to 0; the 3D default), 0 one warp per work item and coil group

@@ -289,7 +289,8 @@ constexpr int ROW_WARPS = ROW_NT / 32;
 
 template <int G1>
 __global__ void __launch_bounds__(ROW_NT) fwd_rows_kernel(const float2* __restrict__ x, const float2* __restrict__ maps,
-                                                          const float* __restrict__ invdeap, float2* __restrict__ Tb,
+                                                          const float* __restrict__ rowfac,
+                                                          const float* __restrict__ coldeap, float2* __restrict__ Tb,
                                                           const float2* __restrict__ tw, Geo2 g, long long nrows,
                                                           int coil_images) {
   constexpr int LD = padded_len(G1);
@@ -305,14 +306,14 @@ __global__ void __launch_bounds__(ROW_NT) fwd_rows_kernel(const float2* __restri
   const int c = (int)(vol - be * g.C);
   const float2* xr = x + (coil_images ? vol : be) * g.stot + (long long)r * g.S1;
   const float2* mr = maps + (long long)c * g.stot + (long long)r * g.S1;
-  const float dr = ((r + g.off0) & 1) ? -__ldg(invdeap + r) : __ldg(invdeap + r);
+  const float dr = __ldg(rowfac + r);   // signed deapodisation of the row
   float2* out = Tb + row * G1;
   auto load0 = [&](int, int n1) -> float2 {
     const int i1 = n1 - g.off1;
     if ((unsigned)i1 >= (unsigned)g.S1) return make_float2(0.f, 0.f);
     const float2 xv = xr[i1];
     const float2 mv = coil_images ? make_float2(1.f, 0.f) : __ldg(mr + i1);
-    float s = dr * __ldg(invdeap + g.S0 + i1);
+    float s = dr * __ldg(coldeap + i1);
     if (n1 & 1) s = -s;
     return make_float2((xv.x * mv.x - xv.y * mv.y) * s, (xv.x * mv.y + xv.y * mv.x) * s);
   };
@@ -417,7 +418,8 @@ __global__ void __launch_bounds__(COL_NT) toeplitz_cols_kernel(float2* __restric
 // coils in passes of ROWS
 template <int G1>
 __global__ void __launch_bounds__(ROW_NT) adj_rows_kernel(const float2* __restrict__ Tb, const float2* __restrict__ maps,
-                                                          const float* __restrict__ invdeap, float2* __restrict__ x,
+                                                          const float* __restrict__ rowfac,
+                                                          const float* __restrict__ coldeap, float2* __restrict__ x,
                                                           const float2* __restrict__ tw, Geo2 g, float scale) {
   constexpr int ROWS = rows_per_block(G1);
   constexpr int LD = padded_len(G1);
@@ -454,8 +456,8 @@ __global__ void __launch_bounds__(ROW_NT) adj_rows_kernel(const float2* __restri
     __syncthreads();
   }
   for (int i = threadIdx.x; i < g.S1; i += ROW_NT) {
-    float d = scale * __ldg(invdeap + r) * __ldg(invdeap + g.S0 + i);
-    if ((r + g.off0 + i + g.off1) & 1) d = -d;
+    float d = scale * __ldg(rowfac + r) * __ldg(coldeap + i);
+    if ((i + g.off1) & 1) d = -d;
     const float2 s = acc[i];
     x[((long long)be * g.S0 + r) * g.S1 + i] = make_float2(s.x * d, s.y * d);
   }
@@ -486,7 +488,8 @@ bool length_supported(int G) {
 }
 
 template <int G1>
-int launch_fwd_rows(const void* x, const float2* maps, const float* invdeap, float2* Tb, const float2* tw,
+int launch_fwd_rows(const void* x, const float2* maps, const float* rowfac, const float* coldeap, float2* Tb,
+                    const float2* tw,
                     const Geo2& g, int nb, int coil_images, cudaStream_t st) {
   const size_t smem = (size_t)ROW_WARPS * padded_len(G1) * sizeof(float2);
   int rc;
@@ -494,7 +497,7 @@ int launch_fwd_rows(const void* x, const float2* maps, const float* invdeap, flo
   const long long nrows = (long long)nb * g.C * g.S0;
   const long long blocks = (nrows + ROW_WARPS - 1) / ROW_WARPS;
   MRB_REQUIRE(blocks < (1LL << 31), "too many rows");
-  fwd_rows_kernel<G1><<<(unsigned)blocks, ROW_NT, smem, st>>>((const float2*)x, maps, invdeap, Tb, tw, g, nrows,
+  fwd_rows_kernel<G1><<<(unsigned)blocks, ROW_NT, smem, st>>>((const float2*)x, maps, rowfac, coldeap, Tb, tw, g, nrows,
                                                               coil_images);
   MRB_LAUNCH_CHECK();
   return 0;
@@ -533,7 +536,8 @@ int launch_toeplitz_cols(float2* Tb, const float* P, const float2* tw, const Geo
 }
 
 template <int G1>
-int launch_adj_rows(const float2* Tb, const float2* maps, const float* invdeap, void* x, const float2* tw,
+int launch_adj_rows(const float2* Tb, const float2* maps, const float* rowfac, const float* coldeap, void* x,
+                    const float2* tw,
                     const Geo2& g, int nb, float scale, cudaStream_t st) {
   constexpr int ROWS = rows_per_block(G1);
   const size_t smem = ((size_t)ROWS * padded_len(G1) + g.S1) * sizeof(float2);
@@ -541,7 +545,7 @@ int launch_adj_rows(const float2* Tb, const float2* maps, const float* invdeap, 
   if ((rc = set_smem((const void*)adj_rows_kernel<G1>, smem))) return rc;
   const long long blocks = (long long)nb * g.S0;
   MRB_REQUIRE(blocks < (1LL << 31), "too many rows");
-  adj_rows_kernel<G1><<<(unsigned)blocks, ROW_NT, smem, st>>>(Tb, maps, invdeap, (float2*)x, tw, g, scale);
+  adj_rows_kernel<G1><<<(unsigned)blocks, ROW_NT, smem, st>>>(Tb, maps, rowfac, coldeap, (float2*)x, tw, g, scale);
   MRB_LAUNCH_CHECK();
   return 0;
 }
@@ -565,13 +569,14 @@ int fft2_twiddles(DevBuf& tw, int G, const float2** out) {
   return 0;
 }
 
-int fft2_forward_rows(const void* x, const float2* maps, const float* invdeap, float2* Tb, const float2* tw1, int S0,
+int fft2_forward_rows(const void* x, const float2* maps, const float* rowfac, const float* coldeap, float2* Tb,
+                      const float2* tw1, int S0,
                       int S1, int G0, int G1, int C, int nb, int coil_images, const double* skip,
                       cudaStream_t st) {
   const Geo2 g = make_geo2(S0, S1, G0, G1, C, skip);
   switch (G1) {
 #define MRB_CASE(n) \
-  case n: return launch_fwd_rows<n>(x, maps, invdeap, Tb, tw1, g, nb, coil_images, st);
+  case n: return launch_fwd_rows<n>(x, maps, rowfac, coldeap, Tb, tw1, g, nb, coil_images, st);
     MRB_FFT_LENGTHS(MRB_CASE)
 #undef MRB_CASE
     default:
@@ -605,13 +610,14 @@ int fft2_toeplitz_columns(float2* Tb, const float* P, const float2* tw0, int S0,
   }
 }
 
-int fft2_adjoint_rows(const float2* Tb, const float2* maps, const float* invdeap, void* x, const float2* tw1, int S0,
+int fft2_adjoint_rows(const float2* Tb, const float2* maps, const float* rowfac, const float* coldeap, void* x,
+                      const float2* tw1, int S0,
                       int S1, int G0, int G1, int C, int nb, float scale, const double* skip,
                       cudaStream_t st) {
   const Geo2 g = make_geo2(S0, S1, G0, G1, C, skip);
   switch (G1) {
 #define MRB_CASE(n) \
-  case n: return launch_adj_rows<n>(Tb, maps, invdeap, x, tw1, g, nb, scale, st);
+  case n: return launch_adj_rows<n>(Tb, maps, rowfac, coldeap, x, tw1, g, nb, scale, st);
     MRB_FFT_LENGTHS(MRB_CASE)
 #undef MRB_CASE
     default:

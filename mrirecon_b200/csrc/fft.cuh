@@ -17,8 +17,13 @@ size_t fft2_tmp_bytes(int S0, int G1, int C, int nb);
 int fft2_twiddles(DevBuf& tw, int G, const float2** out);
 
 // skip: device flag, the kernels return at once when it is non-zero (may be null)
+// The row passes see a frame as S0 rows of S1 samples (a 3D volume S0 x S1 x S2
+// is S0*S1 rows of S2); rowfac (S0) holds each row's signed deapodisation
+// (-1)^(row parity) prod 1/Phi over the leading dims, coldeap (S1) the last
+// dim's 1/Phi; the last dim's sign (-1)^(i + G1/2 - S1/2) is applied here.
 // image (nb, S0, S1) [or coil images (nb, C, S0, S1)] -> T (nb, C, S0, G1)
-int fft2_forward_rows(const void* x, const float2* maps, const float* invdeap, float2* Tb, const float2* tw1, int S0,
+int fft2_forward_rows(const void* x, const float2* maps, const float* rowfac, const float* coldeap, float2* Tb,
+                      const float2* tw1, int S0,
                       int S1, int G0, int G1, int C, int nb, int coil_images, const double* skip,
                       cudaStream_t st);
 // forward != 0: T -> grid (nb, C, G0, G1); else grid -> T
@@ -29,7 +34,8 @@ int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, 
 int fft2_toeplitz_columns(float2* Tb, const float* P, const float2* tw0, int S0, int S1, int G0, int G1, int C, int nb,
                           int B, const double* skip, cudaStream_t st);
 // T -> image (nb, S0, S1), coil-combined with conj(maps), scaled
-int fft2_adjoint_rows(const float2* Tb, const float2* maps, const float* invdeap, void* x, const float2* tw1, int S0,
+int fft2_adjoint_rows(const float2* Tb, const float2* maps, const float* rowfac, const float* coldeap, void* x,
+                      const float2* tw1, int S0,
                       int S1, int G0, int G1, int C, int nb, float scale, const double* skip,
                       cudaStream_t st);
 

@@ -83,14 +83,18 @@ struct mrb_plan {
   int fft_batch = 0;
   int fft_mode = 0;   // 0 cuFFT dense transform + pad/crop kernels, 1 fused zero-pruned passes (fft.cu)
   DevBuf band;        // fused mode: (nb, C, S0, G1) float2 row-transformed band
-  DevBuf tw0, tw1;    // fused mode: twiddle tables of G0 and G1
+                      //             3D: (nb, C, S0, S1, G2) after the z pass
+  DevBuf band2;       // fused mode, 3D: (nb, C, S0, G1, G2) after the y pass
+  DevBuf tw0, tw1, tw2;   // fused mode: twiddle tables of G0, G1 (and G2)
   const float2* tw0p = nullptr;
   const float2* tw1p = nullptr;
+  const float2* tw2p = nullptr;
+  DevBuf rowfac;      // fused mode: signed deapodisation of each image row (S0, or S0*S1 in 3D)
   const double* skip = nullptr;   // device flag: operator kernels return when it is non-zero
   int il = 0;         // 1: forward interp reads a coil-interleaved copy of the grid (3D, cuFFT mode)
   DevBuf grid_il;     // (nb, gtot, C) float2, written by the transpose at the start of the interp stage
   DevBuf psf;         // Toeplitz transfer functions (B, G0, G1) float (mrb_plan_set_toeplitz)
-  DevBuf ones;        // S0 + S1 ones: the row passes without deapodisation
+  DevBuf ones;        // 2D: S0 signs (-1)^(r + G0/2 - S0/2), then S1 ones: the row passes without deapodisation
   bool have_psf = false;
   DevBuf tmp;         // scratch for set_points
 
@@ -1483,6 +1487,12 @@ int check_nb(mrb_plan* p, int nb) {
 // ===========================================================================
 // C ABI
 // ===========================================================================
+// compiled zero-pruned passes exist for every dim of this grid
+static bool fused_supported(const mrb_plan* p) {
+  if (p->nd == 2) return mrb::fft2_supported(p->S[0], p->S[1], p->G[0], p->G[1]);
+  return mrb::fft2_supported(p->S[0], p->S[1], p->G[0], p->G[1]) && mrb::fft2_supported(p->S[1], p->S[2], p->G[1], p->G[2]);
+}
+
 extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int B, int64_t K, int W, double osf,
                                int norm_ortho) {
   if (!out) return mrb::fail(MRB_EINVAL, "null output pointer");
@@ -1550,7 +1560,27 @@ extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int 
   int rc = p->invdeap.ensure(dap.size() * sizeof(float));
   if (!rc && cudaMemcpy(p->invdeap.p, dap.data(), dap.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
     rc = mrb::fail(MRB_ECUDA, "copying deapodisation failed");
-  if (!rc && nd == 2 && mrb::fft2_supported(p->S[0], p->S[1], p->G[0], p->G[1])) rc = mrb_plan_set_option(p, 4, 1);
+  // the fused row passes see a frame as rows of the last dim: each row's
+  // deapodisation over the leading dims with the sign (-1)^(sum of their
+  // centred indices)
+  if (!rc) {
+    std::vector<float> rf;
+    const int off0 = p->G[0] / 2 - S[0] / 2;
+    if (nd == 2) {
+      for (int r = 0; r < S[0]; ++r) rf.push_back(((r + off0) & 1) ? -dap[r] : dap[r]);
+    } else {
+      const int off1 = p->G[1] / 2 - S[1] / 2;
+      for (int a = 0; a < S[0]; ++a)
+        for (int b = 0; b < S[1]; ++b) {
+          const float v = dap[a] * dap[S[0] + b];
+          rf.push_back(((a + off0 + b + off1) & 1) ? -v : v);
+        }
+    }
+    rc = p->rowfac.ensure(rf.size() * sizeof(float));
+    if (!rc && cudaMemcpy(p->rowfac.p, rf.data(), rf.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+      rc = mrb::fail(MRB_ECUDA, "copying row deapodisation failed");
+  }
+  if (!rc && fused_supported(p)) rc = mrb_plan_set_option(p, 4, 1);
   if (!rc && nd == 3) p->il = 1;
   if (rc) {
     delete p;
@@ -1565,6 +1595,7 @@ extern "C" int mrb_plan_destroy(mrb_plan* p) {
   if (p->fft) cufftDestroy(p->fft);
   for (DevBuf* b : {&p->gx, &p->entries, &p->tile_start, &p->items, &p->multi, &p->partials, &p->empty_keys, &p->maps, &p->invdeap, &p->wfwd,
                     &p->wadj, &p->grid, &p->tmp, &p->band, &p->tw0, &p->tw1, &p->psf, &p->ones, &p->grid_il,
+                    &p->band2, &p->tw2, &p->rowfac,
                     &p->seg_order, &p->touch, &p->grid_adj})
     b->release();
   delete p;
@@ -1596,12 +1627,13 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
     case 4:
       MRB_REQUIRE(value == 0 || value == 1, "fft mode must be 0 (cuFFT) or 1 (fused)");
       if (value == 1) {
-        MRB_REQUIRE(p->nd == 2 && mrb::fft2_supported(p->S[0], p->S[1], p->G[0], p->G[1]),
-                    "no fused FFT kernels for this grid (%d x %d)", p->G[0], p->G[1]);
+        MRB_REQUIRE(fused_supported(p), "no fused FFT kernels for this grid (%d x %d x %d)", p->G[0], p->G[1],
+                    p->nd == 3 ? p->G[2] : 1);
         if (!p->tw0p) {
           int rc;
           if ((rc = mrb::fft2_twiddles(p->tw0, p->G[0], &p->tw0p))) return rc;
           if ((rc = mrb::fft2_twiddles(p->tw1, p->G[1], &p->tw1p))) return rc;
+          if (p->nd == 3 && (rc = mrb::fft2_twiddles(p->tw2, p->G[2], &p->tw2p))) return rc;
         }
       }
       p->fft_mode = (int)value;
@@ -1865,6 +1897,13 @@ static int ensure_grid(mrb_plan* p, int nb, cudaStream_t st) {
       if (cs == cudaStreamCaptureStatusNone) p->adj_zero = true;
     }
   }
+  if (p->fft_mode == 1 && p->nd == 3) {
+    const size_t vol = (size_t)nb * p->C * sizeof(float2);
+    if ((rc = p->band.ensure(vol * p->S[0] * p->S[1] * p->G[2]))) return rc;
+    if ((rc = p->band2.ensure(vol * p->S[0] * p->G[1] * p->G[2]))) return rc;
+    if (p->il && (rc = p->grid_il.ensure(bytes))) return rc;
+    return 0;
+  }
   if (p->fft_mode == 1) return p->band.ensure(mrb::fft2_tmp_bytes(p->S[0], p->G[1], p->C, nb));
   if (p->il && (rc = p->grid_il.ensure(bytes))) return rc;
   return ensure_fft(p, nb);
@@ -1896,12 +1935,48 @@ static int ensure_smem(const void* fn, size_t smem) {
 // one stage of the forward/adjoint pipeline; x/y are the user image / samples
 static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cudaStream_t st, int coil_images) {
   Geo g = make_geo(p);
+  if (p->fft_mode == 1 && p->nd == 3) {
+    // fused 3D passes on (vol, x, y, z): 0 = SENSE/deapod/pad + z transforms of
+    // the S0*S1 image rows -> band (vol, S0, S1, G2); 1 = input-pruned y
+    // transforms (the y columns of each (vol, x) slab) -> band2 (vol, S0, G1, G2),
+    // then input-pruned x transforms (band2 as S0 rows of G1*G2 columns) -> grid;
+    // 4 and 5 the same in reverse, output-pruned, with crop, deapodisation and
+    // the conj(S_c) coil sum in the z pass
+    const float* rowfac = p->rowfac.as<float>();
+    const float* coldeap = p->invdeap.as<float>() + p->S[0] + p->S[1];
+    const int R = p->S[0] * p->S[1];
+    const int GG = p->G[1] * p->G[2];
+    MRB_REQUIRE((long long)p->C * p->S[0] < (1LL << 31), "too many coil slabs");
+    float2* b1 = p->band.as<float2>();
+    float2* b2 = p->band2.as<float2>();
+    int rc3;
+    if (stage == 0)
+      return mrb::fft2_forward_rows(x, p->maps.as<float2>(), rowfac, coldeap, b1, p->tw2p, R, p->S[2], R, p->G[2],
+                                    p->C, nb, coil_images, p->skip, st);
+    if (stage == 1) {
+      if ((rc3 = mrb::fft2_columns(1, b1, b2, p->tw1p, p->S[1], p->S[2], p->G[1], p->G[2], p->C * p->S[0], nb,
+                                   p->skip, st)))
+        return rc3;
+      return mrb::fft2_columns(1, b2, p->grid.as<float2>(), p->tw0p, p->S[0], GG, p->G[0], GG, p->C, nb, p->skip,
+                               st);
+    }
+    if (stage == 4) {
+      if ((rc3 = mrb::fft2_columns(0, adj_grid(p), b2, p->tw0p, p->S[0], GG, p->G[0], GG, p->C, nb, p->skip, st)))
+        return rc3;
+      return mrb::fft2_columns(0, b2, b1, p->tw1p, p->S[1], p->S[2], p->G[1], p->G[2], p->C * p->S[0], nb, p->skip,
+                               st);
+    }
+    if (stage == 5)
+      return mrb::fft2_adjoint_rows(b1, p->maps.as<float2>(), rowfac, coldeap, (void*)x, p->tw2p, R, p->S[2], R,
+                                    p->G[2], p->C, nb, p->scale, p->skip, st);
+  }
   if (p->fft_mode == 1) {
     // fused passes: 0 = SENSE/deapod/pad + row FFTs, 1 = column FFTs,
     // 4 = inverse column FFTs, 5 = inverse row FFTs + crop/deapod/coil sum
     if (stage == 0)
-      return mrb::fft2_forward_rows(x, p->maps.as<float2>(), p->invdeap.as<float>(), p->band.as<float2>(), p->tw1p,
-                                    p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb, coil_images, p->skip, st);
+      return mrb::fft2_forward_rows(x, p->maps.as<float2>(), p->rowfac.as<float>(), p->invdeap.as<float>() + p->S[0],
+                                    p->band.as<float2>(), p->tw1p, p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb,
+                                    coil_images, p->skip, st);
     if (stage == 1)
       return mrb::fft2_columns(1, p->band.as<float2>(), p->grid.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
                                p->G[1], p->C, nb, p->skip, st);
@@ -1909,8 +1984,9 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       return mrb::fft2_columns(0, adj_grid(p), p->band.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
                                p->G[1], p->C, nb, p->skip, st);
     if (stage == 5)
-      return mrb::fft2_adjoint_rows(p->band.as<float2>(), p->maps.as<float2>(), p->invdeap.as<float>(), (void*)x,
-                                    p->tw1p, p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb, p->scale, p->skip, st);
+      return mrb::fft2_adjoint_rows(p->band.as<float2>(), p->maps.as<float2>(), p->rowfac.as<float>(),
+                                    p->invdeap.as<float>() + p->S[0], (void*)x, p->tw1p, p->S[0], p->S[1], p->G[0],
+                                    p->G[1], p->C, nb, p->scale, p->skip, st);
   }
   if (stage == 0) {
     const int Gl = p->G[p->nd - 1];
@@ -2175,13 +2251,17 @@ extern "C" int mrb_plan_info(mrb_plan* p, int64_t* out, int nout) {
 
 extern "C" int mrb_plan_set_toeplitz(mrb_plan* p, const float* psf, mrb_stream_t stream) {
   MRB_REQUIRE(p != nullptr && psf != nullptr, "null plan or transfer function");
-  MRB_REQUIRE(p->fft_mode == 1, "the Toeplitz normal operator needs the fused FFT mode (2D, compiled grid sizes)");
+  MRB_REQUIRE(p->nd == 2 && p->fft_mode == 1,
+              "the Toeplitz normal operator needs a 2D plan in the fused FFT mode (compiled grid sizes)");
   const size_t bytes = (size_t)p->B * p->gtot() * sizeof(float);
   int rc;
   if ((rc = p->psf.ensure(bytes))) return rc;
   MRB_CUDA_TRY(cudaMemcpyAsync(p->psf.p, psf, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
   if (!p->ones.p) {
     std::vector<float> one((size_t)p->S[0] + p->S[1], 1.f);
+    const int off0 = p->G[0] / 2 - p->S[0] / 2;
+    for (int r = 0; r < p->S[0]; ++r)
+      if ((r + off0) & 1) one[r] = -1.f;   // the row sign the deapodisation table would carry
     if ((rc = p->ones.ensure(one.size() * sizeof(float)))) return rc;
     MRB_CUDA_TRY(cudaMemcpy(p->ones.p, one.data(), one.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
@@ -2199,14 +2279,14 @@ extern "C" int mrb_nufft_normal(mrb_plan* p, const void* x, void* out, int nb, m
   cudaStream_t st = (cudaStream_t)stream;
   const float* one = p->ones.as<float>();
   float2* band = p->band.as<float2>();
-  if ((rc = mrb::fft2_forward_rows(x, p->maps.as<float2>(), one, band, p->tw1p, p->S[0], p->S[1], p->G[0], p->G[1],
-                                   p->C, nb, 0, p->skip, st)))
+  if ((rc = mrb::fft2_forward_rows(x, p->maps.as<float2>(), one, one + p->S[0], band, p->tw1p, p->S[0], p->S[1],
+                                   p->G[0], p->G[1], p->C, nb, 0, p->skip, st)))
     return rc;
   if ((rc = mrb::fft2_toeplitz_columns(band, p->psf.as<float>(), p->tw0p, p->S[0], p->S[1], p->G[0], p->G[1], p->C,
                                        nb, p->B, p->skip, st)))
     return rc;
-  return mrb::fft2_adjoint_rows(band, p->maps.as<float2>(), one, out, p->tw1p, p->S[0], p->S[1], p->G[0], p->G[1],
-                                p->C, nb, 1.f, p->skip, st);
+  return mrb::fft2_adjoint_rows(band, p->maps.as<float2>(), one, one + p->S[0], out, p->tw1p, p->S[0], p->S[1],
+                                p->G[0], p->G[1], p->C, nb, 1.f, p->skip, st);
 }
 
 extern "C" int mrb_plan_set_skip_flag(mrb_plan* p, const double* flag) {
