@@ -997,7 +997,7 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
 // ---------------------------------------------------------------------------
 constexpr int S3_T = 8;         // tile edge (cells)
 constexpr int S3_WARPS = 8;     // one warp per tile plane
-constexpr int S3_BATCH = 32;    // samples staged per pass (3 blocks of 70 KB per SM)
+constexpr int S3_BATCH = 64;    // samples staged per pass (two ballots of 32)
 constexpr int S3_CPB = 16;      // coils per block (group)
 
 template <int PPL>
@@ -1084,20 +1084,22 @@ __global__ void __launch_bounds__(S3_WARPS * 32) spread3_kernel(SpreadArgs a, Ge
     }
     __syncthreads();
     if (P0 >= g.G[0]) continue;   // plane beyond a partial last tile: nothing lands here
-    // lane j tests sample j against this warp's plane; the warp then visits
-    // only the samples whose support meets it
+    // lane j tests sample h + j against this warp's plane; the warp then
+    // visits only the samples whose support meets it
+    for (int h = 0; h < nbat; h += 32) {
     int myd0 = 4;
-    if (lane < nbat) {
-      myd0 = P0 - sb[lane].x;
+    if (h + lane < nbat) {
+      myd0 = P0 - sb[h + lane].x;
       myd0 += myd0 < 0 ? g.G[0] : 0;
       myd0 -= myd0 >= g.G[0] ? g.G[0] : 0;
     }
     unsigned todo = __ballot_sync(0xffffffffu, myd0 < 4);
     while (todo) {
-      const int j = __ffs(todo) - 1;
+      const int jl = __ffs(todo) - 1;
       todo &= todo - 1;
+      const int j = h + jl;
       const int4 bb = sb[j];
-      const int d0 = __shfl_sync(0xffffffffu, myd0, j);
+      const int d0 = __shfl_sync(0xffffffffu, myd0, jl);
       int n2 = bb.z + a2;
       n2 += n2 < 0 ? g.G[2] : 0;
       n2 -= n2 >= g.G[2] ? g.G[2] : 0;
@@ -1125,6 +1127,7 @@ __global__ void __launch_bounds__(S3_WARPS * 32) spread3_kernel(SpreadArgs a, Ge
         }
       }
       __syncwarp();
+    }
     }
   }
   __syncthreads();
