@@ -40,18 +40,40 @@ static double i0_series(double x) {
 }
 
 void kb_poly_init(KBPoly& p, int W, double beta) {
-  double i0b = i0_series(beta);
-  double q = 0.25 * beta * beta;
-  double ck = 1.0 / i0b;
-  int n = 0;
-  for (int k = 0; k < KB_MAX_TERMS; ++k) {
-    if (k > 0) ck *= q / ((double)k * (double)k);
-    p.c[k] = (float)ck;
-    n = k + 1;
-    if (k > 2 && ck < 1e-10) break;
+  const double i0b = i0_series(beta);
+  auto phi = [&](double d) {
+    const double z = 1.0 - (2.0 * d / W) * (2.0 * d / W);
+    return z > 0.0 ? i0_series(beta * std::sqrt(z)) / i0b : 1.0 / i0b;
+  };
+  constexpr int D = KB_TAP_DEG, M = KB_TAP_DEG + 1;
+  for (int t = 0; t < 4; ++t) {
+    // Chebyshev interpolation at the M first-kind nodes of u in [-1, 1]
+    double v[M], a[M];
+    for (int j = 0; j < M; ++j) {
+      const double u = std::cos(M_PI * (j + 0.5) / M);
+      v[j] = phi(0.5 * (u + 1.0) + 1.0 - t);
+    }
+    for (int k = 0; k < M; ++k) {
+      double s = 0.0;
+      for (int j = 0; j < M; ++j) s += v[j] * std::cos(M_PI * k * (j + 0.5) / M);
+      a[k] = (k == 0 ? 1.0 : 2.0) * s / M;
+    }
+    // sum a_k T_k(u) as monomials: T_0 = 1, T_1 = u, T_{k+1} = 2u T_k - T_{k-1}
+    double mono[M] = {0.0}, tkm1[M] = {0.0}, tk[M] = {0.0}, tkp1[M];
+    tkm1[0] = 1.0;
+    tk[1] = 1.0;
+    mono[0] += a[0];
+    for (int i = 0; i < M; ++i) mono[i] += a[1] * tk[i];
+    for (int k = 1; k < D; ++k) {
+      for (int i = 0; i < M; ++i) tkp1[i] = (i > 0 ? 2.0 * tk[i - 1] : 0.0) - tkm1[i];
+      for (int i = 0; i < M; ++i) {
+        mono[i] += a[k + 1] * tkp1[i];
+        tkm1[i] = tk[i];
+        tk[i] = tkp1[i];
+      }
+    }
+    for (int i = 0; i < M; ++i) p.tap[t][i] = (float)mono[i];
   }
-  p.n = n;
-  p.inv_half_w2 = (float)(4.0 / ((double)W * (double)W));
 }
 
 }  // namespace mrb

@@ -423,10 +423,11 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly
   for (int d = 0; d < ND; ++d) {
     float x = a.gx[((long long)b * ND + d) * g.K + k];
     int base = (int)floorf(x);
+    const float fx = x - (float)base;
 #pragma unroll
     for (int o = 0; o < W; ++o) {
       int n = base - (W / 2 - 1) + o;
-      float wd = mrb::kb_eval(kb, x - (float)n);
+      float wd = mrb::kb_tap(kb, o, fx);
       w[d][o] = (n & 1) ? -wd : wd;
       nidx[d][o] = mrb::wrap_i(n, g.G[d]);
     }
@@ -538,10 +539,11 @@ __global__ void __launch_bounds__(256) interp2p_kernel(InterpArgs a, Geo g, KBPo
   for (int d = 0; d < 2; ++d) {
     const float x = a.gx[((long long)b * 2 + d) * g.K + k];
     const int base = (int)floorf(x);
+    const float fx = x - (float)base;
 #pragma unroll
     for (int o = 0; o < W; ++o) {
       const int n = base - (W / 2 - 1) + o;
-      const float wd = mrb::kb_eval(kb, x - (float)n);
+      const float wd = mrb::kb_tap(kb, o, fx);
       w[d][o] = (n & 1) ? -wd : wd;
       nidx[d][o] = mrb::wrap_i(n, g.G[d]);
     }
@@ -664,10 +666,11 @@ __global__ void __launch_bounds__(256, 4) interp3_il_kernel(InterpArgs a, Geo g,
   for (int d = 0; d < 3; ++d) {
     const float x = a.gx[((long long)b * 3 + d) * g.K + k];
     const int base = (int)floorf(x);
+    const float fx = x - (float)base;
 #pragma unroll
     for (int o = 0; o < W; ++o) {
       const int n = base - (W / 2 - 1) + o;
-      const float wd = mrb::kb_eval(kb, x - (float)n);
+      const float wd = mrb::kb_tap(kb, o, fx);
       w[d][o] = (n & 1) ? -wd : wd;
       nidx[d][o] = mrb::wrap_i(n, g.G[d]);
     }
@@ -889,10 +892,11 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
       for (int d = 0; d < ND; ++d) {
         const float x = gxp[(long long)d * g.K + k];
         base[d] = (int)floorf(x) - 1;
+        const float fx = x - (float)(base[d] + 1);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const int n = base[d] + q;
-          float w = mrb::kb_eval(kb, x - (float)n);
+          float w = mrb::kb_tap(kb, q, fx);
           if (n & 1) w = -w;
           if (d == 0) w *= ws;
           sw[lane * NW + d * 4 + q] = w;
@@ -1066,10 +1070,11 @@ __global__ void __launch_bounds__(S3_WARPS * 32) spread3_kernel(SpreadArgs a, Ge
         ws = a.gsign;
         if (a.wadj) ws *= a.wadj[(long long)b * g.K + k];
       }
+      const float fx = x - (float)(base + 1);
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int n = base + t;
-        float w = mrb::kb_eval(kb, x - (float)n);
+        float w = mrb::kb_tap(kb, t, fx);
         if (n & 1) w = -w;
         sw[j * 12 + d * 4 + t] = w * ws;
       }
@@ -1228,10 +1233,11 @@ __global__ void __launch_bounds__(S2_WARPS * 32) spread2_kernel(SpreadArgs a, Ge
         ws = a.gsign;
         if (a.wadj) ws *= a.wadj[(long long)b * g.K + k];
       }
+      const float fx = x - (float)(base + 1);
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int n = base + t;
-        float w = mrb::kb_eval(kb, x - (float)n);
+        float w = mrb::kb_tap(kb, t, fx);
         if (n & 1) w = -w;
         sw[j * 8 + d * 4 + t] = w * ws;
       }
