@@ -881,16 +881,33 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
   const float* gxp = a.gx + (long long)b * ND * g.K;
   const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
   const int ntask = NTAP * npair;
+  // the next batch's sample index, coordinates, weight and first coil values
+  // are loaded into registers while the warp works on the current batch
+  constexpr int PF = 4;
+  int pk = 0;
+  float px[ND], pwa = 1.f;
+  float2 py[PF];
+  auto fetch = [&](int e, int nbat) {
+    if (lane < nbat) {
+      pk = a.entries[e + lane];
+#pragma unroll
+      for (int d = 0; d < ND; ++d) px[d] = gxp[(long long)d * g.K + pk];
+      if (a.wadj) pwa = a.wadj[(long long)b * g.K + pk];
+#pragma unroll
+      for (int cl = 0; cl < PF; ++cl) py[cl] = cl < nc ? yb[(long long)cl * g.K + pk] : make_float2(0.f, 0.f);
+    }
+  };
+  if (e0 < e1) fetch(e0, min(SPREAD_BATCH, e1 - e0));
   for (int e = e0; e < e1; e += SPREAD_BATCH) {
     const int nbat = min(SPREAD_BATCH, e1 - e);
     if (lane < nbat) {
-      const int k = a.entries[e + lane];
+      const int k = pk;
       float ws = a.gsign;
-      if (a.wadj) ws *= a.wadj[(long long)b * g.K + k];
+      if (a.wadj) ws *= pwa;
       int base[3] = {0, 0, 0};
 #pragma unroll
       for (int d = 0; d < ND; ++d) {
-        const float x = gxp[(long long)d * g.K + k];
+        const float x = px[d];
         base[d] = (int)floorf(x) - 1;
         const float fx = x - (float)(base[d] + 1);
 #pragma unroll
@@ -903,10 +920,14 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
         }
       }
       sb[lane] = make_int4(base[0], base[1], base[2], 0);
-      for (int cl = 0; cl < cps; ++cl)
+#pragma unroll
+      for (int cl = 0; cl < PF; ++cl)
+        if (cl < cps) sy[lane * cps + cl] = py[cl];
+      for (int cl = PF; cl < cps; ++cl)
         sy[lane * cps + cl] = cl < nc ? yb[(long long)cl * g.K + k] : make_float2(0.f, 0.f);
     }
     __syncwarp();
+    if (e + SPREAD_BATCH < e1) fetch(e + SPREAD_BATCH, min(SPREAD_BATCH, e1 - e - SPREAD_BATCH));
     for (int j = 0; j < nbat; ++j) {
       const int4 bb = sb[j];
       const float* wj = sw + j * NW;
