@@ -80,6 +80,10 @@ int mrb_plan_destroy(mrb_plan* plan);
  *         stores, and the adjoint column pass loads, only the grid cells inside
  *         some sample's support (per-frame bitmaps built by set_points), and the
  *         spread stores no zeros outside them; 0 full grid passes,
+ * key 8 = 2D fused mode: the forward column pass interpolates the samples of
+ *         each column strip from shared memory and never writes the grid
+ *         (1, the default; set_points builds the per-frame strip lists) or
+ *         writes the grid for a separate interp pass (0); same samples,
  * key 5 = 3D forward interp on a coil-interleaved copy of the grid (1, the 3D
  *         default: a tiled transpose then 128-bit gathers of all coils of a
  *         cell; costs one more grid-sized buffer) or on the planar grid (0). */
@@ -117,7 +121,10 @@ int mrb_nufft_adjoint(mrb_plan* plan, const void* y, void* x, int nb, mrb_stream
  * deapodisation, conj-maps coil sum; grid -> x).  The grid is the plan's.
  * In FFT mode 1 stage 0 also runs the row transforms (x -> band buffer),
  * 1 the column transforms (band -> grid), 4 the inverse column transforms
- * (grid -> band) and 5 the inverse row transforms with crop and coil sum. */
+ * (grid -> band) and 5 the inverse row transforms with crop and coil sum.
+ * With option key 8 on (2D), stage 1 given a non-null y runs the column
+ * transforms fused with the interp (band -> y, no grid) and stage 2 is not
+ * needed; given a null y it writes the grid as above. */
 int mrb_nufft_stage(mrb_plan* plan, int stage, const void* x, void* y, int nb, mrb_stream_t stream);
 
 /* Plan facts for tests and the bench (host copies, synchronous):
@@ -125,7 +132,8 @@ int mrb_nufft_stage(mrb_plan* plan, int stage, const void* x, void* y, int nb, m
  * out[2] = touched grid cells summed over frames, out[3] = spread tile edge,
  * out[4] = coils per spread work item, out[5] = grid cells per frame,
  * out[6] = FFT mode (option key 4), out[7] = 1 when the spread runs the
- * block-per-tile kernel (option key 6). */
+ * block-per-tile kernel (option key 6), out[8] = 1 when the forward column
+ * pass interpolates (option key 8). */
 int mrb_plan_info(mrb_plan* plan, int64_t* out, int nout);
 
 /* Toeplitz normal operator (no counterpart in the reference; its item

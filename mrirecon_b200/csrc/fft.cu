@@ -346,6 +346,94 @@ __global__ void __launch_bounds__(COL_NT) fwd_cols_kernel(const float2* __restri
   fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
 }
 
+// forward column pass fused with the interp (see fft.cuh): COLS columns per
+// block, the first COLS - 3 owned by the block's strip, the last three its
+// halo; the column transforms end in shared memory, then the threads walk the
+// strip's sample list.  Taps, signs, weights and the summation order are those
+// of the gridded interp (rows i0 outer, columns i1 inner), so the samples are
+// the same bit for bit.
+template <int G0>
+__global__ void __launch_bounds__(COL_NT, 2) fwd_cols_interp_kernel(const float2* __restrict__ Tb,
+                                                                 const float2* __restrict__ tw, Geo2 g,
+                                                                 mrb::ColInterp ci) {
+  constexpr int COLS = cols_per_block(G0);
+  constexpr int SW = COLS - 3;
+  constexpr int LD = G0 | 1;
+  constexpr int W = 4;
+  extern __shared__ float2 sm[];
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+  const int vol = blockIdx.x / ci.nstrips;
+  const int strip = blockIdx.x - vol * ci.nstrips;
+  const int k0 = strip * SW;
+  const float2* tv = Tb + (long long)vol * g.S0 * g.G1;
+  // the strip's first COL_NT samples (index and coordinates) are loaded while
+  // the columns transform
+  const int be = vol / g.C;
+  const int b = ci.B == 1 ? 0 : be / (ci.nb / ci.B);
+  const int key = b * ci.nstrips + strip;
+  const int e0 = ci.strip_start[key], e1 = ci.strip_start[key + 1];
+  const float* gx0 = ci.gx + (long long)b * 2 * ci.K;
+  int pk = 0;
+  float px[2] = {0.f, 0.f};
+  if (e0 + (int)threadIdx.x < e1) {
+    pk = ci.strip_entries[e0 + threadIdx.x];
+    px[0] = gx0[pk];
+    px[1] = gx0[ci.K + pk];
+  }
+  auto load0 = [&](int q, int n0) -> float2 {
+    const int r = n0 - g.off0;
+    if ((unsigned)r >= (unsigned)g.S0) return make_float2(0.f, 0.f);
+    int col = k0 + q;
+    col -= col >= g.G1 ? g.G1 : 0;
+    return tv[(long long)r * g.G1 + col];
+  };
+  auto store = [&](int q, int n0, float2 v) { sm[q * LD + n0] = v; };
+  fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
+  __syncthreads();
+  float2* yo = ci.y + (long long)vol * ci.K;
+  for (int e = e0 + threadIdx.x; e < e1; e += COL_NT) {
+    const bool first = e < e0 + COL_NT;
+    const int k = first ? pk : ci.strip_entries[e];
+    float w[2][W];
+    int row[W], cq[W];
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+      const float x = first ? px[d] : gx0[(long long)d * ci.K + k];
+      const int base = (int)floorf(x);
+      const float fx = x - (float)base;
+#pragma unroll
+      for (int o = 0; o < W; ++o) {
+        const int n = base - (W / 2 - 1) + o;
+        const float wd = mrb::kb_tap(ci.kb, o, fx);
+        w[d][o] = (n & 1) ? -wd : wd;
+        if (d == 0) {
+          row[o] = mrb::wrap_i(n, g.G0);
+        } else {
+          int q = mrb::wrap_i(n, g.G1) - k0;
+          q += q < 0 ? g.G1 : 0;
+          cq[o] = q * LD;
+        }
+      }
+    }
+    float s = ci.scale;
+    if (ci.wfwd) s *= ci.wfwd[(long long)b * ci.K + k];
+    float re = 0.f, im = 0.f;
+#pragma unroll
+    for (int i0 = 0; i0 < W; ++i0) {
+      float a0 = 0.f, b0 = 0.f;
+#pragma unroll
+      for (int i1 = 0; i1 < W; ++i1) {
+        const float2 v = sm[cq[i1] + row[i0]];
+        a0 = fmaf(w[1][i1], v.x, a0);
+        b0 = fmaf(w[1][i1], v.y, b0);
+      }
+      re = fmaf(w[0][i0], a0, re);
+      im = fmaf(w[0][i0], b0, im);
+    }
+    yo[k] = make_float2(re * s, im * s);
+  }
+}
+
 // adjoint column pass: T[vol][r][k1] = IFFT_G0(grid[vol][:][k1])[r + off0]
 template <int G0>
 __global__ void __launch_bounds__(COL_NT) adj_cols_kernel(const float2* __restrict__ grid, float2* __restrict__ Tb,
@@ -522,6 +610,22 @@ int launch_cols(bool forward, const float2* in, float2* out, const float2* tw, c
 }
 
 template <int G0>
+int launch_cols_interp(const float2* in, const float2* tw, const Geo2& g, int nb, const mrb::ColInterp& ci,
+                       cudaStream_t st) {
+  constexpr int COLS = cols_per_block(G0);
+  static_assert(COLS >= 4, "a strip needs at least one own column besides the 3 halo columns");
+  const size_t smem = (size_t)COLS * (G0 | 1) * sizeof(float2);
+  const long long blocks = (long long)nb * g.C * ci.nstrips;
+  MRB_REQUIRE(blocks < (1LL << 31), "too many column strips");
+  MRB_REQUIRE(g.G1 >= COLS, "grid narrower than a column block");
+  int rc;
+  if ((rc = set_smem((const void*)fwd_cols_interp_kernel<G0>, smem))) return rc;
+  fwd_cols_interp_kernel<G0><<<(unsigned)blocks, COL_NT, smem, st>>>(in, tw, g, ci);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+template <int G0>
 int launch_toeplitz_cols(float2* Tb, const float* P, const float2* tw, const Geo2& g, int nb, int B,
                          cudaStream_t st) {
   constexpr int COLS = cols_per_block(G0);
@@ -590,6 +694,30 @@ int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, 
   switch (G0) {
 #define MRB_CASE(n) \
   case n: return launch_cols<n>(forward != 0, in, out, tw0, g, nb, st);
+    MRB_FFT_LENGTHS(MRB_CASE)
+#undef MRB_CASE
+    default:
+      return fail(MRB_EINVAL, "no fused FFT for length %d", G0);
+  }
+}
+
+int interp_strip_width(int G0) {
+  switch (G0) {
+#define MRB_CASE(n) \
+  case n: return cols_per_block(n) - 3;
+    MRB_FFT_LENGTHS(MRB_CASE)
+#undef MRB_CASE
+    default:
+      return 0;
+  }
+}
+
+int fft2_columns_interp(const float2* Tb, const float2* tw0, int S0, int S1, int G0, int G1, int C, int nb,
+                        const ColInterp& ci, const double* skip, cudaStream_t st) {
+  const Geo2 g = make_geo2(S0, S1, G0, G1, C, skip);
+  switch (G0) {
+#define MRB_CASE(n) \
+  case n: return launch_cols_interp<n>(Tb, tw0, g, nb, ci, st);
     MRB_FFT_LENGTHS(MRB_CASE)
 #undef MRB_CASE
     default:

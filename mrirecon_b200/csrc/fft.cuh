@@ -29,6 +29,26 @@ int fft2_forward_rows(const void* x, const float2* maps, const float* rowfac, co
 // forward != 0: T -> grid (nb, C, G0, G1); else grid -> T
 int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, int S0, int S1, int G0, int G1, int C,
                  int nb, const double* skip, cudaStream_t st);
+// Forward column pass fused with the KB interp (2D): the block of a coil and
+// a strip of interp_strip_width(G0) grid columns transforms those columns and
+// the next three (the support of a sample starting in the strip reaches three
+// columns further; wrapped at G1) in shared memory and interpolates every
+// sample of the strip for that coil straight from there.  The oversampled
+// grid is never written.
+struct ColInterp {
+  const float* gx;           // (B, 2, K) grid coordinates
+  const float* wfwd;         // (B, K) forward weights or null
+  const int* strip_start;    // (B * nstrips + 1): per-frame strip lists
+  const int* strip_entries;  // sample indices, by (frame, strip), acquisition order within
+  float2* y;                 // (nb, C, K)
+  long long K;
+  int B, nb, nstrips;
+  float scale;               // ortho scale times the sample-side sign
+  KBPoly kb;
+};
+int interp_strip_width(int G0);
+int fft2_columns_interp(const float2* Tb, const float2* tw0, int S0, int S1, int G0, int G1, int C, int nb,
+                        const ColInterp& ci, const double* skip, cudaStream_t st);
 // Toeplitz normal operator on the band, in place: T <- IFFT_G0(P[frame] * FFT_G0(T)) per
 // column; P (B, G0, G1) real, frame = be / (nb / B) (0 when B == 1)
 int fft2_toeplitz_columns(float2* Tb, const float* P, const float2* tw0, int S0, int S1, int G0, int G1, int C, int nb,

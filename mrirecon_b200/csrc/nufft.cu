@@ -50,6 +50,10 @@ struct mrb_plan {
   int interp_mode = 0;
   int spread_kernel = 1;   // 1: block-per-tile kernels (2D tile 16, 3D tile 8) where they apply (3D default)
   int grid_mask = 1;       // fused FFT mode: the spread stores only cell pairs inside some support
+  int col_interp = 1;      // fused 2D mode: forward column pass and interp in one kernel (option key 8)
+  DevBuf strip_start;      // (B * nstrips + 1) per-frame lists of the samples starting in each column strip
+  DevBuf strip_entries;    // (B * K) sample indices
+  int nstrips = 0;
   DevBuf touch;            // (B, twords) bitmaps of the cells inside some sample's support
   long long twords = 0;
   DevBuf grid_adj;         // fused mode with the mask: the spread's own grid, zero outside the supports
@@ -1480,6 +1484,19 @@ __global__ void cell_base_kernel(const float* __restrict__ gx, int* __restrict__
 
 int grid_blocks(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
+// 2D column-strip key of each sample: frame, then the strip of sw columns that
+// holds its first tap column floor(gx1) - 1 (wrapped)
+__global__ void strip_key_kernel(const float* __restrict__ gx, unsigned* __restrict__ keys, int* __restrict__ vals,
+                                 long long K, int B, int G1, int sw, int nstrips) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)B * K) return;
+  const int b = (int)(i / K);
+  const long long k = i - (long long)b * K;
+  const int c = mrb::wrap_i((int)floorf(gx[((long long)b * 2 + 1) * K + k]) - 1, G1);
+  keys[i] = (unsigned)(b * nstrips + c / sw);
+  vals[i] = (int)k;
+}
+
 int ensure_fft(mrb_plan* p, int nb) {
   int batch = nb * p->C;
   if (p->fft && p->fft_batch == batch) return 0;
@@ -1626,7 +1643,8 @@ extern "C" int mrb_plan_destroy(mrb_plan* p) {
   for (DevBuf* b : {&p->gx, &p->entries, &p->tile_start, &p->items, &p->multi, &p->partials, &p->empty_keys, &p->maps, &p->invdeap, &p->wfwd,
                     &p->wadj, &p->grid, &p->tmp, &p->band, &p->tw0, &p->tw1, &p->psf, &p->ones, &p->grid_il,
                     &p->band2, &p->tw2, &p->rowfac,
-                    &p->seg_order, &p->touch, &p->grid_adj})
+                    &p->seg_order, &p->touch, &p->grid_adj,
+                    &p->strip_start, &p->strip_entries})
     b->release();
   delete p;
   return 0;
@@ -1671,6 +1689,10 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
     case 6:
       MRB_REQUIRE(value == 0 || value == 1, "spread kernel must be 0 (per-warp) or 1 (block per tile)");
       p->spread_kernel = (int)value;
+      return 0;
+    case 8:
+      MRB_REQUIRE(value == 0 || value == 1, "column interp must be 0 or 1");
+      p->col_interp = (int)value;
       return 0;
     case 7:
       MRB_REQUIRE(value == 0 || value == 1, "grid mask must be 0 or 1");
@@ -1853,6 +1875,37 @@ extern "C" int mrb_plan_set_points(mrb_plan* p, const float* traj, mrb_stream_t 
       popc_kernel<<<grid_blocks(nwords, 256), 256, 0, st>>>(bits, nwords, cntd.as<unsigned long long>());
     }
     p->twords = nwords;
+    // 2D: per-frame lists of the samples of each column strip (the fused
+    // forward column pass interpolates a strip's samples from shared memory)
+    p->nstrips = 0;
+    const int sw = p->nd == 2 ? mrb::interp_strip_width(p->G[0]) : 0;
+    if (sw > 0 && p->G[1] >= sw + 3) {
+      const int nstrips = (p->G[1] + sw - 1) / sw;
+      const long long n = (long long)p->B * p->K;
+      MRB_REQUIRE(n < (1LL << 31) && (long long)p->B * nstrips < (1LL << 31), "too many samples for strip lists");
+      int nkeys = p->B * nstrips;
+      int eb = 1;
+      while ((1LL << eb) <= nkeys) ++eb;
+      DevBuf sk, sks, sv;
+      if ((rc = sk.ensure(n * sizeof(unsigned)))) return rc;
+      if ((rc = sks.ensure(n * sizeof(unsigned)))) return rc;
+      if ((rc = sv.ensure(n * sizeof(int)))) return rc;
+      if ((rc = p->strip_entries.ensure(n * sizeof(int)))) return rc;
+      if ((rc = p->strip_start.ensure(((size_t)nkeys + 1) * sizeof(int)))) return rc;
+      strip_key_kernel<<<grid_blocks(n, 256), 256, 0, st>>>(p->gx.as<float>(), sk.as<unsigned>(), sv.as<int>(), p->K,
+                                                             p->B, p->G[1], sw, nstrips);
+      MRB_LAUNCH_CHECK();
+      size_t tb3 = 0;
+      cub::DeviceRadixSort::SortPairs(nullptr, tb3, sk.as<unsigned>(), sks.as<unsigned>(), sv.as<int>(),
+                                      p->strip_entries.as<int>(), (int)n, 0, eb, st);
+      if ((rc = p->tmp.ensure(tb3))) return rc;
+      cub::DeviceRadixSort::SortPairs(p->tmp.p, tb3, sk.as<unsigned>(), sks.as<unsigned>(), sv.as<int>(),
+                                      p->strip_entries.as<int>(), (int)n, 0, eb, st);
+      tile_start_kernel<<<grid_blocks(n, 256), 256, 0, st>>>(sks.as<unsigned>(), n, p->strip_start.as<int>(), nkeys);
+      MRB_LAUNCH_CHECK();
+      MRB_CUDA_TRY(cudaStreamSynchronize(st));   // the temporaries are freed on return
+      p->nstrips = nstrips;
+    }
     p->adj_zero = false;   // the supports changed: the spread grid is zeroed again before its next use
     MRB_LAUNCH_CHECK();
     unsigned long long touched = 0;
@@ -1939,6 +1992,11 @@ static int ensure_grid(mrb_plan* p, int nb, cudaStream_t st) {
   return ensure_fft(p, nb);
 }
 
+// the forward column pass also interpolates (fused 2D mode with strip lists)
+static bool col_interp_active(const mrb_plan* p) {
+  return p->fft_mode == 1 && p->nd == 2 && p->col_interp == 1 && p->nstrips > 0;
+}
+
 // the spread writes only touched cell pairs into a grid of its own (fused FFT mode)
 static bool spread_masked(const mrb_plan* p) {
   return p->fft_mode == 1 && p->grid_mask == 1 && p->touch.p != nullptr && p->adj_zero;
@@ -2007,6 +2065,22 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       return mrb::fft2_forward_rows(x, p->maps.as<float2>(), p->rowfac.as<float>(), p->invdeap.as<float>() + p->S[0],
                                     p->band.as<float2>(), p->tw1p, p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb,
                                     coil_images, p->skip, st);
+    if (stage == 1 && y != nullptr && col_interp_active(p)) {
+      mrb::ColInterp ci{};
+      ci.gx = p->gx.as<float>();
+      ci.wfwd = p->has_wfwd ? p->wfwd.as<float>() : nullptr;
+      ci.strip_start = p->strip_start.as<int>();
+      ci.strip_entries = p->strip_entries.as<int>();
+      ci.y = (float2*)y;
+      ci.K = p->K;
+      ci.B = p->B;
+      ci.nb = nb;
+      ci.nstrips = p->nstrips;
+      ci.scale = p->scale * p->gsign;
+      ci.kb = p->kb;
+      return mrb::fft2_columns_interp(p->band.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb,
+                                      ci, p->skip, st);
+    }
     if (stage == 1)
       return mrb::fft2_columns(1, p->band.as<float2>(), p->grid.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
                                p->G[1], p->C, nb, p->skip, st);
@@ -2236,8 +2310,11 @@ static int forward_impl(mrb_plan* p, const void* x, void* y, int nb, cudaStream_
   if ((rc = check_nb(p, nb))) return rc;
   MRB_REQUIRE(x != nullptr && y != nullptr, "null x or y");
   if ((rc = ensure_grid(p, nb, st))) return rc;
-  for (int stage : {0, 1, 2})
+  const bool fused_interp = col_interp_active(p);   // stage 1 interpolates as well
+  for (int stage : {0, 1, 2}) {
+    if (stage == 2 && fused_interp) break;
     if ((rc = run_stage(p, stage, x, y, nb, st, coil_images))) return rc;
+  }
   return 0;
 }
 
@@ -2274,8 +2351,9 @@ extern "C" int mrb_nufft_stage(mrb_plan* p, int stage, const void* x, void* y, i
 extern "C" int mrb_plan_info(mrb_plan* p, int64_t* out, int nout) {
   MRB_REQUIRE(p != nullptr && out != nullptr, "null plan or output");
   const int blk = p->spread_kernel == 1 && ((p->nd == 2 && p->tile == S2_T) || (p->nd == 3 && p->tile == S3_T));
-  int64_t v[8] = {p->n_entries, p->ntiles, p->touched, p->tile, p->coils_per_item, p->gtot(), p->fft_mode, blk};
-  for (int i = 0; i < nout && i < 8; ++i) out[i] = v[i];
+  int64_t v[9] = {p->n_entries, p->ntiles,  p->touched, p->tile, p->coils_per_item, p->gtot(), p->fft_mode, blk,
+                  col_interp_active(p)};
+  for (int i = 0; i < nout && i < 9; ++i) out[i] = v[i];
   return 0;
 }
 

@@ -32,7 +32,7 @@ from .layout import (AxisSpec, plan_image_layout, plan_kspace_layout, plan_image
 from .roles import Roles
 
 OPT_TILE, OPT_COILS_PER_ITEM, OPT_INTERP_MODE, OPT_CHUNK, OPT_FFT_MODE, OPT_INTERLEAVE, OPT_SPREAD_KERNEL, \
-    OPT_GRID_MASK = 0, 1, 2, 3, 4, 5, 6, 7
+    OPT_GRID_MASK, OPT_COL_INTERP = 0, 1, 2, 3, 4, 5, 6, 7, 8
 FFT_CUFFT, FFT_FUSED = 0, 1
 _DCF_MODES = {"none": 0, "balanced": 1, "standard": 2}
 
@@ -129,10 +129,10 @@ class KBPlan:
         _lib.check(self.lib.mrb_plan_set_skip_flag(self.h, ptr), "plan_set_skip_flag")
 
     def info(self) -> dict:
-        out = (ct.c_int64 * 8)()
-        _lib.check(self.lib.mrb_plan_info(self.h, out, 8), "plan_info")
+        out = (ct.c_int64 * 9)()
+        _lib.check(self.lib.mrb_plan_info(self.h, out, 9), "plan_info")
         keys = ("entries", "tiles_per_frame", "touched_cells", "tile", "coils_per_item", "grid_cells", "fft_mode",
-                "block_spread")
+                "block_spread", "col_interp")
         return {k: int(v) for k, v in zip(keys, out)}
 
     def cell_base(self) -> torch.Tensor:
@@ -196,6 +196,7 @@ class B200NUFFTAdapter:
     fft_mode: Optional[int] = None
     interleave: Optional[int] = None   # 3D: interp on a coil-interleaved grid copy (default 1)
     spread_kernel: Optional[int] = None  # 1 block per tile (default), 0 warp per tile and coil group
+    col_interp: Optional[int] = None     # 2D fused mode: interp inside the forward column pass (default 1)
     autotune: bool = False
     tuned: Optional[dict] = None
 
@@ -266,6 +267,8 @@ class B200NUFFTAdapter:
                 plan.set_option(OPT_INTERLEAVE, self.interleave)
             if self.spread_kernel is not None:
                 plan.set_option(OPT_SPREAD_KERNEL, self.spread_kernel)
+            if self.col_interp is not None:
+                plan.set_option(OPT_COL_INTERP, self.col_interp)
             plan.set_points(self._traj_BndK)
             plan.set_dcf(self._dcf_BK, self.dcf_mode, self.apply_dcf_in_fwd, self.apply_dcf_in_adj)
             plan.set_maps(self._maps)

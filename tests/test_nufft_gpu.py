@@ -410,3 +410,28 @@ def test_fused_fft_3d_matches_cufft(cuda, S, C, nb, B):
     _lib_forward_coils(fused, xc, yf, nb)
     _lib_forward_coils(dense, xc, yd, nb)
     assert rel(yf, yd) < 2e-6
+
+
+@pytest.mark.parametrize("S,C,nb,B,dcf", [((256, 256), 4, 2, 2, False), ((40, 48), 3, 4, 2, True),
+                                          ((64, 48), 1, 1, 1, False), ((24, 40), 5, 3, 1, True)])
+def test_fused_column_interp_identical(cuda, S, C, nb, B, dcf):
+    """2D fused mode: the forward column pass that interpolates each column
+    strip's samples from shared memory (option key 8, the default) gives the
+    same samples bit for bit as the column pass that writes the grid followed
+    by the interp kernel, including strips that wrap at the grid edge, the
+    frame mapping of a repeated trajectory and forward DCF weights."""
+    maps = _rand_c((C,) + S, 91, torch.complex64)
+    traj = torch.stack([phantoms.golden_angle_radial(9, 2 * S[0], 9 * f) for f in range(B)])
+    w = torch.rand(B, traj.shape[-1], generator=torch.Generator().manual_seed(92)) + 0.1 if dcf else None
+    kw = dict(dcf_mode="standard", apply_dcf_in_fwd=True, apply_dcf_in_adj=False) if dcf else {}
+    on = _adapter(maps, traj, w, **kw)
+    off = _adapter(maps, traj, w, col_interp=0, **kw)
+    assert on.plan.info()["col_interp"] == 1 and off.plan.info()["col_interp"] == 0
+    x = _rand_c((nb, 1) + S, 93, torch.complex64).to(cuda)
+    assert torch.equal(on.A(x), off.A(x))
+    xc = _rand_c((nb, C) + S, 94, torch.complex64).to(cuda)
+    y1 = torch.empty((nb, C, traj.shape[-1]), dtype=torch.complex64, device=cuda)
+    y0 = torch.empty_like(y1)
+    _lib_forward_coils(on, xc, y1, nb)
+    _lib_forward_coils(off, xc, y0, nb)
+    assert torch.equal(y1, y0)
