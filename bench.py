@@ -484,6 +484,9 @@ def e2e_solves(y, traj, maps, regm, cfgN, cnn, steps, ws, dev):
     torch.cuda.synchronize()
     per_step = []
     for _ in range(steps):
+        # the previous step's operator and solver are released before the clock starts
+        gc.collect()
+        torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
         x_h = one()
