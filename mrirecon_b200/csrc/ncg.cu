@@ -326,7 +326,7 @@ struct GradArgs {
 };
 
 template <int NS, int NU>
-__global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P, double* __restrict__ partials,
+__global__ void __launch_bounds__(RED_THREADS, NS <= 3 ? 4 : 1) grad_kernel(GradArgs a, TVPlan P, double* __restrict__ partials,
                                                            RedOut ro) {
   // dot products (which may cancel) accumulate in FP64 per thread; the TV
   // energies (non-negative terms) in FP32 per thread; reductions in FP64
@@ -453,17 +453,17 @@ __global__ void __launch_bounds__(RED_THREADS) grad_kernel(GradArgs a, TVPlan P,
 // trial step costs two FMAs and a square root per unit.
 constexpr int MT_MAX_J = 24;
 
-template <int NS, int NU>
-__global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __restrict__ x,
+template <int NS, int NU, int JMAX>
+__global__ void __launch_bounds__(RED_THREADS, JMAX <= 8 ? 4 : 1) tv_multi_kernel(const float2* __restrict__ x,
                                                                const float2* __restrict__ d,
                                                                const double* __restrict__ ts, int J, TVPlan P,
                                                                const double* skip, double* __restrict__ partials,
                                                                RedOut ro) {
   // energies are sums of non-negative terms: a thread sums its ~n / (blocks x threads)
   // voxels in FP32, the block and grid reductions run in FP64
-  float facc[MT_MAX_J];
+  float facc[JMAX];
 #pragma unroll
-  for (int j = 0; j < MT_MAX_J; ++j) facc[j] = 0.f;
+  for (int j = 0; j < JMAX; ++j) facc[j] = 0.f;
   if (skipped(skip) != 0.0) return;   // uniform over the grid: no partials, no counter
   const bool sk = false;
   __shared__ float tf[MT_MAX_J];   // trial steps, broadcast from shared memory
@@ -497,7 +497,7 @@ __global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __r
         }
       }
 #pragma unroll
-      for (int j = 0; j < MT_MAX_J; ++j) {
+      for (int j = 0; j < JMAX; ++j) {
         if (j >= J) continue;
         const float t = tf[j];
         float e = 0.f;
@@ -511,10 +511,10 @@ __global__ void __launch_bounds__(RED_THREADS) tv_multi_kernel(const float2* __r
       }
     }
   }
-  double acc[MT_MAX_J];
+  double acc[JMAX];
 #pragma unroll
-  for (int j = 0; j < MT_MAX_J; ++j) acc[j] = (double)facc[j];
-  block_reduce_finish<MT_MAX_J>(acc, partials, ro);
+  for (int j = 0; j < JMAX; ++j) acc[j] = (double)facc[j];
+  block_reduce_finish<JMAX>(acc, partials, ro);
 }
 
 // ---------------------------------------------------------------------------
@@ -863,9 +863,13 @@ struct GradLaunch {
   template <int NS, int NU, class... A>
   static void go(int nb, cudaStream_t st, A... args) { grad_kernel<NS, NU><<<nb, RED_THREADS, 0, st>>>(args...); }
 };
+// trial steps per launch: up to 8 (the first Armijo phase) or up to MT_MAX_J
+template <int JMAX>
 struct MultiLaunch {
   template <int NS, int NU, class... A>
-  static void go(int nb, cudaStream_t st, A... args) { tv_multi_kernel<NS, NU><<<nb, RED_THREADS, 0, st>>>(args...); }
+  static void go(int nb, cudaStream_t st, A... args) {
+    tv_multi_kernel<NS, NU, JMAX><<<nb, RED_THREADS, 0, st>>>(args...);
+  }
 };
 
 template <class L, int NS, class... A>
@@ -884,15 +888,15 @@ void launch_tv(const TVPlan& P, int nb, cudaStream_t st, A... args) {
   else launch_tv_nu<L, NSLOT>(P, nb, st, args...);
 }
 
-// grid of the TV passes: one wave of 3 resident 256-thread blocks per SM
-int tv_grid() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0, sms = 148;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    n = std::max(1, std::min(RED_MAX_BLOCKS, 3 * sms));
+// grid of the TV passes: one wave of `per_sm` resident 256-thread blocks on every SM
+int tv_grid(int per_sm = 3) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0, n = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    sms = n;
   }
-  return n;
+  return std::max(1, std::min(RED_MAX_BLOCKS, per_sm * sms));
 }
 
 int build_plan(TVPlan& P, int nd, const int* S, int F, const mrb_tv_term* terms, int nterms) {
@@ -1077,7 +1081,8 @@ extern "C" int mrb_tv_grad(int nd, const int* S, int F, const mrb_tv_term* terms
   a.skip = skip;
   a.skip_if_zero = skip_if_zero;
   cudaStream_t st = (cudaStream_t)stream;
-  int nb = std::min(red_blocks(P.n, 2), tv_grid());
+  // up to 3 difference axes the gradient pass keeps to 64 registers: 4 blocks per SM
+  int nb = std::min(red_blocks(P.n, 2), tv_grid(P.ns <= 3 ? 4 : 3));
   double* part = (double*)ws;
   launch_tv<GradLaunch>(P, nb, st, a, P, part, red_out(ws, out, GP_NV, 0, nullptr));
   MRB_LAUNCH_CHECK();
@@ -1093,10 +1098,15 @@ extern "C" int mrb_tv_multi(int nd, const int* S, int F, const mrb_tv_term* term
   int rc = build_plan(P, nd, S, F, terms, nterms);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  int nb = std::min(red_blocks(P.n, 2), tv_grid());
+  // up to 8 trial steps the kernel keeps to 64 registers: 4 resident blocks per SM
+  int nb = std::min(red_blocks(P.n, 2), tv_grid(J <= 8 ? 4 : 3));
   double* part = (double*)ws;
-  launch_tv<MultiLaunch>(P, nb, st, (const float2*)x, (const float2*)d, ts, J, P, skip, part,
-                         red_out(ws, out, J, 0, skip));
+  if (J <= 8)
+    launch_tv<MultiLaunch<8>>(P, nb, st, (const float2*)x, (const float2*)d, ts, J, P, skip, part,
+                              red_out(ws, out, J, 0, skip));
+  else
+    launch_tv<MultiLaunch<MT_MAX_J>>(P, nb, st, (const float2*)x, (const float2*)d, ts, J, P, skip, part,
+                                     red_out(ws, out, J, 0, skip));
   MRB_LAUNCH_CHECK();
   return 0;
 }
