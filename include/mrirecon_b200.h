@@ -133,7 +133,8 @@ int mrb_nufft_stage(mrb_plan* plan, int stage, const void* x, void* y, int nb, m
  * out[4] = coils per spread work item, out[5] = grid cells per frame,
  * out[6] = FFT mode (option key 4), out[7] = 1 when the spread runs the
  * block-per-tile kernel (option key 6), out[8] = 1 when the forward column
- * pass interpolates (option key 8). */
+ * pass interpolates (option key 8), out[9] = 1 when the sample lists match
+ * the current tile and chunk options (no set_points needed). */
 int mrb_plan_info(mrb_plan* plan, int64_t* out, int nout);
 
 /* Toeplitz normal operator (no counterpart in the reference; its item

@@ -82,7 +82,8 @@ def apply(plan, traj: torch.Tensor, tile: int, cpi: int, chunk: int, kernel: int
     plan.set_option(OPT_COILS_PER_ITEM, cpi)
     plan.set_option(OPT_CHUNK, chunk)
     plan.set_option(OPT_SPREAD_KERNEL, kernel)
-    plan.set_points(traj)
+    if not plan.info()["points_ready"]:      # the lists depend on the tile and chunk only
+        plan.set_points(traj)
 
 
 def tune(plan, traj: torch.Tensor, candidates: Optional[Iterable[Tuple[int, ...]]] = None,

@@ -1656,8 +1656,8 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
     case 0:
       MRB_REQUIRE(value == 4 || value == 8 || value == 16 || value == 32, "tile edge must be 4, 8, 16 or 32");
       MRB_REQUIRE(p->nd == 2 || value <= 8, "3D tile edge must be <= 8");
+      if (p->tile != (int)value) p->have_points = false;   // lists depend on the tile
       p->tile = (int)value;
-      p->have_points = false;   // lists depend on the tile
       return 0;
     case 1:
       MRB_REQUIRE(value >= 1 && value <= 64, "coils per item out of range");
@@ -1669,8 +1669,8 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
       return 0;
     case 3:
       MRB_REQUIRE(value >= 16 && value <= (1 << 20), "chunk must be 16 .. 2^20 samples");
+      if (p->chunk != (int)value) p->have_points = false;   // the item table depends on it
       p->chunk = (int)value;
-      p->have_points = false;   // the item table depends on it
       return 0;
     case 4:
       MRB_REQUIRE(value == 0 || value == 1, "fft mode must be 0 (cuFFT) or 1 (fused)");
@@ -2351,9 +2351,9 @@ extern "C" int mrb_nufft_stage(mrb_plan* p, int stage, const void* x, void* y, i
 extern "C" int mrb_plan_info(mrb_plan* p, int64_t* out, int nout) {
   MRB_REQUIRE(p != nullptr && out != nullptr, "null plan or output");
   const int blk = p->spread_kernel == 1 && ((p->nd == 2 && p->tile == S2_T) || (p->nd == 3 && p->tile == S3_T));
-  int64_t v[9] = {p->n_entries, p->ntiles,  p->touched, p->tile, p->coils_per_item, p->gtot(), p->fft_mode, blk,
-                  col_interp_active(p)};
-  for (int i = 0; i < nout && i < 9; ++i) out[i] = v[i];
+  int64_t v[10] = {p->n_entries, p->ntiles,  p->touched, p->tile, p->coils_per_item, p->gtot(), p->fft_mode, blk,
+                   col_interp_active(p), p->have_points ? 1 : 0};
+  for (int i = 0; i < nout && i < 10; ++i) out[i] = v[i];
   return 0;
 }
 

@@ -129,10 +129,10 @@ class KBPlan:
         _lib.check(self.lib.mrb_plan_set_skip_flag(self.h, ptr), "plan_set_skip_flag")
 
     def info(self) -> dict:
-        out = (ct.c_int64 * 9)()
-        _lib.check(self.lib.mrb_plan_info(self.h, out, 9), "plan_info")
+        out = (ct.c_int64 * 10)()
+        _lib.check(self.lib.mrb_plan_info(self.h, out, 10), "plan_info")
         keys = ("entries", "tiles_per_frame", "touched_cells", "tile", "coils_per_item", "grid_cells", "fft_mode",
-                "block_spread", "col_interp")
+                "block_spread", "col_interp", "points_ready")
         return {k: int(v) for k, v in zip(keys, out)}
 
     def cell_base(self) -> torch.Tensor:
