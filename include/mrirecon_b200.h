@@ -45,6 +45,13 @@ const char* mrb_last_error(void);
 /* Number of kernel launches this library has issued in the process (host
  * side; a launch recorded into a CUDA graph counts once, at capture). */
 int64_t mrb_launch_count(void);
+/* Device blocks of 1 MiB and more that destroyed plans released are cached
+ * (per device, up to 8 GiB) for the next plans, so that building operators
+ * repeatedly (a new trajectory per scan) avoids gigabyte cudaMalloc / cudaFree
+ * calls of very variable cost.  This returns the cached blocks to the driver
+ * (like torch.cuda.empty_cache); the cache is also emptied when an allocation
+ * would otherwise fail.  No reference counterpart. */
+int mrb_release_cached_memory(void);
 
 /* ------------------------------------------------------------------------
  * NUFFT plan (Kaiser-Bessel, oversampled grid, SENSE coils, B frames)
@@ -82,8 +89,9 @@ int mrb_plan_destroy(mrb_plan* plan);
  *         spread stores no zeros outside them; 0 full grid passes,
  * key 8 = 2D fused mode: the forward column pass interpolates the samples of
  *         each column strip from shared memory and never writes the grid
- *         (1, the default; set_points builds the per-frame strip lists) or
- *         writes the grid for a separate interp pass (0); same samples,
+ *         (1; set before set_points, which then builds the per-frame strip
+ *         lists) or writes the grid for a separate interp pass (0, the
+ *         default: 2% slower forward, but each kernel on its own); same samples,
  * key 5 = 3D forward interp on a coil-interleaved copy of the grid (1, the 3D
  *         default: a tiled transpose then 128-bit gathers of all coils of a
  *         cell; costs one more grid-sized buffer) or on the planar grid (0). */

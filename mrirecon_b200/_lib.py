@@ -43,6 +43,7 @@ _SIGS = {
     "mrb_version": (ct.c_int, []),
     "mrb_last_error": (ct.c_char_p, []),
     "mrb_launch_count": (ct.c_int64, []),
+    "mrb_release_cached_memory": (ct.c_int, []),
     "mrb_nufft_stage": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p]),
     "mrb_plan_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, c_int_p, ct.c_int, ct.c_int, ct.c_int64,
                                    ct.c_int, ct.c_double, ct.c_int]),

@@ -3,6 +3,8 @@
 #include <cstdarg>
 #include <atomic>
 #include <cstring>
+#include <mutex>
+#include <vector>
 
 #include "mrb_common.cuh"
 
@@ -26,6 +28,76 @@ int fail(int code, const char* fmt, ...) {
   vsnprintf(g_err, sizeof(g_err), fmt, ap);
   va_end(ap);
   return code;
+}
+
+// ---------------------------------------------------------------------------
+// block cache of dev_alloc / dev_free
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t POOL_MIN_BLOCK = 1u << 20;            // smaller blocks go straight to the driver
+constexpr size_t POOL_CAP = (size_t)8 << 30;           // bytes kept per device
+
+struct PoolBlock {
+  void* p;
+  size_t bytes;
+  int dev;
+};
+
+std::mutex g_pool_mu;
+std::vector<PoolBlock> g_pool;
+
+size_t pool_bytes(int dev) {
+  size_t t = 0;
+  for (const PoolBlock& b : g_pool)
+    if (b.dev == dev) t += b.bytes;
+  return t;
+}
+}  // namespace
+
+void* dev_alloc(size_t n, size_t* got) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (n >= POOL_MIN_BLOCK) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    int best = -1;
+    for (int i = 0; i < (int)g_pool.size(); ++i) {
+      const PoolBlock& b = g_pool[i];
+      if (b.dev == dev && b.bytes >= n && b.bytes <= 2 * n && (best < 0 || b.bytes < g_pool[best].bytes)) best = i;
+    }
+    if (best >= 0) {
+      void* p = g_pool[best].p;
+      *got = g_pool[best].bytes;
+      g_pool.erase(g_pool.begin() + best);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  if (cudaMalloc(&p, n) != cudaSuccess) {
+    cudaGetLastError();
+    // the cache may hold the memory: hand it back and try once more
+    mrb_release_cached_memory();
+    if (cudaMalloc(&p, n) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+  }
+  *got = n;
+  return p;
+}
+
+void dev_free(void* p, size_t bytes) {
+  if (!p) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (bytes >= POOL_MIN_BLOCK) {
+    cudaDeviceSynchronize();   // what cudaFree would wait for: no kernel may still use the block
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (pool_bytes(dev) + bytes <= POOL_CAP) {
+      g_pool.push_back(PoolBlock{p, bytes, dev});
+      return;
+    }
+  }
+  cudaFree(p);
 }
 
 // I0 by its power series (A&S 9.6.10), double precision, host only.
@@ -77,6 +149,22 @@ void kb_poly_init(KBPoly& p, int W, double beta) {
 }
 
 }  // namespace mrb
+
+extern "C" int mrb_release_cached_memory(void) {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  std::vector<mrb::PoolBlock> keep;
+  {
+    std::lock_guard<std::mutex> lk(mrb::g_pool_mu);
+    keep.swap(mrb::g_pool);
+  }
+  for (const mrb::PoolBlock& b : keep) {
+    cudaSetDevice(b.dev);
+    cudaFree(b.p);
+  }
+  cudaSetDevice(cur);
+  return 0;
+}
 
 extern "C" int mrb_version(void) { return 1; }
 extern "C" int64_t mrb_launch_count(void) { return (int64_t)mrb::g_launches.load(); }

@@ -40,6 +40,18 @@ void count_launch();
 
 inline int ceil_div_i(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
+// Device memory of the plans.  Large blocks (>= 1 MiB) released by one plan
+// are kept, per device and up to a cap, for the next plan of a similar size:
+// a process that builds operators repeatedly (a new trajectory per scan) then
+// does not pay a cudaMalloc / cudaFree of gigabytes each time, whose cost
+// varies by orders of magnitude.  A released block joins the cache only after
+// the device has finished its work (a device synchronisation, as cudaFree
+// itself implies), so a later owner never races the previous one; like
+// cudaFree, releasing is not allowed inside a stream capture.
+// mrb_release_cached_memory() returns the cached blocks to the driver.
+void* dev_alloc(size_t n, size_t* got);   // nullptr on failure
+void dev_free(void* p, size_t bytes);
+
 // Device buffer owned by a plan.
 struct DevBuf {
   void* p = nullptr;
@@ -50,20 +62,16 @@ struct DevBuf {
   ~DevBuf() { release(); }
   int ensure(size_t n) {
     if (n <= bytes) return 0;
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
+    release();
     if (n == 0) return 0;
-    cudaError_t e = cudaMalloc(&p, n);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      return fail(MRB_ENOMEM, "cudaMalloc(%zu) failed: %s", n, cudaGetErrorString(e));
-    }
-    bytes = n;
+    size_t got = 0;
+    p = dev_alloc(n, &got);
+    if (!p) return fail(MRB_ENOMEM, "device allocation of %zu bytes failed", n);
+    bytes = got;
     return 0;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) dev_free(p, bytes);
     p = nullptr;
     bytes = 0;
   }

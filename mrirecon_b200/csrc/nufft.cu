@@ -50,7 +50,7 @@ struct mrb_plan {
   int interp_mode = 0;
   int spread_kernel = 1;   // 1: block-per-tile kernels (2D tile 16, 3D tile 8) where they apply (3D default)
   int grid_mask = 1;       // fused FFT mode: the spread stores only cell pairs inside some support
-  int col_interp = 1;      // fused 2D mode: forward column pass and interp in one kernel (option key 8)
+  int col_interp = 0;      // fused 2D mode: forward column pass and interp in one kernel (option key 8)
   DevBuf strip_start;      // (B * nstrips + 1) per-frame lists of the samples starting in each column strip
   DevBuf strip_entries;    // (B * K) sample indices
   int nstrips = 0;
@@ -1692,6 +1692,7 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
       return 0;
     case 8:
       MRB_REQUIRE(value == 0 || value == 1, "column interp must be 0 or 1");
+      if (value == 1 && p->nstrips == 0) p->have_points = false;   // set_points builds the strip lists
       p->col_interp = (int)value;
       return 0;
     case 7:
@@ -1878,7 +1879,7 @@ extern "C" int mrb_plan_set_points(mrb_plan* p, const float* traj, mrb_stream_t 
     // 2D: per-frame lists of the samples of each column strip (the fused
     // forward column pass interpolates a strip's samples from shared memory)
     p->nstrips = 0;
-    const int sw = p->nd == 2 ? mrb::interp_strip_width(p->G[0]) : 0;
+    const int sw = p->nd == 2 && p->col_interp == 1 ? mrb::interp_strip_width(p->G[0]) : 0;
     if (sw > 0 && p->G[1] >= sw + 3) {
       const int nstrips = (p->G[1] + sw - 1) / sw;
       const long long n = (long long)p->B * p->K;

@@ -196,7 +196,7 @@ class B200NUFFTAdapter:
     fft_mode: Optional[int] = None
     interleave: Optional[int] = None   # 3D: interp on a coil-interleaved grid copy (default 1)
     spread_kernel: Optional[int] = None  # 1 block per tile (default), 0 warp per tile and coil group
-    col_interp: Optional[int] = None     # 2D fused mode: interp inside the forward column pass (default 1)
+    col_interp: Optional[int] = None     # 2D fused mode: interp inside the forward column pass (default 0)
     autotune: bool = False
     tuned: Optional[dict] = None
 

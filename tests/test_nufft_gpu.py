@@ -416,7 +416,7 @@ def test_fused_fft_3d_matches_cufft(cuda, S, C, nb, B):
                                           ((64, 48), 1, 1, 1, False), ((24, 40), 5, 3, 1, True)])
 def test_fused_column_interp_identical(cuda, S, C, nb, B, dcf):
     """2D fused mode: the forward column pass that interpolates each column
-    strip's samples from shared memory (option key 8, the default) gives the
+    strip's samples from shared memory (option key 8) gives the
     same samples bit for bit as the column pass that writes the grid followed
     by the interp kernel, including strips that wrap at the grid edge, the
     frame mapping of a repeated trajectory and forward DCF weights."""
@@ -424,8 +424,8 @@ def test_fused_column_interp_identical(cuda, S, C, nb, B, dcf):
     traj = torch.stack([phantoms.golden_angle_radial(9, 2 * S[0], 9 * f) for f in range(B)])
     w = torch.rand(B, traj.shape[-1], generator=torch.Generator().manual_seed(92)) + 0.1 if dcf else None
     kw = dict(dcf_mode="standard", apply_dcf_in_fwd=True, apply_dcf_in_adj=False) if dcf else {}
-    on = _adapter(maps, traj, w, **kw)
-    off = _adapter(maps, traj, w, col_interp=0, **kw)
+    on = _adapter(maps, traj, w, col_interp=1, **kw)
+    off = _adapter(maps, traj, w, **kw)
     assert on.plan.info()["col_interp"] == 1 and off.plan.info()["col_interp"] == 0
     x = _rand_c((nb, 1) + S, 93, torch.complex64).to(cuda)
     assert torch.equal(on.A(x), off.A(x))
@@ -435,3 +435,25 @@ def test_fused_column_interp_identical(cuda, S, C, nb, B, dcf):
     _lib_forward_coils(on, xc, y1, nb)
     _lib_forward_coils(off, xc, y0, nb)
     assert torch.equal(y1, y0)
+
+
+def test_plan_memory_reuse_and_release(cuda):
+    """Plans built one after another reuse the device blocks of destroyed plans
+    (a block cache instead of cudaMalloc / cudaFree per plan); results stay
+    identical, and mrb_release_cached_memory hands the cache back."""
+    import gc
+    from mrirecon_b200 import _lib
+    maps = phantoms.coil_maps(64, 4).to(torch.complex64)
+    traj = phantoms.grasp_trajectory(3, 9, 128)
+    x = _rand_c((3, 1, 64, 64), 101, torch.complex64).to(cuda)
+    y = _rand_c((3, 4, traj.shape[-1]), 102, torch.complex64).to(cuda)
+    outs = []
+    for rnd in range(3):
+        ad = _adapter(maps, traj)
+        outs.append((ad.A(x), ad.AH(y)))
+        del ad
+        gc.collect()
+        if rnd == 1:
+            assert _lib.load().mrb_release_cached_memory() == 0
+    for ya, xa in outs[1:]:
+        assert torch.equal(ya, outs[0][0]) and torch.equal(xa, outs[0][1])
