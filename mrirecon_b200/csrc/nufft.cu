@@ -247,9 +247,13 @@ __global__ void fill_int_kernel(int* p, long long n, int v) {
 }
 
 // touched-cell count (for roofline bookkeeping): marks cells in a bitmap
-__global__ void touch_kernel(const float* __restrict__ gx, unsigned* __restrict__ bits, Geo g, int W, int b) {
+// frame b = blockIdx.y marks the cells of its samples' supports in its bitmap
+__global__ void touch_kernel(const float* __restrict__ gx, unsigned* __restrict__ bits_all, long long nwords, Geo g,
+                             int W) {
   long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= g.K) return;
+  const int b = blockIdx.y;
+  unsigned* bits = bits_all + (long long)b * nwords;
   int base[3] = {0, 0, 0};
   for (int d = 0; d < g.nd; ++d) base[d] = (int)floorf(gx[((long long)b * g.nd + d) * g.K + k]);
   int lo = W / 2 - 1;
@@ -1870,11 +1874,12 @@ extern "C" int mrb_plan_set_points(mrb_plan* p, const float* traj, mrb_stream_t 
     if ((rc = cntd.ensure(sizeof(unsigned long long)))) return rc;
     MRB_CUDA_TRY(cudaMemsetAsync(cntd.p, 0, sizeof(unsigned long long), st));
     MRB_CUDA_TRY(cudaMemsetAsync(p->touch.p, 0, (size_t)p->B * nwords * sizeof(unsigned), st));
-    for (int b = 0; b < p->B; ++b) {
-      unsigned* bits = p->touch.as<unsigned>() + (long long)b * nwords;
-      touch_kernel<<<grid_blocks(p->K, 256), 256, 0, st>>>(p->gx.as<float>(), bits, g, p->W, b);
-      popc_kernel<<<grid_blocks(nwords, 256), 256, 0, st>>>(bits, nwords, cntd.as<unsigned long long>());
-    }
+    MRB_REQUIRE(p->B <= 65535, "too many trajectory frames");
+    touch_kernel<<<dim3(grid_blocks(p->K, 256), p->B), 256, 0, st>>>(p->gx.as<float>(), p->touch.as<unsigned>(),
+                                                                      nwords, g, p->W);
+    popc_kernel<<<grid_blocks((long long)p->B * nwords, 256), 256, 0, st>>>(p->touch.as<unsigned>(),
+                                                                           (long long)p->B * nwords,
+                                                                           cntd.as<unsigned long long>());
     p->twords = nwords;
     // 2D: per-frame lists of the samples of each column strip (the fused
     // forward column pass interpolates a strip's samples from shared memory)
