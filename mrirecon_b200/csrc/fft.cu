@@ -346,6 +346,36 @@ __global__ void __launch_bounds__(COL_NT) fwd_cols_kernel(const float2* __restri
   fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
 }
 
+// forward column pass with a coil-interleaved output (3D x pass, see fft.cuh):
+// a block transforms IL_ROWS (column, coil) pairs, coil fastest, so that each
+// output row is IL_ROWS contiguous values of the (cell, coil) layout; the band
+// is read CT coils at a time per column
+constexpr int IL_ROWS = 32;
+
+template <int G0, int CT>
+__global__ void __launch_bounds__(COL_NT, G0 <= 320 ? 2 : 1) fwd_cols_il_kernel(const float2* __restrict__ Tb, float2* __restrict__ out,
+                                                             const float2* __restrict__ tw, Geo2 g) {
+  constexpr int LD = G0 | 1;
+  constexpr int CB = IL_ROWS / CT;   // columns per block
+  extern __shared__ float2 sm[];
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+  const int cblocks = (g.G1 + CB - 1) / CB;
+  const int be = blockIdx.x / cblocks;
+  const int k0 = (blockIdx.x - be * cblocks) * CB;
+  const float2* tb = Tb + (long long)be * CT * g.S0 * g.G1;   // (coil, band row, column)
+  float2* ob = out + (long long)be * g.gtot * CT;              // (cell, coil)
+  auto load0 = [&](int q, int n0) -> float2 {
+    const int j = q / CT, c = q - j * CT;
+    const int r = n0 - g.off0;
+    if ((unsigned)r >= (unsigned)g.S0 || k0 + j >= g.G1) return make_float2(0.f, 0.f);
+    return tb[((long long)c * g.S0 + r) * g.G1 + k0 + j];
+  };
+  auto store = [&](int q, int n0, float2 v) {
+    if (k0 + q / CT < g.G1) ob[((long long)n0 * g.G1 + k0) * CT + q] = v;
+  };
+  fft_stages<G0, 0, IL_ROWS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
+}
+
 // forward column pass fused with the interp (see fft.cuh): COLS columns per
 // block, the first COLS - 3 owned by the block's strip, the last three its
 // halo; the column transforms end in shared memory, then the threads walk the
@@ -609,6 +639,20 @@ int launch_cols(bool forward, const float2* in, float2* out, const float2* tw, c
   return 0;
 }
 
+template <int G0, int CT>
+int launch_cols_il(const float2* in, float2* out, const float2* tw, const Geo2& g, int nb, cudaStream_t st) {
+  constexpr int CB = IL_ROWS / CT;
+  const size_t smem = (size_t)IL_ROWS * (G0 | 1) * sizeof(float2);
+  MRB_REQUIRE(smem <= 200 * 1024, "interleaved column pass needs %zu bytes of shared memory", smem);
+  const long long blocks = (long long)nb * ((g.G1 + CB - 1) / CB);
+  MRB_REQUIRE(blocks < (1LL << 31), "too many columns");
+  int rc;
+  if ((rc = set_smem((const void*)fwd_cols_il_kernel<G0, CT>, smem))) return rc;
+  fwd_cols_il_kernel<G0, CT><<<(unsigned)blocks, COL_NT, smem, st>>>(in, out, tw, g);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
 template <int G0>
 int launch_cols_interp(const float2* in, const float2* tw, const Geo2& g, int nb, const mrb::ColInterp& ci,
                        cudaStream_t st) {
@@ -699,6 +743,28 @@ int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, 
     default:
       return fail(MRB_EINVAL, "no fused FFT for length %d", G0);
   }
+}
+
+bool fft2_columns_il_supported(int G0, int C) {
+  return (C == 8 || C == 16 || C == 32) && length_supported(G0) && (size_t)IL_ROWS * (G0 | 1) * 8 <= 200 * 1024;
+}
+
+int fft2_columns_il(const float2* Tb, float2* out, const float2* tw0, int S0, int G0, int G1, int C, int nb,
+                    const double* skip, cudaStream_t st) {
+  const Geo2 g = make_geo2(S0, G1, G0, G1, C, skip);
+  switch (G0) {
+#define MRB_CASE(n)                                                             \
+  case n:                                                                       \
+    if (C == 8) return launch_cols_il<n, 8>(Tb, out, tw0, g, nb, st);           \
+    if (C == 16) return launch_cols_il<n, 16>(Tb, out, tw0, g, nb, st);         \
+    if (C == 32) return launch_cols_il<n, 32>(Tb, out, tw0, g, nb, st);         \
+    break;
+    MRB_FFT_LENGTHS(MRB_CASE)
+#undef MRB_CASE
+    default:
+      break;
+  }
+  return fail(MRB_EINVAL, "no interleaved column pass for length %d and %d coils", G0, C);
 }
 
 int interp_strip_width(int G0) {

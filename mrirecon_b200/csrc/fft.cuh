@@ -29,6 +29,12 @@ int fft2_forward_rows(const void* x, const float2* maps, const float* rowfac, co
 // forward != 0: T -> grid (nb, C, G0, G1); else grid -> T
 int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, int S0, int S1, int G0, int G1, int C,
                  int nb, const double* skip, cudaStream_t st);
+// Forward column pass whose output is coil-interleaved: in (nb, C, S0, G1)
+// band rows -> out (nb, G0 * G1 cells, C), for C in {8, 16, 32} (the 3D x pass
+// writing the interp's (cell, coil) grid copy directly)
+bool fft2_columns_il_supported(int G0, int C);
+int fft2_columns_il(const float2* Tb, float2* out, const float2* tw0, int S0, int G0, int G1, int C, int nb,
+                    const double* skip, cudaStream_t st);
 // Forward column pass fused with the KB interp (2D): the block of a coil and
 // a strip of interp_strip_width(G0) grid columns transforms those columns and
 // the next three (the support of a sample starting in the strip reaches three

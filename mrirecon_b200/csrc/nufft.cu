@@ -1998,6 +1998,12 @@ static int ensure_grid(mrb_plan* p, int nb, cudaStream_t st) {
   return ensure_fft(p, nb);
 }
 
+// fused 3D mode with the interleaved interp: the x column pass writes the
+// (cell, coil) copy itself, the interp stage needs no transpose
+static bool il_direct(const mrb_plan* p) {
+  return p->fft_mode == 1 && p->nd == 3 && p->il == 1 && mrb::fft2_columns_il_supported(p->G[0], p->C);
+}
+
 // the forward column pass also interpolates (fused 2D mode with strip lists)
 static bool col_interp_active(const mrb_plan* p) {
   return p->fft_mode == 1 && p->nd == 2 && p->col_interp == 1 && p->nstrips > 0;
@@ -2051,6 +2057,9 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       if ((rc3 = mrb::fft2_columns(1, b1, b2, p->tw1p, p->S[1], p->S[2], p->G[1], p->G[2], p->C * p->S[0], nb,
                                    p->skip, st)))
         return rc3;
+      if (il_direct(p))
+        return mrb::fft2_columns_il(b2, p->grid_il.as<float2>(), p->tw0p, p->S[0], p->G[0], GG, p->C, nb, p->skip,
+                                    st);
       return mrb::fft2_columns(1, b2, p->grid.as<float2>(), p->tw0p, p->S[0], GG, p->G[0], GG, p->C, nb, p->skip,
                                st);
     }
@@ -2135,11 +2144,13 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     if (p->il && p->nd == 3) {
       MRB_REQUIRE(nb <= 65535, "too many frames in one call");
       MRB_REQUIRE(p->gtot() * p->C < (1LL << 31), "interleaved grid of one frame exceeds 2^31 elements");
-      const long long tb = (p->gtot() + TR_CELLS - 1) / TR_CELLS;
-      MRB_REQUIRE(tb < (1LL << 31), "grid too large for the coil transpose");
-      coil_interleave_kernel<<<dim3((unsigned)tb, nb), 256, 0, st>>>(p->grid.as<float2>(), p->grid_il.as<float2>(),
-                                                                     p->gtot(), p->C, p->skip);
-      MRB_LAUNCH_CHECK();
+      if (!il_direct(p)) {   // else the x column pass wrote the interleaved copy
+        const long long tb = (p->gtot() + TR_CELLS - 1) / TR_CELLS;
+        MRB_REQUIRE(tb < (1LL << 31), "grid too large for the coil transpose");
+        coil_interleave_kernel<<<dim3((unsigned)tb, nb), 256, 0, st>>>(p->grid.as<float2>(), p->grid_il.as<float2>(),
+                                                                       p->gtot(), p->C, p->skip);
+        MRB_LAUNCH_CHECK();
+      }
       a.grid = p->grid_il.as<float2>();
       a.seg = p->nseg > 0 && p->interp_mode == 1 ? p->seg_order.as<int>() : nullptr;
       a.nseg = p->nseg;

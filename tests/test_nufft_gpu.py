@@ -389,7 +389,8 @@ def test_2d_pair_parallel_interp_identical(cuda, C, nb, B):
         assert torch.equal(ad.A(x), y1)
 
 
-@pytest.mark.parametrize("S,C,nb,B", [((16, 20, 24), 3, 2, 1), ((24, 16, 32), 4, 2, 2), ((20, 20, 20), 1, 1, 1)])
+@pytest.mark.parametrize("S,C,nb,B", [((16, 20, 24), 3, 2, 1), ((24, 16, 32), 4, 2, 2), ((20, 20, 20), 1, 1, 1),
+                                      ((16, 20, 24), 16, 2, 2), ((20, 16, 24), 8, 1, 1)])
 def test_fused_fft_3d_matches_cufft(cuda, S, C, nb, B):
     """3D zero-pruned passes (z rows fused with SENSE/deapodisation, then y and x
     columns, and the reverse with crop and coil sum; the default where every
@@ -410,6 +411,10 @@ def test_fused_fft_3d_matches_cufft(cuda, S, C, nb, B):
     _lib_forward_coils(fused, xc, yf, nb)
     _lib_forward_coils(dense, xc, yd, nb)
     assert rel(yf, yd) < 2e-6
+    # with 8 / 16 / 32 coils the x pass writes the interp's (cell, coil) copy
+    # itself; the planar interp reads the same values in the same order
+    planar = _adapter(maps, traj, interleave=0)
+    assert torch.equal(fused.A(x), planar.A(x))
 
 
 @pytest.mark.parametrize("S,C,nb,B,dcf", [((256, 256), 4, 2, 2, False), ((40, 48), 3, 4, 2, True),
