@@ -530,6 +530,7 @@ def main(argv=None):
     ap.add_argument("--batch", type=int, default=2)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--frames", type=int, default=8)
+    ap.add_argument("--init", default=None, help="start training from these weights (fine-tuning)")
     a = ap.parse_args(argv)
     if a.eval:
         net = WarmStartCNN("cuda", seed=0)
@@ -543,6 +544,8 @@ def main(argv=None):
     xa, xr = make_pairs(a.series, spec, per_solve=a.per_solve, log=lambda m: print(m, flush=True))
     print(f"pairs: {time.time() - t0:.1f} s", flush=True)
     net = WarmStartCNN("cuda", seed=0)
+    if a.init:
+        net.load(a.init)
     t1 = time.time()
     hist = net.train(xa, xr, epochs=a.epochs, batch=a.batch, lr=a.lr, log=lambda m: print(m, flush=True))
     print(f"training: {time.time() - t1:.1f} s, loss per epoch {hist}", flush=True)
