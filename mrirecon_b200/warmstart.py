@@ -412,21 +412,31 @@ def ramp_adjoint(op, y: torch.Tensor) -> torch.Tensor:
     """The network input: the density-compensated adjoint A^H(w * y) (gridding
     reconstruction) with the radial ramp w = max(|k|, pi / (2 max S)) / pi.
     `op` is a B200 NUFFT front-end or adapter and y is in its canonical
-    (B, C, K) layout; the ramp operator is built once and cached on the adapter."""
+    (B, C, K) layout; the ramp weights are computed once and cached on the adapter."""
     from .nufft import B200NUFFTAdapter
     ad = getattr(op, "backend", op)
+    C, K = int(ad._im_shape[0]), int(ad._K)
+    w = getattr(ad, "_ramp_w", None)
+    if w is None:
+        S = ad._im_shape[1:]
+        kr = torch.linalg.vector_norm(ad._traj_BndK, dim=1)
+        w = (kr.clamp_min(math.pi / (2.0 * max(S))) / math.pi).to(torch.float32)
+        ad._ramp_w = w
+    yy = y.reshape(-1, C, K)
+    if ad._dcf_BK is None or ad.dcf_mode == "none" or not ad.apply_dcf_in_adj:
+        # the operator's own adjoint applied to the ramp-weighted samples (frame
+        # be of a B_eff batch uses trajectory frame be // (nb / B))
+        nb, B = int(yy.shape[0]), int(w.shape[0])
+        wb = w if B in (1, nb) else w.repeat_interleave(nb // B, dim=0)
+        return ad.AH((yy * wb[:, None, :]).contiguous())
+    # an operator with its own adjoint weights: a second plan with the ramp alone
     r = getattr(ad, "_ramp_adapter", None)
     if r is None:
-        traj = ad._traj_BndK
-        S = ad._im_shape[1:]
-        kr = torch.linalg.vector_norm(traj, dim=1)
-        w = kr.clamp_min(math.pi / (2.0 * max(S))) / math.pi
         r = B200NUFFTAdapter(ndim=ad.ndim, dcf_mode="standard", apply_dcf_in_fwd=False, apply_dcf_in_adj=True,
                              kwidth=ad.kwidth, osf=ad.osf, norm=ad.norm)
-        r.prepare(ad._im_shape, traj, w, ad._maps, torch.complex64, ad._dev)
+        r.prepare(ad._im_shape, ad._traj_BndK, w, ad._maps, torch.complex64, ad._dev)
         ad._ramp_adapter = r
-    C, K = int(ad._im_shape[0]), int(ad._K)
-    return r.AH(y.reshape(-1, C, K))
+    return r.AH(yy)
 
 
 def _ls_scaled(op, y, x):

@@ -48,3 +48,28 @@ def test_fallback_to_adjoint_start(cuda):
     assert torch.equal(s.x, _ls_scaled(ad, y, ad.AH(y)))
     s.run()
     assert s.stop_reason.startswith("relative")
+
+
+@pytest.mark.parametrize("nb,B", [(4, 4), (4, 2), (3, 1)])
+def test_ramp_adjoint_through_the_operator(cuda, nb, B):
+    """The network input A^H(w y) with the radial ramp w, computed by the
+    operator's own adjoint on ramp-weighted samples, equals the adjoint of a
+    second plan that carries w as its adjoint weights (FP32 rounding apart),
+    including the frame mapping of a repeated trajectory."""
+    from mrirecon_b200.warmstart import ramp_adjoint
+    import math
+    N, C = 48, 3
+    maps = phantoms.coil_maps(N, C)
+    traj = phantoms.grasp_trajectory(B, 11, 2 * N)
+    ad = B200NUFFTAdapter(ndim=2)
+    ad.prepare((C, N, N), traj.to(cuda), None, maps.to(cuda), torch.complex64, cuda)
+    g = torch.Generator().manual_seed(5)
+    y = (torch.randn((nb, C, traj.shape[-1]), generator=g)
+         + 1j * torch.randn((nb, C, traj.shape[-1]), generator=g)).to(torch.complex64).to(cuda)
+    kr = torch.linalg.vector_norm(traj.to(cuda), dim=1)
+    w = kr.clamp_min(math.pi / (2.0 * N)) / math.pi
+    r = B200NUFFTAdapter(ndim=2, dcf_mode="standard", apply_dcf_in_fwd=False, apply_dcf_in_adj=True)
+    r.prepare((C, N, N), traj.to(cuda), w, maps.to(cuda), torch.complex64, cuda)
+    ref = r.AH(y)
+    out = ramp_adjoint(ad, y)
+    assert float(torch.linalg.vector_norm(out - ref) / torch.linalg.vector_norm(ref)) < 1e-6
