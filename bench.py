@@ -595,7 +595,7 @@ def run_b200(args, w, ws, rank, local):
         ("pre", "interp", "spread", "post")
     mine = {k: stages[k] for k in own}
     dom = max(mine, key=mine.get)
-    kname = {"pre": "fwd_rows_kernel", "fft": "fwd_cols_kernel", "interp": "interp_kernel",
+    kname = {"pre": "fwd_rows_kernel", "fft": "fwd_cols_kernel", "interp": "interp2p_kernel",
              "spread": "spread_kernel", "ifft": "adj_cols_kernel", "post": "adj_rows_kernel"}
     if info.get("fft_mode", 0) != 1:
         kname.update(pre="pre_fft_kernel", post="post_ifft_kernel")
