@@ -462,3 +462,19 @@ def test_plan_memory_reuse_and_release(cuda):
             assert _lib.load().mrb_release_cached_memory() == 0
     for ya, xa in outs[1:]:
         assert torch.equal(ya, outs[0][0]) and torch.equal(xa, outs[0][1])
+
+
+@pytest.mark.parametrize("S,B,spokes", [((32, 32), 2, 24), ((20, 24), 1, 16), ((12, 10, 8), 1, 0)])
+def test_estimate_dcf_vs_oracle(cuda, S, B, spokes):
+    """Density compensation by the Pipe-Menon iteration on the GPU gridding
+    (spread then interp on the plan's grid, no FFT) against the FP64 CPU
+    restatement: relative L2 <= 1e-4 after 20 iterations (FP32 grid sums)."""
+    from mrirecon_b200.dcf import estimate_dcf
+    from oracle.dcf import pipe_menon
+    if len(S) == 2:
+        traj = torch.stack([phantoms.golden_angle_radial(spokes, 2 * max(S), spokes * f) for f in range(B)])
+    else:
+        traj = phantoms.random_traj(B, 3, 600, seed=111)
+    w = estimate_dcf(traj.to(cuda), S, iters=20)
+    wo = pipe_menon(traj, S, iters=20)
+    assert rel(w, wo) < 1e-4

@@ -96,3 +96,30 @@ def test_ncg_oracle_reproduces_reference_history(run, direction, ls, iters):
     np.testing.assert_array_equal([h["step"] for h in o.hist], g[f"{run}_step"])
     np.testing.assert_allclose([h["xnorm"] for h in o.hist], g[f"{run}_xnorm"], rtol=1e-4)
     assert rel(o.x, torch.from_numpy(g[f"{run}_x"])) < 1e-4
+
+
+def test_pipe_menon_oracle_flattens_radial_density():
+    """Oracle of the density-compensation estimator: after the iterations the
+    spread of the weighted samples is flat (G G^H w = 1 at the samples) and the
+    weights of a radial trajectory grow with |k| (fewer samples per area
+    farther out)."""
+    import numpy as np
+    from oracle.dcf import pipe_menon
+    from oracle.kb import KBNufft
+    from mrirecon_b200 import phantoms
+    N = 32
+    traj = phantoms.golden_angle_radial(24, 2 * N).unsqueeze(0)
+    w = pipe_menon(traj, (N, N), iters=30)[0]
+    k = KBNufft(torch.ones((1, N, N), dtype=torch.complex128), traj, None, norm="none")
+    idx, wt = k.idx[0], k.w[0].to(torch.float64)
+    grid = torch.zeros(int(np.prod(k.G)), dtype=torch.float64)
+    grid.index_add_(0, idx.reshape(-1), (wt * w[:, None]).reshape(-1))
+    c = (grid[idx] * wt).sum(-1)
+    assert float((c - 1).abs().median()) < 0.05
+    # averaged over the spokes (golden-angle gaps vary), the weight is linear in |k|
+    spokes, nread = 48, 2 * N
+    traj = phantoms.golden_angle_radial(spokes, nread).unsqueeze(0)
+    prof = pipe_menon(traj, (N, N), iters=30)[0].reshape(spokes, nread).mean(0)
+    kr = torch.linalg.vector_norm(traj[0].to(torch.float64), dim=0).reshape(spokes, nread)[0]
+    mid = (kr > 0.3) & (kr < 2.5)
+    assert np.corrcoef(kr[mid].numpy(), prof[mid].numpy())[0, 1] > 0.99
