@@ -84,6 +84,7 @@ def parse():
     ap.add_argument("--no-3d", action="store_true", help="skip the 3D koosh-ball NUFFT throughput block")
     ap.add_argument("--no-batched", action="store_true", help="skip the 16-instance uneven batch block")
     ap.add_argument("--no-toeplitz", action="store_true", help="skip the Toeplitz-schedule solve block")
+    ap.add_argument("--no-jacobi", action="store_true", help="skip the Jacobi-preconditioned solve block")
     ap.add_argument("--nufft-only", action="store_true",
                     help="profiling case: prepare the workload's operator and run 3 forward/adjoint pairs")
     ap.add_argument("--koosh-only", type=int, default=0, metavar="N",
@@ -537,6 +538,39 @@ def toeplitz_solve(op, y, regm, x_ref, f_ref, steps=3):
             "objective_rel_diff_vs_gridded_plain": (f - f_ref) / abs(f_ref), "stop": s.stop_reason}
 
 
+def jacobi_solve(op, y, regm, x_ref, f_ref, steps=3):
+    """Plain NCG with the Jacobi diagonal (precond="jacobi": alpha sum|S|^2 plus the
+    regularisers' add_diag at the zero start) on the same problem and stop rule:
+    device seconds per solve including the diagonal set-up, iterations, image
+    error and objective against the unpreconditioned solve."""
+    from mrirecon_b200.solver import CGSolver
+    cfg = solver_cfg()
+    cfg.precond = "jacobi"
+    s = CGSolver(y, op, regm, cfg)
+    s.reset().run()
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    a, b = ev(), ev()
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(steps):
+        s.reset().run()
+    b.record()
+    torch.cuda.synchronize()
+    t = a.elapsed_time(b) / 1e3 / steps
+    xr = s.result()
+    err = float(torch.linalg.vector_norm(xr - x_ref) / torch.linalg.vector_norm(x_ref))
+    f = s.objective()
+    # the two solves stop at different objectives: also the first iteration at
+    # which the preconditioned solve reaches the plain solve's final objective
+    fa = [h["f_accepted"] for h in s.history()]
+    k_ref = next((k + 1 for k, v in enumerate(fa) if v <= f_ref), None)
+    ms_it = t * 1e3 / max(1, s.iter)
+    return {"s_to_tol": t, "iters_to_tol": s.iter, "ms_per_iter": ms_it,
+            "image_err_vs_plain": err, "objective": f, "objective_rel_diff_vs_plain": (f - f_ref) / abs(f_ref),
+            "iters_to_plain_objective": k_ref,
+            "s_to_plain_objective_est": None if k_ref is None else k_ref * ms_it / 1e3, "stop": s.stop_reason}
+
+
 def run_b200(args, w, ws, rank, local):
     from mrirecon_b200 import _lib, phantoms
     from mrirecon_b200.nufft import NUFFT, NUFFTConfig
@@ -620,6 +654,8 @@ def run_b200(args, w, ws, rank, local):
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "per_step": e2e_steps},
             "gpu_launches": launches, "clocks": clocks}
+    if not args.no_jacobi:
+        line["jacobi"] = jacobi_solve(op, y, regm, x_plain, f_plain)
     if not args.no_toeplitz:
         line["toeplitz"] = toeplitz_solve(op, y, regm, x_plain, f_plain)
     if not args.no_batched:

@@ -296,6 +296,25 @@ int mrb_ncg_err_step(double* slots, mrb_stream_t stream);
 int mrb_ncg_restart(int64_t n, void* d, const void* g, const float* diag, int64_t ndiag, double* slots,
                     mrb_stream_t stream);
 
+/* Jacobi diagonal of the preconditioner (float32, F*P entries, the layout of
+ * the image (F, 1, *S); P pixels per frame).
+ * mrb_precond_init: diag = base + alpha * sum_c |maps_c|^2 per pixel (maps
+ * (C, *S) complex64, or NULL for diag = base).  The reference initialises the
+ * diagonal to ones (graspcg/solvers/cg.py:95: base 1, maps NULL) and exposes
+ * alpha as TorchKbNUFFTAdapter.diag_AHA_scalar (graspcg/nufft/backends/torchkb.py:341-364).
+ * mrb_tv_add_diag: diag += the terms' diagonal at x, as
+ * RegManager.add_diag (graspcg/regularization/manager.py:145-218) adds it for
+ * identity regularisers: a term with the frame axis adds its frame profile
+ * 2 lambda w_0^2 deg(f) (TVND.majorizer_profile, tv_nd.py:187-214; deg 1 at
+ * the ends of each series of frame_period frames, 2 inside) when
+ * frame_profile != 0; any other term adds per axis
+ * lambda w^2 / sqrt(|D_a x|^2 + eps^2), once on the first and last slice and
+ * twice inside (TVND.add_diag, tv_nd.py:113-164). */
+int mrb_precond_init(int64_t P, int F, int C, const void* maps, float alpha, float base, float* diag,
+                     mrb_stream_t stream);
+int mrb_tv_add_diag(int nd, const int* S, int F, const mrb_tv_term* terms, int nterms, const void* x,
+                    int frame_profile, float* diag, mrb_stream_t stream);
+
 /* ------------------------------------------------------------------------
  * Learned warm start (no counterpart in the reference).  Activations are
  * channels-last BF16 volumes (Nb, D, H, W, channels) with a channel stride

@@ -87,6 +87,10 @@ _SIGS = {
     "mrb_ncg_err_step": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
     "mrb_ncg_restart": (ct.c_int, [ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_void_p,
                                    ct.c_void_p]),
+    "mrb_precond_init": (ct.c_int, [ct.c_int64, ct.c_int, ct.c_int, ct.c_void_p, ct.c_float, ct.c_float,
+                                    ct.c_void_p, ct.c_void_p]),
+    "mrb_tv_add_diag": (ct.c_int, [ct.c_int, c_int_p, ct.c_int, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int,
+                                   ct.c_void_p, ct.c_void_p]),
 }
 
 

@@ -1190,6 +1190,185 @@ extern "C" int mrb_ncg_set_steps(double* ts, int J, double beta, mrb_stream_t st
 }
 
 // ===========================================================================
+// Jacobi diagonal D of the NCG preconditioner (d = beta d - g/D).
+//
+// Data part: D = base + alpha * sum_c |S_c|^2 per pixel, alpha the calibrated
+// A^H A gain at the image centre (diag_AHA_scalar, torchkb.py:341-364).
+// Regulariser part, one term at a time as RegManager.add_diag adds them
+// (graspcg/regularization/manager.py:145-218):
+//  * a term whose axes include the frame axis adds its frame profile
+//    2 lambda w_0^2 deg(f), deg 1 at both ends of a series and 2 inside
+//    (TVND.majorizer_profile, tv_nd.py:187-214), and nothing else;
+//  * any other term adds per axis a the lagged diffusivity
+//    lambda w_a^2 / sqrt(|D_a x|^2 + eps^2) of the forward difference D_a x
+//    (zero on the last slice), once on the first and last slice along a and
+//    twice inside (TVND.add_diag, tv_nd.py:113-164).  With frame_profile = 0
+//    every term takes this form, the frame axis included (TVND.add_diag
+//    called on its own).  The difference is of x
+//    itself; the axis weight enters only squared, as in the reference.
+// One pass over x and D: elementwise, HBM bound, once per solve.
+// ===========================================================================
+namespace {
+
+constexpr int PD_MAX_TERMS = 8;
+
+struct PrecondTerms {
+  int nt;
+  int profile[PD_MAX_TERMS];       // 1: frame profile
+  float prof_scale[PD_MAX_TERMS];  // 2 lambda w_0^2 (profile terms)
+  float lam[PD_MAX_TERMS];
+  float eps2[PD_MAX_TERMS];
+  int naxes[PD_MAX_TERMS];
+  int axis[PD_MAX_TERMS][4];       // 0 (frames), 1 (size-1 axis) or 2.. (spatial)
+  float w2[PD_MAX_TERMS][4];
+};
+
+struct PrecondGeom {
+  int nd;
+  int S[3];
+  long long stride[3];  // element strides of the spatial axes
+  long long P;          // pixels per frame
+  int period;           // frames per series
+};
+
+__global__ void __launch_bounds__(256) precond_sense_kernel(long long n, long long P, int C,
+                                                             const float2* __restrict__ maps, float alpha,
+                                                             float base, float* __restrict__ D) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+    float s = 0.f;
+    if (maps) {
+      const long long p = v % P;
+      for (int c = 0; c < C; ++c) {
+        const float2 m = maps[(long long)c * P + p];
+        s = fmaf(m.x, m.x, fmaf(m.y, m.y, s));
+      }
+    }
+    D[v] = fmaf(alpha, s, base);
+  }
+}
+
+__global__ void __launch_bounds__(256) precond_tv_kernel(long long n, PrecondGeom g, PrecondTerms T,
+                                                          const float2* __restrict__ x, float* __restrict__ D) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += stride) {
+    const long long f = v / g.P;
+    long long p = v - f * g.P;
+    int c[3] = {0, 0, 0};
+    for (int k = g.nd - 1; k >= 0; --k) {
+      c[k] = (int)(p % g.S[k]);
+      p /= g.S[k];
+    }
+    const int fl = (int)(f % g.period);
+    const float2 xv = x[v];
+    float acc = D[v];
+    for (int t = 0; t < T.nt; ++t) {
+      if (T.profile[t]) {
+        const float deg = (g.period > 2 && fl > 0 && fl < g.period - 1) ? 2.f : 1.f;
+        acc += deg * T.prof_scale[t];
+        continue;
+      }
+      for (int q = 0; q < T.naxes[t]; ++q) {
+        const int a = T.axis[t][q];
+        int na = 1, ca = 0;
+        long long sa = 0;
+        if (a >= 2) {
+          na = g.S[a - 2];
+          ca = c[a - 2];
+          sa = g.stride[a - 2];
+        } else if (a == 0) {  // frames, within a series
+          na = g.period;
+          ca = fl;
+          sa = g.P;
+        }
+        float dx = 0.f, dy = 0.f;
+        if (ca < na - 1) {
+          const float2 xn = x[v + sa];
+          dx = xn.x - xv.x;
+          dy = xn.y - xv.y;
+        }
+        const float wi = rsqrtf(dx * dx + dy * dy + T.eps2[t]);
+        const float s = (T.lam[t] * T.w2[t][q]) * wi;
+        acc += (na >= 3 && ca > 0 && ca < na - 1) ? 2.f * s : s;
+      }
+    }
+    D[v] = acc;
+  }
+}
+
+int precond_blocks(long long n) {
+  long long nb = (n + 255) / 256;
+  return (int)(nb < 148LL * 16 ? (nb < 1 ? 1 : nb) : 148LL * 16);
+}
+
+}  // namespace
+
+extern "C" int mrb_precond_init(int64_t P, int F, int C, const void* maps, float alpha, float base, float* diag,
+                                mrb_stream_t stream) {
+  MRB_REQUIRE(diag != nullptr, "null diagonal");
+  MRB_REQUIRE(P >= 1 && F >= 1, "bad image size");
+  MRB_REQUIRE(maps == nullptr || C >= 1, "bad coil count %d", C);
+  const long long n = (long long)P * F;
+  precond_sense_kernel<<<precond_blocks(n), 256, 0, (cudaStream_t)stream>>>(n, P, C, (const float2*)maps, alpha,
+                                                                             base, diag);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_tv_add_diag(int nd, const int* S, int F, const mrb_tv_term* terms, int nterms, const void* x,
+                               int frame_profile, float* diag, mrb_stream_t stream) {
+  MRB_REQUIRE(nd >= 1 && nd <= 3 && S != nullptr && F >= 1, "bad image geometry");
+  MRB_REQUIRE(x != nullptr && diag != nullptr, "null pointer");
+  MRB_REQUIRE(nterms >= 0 && (nterms == 0 || terms != nullptr), "bad term list");
+  PrecondGeom g{};
+  g.nd = nd;
+  g.P = 1;
+  for (int k = nd - 1; k >= 0; --k) {
+    MRB_REQUIRE(S[k] >= 1, "bad image size");
+    g.S[k] = S[k];
+    g.stride[k] = g.P;
+    g.P *= S[k];
+  }
+  g.period = F;
+  PrecondTerms T{};
+  for (int i = 0; i < nterms; ++i) {
+    const mrb_tv_term& t = terms[i];
+    if (!t.enabled || t.weight == 0.f || t.naxes == 0) continue;
+    MRB_REQUIRE(t.naxes >= 1 && t.naxes <= 4, "at most 4 axes per TV term");
+    MRB_REQUIRE(T.nt < PD_MAX_TERMS, "at most %d TV terms", PD_MAX_TERMS);
+    if (t.frame_period > 0) {
+      MRB_REQUIRE(F % t.frame_period == 0, "frame period %d does not divide %d frames", t.frame_period, F);
+      MRB_REQUIRE(g.period == F || g.period == t.frame_period, "TV terms disagree on the frame period");
+      g.period = t.frame_period;
+    }
+    const int k = T.nt++;
+    int q0 = -1;
+    for (int q = 0; q < t.naxes; ++q) {
+      MRB_REQUIRE(t.axes[q] >= 0 && t.axes[q] < 2 + nd, "TV axis %d out of range", t.axes[q]);
+      if (t.axes[q] == 0) q0 = q;
+    }
+    if (q0 >= 0 && frame_profile) {
+      const double w0 = t.axis_weights[q0];
+      T.profile[k] = 1;
+      T.prof_scale[k] = (float)(2.0 * (double)t.weight * w0 * w0);
+      continue;
+    }
+    T.lam[k] = t.weight;
+    T.eps2[k] = t.eps * t.eps;
+    T.naxes[k] = t.naxes;
+    for (int q = 0; q < t.naxes; ++q) {
+      T.axis[k][q] = t.axes[q];
+      T.w2[k][q] = (float)((double)t.axis_weights[q] * (double)t.axis_weights[q]);
+    }
+  }
+  if (T.nt == 0) return 0;
+  const long long n = g.P * F;
+  precond_tv_kernel<<<precond_blocks(n), 256, 0, (cudaStream_t)stream>>>(n, g, T, (const float2*)x, diag);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+// ===========================================================================
 // Allocation-free variant of mrb_dots_f64.
 //
 // Some callers cannot allocate device memory at the point where they need a

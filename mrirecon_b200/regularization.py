@@ -128,6 +128,65 @@ class TVND:
         axes = roles.resolve_axes(self.params.axes)
         return {0: 1} if any(a == 0 for a in axes) else {}
 
+    # -- diagonal preconditioner (graspcg/regularization/tv_nd.py:113-214) ----
+    @torch.no_grad()
+    def add_diag(self, ctx: RegContext) -> bool:
+        """ctx.diag += lambda w_a^2 / sqrt(|D_a x|^2 + eps^2) per axis (once on the
+        first and last slice, twice inside), on every axis of the term, the frame
+        axis included (tv_nd.py:113-164); ``mrb_tv_add_diag`` with no frame profile."""
+        if ctx.diag is None or self.params.weight == 0.0:
+            return False
+        axes = self._resolve_axes(ctx)
+        if not axes:
+            return False
+        _add_diag_kernel(ctx.x, ctx.diag, ctx.roles_image, [tv_term_struct(self.params, axes)], frame_profile=0)
+        return True
+
+    def majorizer_diag(self, ctx: RegContext) -> torch.Tensor:
+        """0-D k = 2 lambda sum_a w_a^2 (tv_nd.py:166-185; zero when the axis
+        weights do not match the axes)."""
+        axes = self._resolve_axes(ctx)
+        k = 0.0
+        if axes and self.params.weight != 0.0:
+            aw = self.params.axis_weights
+            if aw is None:
+                k = 2.0 * self.params.weight * float(len(axes))
+            elif len(aw) == len(axes):
+                k = 2.0 * self.params.weight * sum(float(w) ** 2 for w in aw)
+        return torch.tensor(k, device=ctx.device, dtype=ctx.dtype_r)
+
+    def majorizer_profile(self, ctx: RegContext) -> Optional[List[Tuple[int, torch.Tensor]]]:
+        """[(0, v)] with v = 2 lambda w_0^2 (1, 2, ..., 2, 1) over the frames when the
+        term includes the frame axis, else None (tv_nd.py:187-214)."""
+        axes = self._resolve_axes(ctx)
+        if self.params.weight == 0.0 or 0 not in axes:
+            return None
+        w0 = 1.0
+        if self.params.axis_weights is not None:
+            if len(self.params.axis_weights) != len(axes):
+                return None
+            w0 = float(dict(zip(axes, self.params.axis_weights)).get(0, 1.0))
+        B = int(ctx.x.shape[0])
+        v = torch.ones(B, device=ctx.device, dtype=ctx.dtype_r)
+        if B > 2:
+            v[1:-1] = 2.0
+        return [(0, v * (2.0 * self.params.weight * w0 * w0))]
+
+
+def _add_diag_kernel(x: torch.Tensor, D: torch.Tensor, roles: Roles, terms: Sequence[_lib.TVTerm],
+                     frame_profile: int) -> None:
+    _lib.require_cuda(x, "x")
+    _lib.require_cuda(D, "diag")
+    if x.dtype != torch.complex64 or not x.is_contiguous():
+        raise ValueError("the diagonal pass needs a contiguous complex64 x")
+    if D.dtype != torch.float32 or not D.is_contiguous() or D.numel() != x.numel():
+        raise ValueError("diag must be a contiguous float32 tensor with one entry per voxel of x")
+    nd, S, F = image_geometry(x, roles)
+    Sarr = (ct.c_int * 3)(*(list(S) + [1] * (3 - nd)))
+    arr = (_lib.TVTerm * max(1, len(terms)))(*terms)
+    _lib.check(_lib.load().mrb_tv_add_diag(nd, Sarr, F, arr, len(terms), _lib.ptr(x), int(frame_profile),
+                                           _lib.ptr(D), _lib.stream_ptr(x.device)), "tv_add_diag")
+
 
 _WS = {}
 
@@ -167,6 +226,19 @@ class RegManager:
         if len(out) > 4:
             raise ValueError("at most 4 active TV terms")
         return out
+
+    @torch.no_grad()
+    def add_diag(self, ws, series_length: int = 0) -> None:
+        """ws "diag" += the regularisers' diagonal at ws "var" (manager.py:145-218,
+        one shard, identity regularisers): a term over the frame axis adds its frame
+        profile (preference (1) of the reference), any other term its lagged
+        diffusivity (preference (2)).  One ``mrb_tv_add_diag`` pass for all terms."""
+        if not ws.has("diag"):
+            return
+        roles = ws.plan.roles_image
+        terms = self.terms(roles, series_length)
+        if terms:
+            _add_diag_kernel(ws.get("var", 0), ws.get("diag", 0), roles, terms, frame_profile=1)
 
     @torch.no_grad()
     def energy_and_grad(self, ws) -> torch.Tensor:

@@ -87,6 +87,11 @@ class CGConfig:
     # > 0: the frame axis holds independent series of this many frames (a batch of
     # separate problems; temporal TV does not couple series)
     series_length: int = 0
+    # diagonal D of d = beta d - g/D: "none" keeps D = 1 as the reference solve does
+    # (graspcg/solvers/cg.py:95); "jacobi" sets D = alpha sum_c |S_c|^2 (alpha the
+    # operator's diag_AHA_scalar) plus RegManager.add_diag at the starting image,
+    # once per run.  The gradient-norm stop then reads sqrt(<g, g/D>).
+    precond: str = "none"
 
 
 class _Shard:
@@ -141,6 +146,8 @@ class CGSolver:
             raise ValueError("the fast schedules implement Armijo; use schedule='reference' for Wolfe")
         if c.schedule != "reference" and not (1 <= c.ls_max_iter <= 23):
             raise ValueError("the fast schedule evaluates at most 23 trial steps per pass")
+        if c.precond not in ("none", "jacobi"):
+            raise ValueError("precond must be 'none' or 'jacobi'")
         _lib.require_cuda(y, "y")
         self.lib = _lib.load()
         self.y = y.to(torch.complex64).contiguous()
@@ -169,6 +176,9 @@ class CGSolver:
         self.g_prev = z(ishape) if c.direction.lower() in ("prplus", "dy") else None
         self.r, self.Ad = torch.empty_like(self.y), torch.empty_like(self.y)
         self.n_img, self.n_k = self.x.numel(), self.y.numel()
+        self.D = torch.ones(ishape, dtype=torch.float32, device=dev) if c.precond == "jacobi" else None
+        self._ndiag = self.n_img if self.D is not None else 0
+        self.precond_alpha = None
         nslots, self.hist_cols = _lib.ncg_slot_count()
         self.s = torch.zeros(nslots, dtype=torch.float64, device=dev)
         self.hist = torch.zeros((max(1, c.max_iter), self.hist_cols), dtype=torch.float64, device=dev)
@@ -193,8 +203,11 @@ class CGSolver:
             self._dot_a = (ct.c_void_p * 2)(_lib.ptr(self.gr), _lib.ptr(self.gAd))
             self._dot_b = (ct.c_void_p * 2)(_lib.ptr(self.d), _lib.ptr(self.d))
             self._dot_w = (ct.c_void_p * 2)(None, None)
-        self.ws = SolverWorkspace({"var": self.x, "grad": self.g, "dir": self.d, "data": self.y,
-                                   "fwd_dir_sh": self.Ad, "resid_sh": self.r}, roles, dev)
+        bufs = {"var": self.x, "grad": self.g, "dir": self.d, "data": self.y, "fwd_dir_sh": self.Ad,
+                "resid_sh": self.r}
+        if self.D is not None:
+            bufs["diag"] = self.D
+        self.ws = SolverWorkspace(bufs, roles, dev)
         self.iter = 0
         self._graph = None
         self._host_hist: List[dict] = []
@@ -231,14 +244,38 @@ class CGSolver:
     def _tv_grad(self, d, t_dev, t_host, g_base, g_dir, g_out, out, skip=None, skip_if_zero=0):
         _lib.check(self.lib.mrb_tv_grad(self.nd, self._Sarr, self.F, self._terms_arr, self.nterms,
                                         _lib.ptr(self.x), _lib.ptr(d), t_dev, float(t_host), _lib.ptr(g_base),
-                                        _lib.ptr(g_dir), _lib.ptr(g_out), None, 0, _lib.ptr(self.g_prev), skip,
+                                        _lib.ptr(g_dir), _lib.ptr(g_out), _lib.ptr(self.D), self._ndiag,
+                                        _lib.ptr(self.g_prev), skip,
                                         skip_if_zero, out, _lib.ptr(self.ws_buf), self._st()), "tv_grad")
 
     def _slot(self, i):
         return self.s.data_ptr() + 8 * i
 
+    def _backend(self):
+        return getattr(self.op, "backend", self.op)
+
+    @torch.no_grad()
+    def build_preconditioner(self) -> Optional[torch.Tensor]:
+        """Fill D for precond="jacobi" at the current x (no-op for "none")."""
+        if self.D is None:
+            return None
+        backend = self._backend()
+        maps = getattr(backend, "_maps", None)
+        if self.precond_alpha is None:
+            if not hasattr(backend, "diag_AHA_scalar") or maps is None:
+                raise ValueError("precond='jacobi' needs an operator with diag_AHA_scalar and coil maps")
+            self.precond_alpha = float(backend.diag_AHA_scalar())
+        P = self.n_img // self.F
+        _lib.check(self.lib.mrb_precond_init(P, self.F, int(maps.shape[0]), _lib.ptr(maps),
+                                             float(self.precond_alpha), 0.0, _lib.ptr(self.D), self._st()),
+                   "precond_init")
+        if self.regm is not None:
+            self.regm.add_diag(self.ws, self.cfg.series_length)
+        return self.D
+
     # ------------------------------------------------------------- fast path
     def _prime_fast(self):
+        self.build_preconditioner()
         st = self._st()
         self._A(self.x, self.Ad)                               # Ax (into the Ad buffer)
         _lib.check(self.lib.mrb_kspace_pass(1, self.n_k, _lib.ptr(self.r), None, _lib.ptr(self.Ad),
@@ -253,7 +290,8 @@ class CGSolver:
             self._AH(self.r, self.gr)
         self._tv_grad(None, None, 0.0, self.gr, None, self.g, self._slot(S_RED))
         _lib.check(self.lib.mrb_ncg_steepest(self.n_img, _lib.ptr(self.d), _lib.ptr(self.g), _lib.ptr(self.g_prev),
-                                             None, 0, self._slot(S_G0D), _lib.ptr(self.ws_buf), st), "steepest")
+                                             _lib.ptr(self.D), self._ndiag, self._slot(S_G0D), _lib.ptr(self.ws_buf),
+                                             st), "steepest")
         J = self.cfg.ls_max_iter + 1
         _lib.check(self.lib.mrb_ncg_set_steps(_lib.ptr(self.ts), J, float(self.cfg.ls_beta), st), "set_steps")
         for i, v in ((S_DONE, 0.0), (S_REASON, 0.0), (S_ITER, float(self.iter)), (S_RHO_INIT, 0.0),
@@ -295,10 +333,12 @@ class CGSolver:
         _lib.check(lib.mrb_ncg_control(_lib.ptr(self.s), _lib.ptr(self.hist), _lib.ptr(self.cfg_dev),
                                        self.nterms, 1, st), "ncg_control")
         _lib.check(lib.mrb_ncg_update(self.n_img, _lib.ptr(self.x), _lib.ptr(self.d), _lib.ptr(self.g),
-                                      _lib.ptr(self.gr), _lib.ptr(self.gAd), _lib.ptr(self.g_prev), None, 0,
+                                      _lib.ptr(self.gr), _lib.ptr(self.gAd), _lib.ptr(self.g_prev),
+                                      _lib.ptr(self.D), self._ndiag,
                                       _lib.ptr(self.s), ws, st), "ncg_update")
         if self.cfg.restart:
-            _lib.check(lib.mrb_ncg_restart(self.n_img, _lib.ptr(self.d), _lib.ptr(self.g), None, 0,
+            _lib.check(lib.mrb_ncg_restart(self.n_img, _lib.ptr(self.d), _lib.ptr(self.g), _lib.ptr(self.D),
+                                           self._ndiag,
                                            _lib.ptr(self.s), st), "ncg_restart")
         if self._toep is not None:
             _lib.check(lib.mrb_ncg_err_step(_lib.ptr(self.s), st), "err_step")
@@ -448,12 +488,14 @@ class CGSolver:
         if self.Ax is None:
             self.Ax = torch.empty_like(self.y)
         out = torch.zeros(24, dtype=torch.float64, device=self.device)
+        self.build_preconditioner()
         # prime (cg.py:178-190): f_g(0) at x with d as it is, then d = -g/D
         self._A(self.x, self.Ax)
         self._A(self.d, self.Ad)
         self._fg(0.0, out)
         _lib.check(self.lib.mrb_ncg_steepest(self.n_img, _lib.ptr(self.d), _lib.ptr(self.g), _lib.ptr(self.g_prev),
-                                             None, 0, self._slot(S_G0D), _lib.ptr(self.ws_buf), st), "steepest")
+                                             _lib.ptr(self.D), self._ndiag, self._slot(S_G0D), _lib.ptr(self.ws_buf),
+                                             st), "steepest")
         rho_prev = None
         cum = {"x": 0.0, "g": 0.0, "s": 0.0}
         fa: List[float] = []
@@ -503,7 +545,8 @@ class CGSolver:
             self.s[S_DONE] = 1.0 if done else 0.0
             self.s[S_BETA] = beta
             _lib.check(self.lib.mrb_ncg_update(self.n_img, _lib.ptr(self.x), _lib.ptr(self.d), _lib.ptr(self.g),
-                                               None, None, _lib.ptr(self.g_prev), None, 0, _lib.ptr(self.s),
+                                               None, None, _lib.ptr(self.g_prev), _lib.ptr(self.D), self._ndiag,
+                                               _lib.ptr(self.s),
                                                _lib.ptr(self.ws_buf), st), "ncg_update")
             if done:
                 self.stop_reason = REASONS[reason]

@@ -1,6 +1,7 @@
 """Non-linear CG restatement, reference schedule (CPU; TEST INFRASTRUCTURE ONLY).
 
-One shard, diag preconditioner = ones (the reference never fills it), policy a
+One shard, diag preconditioner = ones (the reference never fills it) unless a
+diagonal D is given (then d = beta d - g/D and every rho is <g, g/D>), policy a
 no-op.  Follows:
 
 * CGSolver.run                 graspcg/solvers/cg.py:162-246
@@ -62,14 +63,15 @@ class NCGOracle:
     """x, y are CPU tensors; A/AH map between them; regs are TVSpec."""
 
     def __init__(self, A: Callable, AH: Callable, y: torch.Tensor, x0: torch.Tensor,
-                 regs: Sequence[TVSpec], cfg: Optional[NCGConfig] = None):
+                 regs: Sequence[TVSpec], cfg: Optional[NCGConfig] = None, D: Optional[torch.Tensor] = None):
         self.Aop, self.AHop = A, AH
         self.cfg = cfg or NCGConfig()
         self.y = y
         self.x = x0.clone()
         self.d = torch.zeros_like(x0)
         self.g = torch.zeros_like(x0)
-        self.D = torch.ones(x0.shape, dtype=x0.real.dtype)
+        # preconditioner diagonal: ones as in the reference solve, or a given D
+        self.D = torch.ones(x0.shape, dtype=x0.real.dtype) if D is None else D.to(x0.real.dtype).reshape(x0.shape)
         self.regs = list(regs)
         self.Ax = None
         self.Ad = None

@@ -123,3 +123,77 @@ def test_pipe_menon_oracle_flattens_radial_density():
     kr = torch.linalg.vector_norm(traj[0].to(torch.float64), dim=0).reshape(spokes, nread)[0]
     mid = (kr > 0.3) & (kr < 2.5)
     assert np.corrcoef(kr[mid].numpy(), prof[mid].numpy())[0, 1] > 0.99
+
+
+# --- Jacobi diagonal (RegManager.add_diag, manager.py:145-218) ------------------
+def _diag_loops(x, axes, lam, eps, aw, frame_profile, period=0):
+    """Per-voxel loops over the formula of tv_nd.py:113-164 / :187-214."""
+    F, _, H, W = x.shape
+    P = period or F
+    out = np.zeros((F, 1, H, W))
+    xs = x.numpy().astype(np.complex128)
+    size = {0: P, 1: 1, 2: H, 3: W}
+    for f in range(F):
+        for i in range(H):
+            for j in range(W):
+                acc = 0.0
+                if frame_profile and 0 in axes:
+                    w0 = aw[list(axes).index(0)]
+                    fl = f % P
+                    acc += 2 * lam * w0 * w0 * (2.0 if (P > 2 and 0 < fl < P - 1) else 1.0)
+                else:
+                    for a, w in zip(axes, aw):
+                        c = {0: f % P, 1: 0, 2: i, 3: j}[a]
+                        n = size[a]
+                        nb = {0: (f + 1, 0, i, j), 2: (f, 0, i + 1, j), 3: (f, 0, i, j + 1)}.get(a)
+                        dv = xs[nb] - xs[f, 0, i, j] if c < n - 1 else 0.0
+                        s = lam * w * w / math.sqrt(abs(dv) ** 2 + eps * eps)
+                        acc += 2 * s if (n >= 3 and 0 < c < n - 1) else s
+                out[f, 0, i, j] = acc
+    return out
+
+
+@pytest.mark.parametrize("axes,aw,profile,period", [((2, 3), (1.0, 1.0), True, 0), ((2, 3), (2.0, 0.5), True, 0),
+                                                    ((0,), (1.0,), True, 0), ((0,), (1.5,), False, 0),
+                                                    ((0,), (1.0,), False, 3), ((0, 2, 3), (1.0, 1.0, 1.0), True, 3)])
+def test_diag_oracle_matches_loops(axes, aw, profile, period):
+    from oracle.tv import tv_add_diag
+    g = torch.Generator().manual_seed(3)
+    x = torch.complex(torch.randn(6, 1, 4, 5, generator=g), torch.randn(6, 1, 4, 5, generator=g)) * 0.01
+    D = torch.zeros(6, 1, 4, 5, dtype=torch.float64)
+    tv_add_diag(D, x, axes, 2e-3, 1e-3, aw, frame_profile=profile, frame_period=period)
+    np.testing.assert_allclose(D.numpy(), _diag_loops(x, axes, 2e-3, 1e-3, aw, profile, period), rtol=1e-12)
+
+
+def test_diag_oracle_reference_expectations():
+    """The reference's own add_diag expectations: the temporal profile of
+    test_reg_diag_mapped.py:122-134 (frames 5: (1,2,2,2,1) * 2 lambda) and the
+    identity case of test_regularization_ns.py:168-178 (the diagonal grows)."""
+    from oracle.tv import tv_add_diag
+    D = torch.zeros(5, 1, 2, 2, dtype=torch.float64)
+    tv_add_diag(D, torch.zeros(5, 1, 2, 2, dtype=torch.complex64), (0,), 1e-3, 1e-3)
+    np.testing.assert_allclose(D.mean(dim=(1, 2, 3)).numpy(), np.array([1, 2, 2, 2, 1]) * 2e-3, atol=1e-12)
+    x = torch.randn(4, 1, 8, 8, dtype=torch.complex64, generator=torch.Generator().manual_seed(0)) * 0.01
+    D = torch.zeros(4, 1, 8, 8, dtype=torch.float64)
+    before = D.clone()
+    tv_add_diag(D, x, (2, 3), 1.0, 1e-3)
+    assert torch.all(D > before)
+
+
+def test_majorizer_host_logic():
+    """TVND.majorizer_diag / majorizer_profile (tv_nd.py:166-214): host arithmetic."""
+    from mrirecon_b200.regularization import RegContext, TVND, TVParams
+    from mrirecon_b200.roles import Roles
+    roles = Roles(1, 1, 2)
+    x = torch.zeros(5, 1, 2, 2, dtype=torch.complex64)
+    ctx = RegContext(x=x, g=x, diag=None, roles_image=roles, device=x.device, dtype_c=x.dtype,
+                     dtype_r=torch.float32)
+    sp = TVND("s", TVParams(weight=1e-3, eps=1e-3, axes="spatial"))
+    assert abs(float(sp.majorizer_diag(ctx)) - 2 * 1e-3 * 2) < 1e-9
+    assert sp.majorizer_profile(ctx) is None
+    aw = TVND("s", TVParams(weight=1e-3, eps=1e-3, axes="spatial", axis_weights=(2.0, 0.5)))
+    assert abs(float(aw.majorizer_diag(ctx)) - 2 * 1e-3 * 4.25) < 1e-9
+    tm = TVND("t", TVParams(weight=1e-3, eps=1e-3, axes="temporal"))
+    (ax, v), = tm.majorizer_profile(ctx)
+    assert ax == 0
+    np.testing.assert_allclose(v.numpy(), np.array([1, 2, 2, 2, 1]) * 2e-3, rtol=1e-6)
