@@ -314,6 +314,46 @@ int mrb_precond_init(int64_t P, int F, int C, const void* maps, float alpha, flo
                      mrb_stream_t stream);
 int mrb_tv_add_diag(int nd, const int* S, int F, const mrb_tv_term* terms, int nterms, const void* x,
                     int frame_profile, float* diag, mrb_stream_t stream);
+/* diag[f*P + p] += v[f] (dev v, F values): a per-frame diagonal profile, e.g.
+ * GraphLaplacian.add_diag's lambda*deg (graspcg/regularization/graph_laplacian.py:236-275). */
+int mrb_diag_add_frames(int64_t P, int F, const float* v, float* diag, mrb_stream_t stream);
+
+/* Graph Laplacian regulariser over the frame axis of an image (B, N) complex64
+ * (B frames of N voxels), L (dev, B x B float32, row-major) the weighted
+ * Laplacian sum_i lambda_i L_i (B <= 128):
+ *   mode 0: z = x + t*d (d may be NULL), acc += L z (acc may be NULL),
+ *           out[0] = 1/2 Re<z, L z>  (the energy)
+ *   mode 1: acc += L d, out[0] = Re<x, L d>, out[1] = Re<d, L d>
+ *   mode 2: as mode 1 for a non-symmetric L ("rw"): out[0] = Re<x, (L + L^T)/2 d>,
+ *           the slope of the energy along d (acc still gets L d)
+ * (t from t_dev if non-NULL, else t_host; skipped when skip != NULL and
+ * *skip != 0; FP64 reductions).
+ * Replaces: GraphLaplacian.energy_grad  graspcg/regularization/graph_laplacian.py:171-234
+ *           (_apply_L :135-168, normalisations none / rw / sym folded into L) */
+int mrb_graph_pass(int mode, int B, int64_t N, const float* L, const void* x, const void* d,
+                   const double* t_dev, double t_host, void* acc, const double* skip, double* out, void* ws,
+                   mrb_stream_t stream);
+/* Quadratic-term bookkeeping of the fast NCG schedule (slots 21..23 hold the
+ * graph energy q0 and, per iteration, q1 = Re<x, L d>, q2 = Re<d, L d>):
+ * phase 0 err += 2 q0; phase 1 (unless done) err += 2 q0, erd += q1,
+ * edd += q2; phase 2 (accepted step) q0 += t q1 + t^2 q2 / 2.
+ * No reference counterpart (the reference re-evaluates every regulariser at
+ * each trial step, graspcg/ops/objective.py:255-262). */
+int mrb_ncg_quad_fold(double* slots, int phase, mrb_stream_t stream);
+
+/* Frame mixing over the leading (frame) axis: out (rows_out, N) (+)= M in,
+ * in (rows_in, N); rows <= 128; in and out must not alias.
+ * mrb_frame_mix: complex64 data, M complex64 row-major (rows_out x rows_in),
+ * or, with conj_transpose, M given as (rows_in x rows_out) and applied as M^H.
+ * mrb_frame_mix_real: float32 data and M (transpose: M given as
+ * rows_in x rows_out, applied as M^T).
+ * Replaces: TemporalBasisOp.forward_apply / adjoint_apply / diag_push
+ *           graspcg/regularization/mapping.py:112-236 (u = U V, g_V += U^H g_u,
+ *           diag_V += |U|^T k_u) and the per-frame factors of ScaleOp :44-110. */
+int mrb_frame_mix(int rows_out, int rows_in, int64_t N, const void* M, int conj_transpose, const void* in,
+                  void* out, int accumulate, mrb_stream_t stream);
+int mrb_frame_mix_real(int rows_out, int rows_in, int64_t N, const float* M, int transpose, const float* in,
+                       float* out, int accumulate, mrb_stream_t stream);
 
 /* ------------------------------------------------------------------------
  * Learned warm start (no counterpart in the reference).  Activations are

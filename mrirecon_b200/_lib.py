@@ -91,6 +91,15 @@ _SIGS = {
                                     ct.c_void_p, ct.c_void_p]),
     "mrb_tv_add_diag": (ct.c_int, [ct.c_int, c_int_p, ct.c_int, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int,
                                    ct.c_void_p, ct.c_void_p]),
+    "mrb_diag_add_frames": (ct.c_int, [ct.c_int64, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "mrb_graph_pass": (ct.c_int, [ct.c_int, ct.c_int, ct.c_int64, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                  ct.c_void_p, ct.c_double, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                  ct.c_void_p]),
+    "mrb_ncg_quad_fold": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p]),
+    "mrb_frame_mix": (ct.c_int, [ct.c_int, ct.c_int, ct.c_int64, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p,
+                                 ct.c_int, ct.c_void_p]),
+    "mrb_frame_mix_real": (ct.c_int, [ct.c_int, ct.c_int, ct.c_int64, ct.c_void_p, ct.c_int, ct.c_void_p,
+                                      ct.c_void_p, ct.c_int, ct.c_void_p]),
 }
 
 

@@ -524,6 +524,7 @@ enum Slot {
   S_T = 0, S_LS_OK, S_DONE, S_REASON, S_ITER, S_F0, S_G0D, S_FT, S_GDT,
   S_ERR, S_ERD, S_EDD, S_RHO_PREV, S_RHO_INIT, S_BETA,
   S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL, S_NRESTART, S_NOMORE,
+  S_GQ0, S_GQ1, S_GQ2,   // quadratic (graph Laplacian) energy and its slope / curvature along d
   S_RED = 24,            // reduction outputs of the gradient pass (GP_NV values)
   S_EJ = 48,             // multi-t energies (MT_MAX_J values)
   S_G0D_NEXT = 80,
@@ -1364,6 +1365,298 @@ extern "C" int mrb_tv_add_diag(int nd, const int* S, int F, const mrb_tv_term* t
   if (T.nt == 0) return 0;
   const long long n = g.P * F;
   precond_tv_kernel<<<precond_blocks(n), 256, 0, (cudaStream_t)stream>>>(n, g, T, (const float2*)x, diag);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+// ===========================================================================
+// Graph Laplacian over the frame axis (GraphLaplacian,
+// graspcg/regularization/graph_laplacian.py:22-321).
+//
+// E(z) = 1/2 sum_p <z[:, p], L z[:, p]>, gradient L z, with L the B x B real
+// matrix that already carries the weights (sum_i lambda_i L_i, L_i = D - W,
+// I - D^-1 W or I - D^-1/2 W D^-1/2).  A block stages a tile of 32 pixel
+// columns of all B frames in shared memory and every warp forms whole rows
+// of L z for them: x (and d) are read once, the accumulator read and written
+// once; B^2 FMAs per column stay below the CUDA-core rate up to B = 128.
+// ===========================================================================
+namespace {
+
+constexpr int GRAPH_MAX_FRAMES = 128;
+constexpr int GRAPH_TILE = 32;
+
+// mode 0: z = x + t d (d may be null), y = L z, acc += y, out[0] = 1/2 Re<z, y>
+// mode 1: y = L d, acc += y, out[0] = Re<x, y>, out[1] = Re<d, y>
+// mode 2: mode 1 for a non-symmetric L: out[0] = Re<x, (L + L^T)/2 d> (the slope
+//         of the energy along d; the accumulated L d stays the reference's gradient)
+__global__ void __launch_bounds__(RED_THREADS) graph_kernel(int mode, int B, long long N, const float* __restrict__ L,
+                                                            const float2* __restrict__ x,
+                                                            const float2* __restrict__ d, const double* t_dev,
+                                                            double t_host, float2* __restrict__ acc,
+                                                            const double* skip, double* __restrict__ partials,
+                                                            RedOut ro) {
+  if (skipped(skip) != 0.0) return;   // uniform over the grid: no partials, no counter
+  extern __shared__ __align__(16) unsigned char graph_smem[];
+  float2* Z = reinterpret_cast<float2*>(graph_smem);         // B x GRAPH_TILE
+  float* Ls = reinterpret_cast<float*>(Z + B * GRAPH_TILE);  // B x B
+  for (int i = threadIdx.x; i < B * B; i += blockDim.x) Ls[i] = L[i];
+  const float t = (float)(t_dev ? *t_dev : t_host);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double r0 = 0.0, r1 = 0.0;
+  const long long ntiles = (N + GRAPH_TILE - 1) / GRAPH_TILE;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long p = tile * GRAPH_TILE + lane;
+    const bool in = p < N;
+    __syncthreads();   // L staged; the previous tile's columns consumed
+    for (int f = warp; f < B; f += nw) {
+      float2 v = make_float2(0.f, 0.f);
+      if (in) {
+        const long long i = (long long)f * N + p;
+        if (mode == 0) {
+          v = x[i];
+          if (d) {
+            const float2 dv = d[i];
+            v.x = __fadd_rn(v.x, __fmul_rn(dv.x, t));
+            v.y = __fadd_rn(v.y, __fmul_rn(dv.y, t));
+          }
+        } else {
+          v = d[i];
+        }
+      }
+      Z[f * GRAPH_TILE + lane] = v;
+    }
+    __syncthreads();
+    for (int f = warp; f < B; f += nw) {
+      const float* Lr = Ls + f * B;
+      float yx = 0.f, yy = 0.f, tx = 0.f, ty = 0.f;
+      for (int s2 = 0; s2 < B; ++s2) {
+        const float l = Lr[s2];
+        const float2 z = Z[s2 * GRAPH_TILE + lane];
+        yx = fmaf(l, z.x, yx);
+        yy = fmaf(l, z.y, yy);
+        if (mode == 2) {
+          const float lt = Ls[s2 * B + f];
+          tx = fmaf(lt, z.x, tx);
+          ty = fmaf(lt, z.y, ty);
+        }
+      }
+      if (in) {
+        const long long i = (long long)f * N + p;
+        const float2 zf = Z[f * GRAPH_TILE + lane];
+        if (acc) {
+          float2 a = acc[i];
+          a.x += yx;
+          a.y += yy;
+          acc[i] = a;
+        }
+        if (mode == 0) {
+          r0 += (double)(zf.x * yx + zf.y * yy);
+        } else {
+          const float2 xv = x[i];
+          if (mode == 1)
+            r0 += (double)(xv.x * yx + xv.y * yy);
+          else
+            r0 += 0.5 * (double)(xv.x * (yx + tx) + xv.y * (yy + ty));
+          r1 += (double)(zf.x * yx + zf.y * yy);
+        }
+      }
+    }
+  }
+  double v[2] = {mode == 0 ? 0.5 * r0 : r0, r1};
+  block_reduce_finish<2>(v, partials, ro);
+}
+
+// The graph term is quadratic, so the fast schedule carries it beside the
+// data term (0.5 (err + 2 t erd + t^2 edd)):
+// phase 0 (prime):     err += 2 q0
+// phase 1 (iteration): err += 2 q0, erd += q1, edd += q2 (after the k-space scalars)
+// phase 2 (update):    q0 += t q1 + t^2 q2 / 2 at the accepted step
+__global__ void quad_fold_kernel(double* s, int phase) {
+  if (threadIdx.x != 0) return;
+  if (phase == 0) {
+    s[S_ERR] += 2.0 * s[S_GQ0];
+  } else if (phase == 1) {
+    if (s[S_DONE] != 0.0) return;
+    s[S_ERR] += 2.0 * s[S_GQ0];
+    s[S_ERD] += s[S_GQ1];
+    s[S_EDD] += s[S_GQ2];
+  } else {
+    if (s[S_LS_OK] == 0.0) return;
+    const double t = s[S_T];
+    s[S_GQ0] += t * s[S_GQ1] + 0.5 * t * t * s[S_GQ2];
+  }
+}
+
+__global__ void __launch_bounds__(256) diag_frames_kernel(long long n, long long P, const float* __restrict__ v,
+                                                           float* __restrict__ D) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) D[i] += v[i / P];
+}
+
+}  // namespace
+
+extern "C" int mrb_graph_pass(int mode, int B, int64_t N, const float* L, const void* x, const void* d,
+                              const double* t_dev, double t_host, void* acc, const double* skip, double* out,
+                              void* ws, mrb_stream_t stream) {
+  MRB_REQUIRE(mode >= 0 && mode <= 2, "mode must be 0, 1 or 2");
+  MRB_REQUIRE(B >= 1 && B <= GRAPH_MAX_FRAMES, "graph over %d frames (1..%d supported)", B, GRAPH_MAX_FRAMES);
+  MRB_REQUIRE(N >= 1, "bad pixel count");
+  MRB_REQUIRE(L && x && out && ws, "null pointer");
+  MRB_REQUIRE(mode == 0 || d, "modes 1 and 2 need d");
+  const size_t smem = (size_t)B * GRAPH_TILE * sizeof(float2) + (size_t)B * B * sizeof(float);
+  static bool attr_set[64] = {};
+  int dev = 0;
+  MRB_CUDA_TRY(cudaGetDevice(&dev));
+  if (smem > 48 * 1024 && dev < 64 && !attr_set[dev]) {
+    MRB_CUDA_TRY(cudaFuncSetAttribute(graph_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)((size_t)GRAPH_MAX_FRAMES * GRAPH_TILE * sizeof(float2) +
+                                            (size_t)GRAPH_MAX_FRAMES * GRAPH_MAX_FRAMES * sizeof(float))));
+    attr_set[dev] = true;
+  }
+  const long long ntiles = (N + GRAPH_TILE - 1) / GRAPH_TILE;
+  const int nb = (int)std::min<long long>(ntiles, 148LL * 6);
+  double* part = (double*)ws;
+  graph_kernel<<<nb, RED_THREADS, smem, (cudaStream_t)stream>>>(
+      mode, B, (long long)N, L, (const float2*)x, (const float2*)d, t_dev, t_host, (float2*)acc, skip, part,
+      red_out(ws, out, mode == 0 ? 1 : 2, 0, skip));
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_ncg_quad_fold(double* slots, int phase, mrb_stream_t stream) {
+  MRB_REQUIRE(slots != nullptr, "null pointer");
+  MRB_REQUIRE(phase >= 0 && phase <= 2, "phase must be 0, 1 or 2");
+  quad_fold_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slots, phase);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+// ===========================================================================
+// Frame mixing out[r, p] (+)= sum_k M[r, k] in[k, p] over the frame axis
+// (TemporalBasisOp u = U V and its adjoint g_V += U^H g_u, mapping.py:112-236;
+// per-frame scalings of ScaleOp :44-110 as diagonal M).  Same tiling as the
+// graph pass: 32 pixel columns of all input rows staged in shared memory.
+// ===========================================================================
+namespace {
+
+constexpr int MIX_MAX_ROWS = 128;
+
+// complex data, complex M (row-major rows_out x rows_in, or rows_in x rows_out
+// conjugated when conj_t)
+__global__ void __launch_bounds__(256) mix_complex_kernel(int Ro, int Ri, long long N, const float2* __restrict__ M,
+                                                          int conj_t, const float2* __restrict__ in,
+                                                          float2* __restrict__ out, int accumulate) {
+  extern __shared__ __align__(16) unsigned char mix_smem[];
+  float2* Z = reinterpret_cast<float2*>(mix_smem);          // Ri x 32
+  float2* Ms = Z + Ri * GRAPH_TILE;                          // Ro x Ri
+  for (int i = threadIdx.x; i < Ro * Ri; i += blockDim.x) {
+    const int r = i / Ri, k = i - r * Ri;
+    float2 m = conj_t ? M[k * Ro + r] : M[i];
+    if (conj_t) m.y = -m.y;
+    Ms[i] = m;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long long ntiles = (N + GRAPH_TILE - 1) / GRAPH_TILE;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long p = tile * GRAPH_TILE + lane;
+    const bool ok = p < N;
+    __syncthreads();
+    for (int k = warp; k < Ri; k += nw) Z[k * GRAPH_TILE + lane] = ok ? in[(long long)k * N + p] : make_float2(0.f, 0.f);
+    __syncthreads();
+    if (!ok) continue;
+    for (int r = warp; r < Ro; r += nw) {
+      const float2* Mr = Ms + r * Ri;
+      float ax = 0.f, ay = 0.f;
+      for (int k = 0; k < Ri; ++k) {
+        const float2 m = Mr[k], z = Z[k * GRAPH_TILE + lane];
+        ax = fmaf(m.x, z.x, ax);
+        ax = fmaf(-m.y, z.y, ax);
+        ay = fmaf(m.x, z.y, ay);
+        ay = fmaf(m.y, z.x, ay);
+      }
+      const long long i = (long long)r * N + p;
+      if (accumulate) {
+        const float2 o = out[i];
+        ax += o.x;
+        ay += o.y;
+      }
+      out[i] = make_float2(ax, ay);
+    }
+  }
+}
+
+// real data, real M (row-major rows_out x rows_in, or transposed when trans)
+__global__ void __launch_bounds__(256) mix_real_kernel(int Ro, int Ri, long long N, const float* __restrict__ M,
+                                                       int trans, const float* __restrict__ in,
+                                                       float* __restrict__ out, int accumulate) {
+  extern __shared__ __align__(16) unsigned char mix_smem_r[];
+  float* Z = reinterpret_cast<float*>(mix_smem_r);  // Ri x 32
+  float* Ms = Z + Ri * GRAPH_TILE;                   // Ro x Ri
+  for (int i = threadIdx.x; i < Ro * Ri; i += blockDim.x) {
+    const int r = i / Ri, k = i - r * Ri;
+    Ms[i] = trans ? M[k * Ro + r] : M[i];
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long long ntiles = (N + GRAPH_TILE - 1) / GRAPH_TILE;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long p = tile * GRAPH_TILE + lane;
+    const bool ok = p < N;
+    __syncthreads();
+    for (int k = warp; k < Ri; k += nw) Z[k * GRAPH_TILE + lane] = ok ? in[(long long)k * N + p] : 0.f;
+    __syncthreads();
+    if (!ok) continue;
+    for (int r = warp; r < Ro; r += nw) {
+      const float* Mr = Ms + r * Ri;
+      float a = 0.f;
+      for (int k = 0; k < Ri; ++k) a = fmaf(Mr[k], Z[k * GRAPH_TILE + lane], a);
+      const long long i = (long long)r * N + p;
+      out[i] = accumulate ? out[i] + a : a;
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int mrb_frame_mix(int rows_out, int rows_in, int64_t N, const void* M, int conj_transpose, const void* in,
+                             void* out, int accumulate, mrb_stream_t stream) {
+  MRB_REQUIRE(rows_out >= 1 && rows_out <= MIX_MAX_ROWS && rows_in >= 1 && rows_in <= MIX_MAX_ROWS,
+              "frame mix of %d x %d rows (1..%d supported)", rows_out, rows_in, MIX_MAX_ROWS);
+  MRB_REQUIRE(N >= 1 && M && in && out, "bad arguments");
+  MRB_REQUIRE(in != out, "in and out must not alias");
+  const size_t smem = ((size_t)rows_in * GRAPH_TILE + (size_t)rows_out * rows_in) * sizeof(float2);
+  if (smem > 48 * 1024)
+    MRB_CUDA_TRY(cudaFuncSetAttribute(mix_complex_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long ntiles = (N + GRAPH_TILE - 1) / GRAPH_TILE;
+  const int nb = (int)std::min<long long>(ntiles, 148LL * 6);
+  mix_complex_kernel<<<nb, 256, smem, (cudaStream_t)stream>>>(rows_out, rows_in, (long long)N, (const float2*)M,
+                                                                conj_transpose, (const float2*)in, (float2*)out,
+                                                                accumulate);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_frame_mix_real(int rows_out, int rows_in, int64_t N, const float* M, int transpose,
+                                  const float* in, float* out, int accumulate, mrb_stream_t stream) {
+  MRB_REQUIRE(rows_out >= 1 && rows_out <= MIX_MAX_ROWS && rows_in >= 1 && rows_in <= MIX_MAX_ROWS,
+              "frame mix of %d x %d rows (1..%d supported)", rows_out, rows_in, MIX_MAX_ROWS);
+  MRB_REQUIRE(N >= 1 && M && in && out, "bad arguments");
+  MRB_REQUIRE(in != out, "in and out must not alias");
+  const size_t smem = ((size_t)rows_in * GRAPH_TILE + (size_t)rows_out * rows_in) * sizeof(float);
+  if (smem > 48 * 1024)
+    MRB_CUDA_TRY(cudaFuncSetAttribute(mix_real_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long ntiles = (N + GRAPH_TILE - 1) / GRAPH_TILE;
+  const int nb = (int)std::min<long long>(ntiles, 148LL * 6);
+  mix_real_kernel<<<nb, 256, smem, (cudaStream_t)stream>>>(rows_out, rows_in, (long long)N, M, transpose, in, out,
+                                                             accumulate);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int mrb_diag_add_frames(int64_t P, int F, const float* v, float* diag, mrb_stream_t stream) {
+  MRB_REQUIRE(v && diag, "null pointer");
+  MRB_REQUIRE(P >= 1 && F >= 1, "bad image size");
+  const long long n = (long long)P * F;
+  diag_frames_kernel<<<precond_blocks(n), 256, 0, (cudaStream_t)stream>>>(n, P, v, diag);
   MRB_LAUNCH_CHECK();
   return 0;
 }

@@ -5,6 +5,8 @@ Mirrors the reference's regulariser plug-in surface:
 * ``RegContext`` / ``RegParams`` graspcg/regularization/base.py:12-84
 * ``RegManager.energy_and_grad`` graspcg/regularization/manager.py:38-142
   (one shard: the temporal halo of manager.py:268-301 is the identity)
+* ``RegManager.add_diag`` / ``TVND.add_diag`` manager.py:145-218, tv_nd.py:113-214
+* ``GraphLapParams`` / ``GraphLaplacian`` graspcg/regularization/graph_laplacian.py:11-321
 
 ``TVND.energy_grad_fixed_axes(ctx, axes)`` adds its gradient into ``ctx.g``
 in place and returns the energy as a 0-D FP64 device tensor, computed by
@@ -173,6 +175,14 @@ class TVND:
         return [(0, v * (2.0 * self.params.weight * w0 * w0))]
 
 
+def _frame_profile(D: torch.Tensor, v: torch.Tensor) -> None:
+    """D[f, ...] += v[f] (mrb_diag_add_frames)."""
+    F = int(D.shape[0])
+    vv = v.detach().to(device=D.device, dtype=torch.float32).contiguous()
+    _lib.check(_lib.load().mrb_diag_add_frames(D.numel() // F, F, _lib.ptr(vv), _lib.ptr(D),
+                                               _lib.stream_ptr(D.device)), "diag_add_frames")
+
+
 def _add_diag_kernel(x: torch.Tensor, D: torch.Tensor, roles: Roles, terms: Sequence[_lib.TVTerm],
                      frame_profile: int) -> None:
     _lib.require_cuda(x, "x")
@@ -186,6 +196,123 @@ def _add_diag_kernel(x: torch.Tensor, D: torch.Tensor, roles: Roles, terms: Sequ
     arr = (_lib.TVTerm * max(1, len(terms)))(*terms)
     _lib.check(_lib.load().mrb_tv_add_diag(nd, Sarr, F, arr, len(terms), _lib.ptr(x), int(frame_profile),
                                            _lib.ptr(D), _lib.stream_ptr(x.device)), "tv_add_diag")
+
+
+@dataclass(frozen=True)
+class GraphLapParams(RegParams):   # graph_laplacian.py:11-20
+    weight: float = 0.0
+    normalize: str = "none"        # "none": L = D - W; "rw": I - D^-1 W; "sym": I - D^-1/2 W D^-1/2
+    mm_chunk_cols: int = 65536     # accepted for interface parity; the kernel tiles 32 columns at a time
+
+
+class GraphLaplacian:
+    """Graph Laplacian over the frame axis (graspcg/regularization/graph_laplacian.py:22-321):
+    E(x) = lambda/2 sum_p <x[:, p], L x[:, p]>, gradient lambda L x.
+
+    W (B x B, dense or sparse COO) is symmetrised as (W + W^T)/2 with a zero
+    diagonal and its degrees taken on the host (:45-80); the weighted Laplacian
+    lambda L is built once per device as a dense B x B float32 matrix, and
+    ``mrb_graph_pass`` applies it to all pixel columns in one pass.  The
+    reference's "row" spelling fails there (its code tests "rw"); here it is an
+    error at construction."""
+
+    Params = GraphLapParams
+
+    def __init__(self, name: str, W: torch.Tensor, params: GraphLapParams):
+        self.name = name
+        self.params = params
+        norm = (params.normalize or "none").lower()
+        if norm not in ("none", "rw", "sym"):
+            raise ValueError("normalize must be 'none', 'rw' or 'sym'")
+        Wc = W.detach().to("cpu")
+        Wd = Wc.to_dense() if Wc.is_sparse else Wc
+        Wd = (0.5 * (Wd + Wd.transpose(0, 1))).to(torch.float32).clone()
+        Wd.fill_diagonal_(0.0)
+        self._W_cpu = Wd
+        self._deg_cpu = Wd.sum(dim=1).clamp_min(0.0)
+        self._cache = {}
+
+    @property
+    def frames(self) -> int:
+        return int(self._W_cpu.shape[0])
+
+    def laplacian(self) -> torch.Tensor:
+        """lambda L as a dense FP64 CPU matrix."""
+        W = self._W_cpu.to(torch.float64)
+        deg = self._deg_cpu.to(torch.float64)
+        norm = (self.params.normalize or "none").lower()
+        eye = torch.eye(W.shape[0], dtype=torch.float64)
+        if norm == "none":
+            L = torch.diag(deg) - W
+        elif norm == "rw":
+            L = eye - W / deg.clamp_min(1e-20).view(-1, 1)
+        else:
+            dmh = torch.rsqrt(deg.clamp_min(1e-20))
+            L = eye - dmh.view(-1, 1) * W * dmh.view(1, -1)
+            L = 0.5 * (L + L.t())      # exactly symmetric after rounding
+        return float(self.params.weight) * L
+
+    def matrix(self, device) -> torch.Tensor:
+        device = torch.device(device)
+        key = (device.type, device.index)
+        m = self._cache.get(key)
+        if m is None:
+            m = self.laplacian().to(torch.float32).contiguous().to(device)
+            self._cache[key] = m
+        return m
+
+    def halo(self, roles: Roles):
+        return {}
+
+    @torch.no_grad()
+    def energy_grad(self, ctx: RegContext) -> torch.Tensor:
+        """ctx.g += lambda L x; returns lambda/2 sum Re<x, L x> (0-D FP64) (:171-234)."""
+        if self.params.weight == 0.0:
+            return torch.zeros((), device=ctx.device, dtype=torch.float64)
+        x, g = ctx.x, ctx.g
+        _lib.require_cuda(x, "x")
+        if x.dtype != torch.complex64 or not x.is_contiguous() or (g is not None and not g.is_contiguous()):
+            raise ValueError("GraphLaplacian (B200) needs contiguous complex64 x and g")
+        B = int(x.shape[0])
+        if B != self.frames:
+            raise ValueError(f"W is {self.frames} x {self.frames} but the image has {B} frames")
+        out = torch.zeros(2, dtype=torch.float64, device=x.device)
+        _lib.check(_lib.load().mrb_graph_pass(0, B, x.numel() // B, _lib.ptr(self.matrix(x.device)), _lib.ptr(x),
+                                              None, None, 0.0, _lib.ptr(g), None, _lib.ptr(out),
+                                              _lib.ptr(workspace(x.device)), _lib.stream_ptr(x.device)),
+                   "graph_pass")
+        return out[0]
+
+    def energy_grad_fixed_axes(self, ctx: RegContext, axes=None) -> torch.Tensor:
+        return self.energy_grad(ctx)
+
+    def _profile(self) -> torch.Tensor:
+        norm = (self.params.normalize or "none").lower()
+        v = self._deg_cpu if norm == "none" else (self._deg_cpu > 0).to(torch.float32)
+        return v * float(self.params.weight)
+
+    @torch.no_grad()
+    def add_diag(self, ctx: RegContext) -> bool:
+        """ctx.diag += lambda deg (none) or lambda 1{deg > 0} (rw, sym) per frame (:236-275)."""
+        if ctx.diag is None or self.params.weight == 0.0:
+            return False
+        D = ctx.diag
+        _lib.require_cuda(D, "diag")
+        if D.dtype != torch.float32 or not D.is_contiguous():
+            raise ValueError("diag must be contiguous float32")
+        B = int(D.shape[0])
+        v = self._profile().to(D.device)
+        _lib.check(_lib.load().mrb_diag_add_frames(D.numel() // B, B, _lib.ptr(v), _lib.ptr(D),
+                                                   _lib.stream_ptr(D.device)), "diag_add_frames")
+        return True
+
+    def majorizer_diag(self, ctx: RegContext) -> torch.Tensor:
+        return torch.zeros((), device=ctx.device, dtype=ctx.dtype_r)
+
+    def majorizer_profile(self, ctx: RegContext):
+        if self.params.weight == 0.0:
+            return None
+        return [(0, self._profile().to(device=ctx.device, dtype=ctx.dtype_r))]
 
 
 _WS = {}
@@ -215,10 +342,15 @@ class RegManager:
     def terms(self, roles: Roles, series_length: int = 0) -> List[_lib.TVTerm]:
         """Kernel descriptors of the active TV terms.  series_length > 0 splits the
         frame axis into independent series (several problems solved in one batch)."""
+        from .mapping import fused_tv
         out = []
-        for r in self._regs:
-            if not isinstance(r.params, TVParams):
-                raise TypeError(f"regulariser {r.name!r} is not a TV term")
+        for r0 in self._regs:
+            if isinstance(r0, GraphLaplacian):
+                continue                      # applied by graph_matrix / mrb_graph_pass
+            r = fused_tv(r0)
+            if r is None or not isinstance(r.params, TVParams):
+                raise TypeError(f"regulariser {r0.name!r} is neither a TV term (possibly behind an identity map) "
+                                "nor a graph Laplacian: the fused solver cannot evaluate it")
             axes = roles.resolve_axes(r.params.axes)
             t = tv_term_struct(r.params, axes, series_length)
             if t.enabled:
@@ -227,18 +359,60 @@ class RegManager:
             raise ValueError("at most 4 active TV terms")
         return out
 
+    def graph_matrix(self, frames: int, device) -> Optional[torch.Tensor]:
+        """Sum of the GraphLaplacian terms' lambda L (frames x frames float32 on
+        device), or None when there is none."""
+        g = [r for r in self._regs if isinstance(r, GraphLaplacian) and r.params.weight != 0.0]
+        if not g:
+            return None
+        for r in g:
+            if r.frames != frames:
+                raise ValueError(f"graph regulariser {r.name!r} is over {r.frames} frames, the image has {frames}")
+        L = sum(r.laplacian() for r in g)
+        return L.to(torch.float32).contiguous().to(device)
+
     @torch.no_grad()
     def add_diag(self, ws, series_length: int = 0) -> None:
         """ws "diag" += the regularisers' diagonal at ws "var" (manager.py:145-218,
-        one shard, identity regularisers): a term over the frame axis adds its frame
-        profile (preference (1) of the reference), any other term its lagged
-        diffusivity (preference (2)).  One ``mrb_tv_add_diag`` pass for all terms."""
-        if not ws.has("diag"):
-            return
+        one shard).  TV terms: a term over the frame axis adds its frame profile
+        (preference (1) of the reference), any other its lagged diffusivity
+        (preference (2)), in one ``mrb_tv_add_diag`` pass.  Other regularisers,
+        in the reference's order: frame profile, own add_diag (which may write a
+        parameter diagonal even without an image one), scalar majorizer."""
+        from .mapping import fused_tv
         roles = ws.plan.roles_image
-        terms = self.terms(roles, series_length)
-        if terms:
-            _add_diag_kernel(ws.get("var", 0), ws.get("diag", 0), roles, terms, frame_profile=1)
+        x = ws.get("var", 0)
+        D = ws.get("diag", 0) if ws.has("diag") else None
+        tv = [r for r in self._regs if isinstance(r, TVND)]
+        terms = RegManager(tv).terms(roles, series_length) if tv else []
+        if terms and D is not None:
+            _add_diag_kernel(x, D, roles, terms, frame_profile=1)
+        for r in self._regs:
+            if isinstance(r, TVND):
+                continue
+            ctx = RegContext(x=x, g=None, diag=D, roles_image=roles, device=x.device, dtype_c=x.dtype,
+                             dtype_r=torch.float32, ws=ws, shard_index=0)
+            # (1) frame profile, (2) the regulariser's own add_diag, (3) its scalar majorizer
+            prof_fn = getattr(r, "majorizer_profile", None)
+            if D is not None and callable(prof_fn):
+                prof = prof_fn(ctx)
+                if prof:
+                    for axis, v in prof:
+                        if int(axis) != 0:
+                            raise NotImplementedError("only frame-axis profiles are supported")
+                        _frame_profile(D, v)
+                    continue
+            add = getattr(r, "add_diag", None)
+            if callable(add):
+                add(ctx)
+                continue
+            maj = getattr(r, "majorizer_diag", None)
+            k = maj(ctx) if callable(maj) else None
+            if k is not None and D is not None:
+                if k.ndim == 0:
+                    _frame_profile(D, torch.full((int(D.shape[0]),), float(k)))
+                elif k.ndim == 1 and int(k.shape[0]) == int(D.shape[0]):
+                    _frame_profile(D, k)
 
     @torch.no_grad()
     def energy_and_grad(self, ws) -> torch.Tensor:
@@ -247,8 +421,8 @@ class RegManager:
         g = ws.get("grad", 0)
         total = torch.zeros((), device=x.device, dtype=torch.float64)
         for r in self._regs:
-            axes = roles.resolve_axes(r.params.axes)
+            axes = roles.resolve_axes(getattr(r.params, "axes", "spatial"))
             ctx = RegContext(x=x, g=g, diag=None, roles_image=roles, device=x.device, dtype_c=x.dtype,
-                             dtype_r=torch.float32)
+                             dtype_r=torch.float32, ws=ws, shard_index=0)
             total = total + r.energy_grad_fixed_axes(ctx, axes)
         return total

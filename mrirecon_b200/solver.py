@@ -50,6 +50,7 @@ from .roles import Roles
 S_T, S_LS_OK, S_DONE, S_REASON, S_ITER, S_F0, S_G0D, S_FT, S_GDT = range(9)
 S_ERR, S_ERD, S_EDD, S_RHO_PREV, S_RHO_INIT, S_BETA = range(9, 15)
 S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL, S_NRESTART, S_NOMORE = range(15, 21)
+S_GQ0, S_GQ1, S_GQ2 = range(21, 24)
 ARMIJO_J1 = 6   # trial steps of the first energy pass (t = 0, 1, 1/2, ..., 1/16)
 S_RED, S_EJ, S_G0D_NEXT = 24, 48, 80
 MAX_TERMS = 4
@@ -164,6 +165,12 @@ class CGSolver:
         self.S = tuple(int(s) for s in ishape[2:])
         self.F = int(ishape[0])
         self.terms = regm.terms(roles, c.series_length) if regm is not None else []
+        # graph Laplacian terms over the frame axis: one weighted B x B matrix
+        self._L = regm.graph_matrix(self.F, dev) if regm is not None and hasattr(regm, "graph_matrix") else None
+        # the direction pass of a non-symmetric L ("rw") also forms L^T d for the energy slope
+        self._gmode = 1 if self._L is None or bool(torch.equal(self._L, self._L.t())) else 2
+        if self._gmode == 2 and c.schedule == "toeplitz":
+            raise ValueError("the toeplitz schedule needs a symmetric graph Laplacian (normalize 'none' or 'sym')")
         self.nterms = len(self.terms)
         self._terms_arr = (_lib.TVTerm * max(1, self.nterms))(*self.terms)
         self._Sarr = (ct.c_int * 3)(*(list(self.S) + [1] * (3 - self.nd)))
@@ -251,6 +258,18 @@ class CGSolver:
     def _slot(self, i):
         return self.s.data_ptr() + 8 * i
 
+    def _graph_pass(self, mode, d, t_dev, t_host, acc, out, skip=None):
+        """mrb_graph_pass on the current x (no-op without graph terms)."""
+        if self._L is None:
+            return
+        _lib.check(self.lib.mrb_graph_pass(mode, self.F, self.n_img // self.F, _lib.ptr(self._L), _lib.ptr(self.x),
+                                           _lib.ptr(d), t_dev, float(t_host), _lib.ptr(acc), skip, out,
+                                           _lib.ptr(self.ws_buf), self._st()), "graph_pass")
+
+    def _quad_fold(self, phase):
+        if self._L is not None:
+            _lib.check(self.lib.mrb_ncg_quad_fold(_lib.ptr(self.s), phase, self._st()), "quad_fold")
+
     def _backend(self):
         return getattr(self.op, "backend", self.op)
 
@@ -288,6 +307,9 @@ class CGSolver:
             self.gr.sub_(self.ahy)
         else:
             self._AH(self.r, self.gr)
+        # graph terms: gr += L x, q0 = 1/2 <x, L x>, err += 2 q0
+        self._graph_pass(0, None, None, 0.0, self.gr, self._slot(S_GQ0))
+        self._quad_fold(0)
         self._tv_grad(None, None, 0.0, self.gr, None, self.g, self._slot(S_RED))
         _lib.check(self.lib.mrb_ncg_steepest(self.n_img, _lib.ptr(self.d), _lib.ptr(self.g), _lib.ptr(self.g_prev),
                                              _lib.ptr(self.D), self._ndiag, self._slot(S_G0D), _lib.ptr(self.ws_buf),
@@ -312,6 +334,8 @@ class CGSolver:
                                         _lib.stream_ptr(self.device)), "tv_multi")
         if self._toep is not None:
             self._toep.AHA(self.d, out=self.gAd)
+            # graph terms join the normal operator before Re<gr, d>, Re<gAd, d>
+            self._graph_pass(self._gmode, self.d, None, 0.0, self.gAd, self._slot(S_GQ1), skip=self._slot(S_DONE))
             _lib.check(lib.mrb_dots_f64(self.n_img, 2, self._dot_a, self._dot_b, self._dot_w, 0,
                                         self._slot(S_ERD), ws, st), "dots")
         else:
@@ -319,6 +343,9 @@ class CGSolver:
             _lib.check(lib.mrb_kspace_pass(0, self.n_k, _lib.ptr(self.r), _lib.ptr(self.Ad), None, None, None,
                                            0.0, self._slot(S_DONE), self._slot(S_ERR), ws, st), "kspace_pass")
             self._AH(self.Ad, self.gAd)
+            # graph terms: gAd += L d, q1 = Re<x, L d>, q2 = Re<d, L d> folded into the data scalars
+            self._graph_pass(self._gmode, self.d, None, 0.0, self.gAd, self._slot(S_GQ1), skip=self._slot(S_DONE))
+            self._quad_fold(1)
         # Armijo in two phases: the TV energies of the first ARMIJO_J1 trial steps
         # (side stream, above), the rest only when none of those is accepted
         main.wait_stream(self._side)
@@ -345,6 +372,7 @@ class CGSolver:
         else:
             _lib.check(lib.mrb_kspace_pass(2, self.n_k, _lib.ptr(self.r), _lib.ptr(self.Ad), None, None,
                                            self._slot(S_T), 0.0, self._slot(S_DONE), None, ws, st), "kspace_pass")
+            self._quad_fold(2)
 
     def _plan(self):
         """The B200 NUFFT plan behind the operator (front-end or adapter), if any."""
@@ -414,9 +442,10 @@ class CGSolver:
                                             _lib.ptr(self.y), None, float(t), None, out.data_ptr(),
                                             _lib.ptr(self.ws_buf), st), "kspace_pass")
         self._AH(self.r, self.gr)
+        self._graph_pass(0, self.d, None, t, self.gr, out.data_ptr() + 8 * 20)
         self._tv_grad(self.d, None, t, self.gr, None, self.g, out.data_ptr() + 8 * 8)
         v = out.tolist()
-        f = 0.5 * v[0] + sum(v[8:8 + self.nterms])
+        f = 0.5 * v[0] + sum(v[8:8 + self.nterms]) + (v[20] if self._L is not None else 0.0)
         return f, v[8 + MAX_TERMS], v
 
     def _armijo_ref(self, out):
@@ -611,5 +640,6 @@ class CGSolver:
                                         _lib.ptr(self.x), None, None, 0.0, None, None, None, None, 0, None,
                                         None, 0, out.data_ptr() + 64, _lib.ptr(self.ws_buf), self._st()),
                    "tv_grad")
+        self._graph_pass(0, None, None, 0.0, None, out.data_ptr() + 8 * 20)
         v = out.tolist()
-        return 0.5 * v[0] + sum(v[8:8 + self.nterms])
+        return 0.5 * v[0] + sum(v[8:8 + self.nterms]) + (v[20] if self._L is not None else 0.0)

@@ -29,6 +29,7 @@ from typing import Callable, Dict, List, Optional, Sequence
 
 import torch
 
+from .graph import GraphSpec, graph_energy_grad
 from .tv import tv_energy_grad
 
 
@@ -97,7 +98,11 @@ class NCGOracle:
         xt = self.x + self.d * t
         f_reg = torch.zeros((), dtype=f_data.dtype)
         for s in self.regs:
-            E, gr = tv_energy_grad(xt, s.axes, s.weight, s.eps, s.isotropic, s.axis_weights)
+            if isinstance(s, GraphSpec):
+                E, gr = graph_energy_grad(xt, s.L, s.weight)
+                E = E.to(f_data.dtype)
+            else:
+                E, gr = tv_energy_grad(xt, s.axes, s.weight, s.eps, s.isotropic, s.axis_weights)
             f_reg = f_reg + E
             g = g + gr
         self.g = g

@@ -197,3 +197,63 @@ def test_majorizer_host_logic():
     (ax, v), = tm.majorizer_profile(ctx)
     assert ax == 0
     np.testing.assert_allclose(v.numpy(), np.array([1, 2, 2, 2, 1]) * 2e-3, rtol=1e-6)
+
+
+# --- graph Laplacian (graph_laplacian.py:22-321) --------------------------------
+def test_graph_oracle_degree_profile_reference_case():
+    """Chain graph over 5 frames, weight 2: diagonal (1,2,2,2,1) * 2
+    (the expectation of the reference's test_regularization_ns.py:206-235)."""
+    from oracle.graph import degree_profile
+    W = torch.zeros(5, 5)
+    for t in range(4):
+        W[t, t + 1] = W[t + 1, t] = 1.0
+    np.testing.assert_allclose(degree_profile(W, "none", 2.0).numpy(), [2, 4, 4, 4, 2])
+    np.testing.assert_allclose(degree_profile(W, "sym", 2.0).numpy(), [2, 2, 2, 2, 2])
+
+
+@pytest.mark.parametrize("norm", ["none", "rw", "sym"])
+def test_graph_oracle_gradient_matches_finite_difference(norm):
+    """Directional derivative of the energy against central differences (the
+    reference's test_regularization_ns.py:238-280 checks the sym case the same way)."""
+    from oracle.graph import graph_energy_grad, laplacian
+    g = torch.Generator().manual_seed(4)
+    W = torch.rand(6, 6, generator=g, dtype=torch.float64)
+    L = laplacian(W, norm)
+    if norm == "rw":   # I - D^-1 W is not symmetric: the energy's gradient is (L + L^T)/2 x
+        L = 0.5 * (L + L.T)
+    x = torch.randn(6, 1, 4, 4, dtype=torch.complex128, generator=g) * 0.05
+    d = torch.randn(6, 1, 4, 4, dtype=torch.complex128, generator=g) * 0.1
+    _, gr = graph_energy_grad(x, L, 1e-3)
+    h = 1e-5
+    fd = (graph_energy_grad(x + h * d, L, 1e-3)[0] - graph_energy_grad(x - h * d, L, 1e-3)[0]) / (2 * h)
+    an = (gr.conj() * d).real.sum()
+    assert abs(float(an - fd)) <= 1e-9 * max(1.0, abs(float(an)))
+
+
+def test_graph_laplacian_host_matrix_matches_oracle():
+    """GraphLaplacian's dense lambda L (host arithmetic) equals the oracle's for
+    dense and sparse W and all three normalisations."""
+    from oracle.graph import laplacian
+    from mrirecon_b200.regularization import GraphLaplacian, GraphLapParams
+    g = torch.Generator().manual_seed(5)
+    W = torch.rand(7, 7, generator=g)
+    W[3, :] = 0
+    W[:, 3] = 0                      # an isolated frame
+    for norm in ("none", "rw", "sym"):
+        for Win in (W, W.to_sparse()):
+            r = GraphLaplacian("g", Win, GraphLapParams(weight=0.5, normalize=norm))
+            np.testing.assert_allclose(r.laplacian().numpy(), 0.5 * laplacian(W, norm).numpy(), rtol=1e-6,
+                                       atol=1e-7)
+    with pytest.raises(ValueError):
+        GraphLaplacian("g", W, GraphLapParams(weight=0.5, normalize="row"))
+
+
+def test_basis_push_oracle_reference_expectations():
+    """The reference's temporal-basis push (test_reg_diag_mapped.py:93-122):
+    |U|^2 = [[1,0,0],[0,4,0]], k = 2 lambda * 2 axes: diag_V = (k, 4k, 0)."""
+    from oracle.mapping import basis_diag_push, basis_profile_push
+    U = torch.tensor([[1.0, 0.0, 0.0], [0.0, 2.0, 0.0]])
+    k = 2.0 * 1e-3 * 2.0
+    DV = basis_diag_push(U, torch.full((2, 1, 3, 2), k, dtype=torch.float64))
+    np.testing.assert_allclose(DV[:, 0, 0, 0].numpy(), [k, 4 * k, 0.0], atol=1e-15)
+    np.testing.assert_allclose(basis_profile_push(U, torch.tensor([1.0, 1.0])).numpy(), [1.0, 4.0, 0.0])
