@@ -21,7 +21,7 @@ from typing import List, Optional, Sequence, Tuple
 import torch
 
 from . import _lib
-from .solver import CGConfig, CGSolver, REASONS, S_DONE, S_ITER, S_REASON
+from .solver import CGConfig, CGSolver, REASONS, S_DONE, S_ITER, S_REASON, capture_graph
 
 
 class BatchedSolver:
@@ -87,7 +87,7 @@ class BatchedSolver:
                         torch.cuda.synchronize(self.device)
                         g = torch.cuda.CUDAGraph()
                         n1 = _lib.launch_count()
-                        with torch.cuda.graph(g):
+                        with capture_graph(g, self.device):
                             def body(s):
                                 for _ in range(max(1, c.iters_per_graph)):
                                     s._iteration_fast()

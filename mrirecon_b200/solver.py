@@ -95,6 +95,36 @@ class CGConfig:
     precond: str = "none"
 
 
+class capture_graph:
+    """Capture the launches of a block into a CUDA graph on a side stream.
+
+    torch.cuda.graph also empties torch's device and pinned-host caches before
+    every capture, so the next solve's allocations go back to cudaMalloc /
+    cudaHostAlloc; that costs tens to hundreds of milliseconds at random when
+    a solver (and its graph) is built per scan.  The solvers allocate nothing
+    inside the captured region, so the caches can stay."""
+
+    def __init__(self, graph: torch.cuda.CUDAGraph, device):
+        self.graph = graph
+        self.device = device
+        self.stream = torch.cuda.Stream(device)
+
+    def __enter__(self):
+        self.stream.wait_stream(torch.cuda.current_stream(self.device))
+        self._ctx = torch.cuda.stream(self.stream)
+        self._ctx.__enter__()
+        self.graph.capture_begin()
+        return self.graph
+
+    def __exit__(self, *exc):
+        try:
+            self.graph.capture_end()
+        finally:
+            self._ctx.__exit__(*exc)
+            torch.cuda.current_stream(self.device).wait_stream(self.stream)
+        return False
+
+
 class _Shard:
     def __init__(self, device):
         self.device = device
@@ -418,7 +448,7 @@ class CGSolver:
             torch.cuda.synchronize(self.device)
             g = torch.cuda.CUDAGraph()
             n1 = _lib.launch_count()
-            with torch.cuda.graph(g):
+            with capture_graph(g, self.device):
                 for _ in range(max(1, c.iters_per_graph)):
                     self._iteration_fast()
             self.launch_stats["per_graph"] = _lib.launch_count() - n1
