@@ -87,6 +87,9 @@ def parse():
     ap.add_argument("--no-jacobi", action="store_true", help="skip the Jacobi-preconditioned solve block")
     ap.add_argument("--nufft-only", action="store_true",
                     help="profiling case: prepare the workload's operator and run 3 forward/adjoint pairs")
+    ap.add_argument("--ncg-only", type=int, default=0, metavar="K",
+                    help="profiling case: K eager iterations of the workload's plain NCG solver between "
+                         "cudaProfilerStart/Stop")
     ap.add_argument("--koosh-only", type=int, default=0, metavar="N",
                     help="profiling case: the 3D koosh-ball operator scaled to an N^3 image (spokes x (N/160)^2, "
                          "samples per spoke x N/160, 16 coils), 3 forward/adjoint pairs")
@@ -308,6 +311,34 @@ def run_nufft_only(w, local):
         op.AH(y, out=x)
     torch.cuda.synchronize()
     print(json.dumps({"nufft_only": w["name"], "plan": op.backend.plan.info()}))
+    return 0
+
+
+def run_ncg_only(w, n_iter, local):
+    """Profiling case: the workload's plain NCG solver (fast schedule, eager
+    launches), primed outside the profiled range; n_iter iterations between
+    cudaProfilerStart and cudaProfilerStop (ncu --profile-from-start off)."""
+    from mrirecon_b200 import phantoms
+    from mrirecon_b200.nufft import NUFFT, NUFFTConfig
+    from mrirecon_b200.solver import CGSolver
+    dev = torch.device("cuda", local)
+    x_true, maps, traj = make_inputs(w)
+    op = NUFFT(maps.to(dev), traj.to(dev), None, axis=axis_spec(), config=NUFFTConfig(ndim=2, traj_units="rad"),
+               device=dev)
+    y = phantoms.add_noise(op.A(x_true.to(dev)), w["sigma"], seed=1) if w["sigma"] > 0 else op.A(x_true.to(dev))
+    cfg = solver_cfg()
+    cfg.cuda_graph = False
+    s = CGSolver(y, op, regs(w), cfg)
+    s._fast_setup(cfg.max_iter)
+    s._prime_fast()
+    s._iteration_fast()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    for _ in range(n_iter):
+        s._iteration_fast()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"ncg_only": w["name"], "iterations": n_iter, "iter": int(s.s[4].item())}))
     return 0
 
 
@@ -689,6 +720,8 @@ def main():
             return run_nufft_only(w, local)
         if args.koosh_only:
             return run_koosh_only(args.koosh_only, local)
+        if args.ncg_only:
+            return run_ncg_only(w, args.ncg_only, local)
         return run_b200(args, w, ws, rank, local)
     finally:
         if ws > 1:

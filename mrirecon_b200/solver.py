@@ -51,7 +51,11 @@ S_T, S_LS_OK, S_DONE, S_REASON, S_ITER, S_F0, S_G0D, S_FT, S_GDT = range(9)
 S_ERR, S_ERD, S_EDD, S_RHO_PREV, S_RHO_INIT, S_BETA = range(9, 15)
 S_CUM_X, S_CUM_G, S_CUM_S, S_NTRIAL, S_NRESTART, S_NOMORE = range(15, 21)
 S_GQ0, S_GQ1, S_GQ2 = range(21, 24)
-ARMIJO_J1 = 6   # trial steps of the first energy pass (t = 0, 1, 1/2, ..., 1/16)
+# trial steps of the first energy pass (t = 0, 1, 1/2, ..., 1/64): on the GRASP workload
+# the accepted steps are 2^-3 .. 2^-11, three quarters of them >= 2^-6, so the second
+# pass runs in a quarter of the iterations (8 is also the largest pass the 64-register
+# variant of tv_multi_kernel takes)
+ARMIJO_J1 = 8
 S_RED, S_EJ, S_G0D_NEXT = 24, 48, 80
 MAX_TERMS = 4
 REASONS = {0: "running", 1: "line-search failed", 2: "converged (tol_g/tol_step)",
