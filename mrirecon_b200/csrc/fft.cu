@@ -87,7 +87,15 @@ __host__ __device__ constexpr int clamp_rows(int r) { return r < 1 ? 1 : r > 16 
 // transforms per block: about 8 (rows) / 16 (columns) complex values per thread
 __host__ __device__ constexpr int rows_per_block(int G) { return clamp_rows(8 * ROW_NT / G); }
 __host__ __device__ constexpr int cols_per_block(int G) { return clamp_rows(16 * COL_NT / G); }
-__host__ __device__ constexpr int padded_len(int G) { return G + (G >> 3) + 1; }
+// Row transforms keep their intermediate values in shared memory at the
+// swizzled slot e ^ ((e >> 3) & 15) (a bijection inside each aligned group of
+// 16), rows LD = roundup16(G) + 8 apart.  Against a plain layout this removes
+// the 2-way bank conflicts of the radix-8 Stockham exchanges (stride-8 stores,
+// runs of 8 at stride 64) for every compiled length; with the 64-bit accesses
+// of a warp split in two 16-lane halves, G = 512 needs 128 wavefronts per row
+// instead of 192 with the earlier "one pad slot per 8" layout.
+__host__ __device__ constexpr int row_ld(int G) { return ((G + 15) & ~15) + 8; }
+__host__ __device__ __forceinline__ int swz(int e) { return e ^ ((e >> 3) & 15); }
 
 std::vector<float2> host_twiddles(int G) {
   std::vector<float2> t;
@@ -261,14 +269,14 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load
 
 // All stages of a length-G transform of ROWS rows: the first stage loads
 // through load0, the last stores through store_last, and intermediate results
-// live in buf (row q at q * LD, element e at e + e / 8 when PAD).
+// live in buf (row q at q * LD, element e at slot swz(e) when PAD).
 template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool PAD, int LD, bool WARP = false, class LD0,
           class STL>
 __device__ __forceinline__ void fft_stages(float2* buf, const float2* tw, LD0 load0, STL store_last) {
   constexpr int NS = n_stages(G);
   if constexpr (S < NS) {
-    auto sload = [&](int q, int e) { return buf[q * LD + (PAD ? e + (e >> 3) : e)]; };
-    auto sstore = [&](int q, int e, float2 v) { buf[q * LD + (PAD ? e + (e >> 3) : e)] = v; };
+    auto sload = [&](int q, int e) { return buf[q * LD + (PAD ? swz(e) : e)]; };
+    auto sstore = [&](int q, int e, float2 v) { buf[q * LD + (PAD ? swz(e) : e)] = v; };
     if constexpr (S == 0 && S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP>(tw, load0, store_last);
     else if constexpr (S == 0) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP>(tw, load0, sstore);
     else if constexpr (S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP>(tw, sload, store_last);
@@ -293,7 +301,7 @@ __global__ void __launch_bounds__(ROW_NT) fwd_rows_kernel(const float2* __restri
                                                           const float* __restrict__ coldeap, float2* __restrict__ Tb,
                                                           const float2* __restrict__ tw, Geo2 g, long long nrows,
                                                           int coil_images) {
-  constexpr int LD = padded_len(G1);
+  constexpr int LD = row_ld(G1);
   extern __shared__ float2 sm[];
   if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   const int warp = threadIdx.x >> 5;
@@ -540,7 +548,7 @@ __global__ void __launch_bounds__(ROW_NT) adj_rows_kernel(const float2* __restri
                                                           const float* __restrict__ coldeap, float2* __restrict__ x,
                                                           const float2* __restrict__ tw, Geo2 g, float scale) {
   constexpr int ROWS = rows_per_block(G1);
-  constexpr int LD = padded_len(G1);
+  constexpr int LD = row_ld(G1);
   extern __shared__ float2 sm[];
   if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   float2* acc = sm + ROWS * LD;   // S1 accumulators
@@ -556,12 +564,12 @@ __global__ void __launch_bounds__(ROW_NT) adj_rows_kernel(const float2* __restri
       if (q >= ncl) return make_float2(0.f, 0.f);
       return tb[q * cstride + n1];
     };
-    auto sstore = [&](int q, int e, float2 v) { sm[q * LD + e + (e >> 3)] = v; };
+    auto sstore = [&](int q, int e, float2 v) { sm[q * LD + swz(e)] = v; };
     fft_stages<G1, 0, ROWS, ROW_NT, +1, false, true, LD>(sm, tw, load0, sstore);
     for (int i = threadIdx.x; i < g.S1; i += ROW_NT) {
       float2 s = acc[i];
       const int e = i + g.off1;
-      const int pe = e + (e >> 3);
+      const int pe = swz(e);
       const float2* mp = maps + (long long)c0 * g.stot + (long long)r * g.S1 + i;
       for (int q = 0; q < ncl; ++q) {
         const float2 v = sm[q * LD + pe];
@@ -609,7 +617,7 @@ template <int G1>
 int launch_fwd_rows(const void* x, const float2* maps, const float* rowfac, const float* coldeap, float2* Tb,
                     const float2* tw,
                     const Geo2& g, int nb, int coil_images, cudaStream_t st) {
-  const size_t smem = (size_t)ROW_WARPS * padded_len(G1) * sizeof(float2);
+  const size_t smem = (size_t)ROW_WARPS * row_ld(G1) * sizeof(float2);
   int rc;
   if ((rc = set_smem((const void*)fwd_rows_kernel<G1>, smem))) return rc;
   const long long nrows = (long long)nb * g.C * g.S0;
@@ -688,7 +696,7 @@ int launch_adj_rows(const float2* Tb, const float2* maps, const float* rowfac, c
                     const float2* tw,
                     const Geo2& g, int nb, float scale, cudaStream_t st) {
   constexpr int ROWS = rows_per_block(G1);
-  const size_t smem = ((size_t)ROWS * padded_len(G1) + g.S1) * sizeof(float2);
+  const size_t smem = ((size_t)ROWS * row_ld(G1) + g.S1) * sizeof(float2);
   int rc;
   if ((rc = set_smem((const void*)adj_rows_kernel<G1>, smem))) return rc;
   const long long blocks = (long long)nb * g.S0;
