@@ -782,12 +782,13 @@ template <int ND, int T>
 struct SpreadSmem {
   static constexpr int CELLS = ND == 2 ? T * T : T * T * T;
   static constexpr int NW = 4 * ND;                               // staged weights per sample
+  static constexpr int NWP = NW + 1;                              // their stride (odd: no bank conflicts)
   static constexpr int NTAP = ND == 2 ? 16 : 64;
   // the shared tile is coil-interleaved, [cell][coil] with an even coil stride, so
   // one lane updates a pair of coils with one 128-bit read-modify-write
   __host__ __device__ static int cstride(int cpi) { return (cpi + 1) & ~1; }
   __host__ __device__ static size_t warp_bytes(int cpi) {
-    return (size_t)cstride(cpi) * CELLS * sizeof(float2) + SPREAD_BATCH * (sizeof(int4) + NW * sizeof(float)) +
+    return (size_t)cstride(cpi) * CELLS * sizeof(float2) + SPREAD_BATCH * (sizeof(int4) + NWP * sizeof(float)) +
            (size_t)SPREAD_BATCH * cstride(cpi) * sizeof(float2);
   }
 };
@@ -797,7 +798,7 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
   if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   using SM = SpreadSmem<ND, T>;
   constexpr int CELLS = SM::CELLS;
-  constexpr int NW = SM::NW;
+  constexpr int NW = SM::NWP;   // stride of the staged weights
   constexpr int NTAP = SM::NTAP;
   extern __shared__ float4 smem4[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -940,9 +941,13 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
       const int4 bb = sb[j];
       const float* wj = sw + j * NW;
       const float4* yj = reinterpret_cast<const float4*>(sy + j * cps);
-      // lane tasks: (tap, coil pair), every task of a sample touches a distinct float4
+      // lane tasks: (tap, coil pair), every task of a sample touches a distinct float4;
+      // coil pair fastest, so that the 8 lanes of a 128-bit access phase cover
+      // consecutive (cell, pair) slots (taps first: all 4 taps of a row land on
+      // the same bank group and conflict 2-way)
       for (int tk = lane; tk < ntask; tk += 32) {
-        const int tap = tk & (NTAP - 1), pr = tk / NTAP;
+        const int pr = npair == 2 ? (tk & 1) : tk % npair;
+        const int tap = npair == 2 ? (tk >> 1) : tk / npair;
         int cell;
         float w;
         bool inside;
