@@ -341,15 +341,18 @@ __global__ void __launch_bounds__(COL_NT) fwd_cols_kernel(const float2* __restri
   const int cblocks = (g.G1 + COLS - 1) / COLS;
   const int vol = blockIdx.x / cblocks;
   const int k0 = (blockIdx.x - vol * cblocks) * COLS;
-  const float2* tv = Tb + (long long)vol * g.S0 * g.G1;
-  float2* gv = grid + (long long)vol * g.gtot;
+  // 32-bit offsets inside one volume (at most 1024^3 = 2^30 cells for the compiled lengths)
+  const int G1 = g.G1;
+  const bool full = k0 + COLS <= G1;
+  const float2* tv = Tb + (long long)vol * g.S0 * G1 + k0;
+  float2* gv = grid + (long long)vol * g.gtot + k0;
   auto load0 = [&](int q, int n0) -> float2 {
     const int r = n0 - g.off0;
-    if ((unsigned)r >= (unsigned)g.S0 || k0 + q >= g.G1) return make_float2(0.f, 0.f);
-    return tv[(long long)r * g.G1 + k0 + q];
+    if ((unsigned)r >= (unsigned)g.S0 || (!full && k0 + q >= G1)) return make_float2(0.f, 0.f);
+    return tv[r * G1 + q];
   };
   auto store = [&](int q, int n0, float2 v) {
-    if (k0 + q < g.G1) gv[(long long)n0 * g.G1 + k0 + q] = v;
+    if (full || k0 + q < G1) gv[n0 * G1 + q] = v;
   };
   fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
 }
@@ -483,15 +486,18 @@ __global__ void __launch_bounds__(COL_NT) adj_cols_kernel(const float2* __restri
   const int cblocks = (g.G1 + COLS - 1) / COLS;
   const int vol = blockIdx.x / cblocks;
   const int k0 = (blockIdx.x - vol * cblocks) * COLS;
-  const float2* gv = grid + (long long)vol * g.gtot;
-  float2* tv = Tb + (long long)vol * g.S0 * g.G1;
+  // 32-bit offsets inside one volume (at most 1024^3 = 2^30 cells for the compiled lengths)
+  const int G1 = g.G1;
+  const bool full = k0 + COLS <= G1;
+  const float2* gv = grid + (long long)vol * g.gtot + k0;
+  float2* tv = Tb + (long long)vol * g.S0 * G1 + k0;
   auto load0 = [&](int q, int n0) -> float2 {
-    if (k0 + q >= g.G1) return make_float2(0.f, 0.f);
-    return gv[(long long)n0 * g.G1 + k0 + q];
+    if (!full && k0 + q >= G1) return make_float2(0.f, 0.f);
+    return gv[n0 * G1 + q];
   };
   auto store = [&](int q, int n0, float2 v) {
     const int r = n0 - g.off0;
-    if ((unsigned)r < (unsigned)g.S0 && k0 + q < g.G1) tv[(long long)r * g.G1 + k0 + q] = v;
+    if ((unsigned)r < (unsigned)g.S0 && (full || k0 + q < G1)) tv[r * G1 + q] = v;
   };
   fft_stages<G0, 0, COLS, COL_NT, +1, true, false, LD>(sm, tw, load0, store);
 }
