@@ -83,10 +83,10 @@ int mrb_plan_destroy(mrb_plan* plan);
  *         sharing the staged samples (2D tile 16, 3D tile 8; other tiles fall
  *         back to 0; the 3D default), 0 one warp per work item and coil group
  *         (the 2D default),
- * key 7 = grid mask (fused FFT mode): 1 (default) the forward column pass
- *         stores, and the adjoint column pass loads, only the grid cells inside
- *         some sample's support (per-frame bitmaps built by set_points), and the
- *         spread stores no zeros outside them; 0 full grid passes,
+ * key 7 = grid mask (fused FFT mode): 1 (default) the adjoint spread keeps its
+ *         own grid, zeroed once per trajectory and batch size, and stores only
+ *         the cell pairs inside some sample's support (per-frame bitmaps built by
+ *         set_points); 0 the spread writes every cell of every tile,
  * key 8 = 2D fused mode: the forward column pass interpolates the samples of
  *         each column strip from shared memory and never writes the grid
  *         (1; set before set_points, which then builds the per-frame strip
