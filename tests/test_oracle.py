@@ -257,3 +257,28 @@ def test_basis_push_oracle_reference_expectations():
     DV = basis_diag_push(U, torch.full((2, 1, 3, 2), k, dtype=torch.float64))
     np.testing.assert_allclose(DV[:, 0, 0, 0].numpy(), [k, 4 * k, 0.0], atol=1e-15)
     np.testing.assert_allclose(basis_profile_push(U, torch.tensor([1.0, 1.0])).numpy(), [1.0, 4.0, 0.0])
+
+
+def test_fused_solver_term_classification():
+    """Host logic: which regularisers the fused solver evaluates as TV terms
+    (a TVND, bare or behind identity / scale maps), which as graph terms, and
+    which it refuses (parameter-space mappings)."""
+    from mrirecon_b200.mapping import (ComposeOp, IdentityOp, MappedRegularizer, ScaleOp, TemporalBasisOp,
+                                       Transformed, fused_tv)
+    from mrirecon_b200.regularization import GraphLaplacian, GraphLapParams, RegManager, TVND, TVParams
+    from mrirecon_b200.roles import Roles
+    tv = TVND("s", TVParams(weight=1e-3, eps=1e-3, axes="spatial"))
+    assert fused_tv(tv) is tv
+    assert fused_tv(MappedRegularizer("m", tv, IdentityOp())) is tv
+    assert fused_tv(Transformed(tv, ScaleOp(), "t")) is tv
+    assert fused_tv(MappedRegularizer("c", tv, ComposeOp([IdentityOp(), ScaleOp()]))) is tv
+    basis = MappedRegularizer("p", tv, TemporalBasisOp(U=torch.randn(4, 2)))
+    assert fused_tv(basis) is None
+    gl = GraphLaplacian("g", torch.ones(4, 4), GraphLapParams(weight=1.0))
+    roles = Roles(1, 1, 2)
+    terms = RegManager([tv, gl, Transformed(tv, IdentityOp(), "t")]).terms(roles)
+    assert len(terms) == 2 and all(t.naxes == 2 for t in terms)
+    with pytest.raises(TypeError):
+        RegManager([basis]).terms(roles)
+    Lg = gl.laplacian().numpy()          # W = ones, diagonal removed: deg 3, L = 3 I - (J - I) = 4 I - J
+    np.testing.assert_allclose(Lg, 4 * np.eye(4) - np.ones((4, 4)), atol=1e-12)
