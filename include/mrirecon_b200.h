@@ -202,9 +202,11 @@ int mrb_dots_f64(int64_t n, int npairs, const void* const* a, const void* const*
  * the process exits.  For callers that cannot allocate device memory where
  * they need the dots (inside a CUDA stream capture, in real-time loops where
  * cudaMalloc/cudaFree would synchronise the device, or when another allocator
- * owns all device memory).  npairs above 8 is rejected (MRB_ERANGE).  The
- * first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) and should come before any stream capture.  All
+ * owns all device memory).  npairs above 8 is rejected (MRB_ERANGE).  A call
+ * outside a stream capture looks up the array's device address on the current
+ * device (cudaGetSymbolAddress, so a cudaDeviceReset leaves nothing stale); a
+ * call inside a capture reuses the address of the last call outside one, so
+ * the first call on a device must come before any capture (else MRB_ESTATE).  All
  * calls share the one array, so calls that overlap on the GPU (other streams,
  * other host threads) race; serialise them.  No part of the array needs to
  * start at zero: every call overwrites each partial it reads.

@@ -180,6 +180,8 @@ __global__ void __launch_bounds__(RED_THREADS) dots_kernel(DotArgs a, double* __
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
 #pragma unroll
     for (int j = 0; j < NP; ++j) {
+      // the 8-wide instance serves npairs 5..8: slots past npairs hold no operands
+      if (NP > 4 && j >= a.npairs) continue;
       float2 u = a.a[j][i], v = a.b[j][i];
       float r = u.x * v.x + u.y * v.y;
       if (a.diag[j]) r /= a.diag[j][i % a.ndiag];
@@ -1687,20 +1689,30 @@ double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
 
 // Device address of the scratch array on the current device.  The host-side
 // name g_noalloc_partials is only a stand-in and must never be passed to a
-// kernel; the address is looked up once per device, with that device current.
-int noalloc_scratch(double** out) {
+// kernel; the address is looked up with that device current.  Outside a
+// stream capture the lookup is repeated on every call (a host-side table
+// lookup once the module is loaded), so a cudaDeviceReset, which reloads the
+// module at a possibly different address, cannot leave a stale pointer behind;
+// inside a capture the address cached by the last call outside one is used,
+// so the first call on a device has to come before any capture.
+int noalloc_scratch(cudaStream_t st, double** out) {
   int dev = -1;
   MRB_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
     return mrb::fail(MRB_ERANGE, "device ordinal %d above the %d supported", dev, NOALLOC_MAX_DEVICES);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  MRB_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  if (cs == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
     if (e != cudaSuccess || p == nullptr)
       return mrb::fail(MRB_ECUDA, "cudaGetSymbolAddress(scratch) failed on device %d: %s", dev,
                        cudaGetErrorString(e));
     g_noalloc_ptr[dev] = (double*)p;
+  } else if (!g_noalloc_ptr[dev]) {
+    return mrb::fail(MRB_ESTATE, "mrb_dots_f64_noalloc: the first call on device %d must come before "
+                                 "any stream capture", dev);
   }
   *out = g_noalloc_ptr[dev];
   return 0;
@@ -1715,10 +1727,10 @@ extern "C" int mrb_dots_f64_noalloc(int64_t n, int npairs, const void* const* a,
                      npairs, NOALLOC_MAX_PAIRS);
   MRB_REQUIRE(n >= 0, "mrb_dots_f64_noalloc: negative length");
   MRB_REQUIRE(a && b && out, "mrb_dots_f64_noalloc: null pointer");
-  double* part = nullptr;
-  int rc = noalloc_scratch(&part);
-  if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
+  double* part = nullptr;
+  int rc = noalloc_scratch(st, &part);
+  if (rc) return rc;
   DotArgs d{};
   for (int j = 0; j < npairs; ++j) {
     MRB_REQUIRE(a[j] && b[j], "mrb_dots_f64_noalloc: null operand %d", j);
