@@ -1,22 +1,33 @@
 """Axis grammar and layout planners of the NUFFT front-end.
 
-Same behaviour as graspcg/nufft/layout.py:11-193: ``AxisSpec`` accepts the new
-(``image_labels``...) or legacy (``image``...) keyword names; the planners
-infer B, the "like" labels/sizes (every image label that is not 'B', the coil
-label or an FFT label) and the spatial / coil / K sizes from a tensor or from
-bare sizes.  Images must be coil-combined (coil axis of size 1 if present).
+The interface follows graspcg/nufft/layout.py:11-193 so that reference callers
+construct axis specs and read plans unchanged: ``AxisSpec`` takes either the
+``*_labels`` keyword names or the shorter legacy names (``image``, ``kspace``,
+``image_fft``, ``kspace_fft``, ``coil``), the coil label defaults to 'coil' and
+the k-space FFT labels to ('K',); a plan carries B, the "like" labels and
+sizes (image or k-space labels that are neither 'B', the coil label nor an FFT
+label) with their product, and the spatial sizes or the coil count and K.
+Errors keep the reference's exception types: TypeError for a spec without its
+three required label groups, ValueError for a tensor that does not fit.
+
+Here an AxisSpec resolves its keywords through one alias table, and the
+planners share one classification of labels into roles.
 """
 from __future__ import annotations
 
 from dataclasses import dataclass
-from functools import reduce
-import operator
+import math
 from typing import Dict, Sequence, Tuple
 
 import torch
 
+# (field, its legacy keyword)
+_FIELDS = (("image_labels", "image"), ("kspace_labels", "kspace"), ("image_fft_labels", "image_fft"),
+           ("kspace_fft_labels", "kspace_fft"), ("coil_label", "coil"))
+_DEFAULTS = {"kspace_fft_labels": ("K",), "coil_label": "coil"}
 
-@dataclass(init=False)
+
+@dataclass(frozen=True, init=False)
 class AxisSpec:
     image_labels: Tuple[str, ...]
     kspace_labels: Tuple[str, ...]
@@ -24,55 +35,42 @@ class AxisSpec:
     kspace_fft_labels: Tuple[str, ...]
     coil_label: str
 
-    def __init__(self, *, image_labels=None, kspace_labels=None, image_fft_labels=None, kspace_fft_labels=None,
-                 coil_label=None, image=None, kspace=None, image_fft=None, kspace_fft=None, coil=None):
-        image_labels = image_labels if image_labels is not None else image
-        kspace_labels = kspace_labels if kspace_labels is not None else kspace
-        image_fft_labels = image_fft_labels if image_fft_labels is not None else image_fft
-        kspace_fft_labels = kspace_fft_labels if kspace_fft_labels is not None else kspace_fft
-        if coil_label is None:
-            coil_label = coil if coil is not None else "coil"
-        if image_labels is None or kspace_labels is None or image_fft_labels is None:
-            raise TypeError("AxisSpec requires image(_labels)=..., kspace(_labels)=..., image_fft(_labels)=...")
-        if kspace_fft_labels is None:
-            kspace_fft_labels = ("K",)
-        object.__setattr__(self, "image_labels", tuple(image_labels))
-        object.__setattr__(self, "kspace_labels", tuple(kspace_labels))
-        object.__setattr__(self, "image_fft_labels", tuple(image_fft_labels))
-        object.__setattr__(self, "kspace_fft_labels", tuple(kspace_fft_labels))
-        object.__setattr__(self, "coil_label", str(coil_label))
+    def __init__(self, **names):
+        legacy_of = dict(_FIELDS)
+        known = set(legacy_of) | set(legacy_of.values())
+        unknown = sorted(set(names) - known)
+        if unknown:
+            raise TypeError(f"AxisSpec got unexpected keyword(s) {unknown}")
+        for field, legacy in _FIELDS:
+            v = names.get(field)
+            if v is None:
+                v = names.get(legacy)
+            if v is None:
+                v = _DEFAULTS.get(field)
+            if v is None:
+                raise TypeError(f"AxisSpec needs {field}= (or {legacy}=); the image, k-space and image FFT "
+                                f"labels have no default")
+            object.__setattr__(self, field, str(v) if field == "coil_label" else tuple(v))
 
-    @property
-    def image(self):
-        return self.image_labels
-
-    @property
-    def kspace(self):
-        return self.kspace_labels
-
-    @property
-    def image_fft(self):
-        return self.image_fft_labels
-
-    @property
-    def kspace_fft(self):
-        return self.kspace_fft_labels
-
-    @property
-    def coil(self):
-        return self.coil_label
+    image = property(lambda self: self.image_labels)
+    kspace = property(lambda self: self.kspace_labels)
+    image_fft = property(lambda self: self.image_fft_labels)
+    kspace_fft = property(lambda self: self.kspace_fft_labels)
+    coil = property(lambda self: self.coil_label)
 
 
-def _prod(seq: Sequence[int]) -> int:
-    return int(reduce(operator.mul, seq, 1))
+def _like(labels: Sequence[str], fft: Sequence[str], coil: str) -> Tuple[str, ...]:
+    """Labels that are neither the batch 'B', the coil label nor an FFT label."""
+    skip = set(fft) | {"B", coil}
+    return tuple(l for l in labels if l not in skip)
 
 
 def like_labels_image(axis: AxisSpec) -> Tuple[str, ...]:
-    return tuple(l for l in axis.image if l not in axis.image_fft and l != "B" and l != axis.coil)
+    return _like(axis.image, axis.image_fft, axis.coil)
 
 
 def like_labels_kspace(axis: AxisSpec) -> Tuple[str, ...]:
-    return tuple(l for l in axis.kspace if l not in axis.kspace_fft and l not in ("B", axis.coil))
+    return _like(axis.kspace, axis.kspace_fft, axis.coil)
 
 
 @dataclass(frozen=True)
@@ -96,63 +94,67 @@ class KspaceLayoutPlan:
     K: int
 
 
+def _sizes_by_label(t: torch.Tensor, labels: Sequence[str], what: str) -> Dict[str, int]:
+    if t.ndim != len(labels):
+        raise ValueError(f"{what} tensor of shape {tuple(t.shape)} does not match the {len(labels)} labels "
+                         f"{tuple(labels)}")
+    return {l: int(n) for l, n in zip(labels, t.shape)}
+
+
 def plan_image_layout(x_user: torch.Tensor, axis: AxisSpec) -> ImageLayoutPlan:
-    if x_user.ndim != len(axis.image):
-        raise ValueError(f"image tensor has {x_user.ndim} dims but the axis spec names {len(axis.image)}")
-    sizes = {l: int(x_user.shape[i]) for i, l in enumerate(axis.image)}
-    if axis.coil in sizes and sizes[axis.coil] != 1:
-        raise ValueError("Image is expected coil-combined; axis.coil dim must be size 1 if present.")
-    ll = like_labels_image(axis)
-    ls = tuple(sizes[l] for l in ll)
-    return ImageLayoutPlan(axis, sizes.get("B", 1), ll, ls, _prod(ls) if ll else 1,
-                           tuple(sizes[l] for l in axis.image_fft))
+    size = _sizes_by_label(x_user, axis.image, "image")
+    ncoil = size.get(axis.coil, 1)
+    if ncoil != 1:
+        raise ValueError(f"images are coil-combined: axis {axis.coil!r} has size {ncoil} instead of 1")
+    like = like_labels_image(axis)
+    ls = tuple(size[l] for l in like)
+    return ImageLayoutPlan(axis, size.get("B", 1), like, ls, math.prod(ls), tuple(size[l] for l in axis.image_fft))
 
 
 def plan_kspace_layout(y_user: torch.Tensor, axis: AxisSpec) -> KspaceLayoutPlan:
-    if y_user.ndim != len(axis.kspace):
-        raise ValueError(f"k-space tensor has {y_user.ndim} dims but the axis spec names {len(axis.kspace)}")
-    sizes = {l: int(y_user.shape[i]) for i, l in enumerate(axis.kspace)}
-    ll = like_labels_kspace(axis)
-    ls = tuple(sizes[l] for l in ll)
-    return KspaceLayoutPlan(axis, sizes.get("B", 1), ll, ls, _prod(ls) if ll else 1, sizes[axis.coil],
-                            sizes[axis.kspace_fft[0]])
+    size = _sizes_by_label(y_user, axis.kspace, "k-space")
+    like = like_labels_kspace(axis)
+    ls = tuple(size[l] for l in like)
+    return KspaceLayoutPlan(axis, size.get("B", 1), like, ls, math.prod(ls), size[axis.coil],
+                            size[axis.kspace_fft[0]])
 
 
-def _like_from_sizes(like_labels, L_sizes):
-    if len(like_labels) == 0:
-        return tuple(), 1
-    if len(L_sizes) == len(like_labels):
-        ls = tuple(int(v) for v in L_sizes)
-        return ls, _prod(ls)
+def _like_sizes(like: Tuple[str, ...], L_sizes: Sequence[int]) -> Tuple[Tuple[int, ...], int]:
+    """Sizes of the like labels from bare sizes: none, one per label, or a single
+    product that goes to the first label (the others get 1)."""
+    L_sizes = [int(v) for v in L_sizes]
+    if not like:
+        return (), 1
+    if len(L_sizes) == len(like):
+        return tuple(L_sizes), math.prod(L_sizes)
     if len(L_sizes) == 1:
-        pad = [1] * len(like_labels)
-        pad[0] = int(L_sizes[0])
-        return tuple(pad), int(L_sizes[0])
-    raise ValueError("L_sizes length must be 0, 1, or match number of like labels.")
+        return (L_sizes[0],) + (1,) * (len(like) - 1), L_sizes[0]
+    raise ValueError(f"{len(L_sizes)} like sizes given for the like labels {like}: give none, one, "
+                     f"or {len(like)}")
 
 
 def plan_image_layout_from_sizes(B, L_sizes, spatial, axis: AxisSpec) -> ImageLayoutPlan:
-    ll = like_labels_image(axis)
-    ls, L = _like_from_sizes(ll, L_sizes)
-    return ImageLayoutPlan(axis, int(B), ll, ls, int(L), tuple(int(s) for s in spatial))
+    like = like_labels_image(axis)
+    ls, L = _like_sizes(like, L_sizes)
+    return ImageLayoutPlan(axis, int(B), like, ls, L, tuple(int(s) for s in spatial))
 
 
 def plan_kspace_layout_from_sizes(B, L_sizes, C, K, axis: AxisSpec) -> KspaceLayoutPlan:
-    ll = like_labels_kspace(axis)
-    ls, L = _like_from_sizes(ll, L_sizes)
-    return KspaceLayoutPlan(axis, int(B), ll, ls, int(L), int(C), int(K))
+    like = like_labels_kspace(axis)
+    ls, L = _like_sizes(like, L_sizes)
+    return KspaceLayoutPlan(axis, int(B), like, ls, L, int(C), int(K))
 
 
 def user_kspace_shape(axis: AxisSpec, B, L_sizes, C, K) -> Tuple[int, ...]:
     plan = plan_kspace_layout_from_sizes(B, L_sizes, C, K, axis)
-    size: Dict[str, int] = {"B": plan.B, axis.coil: plan.C, axis.kspace_fft[0]: plan.K}
-    size.update({l: int(s) for l, s in zip(plan.like_labels, plan.like_sizes)})
+    size = dict(zip(plan.like_labels, plan.like_sizes))
+    size.update({"B": plan.B, axis.coil: plan.C, axis.kspace_fft[0]: plan.K})
     return tuple(int(size[l]) for l in axis.kspace)
 
 
 def user_image_shape(axis: AxisSpec, B, L_sizes, spatial) -> Tuple[int, ...]:
     plan = plan_image_layout_from_sizes(B, L_sizes, spatial, axis)
-    size: Dict[str, int] = {"B": plan.B, axis.coil: 1}
-    size.update({l: int(s) for l, s in zip(plan.like_labels, plan.like_sizes)})
-    size.update({l: int(spatial[i]) for i, l in enumerate(axis.image_fft)})
+    size = dict(zip(plan.like_labels, plan.like_sizes))
+    size.update(zip(axis.image_fft, plan.spatial))
+    size.update({"B": plan.B, axis.coil: 1})
     return tuple(int(size[l]) for l in axis.image)

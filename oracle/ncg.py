@@ -54,6 +54,11 @@ class NCGConfig:
     tol_g: float = 1e-4
     tol_step: float = 1e-9
     restart: bool = False   # not in the reference: non-descent direction -> -g/D
+    # not in the reference: windowed relative objective change on the accepted
+    # objectives fa = [f(x_0), f(x_1), ...]: stop after iteration k when
+    # fa[k+1-W] - fa[k+1] <= W * stop_tol * |fa[k+1]| (W = stop_window > 0)
+    stop_window: int = 0
+    stop_tol: float = 1e-4
 
 
 def _rdot(a, b):
@@ -197,8 +202,11 @@ class NCGOracle:
         return beta
 
     # --- driver ----------------------------------------------------------------
-    def run(self, max_iter: Optional[int] = None, stop: Optional[Callable[[List[float]], bool]] = None):
+    def run(self, max_iter: Optional[int] = None, stop: Optional[Callable[[List[float]], bool]] = None,
+            log: Optional[Callable[[int, float], None]] = None):
         c = self.cfg
+        self.stop_reason = "max_iter"
+        fa: List[float] = []
         max_iter = int(max_iter or c.max_iter)
         self.begin_linesearch()
         self.f_g(0.0)
@@ -208,6 +216,7 @@ class NCGOracle:
         for k in range(max_iter):
             ok, t, f_t, g_t = ls()
             if not ok:
+                self.stop_reason = "line search failed"
                 break
             self.x = self.x + self.d * t
             xn = math.sqrt(max(float(_rdot(self.x, self.x)), 0.0))
@@ -216,13 +225,24 @@ class NCGOracle:
             for kk, v in (("xnorm", xn), ("stepnorm", sn), ("gnorm", gn)):
                 self._cum[kk] += v
             f0, g0d = self._ls0
+            if not fa:
+                fa.append(f0)
+            fa.append(f_t)
             self.hist.append(dict(iter=k, f=f0, gdot=g0d, gdot_at_step=g_t, step=t,
                                   xnorm=self._cum["xnorm"], gnorm=self._cum["gnorm"],
                                   stepnorm=self._cum["stepnorm"],
-                                  xnorm_iter=xn, gnorm_iter=gn, stepnorm_iter=sn))
+                                  xnorm_iter=xn, gnorm_iter=gn, stepnorm_iter=sn, f_accepted=f_t))
+            if log is not None:
+                log(k, f_t)
             if gn <= (1.0 + xn) * c.tol_g and sn <= (1.0 + xn) * c.tol_step:
+                self.stop_reason = "converged"
+                break
+            W = c.stop_window
+            if W > 0 and len(fa) - 1 >= W and fa[-1 - W] - fa[-1] <= W * c.stop_tol * abs(fa[-1]):
+                self.stop_reason = "relative objective change"
                 break
             if stop is not None and stop([h["f"] for h in self.hist]):
+                self.stop_reason = "callback"
                 break
             self.dir_update()
         return self
