@@ -525,6 +525,71 @@ def evaluate(cnn: "WarmStartCNN", workload: str = "grasp", device="cuda", reps: 
             "adjoint_start_err_vs_plain": rel(x_adj, x_plain), **info}
 
 
+def tolerance_study(cnn: "WarmStartCNN", tols=(1e-4, 3e-5, 1e-5, 3e-6, 1e-6), star_tol: float = 1e-8,
+                    star_max_iter: int = 12000, workload: str = "grasp", device="cuda") -> dict:
+    """How close the warm-started and the plain solve land at each windowed
+    tolerance, measured against a tightly converged minimiser x*.
+
+    x* is plain NCG from x = 0 run to the windowed tolerance `star_tol` (or its
+    first line-search failure, or `star_max_iter` iterations).  For every tol in
+    `tols`, both solves run to that tolerance on the same GPU (device seconds of
+    one solve after an untimed one that captures the graphs); each row reports
+    their times, iterations, the image difference of the two results
+    (rel-L2 against the plain one) and each result's rel-L2 distance to x*.
+    `first_tol_within_1e-3` is the loosest tolerance at which the two results
+    differ by at most 1e-3."""
+    from .solver import CGSolver
+    from .workloads import WORKLOADS, build, regs, solver_cfg
+    w = WORKLOADS[workload]
+    dev = torch.device(device)
+    op, y, x_true, _, _ = build(w, dev)
+    regm = regs(w)
+    rel = lambda u, v: float(torch.linalg.vector_norm(u - v) / torch.linalg.vector_norm(v))
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def solver_at(tol, max_iter):
+        cfg = solver_cfg(max_iter)
+        cfg.stop_tol = tol
+        return CGSolver(y, op, regm, cfg)
+
+    def timed(fn):
+        fn()                                   # graph capture, allocations
+        a, b = ev(), ev()
+        torch.cuda.synchronize()
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / 1e3
+
+    star = solver_at(star_tol, star_max_iter)
+    t_star = timed(lambda: star.reset().run())
+    x_star = star.result().clone()
+    out = {"workload": w["name"], "x_star": {"stop_tol": star_tol, "iters": star.iter, "stop": star.stop_reason,
+                                              "objective": star.objective(), "s": t_star,
+                                              "err_vs_truth": rel(x_star, x_true.to(dev).reshape(x_star.shape))},
+           "rows": []}
+    del star
+    for tol in tols:
+        s = solver_at(tol, star_max_iter)
+        t_plain = timed(lambda: s.reset().run())
+        it_plain, x_plain, f_plain = s.iter, s.result().clone(), s.objective()
+
+        def warm():
+            warm_start(s, cnn)
+            s.run()
+        t_warm = timed(warm)
+        x_warm = s.result()
+        out["rows"].append({"stop_tol": tol, "plain_s": t_plain, "plain_iters": it_plain, "warm_s": t_warm,
+                            "warm_iters": s.iter, "f_plain": f_plain, "f_warm": s.objective(),
+                            "err_vs_plain": rel(x_warm, x_plain), "plain_err_vs_star": rel(x_plain, x_star),
+                            "warm_err_vs_star": rel(x_warm, x_star)})
+        del s
+    ok = [r for r in out["rows"] if r["err_vs_plain"] <= 1e-3]
+    out["first_tol_within_1e-3"] = ok[0]["stop_tol"] if ok else None
+    return out
+
+
 def main(argv=None):
     """Generate training pairs, train, save:  python -m mrirecon_b200.warmstart --out w.npz
     Evaluate saved weights on the GRASP workload:  python -m mrirecon_b200.warmstart --eval w.npz"""

@@ -1,12 +1,15 @@
 """Generate the golden fixtures in this folder from the reference itself.
 
-Run in a container where the reference package is importable (its path is the
-first argument, default /root/reference).  The reference is pure Python; it is
+Run where the reference package is importable: its path is the first argument
+or, without one, the environment variable MRB_REFERENCE_PATH (there is no
+default).  The reference is pure Python; it is
 imported with two environment workarounds that change no arithmetic:
 ``DeviceArena`` is created without pinned host memory (no CUDA driver) and
 TorchDynamo is disabled (no Inductor toolchain).
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference [fixture ...]
+
+(fixture names: ptnufft_idx nudft_a tv ncg_small ncg_radial128; all by default)
 
 Writes:
   ptnufft_idx.npz  PTNUFFTAdapter.prepare index tables (the reference's literal
@@ -15,6 +18,10 @@ Writes:
   tv.npz           TVND energy/gradient (iso, aniso, axis weights, temporal)
   ncg_small.npz    CGSolver histories and iterates on a small 2D+t problem,
                    driven by the oracle's KB operator (oracle.kb.KBNufft)
+  ncg_radial128.npz  CGSolver (FR, Armijo) for 20 iterations on the 128x128,
+                   8-coil, 64-spoke x 256-sample golden-angle workload with
+                   spatial TV 1e-3, driven by the same KB operator: data,
+                   history and final image
 """
 from __future__ import annotations
 
@@ -135,15 +142,12 @@ def ncg_problem():
     return maps, traj, xt, noise
 
 
-def make_ncg():
+def kb_operator(maps, traj):
+    """The oracle's FP32 KB operator (ortho) with the operator surface the
+    reference CGSolver consumes, and Roles(1, 1, 2) for (B, 1, X, Y) images."""
     sys.path.insert(0, REPO)
     from oracle.kb import KBNufft
     from graspcg.core.roles import Roles
-    from graspcg.solvers.cg import CGSolver, CGConfig
-    from graspcg.regularization.manager import RegManager
-    from graspcg.regularization.tv_nd import TVND, TVParams
-
-    maps, traj, xt, noise = ncg_problem()
     kb = KBNufft(maps, traj, None, dtype=torch.complex64, norm="ortho")
 
     class Op:
@@ -161,7 +165,19 @@ def make_ncg():
             r = kb.AH(y).to(y.dtype)
             return r if out is None else out.copy_(r)
 
-    op = Op()
+    return Op()
+
+
+HIST_KEYS = ("f", "gdot", "gdot_at_step", "step", "xnorm", "gnorm", "stepnorm")
+
+
+def make_ncg():
+    from graspcg.solvers.cg import CGSolver, CGConfig
+    from graspcg.regularization.manager import RegManager
+    from graspcg.regularization.tv_nd import TVND, TVParams
+
+    maps, traj, xt, noise = ncg_problem()
+    op = kb_operator(maps, traj)
     y = op.A(xt) + 0.01 * noise
     out = dict(maps=maps.numpy(), traj=traj.numpy(), xt=xt.numpy(), y=y.numpy())
     runs = {
@@ -170,7 +186,7 @@ def make_ncg():
         "dy_armijo": dict(direction="dy", ls_name="armijo", max_iter=8),
         "fr_wolfe": dict(direction="fr", ls_name="wolfe", max_iter=6),
     }
-    keys = ("f", "gdot", "gdot_at_step", "step", "xnorm", "gnorm", "stepnorm")
+    keys = HIST_KEYS
     for name, kw in runs.items():
         regm = RegManager([TVND("s", TVParams(weight=1e-3, eps=1e-3, axes=(2, 3))),
                            TVND("t", TVParams(weight=5e-3, eps=1e-3, axes="temporal"))],
@@ -185,14 +201,43 @@ def make_ncg():
     np.savez_compressed(os.path.join(HERE, "ncg_small.npz"), **out)
 
 
+def make_ncg_radial128():
+    """The reference CGSolver on the single-frame 128x128 golden-angle workload
+    (8 coils, 64 spokes x 256 samples, spatial TV 1e-3, no noise), 20 FR/Armijo
+    iterations from x = 0."""
+    sys.path.insert(0, REPO)
+    from mrirecon_b200.workloads import WORKLOADS, make_inputs
+    from graspcg.solvers.cg import CGSolver, CGConfig
+    from graspcg.regularization.manager import RegManager
+    from graspcg.regularization.tv_nd import TVND, TVParams
+    w = WORKLOADS["radial128"]
+    xt, maps, traj = make_inputs(w)
+    op = kb_operator(maps, traj)
+    y = op.A(xt)
+    regm = RegManager([TVND("s", TVParams(weight=w["lam_s"], eps=w["eps"], axes=(2, 3)))],
+                      compile_kernels=False)
+    s = CGSolver(y=y, nufft_op=op, regm=regm,
+                 cfg=CGConfig(devices="cpu", direction="fr", ls_name="armijo", max_iter=20, tol_g=0.0,
+                              tol_step=0.0))
+    s.run()
+    h = s.history()
+    out = dict(y=y.numpy(), x=s.result().numpy())
+    for k in HIST_KEYS:
+        out[k] = np.array([r[k] for r in h], dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, "ncg_radial128.npz"), **out)
+
+
+FIXTURES = {"ptnufft_idx": make_ptnufft_idx, "nudft_a": make_nudft, "tv": make_tv, "ncg_small": make_ncg,
+            "ncg_radial128": make_ncg_radial128}
+
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MRB_REFERENCE_PATH")
+    if not ref:
+        sys.exit("usage: make_golden.py /path/to/reference [fixture ...] (or set MRB_REFERENCE_PATH)")
     _import_reference(ref)
     torch.set_num_threads(max(1, os.cpu_count() or 1))
-    make_ptnufft_idx()
-    make_nudft()
-    make_tv()
-    make_ncg()
+    for name in (sys.argv[2:] or list(FIXTURES)):
+        FIXTURES[name]()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
