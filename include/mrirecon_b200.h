@@ -82,7 +82,10 @@ int mrb_plan_destroy(mrb_plan* plan);
  * key 6 = spread kernel: 1 one block per work item, all coils of a group
  *         sharing the staged samples (2D tile 16, 3D tile 8; other tiles fall
  *         back to 0; the 3D default), 0 one warp per work item and coil group
- *         (the 2D default),
+ *         (the 2D default; in 2D with coil groups of up to 16 the warp first
+ *         tabulates each staged sample's inside taps, then runs only those),
+ *         2 one warp per work item evaluating every tap per lane task (the
+ *         earlier 2D kernel); all give identical grids,
  * key 7 = grid mask (fused FFT mode): 1 (default) the adjoint spread keeps its
  *         own grid, zeroed once per trajectory and batch size, and stores only
  *         the cell pairs inside some sample's support (per-frame bitmaps built by
@@ -92,9 +95,13 @@ int mrb_plan_destroy(mrb_plan* plan);
  *         (1; set before set_points, which then builds the per-frame strip
  *         lists) or writes the grid for a separate interp pass (0, the
  *         default: 2% slower forward, but each kernel on its own); same samples,
- * key 5 = 3D forward interp on a coil-interleaved copy of the grid (1, the 3D
- *         default: a tiled transpose then 128-bit gathers of all coils of a
- *         cell; costs one more grid-sized buffer) or on the planar grid (0). */
+ * key 5 = forward interp on a coil-interleaved grid (1, the default) or on the
+ *         coil-planar grid (0).  3D: a copy of the grid (written by the x
+ *         column pass for 8/16/32 coils, else by a tiled transpose; one more
+ *         grid-sized buffer), then 128-bit gathers of all coils of a cell.
+ *         2D fused FFT mode: the forward column pass writes the plan's grid
+ *         itself as (cell, coil) (blocks of 4 columns x 4 coils) and the interp
+ *         gathers each cell's coils as one run; no extra buffer.  Same samples. */
 int mrb_plan_set_option(mrb_plan* plan, int key, int64_t value);
 
 /* Trajectory (dev, (B, nd, K) float32 radians in [-pi, pi)): float32 grid

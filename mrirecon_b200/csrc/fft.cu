@@ -387,6 +387,53 @@ __global__ void __launch_bounds__(COL_NT, G0 <= 320 ? 2 : 1) fwd_cols_il_kernel(
   fft_stages<G0, 0, IL_ROWS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
 }
 
+// forward column pass writing a coil-interleaved grid (2D, see fft.cuh): a
+// block transforms its COLS (column, coil) pairs as CJ consecutive columns of
+// CG consecutive coils of one frame, so that its band reads are runs of CJ
+// columns of a coil and its grid stores runs of CG coils of a cell (32 bytes
+// each for the usual CJ = CG = 4: whole sectors on both sides when C % 4 == 0).
+// Same transforms as fwd_cols_kernel: the grid values are identical, only
+// their order in memory differs.
+template <int G0>
+struct ColGroups {
+  static constexpr int COLS = cols_per_block(G0);
+  static constexpr int CG = COLS % 4 == 0 ? 4 : COLS % 2 == 0 ? 2 : 1;
+  static constexpr int CJ = COLS / CG;
+};
+
+template <int G0>
+__global__ void __launch_bounds__(COL_NT) fwd_cols_cg_kernel(const float2* __restrict__ Tb, float2* __restrict__ out,
+                                                             const float2* __restrict__ tw, Geo2 g) {
+  constexpr int COLS = ColGroups<G0>::COLS;
+  constexpr int CG = ColGroups<G0>::CG;
+  constexpr int CJ = ColGroups<G0>::CJ;
+  constexpr int LD = G0 | 1;
+  extern __shared__ float2 sm[];
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+  const int G1 = g.G1, C = g.C;
+  const int cblocks = (G1 + CJ - 1) / CJ;
+  const int cgroups = (C + CG - 1) / CG;
+  int blk = blockIdx.x;
+  const int cb = blk % cblocks;
+  blk /= cblocks;
+  const int cgi = blk % cgroups;
+  const int be = blk / cgroups;
+  const int k0 = cb * CJ, c0 = cgi * CG;
+  const float2* tb = Tb + ((long long)be * C + c0) * g.S0 * G1 + k0;          // (coil, band row, column)
+  float2* ob = out + (long long)be * g.gtot * C + (long long)k0 * C + c0;      // (cell, coil)
+  auto load0 = [&](int q, int n0) -> float2 {
+    const int j = q % CJ, cc = q / CJ;
+    const int r = n0 - g.off0;
+    if ((unsigned)r >= (unsigned)g.S0 || k0 + j >= G1 || c0 + cc >= C) return make_float2(0.f, 0.f);
+    return tb[((long long)cc * g.S0 + r) * G1 + j];
+  };
+  auto store = [&](int q, int n0, float2 v) {
+    const int j = q % CJ, cc = q / CJ;
+    if (k0 + j < G1 && c0 + cc < C) ob[((long long)n0 * G1 + j) * C + cc] = v;
+  };
+  fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
+}
+
 // forward column pass fused with the interp (see fft.cuh): COLS columns per
 // block, the first COLS - 3 owned by the block's strip, the last three its
 // halo; the column transforms end in shared memory, then the threads walk the
@@ -668,6 +715,21 @@ int launch_cols_il(const float2* in, float2* out, const float2* tw, const Geo2& 
 }
 
 template <int G0>
+int launch_cols_cg(const float2* in, float2* out, const float2* tw, const Geo2& g, int nb, cudaStream_t st) {
+  constexpr int COLS = ColGroups<G0>::COLS;
+  constexpr int CG = ColGroups<G0>::CG;
+  constexpr int CJ = ColGroups<G0>::CJ;
+  const size_t smem = (size_t)COLS * (G0 | 1) * sizeof(float2);
+  const long long blocks = (long long)nb * ((g.C + CG - 1) / CG) * ((g.G1 + CJ - 1) / CJ);
+  MRB_REQUIRE(blocks < (1LL << 31), "too many columns");
+  int rc;
+  if ((rc = set_smem((const void*)fwd_cols_cg_kernel<G0>, smem))) return rc;
+  fwd_cols_cg_kernel<G0><<<(unsigned)blocks, COL_NT, smem, st>>>(in, out, tw, g);
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+template <int G0>
 int launch_cols_interp(const float2* in, const float2* tw, const Geo2& g, int nb, const mrb::ColInterp& ci,
                        cudaStream_t st) {
   constexpr int COLS = cols_per_block(G0);
@@ -779,6 +841,19 @@ int fft2_columns_il(const float2* Tb, float2* out, const float2* tw0, int S0, in
       break;
   }
   return fail(MRB_EINVAL, "no interleaved column pass for length %d and %d coils", G0, C);
+}
+
+int fft2_columns_cg(const float2* Tb, float2* out, const float2* tw0, int S0, int S1, int G0, int G1, int C, int nb,
+                    const double* skip, cudaStream_t st) {
+  const Geo2 g = make_geo2(S0, S1, G0, G1, C, skip);
+  switch (G0) {
+#define MRB_CASE(n) \
+  case n: return launch_cols_cg<n>(Tb, out, tw0, g, nb, st);
+    MRB_FFT_LENGTHS(MRB_CASE)
+#undef MRB_CASE
+    default:
+      return fail(MRB_EINVAL, "no fused FFT for length %d", G0);
+  }
 }
 
 int interp_strip_width(int G0) {

@@ -95,7 +95,8 @@ struct mrb_plan {
   const float2* tw2p = nullptr;
   DevBuf rowfac;      // fused mode: signed deapodisation of each image row (S0, or S0*S1 in 3D)
   const double* skip = nullptr;   // device flag: operator kernels return when it is non-zero
-  int il = 0;         // 1: forward interp reads a coil-interleaved copy of the grid (3D, cuFFT mode)
+  int il = 0;         // 1: forward interp on a coil-interleaved grid (3D: a copy of the grid; 2D fused mode:
+                      // the forward column pass writes the grid itself as (cell, coil))
   DevBuf grid_il;     // (nb, gtot, C) float2, written by the transpose at the start of the interp stage
   DevBuf psf;         // Toeplitz transfer functions (B, G0, G1) float (mrb_plan_set_toeplitz)
   DevBuf ones;        // 2D: S0 signs (-1)^(r + G0/2 - S0/2), then S1 ones: the row passes without deapodisation
@@ -593,6 +594,94 @@ __global__ void __launch_bounds__(256) interp2p_kernel(InterpArgs a, Geo g, KBPo
   if (two) yo[g.K] = make_float2(r1 * s, m1 * s);
 }
 
+// 2D forward interp on the coil-interleaved grid (be, cell, coil) that the
+// coil-grouped forward column pass writes.  One thread per (sample, coil pair)
+// with the P pairs of a sample on adjacent threads, so that each tap's C coils
+// are read as one contiguous run (C = 12: 96 bytes per cell, whole sectors)
+// with 128-bit loads when C is even; on the coil-planar grid every 4-cell tap
+// row of a coil is a 32-byte piece that straddles two sectors three times in
+// four.  A block covers S = 256 / P consecutive samples; the results go
+// through shared memory so that each coil's samples are stored as one run.
+// Taps, weights and summation order are those of interp2p_kernel: identical
+// samples.
+template <bool V4>
+__global__ void __launch_bounds__(256) interp2_il_kernel(InterpArgs a, Geo g, KBPoly kb) {
+  constexpr int W = 4;
+  __shared__ float2 ys[512];   // [coil][sample]: C * S <= 2 * P * S <= 512
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+  const int C = g.C;
+  const int P = (C + 1) >> 1;
+  const int S = 256 / P;
+  const long long k0 = (long long)blockIdx.x * S;
+  const int be = blockIdx.y;
+  const int b = frame_of(be, a.nb, g.B);
+  const int ks = threadIdx.x / P, pr = threadIdx.x - ks * P;
+  const long long k = k0 + ks;
+  if (ks < S && k < g.K) {
+    float w[2][W];
+    int nidx[2][W];
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+      const float x = a.gx[((long long)b * 2 + d) * g.K + k];
+      const int base = (int)floorf(x);
+      const float fx = x - (float)base;
+#pragma unroll
+      for (int o = 0; o < W; ++o) {
+        const int n = base - (W / 2 - 1) + o;
+        const float wd = mrb::kb_tap(kb, o, fx);
+        w[d][o] = (n & 1) ? -wd : wd;
+        nidx[d][o] = mrb::wrap_i(n, g.G[d]);
+      }
+    }
+    float s = a.scale * a.gsign;
+    if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
+    const int c = 2 * pr;
+    const bool two = c + 1 < C;
+    const float2* gb = a.grid + (long long)be * g.gtot * C + c;
+    float4 v[W][W];
+#pragma unroll
+    for (int i0 = 0; i0 < W; ++i0) {
+      const long long roff = (long long)nidx[0][i0] * g.G[1];
+#pragma unroll
+      for (int i1 = 0; i1 < W; ++i1) {
+        const float2* q = gb + (roff + nidx[1][i1]) * C;
+        if (V4) {
+          v[i0][i1] = __ldg(reinterpret_cast<const float4*>(q));
+        } else {
+          const float2 u0 = __ldg(q);
+          const float2 u1 = two ? __ldg(q + 1) : make_float2(0.f, 0.f);
+          v[i0][i1] = make_float4(u0.x, u0.y, u1.x, u1.y);
+        }
+      }
+    }
+    float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
+#pragma unroll
+    for (int i0 = 0; i0 < W; ++i0) {
+      float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
+#pragma unroll
+      for (int i1 = 0; i1 < W; ++i1) {
+        a0 = fmaf(w[1][i1], v[i0][i1].x, a0);
+        b0 = fmaf(w[1][i1], v[i0][i1].y, b0);
+        a1 = fmaf(w[1][i1], v[i0][i1].z, a1);
+        b1 = fmaf(w[1][i1], v[i0][i1].w, b1);
+      }
+      r0 = fmaf(w[0][i0], a0, r0);
+      m0 = fmaf(w[0][i0], b0, m0);
+      r1 = fmaf(w[0][i0], a1, r1);
+      m1 = fmaf(w[0][i0], b1, m1);
+    }
+    ys[c * S + ks] = make_float2(r0 * s, m0 * s);
+    if (two) ys[(c + 1) * S + ks] = make_float2(r1 * s, m1 * s);
+  }
+  __syncthreads();
+  const int ns = (int)min((long long)S, g.K - k0);
+  float2* yo = a.y + (long long)be * C * g.K + k0;
+  for (int e = threadIdx.x; e < C * S; e += blockDim.x) {
+    const int c = e / S, j = e - c * S;
+    if (j < ns) yo[(long long)c * g.K + j] = ys[c * S + j];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // 3D forward interp on a coil-interleaved grid.  The dense cuFFT leaves the
 // oversampled grid planar, (be, coil, cell); a 64-tap gather from it touches
@@ -1013,6 +1102,241 @@ __global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a,
       } else if (ok) {
         *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = v;
       }
+    }
+  }
+}
+
+// 2D per-warp spread with per-sample tap tables.  Ownership, sample order and
+// arithmetic are those of spread_kernel<2, T> (identical grids); what moves is
+// the per-tap work.  While a batch is staged, lane j computes sample j's taps
+// that fall inside the tile once (wrapped node, cell offset, weight product)
+// and stores them compacted, so that the per-sample loop runs over the inside
+// taps x coil pairs only and a lane task is two table reads and one 128-bit
+// shared read-modify-write; (tap, coil pair) of a lane per round is fixed for
+// the work item.  A listing of a sample whose support straddles tiles holds
+// fewer than 16 inside taps.  The tile's touched-cell bitmap rows are read
+// once per work item.  Coil groups of up to 16 coils (8 pairs).
+constexpr int SW2_MAXR = 4;   // rounds of 32 lane tasks per sample: 16 taps x 8 pairs
+
+template <int T>
+struct Spread2wSmem {
+  static constexpr int CELLS = T * T;
+  __host__ __device__ static int cstride(int cpi) { return (cpi + 1) & ~1; }
+  // acc [cell][coil] | tap cells (short) | tap weights | tap counts | bitmap rows | staged coil values
+  __host__ __device__ static size_t acc_bytes(int cpi) { return (size_t)cstride(cpi) * CELLS * sizeof(float2); }
+  static constexpr size_t TAB = SPREAD_BATCH * 16 * (sizeof(short) + sizeof(float)) + SPREAD_BATCH * sizeof(int) +
+                                ((T * sizeof(unsigned) + 15) & ~(size_t)15);
+  __host__ __device__ static size_t warp_bytes(int cpi) {
+    return acc_bytes(cpi) + TAB + (size_t)SPREAD_BATCH * cstride(cpi) * sizeof(float2);
+  }
+};
+
+template <int T>
+__global__ void __launch_bounds__(SPREAD_WARPS * 32) spread2w_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+  using SM = Spread2wSmem<T>;
+  constexpr int CELLS = SM::CELLS;
+  constexpr int PAIRS = CELLS / 2;
+  extern __shared__ float4 smem4[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long item = (long long)blockIdx.x * SPREAD_WARPS + warp;
+  const long long reps = g.B == 1 ? a.nb : a.nb / g.B;
+  const long long nitems = reps * a.n_items * a.ngroups;
+  if (item >= nitems) return;
+  const int grp = (int)(item % a.ngroups);
+  const long long oi = item / a.ngroups;
+  const int4 it = a.items[oi % a.n_items];
+  const int rep = (int)(oi / a.n_items);
+  const int okey = it.x;
+  const int b = okey / tg.ntiles;
+  const int tile = okey - b * tg.ntiles;
+  const int be = (g.B == 1) ? rep : b * (a.nb / g.B) + rep;
+  const int c0 = grp * a.cpi;
+  const int nc = min(a.cpi, g.C - c0);
+  const int o0 = (tile / tg.nt[1]) * T, o1 = (tile % tg.nt[1]) * T;
+  const int k0 = a.tile_start[okey], k1 = a.tile_start[okey + 1];
+  const int e0 = min(k1, k0 + it.y * a.chunk), e1 = min(k1, e0 + a.chunk);
+  float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
+  const int G0 = g.G[0], G1 = g.G[1];
+  float2* pout = it.z >= 0 ? a.partials + (((long long)rep * a.n_slots + it.z) * g.C + c0) * CELLS : nullptr;
+
+  if (e0 == e1 && !pout) {   // no sample touches this tile: zeros
+    if (a.touch) return;     // its cells are outside every support and never read
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = lane; i < nc * PAIRS; i += 32) {
+      const int cl = i / PAIRS, r = i - cl * PAIRS;
+      const int n0 = o0 + r / (T / 2), n1 = o1 + (r % (T / 2)) * 2;
+      if (n0 < G0 && n1 < G1) *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + (long long)n0 * G1 + n1) = z4;
+    }
+    return;
+  }
+
+  const int cps = SM::cstride(a.cpi);
+  const int npair = cps >> 1;
+  char* wbase = reinterpret_cast<char*>(smem4) + (size_t)warp * SM::warp_bytes(a.cpi);
+  float2* acc = reinterpret_cast<float2*>(wbase);
+  short* tcell = reinterpret_cast<short*>(wbase + SM::acc_bytes(a.cpi));
+  float* tw = reinterpret_cast<float*>(tcell + SPREAD_BATCH * 16);
+  int* tcnt = reinterpret_cast<int*>(tw + SPREAD_BATCH * 16);
+  unsigned* tbits = reinterpret_cast<unsigned*>(tcnt + SPREAD_BATCH);
+  float2* sy = reinterpret_cast<float2*>(wbase + SM::acc_bytes(a.cpi) + SM::TAB);
+
+  {
+    float4* acc4 = reinterpret_cast<float4*>(acc);
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = lane; i < cps * CELLS / 2; i += 32) acc4[i] = z4;
+  }
+  // the touched-cell bits of the tile's rows (bit l of row r = cell (o0 + r, o1 + l))
+  if (!pout && a.touch && lane < T) {
+    unsigned m = 0;
+    const int n0 = o0 + lane;
+    if (n0 < G0) {
+      const long long cell = (long long)n0 * G1 + o1;
+      const unsigned* tb = a.touch + (long long)b * a.twords;
+      const long long wi = cell >> 5;
+      const int sh = (int)(cell & 31);
+      unsigned long long v = __ldg(tb + wi);
+      if (sh + T > 32 && wi + 1 < a.twords) v |= (unsigned long long)__ldg(tb + wi + 1) << 32;
+      m = (unsigned)(v >> sh);
+    }
+    tbits[lane] = m;
+  }
+  // this lane's (tap, coil pair) in each round of a sample's tasks
+  int tap_r[SW2_MAXR], pr_r[SW2_MAXR];
+#pragma unroll
+  for (int r = 0; r < SW2_MAXR; ++r) {
+    tap_r[r] = (lane + 32 * r) / npair;
+    pr_r[r] = (lane + 32 * r) - tap_r[r] * npair;
+  }
+  __syncwarp();
+
+  const float* gxp = a.gx + (long long)b * 2 * g.K;
+  const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
+  // the next batch's sample index, coordinates, weight and first coil values
+  // are loaded into registers while the warp works on the current batch
+  constexpr int PF = 4;
+  int pk = 0;
+  float px[2], pwa = 1.f;
+  float2 py[PF];
+  auto fetch = [&](int e, int nbat) {
+    if (lane < nbat) {
+      pk = a.entries[e + lane];
+      px[0] = gxp[pk];
+      px[1] = gxp[g.K + pk];
+      if (a.wadj) pwa = a.wadj[(long long)b * g.K + pk];
+#pragma unroll
+      for (int cl = 0; cl < PF; ++cl) py[cl] = cl < nc ? yb[(long long)cl * g.K + pk] : make_float2(0.f, 0.f);
+    }
+  };
+  if (e0 < e1) fetch(e0, min(SPREAD_BATCH, e1 - e0));
+  for (int e = e0; e < e1; e += SPREAD_BATCH) {
+    const int nbat = min(SPREAD_BATCH, e1 - e);
+    if (lane < nbat) {
+      const int k = pk;
+      float ws = a.gsign;
+      if (a.wadj) ws *= pwa;
+      float wv[2][4];
+      int base[2];
+#pragma unroll
+      for (int d = 0; d < 2; ++d) {
+        const float x = px[d];
+        base[d] = (int)floorf(x) - 1;
+        const float fx = x - (float)(base[d] + 1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int n = base[d] + q;
+          float w = mrb::kb_tap(kb, q, fx);
+          if (n & 1) w = -w;
+          if (d == 0) w *= ws;
+          wv[d][q] = w;
+        }
+      }
+      short* tc = tcell + lane * 16;
+      float* tww = tw + lane * 16;
+      int m = 0;
+#pragma unroll
+      for (int ox = 0; ox < 4; ++ox) {
+        int n0 = base[0] + ox;
+        n0 += n0 < 0 ? G0 : 0;
+        n0 -= n0 >= G0 ? G0 : 0;
+        const int lx = n0 - o0;
+        if ((unsigned)lx < (unsigned)T) {
+#pragma unroll
+          for (int oy = 0; oy < 4; ++oy) {
+            int n1 = base[1] + oy;
+            n1 += n1 < 0 ? G1 : 0;
+            n1 -= n1 >= G1 ? G1 : 0;
+            const int ly = n1 - o1;
+            if ((unsigned)ly < (unsigned)T) {
+              tc[m] = (short)(lx * T + ly);
+              tww[m] = wv[0][ox] * wv[1][oy];
+              ++m;
+            }
+          }
+        }
+      }
+      tcnt[lane] = m;
+#pragma unroll
+      for (int cl = 0; cl < PF; ++cl)
+        if (cl < cps) sy[lane * cps + cl] = py[cl];
+      for (int cl = PF; cl < cps; ++cl)
+        sy[lane * cps + cl] = cl < nc ? yb[(long long)cl * g.K + k] : make_float2(0.f, 0.f);
+    }
+    __syncwarp();
+    if (e + SPREAD_BATCH < e1) fetch(e + SPREAD_BATCH, min(SPREAD_BATCH, e1 - e - SPREAD_BATCH));
+    for (int j = 0; j < nbat; ++j) {
+      const int nt = tcnt[j] * npair;
+      const short* tc = tcell + j * 16;
+      const float* twj = tw + j * 16;
+      const float4* yj = reinterpret_cast<const float4*>(sy + j * cps);
+#pragma unroll
+      for (int r = 0; r < SW2_MAXR; ++r) {
+        if (lane + 32 * r < nt) {
+          const int cell = tc[tap_r[r]];
+          const float w = twj[tap_r[r]];
+          const float4 v = yj[pr_r[r]];
+          float4* p = reinterpret_cast<float4*>(acc + cell * cps) + pr_r[r];
+          float4 t = *p;
+          t.x = fmaf(w, v.x, t.x);
+          t.y = fmaf(w, v.y, t.y);
+          t.z = fmaf(w, v.z, t.z);
+          t.w = fmaf(w, v.w, t.w);
+          *p = t;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  // write the whole tile once (or this chunk's partial tile): lane task = (cell
+  // pair along the row, coil pair), coil pair fastest; two 128-bit shared loads,
+  // one 128-bit global store per coil
+  const int qd = 32 / npair, qr = 32 - qd * npair;
+  int pr = lane % npair, r = lane / npair;
+  for (int i = lane; i < PAIRS * npair; i += 32) {
+    const int l = (r % (T / 2)) * 2;
+    const int rr = r / (T / 2);
+    const int cl0 = rr * T + l;
+    const float4 a0 = reinterpret_cast<const float4*>(acc + cl0 * cps)[pr];
+    const float4 a1 = reinterpret_cast<const float4*>(acc + (cl0 + 1) * cps)[pr];
+    const int n0 = o0 + rr, n1 = o1 + l;
+    const long long cell = (long long)n0 * G1 + n1;
+    const bool ok = n0 < G0 && n1 < G1 && (pout || !a.touch || ((tbits[rr] >> l) & 3u));
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int cl = 2 * pr + h;
+      if (cl >= nc) continue;
+      const float4 v = h == 0 ? make_float4(a0.x, a0.y, a1.x, a1.y) : make_float4(a0.z, a0.w, a1.z, a1.w);
+      if (pout) {
+        *reinterpret_cast<float4*>(pout + (long long)cl * CELLS + cl0) = v;
+      } else if (ok) {
+        *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = v;
+      }
+    }
+    pr += qr;
+    r += qd;
+    if (pr >= npair) {
+      pr -= npair;
+      ++r;
     }
   }
 }
@@ -1637,7 +1961,7 @@ extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int 
       rc = mrb::fail(MRB_ECUDA, "copying row deapodisation failed");
   }
   if (!rc && fused_supported(p)) rc = mrb_plan_set_option(p, 4, 1);
-  if (!rc && nd == 3) p->il = 1;
+  if (!rc) p->il = 1;
   if (rc) {
     delete p;
     return rc;
@@ -1696,7 +2020,8 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
       p->fft_mode = (int)value;
       return 0;
     case 6:
-      MRB_REQUIRE(value == 0 || value == 1, "spread kernel must be 0 (per-warp) or 1 (block per tile)");
+      MRB_REQUIRE(value >= 0 && value <= 2,
+                  "spread kernel must be 0 (per-warp), 1 (block per tile) or 2 (per-warp without tap tables)");
       p->spread_kernel = (int)value;
       return 0;
     case 8:
@@ -1711,7 +2036,6 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
       return 0;
     case 5:
       MRB_REQUIRE(value == 0 || value == 1, "interleaved interp must be 0 or 1");
-      MRB_REQUIRE(value == 0 || p->nd == 3, "the interleaved interp is 3D only");
       p->il = (int)value;
       return 0;
     default:
@@ -1999,7 +2323,7 @@ static int ensure_grid(mrb_plan* p, int nb, cudaStream_t st) {
     return 0;
   }
   if (p->fft_mode == 1) return p->band.ensure(mrb::fft2_tmp_bytes(p->S[0], p->G[1], p->C, nb));
-  if (p->il && (rc = p->grid_il.ensure(bytes))) return rc;
+  if (p->il && p->nd == 3 && (rc = p->grid_il.ensure(bytes))) return rc;
   return ensure_fft(p, nb);
 }
 
@@ -2012,6 +2336,12 @@ static bool il_direct(const mrb_plan* p) {
 // the forward column pass also interpolates (fused 2D mode with strip lists)
 static bool col_interp_active(const mrb_plan* p) {
   return p->fft_mode == 1 && p->nd == 2 && p->col_interp == 1 && p->nstrips > 0;
+}
+
+// fused 2D mode with the interleaved interp: the forward column pass writes the
+// grid as (cell, coil) and the interp gathers all coils of a cell at once
+static bool il2_active(const mrb_plan* p) {
+  return p->fft_mode == 1 && p->nd == 2 && p->il == 1 && p->C <= 512 && !col_interp_active(p);
 }
 
 // the spread writes only touched cell pairs into a grid of its own (fused FFT mode)
@@ -2101,6 +2431,9 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       return mrb::fft2_columns_interp(p->band.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0], p->G[1], p->C, nb,
                                       ci, p->skip, st);
     }
+    if (stage == 1 && il2_active(p))
+      return mrb::fft2_columns_cg(p->band.as<float2>(), p->grid.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
+                                  p->G[1], p->C, nb, p->skip, st);
     if (stage == 1)
       return mrb::fft2_columns(1, p->band.as<float2>(), p->grid.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
                                p->G[1], p->C, nb, p->skip, st);
@@ -2164,6 +2497,15 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       dim3 grid(grid_blocks(nt, 256), nb);
       if (p->C % 2 == 0) interp3_il_kernel<true><<<grid, 256, 0, st>>>(a, g, p->kb);
       else interp3_il_kernel<false><<<grid, 256, 0, st>>>(a, g, p->kb);
+      MRB_LAUNCH_CHECK();
+      return 0;
+    }
+    if (il2_active(p)) {
+      const int S = 256 / ((p->C + 1) / 2);
+      const long long nbx = (p->K + S - 1) / S;
+      MRB_REQUIRE(nbx < (1LL << 31) && nb <= 65535, "too many samples for the interp");
+      if (p->C % 2 == 0) interp2_il_kernel<true><<<dim3((unsigned)nbx, nb), 256, 0, st>>>(a, g, p->kb);
+      else interp2_il_kernel<false><<<dim3((unsigned)nbx, nb), 256, 0, st>>>(a, g, p->kb);
       MRB_LAUNCH_CHECK();
       return 0;
     }
@@ -2252,6 +2594,18 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
         smem = Spread2Smem<8>::BYTES;
       }
     }
+    // 2D per-warp work items: the tap-table kernel (coil groups of up to 16),
+    // or with option key 6 = 2 the kernel that evaluates every tap per lane task
+#define MRB_SPREAD2W_CASE(T_)                                                                 \
+  if (!fn && p->nd == 2 && tg.T == T_ && p->spread_kernel == 0 && a.cpi <= 16) {             \
+    fn = (const void*)spread2w_kernel<T_>;                                                   \
+    smem = SPREAD_WARPS * Spread2wSmem<T_>::warp_bytes(a.cpi);                               \
+  }
+    MRB_SPREAD2W_CASE(4)
+    MRB_SPREAD2W_CASE(8)
+    MRB_SPREAD2W_CASE(16)
+    MRB_SPREAD2W_CASE(32)
+#undef MRB_SPREAD2W_CASE
 #define MRB_SPREAD_CASE(ND_, T_)                                                             \
   if (!fn && p->nd == ND_ && tg.T == T_) {                                                   \
     fn = (const void*)spread_kernel<ND_, T_>;                                                \

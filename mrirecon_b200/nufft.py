@@ -194,7 +194,7 @@ class B200NUFFTAdapter:
     coils_per_item: Optional[int] = None
     chunk: Optional[int] = None
     fft_mode: Optional[int] = None
-    interleave: Optional[int] = None   # 3D: interp on a coil-interleaved grid copy (default 1)
+    interleave: Optional[int] = None   # interp on a coil-interleaved grid (default 1; 2D: fused FFT mode)
     spread_kernel: Optional[int] = None  # 1 block per tile (default), 0 warp per tile and coil group
     col_interp: Optional[int] = None     # 2D fused mode: interp inside the forward column pass (default 0)
     autotune: bool = False

@@ -389,6 +389,46 @@ def test_2d_pair_parallel_interp_identical(cuda, C, nb, B):
         assert torch.equal(ad.A(x), y1)
 
 
+@pytest.mark.parametrize("S,C,nb,B", [((40, 48), 12, 2, 2), ((40, 48), 5, 3, 1), ((32, 32), 1, 1, 1),
+                                      ((48, 40), 4, 4, 2), ((160, 320), 3, 1, 1)])
+def test_2d_interleaved_grid_interp_identical(cuda, S, C, nb, B):
+    """Fused 2D mode: the forward column pass writing the grid as (cell, coil)
+    (coil groups of 4 with a tail group, column groups with a tail at G0 = 640)
+    and the interleaved interp (option key 5, the default) give the samples of
+    the planar column pass and pair-parallel interp bit for bit."""
+    maps = _rand_c((C,) + S, 74, torch.complex64)
+    traj = phantoms.random_traj(B, 2, 1000, seed=75)
+    x = _rand_c((nb, 1) + S, 76, torch.complex64).to(cuda)
+    ad = _adapter(maps, traj)
+    assert ad.plan.info()["fft_mode"] == 1
+    y1 = ad.A(x)
+    ad.plan.set_option(5, 0)
+    assert torch.equal(ad.A(x), y1)
+    ad.plan.set_option(5, 1)
+    assert torch.equal(ad.A(x), y1)
+
+
+@pytest.mark.parametrize("tile,cpi,chunk,fft_mode,mask", [(16, 6, None, 1, 1), (16, 12, 16, 1, 1), (8, 4, None, 1, 0),
+                                                          (4, 3, 32, 1, 1), (32, 2, None, 1, 1), (16, 5, 64, 0, 1),
+                                                          (16, 16, None, 1, 1)])
+def test_2d_tap_table_spread_identical_to_earlier_kernel(cuda, tile, cpi, chunk, fft_mode, mask):
+    """The per-warp 2D spread that tabulates each staged sample's inside taps
+    (option key 6 = 0) gives the grid of the kernel that evaluates every tap per
+    lane task (key 6 = 2) bit for bit: tiles 4 .. 32, odd coil groups, split
+    tiles, the masked write-out and the dense FFT mode."""
+    C = 12
+    maps = _rand_c((C, 48, 40), 53, torch.complex64)
+    traj = phantoms.grasp_trajectory(2, 11, 96)
+    y = _rand_c((2, C, traj.shape[-1]), 54, torch.complex64).to(cuda)
+    ad = _adapter(maps, traj, tile=tile, chunk=chunk, coils_per_item=cpi, fft_mode=fft_mode)
+    ad.plan.set_option(7, mask)
+    x0 = ad.AH(y)
+    ad.plan.set_option(6, 2)
+    assert torch.equal(ad.AH(y), x0)
+    ad.plan.set_option(6, 0)
+    assert torch.equal(ad.AH(y), x0)
+
+
 @pytest.mark.parametrize("S,C,nb,B", [((16, 20, 24), 3, 2, 1), ((24, 16, 32), 4, 2, 2), ((20, 20, 20), 1, 1, 1),
                                       ((16, 20, 24), 16, 2, 2), ((20, 16, 24), 8, 1, 1)])
 def test_fused_fft_3d_matches_cufft(cuda, S, C, nb, B):
