@@ -382,6 +382,20 @@ int mrb_cnn_conv3d_fwd(const void* x, int cx, int ci_off, int cin, const void* w
 int mrb_cnn_conv3d_wgrad(const void* x, int cx, int ci_off, int cin, const void* gz, int cg, int cg_off,
                          int coutp, float* dw, float* dbias, float* part, int64_t part_floats,
                          const int* vol, mrb_stream_t stream);
+/* The same weight and bias gradient on the 5th-generation tensor cores
+ * (tcgen05.mma, FP32 accumulators in tensor memory): x and gz are first
+ * repacked channels-first into `scratch` (x as three copies shifted by -1, 0, +1
+ * voxel along W, so that every TMA box starts at a W coordinate that is a
+ * multiple of 32), then each CTA accumulates a group of taps over a range of
+ * 32-voxel K steps; partial sums (also in `scratch`) are added in a fixed
+ * order.  Needs cin and coutp multiples of 16, the smaller of them <= 256,
+ * coutp dividing 256 and W a multiple of 64 (mrb_cnn_wgrad_tc_scratch_bytes
+ * fails otherwise); scratch: 256-byte aligned, of the size that function
+ * returns for (cin, coutp, vol). */
+int mrb_cnn_wgrad_tc_scratch_bytes(int cin, int coutp, const int* vol, int64_t* bytes);
+int mrb_cnn_conv3d_wgrad_tc(const void* x, int cx, int ci_off, int cin, const void* gz, int cg, int cg_off,
+                            int coutp, float* dw, float* dbias, void* scratch, int64_t scratch_bytes,
+                            const int* vol, mrb_stream_t stream);
 /* Spatially flipped, transposed weights [27][coutp][cinp] for the data gradient. */
 int mrb_cnn_flip_weights(const void* w, int cin, int coutp, void* wd, int cinp, mrb_stream_t stream);
 /* gz = g * (act > 0) over nch channels (BF16 out, padded to nchp). */

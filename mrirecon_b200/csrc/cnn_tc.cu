@@ -24,6 +24,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "mrb_common.cuh"
@@ -280,6 +281,286 @@ __global__ void __launch_bounds__(TC_THREADS) conv3d_tc_kernel(const __grid_cons
   }
 }
 
+// ---------------------------------------------------------------------------
+// Weight gradient on tcgen05: dW[tap][ci][co] = sum_v x[v + o(tap)][ci] gz[v][co]
+// (o(tap) the (dz, dy, dx) offset; out-of-volume x is zero), the
+// reduction over voxels as the GEMM's K.  Both operands must be K-major for
+// the MMA, i.e. voxels contiguous, so they are first repacked channels-first
+// (wg_pack_kernel): gz as gt (Nb, Mg, D, H, W) and x as xs (Nb, 3, Mx, D, H, W),
+// three copies shifted by dx = -1, 0, +1 along W.  A K step is 32 consecutive
+// voxels of one (n, d, h) row; the tap offset then moves only the H and D
+// coordinates of a TMA box (out-of-volume rows read as zero) and picks the dx
+// copy, so every box starts at a W coordinate that is a multiple of 32.
+// The operand with more channels is the MMA's M side (128 rows per tile,
+// channels padded with zeros in the packed copy), the other the N side
+// (16 .. 256).  With x on the M side (xm), A is per tap (shifted) and B once
+// per K step; otherwise A (gz) once per K step and B per tap.  A CTA owns a
+// group of TG taps (TG accumulators of N columns in TMEM), an M tile and a
+// range of K steps; its partial sums go to part[split][tap][ci][co] and are
+// added in a fixed split order (deterministic).
+// ---------------------------------------------------------------------------
+constexpr int WG_STAGES = 4;
+constexpr int WG_KV = 32;   // voxels per K step (one 64-byte swizzle row of BF16)
+
+struct WgArgs {
+  int xm;              // 1: x is the M operand (A per tap), 0: gz is (B per tap)
+  int N;               // columns: channels of the N operand (multiple of 16, <= 256)
+  int Mreal;           // real channels of the M operand
+  int cin, coutp;      // dW is [27][cin][coutp]
+  int TG;              // taps per group
+  int Nb, D, H, W;
+  long long ksteps;    // Nb * D * H * (W / 32)
+  long long kper;      // K steps per split
+  int ngroups, mtiles;
+  float* part;         // [split][27][cin][coutp]
+  int ncols;           // TMEM columns allocated
+  uint32_t shared_bytes, pertap_bytes;   // tile bytes (multiples of 1024)
+};
+
+__global__ void __launch_bounds__(TC_THREADS) wgrad_tc_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                              const __grid_constant__ CUtensorMap gmap, WgArgs a) {
+  extern __shared__ __align__(1024) uint8_t dsm[];
+  __shared__ __align__(8) uint64_t full_bar[WG_STAGES], empty_bar[WG_STAGES], done_bar;
+  __shared__ uint32_t tmem_base;
+  __shared__ volatile int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(dsm) + 1023) & ~uintptr_t(1023));
+  const uint32_t stage_bytes = a.shared_bytes + (uint32_t)a.TG * a.pertap_bytes;
+
+  // block -> (tap group, M tile, split)
+  long long bid = blockIdx.x;
+  const int grp = (int)(bid % a.ngroups);
+  bid /= a.ngroups;
+  const int mt = (int)(bid % a.mtiles);
+  const long long split = bid / a.mtiles;
+  const int tap0 = grp * a.TG;
+  const int ntap = min(a.TG, 27 - tap0);
+  const int m0 = mt * 128;
+  const long long kb0 = split * a.kper;
+  const long long kb1 = min(a.ksteps, kb0 + a.kper);
+  const int nk = (int)(kb1 - kb0);
+  const uint32_t a_tile = 128u * WG_KV * 2u, b_tile = (uint32_t)a.N * WG_KV * 2u;
+
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < WG_STAGES; ++st) {
+      mbar_init(&full_bar[st], 1);
+      mbar_init(&empty_bar[st], 1);
+    }
+    mbar_init(&done_bar, 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(a.ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem_d = tmem_base;
+  const int nwc = a.W / WG_KV;
+
+  if (warp == 0 && lane == 0) {
+    // producer: per K step the shared tile and one tile per tap of the group
+    for (int ks = 0; ks < nk; ++ks) {
+      const int st = ks % WG_STAGES;
+      if (ks >= WG_STAGES && !mbar_wait(&empty_bar[st], ((ks / WG_STAGES) - 1) & 1, &abort_flag)) break;
+      long long kv = kb0 + ks;
+      const int w0 = (int)(kv % nwc) * WG_KV;
+      kv /= nwc;
+      const int h = (int)(kv % a.H);
+      kv /= a.H;
+      const int d = (int)(kv % a.D);
+      const int n = (int)(kv / a.D);
+      uint8_t* sbase = base + (size_t)st * stage_bytes;
+      mbar_expect_tx(&full_bar[st], (a.xm ? b_tile : a_tile) + (uint32_t)ntap * (a.xm ? a_tile : b_tile));
+      // shared tile: the gz rows of this K step (M rows m0.. or all N rows)
+      tma_load_5d(sbase, &gmap, &full_bar[st], w0, h, d, a.xm ? 0 : m0, n);
+      for (int t = 0; t < ntap; ++t) {
+        const int tap = tap0 + t;
+        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+        tma_load_5d(sbase + a.shared_bytes + (size_t)t * a.pertap_bytes, &xmap, &full_bar[st], w0, h + dy, d + dz,
+                    a.xm ? m0 : 0, n * 3 + dx + 1);
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    const uint32_t idesc = f16_idesc(128, a.N);
+    for (int ks = 0; ks < nk; ++ks) {
+      const int st = ks % WG_STAGES;
+      if (!mbar_wait(&full_bar[st], (ks / WG_STAGES) & 1, &abort_flag)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t ssh = smem_u32(base + (size_t)st * stage_bytes);
+      for (int t = 0; t < ntap; ++t) {
+        const uint32_t stp = ssh + a.shared_bytes + (uint32_t)t * a.pertap_bytes;
+        const uint32_t sa = a.xm ? stp : ssh, sb = a.xm ? ssh : stp;
+#pragma unroll
+        for (int kk = 0; kk < WG_KV / 16; ++kk) {
+          const uint64_t adesc = sw64_desc(sa + kk * 32);
+          const uint64_t bdesc = sw64_desc(sb + kk * 32);
+          const uint32_t accum = (ks > 0 || kk > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d + (uint32_t)(t * a.N)),
+              "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+              : "memory");
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&empty_bar[st]))
+                   : "memory");
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(&done_bar))
+                 : "memory");
+  }
+  __syncwarp();
+
+  bool have = nk > 0 && mbar_wait(&done_bar, 0, &abort_flag) && !abort_flag;
+  have = __all_sync(0xffffffffu, have);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const int row = warp * 32 + lane;   // TMEM lane = channel m0 + row of the M operand
+  const int mch = m0 + row;
+  for (int t = 0; t < ntap; ++t) {
+    float* pt = a.part + ((size_t)split * 27 + tap0 + t) * (size_t)a.cin * a.coutp;
+    for (int c0 = 0; c0 < a.N; c0 += 16) {
+      uint32_t r[16];
+      if (have) {
+        const uint32_t taddr = tmem_d + ((uint32_t)(warp * 32) << 16) + (uint32_t)(t * a.N + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) r[j] = 0u;   // no K steps (or an aborted wait): a zero partial
+      }
+      if (mch >= a.Mreal) continue;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int nch = c0 + j;
+        const float v = __uint_as_float(r[j]);
+        if (a.xm) pt[(size_t)mch * a.coutp + nch] = v;   // (ci = m, co = n)
+        else pt[(size_t)nch * a.coutp + mch] = v;        // (ci = n, co = m)
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_d), "r"(a.ncols) : "memory");
+  }
+}
+
+// channels-first repack: out[n][copy][c][d][h][w] = src[n][d][h][w + shift][c_off + c]
+// (shift = copy - 1 with three copies, 0 with one; zero outside the volume and
+// for nch <= c < chp); a block moves a 32-channel x 64-voxel tile of one row
+constexpr int PK_W = 64;
+
+__global__ void __launch_bounds__(256) wg_pack_kernel(const bf16* __restrict__ src, int cs, int c_off, int nch,
+                                                      bf16* __restrict__ out, int chp, int ncopies, int D, int H,
+                                                      int W) {
+  __shared__ bf16 tile[32][PK_W + 3];
+  const int nwt = W / PK_W;
+  const int wt = blockIdx.x % nwt, ct = blockIdx.x / nwt;
+  const int h = blockIdx.y;
+  const int nd = blockIdx.z;
+  const int n = nd / D, d = nd - n * D;
+  const int w0 = wt * PK_W, c0 = ct * 32;
+  const long long row = ((long long)nd * H + h) * W;   // voxel index of (n, d, h, 0)
+  for (int e = threadIdx.x; e < (PK_W + 2) * 32; e += blockDim.x) {
+    const int wl = e >> 5, cl = e & 31;
+    const int w = w0 - 1 + wl, c = c0 + cl;
+    bf16 v = __float2bfloat16_rn(0.f);
+    if (w >= 0 && w < W && c < nch) v = src[(row + w) * cs + c_off + c];
+    tile[cl][wl] = v;
+  }
+  __syncthreads();
+  const long long plane = (long long)D * H * W;
+  for (int copy = 0; copy < ncopies; ++copy) {
+    const int shift = ncopies > 1 ? copy - 1 : 0;
+    bf16* ob = out + (((long long)n * ncopies + copy) * chp) * plane + ((long long)d * H + h) * W + w0;
+    for (int e = threadIdx.x; e < 32 * PK_W; e += blockDim.x) {
+      const int cl = e / PK_W, wl = e - cl * PK_W;
+      const int c = c0 + cl;
+      if (c < chp) ob[(long long)c * plane + wl] = tile[cl][wl + 1 + shift];
+    }
+  }
+}
+
+// dW[i] = sum over splits in order; dbias[co] likewise from per-split sums
+__global__ void wg_sum_kernel(const float* __restrict__ part, int nsplit, long long n, float* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float s = 0.f;
+  for (int k = 0; k < nsplit; ++k) s += part[(long long)k * n + i];
+  out[i] = s;
+}
+
+// per-split channel sums of gz (bias gradient): block = split, thread = (channel, lane of 8)
+__global__ void __launch_bounds__(256) wg_bias_kernel(const bf16* __restrict__ gz, int cg, int cg_off, int coutp,
+                                                      long long voxels, long long vper, float* __restrict__ bpart) {
+  __shared__ float red[256];
+  const long long v0 = (long long)blockIdx.x * vper, v1 = min(voxels, v0 + vper);
+  const int lanes = 256 / coutp;   // coutp <= 256, power of two multiple of 32 here
+  const int co = threadIdx.x % coutp, l = threadIdx.x / coutp;
+  float s = 0.f;
+  if (l < lanes)
+    for (long long v = v0 + l; v < v1; v += lanes) s += __bfloat162float(gz[v * cg + cg_off + co]);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x < coutp) {
+    float t = 0.f;
+    for (int k = 0; k < lanes; ++k) t += red[k * coutp + threadIdx.x];
+    bpart[(long long)blockIdx.x * coutp + threadIdx.x] = t;
+  }
+}
+
+struct WgPlan {
+  int xm, N, Mreal, Mpad, TG, ngroups, mtiles, nsplit;
+  long long ksteps, kper;
+  size_t xs_elems, gt_elems, part_floats;
+  uint32_t shared_bytes, pertap_bytes;
+};
+
+bool wg_plan(int cin, int coutp, int Nb, int D, int H, int W, WgPlan& p) {
+  if (cin <= 0 || coutp <= 0 || cin % 16 != 0 || coutp % 16 != 0 || W % PK_W != 0) return false;
+  p.xm = cin > coutp ? 1 : 0;
+  p.N = p.xm ? coutp : cin;
+  p.Mreal = p.xm ? cin : coutp;
+  if (p.N > 256) return false;
+  p.mtiles = (p.Mreal + 127) / 128;
+  p.Mpad = p.mtiles * 128;
+  const uint32_t a_tile = 128u * WG_KV * 2u, b_tile = (uint32_t)p.N * WG_KV * 2u;
+  auto r1k = [](uint32_t b) { return (b + 1023u) & ~1023u; };
+  p.shared_bytes = r1k(p.xm ? b_tile : a_tile);
+  p.pertap_bytes = r1k(p.xm ? a_tile : b_tile);
+  const uint32_t budget = 200u * 1024u / WG_STAGES;
+  int tg = (int)((budget - p.shared_bytes) / p.pertap_bytes);
+  tg = std::min(tg, 512 / p.N);
+  tg = std::min(tg, 27);
+  if (tg < 1) return false;
+  p.TG = tg;
+  p.ngroups = (27 + tg - 1) / tg;
+  p.ksteps = (long long)Nb * D * H * (W / WG_KV);
+  // about two CTAs per SM over the whole grid, at least 16 K steps per split
+  const long long ctas = (long long)p.ngroups * p.mtiles;
+  long long ns = std::max(1LL, (296 + ctas - 1) / ctas);
+  ns = std::min(ns, std::max(1LL, p.ksteps / 16));
+  p.kper = (p.ksteps + ns - 1) / ns;
+  p.nsplit = (int)((p.ksteps + p.kper - 1) / p.kper);
+  const long long vox = (long long)Nb * D * H * W;
+  p.xs_elems = (size_t)3 * (p.xm ? p.Mpad : cin) * vox;
+  p.gt_elems = (size_t)(p.xm ? coutp : p.Mpad) * vox;
+  p.part_floats = (size_t)p.nsplit * 27 * cin * coutp + (size_t)p.nsplit * coutp;
+  return true;
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -372,6 +653,115 @@ extern "C" int mrb_cnn_conv3d_tc(const void* x, int cx, int ci_off, int cin, con
   MRB_REQUIRE(tiles < (1LL << 31), "volume too large");
   conv3d_tc_kernel<<<(unsigned)tiles, TC_THREADS, smem, (cudaStream_t)stream>>>(xmap, wmap, a);
   MRB_LAUNCH_CHECK();
+  return 0;
+}
+
+// Scratch of mrb_cnn_conv3d_wgrad_tc: packed operands (BF16) then FP32 partials.
+static size_t wg_scratch_bytes(const WgPlan& p) {
+  size_t b = (p.xs_elems + p.gt_elems) * sizeof(bf16);
+  b = (b + 255) & ~(size_t)255;
+  return b + p.part_floats * sizeof(float);
+}
+
+extern "C" int mrb_cnn_wgrad_tc_scratch_bytes(int cin, int coutp, const int* vol, int64_t* bytes) {
+  MRB_REQUIRE(vol && bytes, "null pointer");
+  WgPlan p{};
+  MRB_REQUIRE(wg_plan(cin, coutp, vol[0], vol[1], vol[2], vol[3], p),
+              "shape not supported by the tensor-core weight gradient");
+  *bytes = (int64_t)wg_scratch_bytes(p);
+  return 0;
+}
+
+extern "C" int mrb_cnn_conv3d_wgrad_tc(const void* x, int cx, int ci_off, int cin, const void* gz, int cg, int cg_off,
+                                       int coutp, float* dw, float* dbias, void* scratch, int64_t scratch_bytes,
+                                       const int* vol, mrb_stream_t stream) {
+  MRB_REQUIRE(x && gz && dw && scratch && vol, "null pointer");
+  const int Nb = vol[0], D = vol[1], H = vol[2], W = vol[3];
+  MRB_REQUIRE(Nb >= 1 && D >= 1 && H >= 1 && W >= 1, "bad volume");
+  MRB_REQUIRE(ci_off + cin <= cx && cg_off + coutp <= cg, "channel range outside the tensor");
+  MRB_REQUIRE(coutp <= 256 && 256 % coutp == 0, "bias reduction needs coutp dividing 256");
+  WgPlan p{};
+  MRB_REQUIRE(wg_plan(cin, coutp, Nb, D, H, W, p), "shape not supported by the tensor-core weight gradient");
+  MRB_REQUIRE((size_t)scratch_bytes >= wg_scratch_bytes(p), "scratch of %lld bytes, %zu needed",
+              (long long)scratch_bytes, wg_scratch_bytes(p));
+  MRB_REQUIRE(((uintptr_t)scratch & 255) == 0, "scratch must be 256-byte aligned");
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return mrb::fail(MRB_ECUDA, "cuTensorMapEncodeTiled unavailable");
+  cudaStream_t st = (cudaStream_t)stream;
+  bf16* xs = (bf16*)scratch;
+  bf16* gt = xs + p.xs_elems;
+  float* part = (float*)(((uintptr_t)(gt + p.gt_elems) + 255) & ~(uintptr_t)255);
+  float* bpart = part + (size_t)p.nsplit * 27 * cin * coutp;
+  const int xch = p.xm ? p.Mpad : cin, gch = p.xm ? coutp : p.Mpad;
+  // channels-first copies (x three times, shifted along W)
+  {
+    dim3 gx((unsigned)((W / PK_W) * ((xch + 31) / 32)), (unsigned)H, (unsigned)(Nb * D));
+    wg_pack_kernel<<<gx, 256, 0, st>>>((const bf16*)x, cx, ci_off, cin, xs, xch, 3, D, H, W);
+    MRB_LAUNCH_CHECK();
+    dim3 gg((unsigned)((W / PK_W) * ((gch + 31) / 32)), (unsigned)H, (unsigned)(Nb * D));
+    wg_pack_kernel<<<gg, 256, 0, st>>>((const bf16*)gz, cg, cg_off, coutp, gt, gch, 1, D, H, W);
+    MRB_LAUNCH_CHECK();
+  }
+  // tensor maps: xs (W, H, D, xch, Nb*3), box {32, 1, 1, rows, 1}; gt (W, H, D, gch, Nb)
+  const cuuint64_t plane = (cuuint64_t)D * H * W;
+  CUtensorMap xmap, gmap;
+  cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  {
+    cuuint64_t dims[5] = {(cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D, (cuuint64_t)xch, (cuuint64_t)Nb * 3};
+    cuuint64_t strd[4] = {(cuuint64_t)W * 2, (cuuint64_t)W * H * 2, plane * 2, plane * xch * 2};
+    cuuint32_t box[5] = {(cuuint32_t)WG_KV, 1, 1, (cuuint32_t)(p.xm ? 128 : p.N), 1};
+    CUresult r = enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, xs, dims, strd, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return mrb::fail(MRB_ECUDA, "packed activation tensor map failed (%d)", (int)r);
+  }
+  {
+    cuuint64_t dims[5] = {(cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D, (cuuint64_t)gch, (cuuint64_t)Nb};
+    cuuint64_t strd[4] = {(cuuint64_t)W * 2, (cuuint64_t)W * H * 2, plane * 2, plane * gch * 2};
+    cuuint32_t box[5] = {(cuuint32_t)WG_KV, 1, 1, (cuuint32_t)(p.xm ? p.N : 128), 1};
+    CUresult r = enc(&gmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, gt, dims, strd, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return mrb::fail(MRB_ECUDA, "packed gradient tensor map failed (%d)", (int)r);
+  }
+  WgArgs a{};
+  a.xm = p.xm;
+  a.N = p.N;
+  a.Mreal = p.Mreal;
+  a.cin = cin;
+  a.coutp = coutp;
+  a.TG = p.TG;
+  a.Nb = Nb;
+  a.D = D;
+  a.H = H;
+  a.W = W;
+  a.ksteps = p.ksteps;
+  a.kper = p.kper;
+  a.ngroups = p.ngroups;
+  a.mtiles = p.mtiles;
+  a.part = part;
+  a.ncols = 32;
+  while (a.ncols < p.TG * p.N) a.ncols <<= 1;
+  a.shared_bytes = p.shared_bytes;
+  a.pertap_bytes = p.pertap_bytes;
+  const size_t smem = WG_STAGES * (size_t)(p.shared_bytes + p.TG * p.pertap_bytes) + 1024;
+  MRB_REQUIRE(smem <= 227 * 1024, "weight gradient stages need %zu bytes of shared memory", smem);
+  MRB_CUDA_TRY(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const long long blocks = (long long)p.ngroups * p.mtiles * p.nsplit;
+  MRB_REQUIRE(blocks < (1LL << 31), "volume too large");
+  wgrad_tc_kernel<<<(unsigned)blocks, TC_THREADS, smem, st>>>(xmap, gmap, a);
+  MRB_LAUNCH_CHECK();
+  const long long nw = 27LL * cin * coutp;
+  wg_sum_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(part, p.nsplit, nw, dw);
+  MRB_LAUNCH_CHECK();
+  if (dbias) {
+    const long long vox = (long long)Nb * D * H * W;
+    const long long vper = (vox + p.nsplit - 1) / p.nsplit;
+    wg_bias_kernel<<<(unsigned)p.nsplit, 256, 0, st>>>((const bf16*)gz, cg, cg_off, coutp, vox, vper, bpart);
+    MRB_LAUNCH_CHECK();
+    wg_sum_kernel<<<(unsigned)((coutp + 255) / 256), 256, 0, st>>>(bpart, p.nsplit, coutp, dbias);
+    MRB_LAUNCH_CHECK();
+  }
   return 0;
 }
 

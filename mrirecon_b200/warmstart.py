@@ -70,6 +70,10 @@ _SIGS = {
                           ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_int,
                           ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p],
     "mrb_cnn_tc_error": [ct.c_void_p],
+    "mrb_cnn_wgrad_tc_scratch_bytes": [ct.c_int, ct.c_int, ct.c_void_p, ct.c_void_p],
+    "mrb_cnn_conv3d_wgrad_tc": [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_int,
+                                ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64, ct.c_void_p,
+                                ct.c_void_p],
 }
 
 
@@ -257,6 +261,18 @@ class WarmStartCNN:
     # ---------------------------------------------------------------- training
     def _wgrad(self, name, x, cx, xoff, gz, cg, goff, vol, b):
         _, cinp, _, coutp, _, _ = next(l for l in LAYERS if l[0] == name)
+        if self.use_tc:
+            # tcgen05 weight gradient where the shape allows (scratch shared by all
+            # layers of a batch shape, sized for the largest)
+            nbytes = ct.c_int64(0)
+            if self.lib.mrb_cnn_wgrad_tc_scratch_bytes(cinp, coutp, vol, ct.byref(nbytes)) == 0:
+                sc = b.get("wtc")
+                if sc is None or sc.numel() < nbytes.value:
+                    sc = b["wtc"] = torch.empty(nbytes.value, dtype=torch.uint8, device=self.device)
+                _lib.check(self.lib.mrb_cnn_conv3d_wgrad_tc(_p(x), cx, xoff, cinp, _p(gz), cg, goff, coutp,
+                                                            _p(self.dw[name]), _p(self.db[name]), _p(sc), sc.numel(),
+                                                            vol, _lib.stream_ptr(self.device)), f"wgrad tc {name}")
+                return
         _lib.check(self.lib.mrb_cnn_conv3d_wgrad(_p(x), cx, xoff, cinp, _p(gz), cg, goff, coutp, _p(self.dw[name]),
                                                  _p(self.db[name]), _p(b["wpart"]), b["wpart"].numel(), vol,
                                                  _lib.stream_ptr(self.device)), f"wgrad {name}")

@@ -70,6 +70,59 @@ def test_conv_fwd_dgrad_wgrad_exact(cuda, cin, cout, vol):
     assert rel(dx, x5.grad.permute(0, 2, 3, 4, 1).reshape(V, cin)) < 1e-5
 
 
+def _wgrad_tc(L, xc, cx, ci_off, cin, gyc, cg, cout, vol, dw, db):
+    import ctypes as ct
+    from mrirecon_b200 import _lib
+    from mrirecon_b200.warmstart import _vol
+    nbytes = ct.c_int64(0)
+    _lib.check(L.mrb_cnn_wgrad_tc_scratch_bytes(cin, cout, _vol(*vol), ct.byref(nbytes)), "scratch size")
+    scratch = torch.empty(nbytes.value, dtype=torch.uint8, device=xc.device)
+    _lib.check(L.mrb_cnn_conv3d_wgrad_tc(xc.data_ptr(), cx, ci_off, cin, gyc.data_ptr(), cg, 0, cout, dw.data_ptr(),
+                                         db.data_ptr(), scratch.data_ptr(), scratch.numel(), _vol(*vol),
+                                         _lib.stream_ptr()), "wgrad tc")
+    err = ct.c_int(0)
+    _lib.check(L.mrb_cnn_tc_error(ct.byref(err)), "tc error")
+    assert err.value == 0
+
+
+@pytest.mark.parametrize("cin,cout,vol", [(32, 32, (2, 3, 8, 64)), (64, 128, (1, 4, 6, 64)),
+                                          (192, 64, (1, 2, 4, 128)), (96, 32, (2, 3, 5, 64)),
+                                          (64, 64, (1, 3, 4, 256))])
+def test_conv_wgrad_tensor_cores_exact(cuda, cin, cout, vol):
+    """Weight and bias gradient on tcgen05 (x on the M side when cin > cout, two
+    M tiles at cin = 192, gz on the M side otherwise) against FP64 autograd on
+    the same BF16 values and against the mma.sync kernel; the input is read at a
+    channel offset inside a wider tensor."""
+    from mrirecon_b200 import _lib
+    from mrirecon_b200.warmstart import _lib_cnn, _vol
+    L = _lib_cnn()
+    st = _lib.stream_ptr()
+    g = torch.Generator().manual_seed(7 * cin + cout)
+    Nb, D, H, W = vol
+    V = Nb * D * H * W
+    cx, ci_off = cin + 32, 16
+    xw = _bf(torch.randn((V, cx), generator=g))
+    x = xw[:, ci_off:ci_off + cin]
+    gy = _bf(torch.randn((V, cout), generator=g))
+    x5 = x.double().reshape(Nb, D, H, W, cin).permute(0, 4, 1, 2, 3)
+    w5 = torch.zeros((cout, cin, 3, 3, 3), dtype=torch.float64, requires_grad=True)
+    y5 = Fn.conv3d(x5, w5, padding=1)
+    y5.backward(gy.double().reshape(Nb, D, H, W, cout).permute(0, 4, 1, 2, 3))
+    dw_ref = w5.grad.reshape(cout, cin, 27).permute(2, 1, 0)
+    xc, gyc = xw.contiguous().to(cuda), gy.to(cuda)
+    dw = torch.full((27, cin, cout), float("nan"), dtype=torch.float32, device=cuda)
+    db = torch.full((cout,), float("nan"), dtype=torch.float32, device=cuda)
+    for _ in range(2):                      # the scratch holds no state between calls
+        _wgrad_tc(L, xc, cx, ci_off, cin, gyc, cout, cout, vol, dw, db)
+        assert rel(dw, dw_ref) < 1e-5
+        assert rel(db, gy.double().sum(0)) < 1e-5
+    dw2 = torch.zeros_like(dw)
+    part = torch.zeros(27 * cin * cout * 8, dtype=torch.float32, device=cuda)
+    _lib.check(L.mrb_cnn_conv3d_wgrad(xc.data_ptr(), cx, ci_off, cin, gyc.data_ptr(), cout, 0, cout, dw2.data_ptr(),
+                                      None, part.data_ptr(), part.numel(), _vol(*vol), st), "wgrad")
+    assert rel(dw, dw2) < 1e-5
+
+
 def test_network_loss_and_gradients_vs_autograd(cuda):
     from mrirecon_b200.warmstart import WarmStartCNN, LAYERS
     torch.manual_seed(0)
