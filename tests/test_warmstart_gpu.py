@@ -24,8 +24,20 @@ def test_trained_network_gains_on_grasp(cuda):
     assert r["warm_s"] < r["plain_s"]
     assert r["f_warm"] <= r["f_plain"] * (1 + 1e-3)
     # same tolerance, different start: the two results differ by what the
-    # windowed 1e-4 stop rule leaves unconverged
-    assert r["err_vs_plain"] < 2e-2
+    # windowed 1e-4 stop rule leaves unconverged (measured 6.7e-3)
+    assert r["err_vs_plain"] < 1e-2
+
+
+def test_warm_and_plain_agree_to_1e3_at_tolerance_1e6(cuda):
+    """At the windowed tolerance 1e-6 the warm-started and the plain solve of
+    the GRASP workload agree to <= 1e-3 rel-L2 (measured 7.0e-4; 1.1e-3 at 3e-6),
+    and the warm-started solve still reaches it faster (measured 0.46 s vs 1.18 s)."""
+    from mrirecon_b200.warmstart import tolerance_study
+    r = tolerance_study(WarmStartCNN.pretrained(cuda), tols=(1e-6,), star_tol=1e-6, star_max_iter=4000)
+    row = r["rows"][0]
+    assert row["err_vs_plain"] <= 1e-3
+    assert row["warm_s"] < row["plain_s"] and row["warm_iters"] < row["plain_iters"]
+    assert r["first_tol_within_1e-3"] == 1e-6
 
 
 def test_fallback_to_adjoint_start(cuda):
