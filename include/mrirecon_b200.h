@@ -99,9 +99,10 @@ int mrb_plan_destroy(mrb_plan* plan);
  *         coil-planar grid (0).  3D: a copy of the grid (written by the x
  *         column pass for 8/16/32 coils, else by a tiled transpose; one more
  *         grid-sized buffer), then 128-bit gathers of all coils of a cell.
- *         2D fused FFT mode: the forward column pass writes the plan's grid
- *         itself as (cell, coil) (blocks of 4 columns x 4 coils) and the interp
- *         gathers each cell's coils as one run; no extra buffer.  Same samples. */
+ *         2D fused FFT mode with C % 4 == 0: the forward column pass writes
+ *         the plan's grid itself in coil quads, (quad, cell, 4 coils) (blocks
+ *         of 4 columns x 4 coils, 128-byte stores), and the interp gathers coil
+ *         pairs with 128-bit loads; no extra buffer.  Same samples. */
 int mrb_plan_set_option(mrb_plan* plan, int key, int64_t value);
 
 /* Trajectory (dev, (B, nd, K) float32 radians in [-pi, pi)): float32 grid

@@ -387,13 +387,13 @@ __global__ void __launch_bounds__(COL_NT, G0 <= 320 ? 2 : 1) fwd_cols_il_kernel(
   fft_stages<G0, 0, IL_ROWS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
 }
 
-// forward column pass writing a coil-interleaved grid (2D, see fft.cuh): a
-// block transforms its COLS (column, coil) pairs as CJ consecutive columns of
-// CG consecutive coils of one frame, so that its band reads are runs of CJ
-// columns of a coil and its grid stores runs of CG coils of a cell (32 bytes
-// each for the usual CJ = CG = 4: whole sectors on both sides when C % 4 == 0).
-// Same transforms as fwd_cols_kernel: the grid values are identical, only
-// their order in memory differs.
+// forward column pass writing a coil-quad grid (2D, see fft.cuh): a block
+// transforms its COLS (column, coil) pairs as CJ consecutive columns of CG
+// consecutive coils of one frame, so that its band reads are runs of CJ
+// columns of a coil (32 bytes for CJ = 4) and its grid stores, in the layout
+// (frame, coil quad, cell, coil in quad), runs of CJ cells x 4 coils (one
+// 128-byte line for CJ = CG = 4).  Same transforms as fwd_cols_kernel: the
+// grid values are identical, only their order in memory differs.  C % 4 == 0.
 template <int G0>
 struct ColGroups {
   static constexpr int COLS = cols_per_block(G0);
@@ -420,7 +420,8 @@ __global__ void __launch_bounds__(COL_NT) fwd_cols_cg_kernel(const float2* __res
   const int be = blk / cgroups;
   const int k0 = cb * CJ, c0 = cgi * CG;
   const float2* tb = Tb + ((long long)be * C + c0) * g.S0 * G1 + k0;          // (coil, band row, column)
-  float2* ob = out + (long long)be * g.gtot * C + (long long)k0 * C + c0;      // (cell, coil)
+  // quad plane of coil c0 (4 coils x gtot cells), then (cell, coil in quad)
+  float2* ob = out + ((long long)be * C + (c0 & ~3)) * g.gtot + (long long)k0 * 4 + (c0 & 3);
   auto load0 = [&](int q, int n0) -> float2 {
     const int j = q % CJ, cc = q / CJ;
     const int r = n0 - g.off0;
@@ -429,7 +430,7 @@ __global__ void __launch_bounds__(COL_NT) fwd_cols_cg_kernel(const float2* __res
   };
   auto store = [&](int q, int n0, float2 v) {
     const int j = q % CJ, cc = q / CJ;
-    if (k0 + j < G1 && c0 + cc < C) ob[((long long)n0 * G1 + j) * C + cc] = v;
+    if (k0 + j < G1 && c0 + cc < C) ob[((long long)n0 * G1 + j) * 4 + cc] = v;
   };
   fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
 }

@@ -35,10 +35,10 @@ int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, 
 bool fft2_columns_il_supported(int G0, int C);
 int fft2_columns_il(const float2* Tb, float2* out, const float2* tw0, int S0, int G0, int G1, int C, int nb,
                     const double* skip, cudaStream_t st);
-// Forward column pass of a 2D grid with a coil-interleaved output: in
-// (nb, C, S0, G1) band rows -> out (nb, G0 * G1 cells, C), the same values as
-// fft2_columns in (cell, coil) order (any C; whole 32-byte sectors on both
-// sides when C % 4 == 0), for the interp's 128-bit gathers of a cell's coils
+// Forward column pass of a 2D grid with a coil-quad output: in (nb, C, S0, G1)
+// band rows -> out (nb, C / 4 quads, G0 * G1 cells, 4 coils), the same values
+// as fft2_columns with each cell's coils in groups of four (32 bytes), for the
+// interp's 128-bit gathers of a cell's coil pairs.  C % 4 == 0.
 int fft2_columns_cg(const float2* Tb, float2* out, const float2* tw0, int S0, int S1, int G0, int G1, int C, int nb,
                     const double* skip, cudaStream_t st);
 // Forward column pass fused with the KB interp (2D): the block of a coil and

@@ -96,7 +96,7 @@ struct mrb_plan {
   DevBuf rowfac;      // fused mode: signed deapodisation of each image row (S0, or S0*S1 in 3D)
   const double* skip = nullptr;   // device flag: operator kernels return when it is non-zero
   int il = 0;         // 1: forward interp on a coil-interleaved grid (3D: a copy of the grid; 2D fused mode:
-                      // the forward column pass writes the grid itself as (cell, coil))
+                      // the forward column pass writes the grid itself in coil quads (cell, 4 coils))
   DevBuf grid_il;     // (nb, gtot, C) float2, written by the transpose at the start of the interp stage
   DevBuf psf;         // Toeplitz transfer functions (B, G0, G1) float (mrb_plan_set_toeplitz)
   DevBuf ones;        // 2D: S0 signs (-1)^(r + G0/2 - S0/2), then S1 ones: the row passes without deapodisation
@@ -594,17 +594,15 @@ __global__ void __launch_bounds__(256) interp2p_kernel(InterpArgs a, Geo g, KBPo
   if (two) yo[g.K] = make_float2(r1 * s, m1 * s);
 }
 
-// 2D forward interp on the coil-interleaved grid (be, cell, coil) that the
-// coil-grouped forward column pass writes.  One thread per (sample, coil pair)
-// with the P pairs of a sample on adjacent threads, so that each tap's C coils
-// are read as one contiguous run (C = 12: 96 bytes per cell, whole sectors)
-// with 128-bit loads when C is even; on the coil-planar grid every 4-cell tap
-// row of a coil is a 32-byte piece that straddles two sectors three times in
-// four.  A block covers S = 256 / P consecutive samples; the results go
-// through shared memory so that each coil's samples are stored as one run.
-// Taps, weights and summation order are those of interp2p_kernel: identical
-// samples.
-template <bool V4>
+// 2D forward interp on the coil-quad grid (be, coil quad, cell, coil in quad)
+// that the coil-grouped forward column pass writes.  One thread per (sample,
+// coil pair) with the P pairs of a sample on adjacent threads and 128-bit
+// loads: a 4-cell tap row of a quad is one 128-byte run (at most two lines),
+// where on the coil-planar grid every 4-cell tap row of a coil is a 32-byte
+// piece that straddles two sectors three times in four.  A block covers
+// S = 256 / P consecutive samples; the results go through shared memory so
+// that each coil's samples are stored as one run.  Taps, weights and summation
+// order are those of interp2p_kernel: identical samples.  C % 4 == 0.
 __global__ void __launch_bounds__(256) interp2_il_kernel(InterpArgs a, Geo g, KBPoly kb) {
   constexpr int W = 4;
   __shared__ float2 ys[512];   // [coil][sample]: C * S <= 2 * P * S <= 512
@@ -636,23 +634,15 @@ __global__ void __launch_bounds__(256) interp2_il_kernel(InterpArgs a, Geo g, KB
     float s = a.scale * a.gsign;
     if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
     const int c = 2 * pr;
-    const bool two = c + 1 < C;
-    const float2* gb = a.grid + (long long)be * g.gtot * C + c;
+    const bool two = true;   // C % 4 == 0: every pair is whole
+    const float2* gb = a.grid + ((long long)be * C + (c & ~3)) * g.gtot + (c & 3);
     float4 v[W][W];
 #pragma unroll
     for (int i0 = 0; i0 < W; ++i0) {
       const long long roff = (long long)nidx[0][i0] * g.G[1];
 #pragma unroll
-      for (int i1 = 0; i1 < W; ++i1) {
-        const float2* q = gb + (roff + nidx[1][i1]) * C;
-        if (V4) {
-          v[i0][i1] = __ldg(reinterpret_cast<const float4*>(q));
-        } else {
-          const float2 u0 = __ldg(q);
-          const float2 u1 = two ? __ldg(q + 1) : make_float2(0.f, 0.f);
-          v[i0][i1] = make_float4(u0.x, u0.y, u1.x, u1.y);
-        }
-      }
+      for (int i1 = 0; i1 < W; ++i1)
+        v[i0][i1] = __ldg(reinterpret_cast<const float4*>(gb + (roff + nidx[1][i1]) * 4));
     }
     float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
 #pragma unroll
@@ -2338,10 +2328,11 @@ static bool col_interp_active(const mrb_plan* p) {
   return p->fft_mode == 1 && p->nd == 2 && p->col_interp == 1 && p->nstrips > 0;
 }
 
-// fused 2D mode with the interleaved interp: the forward column pass writes the
-// grid as (cell, coil) and the interp gathers all coils of a cell at once
+// fused 2D mode with the interleaved interp (coil counts divisible by 4): the
+// forward column pass writes the grid in coil quads (cell, 4 coils) and the
+// interp gathers coil pairs with 128-bit loads
 static bool il2_active(const mrb_plan* p) {
-  return p->fft_mode == 1 && p->nd == 2 && p->il == 1 && p->C <= 512 && !col_interp_active(p);
+  return p->fft_mode == 1 && p->nd == 2 && p->il == 1 && p->C % 4 == 0 && p->C <= 512 && !col_interp_active(p);
 }
 
 // the spread writes only touched cell pairs into a grid of its own (fused FFT mode)
@@ -2504,8 +2495,7 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       const int S = 256 / ((p->C + 1) / 2);
       const long long nbx = (p->K + S - 1) / S;
       MRB_REQUIRE(nbx < (1LL << 31) && nb <= 65535, "too many samples for the interp");
-      if (p->C % 2 == 0) interp2_il_kernel<true><<<dim3((unsigned)nbx, nb), 256, 0, st>>>(a, g, p->kb);
-      else interp2_il_kernel<false><<<dim3((unsigned)nbx, nb), 256, 0, st>>>(a, g, p->kb);
+      interp2_il_kernel<<<dim3((unsigned)nbx, nb), 256, 0, st>>>(a, g, p->kb);
       MRB_LAUNCH_CHECK();
       return 0;
     }

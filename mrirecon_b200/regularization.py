@@ -88,6 +88,22 @@ def image_geometry(x: torch.Tensor, roles: Roles):
     return nd, tuple(int(s) for s in x.shape[2:]), int(x.shape[0])
 
 
+def _whole_tensor(interior, shape) -> bool:
+    """True when a write-interior slice tuple covers every index of `shape`: what
+    graspcg's RegManager passes for a single shard (graspcg/regularization/
+    manager.py:268-301 gives slice(0, B) on the frame axis when a temporal term
+    asks for a halo but there is no neighbouring shard)."""
+    if interior is None:
+        return True
+    for sl, n in zip(interior, shape):
+        if not isinstance(sl, slice):
+            return False
+        start, stop, step = sl.indices(int(n))
+        if (start, stop, step) != (0, int(n), 1):
+            return False
+    return True
+
+
 class TVND:
     """N-D Huber TV (reference TVND contract), evaluated by the fused CUDA kernel."""
 
@@ -109,10 +125,9 @@ class TVND:
     def energy_grad_fixed_axes(self, ctx: RegContext, axes: Tuple[int, ...]) -> torch.Tensor:
         if len(axes) == 0 or self.params.weight == 0.0:
             return torch.zeros((), device=ctx.device, dtype=torch.float64)
-        interior = ctx.write_interior_slice
-        if interior is not None and any(s != slice(None) for s in interior):
-            raise NotImplementedError("halo-extended shards are not supported by the single-GPU B200 path")
         x, g = ctx.x, ctx.g
+        if not _whole_tensor(ctx.write_interior_slice, x.shape):
+            raise NotImplementedError("halo-extended shards are not supported by the single-GPU B200 path")
         _lib.require_cuda(x, "x")
         if x.dtype != torch.complex64 or g.dtype != torch.complex64 or not x.is_contiguous() or not g.is_contiguous():
             raise ValueError("TVND (B200) needs contiguous complex64 x and g")

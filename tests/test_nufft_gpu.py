@@ -389,13 +389,13 @@ def test_2d_pair_parallel_interp_identical(cuda, C, nb, B):
         assert torch.equal(ad.A(x), y1)
 
 
-@pytest.mark.parametrize("S,C,nb,B", [((40, 48), 12, 2, 2), ((40, 48), 5, 3, 1), ((32, 32), 1, 1, 1),
-                                      ((48, 40), 4, 4, 2), ((160, 320), 3, 1, 1)])
+@pytest.mark.parametrize("S,C,nb,B", [((40, 48), 12, 2, 2), ((40, 48), 8, 3, 1), ((32, 32), 16, 1, 1),
+                                      ((48, 40), 4, 4, 2), ((320, 160), 4, 1, 1), ((40, 48), 5, 2, 1)])
 def test_2d_interleaved_grid_interp_identical(cuda, S, C, nb, B):
-    """Fused 2D mode: the forward column pass writing the grid as (cell, coil)
-    (coil groups of 4 with a tail group, column groups with a tail at G0 = 640)
-    and the interleaved interp (option key 5, the default) give the samples of
-    the planar column pass and pair-parallel interp bit for bit."""
+    """Fused 2D mode: the forward column pass writing the grid in coil quads
+    (column groups with a tail at G0 = 640) and the interleaved interp (option
+    key 5, the default for coil counts divisible by 4; C = 5 stays planar) give
+    the samples of the planar column pass and pair-parallel interp bit for bit."""
     maps = _rand_c((C,) + S, 74, torch.complex64)
     traj = phantoms.random_traj(B, 2, 1000, seed=75)
     x = _rand_c((nb, 1) + S, 76, torch.complex64).to(cuda)

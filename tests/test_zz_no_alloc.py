@@ -89,14 +89,16 @@ def test_dots_noalloc_inside_a_captured_graph():
     _dots(lib, "mrb_dots_f64_noalloc", n, 3, A, Bp, Dp, eager)
     out = torch.full((3,), float("nan"), dtype=torch.float64, device=dev)
     torch.cuda.synchronize()
-    before = torch.cuda.memory_allocated(dev)
     side = torch.cuda.Stream(dev)
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.stream(side):
         graph.capture_begin()
+        # (torch itself allocates a little state at capture_begin; measure around the call)
+        before = torch.cuda.memory_allocated(dev)
         _dots(lib, "mrb_dots_f64_noalloc", n, 3, A, Bp, Dp, out)
+        after = torch.cuda.memory_allocated(dev)
         graph.capture_end()
-    assert torch.cuda.memory_allocated(dev) == before
+    assert after == before
     graph.replay()
     torch.cuda.synchronize()
     torch.testing.assert_close(out, eager, rtol=0.0, atol=0.0)
