@@ -82,10 +82,10 @@ int mrb_plan_destroy(mrb_plan* plan);
  * key 6 = spread kernel: 1 one block per work item, all coils of a group
  *         sharing the staged samples (2D tile 16, 3D tile 8; other tiles fall
  *         back to 0; the 3D default), 0 one warp per work item and coil group
- *         (the 2D default; in 2D with coil groups of up to 16 the warp first
- *         tabulates each staged sample's inside taps, then runs only those),
- *         2 one warp per work item evaluating every tap per lane task (the
- *         earlier 2D kernel); all give identical grids,
+ *         (the 2D default), 2 (2D, coil groups of up to 16) one warp per work
+ *         item that first tabulates each staged sample's inside taps and then
+ *         runs only those (faster from 6 coils per item on, slower at 4: the
+ *         autotuner times both); all give identical grids,
  * key 7 = grid mask (fused FFT mode): 1 (default) the adjoint spread keeps its
  *         own grid, zeroed once per trajectory and batch size, and stores only
  *         the cell pairs inside some sample's support (per-frame bitmaps built by
@@ -95,14 +95,16 @@ int mrb_plan_destroy(mrb_plan* plan);
  *         (1; set before set_points, which then builds the per-frame strip
  *         lists) or writes the grid for a separate interp pass (0, the
  *         default: 2% slower forward, but each kernel on its own); same samples,
- * key 5 = forward interp on a coil-interleaved grid (1, the default) or on the
- *         coil-planar grid (0).  3D: a copy of the grid (written by the x
+ * key 5 = forward interp on a coil-interleaved grid (1; the 3D default) or on
+ *         the coil-planar grid (0; the 2D default).  3D: a copy of the grid (written by the x
  *         column pass for 8/16/32 coils, else by a tiled transpose; one more
  *         grid-sized buffer), then 128-bit gathers of all coils of a cell.
  *         2D fused FFT mode with C % 4 == 0: the forward column pass writes
  *         the plan's grid itself in coil quads, (quad, cell, 4 coils) (blocks
  *         of 4 columns x 4 coils, 128-byte stores), and the interp gathers coil
- *         pairs with 128-bit loads; no extra buffer.  Same samples. */
+ *         pairs with 128-bit loads; no extra buffer.  Same samples.  On the
+ *         GRASP workload the interp gains 20 us and the column pass loses 46 us,
+ *         so 2D keeps the planar grid by default. */
 int mrb_plan_set_option(mrb_plan* plan, int key, int64_t value);
 
 /* Trajectory (dev, (B, nd, K) float32 radians in [-pi, pi)): float32 grid

@@ -23,7 +23,8 @@ import torch
 # item, 16)), kernel 0 the per-warp spread
 CANDIDATES_2D: Tuple[Tuple[int, int, int, int], ...] = (
     (16, 16, 128, 1), (16, 16, 256, 1), (16, 16, 512, 1), (16, 16, 64, 1),
-    (16, 4, 128, 0), (16, 6, 128, 0), (8, 4, 64, 0), (32, 2, 128, 0))
+    (16, 4, 128, 0), (16, 6, 128, 0), (8, 4, 64, 0), (32, 2, 128, 0),
+    (16, 6, 128, 2), (16, 12, 128, 2), (16, 4, 128, 2))
 CANDIDATES_3D: Tuple[Tuple[int, int, int, int], ...] = (
     (8, 16, 4096, 1), (8, 8, 4096, 1), (8, 16, 1024, 1), (8, 8, 1024, 1), (8, 16, 16384, 1), (4, 4, 256, 0),
     (4, 8, 256, 0))

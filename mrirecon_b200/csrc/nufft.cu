@@ -1951,7 +1951,7 @@ extern "C" int mrb_plan_create(mrb_plan** out, int nd, const int* S, int C, int 
       rc = mrb::fail(MRB_ECUDA, "copying row deapodisation failed");
   }
   if (!rc && fused_supported(p)) rc = mrb_plan_set_option(p, 4, 1);
-  if (!rc) p->il = 1;
+  if (!rc && nd == 3) p->il = 1;   // 2D: the planar column pass + interp is faster overall
   if (rc) {
     delete p;
     return rc;
@@ -2011,7 +2011,7 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
       return 0;
     case 6:
       MRB_REQUIRE(value >= 0 && value <= 2,
-                  "spread kernel must be 0 (per-warp), 1 (block per tile) or 2 (per-warp without tap tables)");
+                  "spread kernel must be 0 (per-warp), 1 (block per tile) or 2 (per-warp with tap tables)");
       p->spread_kernel = (int)value;
       return 0;
     case 8:
@@ -2584,10 +2584,10 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
         smem = Spread2Smem<8>::BYTES;
       }
     }
-    // 2D per-warp work items: the tap-table kernel (coil groups of up to 16),
-    // or with option key 6 = 2 the kernel that evaluates every tap per lane task
+    // 2D per-warp work items with option key 6 = 2: the tap-table kernel (coil
+    // groups of up to 16); key 6 = 0 the kernel that evaluates every tap per lane task
 #define MRB_SPREAD2W_CASE(T_)                                                                 \
-  if (!fn && p->nd == 2 && tg.T == T_ && p->spread_kernel == 0 && a.cpi <= 16) {             \
+  if (!fn && p->nd == 2 && tg.T == T_ && p->spread_kernel == 2 && a.cpi <= 16) {             \
     fn = (const void*)spread2w_kernel<T_>;                                                   \
     smem = SPREAD_WARPS * Spread2wSmem<T_>::warp_bytes(a.cpi);                               \
   }

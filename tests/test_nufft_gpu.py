@@ -394,13 +394,14 @@ def test_2d_pair_parallel_interp_identical(cuda, C, nb, B):
 def test_2d_interleaved_grid_interp_identical(cuda, S, C, nb, B):
     """Fused 2D mode: the forward column pass writing the grid in coil quads
     (column groups with a tail at G0 = 640) and the interleaved interp (option
-    key 5, the default for coil counts divisible by 4; C = 5 stays planar) give
+    key 5 = 1 with coil counts divisible by 4; C = 5 stays planar) give
     the samples of the planar column pass and pair-parallel interp bit for bit."""
     maps = _rand_c((C,) + S, 74, torch.complex64)
     traj = phantoms.random_traj(B, 2, 1000, seed=75)
     x = _rand_c((nb, 1) + S, 76, torch.complex64).to(cuda)
     ad = _adapter(maps, traj)
     assert ad.plan.info()["fft_mode"] == 1
+    ad.plan.set_option(5, 1)
     y1 = ad.A(x)
     ad.plan.set_option(5, 0)
     assert torch.equal(ad.A(x), y1)
@@ -413,8 +414,8 @@ def test_2d_interleaved_grid_interp_identical(cuda, S, C, nb, B):
                                                           (16, 16, None, 1, 1)])
 def test_2d_tap_table_spread_identical_to_earlier_kernel(cuda, tile, cpi, chunk, fft_mode, mask):
     """The per-warp 2D spread that tabulates each staged sample's inside taps
-    (option key 6 = 0) gives the grid of the kernel that evaluates every tap per
-    lane task (key 6 = 2) bit for bit: tiles 4 .. 32, odd coil groups, split
+    (option key 6 = 2) gives the grid of the kernel that evaluates every tap per
+    lane task (key 6 = 0) bit for bit: tiles 4 .. 32, odd coil groups, split
     tiles, the masked write-out and the dense FFT mode."""
     C = 12
     maps = _rand_c((C, 48, 40), 53, torch.complex64)
@@ -422,6 +423,7 @@ def test_2d_tap_table_spread_identical_to_earlier_kernel(cuda, tile, cpi, chunk,
     y = _rand_c((2, C, traj.shape[-1]), 54, torch.complex64).to(cuda)
     ad = _adapter(maps, traj, tile=tile, chunk=chunk, coils_per_item=cpi, fft_mode=fft_mode)
     ad.plan.set_option(7, mask)
+    ad.plan.set_option(6, 0)
     x0 = ad.AH(y)
     ad.plan.set_option(6, 2)
     assert torch.equal(ad.AH(y), x0)
