@@ -283,27 +283,27 @@ __global__ void __launch_bounds__(TC_THREADS) conv3d_tc_kernel(const __grid_cons
 
 // ---------------------------------------------------------------------------
 // Weight gradient on tcgen05: dW[tap][ci][co] = sum_v x[v + o(tap)][ci] gz[v][co]
-// (o(tap) the (dz, dy, dx) offset; out-of-volume x is zero), the
-// reduction over voxels as the GEMM's K.  Both operands must be K-major for
-// the MMA, i.e. voxels contiguous, so they are first repacked channels-first
-// (wg_pack_kernel): gz as gt (Nb, Mg, D, H, W) and x as xs (Nb, 3, Mx, D, H, W),
-// three copies shifted by dx = -1, 0, +1 along W.  A K step is 32 consecutive
-// voxels of one (n, d, h) row; the tap offset then moves only the H and D
-// coordinates of a TMA box (out-of-volume rows read as zero) and picks the dx
-// copy, so every box starts at a W coordinate that is a multiple of 32.
-// The operand with more channels is the MMA's M side (128 rows per tile,
-// channels padded with zeros in the packed copy), the other the N side
-// (16 .. 256).  With x on the M side (xm), A is per tap (shifted) and B once
-// per K step; otherwise A (gz) once per K step and B per tap.  A CTA owns a
-// group of TG taps (TG accumulators of N columns in TMEM), an M tile and a
-// range of K steps; its partial sums go to part[split][tap][ci][co] and are
-// added in a fixed split order (deterministic).
+// (o(tap) the (dz, dy, dx) offset; out-of-volume x is zero), the reduction
+// over voxels as the GEMM's K.  Both operands must be K-major for the MMA,
+// i.e. voxels contiguous, so they are first repacked channels-first
+// (wg_pack_kernel).  The operand with more channels is the MMA's M side (128
+// rows per tile, channels padded with zeros) and is loaded once per K step;
+// the other is the N side (16 .. 256 rows) and carries the tap offset, so a K
+// step loads one M tile and one small N tile per tap.  The offset moves only
+// the H and D coordinates of a TMA box (out-of-volume rows read as zero) and
+// picks one of three copies of the N operand shifted by -1, 0, +1 along W, so
+// every box starts at a W coordinate that is a multiple of 32.  With x on the
+// M side the N operand is gz shifted the other way (sum_u x[u] gz[u - o]); the
+// sums are the same.  A K step is 32 consecutive voxels of one (n, d, h) row.
+// A CTA owns a group of TG taps (TG accumulators of N columns in TMEM), an M
+// tile and a range of K steps; its partial sums go to part[split][tap][ci][co]
+// and are added in a fixed split order (deterministic).
 // ---------------------------------------------------------------------------
 constexpr int WG_STAGES = 4;
 constexpr int WG_KV = 32;   // voxels per K step (one 64-byte swizzle row of BF16)
 
 struct WgArgs {
-  int xm;              // 1: x is the M operand (A per tap), 0: gz is (B per tap)
+  int xm;              // 1: x is the M operand (gz shifted), 0: gz is (x shifted)
   int N;               // columns: channels of the N operand (multiple of 16, <= 256)
   int Mreal;           // real channels of the M operand
   int cin, coutp;      // dW is [27][cin][coutp]
@@ -314,18 +314,18 @@ struct WgArgs {
   int ngroups, mtiles;
   float* part;         // [split][27][cin][coutp]
   int ncols;           // TMEM columns allocated
-  uint32_t shared_bytes, pertap_bytes;   // tile bytes (multiples of 1024)
+  uint32_t m_bytes, n_bytes;   // tile bytes (multiples of 1024)
 };
 
-__global__ void __launch_bounds__(TC_THREADS) wgrad_tc_kernel(const __grid_constant__ CUtensorMap xmap,
-                                                              const __grid_constant__ CUtensorMap gmap, WgArgs a) {
+__global__ void __launch_bounds__(TC_THREADS) wgrad_tc_kernel(const __grid_constant__ CUtensorMap mmap,
+                                                              const __grid_constant__ CUtensorMap nmap, WgArgs a) {
   extern __shared__ __align__(1024) uint8_t dsm[];
   __shared__ __align__(8) uint64_t full_bar[WG_STAGES], empty_bar[WG_STAGES], done_bar;
   __shared__ uint32_t tmem_base;
   __shared__ volatile int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(dsm) + 1023) & ~uintptr_t(1023));
-  const uint32_t stage_bytes = a.shared_bytes + (uint32_t)a.TG * a.pertap_bytes;
+  const uint32_t stage_bytes = a.m_bytes + (uint32_t)a.TG * a.n_bytes;
 
   // block -> (tap group, M tile, split)
   long long bid = blockIdx.x;
@@ -339,7 +339,8 @@ __global__ void __launch_bounds__(TC_THREADS) wgrad_tc_kernel(const __grid_const
   const long long kb0 = split * a.kper;
   const long long kb1 = min(a.ksteps, kb0 + a.kper);
   const int nk = (int)(kb1 - kb0);
-  const uint32_t a_tile = 128u * WG_KV * 2u, b_tile = (uint32_t)a.N * WG_KV * 2u;
+  const uint32_t m_tile = 128u * WG_KV * 2u, n_tile = (uint32_t)a.N * WG_KV * 2u;
+  const int sg = a.xm ? -1 : 1;   // the N operand's offset: gz[u - o] or x[v + o]
 
   if (threadIdx.x == 0) {
     for (int st = 0; st < WG_STAGES; ++st) {
@@ -363,7 +364,7 @@ __global__ void __launch_bounds__(TC_THREADS) wgrad_tc_kernel(const __grid_const
   const int nwc = a.W / WG_KV;
 
   if (warp == 0 && lane == 0) {
-    // producer: per K step the shared tile and one tile per tap of the group
+    // producer: per K step the M tile and one N tile per tap of the group
     for (int ks = 0; ks < nk; ++ks) {
       const int st = ks % WG_STAGES;
       if (ks >= WG_STAGES && !mbar_wait(&empty_bar[st], ((ks / WG_STAGES) - 1) & 1, &abort_flag)) break;
@@ -375,14 +376,13 @@ __global__ void __launch_bounds__(TC_THREADS) wgrad_tc_kernel(const __grid_const
       const int d = (int)(kv % a.D);
       const int n = (int)(kv / a.D);
       uint8_t* sbase = base + (size_t)st * stage_bytes;
-      mbar_expect_tx(&full_bar[st], (a.xm ? b_tile : a_tile) + (uint32_t)ntap * (a.xm ? a_tile : b_tile));
-      // shared tile: the gz rows of this K step (M rows m0.. or all N rows)
-      tma_load_5d(sbase, &gmap, &full_bar[st], w0, h, d, a.xm ? 0 : m0, n);
+      mbar_expect_tx(&full_bar[st], m_tile + (uint32_t)ntap * n_tile);
+      tma_load_5d(sbase, &mmap, &full_bar[st], w0, h, d, m0, n);
       for (int t = 0; t < ntap; ++t) {
         const int tap = tap0 + t;
         const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-        tma_load_5d(sbase + a.shared_bytes + (size_t)t * a.pertap_bytes, &xmap, &full_bar[st], w0, h + dy, d + dz,
-                    a.xm ? m0 : 0, n * 3 + dx + 1);
+        tma_load_5d(sbase + a.m_bytes + (size_t)t * a.n_bytes, &nmap, &full_bar[st], w0, h + sg * dy, d + sg * dz,
+                    0, n * 3 + sg * dx + 1);
       }
     }
   } else if (warp == 1 && lane == 0) {
@@ -391,10 +391,9 @@ __global__ void __launch_bounds__(TC_THREADS) wgrad_tc_kernel(const __grid_const
       const int st = ks % WG_STAGES;
       if (!mbar_wait(&full_bar[st], (ks / WG_STAGES) & 1, &abort_flag)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t ssh = smem_u32(base + (size_t)st * stage_bytes);
+      const uint32_t sa = smem_u32(base + (size_t)st * stage_bytes);
       for (int t = 0; t < ntap; ++t) {
-        const uint32_t stp = ssh + a.shared_bytes + (uint32_t)t * a.pertap_bytes;
-        const uint32_t sa = a.xm ? stp : ssh, sb = a.xm ? ssh : stp;
+        const uint32_t sb = sa + a.m_bytes + (uint32_t)t * a.n_bytes;
 #pragma unroll
         for (int kk = 0; kk < WG_KV / 16; ++kk) {
           const uint64_t adesc = sw64_desc(sa + kk * 32);
@@ -502,12 +501,12 @@ __global__ void wg_sum_kernel(const float* __restrict__ part, int nsplit, long l
   out[i] = s;
 }
 
-// per-split channel sums of gz (bias gradient): block = split, thread = (channel, lane of 8)
+// per-split channel sums of gz (bias gradient): block = split, thread = (channel, lane)
 __global__ void __launch_bounds__(256) wg_bias_kernel(const bf16* __restrict__ gz, int cg, int cg_off, int coutp,
                                                       long long voxels, long long vper, float* __restrict__ bpart) {
   __shared__ float red[256];
   const long long v0 = (long long)blockIdx.x * vper, v1 = min(voxels, v0 + vper);
-  const int lanes = 256 / coutp;   // coutp <= 256, power of two multiple of 32 here
+  const int lanes = 256 / coutp;   // coutp divides 256
   const int co = threadIdx.x % coutp, l = threadIdx.x / coutp;
   float s = 0.f;
   if (l < lanes)
@@ -524,8 +523,8 @@ __global__ void __launch_bounds__(256) wg_bias_kernel(const bf16* __restrict__ g
 struct WgPlan {
   int xm, N, Mreal, Mpad, TG, ngroups, mtiles, nsplit;
   long long ksteps, kper;
-  size_t xs_elems, gt_elems, part_floats;
-  uint32_t shared_bytes, pertap_bytes;
+  size_t m_elems, n_elems, part_floats;   // packed M operand (one copy), N operand (three copies)
+  uint32_t m_bytes, n_bytes;
 };
 
 bool wg_plan(int cin, int coutp, int Nb, int D, int H, int W, WgPlan& p) {
@@ -536,17 +535,16 @@ bool wg_plan(int cin, int coutp, int Nb, int D, int H, int W, WgPlan& p) {
   if (p.N > 256) return false;
   p.mtiles = (p.Mreal + 127) / 128;
   p.Mpad = p.mtiles * 128;
-  const uint32_t a_tile = 128u * WG_KV * 2u, b_tile = (uint32_t)p.N * WG_KV * 2u;
   auto r1k = [](uint32_t b) { return (b + 1023u) & ~1023u; };
-  p.shared_bytes = r1k(p.xm ? b_tile : a_tile);
-  p.pertap_bytes = r1k(p.xm ? a_tile : b_tile);
+  p.m_bytes = r1k(128u * WG_KV * 2u);
+  p.n_bytes = r1k((uint32_t)p.N * WG_KV * 2u);
   const uint32_t budget = 200u * 1024u / WG_STAGES;
-  int tg = (int)((budget - p.shared_bytes) / p.pertap_bytes);
+  int tg = (int)((budget - p.m_bytes) / p.n_bytes);
   tg = std::min(tg, 512 / p.N);
   tg = std::min(tg, 27);
   if (tg < 1) return false;
-  p.TG = tg;
   p.ngroups = (27 + tg - 1) / tg;
+  p.TG = (27 + p.ngroups - 1) / p.ngroups;   // balance the groups
   p.ksteps = (long long)Nb * D * H * (W / WG_KV);
   // about two CTAs per SM over the whole grid, at least 16 K steps per split
   const long long ctas = (long long)p.ngroups * p.mtiles;
@@ -555,8 +553,8 @@ bool wg_plan(int cin, int coutp, int Nb, int D, int H, int W, WgPlan& p) {
   p.kper = (p.ksteps + ns - 1) / ns;
   p.nsplit = (int)((p.ksteps + p.kper - 1) / p.kper);
   const long long vox = (long long)Nb * D * H * W;
-  p.xs_elems = (size_t)3 * (p.xm ? p.Mpad : cin) * vox;
-  p.gt_elems = (size_t)(p.xm ? coutp : p.Mpad) * vox;
+  p.m_elems = (size_t)p.Mpad * vox;
+  p.n_elems = (size_t)3 * p.N * vox;
   p.part_floats = (size_t)p.nsplit * 27 * cin * coutp + (size_t)p.nsplit * coutp;
   return true;
 }
@@ -658,7 +656,7 @@ extern "C" int mrb_cnn_conv3d_tc(const void* x, int cx, int ci_off, int cin, con
 
 // Scratch of mrb_cnn_conv3d_wgrad_tc: packed operands (BF16) then FP32 partials.
 static size_t wg_scratch_bytes(const WgPlan& p) {
-  size_t b = (p.xs_elems + p.gt_elems) * sizeof(bf16);
+  size_t b = (p.m_elems + p.n_elems) * sizeof(bf16);
   b = (b + 255) & ~(size_t)255;
   return b + p.part_floats * sizeof(float);
 }
@@ -688,41 +686,43 @@ extern "C" int mrb_cnn_conv3d_wgrad_tc(const void* x, int cx, int ci_off, int ci
   EncodeTiledFn enc = encode_fn();
   if (!enc) return mrb::fail(MRB_ECUDA, "cuTensorMapEncodeTiled unavailable");
   cudaStream_t st = (cudaStream_t)stream;
-  bf16* xs = (bf16*)scratch;
-  bf16* gt = xs + p.xs_elems;
-  float* part = (float*)(((uintptr_t)(gt + p.gt_elems) + 255) & ~(uintptr_t)255);
+  bf16* mpk = (bf16*)scratch;           // M operand, one copy, Mpad channels
+  bf16* npk = mpk + p.m_elems;          // N operand, three W-shifted copies
+  float* part = (float*)(((uintptr_t)(npk + p.n_elems) + 255) & ~(uintptr_t)255);
   float* bpart = part + (size_t)p.nsplit * 27 * cin * coutp;
-  const int xch = p.xm ? p.Mpad : cin, gch = p.xm ? coutp : p.Mpad;
-  // channels-first copies (x three times, shifted along W)
+  const bf16* msrc = (const bf16*)(p.xm ? x : gz);
+  const bf16* nsrc = (const bf16*)(p.xm ? gz : x);
+  const int ms = p.xm ? cx : cg, moff = p.xm ? ci_off : cg_off, mch = p.xm ? cin : coutp;
+  const int ns = p.xm ? cg : cx, noff = p.xm ? cg_off : ci_off;
   {
-    dim3 gx((unsigned)((W / PK_W) * ((xch + 31) / 32)), (unsigned)H, (unsigned)(Nb * D));
-    wg_pack_kernel<<<gx, 256, 0, st>>>((const bf16*)x, cx, ci_off, cin, xs, xch, 3, D, H, W);
+    dim3 gm((unsigned)((W / PK_W) * (p.Mpad / 32)), (unsigned)H, (unsigned)(Nb * D));
+    wg_pack_kernel<<<gm, 256, 0, st>>>(msrc, ms, moff, mch, mpk, p.Mpad, 1, D, H, W);
     MRB_LAUNCH_CHECK();
-    dim3 gg((unsigned)((W / PK_W) * ((gch + 31) / 32)), (unsigned)H, (unsigned)(Nb * D));
-    wg_pack_kernel<<<gg, 256, 0, st>>>((const bf16*)gz, cg, cg_off, coutp, gt, gch, 1, D, H, W);
+    dim3 gn((unsigned)((W / PK_W) * ((p.N + 31) / 32)), (unsigned)H, (unsigned)(Nb * D));
+    wg_pack_kernel<<<gn, 256, 0, st>>>(nsrc, ns, noff, p.N, npk, p.N, 3, D, H, W);
     MRB_LAUNCH_CHECK();
   }
-  // tensor maps: xs (W, H, D, xch, Nb*3), box {32, 1, 1, rows, 1}; gt (W, H, D, gch, Nb)
+  // tensor maps: M (W, H, D, Mpad, Nb), box {32, 1, 1, 128, 1}; N (W, H, D, N, Nb*3), box {32, 1, 1, N, 1}
   const cuuint64_t plane = (cuuint64_t)D * H * W;
-  CUtensorMap xmap, gmap;
+  CUtensorMap mmap, nmap;
   cuuint32_t es[5] = {1, 1, 1, 1, 1};
   {
-    cuuint64_t dims[5] = {(cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D, (cuuint64_t)xch, (cuuint64_t)Nb * 3};
-    cuuint64_t strd[4] = {(cuuint64_t)W * 2, (cuuint64_t)W * H * 2, plane * 2, plane * xch * 2};
-    cuuint32_t box[5] = {(cuuint32_t)WG_KV, 1, 1, (cuuint32_t)(p.xm ? 128 : p.N), 1};
-    CUresult r = enc(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, xs, dims, strd, box, es,
+    cuuint64_t dims[5] = {(cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D, (cuuint64_t)p.Mpad, (cuuint64_t)Nb};
+    cuuint64_t strd[4] = {(cuuint64_t)W * 2, (cuuint64_t)W * H * 2, plane * 2, plane * p.Mpad * 2};
+    cuuint32_t box[5] = {(cuuint32_t)WG_KV, 1, 1, 128, 1};
+    CUresult r = enc(&mmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, mpk, dims, strd, box, es,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return mrb::fail(MRB_ECUDA, "packed activation tensor map failed (%d)", (int)r);
+    if (r != CUDA_SUCCESS) return mrb::fail(MRB_ECUDA, "packed M-operand tensor map failed (%d)", (int)r);
   }
   {
-    cuuint64_t dims[5] = {(cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D, (cuuint64_t)gch, (cuuint64_t)Nb};
-    cuuint64_t strd[4] = {(cuuint64_t)W * 2, (cuuint64_t)W * H * 2, plane * 2, plane * gch * 2};
-    cuuint32_t box[5] = {(cuuint32_t)WG_KV, 1, 1, (cuuint32_t)(p.xm ? p.N : 128), 1};
-    CUresult r = enc(&gmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, gt, dims, strd, box, es,
+    cuuint64_t dims[5] = {(cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D, (cuuint64_t)p.N, (cuuint64_t)Nb * 3};
+    cuuint64_t strd[4] = {(cuuint64_t)W * 2, (cuuint64_t)W * H * 2, plane * 2, plane * p.N * 2};
+    cuuint32_t box[5] = {(cuuint32_t)WG_KV, 1, 1, (cuuint32_t)p.N, 1};
+    CUresult r = enc(&nmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, npk, dims, strd, box, es,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) return mrb::fail(MRB_ECUDA, "packed gradient tensor map failed (%d)", (int)r);
+    if (r != CUDA_SUCCESS) return mrb::fail(MRB_ECUDA, "packed N-operand tensor map failed (%d)", (int)r);
   }
   WgArgs a{};
   a.xm = p.xm;
@@ -742,14 +742,14 @@ extern "C" int mrb_cnn_conv3d_wgrad_tc(const void* x, int cx, int ci_off, int ci
   a.part = part;
   a.ncols = 32;
   while (a.ncols < p.TG * p.N) a.ncols <<= 1;
-  a.shared_bytes = p.shared_bytes;
-  a.pertap_bytes = p.pertap_bytes;
-  const size_t smem = WG_STAGES * (size_t)(p.shared_bytes + p.TG * p.pertap_bytes) + 1024;
+  a.m_bytes = p.m_bytes;
+  a.n_bytes = p.n_bytes;
+  const size_t smem = WG_STAGES * (size_t)(p.m_bytes + p.TG * p.n_bytes) + 1024;
   MRB_REQUIRE(smem <= 227 * 1024, "weight gradient stages need %zu bytes of shared memory", smem);
   MRB_CUDA_TRY(cudaFuncSetAttribute(wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const long long blocks = (long long)p.ngroups * p.mtiles * p.nsplit;
   MRB_REQUIRE(blocks < (1LL << 31), "volume too large");
-  wgrad_tc_kernel<<<(unsigned)blocks, TC_THREADS, smem, st>>>(xmap, gmap, a);
+  wgrad_tc_kernel<<<(unsigned)blocks, TC_THREADS, smem, st>>>(mmap, nmap, a);
   MRB_LAUNCH_CHECK();
   const long long nw = 27LL * cin * coutp;
   wg_sum_kernel<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(part, p.nsplit, nw, dw);
