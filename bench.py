@@ -113,6 +113,8 @@ def parse():
     ap.add_argument("--ncg-only", type=int, default=0, metavar="K",
                     help="profiling case: K eager iterations of the workload's plain NCG solver between "
                          "cudaProfilerStart/Stop")
+    ap.add_argument("--plan-option", action="append", default=[], metavar="KEY=VALUE",
+                    help="profiling cases: set a NUFFT plan option (mrb_plan_set_option key) before the runs")
     ap.add_argument("--koosh-only", type=int, default=0, metavar="N",
                     help="profiling case: the 3D koosh-ball operator scaled to an N^3 image (spokes x (N/160)^2, "
                          "samples per spoke x N/160, 16 coils), 3 forward/adjoint pairs")
@@ -327,13 +329,23 @@ def run_reference(args, w, ws, rank):
     return 0
 
 
-def run_nufft_only(w, local):
+def set_plan_options(plan, traj, options):
+    """KEY=VALUE strings -> mrb_plan_set_option; the sample lists are rebuilt if an option needs it."""
+    for kv in options:
+        k, v = kv.split("=")
+        plan.set_option(int(k), int(v))
+    if options and not plan.info()["points_ready"]:
+        plan.set_points(traj)
+
+
+def run_nufft_only(w, local, options=()):
     """Profiling case: the workload's operator, three A/A^H pairs, nothing else."""
     from mrirecon_b200.nufft import NUFFT, NUFFTConfig
     dev = torch.device("cuda", local)
     x_true, maps, traj = make_inputs(w)
     op = NUFFT(maps.to(dev), traj.to(dev), None, axis=axis_spec(), config=NUFFTConfig(ndim=2, traj_units="rad"),
                device=dev)
+    set_plan_options(op.backend.plan, traj.to(dev), options)
     x = x_true.to(dev)
     y = op.A(x)
     for _ in range(3):
@@ -783,7 +795,7 @@ def main():
         if args.impl == "reference":
             return run_reference(args, w, ws, rank)
         if args.nufft_only:
-            return run_nufft_only(w, local)
+            return run_nufft_only(w, local, args.plan_option)
         if args.koosh_only:
             return run_koosh_only(args.koosh_only, local)
         if args.ncg_only:
