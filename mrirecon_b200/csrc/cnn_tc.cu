@@ -386,13 +386,18 @@ __global__ void __launch_bounds__(TC_THREADS) wgrad_tc_kernel(const __grid_const
       }
     }
   } else if (warp == 1 && lane == 0) {
-    const uint32_t idesc = f16_idesc(128, a.N);
+    // the N tiles of consecutive taps are contiguous (N x 64 bytes each, whole
+    // swizzle atoms) and so are their accumulators (N TMEM columns each): up to
+    // 256 / N taps go into one MMA of N' = taps x N columns
+    const int ng = 256 / a.N;
     for (int ks = 0; ks < nk; ++ks) {
       const int st = ks % WG_STAGES;
       if (!mbar_wait(&full_bar[st], (ks / WG_STAGES) & 1, &abort_flag)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t sa = smem_u32(base + (size_t)st * stage_bytes);
-      for (int t = 0; t < ntap; ++t) {
+      for (int t = 0; t < ntap; t += ng) {
+        const int nt = min(ng, ntap - t);
+        const uint32_t idesc = f16_idesc(128, nt * a.N);
         const uint32_t sb = sa + a.m_bytes + (uint32_t)t * a.n_bytes;
 #pragma unroll
         for (int kk = 0; kk < WG_KV / 16; ++kk) {
@@ -537,7 +542,7 @@ bool wg_plan(int cin, int coutp, int Nb, int D, int H, int W, WgPlan& p) {
   p.Mpad = p.mtiles * 128;
   auto r1k = [](uint32_t b) { return (b + 1023u) & ~1023u; };
   p.m_bytes = r1k(128u * WG_KV * 2u);
-  p.n_bytes = r1k((uint32_t)p.N * WG_KV * 2u);
+  p.n_bytes = (uint32_t)p.N * WG_KV * 2u;   // N % 16 == 0: whole 1024-byte groups, tiles back to back
   const uint32_t budget = 200u * 1024u / WG_STAGES;
   int tg = (int)((budget - p.m_bytes) / p.n_bytes);
   tg = std::min(tg, 512 / p.N);
