@@ -769,6 +769,8 @@ def run_b200(args, w, ws, rank, local):
         line["koosh3d"] = k3
     if not args.no_tol_study:
         line["tolerance_study"] = tolerance_study(cnn, workload=args.workload, device=dev)
+        from mrirecon_b200.warmstart import training_step_time
+        line["warmstart_training_step"] = training_step_time(dev)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         times, cores, _ = cpu_reference_sample(w, args.cpu_sample_iters, 0)
         s_iter = sum(times) / max(1, len(times))

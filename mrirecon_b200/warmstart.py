@@ -118,6 +118,8 @@ class WarmStartCNN:
         # convolutions run on tcgen05 (tensor memory) where the shape allows,
         # on the warp-level mma.sync kernel otherwise
         self.use_tc = True
+        # weight gradients on tcgen05 too (mrb_cnn_conv3d_wgrad_tc) where the shape allows
+        self.use_tc_wgrad = True
         self.refresh()
 
     # -------------------------------------------------------------- parameters
@@ -261,7 +263,7 @@ class WarmStartCNN:
     # ---------------------------------------------------------------- training
     def _wgrad(self, name, x, cx, xoff, gz, cg, goff, vol, b):
         _, cinp, _, coutp, _, _ = next(l for l in LAYERS if l[0] == name)
-        if self.use_tc:
+        if self.use_tc and self.use_tc_wgrad:
             # tcgen05 weight gradient where the shape allows (scratch shared by all
             # layers of a batch shape, sized for the largest)
             nbytes = ct.c_int64(0)
@@ -539,6 +541,32 @@ def evaluate(cnn: "WarmStartCNN", workload: str = "grasp", device="cuda", reps: 
             "err_vs_plain": rel(x_warm, x_plain), "plain_err_vs_truth": rel(x_plain, xt),
             "warm_err_vs_truth": rel(x_warm, xt), "network_start_err_vs_plain": rel(x_net, x_plain),
             "adjoint_start_err_vs_plain": rel(x_adj, x_plain), **info}
+
+
+def training_step_time(device="cuda", batch: int = 2, frames: int = 8, N: int = 256, reps: int = 5) -> dict:
+    """Device milliseconds of one training step (forward, backward, Adam) of the
+    network on random series of the training shape (batch x frames x N x N), with
+    the weight gradients on tcgen05 and on the mma.sync kernel."""
+    dev = torch.device(device)
+    net = WarmStartCNN(dev, seed=0)
+    g = torch.Generator(device=dev).manual_seed(1)
+    z = torch.randn((batch, frames, N, N), dtype=torch.complex64, device=dev, generator=g)
+    t = z + 0.1 * torch.randn((batch, frames, N, N), dtype=torch.complex64, device=dev, generator=g)
+    out = {"shape": [batch, frames, N, N]}
+    for tc in (True, False):
+        net.use_tc_wgrad = tc
+        net.loss_and_grad(z, t)
+        net.adam_step(lr=1e-5)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        a.record()
+        for _ in range(reps):
+            net.loss_and_grad(z, t)
+            net.adam_step(lr=1e-5)
+        b.record()
+        torch.cuda.synchronize(dev)
+        out["step_ms_tc_wgrad" if tc else "step_ms_mma_wgrad"] = a.elapsed_time(b) / reps
+    return out
 
 
 def tolerance_study(cnn: "WarmStartCNN", tols=(1e-4, 3e-5, 1e-5, 3e-6, 1e-6), star_tol: float = 1e-8,
