@@ -422,15 +422,19 @@ __global__ void __launch_bounds__(COL_NT) fwd_cols_cg_kernel(const float2* __res
   const float2* tb = Tb + ((long long)be * C + c0) * g.S0 * G1 + k0;          // (coil, band row, column)
   // quad plane of coil c0 (4 coils x gtot cells), then (cell, coil in quad)
   float2* ob = out + ((long long)be * C + (c0 & ~3)) * g.gtot + (long long)k0 * 4 + (c0 & 3);
+  // 32-bit offsets inside one frame's band and quad (C * S0 * G1 and 4 * G0 * G1 < 2^31,
+  // checked on the host); a thread's (column, coil) pair is fixed across its elements
+  const int S0G1 = g.S0 * G1;
+  const bool full = k0 + CJ <= G1 && c0 + CG <= C;
   auto load0 = [&](int q, int n0) -> float2 {
     const int j = q % CJ, cc = q / CJ;
     const int r = n0 - g.off0;
-    if ((unsigned)r >= (unsigned)g.S0 || k0 + j >= G1 || c0 + cc >= C) return make_float2(0.f, 0.f);
-    return tb[((long long)cc * g.S0 + r) * G1 + j];
+    if ((unsigned)r >= (unsigned)g.S0 || (!full && (k0 + j >= G1 || c0 + cc >= C))) return make_float2(0.f, 0.f);
+    return tb[cc * S0G1 + r * G1 + j];
   };
   auto store = [&](int q, int n0, float2 v) {
     const int j = q % CJ, cc = q / CJ;
-    if (k0 + j < G1 && c0 + cc < C) ob[((long long)n0 * G1 + j) * 4 + cc] = v;
+    if (full || (k0 + j < G1 && c0 + cc < C)) ob[(n0 * G1 + j) * 4 + cc] = v;
   };
   fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
 }
@@ -723,6 +727,8 @@ int launch_cols_cg(const float2* in, float2* out, const float2* tw, const Geo2& 
   const size_t smem = (size_t)COLS * (G0 | 1) * sizeof(float2);
   const long long blocks = (long long)nb * ((g.C + CG - 1) / CG) * ((g.G1 + CJ - 1) / CJ);
   MRB_REQUIRE(blocks < (1LL << 31), "too many columns");
+  MRB_REQUIRE((long long)g.C * g.S0 * g.G1 < (1LL << 31) && 4LL * g.gtot < (1LL << 31),
+              "frame too large for the coil-quad column pass");
   int rc;
   if ((rc = set_smem((const void*)fwd_cols_cg_kernel<G0>, smem))) return rc;
   fwd_cols_cg_kernel<G0><<<(unsigned)blocks, COL_NT, smem, st>>>(in, out, tw, g);
