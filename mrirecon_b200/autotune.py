@@ -27,7 +27,7 @@ CANDIDATES_2D: Tuple[Tuple[int, int, int, int], ...] = (
     (16, 6, 128, 2), (16, 12, 128, 2), (16, 4, 128, 2))
 CANDIDATES_3D: Tuple[Tuple[int, int, int, int], ...] = (
     (8, 16, 4096, 1), (8, 8, 4096, 1), (8, 16, 1024, 1), (8, 8, 1024, 1), (8, 16, 16384, 1), (4, 4, 256, 0),
-    (4, 8, 256, 0))
+    (4, 8, 256, 0), (8, 16, 4096, 2), (8, 8, 4096, 2), (8, 16, 1024, 2))
 
 
 def _cache_path() -> str:

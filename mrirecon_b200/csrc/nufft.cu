@@ -1505,6 +1505,175 @@ __global__ void __launch_bounds__(S3_WARPS * 32) spread3_kernel(SpreadArgs a, Ge
   }
 }
 
+// 3D adjoint spread with shared staging for two coil groups and per-sample tap
+// tables (option key 6 = 2 in 3D).  One block per work item (8^3 tile, chunk,
+// up to 8 * NG coils) of NG x 8 warps: warp w owns tile plane w % 8 for coil
+// group w / 8 (4 pairs), so the staging of a batch (coordinates, 12 kernel
+// weights, the in-tile row and column of every tap, the coil values) is done
+// once for all 8 * NG coils instead of once per group of 8, and a lane task
+// reads its row and column from the tables instead of wrapping and testing
+// them.  With two groups the pair slots of odd cells are swapped between the
+// groups, so that the 128-bit updates of neighbouring cells by one warp land
+// in different bank halves.  Summation order per (cell, coil) and the weight
+// product are spread3_kernel's: identical grids.
+template <int NG>
+struct Spread3tSmem {
+  static constexpr int CELLS = S3_T * S3_T * S3_T;
+  static constexpr int PT = 4 * NG;     // coil pairs per cell
+  static constexpr int CPS = 2 * PT;    // float2 per cell
+  static constexpr size_t ACC = (size_t)CELLS * CPS * sizeof(float2);
+  static constexpr size_t TAB = S3_BATCH * (sizeof(int4) + 12 * sizeof(float) + 8);
+  static constexpr size_t BYTES = ACC + TAB + (size_t)S3_BATCH * CPS * sizeof(float2);
+};
+
+template <int NG>
+__global__ void __launch_bounds__(NG * S3_WARPS * 32) spread3t_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
+  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+  using SM = Spread3tSmem<NG>;
+  constexpr int T = S3_T;
+  constexpr int PPL = 4;                // pairs per warp group
+  constexpr int PT = SM::PT, CPS = SM::CPS;
+  constexpr int ROWS = (32 / PPL) / 4;  // a1 rows per lane pass (2)
+  extern __shared__ float4 smem4[];
+  float4* acc4 = smem4;                                             // [cell][pair slot]
+  int4* sb = reinterpret_cast<int4*>(reinterpret_cast<char*>(smem4) + SM::ACC);
+  float* sw = reinterpret_cast<float*>(sb + S3_BATCH);
+  signed char* st1 = reinterpret_cast<signed char*>(sw + S3_BATCH * 12);   // [sample][a1]: in-tile row or -1
+  signed char* st2 = st1 + S3_BATCH * 4;                                  // [sample][a2]: in-tile column or -1
+  float4* sy4 = reinterpret_cast<float4*>(reinterpret_cast<char*>(smem4) + SM::ACC + SM::TAB);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int plane = warp % S3_WARPS, grp = warp / S3_WARPS;
+  const long long item = blockIdx.x;
+  const int igrp = (int)(item % a.ngroups);
+  const long long oi = item / a.ngroups;
+  const int4 it = a.items[oi % a.n_items];
+  const int rep = (int)(oi / a.n_items);
+  const int b = it.x / tg.ntiles;
+  const int tile = it.x - b * tg.ntiles;
+  const int be = (g.B == 1) ? rep : b * (a.nb / g.B) + rep;
+  const int c0 = igrp * a.cpi;
+  const int nc = min(a.cpi, g.C - c0);
+  const int o2 = (tile % tg.nt[2]) * T;
+  const int o1 = ((tile / tg.nt[2]) % tg.nt[1]) * T;
+  const int o0 = (tile / (tg.nt[2] * tg.nt[1])) * T;
+  const int k0 = a.tile_start[it.x], k1 = a.tile_start[it.x + 1];
+  const int e0 = min(k1, k0 + it.y * a.chunk), e1 = min(k1, e0 + a.chunk);
+  constexpr int TN = T * T * T;
+  float2* pout = it.z >= 0 ? a.partials + (((long long)rep * a.n_slots + it.z) * g.C + c0) * TN : nullptr;
+
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = threadIdx.x; i < SM::CELLS * PT; i += blockDim.x) acc4[i] = z4;
+
+  const int P0 = o0 + plane;
+  const int p = lane % PPL, q = lane / PPL;
+  const int pg = grp * PPL + p;                 // this lane's pair within the block's coils
+  const bool pair_ok = pg < (nc + 1) / 2;
+  const int a2 = q & 3, arow = q >> 2;
+  const float* gxp = a.gx + (long long)b * 3 * g.K;
+  const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
+  for (int e = e0; e < e1; e += S3_BATCH) {
+    const int nbat = min(S3_BATCH, e1 - e);
+    __syncthreads();   // previous batch consumed (and the zero fill done)
+    // stage: (sample, dim) weights and, for dims 1 and 2, the in-tile node of each tap
+    for (int i = threadIdx.x; i < nbat * 3; i += blockDim.x) {
+      const int j = i / 3, d = i - 3 * j;
+      const int k = a.entries[e + j];
+      const float x = gxp[(long long)d * g.K + k];
+      const int base = (int)floorf(x) - 1;
+      float ws = 1.f;
+      if (d == 0) {
+        ws = a.gsign;
+        if (a.wadj) ws *= a.wadj[(long long)b * g.K + k];
+      }
+      const float fx = x - (float)(base + 1);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int n = base + t;
+        float w = mrb::kb_tap(kb, t, fx);
+        if (n & 1) w = -w;
+        sw[j * 12 + d * 4 + t] = w * ws;
+        if (d > 0) {
+          int nn = n;
+          nn += nn < 0 ? g.G[d] : 0;
+          nn -= nn >= g.G[d] ? g.G[d] : 0;
+          const int l = nn - (d == 1 ? o1 : o2);
+          (d == 1 ? st1 : st2)[j * 4 + t] = (signed char)((unsigned)l < (unsigned)T ? l : -1);
+        }
+      }
+      reinterpret_cast<int*>(sb + j)[d] = base;
+    }
+    for (int i = threadIdx.x; i < S3_BATCH * CPS; i += blockDim.x) {
+      const int j = i % S3_BATCH, c = i / S3_BATCH;   // lanes along the sample list
+      float2 v = make_float2(0.f, 0.f);
+      if (j < nbat && c < nc) v = yb[(long long)c * g.K + a.entries[e + j]];
+      const int slot = (c >> 1) ^ (j & (PT - 1));
+      reinterpret_cast<float2*>(sy4 + j * PT + slot)[c & 1] = v;
+    }
+    __syncthreads();
+    if (P0 >= g.G[0]) continue;   // plane beyond a partial last tile: nothing lands here
+    for (int h = 0; h < nbat; h += 32) {
+      int myd0 = 4;
+      if (h + lane < nbat) {
+        myd0 = P0 - sb[h + lane].x;
+        myd0 += myd0 < 0 ? g.G[0] : 0;
+        myd0 -= myd0 >= g.G[0] ? g.G[0] : 0;
+      }
+      unsigned todo = __ballot_sync(0xffffffffu, myd0 < 4);
+      while (todo) {
+        const int jl = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const int j = h + jl;
+        const int d0 = __shfl_sync(0xffffffffu, myd0, jl);
+        const int l2 = st2[j * 4 + a2];
+        const float* wj = sw + j * 12;
+        const float w0 = wj[d0], w2 = wj[8 + a2];
+        const float4 v = sy4[j * PT + (pg ^ (j & (PT - 1)))];
+#pragma unroll
+        for (int r = 0; r < 4 / ROWS; ++r) {
+          const int a1 = r * ROWS + arow;
+          const int l1 = st1[j * 4 + a1];
+          if (pair_ok && l2 >= 0 && l1 >= 0) {
+            const float w = w0 * wj[4 + a1] * w2;   // the per-warp kernel's product order
+            const int cell = (plane * T + l1) * T + l2;
+            const int slot = NG == 2 ? (pg ^ ((cell & 1) << 2)) : pg;
+            float4* c4 = acc4 + cell * PT + slot;
+            float4 t = *c4;
+            t.x = fmaf(w, v.x, t.x);
+            t.y = fmaf(w, v.y, t.y);
+            t.z = fmaf(w, v.z, t.z);
+            t.w = fmaf(w, v.w, t.w);
+            *c4 = t;
+          }
+        }
+        __syncwarp();
+      }
+    }
+  }
+  __syncthreads();
+  // write-out: lanes (coil, cell pair along l2) read whole cells from shared
+  // memory; each coil row gets 32-byte pieces
+  const float2* acc = reinterpret_cast<const float2*>(acc4);
+  float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
+  for (int i = threadIdx.x; i < (TN / 2) * CPS; i += blockDim.x) {
+    const int c = i % CPS, r = i / CPS;   // r: cell pair
+    if (c >= nc) continue;
+    const int cl = 2 * r;                  // local cell (l0, l1, l2 even)
+    const int s0 = NG == 2 ? ((c >> 1) ^ ((cl & 1) << 2)) : (c >> 1);
+    const int s1 = NG == 2 ? ((c >> 1) ^ (((cl + 1) & 1) << 2)) : (c >> 1);
+    const float2 u0 = acc[cl * CPS + 2 * s0 + (c & 1)], u1 = acc[(cl + 1) * CPS + 2 * s1 + (c & 1)];
+    const float4 v = make_float4(u0.x, u0.y, u1.x, u1.y);
+    if (pout) {
+      *reinterpret_cast<float4*>(pout + (long long)c * TN + cl) = v;
+    } else {
+      const int l0 = cl / (T * T), l1 = (cl / T) % T, l2 = cl % T;
+      const int n0 = o0 + l0, n1 = o1 + l1, n2 = o2 + l2;
+      if (n0 < g.G[0] && n1 < g.G[1] && n2 < g.G[2])
+        *reinterpret_cast<float4*>(gout + (long long)c * g.gtot + ((long long)n0 * g.G[1] + n1) * g.G[2] + n2) = v;
+    }
+  }
+}
+
 // 2D adjoint spread, one block per work item (16x16 tile, chunk of its sample
 // list, group of up to 16 coils): the 2D counterpart of spread3_kernel.  Warp
 // w owns tile rows 2w and 2w+1; lanes are (coil pair p, tap column a1) and a
@@ -2545,7 +2714,8 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     a.touch = masked ? p->touch.as<unsigned>() : nullptr;
     a.twords = p->twords;
     a.grid = adj_grid(p);
-    const bool blk3 = p->spread_kernel == 1 && p->nd == 3 && tg.T == S3_T;   // block-per-tile kernels
+    const bool blk3t = p->spread_kernel == 2 && p->nd == 3 && tg.T == S3_T;  // shared-staging 3D kernel
+    const bool blk3 = (p->spread_kernel == 1 || blk3t) && p->nd == 3 && tg.T == S3_T;   // block-per-tile kernels
     const bool blk2 = p->spread_kernel == 1 && p->nd == 2 && tg.T == S2_T;
     a.cpi = blk3 || blk2 ? std::min(std::min(p->C, S3_CPB), p->coils_per_item) : p->coils_per_item;
     a.ngroups = (p->C + a.cpi - 1) / a.cpi;
@@ -2556,7 +2726,17 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     const void* fn = nullptr;
     size_t smem = 0;
     int threads = SPREAD_WARPS * 32;
-    if (blk3) {
+    if (blk3t) {
+      if (a.cpi > 8) {
+        fn = (const void*)spread3t_kernel<2>;
+        smem = Spread3tSmem<2>::BYTES;
+        threads = 2 * S3_WARPS * 32;
+      } else {
+        fn = (const void*)spread3t_kernel<1>;
+        smem = Spread3tSmem<1>::BYTES;
+        threads = S3_WARPS * 32;
+      }
+    } else if (blk3) {
       const int pairs = (a.cpi + 1) / 2;
       threads = S3_WARPS * 32;
       if (pairs <= 2) {
@@ -2716,7 +2896,8 @@ extern "C" int mrb_nufft_stage(mrb_plan* p, int stage, const void* x, void* y, i
 
 extern "C" int mrb_plan_info(mrb_plan* p, int64_t* out, int nout) {
   MRB_REQUIRE(p != nullptr && out != nullptr, "null plan or output");
-  const int blk = p->spread_kernel == 1 && ((p->nd == 2 && p->tile == S2_T) || (p->nd == 3 && p->tile == S3_T));
+  const int blk = (p->spread_kernel == 1 && ((p->nd == 2 && p->tile == S2_T) || (p->nd == 3 && p->tile == S3_T))) ||
+                  (p->spread_kernel == 2 && p->nd == 3 && p->tile == S3_T);
   int64_t v[10] = {p->n_entries, p->ntiles,  p->touched, p->tile, p->coils_per_item, p->gtot(), p->fft_mode, blk,
                    col_interp_active(p), p->have_points ? 1 : 0};
   for (int i = 0; i < nout && i < 10; ++i) out[i] = v[i];

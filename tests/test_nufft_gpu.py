@@ -333,6 +333,25 @@ def test_3d_block_spread_matches_warp_kernel(cuda):
     assert torch.equal(out, ad.AH(y))
 
 
+@pytest.mark.parametrize("C,cpi,chunk,nb", [(16, 16, None, 1), (16, 16, 64, 2), (12, 16, None, 2), (20, 16, 128, 1),
+                                            (5, 8, None, 1), (8, 8, 32, 2), (16, 8, None, 1)])
+def test_3d_shared_staging_spread_identical(cuda, C, cpi, chunk, nb):
+    """The 3D spread with shared staging and tap tables (option key 6 = 2; one
+    block of 16 warps serves two coil groups of 8 when the coils per item exceed
+    8, swapped pair slots on odd cells) gives the block kernel's grid bit for bit:
+    partial second groups, split tiles, several coil groups per tile."""
+    S = (16, 12, 20)
+    maps = _rand_c((C,) + S, 41, torch.complex64)
+    traj = phantoms.golden_means_koosh(120, 32).unsqueeze(0)
+    y = _rand_c((nb, C, traj.shape[-1]), 42, torch.complex64).to(cuda)
+    ad = _adapter(maps, traj, tile=8, chunk=chunk, coils_per_item=cpi)
+    ad.plan.set_option(6, 1)
+    x1 = ad.AH(y)
+    ad.plan.set_option(6, 2)
+    assert ad.plan.info()["block_spread"] == 1
+    assert torch.equal(ad.AH(y), x1)
+
+
 @pytest.mark.parametrize("C,chunk,nb", [(12, None, 2), (12, 16, 2), (3, 32, 1), (7, None, 2), (20, 64, 2)])
 def test_2d_block_spread_identical_to_warp_kernel(cuda, C, chunk, nb):
     """The block-per-tile 2D spread (tile 16: 2, 4 or 8 coil pairs per lane
