@@ -113,6 +113,8 @@ def parse():
     ap.add_argument("--ncg-only", type=int, default=0, metavar="K",
                     help="profiling case: K eager iterations of the workload's plain NCG solver between "
                          "cudaProfilerStart/Stop")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only the 16-instance uneven batch block (grouped, branch and sequential solves)")
     ap.add_argument("--plan-option", action="append", default=[], metavar="KEY=VALUE",
                     help="profiling cases: set a NUFFT plan option (mrb_plan_set_option key) before the runs")
     ap.add_argument("--koosh-only", type=int, default=0, metavar="N",
@@ -455,9 +457,10 @@ def koosh3d_throughput(dev, reps=10):
 
 
 def batched_throughput(dev, steps=3):
-    """16 uneven independent 2D radial recons to tolerance: all instances in one
-    CUDA graph (parallel branches) against the same solves run one after another
-    (each with its own graph), device seconds per batch."""
+    """16 uneven independent 2D radial recons to tolerance, device seconds per
+    batch: grouped launches (one launch per kernel step over all instances of a
+    kernel shape, captured in one CUDA graph), one graph branch per instance,
+    and the same solves run one after another (each with its own graph)."""
     from mrirecon_b200.batched import BatchedSolver
     from mrirecon_b200.solver import CGSolver
     from mrirecon_b200.workloads import BATCHED, batched_instances
@@ -466,22 +469,29 @@ def batched_throughput(dev, steps=3):
     # densely sampled instances overshoot on the first Armijo step and the first
     # FR update (beta = 1) then gives a non-descent direction: restart instead of stopping
     cfg.restart = True
-    bs = BatchedSolver([(p["y"], p["op"], p["regm"]) for p in inst], cfg)
+    probs = [(p["y"], p["op"], p["regm"]) for p in inst]
+    bs = BatchedSolver(probs, cfg, grouped=True)
+    br = BatchedSolver(probs, cfg, grouped=False)
     seq = [CGSolver(p["y"], p["op"], p["regm"], cfg) for p in inst]
     bs.reset().run()
+    br.reset().run()
     for s in seq:
         s.reset().run()
     ev = lambda: torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    a, b = ev(), ev()
-    l0 = bs.launches()
-    a.record()
-    for _ in range(steps):
-        bs.reset().run()
-    b.record()
-    torch.cuda.synchronize()
-    t_b = a.elapsed_time(b) / 1e3 / steps
-    launches = (bs.launches() - l0) // steps
+
+    def timed(solver):
+        torch.cuda.synchronize()
+        a, b = ev(), ev()
+        l0 = solver.launches()
+        a.record()
+        for _ in range(steps):
+            solver.reset().run()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / 1e3 / steps, (solver.launches() - l0) // steps
+
+    t_b, launches = timed(bs)
+    t_r, launches_r = timed(br)
     a, b = ev(), ev()
     a.record()
     for _ in range(steps):
@@ -491,8 +501,12 @@ def batched_throughput(dev, steps=3):
     torch.cuda.synchronize()
     t_s = a.elapsed_time(b) / 1e3 / steps
     same = all(torch.equal(x, s.result()) for x, s in zip(bs.results(), seq))
+    same_r = all(torch.equal(x, s.result()) for x, s in zip(br.results(), seq))
     return {"workload": BATCHED["name"], "batched_graph_s": t_b, "sequential_s": t_s, "speedup": t_s / t_b,
+            "mode": "grouped launches (one per kernel step and kernel shape, all instances), one CUDA graph",
             "gpu_launches_per_batch": launches, "identical_to_sequential": bool(same),
+            "branch_graph_s": t_r, "branch_gpu_launches_per_batch": launches_r,
+            "branch_identical_to_sequential": bool(same_r),
             "solver": "plain NCG FR+Armijo (fast schedule) with restart on non-descent",
             "instances": [{"N": p["N"], "coils": p["C"], "spokes": p["spokes"], "iters": s.iter,
                            "restarts": s.restarts, "stop": s.stop_reason} for p, s in zip(inst, bs.solvers)]}
@@ -804,6 +818,9 @@ def main():
             return run_koosh_only(args.koosh_only, local)
         if args.ncg_only:
             return run_ncg_only(w, args.ncg_only, local)
+        if args.batched_only:
+            print(json.dumps({"batched16": batched_throughput(torch.device("cuda", local))}))
+            return 0
         return run_b200(args, w, ws, rank, local)
     finally:
         if ws > 1:

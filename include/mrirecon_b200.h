@@ -54,6 +54,36 @@ int64_t mrb_launch_count(void);
 int mrb_release_cached_memory(void);
 
 /* ------------------------------------------------------------------------
+ * Grouped launches: many independent problems, one launch per kernel step
+ *
+ * Between mrb_group_begin(n) and mrb_group_end(stream) the entry points of
+ * this library record their kernel launches instead of issuing them, each
+ * into the list of the problem last chosen with mrb_group_select(i).  Their
+ * stream arguments are ignored; device pointers and scalars are taken at the
+ * call (device memory a call allocates is allocated then).
+ * mrb_group_end issues the records on `stream` in steps: each step launches
+ * the next record of every problem whose next record runs the same kernel as
+ * ONE grouped launch (a table of the problems' arguments in kernel parameter
+ * space, every block finding its problem and its own block coordinates there),
+ * so each problem computes bit for bit what its own launches compute, in the
+ * order it made them.  Problems must not share device buffers they write.
+ * Inside a stream capture the grouped launches become the graph's nodes.
+ * Entry points whose kernels have no grouped form fail inside a recording
+ * (MRB_ESTATE): the 2D NUFFT in the fused FFT mode, the NCG kernels, the TV
+ * passes and graph passes have one; the cuFFT mode, the 3D block spreads,
+ * the Toeplitz column pass, the dots and the preconditioner set-up do not.
+ * One recording per process at a time.  mrb_group_cancel drops an open
+ * recording; mrb_group_stats returns the records and launches of the last
+ * mrb_group_end.
+ * The reference solves one problem per CGSolver call
+ * (graspcg/solvers/cg.py:162-246); this interface has no counterpart there. */
+int mrb_group_begin(int nproblems);
+int mrb_group_select(int problem);
+int mrb_group_end(mrb_stream_t stream);
+int mrb_group_cancel(void);
+int mrb_group_stats(int64_t* records, int64_t* launches);
+
+/* ------------------------------------------------------------------------
  * NUFFT plan (Kaiser-Bessel, oversampled grid, SENSE coils, B frames)
  * ---------------------------------------------------------------------- */
 

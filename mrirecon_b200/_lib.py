@@ -44,6 +44,11 @@ _SIGS = {
     "mrb_last_error": (ct.c_char_p, []),
     "mrb_launch_count": (ct.c_int64, []),
     "mrb_release_cached_memory": (ct.c_int, []),
+    "mrb_group_begin": (ct.c_int, [ct.c_int]),
+    "mrb_group_select": (ct.c_int, [ct.c_int]),
+    "mrb_group_end": (ct.c_int, [ct.c_void_p]),
+    "mrb_group_cancel": (ct.c_int, []),
+    "mrb_group_stats": (ct.c_int, [c_int64_p, c_int64_p]),
     "mrb_nufft_stage": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p]),
     "mrb_plan_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, c_int_p, ct.c_int, ct.c_int, ct.c_int64,
                                    ct.c_int, ct.c_double, ct.c_int]),

@@ -3,19 +3,34 @@
 Each instance keeps its own NUFFT plan (grid, band buffer, spread tile/bin
 sizes autotuned per size class), its own NCG state, FP64 reduction scratch and
 device-side controller, so every instance follows exactly the iterations it
-would follow alone.  One CUDA graph holds `iters_per_graph` NCG iterations of
-every instance as parallel branches: the graph forks from the capture stream to
-one stream per instance and joins back, so the GPU runs the instances' kernels
-concurrently and one graph launch advances every solve.  An instance that has
-met its stop rule sets its device done flag; from then on its operator kernels
-return at once (plan skip flag) and its controller and update kernels leave the
-state unchanged, so replays continue until the last instance stops.
+would follow alone.  An instance that has met its stop rule sets its device
+done flag; from then on its operator kernels return at once (plan skip flag)
+and its controller and update kernels leave the state unchanged, so the solve
+continues until the last instance stops.
 
+Grouped mode (the default): one NCG iteration of every instance is recorded
+through the library's launch recorder (mrb_group_begin / mrb_group_select /
+mrb_group_end) and issued as grouped launches: each kernel step of the
+iteration (row FFTs, column FFTs, interp, k-space pass, spread, split-tile
+reduction, inverse passes, TV energies and gradient, Armijo, controller,
+update, restart) is ONE launch over all instances, whose blocks find their
+instance and its arguments in a table in kernel parameter space.  Instances
+that differ in a kernel's compile-time shape (the FFT length of their size
+class, the spread tile and variant) take one launch per shape.
+`iters_per_graph` iterations of these launches are captured in one CUDA graph.
+
+Branch mode (grouped=False): the graph forks from the capture stream to one
+stream per instance and joins back; every instance issues its own launches.
+It serves the paths without grouped kernels (Toeplitz normal operator, cuFFT
+mode, 3D block spreads).
+
+Both modes are bit-identical to solving the instances one after another.
 The reference solves one problem per CGSolver call (graspcg/solvers/cg.py:162-246);
 this module has no counterpart there.
 """
 from __future__ import annotations
 
+import ctypes as ct
 from typing import List, Optional, Sequence, Tuple
 
 import torch
@@ -27,7 +42,8 @@ from .solver import CGConfig, CGSolver, REASONS, S_DONE, S_ITER, S_REASON, captu
 class BatchedSolver:
     """Solve `problems` = [(y, op, regm), ...] with one CGConfig, all in one graph."""
 
-    def __init__(self, problems: Sequence[Tuple[torch.Tensor, object, object]], cfg: Optional[CGConfig] = None):
+    def __init__(self, problems: Sequence[Tuple[torch.Tensor, object, object]], cfg: Optional[CGConfig] = None,
+                 grouped: bool = True):
         if len(problems) == 0:
             raise ValueError("no problems")
         self.cfg = cfg or CGConfig()
@@ -42,6 +58,8 @@ class BatchedSolver:
         self.device = self.solvers[0].device
         if any(s.device != self.device for s in self.solvers):
             raise ValueError("all instances must live on one device")
+        self.grouped = bool(grouped)
+        self.lib = _lib.load()
         self.streams = [torch.cuda.Stream(self.device) for _ in self.solvers]
         self._graph = None
         self._done = torch.zeros(len(self.solvers), dtype=torch.float64, device=self.device)
@@ -61,6 +79,33 @@ class BatchedSolver:
         for st in self.streams:
             main.wait_stream(st)
 
+    def _record(self, fn):
+        """fn(s) for every instance inside one recording; the recorded kernel
+        launches are issued as grouped launches on the current stream."""
+        lib = self.lib
+        _lib.check(lib.mrb_group_begin(len(self.solvers)), "group_begin")
+        try:
+            for i, s in enumerate(self.solvers):
+                _lib.check(lib.mrb_group_select(i), "group_select")
+                fn(s)
+        except BaseException:
+            lib.mrb_group_cancel()
+            raise
+        _lib.check(lib.mrb_group_end(_lib.stream_ptr(self.device)), "group_end")
+
+    def _step(self, fn):
+        """fn(s) for every instance: grouped launches or one stream per instance."""
+        if self.grouped:
+            self._record(fn)
+        else:
+            self._fork(fn)
+
+    def group_stats(self) -> Tuple[int, int]:
+        """(records, launches) of the last grouped step."""
+        r, l = ct.c_int64(0), ct.c_int64(0)
+        _lib.check(self.lib.mrb_group_stats(ct.byref(r), ct.byref(l)), "group_stats")
+        return int(r.value), int(l.value)
+
     def _all_done(self) -> bool:
         torch.stack([s.s[S_DONE] for s in self.solvers], out=self._done)
         return bool(self._done.min().item() != 0.0)
@@ -79,8 +124,8 @@ class BatchedSolver:
                 def first(s):
                     s._prime_fast()
                     s._skip_on_done(True)
-                    s._iteration_fast()
                 self._fork(first)
+                self._step(lambda s: s._iteration_fast())
                 self.launch_stats["eager"] += _lib.launch_count() - n0
                 if not self._all_done():
                     if c.cuda_graph and self._graph is None:
@@ -88,10 +133,8 @@ class BatchedSolver:
                         g = torch.cuda.CUDAGraph()
                         n1 = _lib.launch_count()
                         with capture_graph(g, self.device):
-                            def body(s):
-                                for _ in range(max(1, c.iters_per_graph)):
-                                    s._iteration_fast()
-                            self._fork(body)
+                            for _ in range(max(1, c.iters_per_graph)):
+                                self._step(lambda s: s._iteration_fast())
                         self.launch_stats["per_graph"] = _lib.launch_count() - n1
                         self._graph = g
                     while not self._all_done():
@@ -100,7 +143,8 @@ class BatchedSolver:
                             self.launch_stats["replays"] += 1
                         else:
                             n2 = _lib.launch_count()
-                            self._fork(lambda s: [s._iteration_fast() for _ in range(max(1, c.iters_per_graph))])
+                            for _ in range(max(1, c.iters_per_graph)):
+                                self._step(lambda s: s._iteration_fast())
                             self.launch_stats["eager"] += _lib.launch_count() - n2
             finally:
                 for s in self.solvers:

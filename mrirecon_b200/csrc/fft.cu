@@ -36,8 +36,12 @@
 
 #include "mrb_common.cuh"
 #include "fft.cuh"
+#include "group.cuh"
 
 namespace {
+
+using mrb::VBlock;
+using mrb::hw_block;
 
 constexpr int ROW_NT = 256;   // threads per row-pass block
 constexpr int COL_NT = 512;   // threads per column-pass block
@@ -114,12 +118,22 @@ std::vector<float2> host_twiddles(int G) {
 
 // ---------------------------------------------------------------------------
 // small DFTs: X_k = sum_n u_n e^{DIR 2 pi i k n / R}, in place
+//
+// Every floating-point operation of the passes is written with its rounding
+// stated (fmaf, __fmul_rn, __fadd_rn, __fsub_rn), so the compiler fuses no
+// multiply into an add on its own: a pass computes the same bits in every
+// kernel that contains it (the named kernels and their grouped forms).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  return make_float2(fmaf(a.x, b.x, -__fmul_rn(a.y, b.y)), fmaf(a.x, b.y, __fmul_rn(a.y, b.x)));
 }
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+  return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+  return make_float2(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y));
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(__fmul_rn(a.x, s), __fmul_rn(a.y, s)); }
 template <int DIR>
 __device__ __forceinline__ float2 cmul_di(float2 a) {   // a * (DIR i)
   return DIR > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
@@ -158,11 +172,10 @@ struct Dft<8, DIR> {
     Dft<4, DIR>::run(e);
     Dft<4, DIR>::run(o);
     const float h = 0.707106781186547524f;
-    const float d = (float)DIR;
-    // o_k * e^{DIR i pi k / 4}
-    const float2 o1 = make_float2(h * (o[1].x - d * o[1].y), h * (o[1].y + d * o[1].x));
+    // o_k * e^{DIR i pi k / 4}: o1 = h (o + DIR i o), o3 = h (DIR i o - o)
+    const float2 o1 = cscale(cadd(o[1], cmul_di<DIR>(o[1])), h);
     const float2 o2 = cmul_di<DIR>(o[2]);
-    const float2 o3 = make_float2(h * (-o[3].x - d * o[3].y), h * (-o[3].y + d * o[3].x));
+    const float2 o3 = cscale(csub(cmul_di<DIR>(o[3]), o[3]), h);
     u[0] = cadd(e[0], o[0]);
     u[4] = csub(e[0], o[0]);
     u[1] = cadd(e[1], o1);
@@ -179,8 +192,8 @@ struct Dft<3, DIR> {
   __device__ __forceinline__ static void run(float2* u) {
     const float c1 = -0.5f, s1 = 0.866025403784438647f * (float)DIR;
     const float2 t1 = cadd(u[1], u[2]), t2 = csub(u[1], u[2]);
-    const float2 m = make_float2(u[0].x + c1 * t1.x, u[0].y + c1 * t1.y);
-    const float2 r = make_float2(-s1 * t2.y, s1 * t2.x);
+    const float2 m = make_float2(fmaf(c1, t1.x, u[0].x), fmaf(c1, t1.y, u[0].y));
+    const float2 r = make_float2(__fmul_rn(-s1, t2.y), __fmul_rn(s1, t2.x));
     u[0] = cadd(u[0], t1);
     u[1] = cadd(m, r);
     u[2] = csub(m, r);
@@ -196,10 +209,10 @@ struct Dft<5, DIR> {
     const float2 a1 = cadd(u[1], u[4]), b1 = csub(u[1], u[4]);
     const float2 a2 = cadd(u[2], u[3]), b2 = csub(u[2], u[3]);
     const float2 x0 = u[0];
-    const float2 m1 = make_float2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
-    const float2 m2 = make_float2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
-    const float2 n1 = make_float2(-(s1 * b1.y + s2 * b2.y), s1 * b1.x + s2 * b2.x);
-    const float2 n2 = make_float2(-(s2 * b1.y - s1 * b2.y), s2 * b1.x - s1 * b2.x);
+    const float2 m1 = make_float2(fmaf(c2, a2.x, fmaf(c1, a1.x, x0.x)), fmaf(c2, a2.y, fmaf(c1, a1.y, x0.y)));
+    const float2 m2 = make_float2(fmaf(c1, a2.x, fmaf(c2, a1.x, x0.x)), fmaf(c1, a2.y, fmaf(c2, a1.y, x0.y)));
+    const float2 n1 = make_float2(-fmaf(s2, b2.y, __fmul_rn(s1, b1.y)), fmaf(s2, b2.x, __fmul_rn(s1, b1.x)));
+    const float2 n2 = make_float2(-fmaf(-s1, b2.y, __fmul_rn(s2, b1.y)), fmaf(-s1, b2.x, __fmul_rn(s2, b1.x)));
     u[0] = cadd(x0, cadd(a1, a2));
     u[1] = cadd(m1, n1);
     u[4] = csub(m1, n1);
@@ -296,65 +309,80 @@ struct Geo2 {
 constexpr int ROW_WARPS = ROW_NT / 32;
 
 template <int G1>
-__global__ void __launch_bounds__(ROW_NT) fwd_rows_kernel(const float2* __restrict__ x, const float2* __restrict__ maps,
-                                                          const float* __restrict__ rowfac,
-                                                          const float* __restrict__ coldeap, float2* __restrict__ Tb,
-                                                          const float2* __restrict__ tw, Geo2 g, long long nrows,
-                                                          int coil_images) {
-  constexpr int LD = row_ld(G1);
-  extern __shared__ float2 sm[];
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  const int warp = threadIdx.x >> 5;
-  const long long row = (long long)blockIdx.x * ROW_WARPS + warp;
-  if (row >= nrows) return;                          // no block-wide barrier below
-  float2* buf = sm + warp * LD;
-  const long long vol = row / g.S0;
-  const int r = (int)(row - vol * g.S0);
-  const long long be = vol / g.C;
-  const int c = (int)(vol - be * g.C);
-  const float2* xr = x + (coil_images ? vol : be) * g.stot + (long long)r * g.S1;
-  const float2* mr = maps + (long long)c * g.stot + (long long)r * g.S1;
-  const float dr = __ldg(rowfac + r);   // signed deapodisation of the row
-  float2* out = Tb + row * G1;
-  auto load0 = [&](int, int n1) -> float2 {
-    const int i1 = n1 - g.off1;
-    if ((unsigned)i1 >= (unsigned)g.S1) return make_float2(0.f, 0.f);
-    const float2 xv = xr[i1];
-    const float2 mv = coil_images ? make_float2(1.f, 0.f) : __ldg(mr + i1);
-    float s = dr * __ldg(coldeap + i1);
-    if (n1 & 1) s = -s;
-    return make_float2((xv.x * mv.x - xv.y * mv.y) * s, (xv.x * mv.y + xv.y * mv.x) * s);
-  };
-  auto store = [&](int, int k1, float2 v) { out[k1] = v; };
-  fft_stages<G1, 0, 1, 32, -1, false, true, LD, true>(buf, tw, load0, store);
+struct FwdRows {
+  static constexpr int NT = ROW_NT, MINB = (G1 <= 256 ? 5 : G1 <= 384 ? 4 : G1 <= 640 ? 3 : G1 <= 768 ? 2 : 1);
+  static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ x,
+      const float2* __restrict__ maps, const float* __restrict__ rowfac, const float* __restrict__ coldeap,
+      float2* __restrict__ Tb, const float2* __restrict__ tw, const Geo2& g, long long nrows, int coil_images) {
+    constexpr int LD = row_ld(G1);
+    extern __shared__ float2 sm[];
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    const int warp = threadIdx.x >> 5;
+    const long long row = (long long)vb.x * ROW_WARPS + warp;
+    if (row >= nrows) return;                          // no block-wide barrier below
+    float2* buf = sm + warp * LD;
+    const long long vol = row / g.S0;
+    const int r = (int)(row - vol * g.S0);
+    const long long be = vol / g.C;
+    const int c = (int)(vol - be * g.C);
+    const float2* xr = x + (coil_images ? vol : be) * g.stot + (long long)r * g.S1;
+    const float2* mr = maps + (long long)c * g.stot + (long long)r * g.S1;
+    const float dr = __ldg(rowfac + r);   // signed deapodisation of the row
+    float2* out = Tb + row * G1;
+    auto load0 = [&](int, int n1) -> float2 {
+      const int i1 = n1 - g.off1;
+      if ((unsigned)i1 >= (unsigned)g.S1) return make_float2(0.f, 0.f);
+      const float2 xv = xr[i1];
+      const float2 mv = coil_images ? make_float2(1.f, 0.f) : __ldg(mr + i1);
+      float s = __fmul_rn(dr, __ldg(coldeap + i1));
+      if (n1 & 1) s = -s;
+      return cscale(cmul(xv, mv), s);
+    };
+    auto store = [&](int, int k1, float2 v) { out[k1] = v; };
+    fft_stages<G1, 0, 1, 32, -1, false, true, LD, true>(buf, tw, load0, store);
+  }
+};
+template <int G1>
+__global__ void __launch_bounds__(ROW_NT) fwd_rows_kernel(const float2* __restrict__ x,
+    const float2* __restrict__ maps, const float* __restrict__ rowfac, const float* __restrict__ coldeap,
+    float2* __restrict__ Tb, const float2* __restrict__ tw, Geo2 g, long long nrows, int coil_images) {
+  FwdRows<G1>::run(hw_block(), x, maps, rowfac, coldeap, Tb, tw, g, nrows, coil_images);
 }
 
 // forward column pass: grid[vol][:][k1] = FFT_G0(band rows of T[vol][:][k1]),
 // COLS consecutive columns per block
 template <int G0>
-__global__ void __launch_bounds__(COL_NT) fwd_cols_kernel(const float2* __restrict__ Tb, float2* __restrict__ grid,
-                                                          const float2* __restrict__ tw, Geo2 g) {
-  constexpr int COLS = cols_per_block(G0);
-  constexpr int LD = G0 | 1;
-  extern __shared__ float2 sm[];
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  const int cblocks = (g.G1 + COLS - 1) / COLS;
-  const int vol = blockIdx.x / cblocks;
-  const int k0 = (blockIdx.x - vol * cblocks) * COLS;
-  // 32-bit offsets inside one volume (at most 1024^3 = 2^30 cells for the compiled lengths)
-  const int G1 = g.G1;
-  const bool full = k0 + COLS <= G1;
-  const float2* tv = Tb + (long long)vol * g.S0 * G1 + k0;
-  float2* gv = grid + (long long)vol * g.gtot + k0;
-  auto load0 = [&](int q, int n0) -> float2 {
-    const int r = n0 - g.off0;
-    if ((unsigned)r >= (unsigned)g.S0 || (!full && k0 + q >= G1)) return make_float2(0.f, 0.f);
-    return tv[r * G1 + q];
-  };
-  auto store = [&](int q, int n0, float2 v) {
-    if (full || k0 + q < G1) gv[n0 * G1 + q] = v;
-  };
-  fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
+struct FwdCols {
+  static constexpr int NT = COL_NT, MINB = (G0 <= 256 ? 3 : 2);
+  static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ Tb,
+      float2* __restrict__ grid, const float2* __restrict__ tw, const Geo2& g) {
+    constexpr int COLS = cols_per_block(G0);
+    constexpr int LD = G0 | 1;
+    extern __shared__ float2 sm[];
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    const int cblocks = (g.G1 + COLS - 1) / COLS;
+    const int vol = vb.x / cblocks;
+    const int k0 = (vb.x - vol * cblocks) * COLS;
+    // 32-bit offsets inside one volume (at most 1024^3 = 2^30 cells for the compiled lengths)
+    const int G1 = g.G1;
+    const bool full = k0 + COLS <= G1;
+    const float2* tv = Tb + (long long)vol * g.S0 * G1 + k0;
+    float2* gv = grid + (long long)vol * g.gtot + k0;
+    auto load0 = [&](int q, int n0) -> float2 {
+      const int r = n0 - g.off0;
+      if ((unsigned)r >= (unsigned)g.S0 || (!full && k0 + q >= G1)) return make_float2(0.f, 0.f);
+      return tv[r * G1 + q];
+    };
+    auto store = [&](int q, int n0, float2 v) {
+      if (full || k0 + q < G1) gv[n0 * G1 + q] = v;
+    };
+    fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
+  }
+};
+template <int G0>
+__global__ void __launch_bounds__(COL_NT) fwd_cols_kernel(const float2* __restrict__ Tb,
+    float2* __restrict__ grid, const float2* __restrict__ tw, Geo2 g) {
+  FwdCols<G0>::run(hw_block(), Tb, grid, tw, g);
 }
 
 // forward column pass with a coil-interleaved output (3D x pass, see fft.cuh):
@@ -529,29 +557,37 @@ __global__ void __launch_bounds__(COL_NT, 2) fwd_cols_interp_kernel(const float2
 
 // adjoint column pass: T[vol][r][k1] = IFFT_G0(grid[vol][:][k1])[r + off0]
 template <int G0>
-__global__ void __launch_bounds__(COL_NT) adj_cols_kernel(const float2* __restrict__ grid, float2* __restrict__ Tb,
-                                                          const float2* __restrict__ tw, Geo2 g) {
-  constexpr int COLS = cols_per_block(G0);
-  constexpr int LD = G0 | 1;
-  extern __shared__ float2 sm[];
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  const int cblocks = (g.G1 + COLS - 1) / COLS;
-  const int vol = blockIdx.x / cblocks;
-  const int k0 = (blockIdx.x - vol * cblocks) * COLS;
-  // 32-bit offsets inside one volume (at most 1024^3 = 2^30 cells for the compiled lengths)
-  const int G1 = g.G1;
-  const bool full = k0 + COLS <= G1;
-  const float2* gv = grid + (long long)vol * g.gtot + k0;
-  float2* tv = Tb + (long long)vol * g.S0 * G1 + k0;
-  auto load0 = [&](int q, int n0) -> float2 {
-    if (!full && k0 + q >= G1) return make_float2(0.f, 0.f);
-    return gv[n0 * G1 + q];
-  };
-  auto store = [&](int q, int n0, float2 v) {
-    const int r = n0 - g.off0;
-    if ((unsigned)r < (unsigned)g.S0 && (full || k0 + q < G1)) tv[r * G1 + q] = v;
-  };
-  fft_stages<G0, 0, COLS, COL_NT, +1, true, false, LD>(sm, tw, load0, store);
+struct AdjCols {
+  static constexpr int NT = COL_NT, MINB = (G0 <= 256 ? 3 : 2);
+  static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ grid,
+      float2* __restrict__ Tb, const float2* __restrict__ tw, const Geo2& g) {
+    constexpr int COLS = cols_per_block(G0);
+    constexpr int LD = G0 | 1;
+    extern __shared__ float2 sm[];
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    const int cblocks = (g.G1 + COLS - 1) / COLS;
+    const int vol = vb.x / cblocks;
+    const int k0 = (vb.x - vol * cblocks) * COLS;
+    // 32-bit offsets inside one volume (at most 1024^3 = 2^30 cells for the compiled lengths)
+    const int G1 = g.G1;
+    const bool full = k0 + COLS <= G1;
+    const float2* gv = grid + (long long)vol * g.gtot + k0;
+    float2* tv = Tb + (long long)vol * g.S0 * G1 + k0;
+    auto load0 = [&](int q, int n0) -> float2 {
+      if (!full && k0 + q >= G1) return make_float2(0.f, 0.f);
+      return gv[n0 * G1 + q];
+    };
+    auto store = [&](int q, int n0, float2 v) {
+      const int r = n0 - g.off0;
+      if ((unsigned)r < (unsigned)g.S0 && (full || k0 + q < G1)) tv[r * G1 + q] = v;
+    };
+    fft_stages<G0, 0, COLS, COL_NT, +1, true, false, LD>(sm, tw, load0, store);
+  }
+};
+template <int G0>
+__global__ void __launch_bounds__(COL_NT) adj_cols_kernel(const float2* __restrict__ grid,
+    float2* __restrict__ Tb, const float2* __restrict__ tw, Geo2 g) {
+  AdjCols<G0>::run(hw_block(), grid, Tb, tw, g);
 }
 
 // Toeplitz column pass (normal operator A^H A by circular convolution on the
@@ -587,7 +623,7 @@ __global__ void __launch_bounds__(COL_NT) toeplitz_cols_kernel(float2* __restric
     const int q = e % COLS, kr = e / COLS;
     const float p = k0 + q < g.G1 ? __ldg(pb + (long long)kr * g.G1 + k0 + q) : 0.f;
     float2 v = sm[q * LD + kr];
-    sm[q * LD + kr] = make_float2(v.x * p, v.y * p);
+    sm[q * LD + kr] = cscale(v, p);
   }
   __syncthreads();
   auto store = [&](int q, int n0, float2 v) {
@@ -601,50 +637,59 @@ __global__ void __launch_bounds__(COL_NT) toeplitz_cols_kernel(float2* __restric
 //   sum_c conj(S_c) IFFT_G1(T[(be, c)][r][:])[i1 + off1], one block per (be, r),
 // coils in passes of ROWS
 template <int G1>
-__global__ void __launch_bounds__(ROW_NT) adj_rows_kernel(const float2* __restrict__ Tb, const float2* __restrict__ maps,
-                                                          const float* __restrict__ rowfac,
-                                                          const float* __restrict__ coldeap, float2* __restrict__ x,
-                                                          const float2* __restrict__ tw, Geo2 g, float scale) {
-  constexpr int ROWS = rows_per_block(G1);
-  constexpr int LD = row_ld(G1);
-  extern __shared__ float2 sm[];
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  float2* acc = sm + ROWS * LD;   // S1 accumulators
-  const int row = blockIdx.x;
-  const int be = row / g.S0;
-  const int r = row - be * g.S0;
-  for (int i = threadIdx.x; i < g.S1; i += ROW_NT) acc[i] = make_float2(0.f, 0.f);
-  for (int c0 = 0; c0 < g.C; c0 += ROWS) {
-    const int ncl = min(ROWS, g.C - c0);
-    const float2* tb = Tb + (((long long)be * g.C + c0) * g.S0 + r) * G1;
-    const long long cstride = (long long)g.S0 * G1;
-    auto load0 = [&](int q, int n1) -> float2 {
-      if (q >= ncl) return make_float2(0.f, 0.f);
-      return tb[q * cstride + n1];
-    };
-    auto sstore = [&](int q, int e, float2 v) { sm[q * LD + swz(e)] = v; };
-    fft_stages<G1, 0, ROWS, ROW_NT, +1, false, true, LD>(sm, tw, load0, sstore);
-    for (int i = threadIdx.x; i < g.S1; i += ROW_NT) {
-      float2 s = acc[i];
-      const int e = i + g.off1;
-      const int pe = swz(e);
-      const float2* mp = maps + (long long)c0 * g.stot + (long long)r * g.S1 + i;
-      for (int q = 0; q < ncl; ++q) {
-        const float2 v = sm[q * LD + pe];
-        const float2 m = __ldg(mp + (long long)q * g.stot);
-        s.x += m.x * v.x + m.y * v.y;
-        s.y += m.x * v.y - m.y * v.x;
+struct AdjRows {
+  static constexpr int NT = ROW_NT, MINB = ((G1 & (G1 - 1)) == 0 && G1 >= 128 ? 4 : G1 <= 64 || G1 == 768 ? 3 : 2);
+  static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ Tb,
+      const float2* __restrict__ maps, const float* __restrict__ rowfac, const float* __restrict__ coldeap,
+      float2* __restrict__ x, const float2* __restrict__ tw, const Geo2& g, float scale) {
+    constexpr int ROWS = rows_per_block(G1);
+    constexpr int LD = row_ld(G1);
+    extern __shared__ float2 sm[];
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    float2* acc = sm + ROWS * LD;   // S1 accumulators
+    const int row = vb.x;
+    const int be = row / g.S0;
+    const int r = row - be * g.S0;
+    for (int i = threadIdx.x; i < g.S1; i += ROW_NT) acc[i] = make_float2(0.f, 0.f);
+    for (int c0 = 0; c0 < g.C; c0 += ROWS) {
+      const int ncl = min(ROWS, g.C - c0);
+      const float2* tb = Tb + (((long long)be * g.C + c0) * g.S0 + r) * G1;
+      const long long cstride = (long long)g.S0 * G1;
+      auto load0 = [&](int q, int n1) -> float2 {
+        if (q >= ncl) return make_float2(0.f, 0.f);
+        return tb[q * cstride + n1];
+      };
+      auto sstore = [&](int q, int e, float2 v) { sm[q * LD + swz(e)] = v; };
+      fft_stages<G1, 0, ROWS, ROW_NT, +1, false, true, LD>(sm, tw, load0, sstore);
+      for (int i = threadIdx.x; i < g.S1; i += ROW_NT) {
+        float2 s = acc[i];
+        const int e = i + g.off1;
+        const int pe = swz(e);
+        const float2* mp = maps + (long long)c0 * g.stot + (long long)r * g.S1 + i;
+        for (int q = 0; q < ncl; ++q) {
+          const float2 v = sm[q * LD + pe];
+          const float2 m = __ldg(mp + (long long)q * g.stot);
+          // s += conj(m) v
+          s.x = __fadd_rn(s.x, fmaf(m.x, v.x, __fmul_rn(m.y, v.y)));
+          s.y = __fadd_rn(s.y, fmaf(m.x, v.y, -__fmul_rn(m.y, v.x)));
+        }
+        acc[i] = s;
       }
-      acc[i] = s;
+      __syncthreads();
     }
-    __syncthreads();
+    for (int i = threadIdx.x; i < g.S1; i += ROW_NT) {
+      float d = __fmul_rn(__fmul_rn(scale, __ldg(rowfac + r)), __ldg(coldeap + i));
+      if ((i + g.off1) & 1) d = -d;
+      const float2 s = acc[i];
+      x[((long long)be * g.S0 + r) * g.S1 + i] = make_float2(s.x * d, s.y * d);
+    }
   }
-  for (int i = threadIdx.x; i < g.S1; i += ROW_NT) {
-    float d = scale * __ldg(rowfac + r) * __ldg(coldeap + i);
-    if ((i + g.off1) & 1) d = -d;
-    const float2 s = acc[i];
-    x[((long long)be * g.S0 + r) * g.S1 + i] = make_float2(s.x * d, s.y * d);
-  }
+};
+template <int G1>
+__global__ void __launch_bounds__(ROW_NT) adj_rows_kernel(const float2* __restrict__ Tb,
+    const float2* __restrict__ maps, const float* __restrict__ rowfac, const float* __restrict__ coldeap,
+    float2* __restrict__ x, const float2* __restrict__ tw, Geo2 g, float scale) {
+  AdjRows<G1>::run(hw_block(), Tb, maps, rowfac, coldeap, x, tw, g, scale);
 }
 
 Geo2 make_geo2(int S0, int S1, int G0, int G1, int C, const double* skip) {
@@ -681,10 +726,8 @@ int launch_fwd_rows(const void* x, const float2* maps, const float* rowfac, cons
   const long long nrows = (long long)nb * g.C * g.S0;
   const long long blocks = (nrows + ROW_WARPS - 1) / ROW_WARPS;
   MRB_REQUIRE(blocks < (1LL << 31), "too many rows");
-  fwd_rows_kernel<G1><<<(unsigned)blocks, ROW_NT, smem, st>>>((const float2*)x, maps, rowfac, coldeap, Tb, tw, g, nrows,
-                                                              coil_images);
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<FwdRows<G1>>(fwd_rows_kernel<G1>, dim3((unsigned)blocks), smem, st, (const float2*)x, maps, rowfac,
+                                  coldeap, Tb, tw, g, nrows, coil_images);
 }
 
 template <int G0>
@@ -696,13 +739,10 @@ int launch_cols(bool forward, const float2* in, float2* out, const float2* tw, c
   int rc;
   if (forward) {
     if ((rc = set_smem((const void*)fwd_cols_kernel<G0>, smem))) return rc;
-    fwd_cols_kernel<G0><<<(unsigned)blocks, COL_NT, smem, st>>>(in, out, tw, g);
-  } else {
-    if ((rc = set_smem((const void*)adj_cols_kernel<G0>, smem))) return rc;
-    adj_cols_kernel<G0><<<(unsigned)blocks, COL_NT, smem, st>>>(in, out, tw, g);
+    return mrb::launch<FwdCols<G0>>(fwd_cols_kernel<G0>, dim3((unsigned)blocks), smem, st, in, out, tw, g);
   }
-  MRB_LAUNCH_CHECK();
-  return 0;
+  if ((rc = set_smem((const void*)adj_cols_kernel<G0>, smem))) return rc;
+  return mrb::launch<AdjCols<G0>>(adj_cols_kernel<G0>, dim3((unsigned)blocks), smem, st, in, out, tw, g);
 }
 
 template <int G0, int CT>
@@ -776,9 +816,8 @@ int launch_adj_rows(const float2* Tb, const float2* maps, const float* rowfac, c
   if ((rc = set_smem((const void*)adj_rows_kernel<G1>, smem))) return rc;
   const long long blocks = (long long)nb * g.S0;
   MRB_REQUIRE(blocks < (1LL << 31), "too many rows");
-  adj_rows_kernel<G1><<<(unsigned)blocks, ROW_NT, smem, st>>>(Tb, maps, rowfac, coldeap, (float2*)x, tw, g, scale);
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<AdjRows<G1>>(adj_rows_kernel<G1>, dim3((unsigned)blocks), smem, st, Tb, maps, rowfac, coldeap,
+                                  (float2*)x, tw, g, scale);
 }
 
 }  // namespace

@@ -25,12 +25,18 @@ int fail(int code, const char* fmt, ...);
   } while (0)
 
 // every kernel launch of the library goes through MRB_LAUNCH_CHECK, which also
-// counts it (host-side; launches recorded into a CUDA graph count once).
+// counts it (host-side; launches recorded into a CUDA graph count once).  A
+// kernel launched directly while grouped launches are being recorded would
+// run ahead of the recorded ones: its entry point fails (group.cuh).
 void count_launch();
-#define MRB_LAUNCH_CHECK()          \
-  do {                              \
-    ::mrb::count_launch();          \
-    MRB_CUDA_TRY(cudaGetLastError()); \
+bool group_recording();
+#define MRB_LAUNCH_CHECK()                                                               \
+  do {                                                                                   \
+    ::mrb::count_launch();                                                               \
+    MRB_CUDA_TRY(cudaGetLastError());                                                    \
+    if (::mrb::group_recording())                                                        \
+      return ::mrb::fail(MRB_ESTATE, "%s:%d: kernel without a grouped form launched "   \
+                         "inside a recording", __FILE__, __LINE__);                      \
   } while (0)
 
 #define MRB_REQUIRE(cond, ...)                                                      \

@@ -24,8 +24,12 @@
 #include <mutex>
 
 #include "mrb_common.cuh"
+#include "group.cuh"
 
 namespace {
+
+using mrb::VBlock;
+using mrb::hw_block;
 
 constexpr int RED_THREADS = 256;
 constexpr int RED_MAX_BLOCKS = 1184;   // 8 x 148 SMs
@@ -40,7 +44,7 @@ __host__ __device__ inline int red_blocks(long long n, int per_thread) {
 
 // Block-level FP64 reduction of NV values; lane/warp order fixed.
 template <int NV>
-__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* __restrict__ partials) {
+__device__ __forceinline__ void block_reduce_store(const VBlock& vb, double (&v)[NV], double* __restrict__ partials) {
   __shared__ double sh[RED_THREADS / 32][NV];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -56,7 +60,7 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* __re
       double s = lane < RED_THREADS / 32 ? sh[lane][j] : 0.0;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-      if (lane == 0) partials[(long long)blockIdx.x * NV + j] = s;
+      if (lane == 0) partials[(long long)vb.x * NV + j] = s;
     }
   }
 }
@@ -99,13 +103,13 @@ struct RedOut {
 };
 
 template <int NV>
-__device__ __forceinline__ void block_reduce_finish(double (&v)[NV], double* __restrict__ partials,
+__device__ __forceinline__ void block_reduce_finish(const VBlock& vb, double (&v)[NV], double* __restrict__ partials,
                                                     const RedOut& r) {
-  block_reduce_store<NV>(v, partials);
+  block_reduce_store<NV>(vb, v, partials);
   __shared__ unsigned s_last;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) s_last = atomicAdd(r.counter, 1u) == gridDim.x - 1 ? 1u : 0u;
+  if (threadIdx.x == 0) s_last = atomicAdd(r.counter, 1u) == vb.nx - 1 ? 1u : 0u;
   __syncthreads();
   if (!s_last) return;
   __threadfence();
@@ -119,7 +123,7 @@ __device__ __forceinline__ void block_reduce_finish(double (&v)[NV], double* __r
     double acc[GRP];
 #pragma unroll
     for (int q = 0; q < GRP; ++q) acc[q] = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    for (int b = threadIdx.x; b < (int)vb.nx; b += blockDim.x) {
 #pragma unroll
       for (int q = 0; q < GRP; ++q)
         if (j0 + q < NV) acc[q] += __ldcg(partials + (long long)b * NV + j0 + q);
@@ -173,6 +177,7 @@ struct DotArgs {
 
 template <int NP>
 __global__ void __launch_bounds__(RED_THREADS) dots_kernel(DotArgs a, double* __restrict__ partials) {
+  const VBlock vb = hw_block();
   double acc[NP];
 #pragma unroll
   for (int j = 0; j < NP; ++j) acc[j] = 0.0;
@@ -188,7 +193,7 @@ __global__ void __launch_bounds__(RED_THREADS) dots_kernel(DotArgs a, double* __
       acc[j] += (double)r;
     }
   }
-  block_reduce_store<NP>(acc, partials);
+  block_reduce_store<NP>(vb, acc, partials);
 }
 
 // ---------------------------------------------------------------------------
@@ -197,47 +202,54 @@ __global__ void __launch_bounds__(RED_THREADS) dots_kernel(DotArgs a, double* __
 // mode 0: scalars e_rr = |r|^2, e_rd = Re<r,Ad>, e_dd = |Ad|^2
 // mode 1: r = Ax + t*Ad - y, returns |r|^2 (reference residual, objective.py:31-45)
 // mode 2: r += t*Ad (accepted step; t from the device), no reduction
-__global__ void __launch_bounds__(RED_THREADS) kspace_kernel(int mode, long long n, float2* __restrict__ r,
-                                                             const float2* __restrict__ Ad,
-                                                             const float2* __restrict__ Ax,
-                                                             const float2* __restrict__ y, const double* t_dev,
-                                                             double t_host, const double* skip,
-                                                             double* __restrict__ partials, RedOut ro) {
-  double acc[3] = {0.0, 0.0, 0.0};
-  if (skipped(skip) != 0.0) return;   // uniform over the grid: no partials, no counter
-  const bool sk = false;
-  float t = (float)(t_dev ? *t_dev : t_host);
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  if (!sk) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-      if (mode == 0) {
-        float2 a = r[i], b = Ad[i];
-        acc[0] += (double)(a.x * a.x + a.y * a.y);
-        acc[1] += (double)(a.x * b.x + a.y * b.y);
-        acc[2] += (double)(b.x * b.x + b.y * b.y);
-      } else if (mode == 1) {
-        float2 d = Ad ? Ad[i] : make_float2(0.f, 0.f);
-        float2 a = Ax[i], yy = y[i];
-        // same operation order as the reference: r = Ad; r *= t; r += Ax; r -= y
-        float rx = __fadd_rn(__fadd_rn(__fmul_rn(d.x, t), a.x), -yy.x);
-        float ry = __fadd_rn(__fadd_rn(__fmul_rn(d.y, t), a.y), -yy.y);
-        r[i] = make_float2(rx, ry);
-        acc[0] += (double)(rx * rx + ry * ry);
-      } else {
-        float2 a = r[i], b = Ad[i];
-        a.x = fmaf(t, b.x, a.x);
-        a.y = fmaf(t, b.y, a.y);
-        r[i] = a;
+struct KSpace {
+  static constexpr int NT = RED_THREADS, MINB = 5;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, int mode, long long n, float2* __restrict__ r,
+      const float2* __restrict__ Ad, const float2* __restrict__ Ax, const float2* __restrict__ y,
+      const double* t_dev, double t_host, const double* skip, double* __restrict__ partials, const RedOut& ro) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (skipped(skip) != 0.0) return;   // uniform over the grid: no partials, no counter
+    const bool sk = false;
+    float t = (float)(t_dev ? *t_dev : t_host);
+    const long long stride = (long long)vb.nx * blockDim.x;
+    if (!sk) {
+      for (long long i = (long long)vb.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        if (mode == 0) {
+          float2 a = r[i], b = Ad[i];
+          acc[0] += (double)(a.x * a.x + a.y * a.y);
+          acc[1] += (double)(a.x * b.x + a.y * b.y);
+          acc[2] += (double)(b.x * b.x + b.y * b.y);
+        } else if (mode == 1) {
+          float2 d = Ad ? Ad[i] : make_float2(0.f, 0.f);
+          float2 a = Ax[i], yy = y[i];
+          // same operation order as the reference: r = Ad; r *= t; r += Ax; r -= y
+          float rx = __fadd_rn(__fadd_rn(__fmul_rn(d.x, t), a.x), -yy.x);
+          float ry = __fadd_rn(__fadd_rn(__fmul_rn(d.y, t), a.y), -yy.y);
+          r[i] = make_float2(rx, ry);
+          acc[0] += (double)(rx * rx + ry * ry);
+        } else {
+          float2 a = r[i], b = Ad[i];
+          a.x = fmaf(t, b.x, a.x);
+          a.y = fmaf(t, b.y, a.y);
+          r[i] = a;
+        }
       }
     }
+    if (mode == 2) return;
+    if (mode == 1) {
+      double v1[1] = {acc[0]};
+      block_reduce_finish<1>(vb, v1, partials, ro);
+    } else {
+      block_reduce_finish<3>(vb, acc, partials, ro);
+    }
   }
-  if (mode == 2) return;
-  if (mode == 1) {
-    double v1[1] = {acc[0]};
-    block_reduce_finish<1>(v1, partials, ro);
-  } else {
-    block_reduce_finish<3>(acc, partials, ro);
-  }
+};
+__global__ void __launch_bounds__(RED_THREADS) kspace_kernel(int mode, long long n, float2* __restrict__ r,
+    const float2* __restrict__ Ad, const float2* __restrict__ Ax, const float2* __restrict__ y,
+    const double* t_dev, double t_host, const double* skip, double* __restrict__ partials, RedOut ro) {
+  KSpace::run(hw_block(), mode, n, r, Ad, Ax, y, t_dev, t_host, skip, partials, ro);
 }
 
 // ---------------------------------------------------------------------------
@@ -328,124 +340,134 @@ struct GradArgs {
 };
 
 template <int NS, int NU>
-__global__ void __launch_bounds__(RED_THREADS, NS <= 3 ? 4 : 1) grad_kernel(GradArgs a, TVPlan P, double* __restrict__ partials,
-                                                           RedOut ro) {
-  // dot products (which may cancel) accumulate in FP64 per thread; the TV
-  // energies (non-negative terms) in FP32 per thread; reductions in FP64
-  double acc[GP_NV];
-#pragma unroll
-  for (int j = 0; j < GP_NV; ++j) acc[j] = 0.0;
-  float eacc[MAX_TERMS];
-#pragma unroll
-  for (int j = 0; j < MAX_TERMS; ++j) eacc[j] = 0.f;
-  if (a.skip && (a.skip_if_zero ? (*a.skip == 0.0) : (*a.skip != 0.0))) return;   // uniform: out untouched
-  const bool sk = false;
-  const float t = (float)(a.t_dev ? *a.t_dev : a.t_host);
-  const unsigned stride_all = gridDim.x * blockDim.x;
-  if (!sk) {
-    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < P.n; v += stride_all) {
-      int c[NS];
-      bool hn[NS], hp[NS];
-      float2 zn[NS], zp[NS];
-      const float2 zv = zload(a.x, a.d, t, v);
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        c[s] = 0;
-        hn[s] = hp[s] = false;
-        zn[s] = zp[s] = make_float2(0.f, 0.f);
-        if (s < P.ns) {
-          c[s] = slot_coord(P, s, v);
-          hn[s] = c[s] + 1 < P.size[s];
-          hp[s] = c[s] > 0;
-          if (hn[s]) zn[s] = zload(a.x, a.d, t, v + P.stride[s]);
-          if (hp[s]) zp[s] = zload(a.x, a.d, t, v - P.stride[s]);
+struct TVGrad {
+  static constexpr int NT = RED_THREADS, MINB = (NS <= 3 ? 4 : 1);
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, const GradArgs& a, const TVPlan& P,
+      double* __restrict__ partials, const RedOut& ro) {
+    // dot products (which may cancel) accumulate in FP64 per thread; the TV
+    // energies (non-negative terms) in FP32 per thread; reductions in FP64
+    double acc[GP_NV];
+  #pragma unroll
+    for (int j = 0; j < GP_NV; ++j) acc[j] = 0.0;
+    float eacc[MAX_TERMS];
+  #pragma unroll
+    for (int j = 0; j < MAX_TERMS; ++j) eacc[j] = 0.f;
+    if (a.skip && (a.skip_if_zero ? (*a.skip == 0.0) : (*a.skip != 0.0))) return;   // uniform: out untouched
+    const bool sk = false;
+    const float t = (float)(a.t_dev ? *a.t_dev : a.t_host);
+    const unsigned stride_all = vb.nx * blockDim.x;
+    if (!sk) {
+      for (unsigned v = vb.x * blockDim.x + threadIdx.x; v < P.n; v += stride_all) {
+        int c[NS];
+        bool hn[NS], hp[NS];
+        float2 zn[NS], zp[NS];
+        const float2 zv = zload(a.x, a.d, t, v);
+  #pragma unroll
+        for (int s = 0; s < NS; ++s) {
+          c[s] = 0;
+          hn[s] = hp[s] = false;
+          zn[s] = zp[s] = make_float2(0.f, 0.f);
+          if (s < P.ns) {
+            c[s] = slot_coord(P, s, v);
+            hn[s] = c[s] + 1 < P.size[s];
+            hp[s] = c[s] > 0;
+            if (hn[s]) zn[s] = zload(a.x, a.d, t, v + P.stride[s]);
+            if (hp[s]) zp[s] = zload(a.x, a.d, t, v - P.stride[s]);
+          }
         }
-      }
-      // forward differences at v
-      float2 D[NS];
-#pragma unroll
-      for (int s = 0; s < NS; ++s)
-        D[s] = hn[s] ? make_float2(zn[s].x - zv.x, zn[s].y - zv.y) : make_float2(0.f, 0.f);
-      // forward differences at v - e_s, along every slot s2: Dp[s][s2]
-      float2 Dp[NS][NS];
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-#pragma unroll
-        for (int s2 = 0; s2 < NS; ++s2) {
-          Dp[s][s2] = make_float2(0.f, 0.f);
-          if (!hp[s]) continue;
-          if (s2 == s) {
-            Dp[s][s2] = make_float2(zv.x - zp[s].x, zv.y - zp[s].y);
-          } else if ((P.diag_mask >> (s * NSLOT + s2)) & 1u) {
-            if (hn[s2]) {
-              float2 zd = zload(a.x, a.d, t, v - P.stride[s] + P.stride[s2]);
-              Dp[s][s2] = make_float2(zd.x - zp[s].x, zd.y - zp[s].y);
+        // forward differences at v
+        float2 D[NS];
+  #pragma unroll
+        for (int s = 0; s < NS; ++s)
+          D[s] = hn[s] ? make_float2(zn[s].x - zv.x, zn[s].y - zv.y) : make_float2(0.f, 0.f);
+        // forward differences at v - e_s, along every slot s2: Dp[s][s2]
+        float2 Dp[NS][NS];
+  #pragma unroll
+        for (int s = 0; s < NS; ++s) {
+  #pragma unroll
+          for (int s2 = 0; s2 < NS; ++s2) {
+            Dp[s][s2] = make_float2(0.f, 0.f);
+            if (!hp[s]) continue;
+            if (s2 == s) {
+              Dp[s][s2] = make_float2(zv.x - zp[s].x, zv.y - zp[s].y);
+            } else if ((P.diag_mask >> (s * NSLOT + s2)) & 1u) {
+              if (hn[s2]) {
+                float2 zd = zload(a.x, a.d, t, v - P.stride[s] + P.stride[s2]);
+                Dp[s][s2] = make_float2(zd.x - zp[s].x, zd.y - zp[s].y);
+              }
             }
           }
         }
-      }
-      float gx = 0.f, gy = 0.f;
-      if (a.g_base) { float2 b = a.g_base[v]; gx = b.x; gy = b.y; }
-      if (a.g_dir) { float2 b = a.g_dir[v]; gx = fmaf(t, b.x, gx); gy = fmaf(t, b.y, gy); }
-#pragma unroll
-      for (int u = 0; u < NU; ++u) {
-        if (u >= P.nu) continue;
-        const float e2 = P.eps[u] * P.eps[u];
-        float ss = 0.f;
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-          const float w = P.w[u][s];
-          float2 q = make_float2(w * D[s].x, w * D[s].y);
-          ss += q.x * q.x + q.y * q.y;
-        }
-        float inv;
-        const float ex = huber_excess(ss, P.eps[u], &inv);
-        const int ti = P.term_of[u];
-#pragma unroll
-        for (int tt = 0; tt < MAX_TERMS; ++tt)
-          if (tt == ti) eacc[tt] = fmaf(P.lam[u], ex, eacc[tt]);
-        float dx = 0.f, dy = 0.f;
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-          const float w = P.w[u][s];
-          if (w == 0.f) continue;
-          dx += w * D[s].x * inv;
-          dy += w * D[s].y * inv;
-          if (hp[s]) {
-            float ssp = 0.f;
-#pragma unroll
-            for (int s2 = 0; s2 < NS; ++s2) {
-              const float w2 = P.w[u][s2];
-              float2 q = make_float2(w2 * Dp[s][s2].x, w2 * Dp[s][s2].y);
-              ssp += q.x * q.x + q.y * q.y;
-            }
-            const float invp = rsqrtf(ssp + e2);
-            dx -= w * Dp[s][s].x * invp;
-            dy -= w * Dp[s][s].y * invp;
+        float gx = 0.f, gy = 0.f;
+        if (a.g_base) { float2 b = a.g_base[v]; gx = b.x; gy = b.y; }
+        if (a.g_dir) { float2 b = a.g_dir[v]; gx = fmaf(t, b.x, gx); gy = fmaf(t, b.y, gy); }
+  #pragma unroll
+        for (int u = 0; u < NU; ++u) {
+          if (u >= P.nu) continue;
+          const float e2 = P.eps[u] * P.eps[u];
+          float ss = 0.f;
+  #pragma unroll
+          for (int s = 0; s < NS; ++s) {
+            const float w = P.w[u][s];
+            float2 q = make_float2(w * D[s].x, w * D[s].y);
+            ss += q.x * q.x + q.y * q.y;
           }
+          float inv;
+          const float ex = huber_excess(ss, P.eps[u], &inv);
+          const int ti = P.term_of[u];
+  #pragma unroll
+          for (int tt = 0; tt < MAX_TERMS; ++tt)
+            if (tt == ti) eacc[tt] = fmaf(P.lam[u], ex, eacc[tt]);
+          float dx = 0.f, dy = 0.f;
+  #pragma unroll
+          for (int s = 0; s < NS; ++s) {
+            const float w = P.w[u][s];
+            if (w == 0.f) continue;
+            dx += w * D[s].x * inv;
+            dy += w * D[s].y * inv;
+            if (hp[s]) {
+              float ssp = 0.f;
+  #pragma unroll
+              for (int s2 = 0; s2 < NS; ++s2) {
+                const float w2 = P.w[u][s2];
+                float2 q = make_float2(w2 * Dp[s][s2].x, w2 * Dp[s][s2].y);
+                ssp += q.x * q.x + q.y * q.y;
+              }
+              const float invp = rsqrtf(ssp + e2);
+              dx -= w * Dp[s][s].x * invp;
+              dy -= w * Dp[s][s].y * invp;
+            }
+          }
+          gx = fmaf(-P.lam[u], dx, gx);
+          gy = fmaf(-P.lam[u], dy, gy);
         }
-        gx = fmaf(-P.lam[u], dx, gx);
-        gy = fmaf(-P.lam[u], dy, gy);
-      }
-      if (a.g_out) a.g_out[v] = make_float2(gx, gy);
-      float2 dv = a.d ? a.d[v] : make_float2(0.f, 0.f);
-      const float Dv = a.diag ? a.diag[v % a.ndiag] : 1.f;
-      const int o = MAX_TERMS;
-      acc[o + 0] += (double)(gx * dv.x + gy * dv.y);
-      acc[o + 1] += (double)((gx * gx + gy * gy) / Dv);
-      acc[o + 2] += (double)(zv.x * zv.x + zv.y * zv.y);
-      acc[o + 3] += (double)(dv.x * dv.x + dv.y * dv.y);
-      if (a.g_prev) {
-        float2 gp = a.g_prev[v];
-        acc[o + 4] += (double)((gp.x * gx + gp.y * gy) / Dv);
-        acc[o + 5] += (double)((gp.x * gp.x + gp.y * gp.y) / Dv);
-        acc[o + 6] += (double)(dv.x * gp.x + dv.y * gp.y);
+        if (a.g_out) a.g_out[v] = make_float2(gx, gy);
+        float2 dv = a.d ? a.d[v] : make_float2(0.f, 0.f);
+        const float Dv = a.diag ? a.diag[v % a.ndiag] : 1.f;
+        const int o = MAX_TERMS;
+        acc[o + 0] += (double)(gx * dv.x + gy * dv.y);
+        acc[o + 1] += (double)((gx * gx + gy * gy) / Dv);
+        acc[o + 2] += (double)(zv.x * zv.x + zv.y * zv.y);
+        acc[o + 3] += (double)(dv.x * dv.x + dv.y * dv.y);
+        if (a.g_prev) {
+          float2 gp = a.g_prev[v];
+          acc[o + 4] += (double)((gp.x * gx + gp.y * gy) / Dv);
+          acc[o + 5] += (double)((gp.x * gp.x + gp.y * gp.y) / Dv);
+          acc[o + 6] += (double)(dv.x * gp.x + dv.y * gp.y);
+        }
       }
     }
+  #pragma unroll
+    for (int j = 0; j < MAX_TERMS; ++j) acc[j] = (double)eacc[j];
+    block_reduce_finish<GP_NV>(vb, acc, partials, ro);
   }
-#pragma unroll
-  for (int j = 0; j < MAX_TERMS; ++j) acc[j] = (double)eacc[j];
-  block_reduce_finish<GP_NV>(acc, partials, ro);
+};
+template <int NS, int NU>
+__global__ void __launch_bounds__(RED_THREADS, NS <= 3 ? 4 : 1) grad_kernel(GradArgs a, TVPlan P,
+    double* __restrict__ partials, RedOut ro) {
+  TVGrad<NS, NU>::run(hw_block(), a, P, partials, ro);
 }
 
 // Sum of all unit energies at z = x + t_j d for J <= MT_MAX_J step sizes, one
@@ -456,67 +478,76 @@ __global__ void __launch_bounds__(RED_THREADS, NS <= 3 ? 4 : 1) grad_kernel(Grad
 constexpr int MT_MAX_J = 24;
 
 template <int NS, int NU, int JMAX>
-__global__ void __launch_bounds__(RED_THREADS, JMAX <= 8 ? 4 : 1) tv_multi_kernel(const float2* __restrict__ x,
-                                                               const float2* __restrict__ d,
-                                                               const double* __restrict__ ts, int J, TVPlan P,
-                                                               const double* skip, double* __restrict__ partials,
-                                                               RedOut ro) {
-  // energies are sums of non-negative terms: a thread sums its ~n / (blocks x threads)
-  // voxels in FP32, the block and grid reductions run in FP64
-  float facc[JMAX];
-#pragma unroll
-  for (int j = 0; j < JMAX; ++j) facc[j] = 0.f;
-  if (skipped(skip) != 0.0) return;   // uniform over the grid: no partials, no counter
-  const bool sk = false;
-  __shared__ float tf[MT_MAX_J];   // trial steps, broadcast from shared memory
-  if (threadIdx.x < MT_MAX_J) tf[threadIdx.x] = threadIdx.x < J ? (float)ts[threadIdx.x] : 0.f;
-  __syncthreads();
-  const unsigned stride_all = gridDim.x * blockDim.x;
-  if (!sk) {
-    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < P.n; v += stride_all) {
-      const float2 xv = x[v], dv = d[v];
-      float2 A[NS], B[NS];
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        A[s] = B[s] = make_float2(0.f, 0.f);
-        if (s < P.ns && slot_coord(P, s, v) + 1 < P.size[s]) {
-          const float2 xn = x[v + P.stride[s]], dn = d[v + P.stride[s]];
-          A[s] = make_float2(xn.x - xv.x, xn.y - xv.y);
-          B[s] = make_float2(dn.x - dv.x, dn.y - dv.y);
-        }
-      }
-      float al[NU], be2[NU], ga[NU];
-#pragma unroll
-      for (int u = 0; u < NU; ++u) {
-        al[u] = be2[u] = ga[u] = 0.f;
-        if (u >= P.nu) continue;
-#pragma unroll
+struct TVMulti {
+  static constexpr int NT = RED_THREADS, MINB = (JMAX <= 8 ? 4 : 1);
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ x,
+      const float2* __restrict__ d, const double* __restrict__ ts, int J, const TVPlan& P, const double* skip,
+      double* __restrict__ partials, const RedOut& ro) {
+    // energies are sums of non-negative terms: a thread sums its ~n / (blocks x threads)
+    // voxels in FP32, the block and grid reductions run in FP64
+    float facc[JMAX];
+  #pragma unroll
+    for (int j = 0; j < JMAX; ++j) facc[j] = 0.f;
+    if (skipped(skip) != 0.0) return;   // uniform over the grid: no partials, no counter
+    const bool sk = false;
+    __shared__ float tf[MT_MAX_J];   // trial steps, broadcast from shared memory
+    if (threadIdx.x < MT_MAX_J) tf[threadIdx.x] = threadIdx.x < J ? (float)ts[threadIdx.x] : 0.f;
+    __syncthreads();
+    const unsigned stride_all = vb.nx * blockDim.x;
+    if (!sk) {
+      for (unsigned v = vb.x * blockDim.x + threadIdx.x; v < P.n; v += stride_all) {
+        const float2 xv = x[v], dv = d[v];
+        float2 A[NS], B[NS];
+  #pragma unroll
         for (int s = 0; s < NS; ++s) {
-          const float w2 = P.w[u][s] * P.w[u][s];
-          al[u] = fmaf(w2, A[s].x * A[s].x + A[s].y * A[s].y, al[u]);
-          be2[u] = fmaf(2.f * w2, A[s].x * B[s].x + A[s].y * B[s].y, be2[u]);
-          ga[u] = fmaf(w2, B[s].x * B[s].x + B[s].y * B[s].y, ga[u]);
+          A[s] = B[s] = make_float2(0.f, 0.f);
+          if (s < P.ns && slot_coord(P, s, v) + 1 < P.size[s]) {
+            const float2 xn = x[v + P.stride[s]], dn = d[v + P.stride[s]];
+            A[s] = make_float2(xn.x - xv.x, xn.y - xv.y);
+            B[s] = make_float2(dn.x - dv.x, dn.y - dv.y);
+          }
         }
-      }
-#pragma unroll
-      for (int j = 0; j < JMAX; ++j) {
-        if (j >= J) continue;
-        const float t = tf[j];
-        float e = 0.f;
-#pragma unroll
+        float al[NU], be2[NU], ga[NU];
+  #pragma unroll
         for (int u = 0; u < NU; ++u) {
+          al[u] = be2[u] = ga[u] = 0.f;
           if (u >= P.nu) continue;
-          const float q = fmaxf(fmaf(t, fmaf(t, ga[u], be2[u]), al[u]), 0.f);
-          e = fmaf(P.lam[u], huber_excess(q, P.eps[u], nullptr), e);
+  #pragma unroll
+          for (int s = 0; s < NS; ++s) {
+            const float w2 = P.w[u][s] * P.w[u][s];
+            al[u] = fmaf(w2, A[s].x * A[s].x + A[s].y * A[s].y, al[u]);
+            be2[u] = fmaf(2.f * w2, A[s].x * B[s].x + A[s].y * B[s].y, be2[u]);
+            ga[u] = fmaf(w2, B[s].x * B[s].x + B[s].y * B[s].y, ga[u]);
+          }
         }
-        facc[j] += e;
+  #pragma unroll
+        for (int j = 0; j < JMAX; ++j) {
+          if (j >= J) continue;
+          const float t = tf[j];
+          float e = 0.f;
+  #pragma unroll
+          for (int u = 0; u < NU; ++u) {
+            if (u >= P.nu) continue;
+            const float q = fmaxf(fmaf(t, fmaf(t, ga[u], be2[u]), al[u]), 0.f);
+            e = fmaf(P.lam[u], huber_excess(q, P.eps[u], nullptr), e);
+          }
+          facc[j] += e;
+        }
       }
     }
+    double acc[JMAX];
+  #pragma unroll
+    for (int j = 0; j < JMAX; ++j) acc[j] = (double)facc[j];
+    block_reduce_finish<JMAX>(vb, acc, partials, ro);
   }
-  double acc[JMAX];
-#pragma unroll
-  for (int j = 0; j < JMAX; ++j) acc[j] = (double)facc[j];
-  block_reduce_finish<JMAX>(acc, partials, ro);
+};
+template <int NS, int NU, int JMAX>
+__global__ void __launch_bounds__(RED_THREADS, JMAX <= 8 ? 4 : 1) tv_multi_kernel(const float2* __restrict__ x,
+    const float2* __restrict__ d, const double* __restrict__ ts, int J, TVPlan P, const double* skip,
+    double* __restrict__ partials, RedOut ro) {
+  TVMulti<NS, NU, JMAX>::run(hw_block(), x, d, ts, J, P, skip, partials, ro);
 }
 
 // ---------------------------------------------------------------------------
@@ -565,42 +596,50 @@ __device__ __forceinline__ NCGCfg load_cfg(const double* c) {
 }
 
 // Armijo selection on the multi-t energies: t_0 = 0, t_j = beta^(j-1).
-__global__ void armijo_select_kernel(double* s, const double* cfg_dev) {
-  if (threadIdx.x != 0) return;
-  const NCGCfg cfg = load_cfg(cfg_dev);
-  if (s[S_DONE] != 0.0) {
-    s[S_LS_OK] = 0.0;
-    return;
-  }
-  const double err = s[S_ERR], erd = s[S_ERD], edd = s[S_EDD];
-  const double f0 = 0.5 * err + s[S_EJ + 0];
-  const double g0d = s[S_G0D];
-  s[S_F0] = f0;
-  bool bad = !(g0d < 0.0) || isnan(g0d) || isinf(g0d);
-  if (bad) {
+struct ArmijoSelect {
+  static constexpr int NT = 32, MINB = 1;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, double* s, const double* cfg_dev) {
+    if (threadIdx.x != 0) return;
+    const NCGCfg cfg = load_cfg(cfg_dev);
+    if (s[S_DONE] != 0.0) {
+      s[S_LS_OK] = 0.0;
+      return;
+    }
+    const double err = s[S_ERR], erd = s[S_ERD], edd = s[S_EDD];
+    const double f0 = 0.5 * err + s[S_EJ + 0];
+    const double g0d = s[S_G0D];
+    s[S_F0] = f0;
+    bool bad = !(g0d < 0.0) || isnan(g0d) || isinf(g0d);
+    if (bad) {
+      s[S_LS_OK] = 0.0;
+      s[S_DONE] = 1.0;
+      s[S_REASON] = 1.0;
+      s[S_T] = 0.0;
+      return;
+    }
+    double t = 1.0;
+    const int jmax = cfg.ls_max_iter < MT_MAX_J - 1 ? cfg.ls_max_iter : MT_MAX_J - 1;
+    for (int j = 1; j <= jmax; ++j) {
+      double ft = 0.5 * (err + 2.0 * t * erd + t * t * edd) + s[S_EJ + j];
+      if (ft <= f0 + cfg.c1 * t * g0d) {
+        s[S_T] = t;
+        s[S_FT] = ft;
+        s[S_LS_OK] = 1.0;
+        s[S_NTRIAL] = (double)j;
+        return;
+      }
+      t *= cfg.ls_beta;
+    }
+    s[S_T] = t;
     s[S_LS_OK] = 0.0;
     s[S_DONE] = 1.0;
     s[S_REASON] = 1.0;
-    s[S_T] = 0.0;
-    return;
   }
-  double t = 1.0;
-  const int jmax = cfg.ls_max_iter < MT_MAX_J - 1 ? cfg.ls_max_iter : MT_MAX_J - 1;
-  for (int j = 1; j <= jmax; ++j) {
-    double ft = 0.5 * (err + 2.0 * t * erd + t * t * edd) + s[S_EJ + j];
-    if (ft <= f0 + cfg.c1 * t * g0d) {
-      s[S_T] = t;
-      s[S_FT] = ft;
-      s[S_LS_OK] = 1.0;
-      s[S_NTRIAL] = (double)j;
-      return;
-    }
-    t *= cfg.ls_beta;
-  }
-  s[S_T] = t;
-  s[S_LS_OK] = 0.0;
-  s[S_DONE] = 1.0;
-  s[S_REASON] = 1.0;
+};
+__global__ void armijo_select_kernel(double* s, const double* cfg_dev) {
+  ArmijoSelect::run(hw_block(), s, cfg_dev);
 }
 
 // Two-phase Armijo selection over the same backtracking sequence: phase 1
@@ -608,204 +647,236 @@ __global__ void armijo_select_kernel(double* s, const double* cfg_dev) {
 // when none satisfies f(t) <= f(0) + c1 t f'(0) it clears S_NOMORE and phase 2,
 // after a second tv_multi pass over the remaining steps, continues at j = J1.
 // S_NOMORE = 1 whenever the second pass and phase 2 have nothing to do.
+struct ArmijoPhase {
+  static constexpr int NT = 32, MINB = 1;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, double* s, const double* cfg_dev, int J1,
+      int phase) {
+    if (threadIdx.x != 0) return;
+    const NCGCfg cfg = load_cfg(cfg_dev);
+    const int jmax = cfg.ls_max_iter < MT_MAX_J - 1 ? cfg.ls_max_iter : MT_MAX_J - 1;
+    const double err = s[S_ERR], erd = s[S_ERD], edd = s[S_EDD];
+    double t;
+    int j0, j1;
+    if (phase == 1) {
+      s[S_NOMORE] = 1.0;
+      if (s[S_DONE] != 0.0) {
+        s[S_LS_OK] = 0.0;
+        return;
+      }
+      const double f0 = 0.5 * err + s[S_EJ + 0];
+      const double g0d = s[S_G0D];
+      s[S_F0] = f0;
+      if (!(g0d < 0.0) || isnan(g0d) || isinf(g0d)) {
+        s[S_LS_OK] = 0.0;
+        s[S_DONE] = 1.0;
+        s[S_REASON] = 1.0;
+        s[S_T] = 0.0;
+        return;
+      }
+      t = 1.0;
+      j0 = 1;
+      j1 = J1 - 1 < jmax ? J1 - 1 : jmax;
+    } else {
+      if (s[S_NOMORE] != 0.0) return;
+      s[S_NOMORE] = 1.0;
+      t = s[S_T];
+      j0 = J1;
+      j1 = jmax;
+    }
+    const double f0 = s[S_F0], g0d = s[S_G0D];
+    for (int j = j0; j <= j1; ++j) {
+      double ft = 0.5 * (err + 2.0 * t * erd + t * t * edd) + s[S_EJ + j];
+      if (ft <= f0 + cfg.c1 * t * g0d) {
+        s[S_T] = t;
+        s[S_FT] = ft;
+        s[S_LS_OK] = 1.0;
+        s[S_NTRIAL] = (double)j;
+        return;
+      }
+      t *= cfg.ls_beta;
+    }
+    s[S_T] = t;
+    s[S_LS_OK] = 0.0;
+    if (phase == 1 && j1 < jmax) {
+      s[S_NOMORE] = 0.0;   // the remaining steps decide
+      return;
+    }
+    s[S_DONE] = 1.0;
+    s[S_REASON] = 1.0;
+  }
+};
 __global__ void armijo_phase_kernel(double* s, const double* cfg_dev, int J1, int phase) {
-  if (threadIdx.x != 0) return;
-  const NCGCfg cfg = load_cfg(cfg_dev);
-  const int jmax = cfg.ls_max_iter < MT_MAX_J - 1 ? cfg.ls_max_iter : MT_MAX_J - 1;
-  const double err = s[S_ERR], erd = s[S_ERD], edd = s[S_EDD];
-  double t;
-  int j0, j1;
-  if (phase == 1) {
-    s[S_NOMORE] = 1.0;
-    if (s[S_DONE] != 0.0) {
-      s[S_LS_OK] = 0.0;
-      return;
-    }
-    const double f0 = 0.5 * err + s[S_EJ + 0];
-    const double g0d = s[S_G0D];
-    s[S_F0] = f0;
-    if (!(g0d < 0.0) || isnan(g0d) || isinf(g0d)) {
-      s[S_LS_OK] = 0.0;
-      s[S_DONE] = 1.0;
-      s[S_REASON] = 1.0;
-      s[S_T] = 0.0;
-      return;
-    }
-    t = 1.0;
-    j0 = 1;
-    j1 = J1 - 1 < jmax ? J1 - 1 : jmax;
-  } else {
-    if (s[S_NOMORE] != 0.0) return;
-    s[S_NOMORE] = 1.0;
-    t = s[S_T];
-    j0 = J1;
-    j1 = jmax;
-  }
-  const double f0 = s[S_F0], g0d = s[S_G0D];
-  for (int j = j0; j <= j1; ++j) {
-    double ft = 0.5 * (err + 2.0 * t * erd + t * t * edd) + s[S_EJ + j];
-    if (ft <= f0 + cfg.c1 * t * g0d) {
-      s[S_T] = t;
-      s[S_FT] = ft;
-      s[S_LS_OK] = 1.0;
-      s[S_NTRIAL] = (double)j;
-      return;
-    }
-    t *= cfg.ls_beta;
-  }
-  s[S_T] = t;
-  s[S_LS_OK] = 0.0;
-  if (phase == 1 && j1 < jmax) {
-    s[S_NOMORE] = 0.0;   // the remaining steps decide
-    return;
-  }
-  s[S_DONE] = 1.0;
-  s[S_REASON] = 1.0;
+  ArmijoPhase::run(hw_block(), s, cfg_dev, J1, phase);
 }
 
 // After the gradient pass at the accepted t: history row, stopping tests and
 // the direction coefficient beta.
-__global__ void ncg_control_kernel(double* s, double* hist, const double* cfg_dev, int nterms, int have_ft) {
-  if (threadIdx.x != 0) return;
-  const NCGCfg cfg = load_cfg(cfg_dev);
-  if (s[S_LS_OK] == 0.0) return;
-  const double* r = s + S_RED;
-  double Esum = 0.0;
-  for (int i = 0; i < nterms; ++i) Esum += r[i];
-  const double gdot = r[MAX_TERMS + 0], rho = r[MAX_TERMS + 1];
-  const double xn = sqrt(fmax(r[MAX_TERMS + 2], 0.0)), sn = sqrt(fmax(r[MAX_TERMS + 3], 0.0));
-  const double gn = sqrt(fmax(rho, 0.0));
-  if (!have_ft) {
-    // objective at the accepted point from the k-space scalars
-    double t = s[S_T];
-    s[S_FT] = 0.5 * (s[S_ERR] + 2.0 * t * s[S_ERD] + t * t * s[S_EDD]) + Esum;
-  }
-  s[S_GDT] = gdot;
-  s[S_CUM_X] += xn;
-  s[S_CUM_G] += gn;
-  s[S_CUM_S] += sn;
-  int k = (int)s[S_ITER];
-  if (k < cfg.nhist) {
-    double* h = hist + (long long)k * HIST_COLS;
-    h[0] = s[S_F0];
-    h[1] = s[S_G0D];
-    h[2] = gdot;
-    h[3] = s[S_T];
-    h[4] = s[S_CUM_X];
-    h[5] = s[S_CUM_G];
-    h[6] = s[S_CUM_S];
-    h[7] = xn;
-    h[8] = gn;
-    h[9] = sn;
-    h[10] = s[S_FT];
-  }
-  s[S_ITER] = (double)(k + 1);
-  // reference convergence test (solvers/utils.py:40-43)
-  if (gn <= (1.0 + xn) * cfg.tol_g && sn <= (1.0 + xn) * cfg.tol_step) {
-    s[S_DONE] = 1.0;
-    s[S_REASON] = 2.0;
-    return;
-  }
-  // windowed relative objective change on the accepted objectives
-  if (cfg.stop_window > 0 && k + 1 >= cfg.stop_window && k < cfg.nhist) {
-    double fk = hist[(long long)k * HIST_COLS + 10];
-    int kk = k + 1 - cfg.stop_window;    // accepted-objective index kk-1 ... use f0 of row kk
-    double fw = hist[(long long)kk * HIST_COLS + 0];
-    if ((fw - fk) <= cfg.stop_window * cfg.stop_tol * fabs(fk)) {
+struct NCGControl {
+  static constexpr int NT = 32, MINB = 1;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, double* s, double* hist, const double* cfg_dev,
+      int nterms, int have_ft) {
+    if (threadIdx.x != 0) return;
+    const NCGCfg cfg = load_cfg(cfg_dev);
+    if (s[S_LS_OK] == 0.0) return;
+    const double* r = s + S_RED;
+    double Esum = 0.0;
+    for (int i = 0; i < nterms; ++i) Esum += r[i];
+    const double gdot = r[MAX_TERMS + 0], rho = r[MAX_TERMS + 1];
+    const double xn = sqrt(fmax(r[MAX_TERMS + 2], 0.0)), sn = sqrt(fmax(r[MAX_TERMS + 3], 0.0));
+    const double gn = sqrt(fmax(rho, 0.0));
+    if (!have_ft) {
+      // objective at the accepted point from the k-space scalars
+      double t = s[S_T];
+      s[S_FT] = 0.5 * (s[S_ERR] + 2.0 * t * s[S_ERD] + t * t * s[S_EDD]) + Esum;
+    }
+    s[S_GDT] = gdot;
+    s[S_CUM_X] += xn;
+    s[S_CUM_G] += gn;
+    s[S_CUM_S] += sn;
+    int k = (int)s[S_ITER];
+    if (k < cfg.nhist) {
+      double* h = hist + (long long)k * HIST_COLS;
+      h[0] = s[S_F0];
+      h[1] = s[S_G0D];
+      h[2] = gdot;
+      h[3] = s[S_T];
+      h[4] = s[S_CUM_X];
+      h[5] = s[S_CUM_G];
+      h[6] = s[S_CUM_S];
+      h[7] = xn;
+      h[8] = gn;
+      h[9] = sn;
+      h[10] = s[S_FT];
+    }
+    s[S_ITER] = (double)(k + 1);
+    // reference convergence test (solvers/utils.py:40-43)
+    if (gn <= (1.0 + xn) * cfg.tol_g && sn <= (1.0 + xn) * cfg.tol_step) {
       s[S_DONE] = 1.0;
-      s[S_REASON] = 3.0;
+      s[S_REASON] = 2.0;
       return;
     }
-  }
-  if (k + 1 >= cfg.max_iter) {
-    s[S_DONE] = 1.0;
-    s[S_REASON] = 4.0;
-    return;
-  }
-  double beta;
-  if (cfg.direction == 0) {
-    if (s[S_RHO_INIT] == 0.0) {
-      s[S_RHO_PREV] = rho;
-      s[S_RHO_INIT] = 1.0;
+    // windowed relative objective change on the accepted objectives
+    if (cfg.stop_window > 0 && k + 1 >= cfg.stop_window && k < cfg.nhist) {
+      double fk = hist[(long long)k * HIST_COLS + 10];
+      int kk = k + 1 - cfg.stop_window;    // accepted-objective index kk-1 ... use f0 of row kk
+      double fw = hist[(long long)kk * HIST_COLS + 0];
+      if ((fw - fk) <= cfg.stop_window * cfg.stop_tol * fabs(fk)) {
+        s[S_DONE] = 1.0;
+        s[S_REASON] = 3.0;
+        return;
+      }
     }
-    beta = rho / fmax(s[S_RHO_PREV], 1e-20);
-    s[S_RHO_PREV] = rho;
-  } else if (cfg.direction == 1) {
-    double num = rho - r[MAX_TERMS + 4];
-    double den = r[MAX_TERMS + 5];
-    beta = fmax(num / fmax(den, 1e-20), 0.0);
-  } else {
-    double num = rho;
-    double den = gdot - r[MAX_TERMS + 6];
-    beta = num / fmax(den, 1e-20);
+    if (k + 1 >= cfg.max_iter) {
+      s[S_DONE] = 1.0;
+      s[S_REASON] = 4.0;
+      return;
+    }
+    double beta;
+    if (cfg.direction == 0) {
+      if (s[S_RHO_INIT] == 0.0) {
+        s[S_RHO_PREV] = rho;
+        s[S_RHO_INIT] = 1.0;
+      }
+      beta = rho / fmax(s[S_RHO_PREV], 1e-20);
+      s[S_RHO_PREV] = rho;
+    } else if (cfg.direction == 1) {
+      double num = rho - r[MAX_TERMS + 4];
+      double den = r[MAX_TERMS + 5];
+      beta = fmax(num / fmax(den, 1e-20), 0.0);
+    } else {
+      double num = rho;
+      double den = gdot - r[MAX_TERMS + 6];
+      beta = num / fmax(den, 1e-20);
+    }
+    s[S_BETA] = beta;
   }
-  s[S_BETA] = beta;
+};
+__global__ void ncg_control_kernel(double* s, double* hist, const double* cfg_dev, int nterms, int have_ft) {
+  NCGControl::run(hw_block(), s, hist, cfg_dev, nterms, have_ft);
 }
 
 // Accept + direction update (one pass):
 //   x += t d ; gr += t gAd (if gr) ; then, unless done: d = beta d - g/D,
 //   g_prev = g (if g_prev), and Re<g, d_new> for the next slope at t = 0.
-__global__ void __launch_bounds__(RED_THREADS) ncg_update_kernel(long long n, float2* __restrict__ x,
-                                                                 float2* __restrict__ d,
-                                                                 const float2* __restrict__ g,
-                                                                 float2* __restrict__ gr,
-                                                                 const float2* __restrict__ gAd,
-                                                                 float2* __restrict__ g_prev,
-                                                                 const float* __restrict__ diag, long long ndiag,
-                                                                 const double* __restrict__ s,
-                                                                 double* __restrict__ partials, RedOut ro) {
-  double acc[1] = {0.0};
-  const bool ok = s[S_LS_OK] != 0.0;
-  const bool upd_dir = ok && s[S_DONE] == 0.0;
-  const float t = (float)s[S_T];
-  const float beta = (float)s[S_BETA];
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  if (ok) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-      float2 dv = d[i];
-      float2 xv = x[i];
-      // x.add_(d * t) (cg.py:205-207)
-      xv.x = __fadd_rn(xv.x, __fmul_rn(dv.x, t));
-      xv.y = __fadd_rn(xv.y, __fmul_rn(dv.y, t));
-      x[i] = xv;
-      if (gr) {
-        float2 a = gr[i], b = gAd[i];
-        a.x = fmaf(t, b.x, a.x);
-        a.y = fmaf(t, b.y, a.y);
-        gr[i] = a;
-      }
-      if (upd_dir) {
-        float2 gv = g[i];
-        float Dv = diag ? diag[i % ndiag] : 1.f;
-        // d.mul_(beta); d.addcdiv_(g, D, value=-1)  (directions.py:158-161)
-        float nx = __fadd_rn(__fmul_rn(dv.x, beta), -(gv.x / Dv));
-        float ny = __fadd_rn(__fmul_rn(dv.y, beta), -(gv.y / Dv));
-        d[i] = make_float2(nx, ny);
-        if (g_prev) g_prev[i] = gv;
-        acc[0] += (double)(gv.x * nx + gv.y * ny);
+struct NCGUpdate {
+  static constexpr int NT = RED_THREADS, MINB = 4;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, long long n, float2* __restrict__ x,
+      float2* __restrict__ d, const float2* __restrict__ g, float2* __restrict__ gr,
+      const float2* __restrict__ gAd, float2* __restrict__ g_prev, const float* __restrict__ diag,
+      long long ndiag, const double* __restrict__ s, double* __restrict__ partials, const RedOut& ro) {
+    double acc[1] = {0.0};
+    const bool ok = s[S_LS_OK] != 0.0;
+    const bool upd_dir = ok && s[S_DONE] == 0.0;
+    const float t = (float)s[S_T];
+    const float beta = (float)s[S_BETA];
+    const long long stride = (long long)vb.nx * blockDim.x;
+    if (ok) {
+      for (long long i = (long long)vb.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        float2 dv = d[i];
+        float2 xv = x[i];
+        // x.add_(d * t) (cg.py:205-207)
+        xv.x = __fadd_rn(xv.x, __fmul_rn(dv.x, t));
+        xv.y = __fadd_rn(xv.y, __fmul_rn(dv.y, t));
+        x[i] = xv;
+        if (gr) {
+          float2 a = gr[i], b = gAd[i];
+          a.x = fmaf(t, b.x, a.x);
+          a.y = fmaf(t, b.y, a.y);
+          gr[i] = a;
+        }
+        if (upd_dir) {
+          float2 gv = g[i];
+          float Dv = diag ? diag[i % ndiag] : 1.f;
+          // d.mul_(beta); d.addcdiv_(g, D, value=-1)  (directions.py:158-161)
+          float nx = __fadd_rn(__fmul_rn(dv.x, beta), -(gv.x / Dv));
+          float ny = __fadd_rn(__fmul_rn(dv.y, beta), -(gv.y / Dv));
+          d[i] = make_float2(nx, ny);
+          if (g_prev) g_prev[i] = gv;
+          acc[0] += (double)(gv.x * nx + gv.y * ny);
+        }
       }
     }
+    block_reduce_finish<1>(vb, acc, partials, ro);
   }
-  block_reduce_finish<1>(acc, partials, ro);
+};
+__global__ void __launch_bounds__(RED_THREADS) ncg_update_kernel(long long n, float2* __restrict__ x,
+    float2* __restrict__ d, const float2* __restrict__ g, float2* __restrict__ gr,
+    const float2* __restrict__ gAd, float2* __restrict__ g_prev, const float* __restrict__ diag,
+    long long ndiag, const double* __restrict__ s, double* __restrict__ partials, RedOut ro) {
+  NCGUpdate::run(hw_block(), n, x, d, g, gr, gAd, g_prev, diag, ndiag, s, partials, ro);
 }
 
 // d = -g/D (priming: cg.py:182-185) and Re<g,d>
-__global__ void __launch_bounds__(RED_THREADS) steepest_kernel(long long n, float2* __restrict__ d,
-                                                               const float2* __restrict__ g,
-                                                               float2* __restrict__ g_prev,
-                                                               const float* __restrict__ diag, long long ndiag,
-                                                               double* __restrict__ partials, RedOut ro) {
-  double acc[1] = {0.0};
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    float2 gv = g[i];
-    float Dv = diag ? diag[i % ndiag] : 1.f;
-    float2 dv = make_float2(-(gv.x / Dv), -(gv.y / Dv));
-    d[i] = dv;
-    if (g_prev) g_prev[i] = gv;
-    acc[0] += (double)(gv.x * dv.x + gv.y * dv.y);
+struct Steepest {
+  static constexpr int NT = RED_THREADS, MINB = 5;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, long long n, float2* __restrict__ d,
+      const float2* __restrict__ g, float2* __restrict__ g_prev, const float* __restrict__ diag,
+      long long ndiag, double* __restrict__ partials, const RedOut& ro) {
+    double acc[1] = {0.0};
+    const long long stride = (long long)vb.nx * blockDim.x;
+    for (long long i = (long long)vb.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+      float2 gv = g[i];
+      float Dv = diag ? diag[i % ndiag] : 1.f;
+      float2 dv = make_float2(-(gv.x / Dv), -(gv.y / Dv));
+      d[i] = dv;
+      if (g_prev) g_prev[i] = gv;
+      acc[0] += (double)(gv.x * dv.x + gv.y * dv.y);
+    }
+    block_reduce_finish<1>(vb, acc, partials, ro);
   }
-  block_reduce_finish<1>(acc, partials, ro);
+};
+__global__ void __launch_bounds__(RED_THREADS) steepest_kernel(long long n, float2* __restrict__ d,
+    const float2* __restrict__ g, float2* __restrict__ g_prev, const float* __restrict__ diag, long long ndiag,
+    double* __restrict__ partials, RedOut ro) {
+  Steepest::run(hw_block(), n, d, g, g_prev, diag, ndiag, partials, ro);
 }
 
 // Optional restart (not in the reference): when the updated direction is not a
@@ -817,78 +888,108 @@ __device__ __forceinline__ bool needs_restart(const double* s) {
   return s[S_LS_OK] != 0.0 && s[S_DONE] == 0.0 && !(s[S_G0D] < 0.0);
 }
 
-__global__ void __launch_bounds__(RED_THREADS) restart_dir_kernel(long long n, float2* __restrict__ d,
-                                                                  const float2* __restrict__ g,
-                                                                  const float* __restrict__ diag, long long ndiag,
-                                                                  const double* __restrict__ s) {
-  if (!needs_restart(s)) return;
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const float2 gv = g[i];
-    const float Dv = diag ? diag[i % ndiag] : 1.f;
-    d[i] = make_float2(-(gv.x / Dv), -(gv.y / Dv));
+struct RestartDir {
+  static constexpr int NT = RED_THREADS, MINB = 5;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, long long n, float2* __restrict__ d,
+      const float2* __restrict__ g, const float* __restrict__ diag, long long ndiag,
+      const double* __restrict__ s) {
+    if (!needs_restart(s)) return;
+    const long long stride = (long long)vb.nx * blockDim.x;
+    for (long long i = (long long)vb.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+      const float2 gv = g[i];
+      const float Dv = diag ? diag[i % ndiag] : 1.f;
+      d[i] = make_float2(-(gv.x / Dv), -(gv.y / Dv));
+    }
   }
+};
+__global__ void __launch_bounds__(RED_THREADS) restart_dir_kernel(long long n, float2* __restrict__ d,
+    const float2* __restrict__ g, const float* __restrict__ diag, long long ndiag, const double* __restrict__ s) {
+  RestartDir::run(hw_block(), n, d, g, diag, ndiag, s);
 }
 
+struct RestartSlot {
+  static constexpr int NT = 32, MINB = 1;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, double* s) {
+    if (threadIdx.x != 0 || !needs_restart(s)) return;
+    s[S_G0D] = -s[S_RED + MAX_TERMS + 1];
+    s[S_G0D_NEXT] = s[S_G0D];
+    s[S_NRESTART] += 1.0;
+  }
+};
 __global__ void restart_slot_kernel(double* s) {
-  if (threadIdx.x != 0 || !needs_restart(s)) return;
-  s[S_G0D] = -s[S_RED + MAX_TERMS + 1];
-  s[S_G0D_NEXT] = s[S_G0D];
-  s[S_NRESTART] += 1.0;
+  RestartSlot::run(hw_block(), s);
 }
 
 // ||r||^2 after an accepted step when r is not kept (Toeplitz schedule):
 // ||r + t Ad||^2 = err + 2 t Re<r, Ad> + t^2 ||Ad||^2.
+struct ErrStep {
+  static constexpr int NT = 32, MINB = 1;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, double* s) {
+    if (threadIdx.x != 0 || s[S_LS_OK] == 0.0) return;
+    const double t = s[S_T];
+    s[S_ERR] += 2.0 * t * s[S_ERD] + t * t * s[S_EDD];
+  }
+};
 __global__ void err_step_kernel(double* s) {
-  if (threadIdx.x != 0 || s[S_LS_OK] == 0.0) return;
-  const double t = s[S_T];
-  s[S_ERR] += 2.0 * t * s[S_ERD] + t * t * s[S_EDD];
+  ErrStep::run(hw_block(), s);
 }
 
-__global__ void copy_slot_kernel(double* s, int dst, int src) {
-  if (threadIdx.x == 0) s[dst] = s[src];
-}
-
-__global__ void set_steps_kernel(double* ts, int J, double beta) {
-  if (threadIdx.x == 0) {
-    ts[0] = 0.0;
-    double t = 1.0;
-    for (int j = 1; j < J; ++j) {
-      ts[j] = t;
-      t *= beta;
+struct SetSteps {
+  static constexpr int NT = 32, MINB = 1;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, double* ts, int J, double beta) {
+    if (threadIdx.x == 0) {
+      ts[0] = 0.0;
+      double t = 1.0;
+      for (int j = 1; j < J; ++j) {
+        ts[j] = t;
+        t *= beta;
+      }
     }
   }
+};
+__global__ void set_steps_kernel(double* ts, int J, double beta) {
+  SetSteps::run(hw_block(), ts, J, beta);
 }
 
 // Kernel instance for the plan's slot / unit counts (rounded up), so the
 // unrolled per-voxel loops keep only the accumulators in use.
 struct GradLaunch {
   template <int NS, int NU, class... A>
-  static void go(int nb, cudaStream_t st, A... args) { grad_kernel<NS, NU><<<nb, RED_THREADS, 0, st>>>(args...); }
+  static int go(int nb, cudaStream_t st, A... args) {
+    return mrb::launch<TVGrad<NS, NU>>(grad_kernel<NS, NU>, dim3(nb), 0, st, args...);
+  }
 };
 // trial steps per launch: up to 8 (the first Armijo phase) or up to MT_MAX_J
 template <int JMAX>
 struct MultiLaunch {
   template <int NS, int NU, class... A>
-  static void go(int nb, cudaStream_t st, A... args) {
-    tv_multi_kernel<NS, NU, JMAX><<<nb, RED_THREADS, 0, st>>>(args...);
+  static int go(int nb, cudaStream_t st, A... args) {
+    return mrb::launch<TVMulti<NS, NU, JMAX>>(tv_multi_kernel<NS, NU, JMAX>, dim3(nb), 0, st, args...);
   }
 };
 
 template <class L, int NS, class... A>
-void launch_tv_nu(const TVPlan& P, int nb, cudaStream_t st, A... args) {
-  if (P.nu <= 1) L::template go<NS, 1>(nb, st, args...);
-  else if (P.nu <= 2) L::template go<NS, 2>(nb, st, args...);
-  else if (P.nu <= 4) L::template go<NS, 4>(nb, st, args...);
-  else L::template go<NS, NUNIT>(nb, st, args...);
+int launch_tv_nu(const TVPlan& P, int nb, cudaStream_t st, A... args) {
+  if (P.nu <= 1) return L::template go<NS, 1>(nb, st, args...);
+  if (P.nu <= 2) return L::template go<NS, 2>(nb, st, args...);
+  if (P.nu <= 4) return L::template go<NS, 4>(nb, st, args...);
+  return L::template go<NS, NUNIT>(nb, st, args...);
 }
 
 template <class L, class... A>
-void launch_tv(const TVPlan& P, int nb, cudaStream_t st, A... args) {
-  if (P.ns <= 1) launch_tv_nu<L, 1>(P, nb, st, args...);
-  else if (P.ns <= 2) launch_tv_nu<L, 2>(P, nb, st, args...);
-  else if (P.ns <= 3) launch_tv_nu<L, 3>(P, nb, st, args...);
-  else launch_tv_nu<L, NSLOT>(P, nb, st, args...);
+int launch_tv(const TVPlan& P, int nb, cudaStream_t st, A... args) {
+  if (P.ns <= 1) return launch_tv_nu<L, 1>(P, nb, st, args...);
+  if (P.ns <= 2) return launch_tv_nu<L, 2>(P, nb, st, args...);
+  if (P.ns <= 3) return launch_tv_nu<L, 3>(P, nb, st, args...);
+  return launch_tv_nu<L, NSLOT>(P, nb, st, args...);
 }
 
 // grid of the TV passes: one wave of `per_sm` resident 256-thread blocks on every SM
@@ -1055,11 +1156,9 @@ extern "C" int mrb_kspace_pass(int mode, int64_t n, void* r, const void* Ad, con
   cudaStream_t st = (cudaStream_t)stream;
   int nb = red_blocks(n, 4);
   double* part = (double*)ws;
-  kspace_kernel<<<nb, RED_THREADS, 0, st>>>(mode, n, (float2*)r, (const float2*)Ad, (const float2*)Ax,
-                                            (const float2*)y, t_dev, t_host, skip, part,
-                                            red_out(ws, out, mode == 0 ? 3 : 1, 0, skip));
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<KSpace>(kspace_kernel, dim3(nb), 0, st, mode, n, (float2*)r, (const float2*)Ad,
+                             (const float2*)Ax, (const float2*)y, t_dev, t_host, skip, part,
+                             red_out(ws, out, mode == 0 ? 3 : 1, 0, skip));
 }
 
 extern "C" int mrb_tv_grad(int nd, const int* S, int F, const mrb_tv_term* terms, int nterms, const void* x,
@@ -1087,9 +1186,7 @@ extern "C" int mrb_tv_grad(int nd, const int* S, int F, const mrb_tv_term* terms
   // up to 3 difference axes the gradient pass keeps to 64 registers: 4 blocks per SM
   int nb = std::min(red_blocks(P.n, 2), tv_grid(P.ns <= 3 ? 4 : 3));
   double* part = (double*)ws;
-  launch_tv<GradLaunch>(P, nb, st, a, P, part, red_out(ws, out, GP_NV, 0, nullptr));
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return launch_tv<GradLaunch>(P, nb, st, a, P, part, red_out(ws, out, GP_NV, 0, nullptr));
 }
 
 extern "C" int mrb_tv_multi(int nd, const int* S, int F, const mrb_tv_term* terms, int nterms, const void* x,
@@ -1105,37 +1202,29 @@ extern "C" int mrb_tv_multi(int nd, const int* S, int F, const mrb_tv_term* term
   int nb = std::min(red_blocks(P.n, 2), tv_grid(J <= 8 ? 4 : 3));
   double* part = (double*)ws;
   if (J <= 8)
-    launch_tv<MultiLaunch<8>>(P, nb, st, (const float2*)x, (const float2*)d, ts, J, P, skip, part,
-                              red_out(ws, out, J, 0, skip));
-  else
-    launch_tv<MultiLaunch<MT_MAX_J>>(P, nb, st, (const float2*)x, (const float2*)d, ts, J, P, skip, part,
+    return launch_tv<MultiLaunch<8>>(P, nb, st, (const float2*)x, (const float2*)d, ts, J, P, skip, part,
                                      red_out(ws, out, J, 0, skip));
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return launch_tv<MultiLaunch<MT_MAX_J>>(P, nb, st, (const float2*)x, (const float2*)d, ts, J, P, skip, part,
+                                          red_out(ws, out, J, 0, skip));
 }
 
 extern "C" int mrb_ncg_armijo_select(double* slots, const double* cfg, mrb_stream_t stream) {
   MRB_REQUIRE(slots != nullptr && cfg != nullptr, "null pointer");
-  armijo_select_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slots, cfg);
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<ArmijoSelect>(armijo_select_kernel, dim3(1), 0, (cudaStream_t)stream, slots, cfg);
 }
 
 extern "C" int mrb_ncg_armijo_phase(double* slots, const double* cfg, int J1, int phase, mrb_stream_t stream) {
   MRB_REQUIRE(slots != nullptr && cfg != nullptr, "null pointer");
   MRB_REQUIRE(phase == 1 || phase == 2, "phase must be 1 or 2");
   MRB_REQUIRE(J1 >= 2 && J1 <= MT_MAX_J, "J1 out of range");
-  armijo_phase_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slots, cfg, J1, phase);
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<ArmijoPhase>(armijo_phase_kernel, dim3(1), 0, (cudaStream_t)stream, slots, cfg, J1, phase);
 }
 
 extern "C" int mrb_ncg_control(double* slots, double* hist, const double* cfg, int nterms, int have_ft,
                                mrb_stream_t stream) {
   MRB_REQUIRE(slots != nullptr && hist != nullptr && cfg != nullptr, "null pointer");
-  ncg_control_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slots, hist, cfg, nterms, have_ft);
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<NCGControl>(ncg_control_kernel, dim3(1), 0, (cudaStream_t)stream, slots, hist, cfg, nterms,
+                                 have_ft);
 }
 
 extern "C" int mrb_ncg_update(int64_t n, void* x, void* d, const void* g, void* gr, const void* gAd, void* g_prev,
@@ -1146,31 +1235,24 @@ extern "C" int mrb_ncg_update(int64_t n, void* x, void* d, const void* g, void* 
   int nb = red_blocks(n, 2);
   double* part = (double*)ws;
   // next slope at t = 0 -> S_G0D_NEXT and S_G0D
-  ncg_update_kernel<<<nb, RED_THREADS, 0, st>>>(n, (float2*)x, (float2*)d, (const float2*)g, (float2*)gr,
-                                                 (const float2*)gAd, (float2*)g_prev, diag, ndiag > 0 ? ndiag : 1,
-                                                 slots, part,
-                                                 red_out(ws, slots + S_G0D_NEXT, 1, 0, nullptr, slots + S_G0D));
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<NCGUpdate>(ncg_update_kernel, dim3(nb), 0, st, n, (float2*)x, (float2*)d, (const float2*)g,
+                                (float2*)gr, (const float2*)gAd, (float2*)g_prev, diag, ndiag > 0 ? ndiag : 1, slots,
+                                part, red_out(ws, slots + S_G0D_NEXT, 1, 0, nullptr, slots + S_G0D));
 }
 
 extern "C" int mrb_ncg_err_step(double* slots, mrb_stream_t stream) {
   MRB_REQUIRE(slots != nullptr, "null slots");
-  err_step_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slots);
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<ErrStep>(err_step_kernel, dim3(1), 0, (cudaStream_t)stream, slots);
 }
 
 extern "C" int mrb_ncg_restart(int64_t n, void* d, const void* g, const float* diag, int64_t ndiag, double* slots,
                                mrb_stream_t stream) {
   MRB_REQUIRE(d && g && slots, "null pointer");
   cudaStream_t st = (cudaStream_t)stream;
-  restart_dir_kernel<<<red_blocks(n, 2), RED_THREADS, 0, st>>>(n, (float2*)d, (const float2*)g, diag,
-                                                               ndiag > 0 ? ndiag : 1, slots);
-  MRB_LAUNCH_CHECK();
-  restart_slot_kernel<<<1, 32, 0, st>>>(slots);
-  MRB_LAUNCH_CHECK();
-  return 0;
+  if (int rc = mrb::launch<RestartDir>(restart_dir_kernel, dim3(red_blocks(n, 2)), 0, st, n, (float2*)d,
+                                      (const float2*)g, diag, ndiag > 0 ? ndiag : 1, slots))
+    return rc;
+  return mrb::launch<RestartSlot>(restart_slot_kernel, dim3(1), 0, st, slots);
 }
 
 extern "C" int mrb_ncg_steepest(int64_t n, void* d, const void* g, void* g_prev, const float* diag, int64_t ndiag,
@@ -1179,17 +1261,13 @@ extern "C" int mrb_ncg_steepest(int64_t n, void* d, const void* g, void* g_prev,
   cudaStream_t st = (cudaStream_t)stream;
   int nb = red_blocks(n, 2);
   double* part = (double*)ws;
-  steepest_kernel<<<nb, RED_THREADS, 0, st>>>(n, (float2*)d, (const float2*)g, (float2*)g_prev, diag,
-                                               ndiag > 0 ? ndiag : 1, part, red_out(ws, out, 1, 0, nullptr));
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<Steepest>(steepest_kernel, dim3(nb), 0, st, n, (float2*)d, (const float2*)g, (float2*)g_prev,
+                               diag, ndiag > 0 ? ndiag : 1, part, red_out(ws, out, 1, 0, nullptr));
 }
 
 extern "C" int mrb_ncg_set_steps(double* ts, int J, double beta, mrb_stream_t stream) {
   MRB_REQUIRE(ts != nullptr && J >= 1 && J <= MT_MAX_J, "bad step table");
-  set_steps_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(ts, J, beta);
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<SetSteps>(set_steps_kernel, dim3(1), 0, (cudaStream_t)stream, ts, J, beta);
 }
 
 // ===========================================================================
@@ -1391,81 +1469,90 @@ constexpr int GRAPH_TILE = 32;
 // mode 1: y = L d, acc += y, out[0] = Re<x, y>, out[1] = Re<d, y>
 // mode 2: mode 1 for a non-symmetric L: out[0] = Re<x, (L + L^T)/2 d> (the slope
 //         of the energy along d; the accumulated L d stays the reference's gradient)
-__global__ void __launch_bounds__(RED_THREADS) graph_kernel(int mode, int B, long long N, const float* __restrict__ L,
-                                                            const float2* __restrict__ x,
-                                                            const float2* __restrict__ d, const double* t_dev,
-                                                            double t_host, float2* __restrict__ acc,
-                                                            const double* skip, double* __restrict__ partials,
-                                                            RedOut ro) {
-  if (skipped(skip) != 0.0) return;   // uniform over the grid: no partials, no counter
-  extern __shared__ __align__(16) unsigned char graph_smem[];
-  float2* Z = reinterpret_cast<float2*>(graph_smem);         // B x GRAPH_TILE
-  float* Ls = reinterpret_cast<float*>(Z + B * GRAPH_TILE);  // B x B
-  for (int i = threadIdx.x; i < B * B; i += blockDim.x) Ls[i] = L[i];
-  const float t = (float)(t_dev ? *t_dev : t_host);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  double r0 = 0.0, r1 = 0.0;
-  const long long ntiles = (N + GRAPH_TILE - 1) / GRAPH_TILE;
-  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long long p = tile * GRAPH_TILE + lane;
-    const bool in = p < N;
-    __syncthreads();   // L staged; the previous tile's columns consumed
-    for (int f = warp; f < B; f += nw) {
-      float2 v = make_float2(0.f, 0.f);
-      if (in) {
-        const long long i = (long long)f * N + p;
-        if (mode == 0) {
-          v = x[i];
-          if (d) {
-            const float2 dv = d[i];
-            v.x = __fadd_rn(v.x, __fmul_rn(dv.x, t));
-            v.y = __fadd_rn(v.y, __fmul_rn(dv.y, t));
+struct GraphPass {
+  static constexpr int NT = RED_THREADS, MINB = 1;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, int mode, int B, long long N,
+      const float* __restrict__ L, const float2* __restrict__ x, const float2* __restrict__ d,
+      const double* t_dev, double t_host, float2* __restrict__ acc, const double* skip,
+      double* __restrict__ partials, const RedOut& ro) {
+    if (skipped(skip) != 0.0) return;   // uniform over the grid: no partials, no counter
+    extern __shared__ __align__(16) unsigned char graph_smem[];
+    float2* Z = reinterpret_cast<float2*>(graph_smem);         // B x GRAPH_TILE
+    float* Ls = reinterpret_cast<float*>(Z + B * GRAPH_TILE);  // B x B
+    for (int i = threadIdx.x; i < B * B; i += blockDim.x) Ls[i] = L[i];
+    const float t = (float)(t_dev ? *t_dev : t_host);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double r0 = 0.0, r1 = 0.0;
+    const long long ntiles = (N + GRAPH_TILE - 1) / GRAPH_TILE;
+    for (long long tile = vb.x; tile < ntiles; tile += vb.nx) {
+      const long long p = tile * GRAPH_TILE + lane;
+      const bool in = p < N;
+      __syncthreads();   // L staged; the previous tile's columns consumed
+      for (int f = warp; f < B; f += nw) {
+        float2 v = make_float2(0.f, 0.f);
+        if (in) {
+          const long long i = (long long)f * N + p;
+          if (mode == 0) {
+            v = x[i];
+            if (d) {
+              const float2 dv = d[i];
+              v.x = __fadd_rn(v.x, __fmul_rn(dv.x, t));
+              v.y = __fadd_rn(v.y, __fmul_rn(dv.y, t));
+            }
+          } else {
+            v = d[i];
           }
-        } else {
-          v = d[i];
         }
+        Z[f * GRAPH_TILE + lane] = v;
       }
-      Z[f * GRAPH_TILE + lane] = v;
-    }
-    __syncthreads();
-    for (int f = warp; f < B; f += nw) {
-      const float* Lr = Ls + f * B;
-      float yx = 0.f, yy = 0.f, tx = 0.f, ty = 0.f;
-      for (int s2 = 0; s2 < B; ++s2) {
-        const float l = Lr[s2];
-        const float2 z = Z[s2 * GRAPH_TILE + lane];
-        yx = fmaf(l, z.x, yx);
-        yy = fmaf(l, z.y, yy);
-        if (mode == 2) {
-          const float lt = Ls[s2 * B + f];
-          tx = fmaf(lt, z.x, tx);
-          ty = fmaf(lt, z.y, ty);
+      __syncthreads();
+      for (int f = warp; f < B; f += nw) {
+        const float* Lr = Ls + f * B;
+        float yx = 0.f, yy = 0.f, tx = 0.f, ty = 0.f;
+        for (int s2 = 0; s2 < B; ++s2) {
+          const float l = Lr[s2];
+          const float2 z = Z[s2 * GRAPH_TILE + lane];
+          yx = fmaf(l, z.x, yx);
+          yy = fmaf(l, z.y, yy);
+          if (mode == 2) {
+            const float lt = Ls[s2 * B + f];
+            tx = fmaf(lt, z.x, tx);
+            ty = fmaf(lt, z.y, ty);
+          }
         }
-      }
-      if (in) {
-        const long long i = (long long)f * N + p;
-        const float2 zf = Z[f * GRAPH_TILE + lane];
-        if (acc) {
-          float2 a = acc[i];
-          a.x += yx;
-          a.y += yy;
-          acc[i] = a;
-        }
-        if (mode == 0) {
-          r0 += (double)(zf.x * yx + zf.y * yy);
-        } else {
-          const float2 xv = x[i];
-          if (mode == 1)
-            r0 += (double)(xv.x * yx + xv.y * yy);
-          else
-            r0 += 0.5 * (double)(xv.x * (yx + tx) + xv.y * (yy + ty));
-          r1 += (double)(zf.x * yx + zf.y * yy);
+        if (in) {
+          const long long i = (long long)f * N + p;
+          const float2 zf = Z[f * GRAPH_TILE + lane];
+          if (acc) {
+            float2 a = acc[i];
+            a.x += yx;
+            a.y += yy;
+            acc[i] = a;
+          }
+          if (mode == 0) {
+            r0 += (double)(zf.x * yx + zf.y * yy);
+          } else {
+            const float2 xv = x[i];
+            if (mode == 1)
+              r0 += (double)(xv.x * yx + xv.y * yy);
+            else
+              r0 += 0.5 * (double)(xv.x * (yx + tx) + xv.y * (yy + ty));
+            r1 += (double)(zf.x * yx + zf.y * yy);
+          }
         }
       }
     }
+    double v[2] = {mode == 0 ? 0.5 * r0 : r0, r1};
+    block_reduce_finish<2>(vb, v, partials, ro);
   }
-  double v[2] = {mode == 0 ? 0.5 * r0 : r0, r1};
-  block_reduce_finish<2>(v, partials, ro);
+};
+__global__ void __launch_bounds__(RED_THREADS) graph_kernel(int mode, int B, long long N,
+    const float* __restrict__ L, const float2* __restrict__ x, const float2* __restrict__ d,
+    const double* t_dev, double t_host, float2* __restrict__ acc, const double* skip,
+    double* __restrict__ partials, RedOut ro) {
+  GraphPass::run(hw_block(), mode, B, N, L, x, d, t_dev, t_host, acc, skip, partials, ro);
 }
 
 // The graph term is quadratic, so the fast schedule carries it beside the
@@ -1473,20 +1560,28 @@ __global__ void __launch_bounds__(RED_THREADS) graph_kernel(int mode, int B, lon
 // phase 0 (prime):     err += 2 q0
 // phase 1 (iteration): err += 2 q0, erd += q1, edd += q2 (after the k-space scalars)
 // phase 2 (update):    q0 += t q1 + t^2 q2 / 2 at the accepted step
-__global__ void quad_fold_kernel(double* s, int phase) {
-  if (threadIdx.x != 0) return;
-  if (phase == 0) {
-    s[S_ERR] += 2.0 * s[S_GQ0];
-  } else if (phase == 1) {
-    if (s[S_DONE] != 0.0) return;
-    s[S_ERR] += 2.0 * s[S_GQ0];
-    s[S_ERD] += s[S_GQ1];
-    s[S_EDD] += s[S_GQ2];
-  } else {
-    if (s[S_LS_OK] == 0.0) return;
-    const double t = s[S_T];
-    s[S_GQ0] += t * s[S_GQ1] + 0.5 * t * t * s[S_GQ2];
+struct QuadFold {
+  static constexpr int NT = 32, MINB = 1;
+  static constexpr bool SHARED_CODE = true;
+  static constexpr int MAXG = 16;
+  static __device__ __forceinline__ void run(const VBlock& vb, double* s, int phase) {
+    if (threadIdx.x != 0) return;
+    if (phase == 0) {
+      s[S_ERR] += 2.0 * s[S_GQ0];
+    } else if (phase == 1) {
+      if (s[S_DONE] != 0.0) return;
+      s[S_ERR] += 2.0 * s[S_GQ0];
+      s[S_ERD] += s[S_GQ1];
+      s[S_EDD] += s[S_GQ2];
+    } else {
+      if (s[S_LS_OK] == 0.0) return;
+      const double t = s[S_T];
+      s[S_GQ0] += t * s[S_GQ1] + 0.5 * t * t * s[S_GQ2];
+    }
   }
+};
+__global__ void quad_fold_kernel(double* s, int phase) {
+  QuadFold::run(hw_block(), s, phase);
 }
 
 __global__ void __launch_bounds__(256) diag_frames_kernel(long long n, long long P, const float* __restrict__ v,
@@ -1518,19 +1613,15 @@ extern "C" int mrb_graph_pass(int mode, int B, int64_t N, const float* L, const 
   const long long ntiles = (N + GRAPH_TILE - 1) / GRAPH_TILE;
   const int nb = (int)std::min<long long>(ntiles, 148LL * 6);
   double* part = (double*)ws;
-  graph_kernel<<<nb, RED_THREADS, smem, (cudaStream_t)stream>>>(
-      mode, B, (long long)N, L, (const float2*)x, (const float2*)d, t_dev, t_host, (float2*)acc, skip, part,
-      red_out(ws, out, mode == 0 ? 1 : 2, 0, skip));
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<GraphPass>(graph_kernel, dim3(nb), smem, (cudaStream_t)stream, mode, B, (long long)N, L,
+                                (const float2*)x, (const float2*)d, t_dev, t_host, (float2*)acc, skip, part,
+                                red_out(ws, out, mode == 0 ? 1 : 2, 0, skip));
 }
 
 extern "C" int mrb_ncg_quad_fold(double* slots, int phase, mrb_stream_t stream) {
   MRB_REQUIRE(slots != nullptr, "null pointer");
   MRB_REQUIRE(phase >= 0 && phase <= 2, "phase must be 0, 1 or 2");
-  quad_fold_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(slots, phase);
-  MRB_LAUNCH_CHECK();
-  return 0;
+  return mrb::launch<QuadFold>(quad_fold_kernel, dim3(1), 0, (cudaStream_t)stream, slots, phase);
 }
 
 // ===========================================================================

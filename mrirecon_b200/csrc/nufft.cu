@@ -26,9 +26,12 @@
 
 #include "mrb_common.cuh"
 #include "fft.cuh"
+#include "group.cuh"
 
 using mrb::DevBuf;
 using mrb::KBPoly;
+using mrb::VBlock;
+using mrb::hw_block;
 
 struct mrb_plan {
   int nd = 2;
@@ -418,113 +421,121 @@ struct InterpArgs {
 };
 
 template <int ND>
-__global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly kb) {
-  constexpr int W = 4;
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  long long kk = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  int be = blockIdx.y;
-  if (kk >= g.K) return;
-  int b = frame_of(be, a.nb, g.B);
-  long long k = a.order ? a.order[(long long)b * g.K + kk] : kk;
-  float w[ND][W];
-  int nidx[ND][W];
-#pragma unroll
-  for (int d = 0; d < ND; ++d) {
-    float x = a.gx[((long long)b * ND + d) * g.K + k];
-    int base = (int)floorf(x);
-    const float fx = x - (float)base;
-#pragma unroll
-    for (int o = 0; o < W; ++o) {
-      int n = base - (W / 2 - 1) + o;
-      float wd = mrb::kb_tap(kb, o, fx);
-      w[d][o] = (n & 1) ? -wd : wd;
-      nidx[d][o] = mrb::wrap_i(n, g.G[d]);
-    }
-  }
-  float s = a.scale * a.gsign;
-  if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
-  const float2* gb = a.grid + (long long)be * g.C * g.gtot;
-  float2* yo = a.y + (long long)be * g.C * g.K + k;
-  if (ND == 2) {
-    // row offsets shared by all coils
-    long long roff[W];
-#pragma unroll
-    for (int i0 = 0; i0 < W; ++i0) roff[i0] = (long long)nidx[0][i0] * g.G[1];
-    // two coils per pass: 32 independent loads in flight per thread
-    int c = 0;
-    for (; c + 1 < g.C; c += 2) {
-      const float2* g0 = gb + (long long)c * g.gtot;
-      const float2* g1 = g0 + g.gtot;
-      float2 v0[W][W], v1[W][W];
-#pragma unroll
-      for (int i0 = 0; i0 < W; ++i0)
-#pragma unroll
-        for (int i1 = 0; i1 < W; ++i1) {
-          v0[i0][i1] = __ldg(g0 + roff[i0] + nidx[1][i1]);
-          v1[i0][i1] = __ldg(g1 + roff[i0] + nidx[1][i1]);
-        }
-      float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
-#pragma unroll
-      for (int i0 = 0; i0 < W; ++i0) {
-        float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
-#pragma unroll
-        for (int i1 = 0; i1 < W; ++i1) {
-          a0 = fmaf(w[1][i1], v0[i0][i1].x, a0);
-          b0 = fmaf(w[1][i1], v0[i0][i1].y, b0);
-          a1 = fmaf(w[1][i1], v1[i0][i1].x, a1);
-          b1 = fmaf(w[1][i1], v1[i0][i1].y, b1);
-        }
-        r0 = fmaf(w[0][i0], a0, r0);
-        m0 = fmaf(w[0][i0], b0, m0);
-        r1 = fmaf(w[0][i0], a1, r1);
-        m1 = fmaf(w[0][i0], b1, m1);
+struct InterpGen {
+  static constexpr int NT = 256, MINB = (ND == 2 ? 4 : 1);
+  static __device__ __forceinline__ void run(const VBlock& vb, const InterpArgs& a, const Geo& g,
+      const KBPoly& kb) {
+    constexpr int W = 4;
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    long long kk = (long long)vb.x * blockDim.x + threadIdx.x;
+    int be = vb.y;
+    if (kk >= g.K) return;
+    int b = frame_of(be, a.nb, g.B);
+    long long k = a.order ? a.order[(long long)b * g.K + kk] : kk;
+    float w[ND][W];
+    int nidx[ND][W];
+  #pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      float x = a.gx[((long long)b * ND + d) * g.K + k];
+      int base = (int)floorf(x);
+      const float fx = x - (float)base;
+  #pragma unroll
+      for (int o = 0; o < W; ++o) {
+        int n = base - (W / 2 - 1) + o;
+        float wd = mrb::kb_tap(kb, o, fx);
+        w[d][o] = (n & 1) ? -wd : wd;
+        nidx[d][o] = mrb::wrap_i(n, g.G[d]);
       }
-      yo[(long long)c * g.K] = make_float2(r0 * s, m0 * s);
-      yo[(long long)(c + 1) * g.K] = make_float2(r1 * s, m1 * s);
     }
-    for (; c < g.C; ++c) {
-      const float2* g0 = gb + (long long)c * g.gtot;
-      float r0 = 0.f, m0 = 0.f;
-#pragma unroll
-      for (int i0 = 0; i0 < W; ++i0) {
-        float a0 = 0.f, b0 = 0.f;
-#pragma unroll
-        for (int i1 = 0; i1 < W; ++i1) {
-          float2 v = __ldg(g0 + roff[i0] + nidx[1][i1]);
-          a0 = fmaf(w[1][i1], v.x, a0);
-          b0 = fmaf(w[1][i1], v.y, b0);
-        }
-        r0 = fmaf(w[0][i0], a0, r0);
-        m0 = fmaf(w[0][i0], b0, m0);
-      }
-      yo[(long long)c * g.K] = make_float2(r0 * s, m0 * s);
-    }
-  } else {
-    for (int c = 0; c < g.C; ++c) {
-      const float2* gc = gb + (long long)c * g.gtot;
-      float re = 0.f, im = 0.f;
-#pragma unroll
-      for (int i0 = 0; i0 < W; ++i0) {
-        float r1 = 0.f, im1 = 0.f;
-#pragma unroll
-        for (int i1 = 0; i1 < W; ++i1) {
-          const float2* row = gc + ((long long)nidx[0][i0] * g.G[1] + nidx[1][i1]) * g.G[ND - 1];
-          float r2 = 0.f, i2 = 0.f;
-#pragma unroll
-          for (int i2x = 0; i2x < W; ++i2x) {
-            float2 v = __ldg(row + nidx[ND - 1][i2x]);
-            r2 = fmaf(w[ND - 1][i2x], v.x, r2);
-            i2 = fmaf(w[ND - 1][i2x], v.y, i2);
+    float s = a.scale * a.gsign;
+    if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
+    const float2* gb = a.grid + (long long)be * g.C * g.gtot;
+    float2* yo = a.y + (long long)be * g.C * g.K + k;
+    if (ND == 2) {
+      // row offsets shared by all coils
+      long long roff[W];
+  #pragma unroll
+      for (int i0 = 0; i0 < W; ++i0) roff[i0] = (long long)nidx[0][i0] * g.G[1];
+      // two coils per pass: 32 independent loads in flight per thread
+      int c = 0;
+      for (; c + 1 < g.C; c += 2) {
+        const float2* g0 = gb + (long long)c * g.gtot;
+        const float2* g1 = g0 + g.gtot;
+        float2 v0[W][W], v1[W][W];
+  #pragma unroll
+        for (int i0 = 0; i0 < W; ++i0)
+  #pragma unroll
+          for (int i1 = 0; i1 < W; ++i1) {
+            v0[i0][i1] = __ldg(g0 + roff[i0] + nidx[1][i1]);
+            v1[i0][i1] = __ldg(g1 + roff[i0] + nidx[1][i1]);
           }
-          r1 = fmaf(w[1][i1], r2, r1);
-          im1 = fmaf(w[1][i1], i2, im1);
+        float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
+  #pragma unroll
+        for (int i0 = 0; i0 < W; ++i0) {
+          float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
+  #pragma unroll
+          for (int i1 = 0; i1 < W; ++i1) {
+            a0 = fmaf(w[1][i1], v0[i0][i1].x, a0);
+            b0 = fmaf(w[1][i1], v0[i0][i1].y, b0);
+            a1 = fmaf(w[1][i1], v1[i0][i1].x, a1);
+            b1 = fmaf(w[1][i1], v1[i0][i1].y, b1);
+          }
+          r0 = fmaf(w[0][i0], a0, r0);
+          m0 = fmaf(w[0][i0], b0, m0);
+          r1 = fmaf(w[0][i0], a1, r1);
+          m1 = fmaf(w[0][i0], b1, m1);
         }
-        re = fmaf(w[0][i0], r1, re);
-        im = fmaf(w[0][i0], im1, im);
+        yo[(long long)c * g.K] = make_float2(r0 * s, m0 * s);
+        yo[(long long)(c + 1) * g.K] = make_float2(r1 * s, m1 * s);
       }
-      yo[(long long)c * g.K] = make_float2(re * s, im * s);
+      for (; c < g.C; ++c) {
+        const float2* g0 = gb + (long long)c * g.gtot;
+        float r0 = 0.f, m0 = 0.f;
+  #pragma unroll
+        for (int i0 = 0; i0 < W; ++i0) {
+          float a0 = 0.f, b0 = 0.f;
+  #pragma unroll
+          for (int i1 = 0; i1 < W; ++i1) {
+            float2 v = __ldg(g0 + roff[i0] + nidx[1][i1]);
+            a0 = fmaf(w[1][i1], v.x, a0);
+            b0 = fmaf(w[1][i1], v.y, b0);
+          }
+          r0 = fmaf(w[0][i0], a0, r0);
+          m0 = fmaf(w[0][i0], b0, m0);
+        }
+        yo[(long long)c * g.K] = make_float2(r0 * s, m0 * s);
+      }
+    } else {
+      for (int c = 0; c < g.C; ++c) {
+        const float2* gc = gb + (long long)c * g.gtot;
+        float re = 0.f, im = 0.f;
+  #pragma unroll
+        for (int i0 = 0; i0 < W; ++i0) {
+          float r1 = 0.f, im1 = 0.f;
+  #pragma unroll
+          for (int i1 = 0; i1 < W; ++i1) {
+            const float2* row = gc + ((long long)nidx[0][i0] * g.G[1] + nidx[1][i1]) * g.G[ND - 1];
+            float r2 = 0.f, i2 = 0.f;
+  #pragma unroll
+            for (int i2x = 0; i2x < W; ++i2x) {
+              float2 v = __ldg(row + nidx[ND - 1][i2x]);
+              r2 = fmaf(w[ND - 1][i2x], v.x, r2);
+              i2 = fmaf(w[ND - 1][i2x], v.y, i2);
+            }
+            r1 = fmaf(w[1][i1], r2, r1);
+            im1 = fmaf(w[1][i1], i2, im1);
+          }
+          re = fmaf(w[0][i0], r1, re);
+          im = fmaf(w[0][i0], im1, im);
+        }
+        yo[(long long)c * g.K] = make_float2(re * s, im * s);
+      }
     }
   }
+};
+template <int ND>
+__global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly kb) {
+  InterpGen<ND>::run(hw_block(), a, g, kb);
 }
 
 // 2D forward interp, one thread per (sample, coil pair): the 16 taps of both
@@ -533,65 +544,72 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly
 // is hidden by parallelism rather than by a per-thread loop over the coils.
 // Blocks cover 256 consecutive samples of one coil pair (coalesced sample
 // reads and result writes).  Same summation order as interp_kernel<2>.
+struct Interp2p {
+  static constexpr int NT = 256, MINB = 4;
+  static __device__ __forceinline__ void run(const VBlock& vb, const InterpArgs& a, const Geo& g,
+      const KBPoly& kb) {
+    constexpr int W = 4;
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    const int kblocks = (int)((g.K + 255) / 256);
+    const int pr = vb.x / kblocks;
+    const long long k = (long long)(vb.x - pr * kblocks) * 256 + threadIdx.x;
+    const int be = vb.y;
+    if (k >= g.K) return;
+    const int b = frame_of(be, a.nb, g.B);
+    float w[2][W];
+    int nidx[2][W];
+  #pragma unroll
+    for (int d = 0; d < 2; ++d) {
+      const float x = a.gx[((long long)b * 2 + d) * g.K + k];
+      const int base = (int)floorf(x);
+      const float fx = x - (float)base;
+  #pragma unroll
+      for (int o = 0; o < W; ++o) {
+        const int n = base - (W / 2 - 1) + o;
+        const float wd = mrb::kb_tap(kb, o, fx);
+        w[d][o] = (n & 1) ? -wd : wd;
+        nidx[d][o] = mrb::wrap_i(n, g.G[d]);
+      }
+    }
+    float s = a.scale * a.gsign;
+    if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
+    const int c = 2 * pr;
+    const bool two = c + 1 < g.C;
+    const float2* g0 = a.grid + ((long long)be * g.C + c) * g.gtot;
+    const float2* g1 = two ? g0 + g.gtot : g0;
+    float2 v0[W][W], v1[W][W];
+  #pragma unroll
+    for (int i0 = 0; i0 < W; ++i0) {
+      const int roff = nidx[0][i0] * g.G[1];
+  #pragma unroll
+      for (int i1 = 0; i1 < W; ++i1) {
+        v0[i0][i1] = __ldg(g0 + roff + nidx[1][i1]);
+        v1[i0][i1] = two ? __ldg(g1 + roff + nidx[1][i1]) : make_float2(0.f, 0.f);
+      }
+    }
+    float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
+  #pragma unroll
+    for (int i0 = 0; i0 < W; ++i0) {
+      float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
+  #pragma unroll
+      for (int i1 = 0; i1 < W; ++i1) {
+        a0 = fmaf(w[1][i1], v0[i0][i1].x, a0);
+        b0 = fmaf(w[1][i1], v0[i0][i1].y, b0);
+        a1 = fmaf(w[1][i1], v1[i0][i1].x, a1);
+        b1 = fmaf(w[1][i1], v1[i0][i1].y, b1);
+      }
+      r0 = fmaf(w[0][i0], a0, r0);
+      m0 = fmaf(w[0][i0], b0, m0);
+      r1 = fmaf(w[0][i0], a1, r1);
+      m1 = fmaf(w[0][i0], b1, m1);
+    }
+    float2* yo = a.y + ((long long)be * g.C + c) * g.K + k;
+    yo[0] = make_float2(r0 * s, m0 * s);
+    if (two) yo[g.K] = make_float2(r1 * s, m1 * s);
+  }
+};
 __global__ void __launch_bounds__(256) interp2p_kernel(InterpArgs a, Geo g, KBPoly kb) {
-  constexpr int W = 4;
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  const int kblocks = (int)((g.K + 255) / 256);
-  const int pr = blockIdx.x / kblocks;
-  const long long k = (long long)(blockIdx.x - pr * kblocks) * 256 + threadIdx.x;
-  const int be = blockIdx.y;
-  if (k >= g.K) return;
-  const int b = frame_of(be, a.nb, g.B);
-  float w[2][W];
-  int nidx[2][W];
-#pragma unroll
-  for (int d = 0; d < 2; ++d) {
-    const float x = a.gx[((long long)b * 2 + d) * g.K + k];
-    const int base = (int)floorf(x);
-    const float fx = x - (float)base;
-#pragma unroll
-    for (int o = 0; o < W; ++o) {
-      const int n = base - (W / 2 - 1) + o;
-      const float wd = mrb::kb_tap(kb, o, fx);
-      w[d][o] = (n & 1) ? -wd : wd;
-      nidx[d][o] = mrb::wrap_i(n, g.G[d]);
-    }
-  }
-  float s = a.scale * a.gsign;
-  if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
-  const int c = 2 * pr;
-  const bool two = c + 1 < g.C;
-  const float2* g0 = a.grid + ((long long)be * g.C + c) * g.gtot;
-  const float2* g1 = two ? g0 + g.gtot : g0;
-  float2 v0[W][W], v1[W][W];
-#pragma unroll
-  for (int i0 = 0; i0 < W; ++i0) {
-    const int roff = nidx[0][i0] * g.G[1];
-#pragma unroll
-    for (int i1 = 0; i1 < W; ++i1) {
-      v0[i0][i1] = __ldg(g0 + roff + nidx[1][i1]);
-      v1[i0][i1] = two ? __ldg(g1 + roff + nidx[1][i1]) : make_float2(0.f, 0.f);
-    }
-  }
-  float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
-#pragma unroll
-  for (int i0 = 0; i0 < W; ++i0) {
-    float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
-#pragma unroll
-    for (int i1 = 0; i1 < W; ++i1) {
-      a0 = fmaf(w[1][i1], v0[i0][i1].x, a0);
-      b0 = fmaf(w[1][i1], v0[i0][i1].y, b0);
-      a1 = fmaf(w[1][i1], v1[i0][i1].x, a1);
-      b1 = fmaf(w[1][i1], v1[i0][i1].y, b1);
-    }
-    r0 = fmaf(w[0][i0], a0, r0);
-    m0 = fmaf(w[0][i0], b0, m0);
-    r1 = fmaf(w[0][i0], a1, r1);
-    m1 = fmaf(w[0][i0], b1, m1);
-  }
-  float2* yo = a.y + ((long long)be * g.C + c) * g.K + k;
-  yo[0] = make_float2(r0 * s, m0 * s);
-  if (two) yo[g.K] = make_float2(r1 * s, m1 * s);
+  Interp2p::run(hw_block(), a, g, kb);
 }
 
 // 2D forward interp on the coil-quad grid (be, coil quad, cell, coil in quad)
@@ -603,73 +621,80 @@ __global__ void __launch_bounds__(256) interp2p_kernel(InterpArgs a, Geo g, KBPo
 // S = 256 / P consecutive samples; the results go through shared memory so
 // that each coil's samples are stored as one run.  Taps, weights and summation
 // order are those of interp2p_kernel: identical samples.  C % 4 == 0.
+struct Interp2Quad {
+  static constexpr int NT = 256, MINB = 4;
+  static __device__ __forceinline__ void run(const VBlock& vb, const InterpArgs& a, const Geo& g,
+      const KBPoly& kb) {
+    constexpr int W = 4;
+    __shared__ float2 ys[512];   // [coil][sample]: C * S <= 2 * P * S <= 512
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    const int C = g.C;
+    const int P = (C + 1) >> 1;
+    const int S = 256 / P;
+    const long long k0 = (long long)vb.x * S;
+    const int be = vb.y;
+    const int b = frame_of(be, a.nb, g.B);
+    const int ks = threadIdx.x / P, pr = threadIdx.x - ks * P;
+    const long long k = k0 + ks;
+    if (ks < S && k < g.K) {
+      float w[2][W];
+      int nidx[2][W];
+  #pragma unroll
+      for (int d = 0; d < 2; ++d) {
+        const float x = a.gx[((long long)b * 2 + d) * g.K + k];
+        const int base = (int)floorf(x);
+        const float fx = x - (float)base;
+  #pragma unroll
+        for (int o = 0; o < W; ++o) {
+          const int n = base - (W / 2 - 1) + o;
+          const float wd = mrb::kb_tap(kb, o, fx);
+          w[d][o] = (n & 1) ? -wd : wd;
+          nidx[d][o] = mrb::wrap_i(n, g.G[d]);
+        }
+      }
+      float s = a.scale * a.gsign;
+      if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
+      const int c = 2 * pr;
+      const bool two = true;   // C % 4 == 0: every pair is whole
+      const float2* gb = a.grid + ((long long)be * C + (c & ~3)) * g.gtot + (c & 3);
+      float4 v[W][W];
+  #pragma unroll
+      for (int i0 = 0; i0 < W; ++i0) {
+        const long long roff = (long long)nidx[0][i0] * g.G[1];
+  #pragma unroll
+        for (int i1 = 0; i1 < W; ++i1)
+          v[i0][i1] = __ldg(reinterpret_cast<const float4*>(gb + (roff + nidx[1][i1]) * 4));
+      }
+      float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
+  #pragma unroll
+      for (int i0 = 0; i0 < W; ++i0) {
+        float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
+  #pragma unroll
+        for (int i1 = 0; i1 < W; ++i1) {
+          a0 = fmaf(w[1][i1], v[i0][i1].x, a0);
+          b0 = fmaf(w[1][i1], v[i0][i1].y, b0);
+          a1 = fmaf(w[1][i1], v[i0][i1].z, a1);
+          b1 = fmaf(w[1][i1], v[i0][i1].w, b1);
+        }
+        r0 = fmaf(w[0][i0], a0, r0);
+        m0 = fmaf(w[0][i0], b0, m0);
+        r1 = fmaf(w[0][i0], a1, r1);
+        m1 = fmaf(w[0][i0], b1, m1);
+      }
+      ys[c * S + ks] = make_float2(r0 * s, m0 * s);
+      if (two) ys[(c + 1) * S + ks] = make_float2(r1 * s, m1 * s);
+    }
+    __syncthreads();
+    const int ns = (int)min((long long)S, g.K - k0);
+    float2* yo = a.y + (long long)be * C * g.K + k0;
+    for (int e = threadIdx.x; e < C * S; e += blockDim.x) {
+      const int c = e / S, j = e - c * S;
+      if (j < ns) yo[(long long)c * g.K + j] = ys[c * S + j];
+    }
+  }
+};
 __global__ void __launch_bounds__(256) interp2_il_kernel(InterpArgs a, Geo g, KBPoly kb) {
-  constexpr int W = 4;
-  __shared__ float2 ys[512];   // [coil][sample]: C * S <= 2 * P * S <= 512
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  const int C = g.C;
-  const int P = (C + 1) >> 1;
-  const int S = 256 / P;
-  const long long k0 = (long long)blockIdx.x * S;
-  const int be = blockIdx.y;
-  const int b = frame_of(be, a.nb, g.B);
-  const int ks = threadIdx.x / P, pr = threadIdx.x - ks * P;
-  const long long k = k0 + ks;
-  if (ks < S && k < g.K) {
-    float w[2][W];
-    int nidx[2][W];
-#pragma unroll
-    for (int d = 0; d < 2; ++d) {
-      const float x = a.gx[((long long)b * 2 + d) * g.K + k];
-      const int base = (int)floorf(x);
-      const float fx = x - (float)base;
-#pragma unroll
-      for (int o = 0; o < W; ++o) {
-        const int n = base - (W / 2 - 1) + o;
-        const float wd = mrb::kb_tap(kb, o, fx);
-        w[d][o] = (n & 1) ? -wd : wd;
-        nidx[d][o] = mrb::wrap_i(n, g.G[d]);
-      }
-    }
-    float s = a.scale * a.gsign;
-    if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
-    const int c = 2 * pr;
-    const bool two = true;   // C % 4 == 0: every pair is whole
-    const float2* gb = a.grid + ((long long)be * C + (c & ~3)) * g.gtot + (c & 3);
-    float4 v[W][W];
-#pragma unroll
-    for (int i0 = 0; i0 < W; ++i0) {
-      const long long roff = (long long)nidx[0][i0] * g.G[1];
-#pragma unroll
-      for (int i1 = 0; i1 < W; ++i1)
-        v[i0][i1] = __ldg(reinterpret_cast<const float4*>(gb + (roff + nidx[1][i1]) * 4));
-    }
-    float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
-#pragma unroll
-    for (int i0 = 0; i0 < W; ++i0) {
-      float a0 = 0.f, b0 = 0.f, a1 = 0.f, b1 = 0.f;
-#pragma unroll
-      for (int i1 = 0; i1 < W; ++i1) {
-        a0 = fmaf(w[1][i1], v[i0][i1].x, a0);
-        b0 = fmaf(w[1][i1], v[i0][i1].y, b0);
-        a1 = fmaf(w[1][i1], v[i0][i1].z, a1);
-        b1 = fmaf(w[1][i1], v[i0][i1].w, b1);
-      }
-      r0 = fmaf(w[0][i0], a0, r0);
-      m0 = fmaf(w[0][i0], b0, m0);
-      r1 = fmaf(w[0][i0], a1, r1);
-      m1 = fmaf(w[0][i0], b1, m1);
-    }
-    ys[c * S + ks] = make_float2(r0 * s, m0 * s);
-    if (two) ys[(c + 1) * S + ks] = make_float2(r1 * s, m1 * s);
-  }
-  __syncthreads();
-  const int ns = (int)min((long long)S, g.K - k0);
-  float2* yo = a.y + (long long)be * C * g.K + k0;
-  for (int e = threadIdx.x; e < C * S; e += blockDim.x) {
-    const int c = e / S, j = e - c * S;
-    if (j < ns) yo[(long long)c * g.K + j] = ys[c * S + j];
-  }
+  Interp2Quad::run(hw_block(), a, g, kb);
 }
 
 // ---------------------------------------------------------------------------
@@ -873,227 +898,235 @@ struct SpreadSmem {
 };
 
 template <int ND, int T>
-__global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  using SM = SpreadSmem<ND, T>;
-  constexpr int CELLS = SM::CELLS;
-  constexpr int NW = SM::NWP;   // stride of the staged weights
-  constexpr int NTAP = SM::NTAP;
-  extern __shared__ float4 smem4[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  long long item = (long long)blockIdx.x * SPREAD_WARPS + warp;
-  const long long reps = g.B == 1 ? a.nb : a.nb / g.B;
-  const long long nitems = reps * a.n_items * a.ngroups;
-  if (item >= nitems) return;
-  // work items run heaviest (frame, tile) first; every frame of a B_eff batch
-  // that shares the trajectory frame repeats the same item list
-  const int grp = (int)(item % a.ngroups);
-  const long long oi = item / a.ngroups;
-  const int4 it = a.items[oi % a.n_items];
-  const int rep = (int)(oi / a.n_items);
-  const int okey = it.x;
-  const int b = okey / tg.ntiles;
-  const int tile = okey - b * tg.ntiles;
-  const int be = (g.B == 1) ? rep : b * (a.nb / g.B) + rep;
-  const int c0 = grp * a.cpi;
-  const int nc = min(a.cpi, g.C - c0);
-  int o[3];
-  if (ND == 2) {
-    o[0] = (tile / tg.nt[1]) * T;
-    o[1] = (tile % tg.nt[1]) * T;
-    o[2] = 0;
-  } else {
-    o[2] = (tile % tg.nt[2]) * T;
-    o[1] = ((tile / tg.nt[2]) % tg.nt[1]) * T;
-    o[0] = (tile / (tg.nt[2] * tg.nt[1])) * T;
-  }
-  const int key = okey;
-  const int k0 = a.tile_start[key], k1 = a.tile_start[key + 1];
-  const int e0 = min(k1, k0 + it.y * a.chunk), e1 = min(k1, e0 + a.chunk);
-  float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
-  const int Gl = g.G[ND - 1];
-  // split keys write their partial tile (unpadded T^nd per coil) to a slot
-  constexpr int TN = ND == 2 ? T * T : T * T * T;
-  float2* pout = it.z >= 0 ? a.partials + (((long long)rep * a.n_slots + it.z) * g.C + c0) * TN : nullptr;
-
-  // cells of the tile as float4 pairs along the last dim
-  constexpr int PAIRS = (ND == 2 ? T * T : T * T * T) / 2;
-  auto cell_of_pair = [&](int r, int* n) -> long long {
-    int l = (r % (T / 2)) * 2;
-    int rr = r / (T / 2);
+struct SpreadWarp {
+  static constexpr int NT = SPREAD_WARPS * 32, MINB = 1;
+  static __device__ __forceinline__ void run(const VBlock& vb, const SpreadArgs& a, const Geo& g,
+      const TileGeo& tg, const KBPoly& kb) {
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    using SM = SpreadSmem<ND, T>;
+    constexpr int CELLS = SM::CELLS;
+    constexpr int NW = SM::NWP;   // stride of the staged weights
+    constexpr int NTAP = SM::NTAP;
+    extern __shared__ float4 smem4[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    long long item = (long long)vb.x * SPREAD_WARPS + warp;
+    const long long reps = g.B == 1 ? a.nb : a.nb / g.B;
+    const long long nitems = reps * a.n_items * a.ngroups;
+    if (item >= nitems) return;
+    // work items run heaviest (frame, tile) first; every frame of a B_eff batch
+    // that shares the trajectory frame repeats the same item list
+    const int grp = (int)(item % a.ngroups);
+    const long long oi = item / a.ngroups;
+    const int4 it = a.items[oi % a.n_items];
+    const int rep = (int)(oi / a.n_items);
+    const int okey = it.x;
+    const int b = okey / tg.ntiles;
+    const int tile = okey - b * tg.ntiles;
+    const int be = (g.B == 1) ? rep : b * (a.nb / g.B) + rep;
+    const int c0 = grp * a.cpi;
+    const int nc = min(a.cpi, g.C - c0);
+    int o[3];
     if (ND == 2) {
-      n[0] = o[0] + rr;
-      n[1] = o[1] + l;
-      return (long long)n[0] * Gl + n[1];
+      o[0] = (tile / tg.nt[1]) * T;
+      o[1] = (tile % tg.nt[1]) * T;
+      o[2] = 0;
     } else {
-      n[0] = o[0] + rr / T;
-      n[1] = o[1] + rr % T;
-      n[2] = o[2] + l;
-      return ((long long)n[0] * g.G[1] + n[1]) * Gl + n[2];
+      o[2] = (tile % tg.nt[2]) * T;
+      o[1] = ((tile / tg.nt[2]) % tg.nt[1]) * T;
+      o[0] = (tile / (tg.nt[2] * tg.nt[1])) * T;
     }
-  };
-  auto in_grid = [&](const int* n) {
-    bool ok = n[0] < g.G[0];
-    if (ND >= 2) ok = ok && n[1] < g.G[1];
-    if (ND == 3) ok = ok && n[2] < g.G[2];
-    return ok;
-  };
+    const int key = okey;
+    const int k0 = a.tile_start[key], k1 = a.tile_start[key + 1];
+    const int e0 = min(k1, k0 + it.y * a.chunk), e1 = min(k1, e0 + a.chunk);
+    float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
+    const int Gl = g.G[ND - 1];
+    // split keys write their partial tile (unpadded T^nd per coil) to a slot
+    constexpr int TN = ND == 2 ? T * T : T * T * T;
+    float2* pout = it.z >= 0 ? a.partials + (((long long)rep * a.n_slots + it.z) * g.C + c0) * TN : nullptr;
 
-  if (e0 == e1 && !pout) {   // no sample touches this tile: zeros
-    if (a.touch) return;     // its cells are outside every support and never read
-    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = lane; i < nc * PAIRS; i += 32) {
-      int cl = i / PAIRS, r = i - cl * PAIRS;
-      int n[3];
-      long long cell = cell_of_pair(r, n);
-      if (in_grid(n)) *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = z4;
-    }
-    return;
-  }
-
-  const int cps = SM::cstride(a.cpi);   // coils per shared cell (even)
-  const int npair = cps >> 1;
-  char* wbase = reinterpret_cast<char*>(smem4) + (size_t)warp * SM::warp_bytes(a.cpi);
-  float2* acc = reinterpret_cast<float2*>(wbase);
-  int4* sb = reinterpret_cast<int4*>(wbase + (size_t)cps * CELLS * sizeof(float2));
-  float* sw = reinterpret_cast<float*>(sb + SPREAD_BATCH);
-  float2* sy = reinterpret_cast<float2*>(sw + SPREAD_BATCH * NW);
-
-  {
-    float4* acc4 = reinterpret_cast<float4*>(acc);
-    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = lane; i < cps * CELLS / 2; i += 32) acc4[i] = z4;
-  }
-  __syncwarp();
-
-  const float* gxp = a.gx + (long long)b * ND * g.K;
-  const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
-  const int ntask = NTAP * npair;
-  // the next batch's sample index, coordinates, weight and first coil values
-  // are loaded into registers while the warp works on the current batch
-  constexpr int PF = 4;
-  int pk = 0;
-  float px[ND], pwa = 1.f;
-  float2 py[PF];
-  auto fetch = [&](int e, int nbat) {
-    if (lane < nbat) {
-      pk = a.entries[e + lane];
-#pragma unroll
-      for (int d = 0; d < ND; ++d) px[d] = gxp[(long long)d * g.K + pk];
-      if (a.wadj) pwa = a.wadj[(long long)b * g.K + pk];
-#pragma unroll
-      for (int cl = 0; cl < PF; ++cl) py[cl] = cl < nc ? yb[(long long)cl * g.K + pk] : make_float2(0.f, 0.f);
-    }
-  };
-  if (e0 < e1) fetch(e0, min(SPREAD_BATCH, e1 - e0));
-  for (int e = e0; e < e1; e += SPREAD_BATCH) {
-    const int nbat = min(SPREAD_BATCH, e1 - e);
-    if (lane < nbat) {
-      const int k = pk;
-      float ws = a.gsign;
-      if (a.wadj) ws *= pwa;
-      int base[3] = {0, 0, 0};
-#pragma unroll
-      for (int d = 0; d < ND; ++d) {
-        const float x = px[d];
-        base[d] = (int)floorf(x) - 1;
-        const float fx = x - (float)(base[d] + 1);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int n = base[d] + q;
-          float w = mrb::kb_tap(kb, q, fx);
-          if (n & 1) w = -w;
-          if (d == 0) w *= ws;
-          sw[lane * NW + d * 4 + q] = w;
-        }
+    // cells of the tile as float4 pairs along the last dim
+    constexpr int PAIRS = (ND == 2 ? T * T : T * T * T) / 2;
+    auto cell_of_pair = [&](int r, int* n) -> long long {
+      int l = (r % (T / 2)) * 2;
+      int rr = r / (T / 2);
+      if (ND == 2) {
+        n[0] = o[0] + rr;
+        n[1] = o[1] + l;
+        return (long long)n[0] * Gl + n[1];
+      } else {
+        n[0] = o[0] + rr / T;
+        n[1] = o[1] + rr % T;
+        n[2] = o[2] + l;
+        return ((long long)n[0] * g.G[1] + n[1]) * Gl + n[2];
       }
-      sb[lane] = make_int4(base[0], base[1], base[2], 0);
-#pragma unroll
-      for (int cl = 0; cl < PF; ++cl)
-        if (cl < cps) sy[lane * cps + cl] = py[cl];
-      for (int cl = PF; cl < cps; ++cl)
-        sy[lane * cps + cl] = cl < nc ? yb[(long long)cl * g.K + k] : make_float2(0.f, 0.f);
+    };
+    auto in_grid = [&](const int* n) {
+      bool ok = n[0] < g.G[0];
+      if (ND >= 2) ok = ok && n[1] < g.G[1];
+      if (ND == 3) ok = ok && n[2] < g.G[2];
+      return ok;
+    };
+
+    if (e0 == e1 && !pout) {   // no sample touches this tile: zeros
+      if (a.touch) return;     // its cells are outside every support and never read
+      const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int i = lane; i < nc * PAIRS; i += 32) {
+        int cl = i / PAIRS, r = i - cl * PAIRS;
+        int n[3];
+        long long cell = cell_of_pair(r, n);
+        if (in_grid(n)) *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = z4;
+      }
+      return;
+    }
+
+    const int cps = SM::cstride(a.cpi);   // coils per shared cell (even)
+    const int npair = cps >> 1;
+    char* wbase = reinterpret_cast<char*>(smem4) + (size_t)warp * SM::warp_bytes(a.cpi);
+    float2* acc = reinterpret_cast<float2*>(wbase);
+    int4* sb = reinterpret_cast<int4*>(wbase + (size_t)cps * CELLS * sizeof(float2));
+    float* sw = reinterpret_cast<float*>(sb + SPREAD_BATCH);
+    float2* sy = reinterpret_cast<float2*>(sw + SPREAD_BATCH * NW);
+
+    {
+      float4* acc4 = reinterpret_cast<float4*>(acc);
+      const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int i = lane; i < cps * CELLS / 2; i += 32) acc4[i] = z4;
     }
     __syncwarp();
-    if (e + SPREAD_BATCH < e1) fetch(e + SPREAD_BATCH, min(SPREAD_BATCH, e1 - e - SPREAD_BATCH));
-    for (int j = 0; j < nbat; ++j) {
-      const int4 bb = sb[j];
-      const float* wj = sw + j * NW;
-      const float4* yj = reinterpret_cast<const float4*>(sy + j * cps);
-      // lane tasks: (tap, coil pair), every task of a sample touches a distinct float4;
-      // coil pair fastest, so that the 8 lanes of a 128-bit access phase cover
-      // consecutive (cell, pair) slots (taps first: all 4 taps of a row land on
-      // the same bank group and conflict 2-way)
-      for (int tk = lane; tk < ntask; tk += 32) {
-        const int pr = npair == 2 ? (tk & 1) : tk % npair;
-        const int tap = npair == 2 ? (tk >> 1) : tk / npair;
-        int cell;
-        float w;
-        bool inside;
-        if (ND == 2) {
-          const int ox = tap >> 2, oy = tap & 3;
-          int n0 = bb.x + ox, n1 = bb.y + oy;
-          n0 += n0 < 0 ? g.G[0] : 0;
-          n0 -= n0 >= g.G[0] ? g.G[0] : 0;
-          n1 += n1 < 0 ? g.G[1] : 0;
-          n1 -= n1 >= g.G[1] ? g.G[1] : 0;
-          const int lx = n0 - o[0], ly = n1 - o[1];
-          inside = (unsigned)lx < (unsigned)T && (unsigned)ly < (unsigned)T;
-          cell = lx * T + ly;
-          w = inside ? wj[ox] * wj[4 + oy] : 0.f;
-        } else {
-          const int a0 = tap >> 4, a1 = (tap >> 2) & 3, a2 = tap & 3;
-          int n0 = bb.x + a0, n1 = bb.y + a1, n2 = bb.z + a2;
-          n0 += n0 < 0 ? g.G[0] : 0;
-          n0 -= n0 >= g.G[0] ? g.G[0] : 0;
-          n1 += n1 < 0 ? g.G[1] : 0;
-          n1 -= n1 >= g.G[1] ? g.G[1] : 0;
-          n2 += n2 < 0 ? g.G[2] : 0;
-          n2 -= n2 >= g.G[2] ? g.G[2] : 0;
-          const int l0 = n0 - o[0], l1 = n1 - o[1], l2 = n2 - o[2];
-          inside = (unsigned)l0 < (unsigned)T && (unsigned)l1 < (unsigned)T && (unsigned)l2 < (unsigned)T;
-          cell = (l0 * T + l1) * T + l2;
-          w = inside ? wj[a0] * wj[4 + a1] * wj[8 + a2] : 0.f;
+
+    const float* gxp = a.gx + (long long)b * ND * g.K;
+    const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
+    const int ntask = NTAP * npair;
+    // the next batch's sample index, coordinates, weight and first coil values
+    // are loaded into registers while the warp works on the current batch
+    constexpr int PF = 4;
+    int pk = 0;
+    float px[ND], pwa = 1.f;
+    float2 py[PF];
+    auto fetch = [&](int e, int nbat) {
+      if (lane < nbat) {
+        pk = a.entries[e + lane];
+  #pragma unroll
+        for (int d = 0; d < ND; ++d) px[d] = gxp[(long long)d * g.K + pk];
+        if (a.wadj) pwa = a.wadj[(long long)b * g.K + pk];
+  #pragma unroll
+        for (int cl = 0; cl < PF; ++cl) py[cl] = cl < nc ? yb[(long long)cl * g.K + pk] : make_float2(0.f, 0.f);
+      }
+    };
+    if (e0 < e1) fetch(e0, min(SPREAD_BATCH, e1 - e0));
+    for (int e = e0; e < e1; e += SPREAD_BATCH) {
+      const int nbat = min(SPREAD_BATCH, e1 - e);
+      if (lane < nbat) {
+        const int k = pk;
+        float ws = a.gsign;
+        if (a.wadj) ws *= pwa;
+        int base[3] = {0, 0, 0};
+  #pragma unroll
+        for (int d = 0; d < ND; ++d) {
+          const float x = px[d];
+          base[d] = (int)floorf(x) - 1;
+          const float fx = x - (float)(base[d] + 1);
+  #pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int n = base[d] + q;
+            float w = mrb::kb_tap(kb, q, fx);
+            if (n & 1) w = -w;
+            if (d == 0) w *= ws;
+            sw[lane * NW + d * 4 + q] = w;
+          }
         }
-        if (inside) {
-          const float4 v = yj[pr];
-          float4* p = reinterpret_cast<float4*>(acc + cell * cps) + pr;
-          float4 t = *p;
-          t.x = fmaf(w, v.x, t.x);
-          t.y = fmaf(w, v.y, t.y);
-          t.z = fmaf(w, v.z, t.z);
-          t.w = fmaf(w, v.w, t.w);
-          *p = t;
-        }
+        sb[lane] = make_int4(base[0], base[1], base[2], 0);
+  #pragma unroll
+        for (int cl = 0; cl < PF; ++cl)
+          if (cl < cps) sy[lane * cps + cl] = py[cl];
+        for (int cl = PF; cl < cps; ++cl)
+          sy[lane * cps + cl] = cl < nc ? yb[(long long)cl * g.K + k] : make_float2(0.f, 0.f);
       }
       __syncwarp();
+      if (e + SPREAD_BATCH < e1) fetch(e + SPREAD_BATCH, min(SPREAD_BATCH, e1 - e - SPREAD_BATCH));
+      for (int j = 0; j < nbat; ++j) {
+        const int4 bb = sb[j];
+        const float* wj = sw + j * NW;
+        const float4* yj = reinterpret_cast<const float4*>(sy + j * cps);
+        // lane tasks: (tap, coil pair), every task of a sample touches a distinct float4;
+        // coil pair fastest, so that the 8 lanes of a 128-bit access phase cover
+        // consecutive (cell, pair) slots (taps first: all 4 taps of a row land on
+        // the same bank group and conflict 2-way)
+        for (int tk = lane; tk < ntask; tk += 32) {
+          const int pr = npair == 2 ? (tk & 1) : tk % npair;
+          const int tap = npair == 2 ? (tk >> 1) : tk / npair;
+          int cell;
+          float w;
+          bool inside;
+          if (ND == 2) {
+            const int ox = tap >> 2, oy = tap & 3;
+            int n0 = bb.x + ox, n1 = bb.y + oy;
+            n0 += n0 < 0 ? g.G[0] : 0;
+            n0 -= n0 >= g.G[0] ? g.G[0] : 0;
+            n1 += n1 < 0 ? g.G[1] : 0;
+            n1 -= n1 >= g.G[1] ? g.G[1] : 0;
+            const int lx = n0 - o[0], ly = n1 - o[1];
+            inside = (unsigned)lx < (unsigned)T && (unsigned)ly < (unsigned)T;
+            cell = lx * T + ly;
+            w = inside ? wj[ox] * wj[4 + oy] : 0.f;
+          } else {
+            const int a0 = tap >> 4, a1 = (tap >> 2) & 3, a2 = tap & 3;
+            int n0 = bb.x + a0, n1 = bb.y + a1, n2 = bb.z + a2;
+            n0 += n0 < 0 ? g.G[0] : 0;
+            n0 -= n0 >= g.G[0] ? g.G[0] : 0;
+            n1 += n1 < 0 ? g.G[1] : 0;
+            n1 -= n1 >= g.G[1] ? g.G[1] : 0;
+            n2 += n2 < 0 ? g.G[2] : 0;
+            n2 -= n2 >= g.G[2] ? g.G[2] : 0;
+            const int l0 = n0 - o[0], l1 = n1 - o[1], l2 = n2 - o[2];
+            inside = (unsigned)l0 < (unsigned)T && (unsigned)l1 < (unsigned)T && (unsigned)l2 < (unsigned)T;
+            cell = (l0 * T + l1) * T + l2;
+            w = inside ? wj[a0] * wj[4 + a1] * wj[8 + a2] : 0.f;
+          }
+          if (inside) {
+            const float4 v = yj[pr];
+            float4* p = reinterpret_cast<float4*>(acc + cell * cps) + pr;
+            float4 t = *p;
+            t.x = fmaf(w, v.x, t.x);
+            t.y = fmaf(w, v.y, t.y);
+            t.z = fmaf(w, v.z, t.z);
+            t.w = fmaf(w, v.w, t.w);
+            *p = t;
+          }
+        }
+        __syncwarp();
+      }
     }
-  }
-  // write the whole tile once (or this chunk's partial tile): lane task = (cell
-  // pair along the last dim, coil pair); two 128-bit shared loads, one 128-bit
-  // global store per coil
-  for (int i = lane; i < PAIRS * npair; i += 32) {
-    const int pr = i % npair, r = i / npair;
-    const int l = (r % (T / 2)) * 2;
-    const int rr = r / (T / 2);
-    const int cl0 = rr * T + l;
-    const float4 a0 = reinterpret_cast<const float4*>(acc + cl0 * cps)[pr];
-    const float4 a1 = reinterpret_cast<const float4*>(acc + (cl0 + 1) * cps)[pr];
-    int n[3];
-    const long long cell = cell_of_pair(r, n);
-    const bool ok = in_grid(n) && (pout || pair_touched(a, b, cell));
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int cl = 2 * pr + h;
-      if (cl >= nc) continue;
-      const float4 v = h == 0 ? make_float4(a0.x, a0.y, a1.x, a1.y) : make_float4(a0.z, a0.w, a1.z, a1.w);
-      if (pout) {
-        *reinterpret_cast<float4*>(pout + (long long)cl * TN + rr * T + l) = v;
-      } else if (ok) {
-        *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = v;
+    // write the whole tile once (or this chunk's partial tile): lane task = (cell
+    // pair along the last dim, coil pair); two 128-bit shared loads, one 128-bit
+    // global store per coil
+    for (int i = lane; i < PAIRS * npair; i += 32) {
+      const int pr = i % npair, r = i / npair;
+      const int l = (r % (T / 2)) * 2;
+      const int rr = r / (T / 2);
+      const int cl0 = rr * T + l;
+      const float4 a0 = reinterpret_cast<const float4*>(acc + cl0 * cps)[pr];
+      const float4 a1 = reinterpret_cast<const float4*>(acc + (cl0 + 1) * cps)[pr];
+      int n[3];
+      const long long cell = cell_of_pair(r, n);
+      const bool ok = in_grid(n) && (pout || pair_touched(a, b, cell));
+  #pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int cl = 2 * pr + h;
+        if (cl >= nc) continue;
+        const float4 v = h == 0 ? make_float4(a0.x, a0.y, a1.x, a1.y) : make_float4(a0.z, a0.w, a1.z, a1.w);
+        if (pout) {
+          *reinterpret_cast<float4*>(pout + (long long)cl * TN + rr * T + l) = v;
+        } else if (ok) {
+          *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = v;
+        }
       }
     }
   }
+};
+template <int ND, int T>
+__global__ void __launch_bounds__(SPREAD_WARPS * 32) spread_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
+  SpreadWarp<ND, T>::run(hw_block(), a, g, tg, kb);
 }
 
 // 2D per-warp spread with per-sample tap tables.  Ownership, sample order and
@@ -1122,213 +1155,221 @@ struct Spread2wSmem {
 };
 
 template <int T>
-__global__ void __launch_bounds__(SPREAD_WARPS * 32) spread2w_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  using SM = Spread2wSmem<T>;
-  constexpr int CELLS = SM::CELLS;
-  constexpr int PAIRS = CELLS / 2;
-  extern __shared__ float4 smem4[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long item = (long long)blockIdx.x * SPREAD_WARPS + warp;
-  const long long reps = g.B == 1 ? a.nb : a.nb / g.B;
-  const long long nitems = reps * a.n_items * a.ngroups;
-  if (item >= nitems) return;
-  const int grp = (int)(item % a.ngroups);
-  const long long oi = item / a.ngroups;
-  const int4 it = a.items[oi % a.n_items];
-  const int rep = (int)(oi / a.n_items);
-  const int okey = it.x;
-  const int b = okey / tg.ntiles;
-  const int tile = okey - b * tg.ntiles;
-  const int be = (g.B == 1) ? rep : b * (a.nb / g.B) + rep;
-  const int c0 = grp * a.cpi;
-  const int nc = min(a.cpi, g.C - c0);
-  const int o0 = (tile / tg.nt[1]) * T, o1 = (tile % tg.nt[1]) * T;
-  const int k0 = a.tile_start[okey], k1 = a.tile_start[okey + 1];
-  const int e0 = min(k1, k0 + it.y * a.chunk), e1 = min(k1, e0 + a.chunk);
-  float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
-  const int G0 = g.G[0], G1 = g.G[1];
-  float2* pout = it.z >= 0 ? a.partials + (((long long)rep * a.n_slots + it.z) * g.C + c0) * CELLS : nullptr;
+struct Spread2Taps {
+  static constexpr int NT = SPREAD_WARPS * 32, MINB = 5;
+  static __device__ __forceinline__ void run(const VBlock& vb, const SpreadArgs& a, const Geo& g,
+      const TileGeo& tg, const KBPoly& kb) {
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    using SM = Spread2wSmem<T>;
+    constexpr int CELLS = SM::CELLS;
+    constexpr int PAIRS = CELLS / 2;
+    extern __shared__ float4 smem4[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long item = (long long)vb.x * SPREAD_WARPS + warp;
+    const long long reps = g.B == 1 ? a.nb : a.nb / g.B;
+    const long long nitems = reps * a.n_items * a.ngroups;
+    if (item >= nitems) return;
+    const int grp = (int)(item % a.ngroups);
+    const long long oi = item / a.ngroups;
+    const int4 it = a.items[oi % a.n_items];
+    const int rep = (int)(oi / a.n_items);
+    const int okey = it.x;
+    const int b = okey / tg.ntiles;
+    const int tile = okey - b * tg.ntiles;
+    const int be = (g.B == 1) ? rep : b * (a.nb / g.B) + rep;
+    const int c0 = grp * a.cpi;
+    const int nc = min(a.cpi, g.C - c0);
+    const int o0 = (tile / tg.nt[1]) * T, o1 = (tile % tg.nt[1]) * T;
+    const int k0 = a.tile_start[okey], k1 = a.tile_start[okey + 1];
+    const int e0 = min(k1, k0 + it.y * a.chunk), e1 = min(k1, e0 + a.chunk);
+    float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
+    const int G0 = g.G[0], G1 = g.G[1];
+    float2* pout = it.z >= 0 ? a.partials + (((long long)rep * a.n_slots + it.z) * g.C + c0) * CELLS : nullptr;
 
-  if (e0 == e1 && !pout) {   // no sample touches this tile: zeros
-    if (a.touch) return;     // its cells are outside every support and never read
-    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = lane; i < nc * PAIRS; i += 32) {
-      const int cl = i / PAIRS, r = i - cl * PAIRS;
-      const int n0 = o0 + r / (T / 2), n1 = o1 + (r % (T / 2)) * 2;
-      if (n0 < G0 && n1 < G1) *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + (long long)n0 * G1 + n1) = z4;
-    }
-    return;
-  }
-
-  const int cps = SM::cstride(a.cpi);
-  const int npair = cps >> 1;
-  char* wbase = reinterpret_cast<char*>(smem4) + (size_t)warp * SM::warp_bytes(a.cpi);
-  float2* acc = reinterpret_cast<float2*>(wbase);
-  short* tcell = reinterpret_cast<short*>(wbase + SM::acc_bytes(a.cpi));
-  float* tw = reinterpret_cast<float*>(tcell + SPREAD_BATCH * 16);
-  int* tcnt = reinterpret_cast<int*>(tw + SPREAD_BATCH * 16);
-  unsigned* tbits = reinterpret_cast<unsigned*>(tcnt + SPREAD_BATCH);
-  float2* sy = reinterpret_cast<float2*>(wbase + SM::acc_bytes(a.cpi) + SM::TAB);
-
-  {
-    float4* acc4 = reinterpret_cast<float4*>(acc);
-    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int i = lane; i < cps * CELLS / 2; i += 32) acc4[i] = z4;
-  }
-  // the touched-cell bits of the tile's rows (bit l of row r = cell (o0 + r, o1 + l))
-  if (!pout && a.touch && lane < T) {
-    unsigned m = 0;
-    const int n0 = o0 + lane;
-    if (n0 < G0) {
-      const long long cell = (long long)n0 * G1 + o1;
-      const unsigned* tb = a.touch + (long long)b * a.twords;
-      const long long wi = cell >> 5;
-      const int sh = (int)(cell & 31);
-      unsigned long long v = __ldg(tb + wi);
-      if (sh + T > 32 && wi + 1 < a.twords) v |= (unsigned long long)__ldg(tb + wi + 1) << 32;
-      m = (unsigned)(v >> sh);
-    }
-    tbits[lane] = m;
-  }
-  // this lane's (tap, coil pair) in each round of a sample's tasks
-  int tap_r[SW2_MAXR], pr_r[SW2_MAXR];
-#pragma unroll
-  for (int r = 0; r < SW2_MAXR; ++r) {
-    tap_r[r] = (lane + 32 * r) / npair;
-    pr_r[r] = (lane + 32 * r) - tap_r[r] * npair;
-  }
-  __syncwarp();
-
-  const float* gxp = a.gx + (long long)b * 2 * g.K;
-  const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
-  // the next batch's sample index, coordinates, weight and first coil values
-  // are loaded into registers while the warp works on the current batch
-  constexpr int PF = 4;
-  int pk = 0;
-  float px[2], pwa = 1.f;
-  float2 py[PF];
-  auto fetch = [&](int e, int nbat) {
-    if (lane < nbat) {
-      pk = a.entries[e + lane];
-      px[0] = gxp[pk];
-      px[1] = gxp[g.K + pk];
-      if (a.wadj) pwa = a.wadj[(long long)b * g.K + pk];
-#pragma unroll
-      for (int cl = 0; cl < PF; ++cl) py[cl] = cl < nc ? yb[(long long)cl * g.K + pk] : make_float2(0.f, 0.f);
-    }
-  };
-  if (e0 < e1) fetch(e0, min(SPREAD_BATCH, e1 - e0));
-  for (int e = e0; e < e1; e += SPREAD_BATCH) {
-    const int nbat = min(SPREAD_BATCH, e1 - e);
-    if (lane < nbat) {
-      const int k = pk;
-      float ws = a.gsign;
-      if (a.wadj) ws *= pwa;
-      float wv[2][4];
-      int base[2];
-#pragma unroll
-      for (int d = 0; d < 2; ++d) {
-        const float x = px[d];
-        base[d] = (int)floorf(x) - 1;
-        const float fx = x - (float)(base[d] + 1);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int n = base[d] + q;
-          float w = mrb::kb_tap(kb, q, fx);
-          if (n & 1) w = -w;
-          if (d == 0) w *= ws;
-          wv[d][q] = w;
-        }
+    if (e0 == e1 && !pout) {   // no sample touches this tile: zeros
+      if (a.touch) return;     // its cells are outside every support and never read
+      const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int i = lane; i < nc * PAIRS; i += 32) {
+        const int cl = i / PAIRS, r = i - cl * PAIRS;
+        const int n0 = o0 + r / (T / 2), n1 = o1 + (r % (T / 2)) * 2;
+        if (n0 < G0 && n1 < G1) *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + (long long)n0 * G1 + n1) = z4;
       }
-      short* tc = tcell + lane * 16;
-      float* tww = tw + lane * 16;
-      int m = 0;
-#pragma unroll
-      for (int ox = 0; ox < 4; ++ox) {
-        int n0 = base[0] + ox;
-        n0 += n0 < 0 ? G0 : 0;
-        n0 -= n0 >= G0 ? G0 : 0;
-        const int lx = n0 - o0;
-        if ((unsigned)lx < (unsigned)T) {
-#pragma unroll
-          for (int oy = 0; oy < 4; ++oy) {
-            int n1 = base[1] + oy;
-            n1 += n1 < 0 ? G1 : 0;
-            n1 -= n1 >= G1 ? G1 : 0;
-            const int ly = n1 - o1;
-            if ((unsigned)ly < (unsigned)T) {
-              tc[m] = (short)(lx * T + ly);
-              tww[m] = wv[0][ox] * wv[1][oy];
-              ++m;
+      return;
+    }
+
+    const int cps = SM::cstride(a.cpi);
+    const int npair = cps >> 1;
+    char* wbase = reinterpret_cast<char*>(smem4) + (size_t)warp * SM::warp_bytes(a.cpi);
+    float2* acc = reinterpret_cast<float2*>(wbase);
+    short* tcell = reinterpret_cast<short*>(wbase + SM::acc_bytes(a.cpi));
+    float* tw = reinterpret_cast<float*>(tcell + SPREAD_BATCH * 16);
+    int* tcnt = reinterpret_cast<int*>(tw + SPREAD_BATCH * 16);
+    unsigned* tbits = reinterpret_cast<unsigned*>(tcnt + SPREAD_BATCH);
+    float2* sy = reinterpret_cast<float2*>(wbase + SM::acc_bytes(a.cpi) + SM::TAB);
+
+    {
+      float4* acc4 = reinterpret_cast<float4*>(acc);
+      const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int i = lane; i < cps * CELLS / 2; i += 32) acc4[i] = z4;
+    }
+    // the touched-cell bits of the tile's rows (bit l of row r = cell (o0 + r, o1 + l))
+    if (!pout && a.touch && lane < T) {
+      unsigned m = 0;
+      const int n0 = o0 + lane;
+      if (n0 < G0) {
+        const long long cell = (long long)n0 * G1 + o1;
+        const unsigned* tb = a.touch + (long long)b * a.twords;
+        const long long wi = cell >> 5;
+        const int sh = (int)(cell & 31);
+        unsigned long long v = __ldg(tb + wi);
+        if (sh + T > 32 && wi + 1 < a.twords) v |= (unsigned long long)__ldg(tb + wi + 1) << 32;
+        m = (unsigned)(v >> sh);
+      }
+      tbits[lane] = m;
+    }
+    // this lane's (tap, coil pair) in each round of a sample's tasks
+    int tap_r[SW2_MAXR], pr_r[SW2_MAXR];
+  #pragma unroll
+    for (int r = 0; r < SW2_MAXR; ++r) {
+      tap_r[r] = (lane + 32 * r) / npair;
+      pr_r[r] = (lane + 32 * r) - tap_r[r] * npair;
+    }
+    __syncwarp();
+
+    const float* gxp = a.gx + (long long)b * 2 * g.K;
+    const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
+    // the next batch's sample index, coordinates, weight and first coil values
+    // are loaded into registers while the warp works on the current batch
+    constexpr int PF = 4;
+    int pk = 0;
+    float px[2], pwa = 1.f;
+    float2 py[PF];
+    auto fetch = [&](int e, int nbat) {
+      if (lane < nbat) {
+        pk = a.entries[e + lane];
+        px[0] = gxp[pk];
+        px[1] = gxp[g.K + pk];
+        if (a.wadj) pwa = a.wadj[(long long)b * g.K + pk];
+  #pragma unroll
+        for (int cl = 0; cl < PF; ++cl) py[cl] = cl < nc ? yb[(long long)cl * g.K + pk] : make_float2(0.f, 0.f);
+      }
+    };
+    if (e0 < e1) fetch(e0, min(SPREAD_BATCH, e1 - e0));
+    for (int e = e0; e < e1; e += SPREAD_BATCH) {
+      const int nbat = min(SPREAD_BATCH, e1 - e);
+      if (lane < nbat) {
+        const int k = pk;
+        float ws = a.gsign;
+        if (a.wadj) ws *= pwa;
+        float wv[2][4];
+        int base[2];
+  #pragma unroll
+        for (int d = 0; d < 2; ++d) {
+          const float x = px[d];
+          base[d] = (int)floorf(x) - 1;
+          const float fx = x - (float)(base[d] + 1);
+  #pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int n = base[d] + q;
+            float w = mrb::kb_tap(kb, q, fx);
+            if (n & 1) w = -w;
+            if (d == 0) w *= ws;
+            wv[d][q] = w;
+          }
+        }
+        short* tc = tcell + lane * 16;
+        float* tww = tw + lane * 16;
+        int m = 0;
+  #pragma unroll
+        for (int ox = 0; ox < 4; ++ox) {
+          int n0 = base[0] + ox;
+          n0 += n0 < 0 ? G0 : 0;
+          n0 -= n0 >= G0 ? G0 : 0;
+          const int lx = n0 - o0;
+          if ((unsigned)lx < (unsigned)T) {
+  #pragma unroll
+            for (int oy = 0; oy < 4; ++oy) {
+              int n1 = base[1] + oy;
+              n1 += n1 < 0 ? G1 : 0;
+              n1 -= n1 >= G1 ? G1 : 0;
+              const int ly = n1 - o1;
+              if ((unsigned)ly < (unsigned)T) {
+                tc[m] = (short)(lx * T + ly);
+                tww[m] = wv[0][ox] * wv[1][oy];
+                ++m;
+              }
             }
           }
         }
-      }
-      tcnt[lane] = m;
-#pragma unroll
-      for (int cl = 0; cl < PF; ++cl)
-        if (cl < cps) sy[lane * cps + cl] = py[cl];
-      for (int cl = PF; cl < cps; ++cl)
-        sy[lane * cps + cl] = cl < nc ? yb[(long long)cl * g.K + k] : make_float2(0.f, 0.f);
-    }
-    __syncwarp();
-    if (e + SPREAD_BATCH < e1) fetch(e + SPREAD_BATCH, min(SPREAD_BATCH, e1 - e - SPREAD_BATCH));
-    for (int j = 0; j < nbat; ++j) {
-      const int nt = tcnt[j] * npair;
-      const short* tc = tcell + j * 16;
-      const float* twj = tw + j * 16;
-      const float4* yj = reinterpret_cast<const float4*>(sy + j * cps);
-#pragma unroll
-      for (int r = 0; r < SW2_MAXR; ++r) {
-        if (lane + 32 * r < nt) {
-          const int cell = tc[tap_r[r]];
-          const float w = twj[tap_r[r]];
-          const float4 v = yj[pr_r[r]];
-          float4* p = reinterpret_cast<float4*>(acc + cell * cps) + pr_r[r];
-          float4 t = *p;
-          t.x = fmaf(w, v.x, t.x);
-          t.y = fmaf(w, v.y, t.y);
-          t.z = fmaf(w, v.z, t.z);
-          t.w = fmaf(w, v.w, t.w);
-          *p = t;
-        }
+        tcnt[lane] = m;
+  #pragma unroll
+        for (int cl = 0; cl < PF; ++cl)
+          if (cl < cps) sy[lane * cps + cl] = py[cl];
+        for (int cl = PF; cl < cps; ++cl)
+          sy[lane * cps + cl] = cl < nc ? yb[(long long)cl * g.K + k] : make_float2(0.f, 0.f);
       }
       __syncwarp();
-    }
-  }
-  // write the whole tile once (or this chunk's partial tile): lane task = (cell
-  // pair along the row, coil pair), coil pair fastest; two 128-bit shared loads,
-  // one 128-bit global store per coil
-  const int qd = 32 / npair, qr = 32 - qd * npair;
-  int pr = lane % npair, r = lane / npair;
-  for (int i = lane; i < PAIRS * npair; i += 32) {
-    const int l = (r % (T / 2)) * 2;
-    const int rr = r / (T / 2);
-    const int cl0 = rr * T + l;
-    const float4 a0 = reinterpret_cast<const float4*>(acc + cl0 * cps)[pr];
-    const float4 a1 = reinterpret_cast<const float4*>(acc + (cl0 + 1) * cps)[pr];
-    const int n0 = o0 + rr, n1 = o1 + l;
-    const long long cell = (long long)n0 * G1 + n1;
-    const bool ok = n0 < G0 && n1 < G1 && (pout || !a.touch || ((tbits[rr] >> l) & 3u));
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int cl = 2 * pr + h;
-      if (cl >= nc) continue;
-      const float4 v = h == 0 ? make_float4(a0.x, a0.y, a1.x, a1.y) : make_float4(a0.z, a0.w, a1.z, a1.w);
-      if (pout) {
-        *reinterpret_cast<float4*>(pout + (long long)cl * CELLS + cl0) = v;
-      } else if (ok) {
-        *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = v;
+      if (e + SPREAD_BATCH < e1) fetch(e + SPREAD_BATCH, min(SPREAD_BATCH, e1 - e - SPREAD_BATCH));
+      for (int j = 0; j < nbat; ++j) {
+        const int nt = tcnt[j] * npair;
+        const short* tc = tcell + j * 16;
+        const float* twj = tw + j * 16;
+        const float4* yj = reinterpret_cast<const float4*>(sy + j * cps);
+  #pragma unroll
+        for (int r = 0; r < SW2_MAXR; ++r) {
+          if (lane + 32 * r < nt) {
+            const int cell = tc[tap_r[r]];
+            const float w = twj[tap_r[r]];
+            const float4 v = yj[pr_r[r]];
+            float4* p = reinterpret_cast<float4*>(acc + cell * cps) + pr_r[r];
+            float4 t = *p;
+            t.x = fmaf(w, v.x, t.x);
+            t.y = fmaf(w, v.y, t.y);
+            t.z = fmaf(w, v.z, t.z);
+            t.w = fmaf(w, v.w, t.w);
+            *p = t;
+          }
+        }
+        __syncwarp();
       }
     }
-    pr += qr;
-    r += qd;
-    if (pr >= npair) {
-      pr -= npair;
-      ++r;
+    // write the whole tile once (or this chunk's partial tile): lane task = (cell
+    // pair along the row, coil pair), coil pair fastest; two 128-bit shared loads,
+    // one 128-bit global store per coil
+    const int qd = 32 / npair, qr = 32 - qd * npair;
+    int pr = lane % npair, r = lane / npair;
+    for (int i = lane; i < PAIRS * npair; i += 32) {
+      const int l = (r % (T / 2)) * 2;
+      const int rr = r / (T / 2);
+      const int cl0 = rr * T + l;
+      const float4 a0 = reinterpret_cast<const float4*>(acc + cl0 * cps)[pr];
+      const float4 a1 = reinterpret_cast<const float4*>(acc + (cl0 + 1) * cps)[pr];
+      const int n0 = o0 + rr, n1 = o1 + l;
+      const long long cell = (long long)n0 * G1 + n1;
+      const bool ok = n0 < G0 && n1 < G1 && (pout || !a.touch || ((tbits[rr] >> l) & 3u));
+  #pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int cl = 2 * pr + h;
+        if (cl >= nc) continue;
+        const float4 v = h == 0 ? make_float4(a0.x, a0.y, a1.x, a1.y) : make_float4(a0.z, a0.w, a1.z, a1.w);
+        if (pout) {
+          *reinterpret_cast<float4*>(pout + (long long)cl * CELLS + cl0) = v;
+        } else if (ok) {
+          *reinterpret_cast<float4*>(gout + (long long)cl * g.gtot + cell) = v;
+        }
+      }
+      pr += qr;
+      r += qd;
+      if (pr >= npair) {
+        pr -= npair;
+        ++r;
+      }
     }
   }
+};
+template <int T>
+__global__ void __launch_bounds__(SPREAD_WARPS * 32) spread2w_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
+  Spread2Taps<T>::run(hw_block(), a, g, tg, kb);
 }
 
 // 3D adjoint spread, one block per work item (8^3 tile, chunk of its sample
@@ -1697,237 +1738,261 @@ struct Spread2Smem {
 };
 
 template <int PPL>
-__global__ void __launch_bounds__(S2_WARPS * 32) spread2_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  using SM = Spread2Smem<PPL>;
-  constexpr int T = S2_T;
-  constexpr int CPS = SM::CPS;
-  constexpr int RI = 8 / PPL;   // tap rows per lane pass
-  extern __shared__ float4 smem4[];
-  float4* acc4 = smem4;                                             // [cell][pair]
-  int4* sb = reinterpret_cast<int4*>(reinterpret_cast<char*>(smem4) + SM::ACC);
-  float* sw = reinterpret_cast<float*>(sb + S2_BATCH);
-  float4* sy4 = reinterpret_cast<float4*>(sw + S2_BATCH * 8);      // [sample][pair slot]
+struct Spread2Block {
+  static constexpr int NT = S2_WARPS * 32, MINB = (PPL <= 4 ? 2 : 1);
+  static __device__ __forceinline__ void run(const VBlock& vb, const SpreadArgs& a, const Geo& g,
+      const TileGeo& tg, const KBPoly& kb) {
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    using SM = Spread2Smem<PPL>;
+    constexpr int T = S2_T;
+    constexpr int CPS = SM::CPS;
+    constexpr int RI = 8 / PPL;   // tap rows per lane pass
+    extern __shared__ float4 smem4[];
+    float4* acc4 = smem4;                                             // [cell][pair]
+    int4* sb = reinterpret_cast<int4*>(reinterpret_cast<char*>(smem4) + SM::ACC);
+    float* sw = reinterpret_cast<float*>(sb + S2_BATCH);
+    float4* sy4 = reinterpret_cast<float4*>(sw + S2_BATCH * 8);      // [sample][pair slot]
 
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const long long item = blockIdx.x;
-  const int grp = (int)(item % a.ngroups);
-  const long long oi = item / a.ngroups;
-  const int4 it = a.items[oi % a.n_items];
-  const int rep = (int)(oi / a.n_items);
-  const int b = it.x / tg.ntiles;
-  const int tile = it.x - b * tg.ntiles;
-  const int be = (g.B == 1) ? rep : b * (a.nb / g.B) + rep;
-  const int c0 = grp * a.cpi;
-  const int nc = min(a.cpi, g.C - c0);
-  const int o0 = (tile / tg.nt[1]) * T;
-  const int o1 = (tile % tg.nt[1]) * T;
-  const int k0 = a.tile_start[it.x], k1 = a.tile_start[it.x + 1];
-  const int e0 = min(k1, k0 + it.y * a.chunk), e1 = min(k1, e0 + a.chunk);
-  constexpr int TN = T * T;
-  float2* pout = it.z >= 0 ? a.partials + (((long long)rep * a.n_slots + it.z) * g.C + c0) * TN : nullptr;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long item = vb.x;
+    const int grp = (int)(item % a.ngroups);
+    const long long oi = item / a.ngroups;
+    const int4 it = a.items[oi % a.n_items];
+    const int rep = (int)(oi / a.n_items);
+    const int b = it.x / tg.ntiles;
+    const int tile = it.x - b * tg.ntiles;
+    const int be = (g.B == 1) ? rep : b * (a.nb / g.B) + rep;
+    const int c0 = grp * a.cpi;
+    const int nc = min(a.cpi, g.C - c0);
+    const int o0 = (tile / tg.nt[1]) * T;
+    const int o1 = (tile % tg.nt[1]) * T;
+    const int k0 = a.tile_start[it.x], k1 = a.tile_start[it.x + 1];
+    const int e0 = min(k1, k0 + it.y * a.chunk), e1 = min(k1, e0 + a.chunk);
+    constexpr int TN = T * T;
+    float2* pout = it.z >= 0 ? a.partials + (((long long)rep * a.n_slots + it.z) * g.C + c0) * TN : nullptr;
 
-  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (int i = threadIdx.x; i < SM::CELLS * PPL; i += blockDim.x) acc4[i] = z4;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = threadIdx.x; i < SM::CELLS * PPL; i += blockDim.x) acc4[i] = z4;
 
-  const int R0 = o0 + warp * S2_RPW;   // the warp's first grid row
-  const int p = lane % PPL, q = lane / PPL;
-  const int a1 = q & 3, rsub = q >> 2;
-  const bool pair_ok = p < (nc + 1) / 2;
-  const float* gxp = a.gx + (long long)b * 2 * g.K;
-  const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
+    const int R0 = o0 + warp * S2_RPW;   // the warp's first grid row
+    const int p = lane % PPL, q = lane / PPL;
+    const int a1 = q & 3, rsub = q >> 2;
+    const bool pair_ok = p < (nc + 1) / 2;
+    const float* gxp = a.gx + (long long)b * 2 * g.K;
+    const float2* yb = a.y + ((long long)be * g.C + c0) * g.K;
 
-  for (int e = e0; e < e1; e += S2_BATCH) {
-    const int nbat = min(S2_BATCH, e1 - e);
-    __syncthreads();   // previous batch consumed (and the zero fill done)
-    for (int i = threadIdx.x; i < nbat * 2; i += blockDim.x) {
-      const int j = i >> 1, d = i & 1;
-      const int k = a.entries[e + j];
-      const float x = gxp[(long long)d * g.K + k];
-      const int base = (int)floorf(x) - 1;
-      float ws = 1.f;
-      if (d == 0) {
-        ws = a.gsign;
-        if (a.wadj) ws *= a.wadj[(long long)b * g.K + k];
+    for (int e = e0; e < e1; e += S2_BATCH) {
+      const int nbat = min(S2_BATCH, e1 - e);
+      __syncthreads();   // previous batch consumed (and the zero fill done)
+      for (int i = threadIdx.x; i < nbat * 2; i += blockDim.x) {
+        const int j = i >> 1, d = i & 1;
+        const int k = a.entries[e + j];
+        const float x = gxp[(long long)d * g.K + k];
+        const int base = (int)floorf(x) - 1;
+        float ws = 1.f;
+        if (d == 0) {
+          ws = a.gsign;
+          if (a.wadj) ws *= a.wadj[(long long)b * g.K + k];
+        }
+        const float fx = x - (float)(base + 1);
+  #pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int n = base + t;
+          float w = mrb::kb_tap(kb, t, fx);
+          if (n & 1) w = -w;
+          sw[j * 8 + d * 4 + t] = w * ws;
+        }
+        reinterpret_cast<int*>(sb + j)[d] = base;
       }
-      const float fx = x - (float)(base + 1);
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const int n = base + t;
-        float w = mrb::kb_tap(kb, t, fx);
-        if (n & 1) w = -w;
-        sw[j * 8 + d * 4 + t] = w * ws;
+      for (int i = threadIdx.x; i < S2_BATCH * CPS; i += blockDim.x) {
+        const int j = i % S2_BATCH, c = i / S2_BATCH;   // lanes along the sample list
+        float2 v = make_float2(0.f, 0.f);
+        if (j < nbat && c < nc) v = yb[(long long)c * g.K + a.entries[e + j]];
+        const int slot = (c >> 1) ^ (j & (PPL - 1));
+        reinterpret_cast<float2*>(sy4 + j * PPL + slot)[c & 1] = v;
       }
-      reinterpret_cast<int*>(sb + j)[d] = base;
-    }
-    for (int i = threadIdx.x; i < S2_BATCH * CPS; i += blockDim.x) {
-      const int j = i % S2_BATCH, c = i / S2_BATCH;   // lanes along the sample list
-      float2 v = make_float2(0.f, 0.f);
-      if (j < nbat && c < nc) v = yb[(long long)c * g.K + a.entries[e + j]];
-      const int slot = (c >> 1) ^ (j & (PPL - 1));
-      reinterpret_cast<float2*>(sy4 + j * PPL + slot)[c & 1] = v;
+      __syncthreads();
+      if (R0 >= g.G[0]) continue;   // rows beyond a partial last tile: nothing lands here
+      // lane j tests sample j against this warp's rows; the warp then visits
+      // only the samples whose support meets them
+      int myd0 = 4;
+      bool hit = false;
+      if (lane < nbat) {
+        myd0 = R0 - sb[lane].x;
+        myd0 += myd0 < 0 ? g.G[0] : 0;
+        myd0 -= myd0 >= g.G[0] ? g.G[0] : 0;
+        hit = myd0 < 4 || myd0 + S2_RPW - 1 >= g.G[0];
+      }
+      unsigned todo = __ballot_sync(0xffffffffu, hit);
+      while (todo) {
+        const int j = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const int4 bb = sb[j];
+        const int d0 = __shfl_sync(0xffffffffu, myd0, j);
+        int n1 = bb.y + a1;
+        n1 += n1 < 0 ? g.G[1] : 0;
+        n1 -= n1 >= g.G[1] ? g.G[1] : 0;
+        const int l1 = n1 - o1;
+        const bool in1 = pair_ok && (unsigned)l1 < (unsigned)T;
+        const float* wj = sw + j * 8;
+        const float w1 = wj[4 + a1];
+        const float4 v = sy4[j * PPL + (p ^ (j & (PPL - 1)))];
+  #pragma unroll
+        for (int r0 = 0; r0 < S2_RPW; r0 += RI) {
+          const int r = r0 + rsub;
+          int a0 = d0 + r;
+          a0 -= a0 >= g.G[0] ? g.G[0] : 0;
+          if (in1 && r < S2_RPW && a0 < 4 && R0 + r < g.G[0]) {
+            const float w = wj[a0] * w1;   // the per-warp kernel's product order
+            float4* c4 = acc4 + ((warp * S2_RPW + r) * T + l1) * PPL + p;
+            float4 t = *c4;
+            t.x = fmaf(w, v.x, t.x);
+            t.y = fmaf(w, v.y, t.y);
+            t.z = fmaf(w, v.z, t.z);
+            t.w = fmaf(w, v.w, t.w);
+            *c4 = t;
+          }
+        }
+        __syncwarp();
+      }
     }
     __syncthreads();
-    if (R0 >= g.G[0]) continue;   // rows beyond a partial last tile: nothing lands here
-    // lane j tests sample j against this warp's rows; the warp then visits
-    // only the samples whose support meets them
-    int myd0 = 4;
-    bool hit = false;
-    if (lane < nbat) {
-      myd0 = R0 - sb[lane].x;
-      myd0 += myd0 < 0 ? g.G[0] : 0;
-      myd0 -= myd0 >= g.G[0] ? g.G[0] : 0;
-      hit = myd0 < 4 || myd0 + S2_RPW - 1 >= g.G[0];
-    }
-    unsigned todo = __ballot_sync(0xffffffffu, hit);
-    while (todo) {
-      const int j = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const int4 bb = sb[j];
-      const int d0 = __shfl_sync(0xffffffffu, myd0, j);
-      int n1 = bb.y + a1;
-      n1 += n1 < 0 ? g.G[1] : 0;
-      n1 -= n1 >= g.G[1] ? g.G[1] : 0;
-      const int l1 = n1 - o1;
-      const bool in1 = pair_ok && (unsigned)l1 < (unsigned)T;
-      const float* wj = sw + j * 8;
-      const float w1 = wj[4 + a1];
-      const float4 v = sy4[j * PPL + (p ^ (j & (PPL - 1)))];
-#pragma unroll
-      for (int r0 = 0; r0 < S2_RPW; r0 += RI) {
-        const int r = r0 + rsub;
-        int a0 = d0 + r;
-        a0 -= a0 >= g.G[0] ? g.G[0] : 0;
-        if (in1 && r < S2_RPW && a0 < 4 && R0 + r < g.G[0]) {
-          const float w = wj[a0] * w1;   // the per-warp kernel's product order
-          float4* c4 = acc4 + ((warp * S2_RPW + r) * T + l1) * PPL + p;
-          float4 t = *c4;
-          t.x = fmaf(w, v.x, t.x);
-          t.y = fmaf(w, v.y, t.y);
-          t.z = fmaf(w, v.z, t.z);
-          t.w = fmaf(w, v.w, t.w);
-          *c4 = t;
-        }
+    // write-out: lanes (coil, cell pair along the row) read whole cells from
+    // shared memory; each coil row gets 32-byte pieces
+    const float2* acc = reinterpret_cast<const float2*>(acc4);
+    float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
+    for (int i = threadIdx.x; i < (TN / 2) * CPS; i += blockDim.x) {
+      const int c = i % CPS, r = i / CPS;
+      if (c >= nc) continue;
+      const int cl = 2 * r;
+      const float2 u0 = acc[cl * CPS + c], u1 = acc[(cl + 1) * CPS + c];
+      const float4 v = make_float4(u0.x, u0.y, u1.x, u1.y);
+      if (pout) {
+        *reinterpret_cast<float4*>(pout + (long long)c * TN + cl) = v;
+      } else {
+        const int n0 = o0 + cl / T, n1 = o1 + cl % T;
+        const long long cell = (long long)n0 * g.G[1] + n1;
+        if (n0 < g.G[0] && n1 < g.G[1] && pair_touched(a, b, cell))
+          *reinterpret_cast<float4*>(gout + (long long)c * g.gtot + cell) = v;
       }
-      __syncwarp();
     }
   }
-  __syncthreads();
-  // write-out: lanes (coil, cell pair along the row) read whole cells from
-  // shared memory; each coil row gets 32-byte pieces
-  const float2* acc = reinterpret_cast<const float2*>(acc4);
-  float2* gout = a.grid + ((long long)be * g.C + c0) * g.gtot;
-  for (int i = threadIdx.x; i < (TN / 2) * CPS; i += blockDim.x) {
-    const int c = i % CPS, r = i / CPS;
-    if (c >= nc) continue;
-    const int cl = 2 * r;
-    const float2 u0 = acc[cl * CPS + c], u1 = acc[(cl + 1) * CPS + c];
-    const float4 v = make_float4(u0.x, u0.y, u1.x, u1.y);
-    if (pout) {
-      *reinterpret_cast<float4*>(pout + (long long)c * TN + cl) = v;
-    } else {
-      const int n0 = o0 + cl / T, n1 = o1 + cl % T;
-      const long long cell = (long long)n0 * g.G[1] + n1;
-      if (n0 < g.G[0] && n1 < g.G[1] && pair_touched(a, b, cell))
-        *reinterpret_cast<float4*>(gout + (long long)c * g.gtot + cell) = v;
-    }
-  }
+};
+template <int PPL>
+__global__ void __launch_bounds__(S2_WARPS * 32) spread2_kernel(SpreadArgs a, Geo g, TileGeo tg, KBPoly kb) {
+  Spread2Block<PPL>::run(hw_block(), a, g, tg, kb);
 }
 
 // Zeros for the tiles no sample touches: a store-only grid-stride pass, one
 // float4 (two cells) per thread, consecutive threads along tile rows.
 template <int ND, int T>
-__global__ void __launch_bounds__(256) zero_tiles_kernel(const int* __restrict__ keys, int n_empty,
-                                                         float2* __restrict__ grid, Geo g, TileGeo tg, int nb) {
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  // block = one (rep, empty key); threads over (coil, cell pair)
-  constexpr int PAIRS = (ND == 2 ? T * T : T * T * T) / 2;
-  const int key = keys[blockIdx.x % n_empty];
-  const int rep = blockIdx.x / n_empty;
-  const int b = key / tg.ntiles;
-  const int tile = key - b * tg.ntiles;
-  const int be = (g.B == 1) ? rep : b * (nb / g.B) + rep;
-  int o0, o1, o2 = 0;
-  if (ND == 2) {
-    o0 = (tile / tg.nt[1]) * T;
-    o1 = (tile % tg.nt[1]) * T;
-  } else {
-    o2 = (tile % tg.nt[2]) * T;
-    o1 = ((tile / tg.nt[2]) % tg.nt[1]) * T;
-    o0 = (tile / (tg.nt[2] * tg.nt[1])) * T;
-  }
-  float2* base = grid + (long long)be * g.C * g.gtot;
-  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (int i = threadIdx.x; i < g.C * PAIRS; i += blockDim.x) {
-    const int c = i / PAIRS, r = i - c * PAIRS;
-    const int l = (r % (T / 2)) * 2;
-    const int rr = r / (T / 2);
-    int n0, n1, n2;
-    long long idx;
+struct ZeroTiles {
+  static constexpr int NT = 256, MINB = 6;
+  static __device__ __forceinline__ void run(const VBlock& vb, const int* __restrict__ keys, int n_empty,
+      float2* __restrict__ grid, const Geo& g, const TileGeo& tg, int nb) {
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    // block = one (rep, empty key); threads over (coil, cell pair)
+    constexpr int PAIRS = (ND == 2 ? T * T : T * T * T) / 2;
+    const int key = keys[vb.x % n_empty];
+    const int rep = vb.x / n_empty;
+    const int b = key / tg.ntiles;
+    const int tile = key - b * tg.ntiles;
+    const int be = (g.B == 1) ? rep : b * (nb / g.B) + rep;
+    int o0, o1, o2 = 0;
     if (ND == 2) {
-      n0 = o0 + rr;
-      n1 = o1 + l;
-      if (n0 >= g.G[0] || n1 >= g.G[1]) continue;
-      idx = (long long)n0 * g.G[1] + n1;
+      o0 = (tile / tg.nt[1]) * T;
+      o1 = (tile % tg.nt[1]) * T;
     } else {
-      n0 = o0 + rr / T;
-      n1 = o1 + rr % T;
-      n2 = o2 + l;
-      if (n0 >= g.G[0] || n1 >= g.G[1] || n2 >= g.G[2]) continue;
-      idx = ((long long)n0 * g.G[1] + n1) * g.G[2] + n2;
+      o2 = (tile % tg.nt[2]) * T;
+      o1 = ((tile / tg.nt[2]) % tg.nt[1]) * T;
+      o0 = (tile / (tg.nt[2] * tg.nt[1])) * T;
     }
-    *reinterpret_cast<float4*>(base + (long long)c * g.gtot + idx) = z4;
+    float2* base = grid + (long long)be * g.C * g.gtot;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = threadIdx.x; i < g.C * PAIRS; i += blockDim.x) {
+      const int c = i / PAIRS, r = i - c * PAIRS;
+      const int l = (r % (T / 2)) * 2;
+      const int rr = r / (T / 2);
+      int n0, n1, n2;
+      long long idx;
+      if (ND == 2) {
+        n0 = o0 + rr;
+        n1 = o1 + l;
+        if (n0 >= g.G[0] || n1 >= g.G[1]) continue;
+        idx = (long long)n0 * g.G[1] + n1;
+      } else {
+        n0 = o0 + rr / T;
+        n1 = o1 + rr % T;
+        n2 = o2 + l;
+        if (n0 >= g.G[0] || n1 >= g.G[1] || n2 >= g.G[2]) continue;
+        idx = ((long long)n0 * g.G[1] + n1) * g.G[2] + n2;
+      }
+      *reinterpret_cast<float4*>(base + (long long)c * g.gtot + idx) = z4;
+    }
   }
+};
+template <int ND, int T>
+__global__ void __launch_bounds__(256) zero_tiles_kernel(const int* __restrict__ keys, int n_empty,
+    float2* __restrict__ grid, Geo g, TileGeo tg, int nb) {
+  ZeroTiles<ND, T>::run(hw_block(), keys, n_empty, grid, g, tg, nb);
 }
 
 // Sum of the chunk partial tiles of split keys, in chunk order, written once
 // into the grid.  Block = (rep, split key, coil); threads over the tile cells.
 template <int ND, int T>
-__global__ void __launch_bounds__(256) spread_reduce_kernel(const float2* __restrict__ partials,
-                                                            const int4* __restrict__ multi, int n_multi,
-                                                            int n_slots, float2* __restrict__ grid, Geo g,
-                                                            TileGeo tg, int nb) {
-  if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-  constexpr int TN = ND == 2 ? T * T : T * T * T;
-  const int c = blockIdx.y;
-  const int rep = blockIdx.z;
-  const int4 m = multi[blockIdx.x];
-  const int b = m.x / tg.ntiles;
-  const int tile = m.x - b * tg.ntiles;
-  const int be = (g.B == 1) ? rep : b * (nb / g.B) + rep;
-  int o[3];
-  if (ND == 2) {
-    o[0] = (tile / tg.nt[1]) * T;
-    o[1] = (tile % tg.nt[1]) * T;
-    o[2] = 0;
-  } else {
-    o[2] = (tile % tg.nt[2]) * T;
-    o[1] = ((tile / tg.nt[2]) % tg.nt[1]) * T;
-    o[0] = (tile / (tg.nt[2] * tg.nt[1])) * T;
-  }
-  for (int cell = threadIdx.x; cell < TN; cell += blockDim.x) {
-    float sx = 0.f, sy = 0.f;
-    for (int j = 0; j < m.y; ++j) {
-      float2 v = partials[(((long long)rep * n_slots + m.z + j) * g.C + c) * TN + cell];
-      sx += v.x;
-      sy += v.y;
-    }
-    int n0, n1, n2 = 0;
-    long long idx;
+struct SpreadReduce {
+  static constexpr int NT = 256, MINB = 6;
+  static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ partials,
+      const int4* __restrict__ multi, int n_multi, int n_slots, float2* __restrict__ grid, const Geo& g,
+      const TileGeo& tg, int nb) {
+    if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
+    constexpr int TN = ND == 2 ? T * T : T * T * T;
+    const int c = vb.y;
+    const int rep = vb.z;
+    const int4 m = multi[vb.x];
+    const int b = m.x / tg.ntiles;
+    const int tile = m.x - b * tg.ntiles;
+    const int be = (g.B == 1) ? rep : b * (nb / g.B) + rep;
+    int o[3];
     if (ND == 2) {
-      n0 = o[0] + cell / T;
-      n1 = o[1] + cell % T;
-      if (n0 >= g.G[0] || n1 >= g.G[1]) continue;
-      idx = (long long)n0 * g.G[1] + n1;
+      o[0] = (tile / tg.nt[1]) * T;
+      o[1] = (tile % tg.nt[1]) * T;
+      o[2] = 0;
     } else {
-      n0 = o[0] + cell / (T * T);
-      n1 = o[1] + (cell / T) % T;
-      n2 = o[2] + cell % T;
-      if (n0 >= g.G[0] || n1 >= g.G[1] || n2 >= g.G[2]) continue;
-      idx = ((long long)n0 * g.G[1] + n1) * g.G[2] + n2;
+      o[2] = (tile % tg.nt[2]) * T;
+      o[1] = ((tile / tg.nt[2]) % tg.nt[1]) * T;
+      o[0] = (tile / (tg.nt[2] * tg.nt[1])) * T;
     }
-    grid[((long long)be * g.C + c) * g.gtot + idx] = make_float2(sx, sy);
+    for (int cell = threadIdx.x; cell < TN; cell += blockDim.x) {
+      float sx = 0.f, sy = 0.f;
+      for (int j = 0; j < m.y; ++j) {
+        float2 v = partials[(((long long)rep * n_slots + m.z + j) * g.C + c) * TN + cell];
+        sx += v.x;
+        sy += v.y;
+      }
+      int n0, n1, n2 = 0;
+      long long idx;
+      if (ND == 2) {
+        n0 = o[0] + cell / T;
+        n1 = o[1] + cell % T;
+        if (n0 >= g.G[0] || n1 >= g.G[1]) continue;
+        idx = (long long)n0 * g.G[1] + n1;
+      } else {
+        n0 = o[0] + cell / (T * T);
+        n1 = o[1] + (cell / T) % T;
+        n2 = o[2] + cell % T;
+        if (n0 >= g.G[0] || n1 >= g.G[1] || n2 >= g.G[2]) continue;
+        idx = ((long long)n0 * g.G[1] + n1) * g.G[2] + n2;
+      }
+      grid[((long long)be * g.C + c) * g.gtot + idx] = make_float2(sx, sy);
+    }
   }
+};
+template <int ND, int T>
+__global__ void __launch_bounds__(256) spread_reduce_kernel(const float2* __restrict__ partials,
+    const int4* __restrict__ multi, int n_multi, int n_slots, float2* __restrict__ grid, Geo g, TileGeo tg,
+    int nb) {
+  SpreadReduce<ND, T>::run(hw_block(), partials, multi, n_multi, n_slots, grid, g, tg, nb);
 }
 
 // literal / corrected index tables for one frame
@@ -2527,6 +2592,31 @@ static int ensure_smem(const void* fn, size_t smem) {
   return 0;
 }
 
+// spread launch of a selected variant; every variant takes (SpreadArgs, Geo, TileGeo, KBPoly)
+using SpreadKern = void (*)(SpreadArgs, Geo, TileGeo, KBPoly);
+using SpreadGo = int (*)(SpreadKern, int, int, size_t, cudaStream_t, const SpreadArgs&, const Geo&, const TileGeo&,
+                         const KBPoly&);
+
+// variants written as bodies (group.cuh): recordable, K::NT threads
+template <class K>
+static int spread_go(SpreadKern fn, int blocks, int, size_t smem, cudaStream_t st, const SpreadArgs& a, const Geo& g,
+                     const TileGeo& tg, const KBPoly& kb) {
+  return mrb::launch<K>(fn, dim3(blocks), smem, st, a, g, tg, kb);
+}
+
+// the 3D block variants: plain launches
+static int spread_go_plain(SpreadKern fn, int blocks, int threads, size_t smem, cudaStream_t st, const SpreadArgs& a,
+                           const Geo& g, const TileGeo& tg, const KBPoly& kb) {
+  SpreadArgs a2 = a;
+  Geo g2 = g;
+  TileGeo tg2 = tg;
+  KBPoly kb2 = kb;
+  void* args[] = {&a2, &g2, &tg2, &kb2};
+  MRB_CUDA_TRY(cudaLaunchKernel((const void*)fn, dim3(blocks), dim3(threads), args, smem, st));
+  MRB_LAUNCH_CHECK();
+  return 0;
+}
+
 // one stage of the forward/adjoint pipeline; x/y are the user image / samples
 static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cudaStream_t st, int coil_images) {
   Geo g = make_geo(p);
@@ -2622,6 +2712,8 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     return 0;
   }
   if (stage == 1 || stage == 4) {
+    // a library transform cannot be recorded: it would run ahead of the recorded launches
+    MRB_REQUIRE(!mrb::group_recording(), "the cuFFT mode cannot run inside a grouped recording");
     cufftResult r = cufftSetStream(p->fft, st);
     if (r == CUFFT_SUCCESS)
       r = cufftExecC2C(p->fft, p->grid.as<cufftComplex>(), p->grid.as<cufftComplex>(),
@@ -2664,22 +2756,16 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       const int S = 256 / ((p->C + 1) / 2);
       const long long nbx = (p->K + S - 1) / S;
       MRB_REQUIRE(nbx < (1LL << 31) && nb <= 65535, "too many samples for the interp");
-      interp2_il_kernel<<<dim3((unsigned)nbx, nb), 256, 0, st>>>(a, g, p->kb);
-      MRB_LAUNCH_CHECK();
-      return 0;
+      return mrb::launch<Interp2Quad>(interp2_il_kernel, dim3((unsigned)nbx, nb), 0, st, a, g, p->kb);
     }
     if (p->nd == 2 && p->interp_mode == 1) {
       const long long nbx = (long long)grid_blocks(p->K, 256) * ((p->C + 1) / 2);
       MRB_REQUIRE(nbx < (1LL << 31) && nb <= 65535, "too many samples for the interp");
-      interp2p_kernel<<<dim3((unsigned)nbx, nb), 256, 0, st>>>(a, g, p->kb);
-      MRB_LAUNCH_CHECK();
-      return 0;
+      return mrb::launch<Interp2p>(interp2p_kernel, dim3((unsigned)nbx, nb), 0, st, a, g, p->kb);
     }
     dim3 grid(grid_blocks(p->K, 256), nb);
-    if (p->nd == 2) interp_kernel<2><<<grid, 256, 0, st>>>(a, g, p->kb);
-    else interp_kernel<3><<<grid, 256, 0, st>>>(a, g, p->kb);
-    MRB_LAUNCH_CHECK();
-    return 0;
+    if (p->nd == 2) return mrb::launch<InterpGen<2>>(interp_kernel<2>, grid, 0, st, a, g, p->kb);
+    return mrb::launch<InterpGen<3>>(interp_kernel<3>, grid, 0, st, a, g, p->kb);
   }
   if (stage == 3) {
     TileGeo tg{};
@@ -2723,16 +2809,17 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     long long items = (long long)reps * p->n_items * a.ngroups;
     MRB_REQUIRE(items < (1LL << 31), "too many spread work items");
     int blocks = blk3 || blk2 ? (int)items : grid_blocks(items, SPREAD_WARPS);
-    const void* fn = nullptr;
+    SpreadKern fn = nullptr;
+    SpreadGo go = spread_go_plain;   // kernels without a grouped form
     size_t smem = 0;
     int threads = SPREAD_WARPS * 32;
     if (blk3t) {
       if (a.cpi > 8) {
-        fn = (const void*)spread3t_kernel<2>;
+        fn = spread3t_kernel<2>;
         smem = Spread3tSmem<2>::BYTES;
         threads = 2 * S3_WARPS * 32;
       } else {
-        fn = (const void*)spread3t_kernel<1>;
+        fn = spread3t_kernel<1>;
         smem = Spread3tSmem<1>::BYTES;
         threads = S3_WARPS * 32;
       }
@@ -2740,13 +2827,13 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       const int pairs = (a.cpi + 1) / 2;
       threads = S3_WARPS * 32;
       if (pairs <= 2) {
-        fn = (const void*)spread3_kernel<2>;
+        fn = spread3_kernel<2>;
         smem = Spread3Smem<2>::BYTES;
       } else if (pairs <= 4) {
-        fn = (const void*)spread3_kernel<4>;
+        fn = spread3_kernel<4>;
         smem = Spread3Smem<4>::BYTES;
       } else {
-        fn = (const void*)spread3_kernel<8>;
+        fn = spread3_kernel<8>;
         smem = Spread3Smem<8>::BYTES;
       }
     }
@@ -2754,13 +2841,16 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       const int pairs = (a.cpi + 1) / 2;
       threads = S2_WARPS * 32;
       if (pairs <= 2) {
-        fn = (const void*)spread2_kernel<2>;
+        fn = spread2_kernel<2>;
+        go = spread_go<Spread2Block<2>>;
         smem = Spread2Smem<2>::BYTES;
       } else if (pairs <= 4) {
-        fn = (const void*)spread2_kernel<4>;
+        fn = spread2_kernel<4>;
+        go = spread_go<Spread2Block<4>>;
         smem = Spread2Smem<4>::BYTES;
       } else {
-        fn = (const void*)spread2_kernel<8>;
+        fn = spread2_kernel<8>;
+        go = spread_go<Spread2Block<8>>;
         smem = Spread2Smem<8>::BYTES;
       }
     }
@@ -2768,7 +2858,8 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     // groups of up to 16); key 6 = 0 the kernel that evaluates every tap per lane task
 #define MRB_SPREAD2W_CASE(T_)                                                                 \
   if (!fn && p->nd == 2 && tg.T == T_ && p->spread_kernel == 2 && a.cpi <= 16) {             \
-    fn = (const void*)spread2w_kernel<T_>;                                                   \
+    fn = spread2w_kernel<T_>;                                                                \
+    go = spread_go<Spread2Taps<T_>>;                                                         \
     smem = SPREAD_WARPS * Spread2wSmem<T_>::warp_bytes(a.cpi);                               \
   }
     MRB_SPREAD2W_CASE(4)
@@ -2778,7 +2869,8 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
 #undef MRB_SPREAD2W_CASE
 #define MRB_SPREAD_CASE(ND_, T_)                                                             \
   if (!fn && p->nd == ND_ && tg.T == T_) {                                                   \
-    fn = (const void*)spread_kernel<ND_, T_>;                                                \
+    fn = spread_kernel<ND_, T_>;                                                             \
+    go = spread_go<SpreadWarp<ND_, T_>>;                                                     \
     smem = SPREAD_WARPS * SpreadSmem<ND_, T_>::warp_bytes(a.cpi);                            \
   }
     MRB_SPREAD_CASE(2, 4)
@@ -2790,15 +2882,18 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
 #undef MRB_SPREAD_CASE
     MRB_REQUIRE(fn != nullptr, "no spread kernel for nd=%d tile=%d", p->nd, tg.T);
     MRB_REQUIRE(smem <= 227 * 1024, "spread tile needs %zu bytes of shared memory", smem);
-    if (int rc3 = ensure_smem(fn, smem)) return rc3;
+    if (int rc3 = ensure_smem((const void*)fn, smem)) return rc3;
     if (p->n_empty > 0 && !masked) {
       long long zbl = (long long)reps * p->n_empty;
       MRB_REQUIRE(zbl < (1LL << 31), "too many empty tiles");
       int zb = (int)zbl;
       const int* ek = p->empty_keys.as<int>();
       float2* gridp = a.grid;
-#define MRB_ZERO_CASE(ND_, T_)                                                                            \
-  if (p->nd == ND_ && tg.T == T_) zero_tiles_kernel<ND_, T_><<<zb, 256, 0, st>>>(ek, p->n_empty, gridp, g, tg, nb);
+      int rz = 0;
+#define MRB_ZERO_CASE(ND_, T_)                                                                      \
+  if (p->nd == ND_ && tg.T == T_)                                                                   \
+    rz = mrb::launch<ZeroTiles<ND_, T_>>(zero_tiles_kernel<ND_, T_>, dim3(zb), 0, st, ek, p->n_empty, gridp, g, \
+                                         tg, nb);
       MRB_ZERO_CASE(2, 4)
       MRB_ZERO_CASE(2, 8)
       MRB_ZERO_CASE(2, 16)
@@ -2806,12 +2901,10 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       MRB_ZERO_CASE(3, 4)
       MRB_ZERO_CASE(3, 8)
 #undef MRB_ZERO_CASE
-      MRB_LAUNCH_CHECK();
+      if (rz) return rz;
     }
     if (items > 0) {
-      void* args[] = {&a, &g, &tg, &p->kb};
-      MRB_CUDA_TRY(cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, smem, st));
-      MRB_LAUNCH_CHECK();
+      if (int rs = go(fn, blocks, threads, smem, st, a, g, tg, p->kb)) return rs;
     }
     if (p->n_multi > 0) {
       MRB_REQUIRE(reps <= 65535 && p->C <= 65535, "too many frames for the split-tile reduction");
@@ -2819,16 +2912,18 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       const float2* part = p->partials.as<float2>();
       const int4* mt = p->multi.as<int4>();
       float2* gridp = a.grid;
-      if (p->nd == 2) {
-        if (tg.T == 4) spread_reduce_kernel<2, 4><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
-        if (tg.T == 8) spread_reduce_kernel<2, 8><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
-        if (tg.T == 16) spread_reduce_kernel<2, 16><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
-        if (tg.T == 32) spread_reduce_kernel<2, 32><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
-      } else {
-        if (tg.T == 4) spread_reduce_kernel<3, 4><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
-        if (tg.T == 8) spread_reduce_kernel<3, 8><<<rg, 256, 0, st>>>(part, mt, p->n_multi, p->n_slots, gridp, g, tg, nb);
-      }
-      MRB_LAUNCH_CHECK();
+#define MRB_REDUCE_CASE(ND_, T_)                                                                      \
+  if (p->nd == ND_ && tg.T == T_)                                                                     \
+    return mrb::launch<SpreadReduce<ND_, T_>>(spread_reduce_kernel<ND_, T_>, rg, 0, st, part, mt, p->n_multi, \
+                                              p->n_slots, gridp, g, tg, nb);
+      MRB_REDUCE_CASE(2, 4)
+      MRB_REDUCE_CASE(2, 8)
+      MRB_REDUCE_CASE(2, 16)
+      MRB_REDUCE_CASE(2, 32)
+      MRB_REDUCE_CASE(3, 4)
+      MRB_REDUCE_CASE(3, 8)
+#undef MRB_REDUCE_CASE
+      return mrb::fail(MRB_EINVAL, "no split-tile reduction for nd=%d tile=%d", p->nd, tg.T);
     }
     return 0;
   }
