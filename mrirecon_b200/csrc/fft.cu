@@ -311,6 +311,7 @@ constexpr int ROW_WARPS = ROW_NT / 32;
 template <int G1>
 struct FwdRows {
   static constexpr int NT = ROW_NT, MINB = (G1 <= 256 ? 5 : G1 <= 384 ? 4 : G1 <= 640 ? 3 : G1 <= 768 ? 2 : 1);
+  static constexpr const char* FAMILY = "fwd_rows";
   static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ x,
       const float2* __restrict__ maps, const float* __restrict__ rowfac, const float* __restrict__ coldeap,
       float2* __restrict__ Tb, const float2* __restrict__ tw, const Geo2& g, long long nrows, int coil_images) {
@@ -354,6 +355,7 @@ __global__ void __launch_bounds__(ROW_NT) fwd_rows_kernel(const float2* __restri
 template <int G0>
 struct FwdCols {
   static constexpr int NT = COL_NT, MINB = (G0 <= 256 ? 3 : 2);
+  static constexpr const char* FAMILY = "fwd_cols";
   static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ Tb,
       float2* __restrict__ grid, const float2* __restrict__ tw, const Geo2& g) {
     constexpr int COLS = cols_per_block(G0);
@@ -559,6 +561,7 @@ __global__ void __launch_bounds__(COL_NT, 2) fwd_cols_interp_kernel(const float2
 template <int G0>
 struct AdjCols {
   static constexpr int NT = COL_NT, MINB = (G0 <= 256 ? 3 : 2);
+  static constexpr const char* FAMILY = "adj_cols";
   static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ grid,
       float2* __restrict__ Tb, const float2* __restrict__ tw, const Geo2& g) {
     constexpr int COLS = cols_per_block(G0);
@@ -639,6 +642,7 @@ __global__ void __launch_bounds__(COL_NT) toeplitz_cols_kernel(float2* __restric
 template <int G1>
 struct AdjRows {
   static constexpr int NT = ROW_NT, MINB = ((G1 & (G1 - 1)) == 0 && G1 >= 128 ? 4 : G1 <= 64 || G1 == 768 ? 3 : 2);
+  static constexpr const char* FAMILY = "adj_rows";
   static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ Tb,
       const float2* __restrict__ maps, const float* __restrict__ rowfac, const float* __restrict__ coldeap,
       float2* __restrict__ x, const float2* __restrict__ tw, const Geo2& g, float scale) {

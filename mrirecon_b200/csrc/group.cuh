@@ -28,10 +28,13 @@
 // add differently in two kernels that contain the same source; the bodies
 // without SHARED_CODE state every rounding explicitly instead).
 // Between mrb_group_begin and mrb_group_end the call is recorded for the
-// problem selected with mrb_group_select; mrb_group_end replays the records,
-// merging the next record of every problem that runs the same body into one
-// grouped launch (group.cu).  A kernel launched any other way while a
-// recording is open makes its entry point fail (MRB_LAUNCH_CHECK).
+// problem selected with mrb_group_select; mrb_group_end replays the records
+// step by step (group.cu): FAMILY names the kernel step a body performs (the
+// bodies of one step differ only in compile-time shape, e.g. the FFT length),
+// the k-th records of a step in every problem form one step of the replay,
+// and the records of one step that run the same body form one grouped launch.
+// A kernel launched any other way while a recording is open makes its entry
+// point fail (MRB_LAUNCH_CHECK).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -81,6 +84,10 @@ template <class T> struct Ident { using type = T; };
 // optional body constants
 template <class K, class = void> struct BodyMaxG { static constexpr int value = 64; };
 template <class K> struct BodyMaxG<K, std::void_t<decltype(K::MAXG)>> { static constexpr int value = K::MAXG; };
+template <class K, class = void> struct BodyFamily { static constexpr const char* value = nullptr; };
+template <class K> struct BodyFamily<K, std::void_t<decltype(K::FAMILY)>> {
+  static constexpr const char* value = K::FAMILY;
+};
 template <class K, class = void> struct BodyShared { static constexpr bool value = false; };
 template <class K> struct BodyShared<K, std::void_t<decltype(K::SHARED_CODE)>> {
   static constexpr bool value = K::SHARED_CODE;
@@ -126,6 +133,8 @@ __global__ void __launch_bounds__(K::NT, K::MINB) grouped_kernel(const __grid_co
 // one recorded launch
 struct LaunchRec {
   const void* key;                  // identifies the body and its argument types
+  const char* family;               // the kernel step the body belongs to (its shapes share it), or null
+  int occ;                          // earlier records of the same step in this problem's list
   const void* kern;                 // the named kernel
   dim3 grid;
   unsigned threads;
@@ -218,6 +227,8 @@ int launch(void (*kern)(A...), dim3 grid, size_t smem, cudaStream_t st, typename
   }
   LaunchRec r;
   r.key = &L::key_tag;
+  r.family = BodyFamily<K>::value;
+  r.occ = 0;
   r.kern = (const void*)kern;
   r.grid = grid;
   r.threads = K::NT;

@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(RED_THREADS) dots_kernel(DotArgs a, double* __
 // mode 2: r += t*Ad (accepted step; t from the device), no reduction
 struct KSpace {
   static constexpr int NT = RED_THREADS, MINB = 5;
+  static constexpr const char* FAMILY = "kspace";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, int mode, long long n, float2* __restrict__ r,
@@ -342,6 +343,7 @@ struct GradArgs {
 template <int NS, int NU>
 struct TVGrad {
   static constexpr int NT = RED_THREADS, MINB = (NS <= 3 ? 4 : 1);
+  static constexpr const char* FAMILY = "tv_grad";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, const GradArgs& a, const TVPlan& P,
@@ -480,6 +482,7 @@ constexpr int MT_MAX_J = 24;
 template <int NS, int NU, int JMAX>
 struct TVMulti {
   static constexpr int NT = RED_THREADS, MINB = (JMAX <= 8 ? 4 : 1);
+  static constexpr const char* FAMILY = "tv_multi";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ x,
@@ -598,6 +601,7 @@ __device__ __forceinline__ NCGCfg load_cfg(const double* c) {
 // Armijo selection on the multi-t energies: t_0 = 0, t_j = beta^(j-1).
 struct ArmijoSelect {
   static constexpr int NT = 32, MINB = 1;
+  static constexpr const char* FAMILY = "armijo_select";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s, const double* cfg_dev) {
@@ -649,6 +653,7 @@ __global__ void armijo_select_kernel(double* s, const double* cfg_dev) {
 // S_NOMORE = 1 whenever the second pass and phase 2 have nothing to do.
 struct ArmijoPhase {
   static constexpr int NT = 32, MINB = 1;
+  static constexpr const char* FAMILY = "armijo_phase";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s, const double* cfg_dev, int J1,
@@ -715,6 +720,7 @@ __global__ void armijo_phase_kernel(double* s, const double* cfg_dev, int J1, in
 // the direction coefficient beta.
 struct NCGControl {
   static constexpr int NT = 32, MINB = 1;
+  static constexpr const char* FAMILY = "ncg_control";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s, double* hist, const double* cfg_dev,
@@ -804,6 +810,7 @@ __global__ void ncg_control_kernel(double* s, double* hist, const double* cfg_de
 //   g_prev = g (if g_prev), and Re<g, d_new> for the next slope at t = 0.
 struct NCGUpdate {
   static constexpr int NT = RED_THREADS, MINB = 4;
+  static constexpr const char* FAMILY = "ncg_update";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, long long n, float2* __restrict__ x,
@@ -855,6 +862,7 @@ __global__ void __launch_bounds__(RED_THREADS) ncg_update_kernel(long long n, fl
 // d = -g/D (priming: cg.py:182-185) and Re<g,d>
 struct Steepest {
   static constexpr int NT = RED_THREADS, MINB = 5;
+  static constexpr const char* FAMILY = "steepest";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, long long n, float2* __restrict__ d,
@@ -890,6 +898,7 @@ __device__ __forceinline__ bool needs_restart(const double* s) {
 
 struct RestartDir {
   static constexpr int NT = RED_THREADS, MINB = 5;
+  static constexpr const char* FAMILY = "restart_dir";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, long long n, float2* __restrict__ d,
@@ -911,6 +920,7 @@ __global__ void __launch_bounds__(RED_THREADS) restart_dir_kernel(long long n, f
 
 struct RestartSlot {
   static constexpr int NT = 32, MINB = 1;
+  static constexpr const char* FAMILY = "restart_slot";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s) {
@@ -928,6 +938,7 @@ __global__ void restart_slot_kernel(double* s) {
 // ||r + t Ad||^2 = err + 2 t Re<r, Ad> + t^2 ||Ad||^2.
 struct ErrStep {
   static constexpr int NT = 32, MINB = 1;
+  static constexpr const char* FAMILY = "err_step";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s) {
@@ -942,6 +953,7 @@ __global__ void err_step_kernel(double* s) {
 
 struct SetSteps {
   static constexpr int NT = 32, MINB = 1;
+  static constexpr const char* FAMILY = "set_steps";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* ts, int J, double beta) {
@@ -1471,6 +1483,7 @@ constexpr int GRAPH_TILE = 32;
 //         of the energy along d; the accumulated L d stays the reference's gradient)
 struct GraphPass {
   static constexpr int NT = RED_THREADS, MINB = 1;
+  static constexpr const char* FAMILY = "graph_pass";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, int mode, int B, long long N,
@@ -1562,6 +1575,7 @@ __global__ void __launch_bounds__(RED_THREADS) graph_kernel(int mode, int B, lon
 // phase 2 (update):    q0 += t q1 + t^2 q2 / 2 at the accepted step
 struct QuadFold {
   static constexpr int NT = 32, MINB = 1;
+  static constexpr const char* FAMILY = "quad_fold";
   static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s, int phase) {

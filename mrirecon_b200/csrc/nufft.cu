@@ -423,6 +423,7 @@ struct InterpArgs {
 template <int ND>
 struct InterpGen {
   static constexpr int NT = 256, MINB = (ND == 2 ? 4 : 1);
+  static constexpr const char* FAMILY = "interp";
   static __device__ __forceinline__ void run(const VBlock& vb, const InterpArgs& a, const Geo& g,
       const KBPoly& kb) {
     constexpr int W = 4;
@@ -546,6 +547,7 @@ __global__ void __launch_bounds__(256) interp_kernel(InterpArgs a, Geo g, KBPoly
 // reads and result writes).  Same summation order as interp_kernel<2>.
 struct Interp2p {
   static constexpr int NT = 256, MINB = 4;
+  static constexpr const char* FAMILY = "interp";
   static __device__ __forceinline__ void run(const VBlock& vb, const InterpArgs& a, const Geo& g,
       const KBPoly& kb) {
     constexpr int W = 4;
@@ -623,6 +625,7 @@ __global__ void __launch_bounds__(256) interp2p_kernel(InterpArgs a, Geo g, KBPo
 // order are those of interp2p_kernel: identical samples.  C % 4 == 0.
 struct Interp2Quad {
   static constexpr int NT = 256, MINB = 4;
+  static constexpr const char* FAMILY = "interp";
   static __device__ __forceinline__ void run(const VBlock& vb, const InterpArgs& a, const Geo& g,
       const KBPoly& kb) {
     constexpr int W = 4;
@@ -900,6 +903,7 @@ struct SpreadSmem {
 template <int ND, int T>
 struct SpreadWarp {
   static constexpr int NT = SPREAD_WARPS * 32, MINB = 1;
+  static constexpr const char* FAMILY = "spread";
   static __device__ __forceinline__ void run(const VBlock& vb, const SpreadArgs& a, const Geo& g,
       const TileGeo& tg, const KBPoly& kb) {
     if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
@@ -1157,6 +1161,7 @@ struct Spread2wSmem {
 template <int T>
 struct Spread2Taps {
   static constexpr int NT = SPREAD_WARPS * 32, MINB = 5;
+  static constexpr const char* FAMILY = "spread";
   static __device__ __forceinline__ void run(const VBlock& vb, const SpreadArgs& a, const Geo& g,
       const TileGeo& tg, const KBPoly& kb) {
     if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
@@ -1740,6 +1745,7 @@ struct Spread2Smem {
 template <int PPL>
 struct Spread2Block {
   static constexpr int NT = S2_WARPS * 32, MINB = (PPL <= 4 ? 2 : 1);
+  static constexpr const char* FAMILY = "spread";
   static __device__ __forceinline__ void run(const VBlock& vb, const SpreadArgs& a, const Geo& g,
       const TileGeo& tg, const KBPoly& kb) {
     if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
@@ -1888,6 +1894,7 @@ __global__ void __launch_bounds__(S2_WARPS * 32) spread2_kernel(SpreadArgs a, Ge
 template <int ND, int T>
 struct ZeroTiles {
   static constexpr int NT = 256, MINB = 6;
+  static constexpr const char* FAMILY = "zero_tiles";
   static __device__ __forceinline__ void run(const VBlock& vb, const int* __restrict__ keys, int n_empty,
       float2* __restrict__ grid, const Geo& g, const TileGeo& tg, int nb) {
     if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
@@ -1942,6 +1949,7 @@ __global__ void __launch_bounds__(256) zero_tiles_kernel(const int* __restrict__
 template <int ND, int T>
 struct SpreadReduce {
   static constexpr int NT = 256, MINB = 6;
+  static constexpr const char* FAMILY = "spread_reduce";
   static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ partials,
       const int4* __restrict__ multi, int n_multi, int n_slots, float2* __restrict__ grid, const Geo& g,
       const TileGeo& tg, int nb) {
