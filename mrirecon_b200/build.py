@@ -30,13 +30,22 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _flags():
-    return ["-O3", "-lineinfo", "-std=c++17", "-fmad=true", "-Xcompiler", "-fPIC",
+# Files whose kernels also run in grouped form (csrc/group.cuh): the compiler
+# fuses no multiply into an add on its own there (every fused multiply-add is
+# written as fmaf / fma), so a kernel and its grouped form, two compilations of
+# the same source, round every operation alike and produce the same bits.
+NO_FMAD = {"ncg.cu", "fft.cu"}
+
+
+def _flags(src: str = ""):
+    fmad = "-fmad=false" if os.path.basename(src) in NO_FMAD else "-fmad=true"
+    return ["-O3", "-lineinfo", "-std=c++17", fmad, "-Xcompiler", "-fPIC",
             "-Xcompiler", "-O3", "--expt-relaxed-constexpr", "-I", os.path.join(PKG, "..", "include")] + ARCH
 
 
 def _deps_mtime(src: str) -> float:
-    hdrs = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(PKG, "..", "include", "*.h"))
+    hdrs = (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(PKG, "..", "include", "*.h")) +
+            [os.path.abspath(__file__)])
     return max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in hdrs])
 
 
@@ -44,7 +53,7 @@ def _compile(src: str, force: bool, verbose: bool) -> str:
     obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= _deps_mtime(src):
         return obj
-    cmd = [nvcc()] + _flags() + ["-c", src, "-o", obj]
+    cmd = [nvcc()] + _flags(src) + ["-c", src, "-o", obj]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), flush=True)

@@ -120,9 +120,11 @@ std::vector<float2> host_twiddles(int G) {
 // small DFTs: X_k = sum_n u_n e^{DIR 2 pi i k n / R}, in place
 //
 // Every floating-point operation of the passes is written with its rounding
-// stated (fmaf, __fmul_rn, __fadd_rn, __fsub_rn), so the compiler fuses no
-// multiply into an add on its own: a pass computes the same bits in every
-// kernel that contains it (the named kernels and their grouped forms).
+// stated (fmaf, __fmul_rn, __fadd_rn, __fsub_rn; the file also compiles with
+// -fmad=false), so the compiler fuses no multiply into an add on its own: a
+// pass computes the same bits in every kernel that contains it (the named
+// kernels and their grouped forms).  The butterflies fuse by hand where a
+// scaled term is added (e +- h p).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -__fmul_rn(a.y, b.y)), fmaf(a.x, b.y, __fmul_rn(a.y, b.x)));
@@ -172,18 +174,19 @@ struct Dft<8, DIR> {
     Dft<4, DIR>::run(e);
     Dft<4, DIR>::run(o);
     const float h = 0.707106781186547524f;
-    // o_k * e^{DIR i pi k / 4}: o1 = h (o + DIR i o), o3 = h (DIR i o - o)
-    const float2 o1 = cscale(cadd(o[1], cmul_di<DIR>(o[1])), h);
+    // o_k * e^{DIR i pi k / 4}: o1 = h p1, p1 = o + DIR i o; o3 = h p3, p3 = DIR i o - o;
+    // e_k +- h p_k as one fused multiply-add per component
+    const float2 p1 = cadd(o[1], cmul_di<DIR>(o[1]));
     const float2 o2 = cmul_di<DIR>(o[2]);
-    const float2 o3 = cscale(csub(cmul_di<DIR>(o[3]), o[3]), h);
+    const float2 p3 = csub(cmul_di<DIR>(o[3]), o[3]);
     u[0] = cadd(e[0], o[0]);
     u[4] = csub(e[0], o[0]);
-    u[1] = cadd(e[1], o1);
-    u[5] = csub(e[1], o1);
+    u[1] = make_float2(fmaf(h, p1.x, e[1].x), fmaf(h, p1.y, e[1].y));
+    u[5] = make_float2(fmaf(-h, p1.x, e[1].x), fmaf(-h, p1.y, e[1].y));
     u[2] = cadd(e[2], o2);
     u[6] = csub(e[2], o2);
-    u[3] = cadd(e[3], o3);
-    u[7] = csub(e[3], o3);
+    u[3] = make_float2(fmaf(h, p3.x, e[3].x), fmaf(h, p3.y, e[3].y));
+    u[7] = make_float2(fmaf(-h, p3.x, e[3].x), fmaf(-h, p3.y, e[3].y));
   }
 };
 
@@ -193,10 +196,10 @@ struct Dft<3, DIR> {
     const float c1 = -0.5f, s1 = 0.866025403784438647f * (float)DIR;
     const float2 t1 = cadd(u[1], u[2]), t2 = csub(u[1], u[2]);
     const float2 m = make_float2(fmaf(c1, t1.x, u[0].x), fmaf(c1, t1.y, u[0].y));
-    const float2 r = make_float2(__fmul_rn(-s1, t2.y), __fmul_rn(s1, t2.x));
+    // m +- r, r = DIR i s1 t2, as fused multiply-adds
     u[0] = cadd(u[0], t1);
-    u[1] = cadd(m, r);
-    u[2] = csub(m, r);
+    u[1] = make_float2(fmaf(-s1, t2.y, m.x), fmaf(s1, t2.x, m.y));
+    u[2] = make_float2(fmaf(s1, t2.y, m.x), fmaf(-s1, t2.x, m.y));
   }
 };
 
@@ -211,13 +214,12 @@ struct Dft<5, DIR> {
     const float2 x0 = u[0];
     const float2 m1 = make_float2(fmaf(c2, a2.x, fmaf(c1, a1.x, x0.x)), fmaf(c2, a2.y, fmaf(c1, a1.y, x0.y)));
     const float2 m2 = make_float2(fmaf(c1, a2.x, fmaf(c2, a1.x, x0.x)), fmaf(c1, a2.y, fmaf(c2, a1.y, x0.y)));
-    const float2 n1 = make_float2(-fmaf(s2, b2.y, __fmul_rn(s1, b1.y)), fmaf(s2, b2.x, __fmul_rn(s1, b1.x)));
-    const float2 n2 = make_float2(-fmaf(-s1, b2.y, __fmul_rn(s2, b1.y)), fmaf(-s1, b2.x, __fmul_rn(s2, b1.x)));
+    // m_k +- n_k with n1 = i (s1 b1 + s2 b2), n2 = i (s2 b1 - s1 b2), as fused multiply-adds
     u[0] = cadd(x0, cadd(a1, a2));
-    u[1] = cadd(m1, n1);
-    u[4] = csub(m1, n1);
-    u[2] = cadd(m2, n2);
-    u[3] = csub(m2, n2);
+    u[1] = make_float2(fmaf(-s2, b2.y, fmaf(-s1, b1.y, m1.x)), fmaf(s2, b2.x, fmaf(s1, b1.x, m1.y)));
+    u[4] = make_float2(fmaf(s2, b2.y, fmaf(s1, b1.y, m1.x)), fmaf(-s2, b2.x, fmaf(-s1, b1.x, m1.y)));
+    u[2] = make_float2(fmaf(s1, b2.y, fmaf(-s2, b1.y, m2.x)), fmaf(-s1, b2.x, fmaf(s2, b1.x, m2.y)));
+    u[3] = make_float2(fmaf(-s1, b2.y, fmaf(s2, b1.y, m2.x)), fmaf(s1, b2.x, fmaf(-s2, b1.x, m2.y)));
   }
 };
 

@@ -21,12 +21,13 @@
 //
 // Launch sites call launch<Body>(named_kernel, grid, smem, stream, args...).
 // Outside a recording that launches the named kernel (a __global__ wrapper
-// that passes hw_block()); a body with SHARED_CODE = true is launched through
-// its grouped kernel with a one-problem table instead, so that a problem
-// solved alone and the same problem inside a group run the same compiled
-// code and produce the same bits (the compiler may fuse a multiply into an
-// add differently in two kernels that contain the same source; the bodies
-// without SHARED_CODE state every rounding explicitly instead).
+// that passes hw_block()).  The named kernel and the grouped kernel are two
+// compilations of one body; they produce the same bits because nothing in a
+// body leaves the rounding to the compiler: the files that hold bodies with
+// arithmetic the compiler could fuse differently in the two kernels (a
+// multiply feeding an add) compile without automatic fusion (-fmad=false,
+// build.py) and write every fused multiply-add as fmaf / fma; the interp and
+// spread bodies use only explicit fused multiply-adds on such paths.
 // Between mrb_group_begin and mrb_group_end the call is recorded for the
 // problem selected with mrb_group_select; mrb_group_end replays the records
 // step by step (group.cu): FAMILY names the kernel step a body performs (the
@@ -87,10 +88,6 @@ template <class K> struct BodyMaxG<K, std::void_t<decltype(K::MAXG)>> { static c
 template <class K, class = void> struct BodyFamily { static constexpr const char* value = nullptr; };
 template <class K> struct BodyFamily<K, std::void_t<decltype(K::FAMILY)>> {
   static constexpr const char* value = K::FAMILY;
-};
-template <class K, class = void> struct BodyShared { static constexpr bool value = false; };
-template <class K> struct BodyShared<K, std::void_t<decltype(K::SHARED_CODE)>> {
-  static constexpr bool value = K::SHARED_CODE;
 };
 
 // kernel parameter space (32764 bytes from CUDA 12.1 on sm_70+), with room to spare
@@ -203,12 +200,7 @@ template <class K, class... A> struct GroupLauncher {
 
   static int single(const LaunchRec& r, cudaStream_t st) {
     if ((long long)r.grid.x * r.grid.y * r.grid.z == 0) return 0;
-    if constexpr (BodyShared<K>::value) {
-      const LaunchRec* one = &r;
-      return group(&one, 1, st);
-    } else {
-      return launch_named(r, st, S{});
-    }
+    return launch_named(r, st, S{});
   }
 };
 
@@ -218,8 +210,7 @@ template <class K, class... A> char GroupLauncher<K, A...>::key_tag = 0;
 template <class K, class... A>
 int launch(void (*kern)(A...), dim3 grid, size_t smem, cudaStream_t st, typename Ident<A>::type... a) {
   using L = GroupLauncher<K, A...>;
-  const bool rec = group_recording();
-  if (!rec && !BodyShared<K>::value) {
+  if (!group_recording()) {
     if ((long long)grid.x * grid.y * grid.z == 0) return 0;
     kern<<<grid, K::NT, smem, st>>>(a...);
     MRB_LAUNCH_CHECK();
@@ -238,8 +229,7 @@ int launch(void (*kern)(A...), dim3 grid, size_t smem, cudaStream_t st, typename
   std::memcpy(r.args.data(), &p, sizeof(p));
   r.single = &L::single;
   r.group = &L::group;
-  if (rec) return group_record(std::move(r));
-  return L::single(r, st);
+  return group_record(std::move(r));
 }
 
 }  // namespace mrb

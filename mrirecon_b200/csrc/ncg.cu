@@ -205,7 +205,6 @@ __global__ void __launch_bounds__(RED_THREADS) dots_kernel(DotArgs a, double* __
 struct KSpace {
   static constexpr int NT = RED_THREADS, MINB = 5;
   static constexpr const char* FAMILY = "kspace";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, int mode, long long n, float2* __restrict__ r,
       const float2* __restrict__ Ad, const float2* __restrict__ Ax, const float2* __restrict__ y,
@@ -344,7 +343,6 @@ template <int NS, int NU>
 struct TVGrad {
   static constexpr int NT = RED_THREADS, MINB = (NS <= 3 ? 4 : 1);
   static constexpr const char* FAMILY = "tv_grad";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, const GradArgs& a, const TVPlan& P,
       double* __restrict__ partials, const RedOut& ro) {
@@ -483,7 +481,6 @@ template <int NS, int NU, int JMAX>
 struct TVMulti {
   static constexpr int NT = RED_THREADS, MINB = (JMAX <= 8 ? 4 : 1);
   static constexpr const char* FAMILY = "tv_multi";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ x,
       const float2* __restrict__ d, const double* __restrict__ ts, int J, const TVPlan& P, const double* skip,
@@ -602,7 +599,6 @@ __device__ __forceinline__ NCGCfg load_cfg(const double* c) {
 struct ArmijoSelect {
   static constexpr int NT = 32, MINB = 1;
   static constexpr const char* FAMILY = "armijo_select";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s, const double* cfg_dev) {
     if (threadIdx.x != 0) return;
@@ -654,7 +650,6 @@ __global__ void armijo_select_kernel(double* s, const double* cfg_dev) {
 struct ArmijoPhase {
   static constexpr int NT = 32, MINB = 1;
   static constexpr const char* FAMILY = "armijo_phase";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s, const double* cfg_dev, int J1,
       int phase) {
@@ -721,7 +716,6 @@ __global__ void armijo_phase_kernel(double* s, const double* cfg_dev, int J1, in
 struct NCGControl {
   static constexpr int NT = 32, MINB = 1;
   static constexpr const char* FAMILY = "ncg_control";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s, double* hist, const double* cfg_dev,
       int nterms, int have_ft) {
@@ -811,7 +805,6 @@ __global__ void ncg_control_kernel(double* s, double* hist, const double* cfg_de
 struct NCGUpdate {
   static constexpr int NT = RED_THREADS, MINB = 4;
   static constexpr const char* FAMILY = "ncg_update";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, long long n, float2* __restrict__ x,
       float2* __restrict__ d, const float2* __restrict__ g, float2* __restrict__ gr,
@@ -863,7 +856,6 @@ __global__ void __launch_bounds__(RED_THREADS) ncg_update_kernel(long long n, fl
 struct Steepest {
   static constexpr int NT = RED_THREADS, MINB = 5;
   static constexpr const char* FAMILY = "steepest";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, long long n, float2* __restrict__ d,
       const float2* __restrict__ g, float2* __restrict__ g_prev, const float* __restrict__ diag,
@@ -899,7 +891,6 @@ __device__ __forceinline__ bool needs_restart(const double* s) {
 struct RestartDir {
   static constexpr int NT = RED_THREADS, MINB = 5;
   static constexpr const char* FAMILY = "restart_dir";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, long long n, float2* __restrict__ d,
       const float2* __restrict__ g, const float* __restrict__ diag, long long ndiag,
@@ -921,7 +912,6 @@ __global__ void __launch_bounds__(RED_THREADS) restart_dir_kernel(long long n, f
 struct RestartSlot {
   static constexpr int NT = 32, MINB = 1;
   static constexpr const char* FAMILY = "restart_slot";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s) {
     if (threadIdx.x != 0 || !needs_restart(s)) return;
@@ -939,7 +929,6 @@ __global__ void restart_slot_kernel(double* s) {
 struct ErrStep {
   static constexpr int NT = 32, MINB = 1;
   static constexpr const char* FAMILY = "err_step";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s) {
     if (threadIdx.x != 0 || s[S_LS_OK] == 0.0) return;
@@ -954,7 +943,6 @@ __global__ void err_step_kernel(double* s) {
 struct SetSteps {
   static constexpr int NT = 32, MINB = 1;
   static constexpr const char* FAMILY = "set_steps";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* ts, int J, double beta) {
     if (threadIdx.x == 0) {
@@ -1484,7 +1472,6 @@ constexpr int GRAPH_TILE = 32;
 struct GraphPass {
   static constexpr int NT = RED_THREADS, MINB = 1;
   static constexpr const char* FAMILY = "graph_pass";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, int mode, int B, long long N,
       const float* __restrict__ L, const float2* __restrict__ x, const float2* __restrict__ d,
@@ -1576,7 +1563,6 @@ __global__ void __launch_bounds__(RED_THREADS) graph_kernel(int mode, int B, lon
 struct QuadFold {
   static constexpr int NT = 32, MINB = 1;
   static constexpr const char* FAMILY = "quad_fold";
-  static constexpr bool SHARED_CODE = true;
   static constexpr int MAXG = 16;
   static __device__ __forceinline__ void run(const VBlock& vb, double* s, int phase) {
     if (threadIdx.x != 0) return;
