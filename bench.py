@@ -115,6 +115,9 @@ def parse():
                          "cudaProfilerStart/Stop")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the 16-instance uneven batch block (grouped, branch and sequential solves)")
+    ap.add_argument("--batched-profile", choices=["grouped", "branch"], default=None,
+                    help="profiling case: one eager NCG iteration of the 16-instance batch (after 3 untimed "
+                         "ones) between cudaProfilerStart/Stop")
     ap.add_argument("--plan-option", action="append", default=[], metavar="KEY=VALUE",
                     help="profiling cases: set a NUFFT plan option (mrb_plan_set_option key) before the runs")
     ap.add_argument("--koosh-only", type=int, default=0, metavar="N",
@@ -386,6 +389,52 @@ def run_ncg_only(w, n_iter, local):
     torch.cuda.profiler.stop()
     print(json.dumps({"ncg_only": w["name"], "iterations": n_iter, "iter": int(s.s[4].item())}))
     return 0
+
+
+def run_batched_profile(mode, local):
+    """Profiling case: the 16-instance uneven batch (grouped launches or one
+    stream per instance), primed and run for 3 eager iterations, then 10 timed
+    iterations (CUDA events) and one iteration between cudaProfilerStart and
+    cudaProfilerStop (ncu --profile-from-start off)."""
+    from mrirecon_b200.batched import BatchedSolver
+    from mrirecon_b200.workloads import batched_instances
+    dev = torch.device("cuda", local)
+    inst = batched_instances(dev)
+    cfg = solver_cfg()
+    cfg.restart = True
+    cfg.cuda_graph = False
+    bs = BatchedSolver([(p["y"], p["op"], p["regm"]) for p in inst], cfg, grouped=(mode == "grouped"))
+    for s in bs.solvers:
+        s._fast_setup(cfg.max_iter)
+
+    def first(s):
+        s._prime_fast()
+        s._skip_on_done(True)
+    bs._fork(first)
+    step = lambda: bs._step(lambda s: s._iteration_fast())
+    for _ in range(3):
+        step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = _lib_launches()
+    a.record()
+    for _ in range(10):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    launches = (_lib_launches() - n0) / 10
+    torch.cuda.profiler.start()
+    step()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"batched_profile": mode, "eager_ms_per_iteration": a.elapsed_time(b) / 10,
+                      "launches_per_iteration": launches}))
+    return 0
+
+
+def _lib_launches():
+    from mrirecon_b200 import _lib
+    return _lib.launch_count()
 
 
 KOOSH = dict(name="koosh3d_160cube_16coil_20000spk_256ro", N=160, C=16, spokes=20000, nread=256)
@@ -818,6 +867,8 @@ def main():
             return run_koosh_only(args.koosh_only, local)
         if args.ncg_only:
             return run_ncg_only(w, args.ncg_only, local)
+        if args.batched_profile:
+            return run_batched_profile(args.batched_profile, local)
         if args.batched_only:
             print(json.dumps({"batched16": batched_throughput(torch.device("cuda", local))}))
             return 0
