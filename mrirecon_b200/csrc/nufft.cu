@@ -885,18 +885,29 @@ __device__ __forceinline__ bool pair_touched(const SpreadArgs& a, int b, long lo
 constexpr int SPREAD_WARPS = 4;
 constexpr int SPREAD_BATCH = 32;
 
+// first grid node of a staged sample along each dim (2D: two ints, 3D: three in an int4)
+__device__ __forceinline__ int2 stage_base(const int* b, int2*) { return make_int2(b[0], b[1]); }
+__device__ __forceinline__ int4 stage_base(const int* b, int4*) { return make_int4(b[0], b[1], b[2], 0); }
+__device__ __forceinline__ int base_z(const int2&) { return 0; }
+__device__ __forceinline__ int base_z(const int4& b) { return b.z; }
+
 template <int ND, int T>
 struct SpreadSmem {
   static constexpr int CELLS = ND == 2 ? T * T : T * T * T;
   static constexpr int NW = 4 * ND;                               // staged weights per sample
   static constexpr int NWP = NW + 1;                              // their stride (odd: no bank conflicts)
   static constexpr int NTAP = ND == 2 ? 16 : 64;
+  // samples staged per batch: 2D tiles hold ~15 samples a frame in radial
+  // acquisitions, and the smaller staging area lets 6 instead of 5 blocks of
+  // 4 coils per item share an SM
+  static constexpr int BATCH = ND == 2 ? 16 : SPREAD_BATCH;
+  using Base = typename std::conditional<ND == 2, int2, int4>::type;
   // the shared tile is coil-interleaved, [cell][coil] with an even coil stride, so
   // one lane updates a pair of coils with one 128-bit read-modify-write
   __host__ __device__ static int cstride(int cpi) { return (cpi + 1) & ~1; }
   __host__ __device__ static size_t warp_bytes(int cpi) {
-    return (size_t)cstride(cpi) * CELLS * sizeof(float2) + SPREAD_BATCH * (sizeof(int4) + NWP * sizeof(float)) +
-           (size_t)SPREAD_BATCH * cstride(cpi) * sizeof(float2);
+    return (size_t)cstride(cpi) * CELLS * sizeof(float2) + BATCH * (sizeof(Base) + NWP * sizeof(float)) +
+           (size_t)BATCH * cstride(cpi) * sizeof(float2);
   }
 };
 
@@ -987,9 +998,11 @@ struct SpreadWarp {
     const int npair = cps >> 1;
     char* wbase = reinterpret_cast<char*>(smem4) + (size_t)warp * SM::warp_bytes(a.cpi);
     float2* acc = reinterpret_cast<float2*>(wbase);
-    int4* sb = reinterpret_cast<int4*>(wbase + (size_t)cps * CELLS * sizeof(float2));
-    float* sw = reinterpret_cast<float*>(sb + SPREAD_BATCH);
-    float2* sy = reinterpret_cast<float2*>(sw + SPREAD_BATCH * NW);
+    constexpr int SB = SM::BATCH;
+    using Base = typename SM::Base;
+    Base* sb = reinterpret_cast<Base*>(wbase + (size_t)cps * CELLS * sizeof(float2));
+    float* sw = reinterpret_cast<float*>(sb + SB);
+    float2* sy = reinterpret_cast<float2*>(sw + SB * NW);
 
     {
       float4* acc4 = reinterpret_cast<float4*>(acc);
@@ -1017,9 +1030,9 @@ struct SpreadWarp {
         for (int cl = 0; cl < PF; ++cl) py[cl] = cl < nc ? yb[(long long)cl * g.K + pk] : make_float2(0.f, 0.f);
       }
     };
-    if (e0 < e1) fetch(e0, min(SPREAD_BATCH, e1 - e0));
-    for (int e = e0; e < e1; e += SPREAD_BATCH) {
-      const int nbat = min(SPREAD_BATCH, e1 - e);
+    if (e0 < e1) fetch(e0, min(SB, e1 - e0));
+    for (int e = e0; e < e1; e += SB) {
+      const int nbat = min(SB, e1 - e);
       if (lane < nbat) {
         const int k = pk;
         float ws = a.gsign;
@@ -1039,7 +1052,7 @@ struct SpreadWarp {
             sw[lane * NW + d * 4 + q] = w;
           }
         }
-        sb[lane] = make_int4(base[0], base[1], base[2], 0);
+        sb[lane] = stage_base(base, (Base*)nullptr);
   #pragma unroll
         for (int cl = 0; cl < PF; ++cl)
           if (cl < cps) sy[lane * cps + cl] = py[cl];
@@ -1047,9 +1060,9 @@ struct SpreadWarp {
           sy[lane * cps + cl] = cl < nc ? yb[(long long)cl * g.K + k] : make_float2(0.f, 0.f);
       }
       __syncwarp();
-      if (e + SPREAD_BATCH < e1) fetch(e + SPREAD_BATCH, min(SPREAD_BATCH, e1 - e - SPREAD_BATCH));
+      if (e + SB < e1) fetch(e + SB, min(SB, e1 - e - SB));
       for (int j = 0; j < nbat; ++j) {
-        const int4 bb = sb[j];
+        const Base bb = sb[j];
         const float* wj = sw + j * NW;
         const float4* yj = reinterpret_cast<const float4*>(sy + j * cps);
         // lane tasks: (tap, coil pair), every task of a sample touches a distinct float4;
@@ -1075,7 +1088,7 @@ struct SpreadWarp {
             w = inside ? wj[ox] * wj[4 + oy] : 0.f;
           } else {
             const int a0 = tap >> 4, a1 = (tap >> 2) & 3, a2 = tap & 3;
-            int n0 = bb.x + a0, n1 = bb.y + a1, n2 = bb.z + a2;
+            int n0 = bb.x + a0, n1 = bb.y + a1, n2 = base_z(bb) + a2;
             n0 += n0 < 0 ? g.G[0] : 0;
             n0 -= n0 >= g.G[0] ? g.G[0] : 0;
             n1 += n1 < 0 ? g.G[1] : 0;
