@@ -913,7 +913,7 @@ struct SpreadSmem {
 
 template <int ND, int T>
 struct SpreadWarp {
-  static constexpr int NT = SPREAD_WARPS * 32, MINB = 1;
+  static constexpr int NT = SPREAD_WARPS * 32, MINB = 6;
   static constexpr const char* FAMILY = "spread";
   static __device__ __forceinline__ void run(const VBlock& vb, const SpreadArgs& a, const Geo& g,
       const TileGeo& tg, const KBPoly& kb) {
@@ -1052,6 +1052,16 @@ struct SpreadWarp {
             sw[lane * NW + d * 4 + q] = w;
           }
         }
+        // tile-relative first node r = base - o, taken modulo G into [-3, G - 4]:
+        // tap t of the sample then sits at local index r + t (+ G when negative),
+        // without the per-tap wrap into the grid
+  #pragma unroll
+        for (int d = 0; d < ND; ++d) {
+          int r = base[d] - o[d];
+          r += r < -3 ? g.G[d] : 0;
+          r -= r > g.G[d] - 4 ? g.G[d] : 0;
+          base[d] = r;
+        }
         sb[lane] = stage_base(base, (Base*)nullptr);
   #pragma unroll
         for (int cl = 0; cl < PF; ++cl)
@@ -1061,6 +1071,35 @@ struct SpreadWarp {
       }
       __syncwarp();
       if (e + SB < e1) fetch(e + SB, min(SB, e1 - e - SB));
+      if (ND == 2 && ntask <= 32) {
+        // one task per lane (coil groups of up to 4 coils): the task's coil pair and
+        // tap are fixed for the whole batch; same cells, weights and order as below
+        const bool act = lane < ntask;
+        const int pr = npair == 2 ? (lane & 1) : lane % npair;
+        const int tap = npair == 2 ? (lane >> 1) : lane / npair;
+        const int ox = tap >> 2, oy = tap & 3;
+        float4* accp = reinterpret_cast<float4*>(acc) + pr;
+        for (int j = 0; j < nbat; ++j) {
+          const Base bb = sb[j];
+          int lx = bb.x + ox, ly = bb.y + oy;
+          lx += lx < 0 ? g.G[0] : 0;
+          ly += ly < 0 ? g.G[1] : 0;
+          if (act && (unsigned)lx < (unsigned)T && (unsigned)ly < (unsigned)T) {
+            const float* wj = sw + j * NW;
+            const float w = wj[ox] * wj[4 + oy];
+            const float4 v = reinterpret_cast<const float4*>(sy + j * cps)[pr];
+            float4* p = accp + (lx * T + ly) * npair;
+            float4 t = *p;
+            t.x = fmaf(w, v.x, t.x);
+            t.y = fmaf(w, v.y, t.y);
+            t.z = fmaf(w, v.z, t.z);
+            t.w = fmaf(w, v.w, t.w);
+            *p = t;
+          }
+          __syncwarp();
+        }
+        continue;
+      }
       for (int j = 0; j < nbat; ++j) {
         const Base bb = sb[j];
         const float* wj = sw + j * NW;
@@ -1077,25 +1116,18 @@ struct SpreadWarp {
           bool inside;
           if (ND == 2) {
             const int ox = tap >> 2, oy = tap & 3;
-            int n0 = bb.x + ox, n1 = bb.y + oy;
-            n0 += n0 < 0 ? g.G[0] : 0;
-            n0 -= n0 >= g.G[0] ? g.G[0] : 0;
-            n1 += n1 < 0 ? g.G[1] : 0;
-            n1 -= n1 >= g.G[1] ? g.G[1] : 0;
-            const int lx = n0 - o[0], ly = n1 - o[1];
+            int lx = bb.x + ox, ly = bb.y + oy;
+            lx += lx < 0 ? g.G[0] : 0;
+            ly += ly < 0 ? g.G[1] : 0;
             inside = (unsigned)lx < (unsigned)T && (unsigned)ly < (unsigned)T;
             cell = lx * T + ly;
             w = inside ? wj[ox] * wj[4 + oy] : 0.f;
           } else {
             const int a0 = tap >> 4, a1 = (tap >> 2) & 3, a2 = tap & 3;
-            int n0 = bb.x + a0, n1 = bb.y + a1, n2 = base_z(bb) + a2;
-            n0 += n0 < 0 ? g.G[0] : 0;
-            n0 -= n0 >= g.G[0] ? g.G[0] : 0;
-            n1 += n1 < 0 ? g.G[1] : 0;
-            n1 -= n1 >= g.G[1] ? g.G[1] : 0;
-            n2 += n2 < 0 ? g.G[2] : 0;
-            n2 -= n2 >= g.G[2] ? g.G[2] : 0;
-            const int l0 = n0 - o[0], l1 = n1 - o[1], l2 = n2 - o[2];
+            int l0 = bb.x + a0, l1 = bb.y + a1, l2 = base_z(bb) + a2;
+            l0 += l0 < 0 ? g.G[0] : 0;
+            l1 += l1 < 0 ? g.G[1] : 0;
+            l2 += l2 < 0 ? g.G[2] : 0;
             inside = (unsigned)l0 < (unsigned)T && (unsigned)l1 < (unsigned)T && (unsigned)l2 < (unsigned)T;
             cell = (l0 * T + l1) * T + l2;
             w = inside ? wj[a0] * wj[4 + a1] * wj[8 + a2] : 0.f;
