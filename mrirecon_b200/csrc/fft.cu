@@ -167,12 +167,33 @@ struct Dft<4, DIR> {
 
 template <int DIR>
 struct Dft<8, DIR> {
+  // radix-2 split into the 4-point DFTs of the even and odd samples
   __device__ __forceinline__ static void run(float2* u) {
-    // radix-2 split into the 4-point DFTs of the even and odd samples
     float2 e[4] = {u[0], u[2], u[4], u[6]};
     float2 o[4] = {u[1], u[3], u[5], u[7]};
     Dft<4, DIR>::run(e);
     Dft<4, DIR>::run(o);
+    combine(e, o, u);
+  }
+  // u = (0, 0, u2, u3, u4, u5, 0, 0): the first stage of a transform whose input
+  // is the centred half of its length (2x oversampled grid, even image size).
+  // The 4-point DFTs of (0, u2, u4, 0) and (0, u3, u5, 0) without the terms in
+  // the zeros: the same values as run() (up to the sign of an exact zero).
+  __device__ __forceinline__ static void run_mid(float2* u) {
+    float2 e[4], o[4];
+    half4(u[2], u[4], e);
+    half4(u[3], u[5], o);
+    combine(e, o, u);
+  }
+  // Dft<4> of (0, b, c, 0): a0 = c, a1 = -c, a2 = b, a3 = DIR i b
+  __device__ __forceinline__ static void half4(float2 b, float2 c, float2* x) {
+    const float2 a3 = cmul_di<DIR>(b);
+    x[0] = cadd(c, b);
+    x[2] = csub(c, b);
+    x[1] = make_float2(__fsub_rn(a3.x, c.x), __fsub_rn(a3.y, c.y));
+    x[3] = make_float2(-__fadd_rn(c.x, a3.x), -__fadd_rn(c.y, a3.y));
+  }
+  __device__ __forceinline__ static void combine(const float2* e, const float2* o, float2* u) {
     const float h = 0.707106781186547524f;
     // o_k * e^{DIR i pi k / 4}: o1 = h p1, p1 = o + DIR i o; o3 = h p3, p3 = DIR i o - o;
     // e_k +- h p_k as one fused multiply-add per component
@@ -236,11 +257,15 @@ __device__ __forceinline__ void stage_sync() {
   else __syncthreads();
 }
 
-template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool WARP, class LD, class ST>
+// MID: the first stage of a transform whose nonzero input is the centred half
+// [G/4, 3G/4): with R = 8 and T = G/8 every butterfly's inputs i + r T are
+// zero for r = 0, 1, 6, 7, so only r = 2..5 are loaded (Dft<8>::run_mid).
+template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool WARP, bool MID, class LD, class ST>
 __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load, ST store) {
   constexpr int R = radix_at(G, S);
   constexpr int P = span_at(G, S);
   constexpr int T = G / R;
+  static_assert(!MID || (R == 8 && S == 0), "the centred-input stage is a first radix-8 stage");
   constexpr int TOTAL = ROWS * T;
   constexpr int NI = (TOTAL + NT - 1) / NT;
   static_assert(!WARP || (NT == 32 && ROWS == 1), "warp transforms are one row of 32 lanes");
@@ -254,7 +279,8 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load
       const int q = QFAST ? w % ROWS : w / T;
       const int i = QFAST ? w / ROWS : w % T;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[c][r] = load(q, i + r * T);
+      for (int r = 0; r < R; ++r)
+        if (!MID || (r >= 2 && r <= 5)) v[c][r] = load(q, i + r * T);
     }
   }
   stage_sync<WARP>();
@@ -273,7 +299,8 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load
           v[c][r] = cmul(v[c][r], t);
         }
       }
-      Dft<R, DIR>::run(v[c]);
+      if constexpr (MID) Dft<8, DIR>::run_mid(v[c]);
+      else Dft<R, DIR>::run(v[c]);
       const int j = (i - k) * R + k;
 #pragma unroll
       for (int r = 0; r < R; ++r) store(q, j + r * P, v[c][r]);
@@ -285,19 +312,27 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load
 // All stages of a length-G transform of ROWS rows: the first stage loads
 // through load0, the last stores through store_last, and intermediate results
 // live in buf (row q at q * LD, element e at slot swz(e) when PAD).
-template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool PAD, int LD, bool WARP = false, class LD0,
-          class STL>
+template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool PAD, int LD, bool WARP = false, bool MID = false,
+          class LD0, class STL>
 __device__ __forceinline__ void fft_stages(float2* buf, const float2* tw, LD0 load0, STL store_last) {
   constexpr int NS = n_stages(G);
+  constexpr bool MID0 = MID && S == 0;
   if constexpr (S < NS) {
     auto sload = [&](int q, int e) { return buf[q * LD + (PAD ? swz(e) : e)]; };
     auto sstore = [&](int q, int e, float2 v) { buf[q * LD + (PAD ? swz(e) : e)] = v; };
-    if constexpr (S == 0 && S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP>(tw, load0, store_last);
-    else if constexpr (S == 0) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP>(tw, load0, sstore);
-    else if constexpr (S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP>(tw, sload, store_last);
-    else fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP>(tw, sload, sstore);
-    fft_stages<G, S + 1, ROWS, NT, DIR, QFAST, PAD, LD, WARP>(buf, tw, load0, store_last);
+    if constexpr (S == 0 && S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, MID0>(tw, load0, store_last);
+    else if constexpr (S == 0) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, MID0>(tw, load0, sstore);
+    else if constexpr (S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, false>(tw, sload, store_last);
+    else fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, false>(tw, sload, sstore);
+    fft_stages<G, S + 1, ROWS, NT, DIR, QFAST, PAD, LD, WARP, MID>(buf, tw, load0, store_last);
   }
+}
+
+// the nonzero input of a length-G transform is its centred half [G/4, 3G/4)
+// and the transform starts with radix 8: the first stage may skip the zeros
+template <int G>
+__device__ __forceinline__ bool centred_half(int S, int off) {
+  return radix_at(G, 0) == 8 && 2 * S == G && 4 * off == G;
 }
 
 struct Geo2 {
@@ -312,7 +347,7 @@ constexpr int ROW_WARPS = ROW_NT / 32;
 
 template <int G1>
 struct FwdRows {
-  static constexpr int NT = ROW_NT, MINB = (G1 <= 256 ? 5 : G1 <= 384 ? 4 : G1 <= 640 ? 3 : G1 <= 768 ? 2 : 1);
+  static constexpr int NT = ROW_NT, MINB = (G1 <= 256 ? 5 : G1 <= 512 ? 4 : G1 <= 640 ? 3 : G1 <= 768 ? 2 : 1);
   static constexpr const char* FAMILY = "fwd_rows";
   static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ x,
       const float2* __restrict__ maps, const float* __restrict__ rowfac, const float* __restrict__ coldeap,
@@ -342,11 +377,17 @@ struct FwdRows {
       return cscale(cmul(xv, mv), s);
     };
     auto store = [&](int, int k1, float2 v) { out[k1] = v; };
+    if constexpr (radix_at(G1, 0) == 8) {
+      if (centred_half<G1>(g.S1, g.off1)) {
+        fft_stages<G1, 0, 1, 32, -1, false, true, LD, true, true>(buf, tw, load0, store);
+        return;
+      }
+    }
     fft_stages<G1, 0, 1, 32, -1, false, true, LD, true>(buf, tw, load0, store);
   }
 };
 template <int G1>
-__global__ void __launch_bounds__(ROW_NT) fwd_rows_kernel(const float2* __restrict__ x,
+__global__ void __launch_bounds__(ROW_NT, FwdRows<G1>::MINB) fwd_rows_kernel(const float2* __restrict__ x,
     const float2* __restrict__ maps, const float* __restrict__ rowfac, const float* __restrict__ coldeap,
     float2* __restrict__ Tb, const float2* __restrict__ tw, Geo2 g, long long nrows, int coil_images) {
   FwdRows<G1>::run(hw_block(), x, maps, rowfac, coldeap, Tb, tw, g, nrows, coil_images);
@@ -380,6 +421,12 @@ struct FwdCols {
     auto store = [&](int q, int n0, float2 v) {
       if (full || k0 + q < G1) gv[n0 * G1 + q] = v;
     };
+    if constexpr (radix_at(G0, 0) == 8) {
+      if (centred_half<G0>(g.S0, g.off0)) {
+        fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD, false, true>(sm, tw, load0, store);
+        return;
+      }
+    }
     fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
   }
 };
