@@ -669,11 +669,22 @@ class CGSolver:
         _lib.check(self.lib.mrb_kspace_pass(1, self.n_k, _lib.ptr(tmp), None, _lib.ptr(tmp), _lib.ptr(self.y),
                                             None, 0.0, None, out.data_ptr(), _lib.ptr(self.ws_buf), self._st()),
                    "kspace_pass")
-        g = torch.empty_like(self.x)
+        self.regularizer_energy_into(self.x, out)
+        v = out.tolist()
+        return 0.5 * v[0] + self.regularizer_energy_from(v)
+
+    def regularizer_energy_into(self, x: torch.Tensor, out: torch.Tensor) -> None:
+        """R(x) terms of image x into the FP64 device vector out (24 values; TV terms
+        at 8 + i, the graph term at 20), on the device without a host read."""
         _lib.check(self.lib.mrb_tv_grad(self.nd, self._Sarr, self.F, self._terms_arr, self.nterms,
-                                        _lib.ptr(self.x), None, None, 0.0, None, None, None, None, 0, None,
+                                        _lib.ptr(x), None, None, 0.0, None, None, None, None, 0, None,
                                         None, 0, out.data_ptr() + 64, _lib.ptr(self.ws_buf), self._st()),
                    "tv_grad")
-        self._graph_pass(0, None, None, 0.0, None, out.data_ptr() + 8 * 20)
-        v = out.tolist()
-        return 0.5 * v[0] + sum(v[8:8 + self.nterms]) + (v[20] if self._L is not None else 0.0)
+        if self._L is not None:
+            _lib.check(self.lib.mrb_graph_pass(0, self.F, self.n_img // self.F, _lib.ptr(self._L), _lib.ptr(x),
+                                               None, None, 0.0, None, None, out.data_ptr() + 8 * 20,
+                                               _lib.ptr(self.ws_buf), self._st()), "graph_pass")
+
+    def regularizer_energy_from(self, v: List[float]) -> float:
+        """R from the values regularizer_energy_into wrote (read to the host as v)."""
+        return sum(v[8:8 + self.nterms]) + (v[20] if self._L is not None else 0.0)

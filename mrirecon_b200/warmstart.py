@@ -458,43 +458,70 @@ def ramp_adjoint(op, y: torch.Tensor) -> torch.Tensor:
 
 
 def _ls_scaled(op, y, x):
-    """x times its least-squares data-consistency factor argmin_a ||a A x - y||."""
+    """x times its least-squares data-consistency factor argmin_a ||a A x - y||
+    (the sums in FP64 on the device, as warm_start forms them)."""
+    from .regularization import workspace
     Ax = op.A(x)
-    den = float(torch.vdot(Ax.reshape(-1), Ax.reshape(-1)).real)
-    a = float(torch.vdot(Ax.reshape(-1), y.reshape(-1)).real) / max(den, 1e-30)
-    return (a * x).to(torch.complex64)
+    s = _dots_f64([(Ax, Ax), (Ax, y)], workspace(x.device))
+    return (x * (s[1] / s[0].clamp_min(1e-30)).to(torch.float32)).to(torch.complex64)
 
 
 def network_start(op, y, cnn: WarmStartCNN, image_shape) -> torch.Tensor:
     """The network's image for data y (LS-scaled), shaped like the solver's image."""
-    z = ramp_adjoint(op, y)
-    F = int(z.shape[0])
-    S = tuple(int(s) for s in z.shape[2:])
-    x = cnn.infer(z.to(torch.complex64).reshape((1, F) + S)).reshape(image_shape)
-    return _ls_scaled(op, y, x)
+    return _ls_scaled(op, y, _network_image(op, y, cnn, image_shape))
 
 
 def warm_start(solver, cnn: WarmStartCNN) -> dict:
     """Initial image for `solver` from the network, with the fallback rule:
     the network output is used only if its objective is below that of the
-    adjoint start (the adjoint recon A^H y scaled by its least-squares factor)."""
+    adjoint start (the adjoint recon A^H y scaled by its least-squares factor).
+
+    Both starts are scaled by their least-squares data-consistency factors
+    a = Re<Ax, y> / ||Ax||^2, whose data terms follow from the same sums:
+    0.5 ||a A x - y||^2 = 0.5 (||y||^2 - Re<Ax, y>^2 / ||Ax||^2).  The sums (FP64
+    on the device) and the regularisers' energies at the scaled starts are read
+    to the host once."""
     op = solver.op
     y = solver.y
-    x_adj = _ls_scaled(op, y, op.AH(y))
-    x_net = network_start(op, y, cnn, x_adj.shape)
-    f_adj = _objective_at(solver, x_adj)
-    f_net = _objective_at(solver, x_net)
+    x_adj = op.AH(y)
+    x_cnn = _network_image(op, y, cnn, x_adj.shape)
+    ax_adj, ax_cnn = op.A(x_adj), op.A(x_cnn)
+    s = _dots_f64([(ax_adj, ax_adj), (ax_adj, y), (ax_cnn, ax_cnn), (ax_cnn, y), (y, y)], solver.ws_buf)
+    # the factors stay on the device: x * (num / den)
+    a = torch.stack([s[1] / s[0].clamp_min(1e-30), s[3] / s[2].clamp_min(1e-30)]).to(torch.float32)
+    x_adj = (x_adj * a[0]).to(torch.complex64)
+    x_net = (x_cnn * a[1]).to(torch.complex64)
+    e_adj = torch.zeros(24, dtype=torch.float64, device=y.device)
+    e_net = torch.zeros(24, dtype=torch.float64, device=y.device)
+    solver.regularizer_energy_into(x_adj, e_adj)
+    solver.regularizer_energy_into(x_net, e_net)
+    v = torch.cat([s, e_adj, e_net]).tolist()
+    den_a, num_a, den_n, num_n, yy = v[:5]
+    f_adj = 0.5 * max(yy - num_a * num_a / max(den_a, 1e-30), 0.0) + solver.regularizer_energy_from(v[5:29])
+    f_net = 0.5 * max(yy - num_n * num_n / max(den_n, 1e-30), 0.0) + solver.regularizer_energy_from(v[29:53])
     use = f_net < f_adj
     solver.reset(x_net if use else x_adj)
     return {"used_network": bool(use), "f_network": f_net, "f_adjoint": f_adj}
 
 
-def _objective_at(solver, x):
-    keep = solver.x.clone()
-    solver.x.copy_(x)
-    f = solver.objective()
-    solver.x.copy_(keep)
-    return f
+def _dots_f64(pairs, ws) -> torch.Tensor:
+    """Re<a_j, b_j> for (a_j, b_j) in pairs (complex64, equal lengths), FP64 on the
+    device; ws is a reduction workspace of the library."""
+    n = int(pairs[0][0].numel())
+    A = (ct.c_void_p * len(pairs))(*[_p(a) for a, _ in pairs])
+    B = (ct.c_void_p * len(pairs))(*[_p(b) for _, b in pairs])
+    out = torch.empty(len(pairs), dtype=torch.float64, device=pairs[0][0].device)
+    _lib.check(_lib.load().mrb_dots_f64(n, len(pairs), A, B, None, 0, _p(out), _p(ws), _lib.stream_ptr(out.device)),
+               "dots_f64")
+    return out
+
+
+def _network_image(op, y, cnn: WarmStartCNN, image_shape) -> torch.Tensor:
+    """The network's image for data y (not yet scaled), shaped like the solver's image."""
+    z = ramp_adjoint(op, y)
+    F = int(z.shape[0])
+    S = tuple(int(s) for s in z.shape[2:])
+    return cnn.infer(z.to(torch.complex64).reshape((1, F) + S)).reshape(image_shape)
 
 
 def evaluate(cnn: "WarmStartCNN", workload: str = "grasp", device="cuda", reps: int = 1) -> dict:
