@@ -345,6 +345,86 @@ __global__ void up2_bwd_kernel(const float* __restrict__ gy, int cgy, int gy_off
   gx[((r * vi.H + h) * vi.W + w) * cgx + gx_off + c] = s;
 }
 
+// The same three data movements with 16-byte accesses: a thread moves 8
+// channels (one uint4) of one voxel, a block row covers one image row, and the
+// voxel index is rebuilt with 32-bit arithmetic from the row (blockIdx.y, grid-
+// strided).  For channel counts, strides and offsets that are multiples of 8
+// (16-byte aligned rows); 1 << lg8 = channels / 8.  Same values as the
+// element kernels above (pooling sums in the same order).
+__device__ __forceinline__ void bf16x8_to_f32(const uint4& u, float* f) {
+  const bf16* h = reinterpret_cast<const bf16*>(&u);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) f[k] = __bfloat162float(h[k]);
+}
+
+// nearest 2x upsample over (H, W): fine row `row` of (Nb, D, 2H) rows
+__global__ void up2_fwd_vec_kernel(const bf16* __restrict__ x, int cx, int x_off, int lg8, Vol vi,
+                                   bf16* __restrict__ y, int cy, int y_off) {
+  const int Ho = vi.H * 2, Wo = vi.W * 2;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (Wo << lg8)) return;
+  const int wo = e >> lg8, c = (e & ((1 << lg8) - 1)) * 8;
+  const int rows = vi.Nb * vi.D * Ho;
+  for (int row = blockIdx.y; row < rows; row += gridDim.y) {
+    const int nd = row / Ho, ho = row - nd * Ho;
+    const long long src = (((long long)nd * vi.H + ho / 2) * vi.W + wo / 2) * cx + x_off + c;
+    const long long dst = ((long long)row * Wo + wo) * cy + y_off + c;
+    *reinterpret_cast<uint4*>(y + dst) = __ldg(reinterpret_cast<const uint4*>(x + src));
+  }
+}
+
+// 2x2 average pool over (H, W): coarse row `row` of (Nb, D, H/2) rows
+__global__ void pool2_fwd_vec_kernel(const bf16* __restrict__ x, int cx, int x_off, int lg8, Vol vi,
+                                     bf16* __restrict__ y, int cy, int y_off) {
+  const int Ho = vi.H / 2, Wo = vi.W / 2;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (Wo << lg8)) return;
+  const int wo = e >> lg8, c = (e & ((1 << lg8) - 1)) * 8;
+  const int rows = vi.Nb * vi.D * Ho;
+  for (int row = blockIdx.y; row < rows; row += gridDim.y) {
+    const int nd = row / Ho, ho = row - nd * Ho;
+    float s[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s[k] = 0.f;
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+      for (int dxx = 0; dxx < 2; ++dxx) {
+        const long long v = ((long long)nd * vi.H + 2 * ho + dy) * vi.W + 2 * wo + dxx;
+        float f[8];
+        bf16x8_to_f32(__ldg(reinterpret_cast<const uint4*>(x + v * cx + x_off + c)), f);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s[k] += f[k];
+      }
+    uint4 out;
+    bf16* h = reinterpret_cast<bf16*>(&out);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) h[k] = __float2bfloat16_rn(0.25f * s[k]);
+    *reinterpret_cast<uint4*>(y + ((long long)row * Wo + wo) * cy + y_off + c) = out;
+  }
+}
+
+// complex -> channels-last BF16 with cx % 8 == 0: frame `fr` = blockIdx.y (grid-strided) of Nb * D
+__global__ void pack_vec_kernel(const float2* __restrict__ z, const float* __restrict__ scale, Vol v,
+                                bf16* __restrict__ x, int cx) {
+  const int hw = v.H * v.W;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= hw) return;
+  const int frames = v.Nb * v.D;
+  for (int fr = blockIdx.y; fr < frames; fr += gridDim.y) {
+    const long long vox = (long long)fr * hw + p;
+    const float sc = scale[fr / v.D];
+    const float2 zz = z[vox];
+    uint4 first = make_uint4(0u, 0u, 0u, 0u);
+    bf16* h = reinterpret_cast<bf16*>(&first);
+    h[0] = __float2bfloat16_rn(zz.x * sc);
+    h[1] = __float2bfloat16_rn(zz.y * sc);
+    uint4* dst = reinterpret_cast<uint4*>(x + vox * cx);
+    dst[0] = first;
+    for (int k = 1; k < cx / 8; ++k) dst[k] = make_uint4(0u, 0u, 0u, 0u);
+  }
+}
+
 // complex (Nb, D, H, W) -> channels-last BF16 (.., cx) channels 0/1 = re/im * scale[n], rest zero
 __global__ void pack_kernel(const float2* __restrict__ z, const float* __restrict__ scale, Vol v, bf16* __restrict__ x,
                             int cx) {
@@ -530,13 +610,31 @@ extern "C" int mrb_cnn_relu_bwd(const float* g, int cgs, int g_off, const void* 
   return 0;
 }
 
+// 16-byte channel groups possible: nch = 8 * 2^lg8, strides and offsets multiples of 8, aligned bases
+static bool vec8(int nch, int cin_s, int in_off, int cout_s, int out_off, const void* in, const void* out, int* lg8) {
+  if (nch <= 0 || nch % 8 || cin_s % 8 || in_off % 8 || cout_s % 8 || out_off % 8) return false;
+  if (((uintptr_t)in & 15) || ((uintptr_t)out & 15)) return false;
+  const int g = nch / 8;
+  if (g & (g - 1)) return false;
+  int l = 0;
+  while ((1 << l) < g) ++l;
+  *lg8 = l;
+  return true;
+}
+
 extern "C" int mrb_cnn_pool2(int dir, const void* in, int cin_s, int in_off, int nch, const int* fine_vol, void* out,
                              int cout_s, int out_off, mrb_stream_t stream) {
   MRB_REQUIRE(in && out && fine_vol, "null pointer");
   Vol v = mkvol(fine_vol);
   MRB_REQUIRE(v.H % 2 == 0 && v.W % 2 == 0, "pooling needs even H and W");
   cudaStream_t st = (cudaStream_t)stream;
-  if (dir == 0) {
+  int lg8 = 0;
+  if (dir == 0 && vec8(nch, cin_s, in_off, cout_s, out_off, in, out, &lg8) && v.voxels() < (1LL << 31)) {
+    const int per_row = (v.W / 2) << lg8;
+    const int rows = v.Nb * v.D * (v.H / 2);
+    pool2_fwd_vec_kernel<<<dim3((unsigned)nblk(per_row, 256), (unsigned)std::min(rows, 65535)), 256, 0, st>>>(
+        (const bf16*)in, cin_s, in_off, lg8, v, (bf16*)out, cout_s, out_off);
+  } else if (dir == 0) {
     long long n = v.voxels() / 4 * nch;
     pool2_fwd_kernel<<<nblk(n, 256), 256, 0, st>>>((const bf16*)in, cin_s, in_off, nch, v, (bf16*)out, cout_s,
                                                    out_off);
@@ -554,7 +652,13 @@ extern "C" int mrb_cnn_up2(int dir, const void* in, int cin_s, int in_off, int n
   MRB_REQUIRE(in && out && coarse_vol, "null pointer");
   Vol v = mkvol(coarse_vol);
   cudaStream_t st = (cudaStream_t)stream;
-  if (dir == 0) {
+  int lg8 = 0;
+  if (dir == 0 && vec8(nch, cin_s, in_off, cout_s, out_off, in, out, &lg8) && v.voxels() * 4 < (1LL << 31)) {
+    const int per_row = (2 * v.W) << lg8;
+    const int rows = v.Nb * v.D * 2 * v.H;
+    up2_fwd_vec_kernel<<<dim3((unsigned)nblk(per_row, 256), (unsigned)std::min(rows, 65535)), 256, 0, st>>>(
+        (const bf16*)in, cin_s, in_off, lg8, v, (bf16*)out, cout_s, out_off);
+  } else if (dir == 0) {
     long long n = v.voxels() * 4 * nch;
     up2_fwd_kernel<<<nblk(n, 256), 256, 0, st>>>((const bf16*)in, cin_s, in_off, nch, v, (bf16*)out, cout_s, out_off);
   } else {
@@ -569,7 +673,14 @@ extern "C" int mrb_cnn_up2(int dir, const void* in, int cin_s, int in_off, int n
 extern "C" int mrb_cnn_pack(const void* z, const float* scale, const int* vol, void* x, int cx, mrb_stream_t stream) {
   MRB_REQUIRE(z && scale && vol && x && cx >= 2, "bad arguments");
   Vol v = mkvol(vol);
-  pack_kernel<<<nblk(v.voxels() * cx, 256), 256, 0, (cudaStream_t)stream>>>((const float2*)z, scale, v, (bf16*)x, cx);
+  if (cx % 8 == 0 && ((uintptr_t)x & 15) == 0 && (long long)v.H * v.W < (1LL << 31)) {
+    const int frames = v.Nb * v.D;
+    pack_vec_kernel<<<dim3((unsigned)nblk((long long)v.H * v.W, 256), (unsigned)std::min(frames, 65535)), 256, 0,
+                      (cudaStream_t)stream>>>((const float2*)z, scale, v, (bf16*)x, cx);
+  } else {
+    pack_kernel<<<nblk(v.voxels() * cx, 256), 256, 0, (cudaStream_t)stream>>>((const float2*)z, scale, v, (bf16*)x,
+                                                                             cx);
+  }
   MRB_LAUNCH_CHECK();
   return 0;
 }
