@@ -686,35 +686,39 @@ __global__ void __launch_bounds__(COL_NT) toeplitz_cols_kernel(float2* __restric
 }
 
 // adjoint row pass: x[be][r][i1] = scale * deapod * sign *
-//   sum_c conj(S_c) IFFT_G1(T[(be, c)][r][:])[i1 + off1], one block per (be, r),
-// coils in passes of ROWS
+//   sum_c conj(S_c) IFFT_G1(T[(be, c)][r][:])[i1 + off1], one block per (be, r).
+// Each of the ARW_WARPS warps transforms one coil row (warp-synchronous stages,
+// no block barrier inside a transform, as the forward row pass); after each pass
+// of ARW_WARPS coils the block adds them to the row's accumulators in coil order.
+constexpr int ARW_WARPS = 4;
+
 template <int G1>
 struct AdjRows {
-  static constexpr int NT = ROW_NT, MINB = ((G1 & (G1 - 1)) == 0 && G1 >= 128 ? 4 : G1 <= 64 || G1 == 768 ? 3 : 2);
+  static constexpr int NT = ARW_WARPS * 32, MINB = (G1 <= 256 ? 8 : G1 <= 512 ? 6 : 4);
   static constexpr const char* FAMILY = "adj_rows";
   static __device__ __forceinline__ void run(const VBlock& vb, const float2* __restrict__ Tb,
       const float2* __restrict__ maps, const float* __restrict__ rowfac, const float* __restrict__ coldeap,
       float2* __restrict__ x, const float2* __restrict__ tw, const Geo2& g, float scale) {
-    constexpr int ROWS = rows_per_block(G1);
     constexpr int LD = row_ld(G1);
     extern __shared__ float2 sm[];
     if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
-    float2* acc = sm + ROWS * LD;   // S1 accumulators
+    float2* acc = sm + ARW_WARPS * LD;   // S1 accumulators
+    const int warp = threadIdx.x >> 5;
     const int row = vb.x;
     const int be = row / g.S0;
     const int r = row - be * g.S0;
-    for (int i = threadIdx.x; i < g.S1; i += ROW_NT) acc[i] = make_float2(0.f, 0.f);
-    for (int c0 = 0; c0 < g.C; c0 += ROWS) {
-      const int ncl = min(ROWS, g.C - c0);
-      const float2* tb = Tb + (((long long)be * g.C + c0) * g.S0 + r) * G1;
-      const long long cstride = (long long)g.S0 * G1;
-      auto load0 = [&](int q, int n1) -> float2 {
-        if (q >= ncl) return make_float2(0.f, 0.f);
-        return tb[q * cstride + n1];
-      };
-      auto sstore = [&](int q, int e, float2 v) { sm[q * LD + swz(e)] = v; };
-      fft_stages<G1, 0, ROWS, ROW_NT, +1, false, true, LD>(sm, tw, load0, sstore);
-      for (int i = threadIdx.x; i < g.S1; i += ROW_NT) {
+    float2* buf = sm + warp * LD;
+    for (int i = threadIdx.x; i < g.S1; i += NT) acc[i] = make_float2(0.f, 0.f);
+    for (int c0 = 0; c0 < g.C; c0 += ARW_WARPS) {
+      const int ncl = min(ARW_WARPS, g.C - c0);
+      if (warp < ncl) {
+        const float2* tb = Tb + (((long long)be * g.C + c0 + warp) * g.S0 + r) * G1;
+        auto load0 = [&](int, int n1) -> float2 { return tb[n1]; };
+        auto sstore = [&](int, int e, float2 v) { buf[swz(e)] = v; };
+        fft_stages<G1, 0, 1, 32, +1, false, true, LD, true>(buf, tw, load0, sstore);
+      }
+      __syncthreads();
+      for (int i = threadIdx.x; i < g.S1; i += NT) {
         float2 s = acc[i];
         const int e = i + g.off1;
         const int pe = swz(e);
@@ -730,7 +734,7 @@ struct AdjRows {
       }
       __syncthreads();
     }
-    for (int i = threadIdx.x; i < g.S1; i += ROW_NT) {
+    for (int i = threadIdx.x; i < g.S1; i += NT) {
       float d = __fmul_rn(__fmul_rn(scale, __ldg(rowfac + r)), __ldg(coldeap + i));
       if ((i + g.off1) & 1) d = -d;
       const float2 s = acc[i];
@@ -739,7 +743,7 @@ struct AdjRows {
   }
 };
 template <int G1>
-__global__ void __launch_bounds__(ROW_NT) adj_rows_kernel(const float2* __restrict__ Tb,
+__global__ void __launch_bounds__(AdjRows<G1>::NT, AdjRows<G1>::MINB) adj_rows_kernel(const float2* __restrict__ Tb,
     const float2* __restrict__ maps, const float* __restrict__ rowfac, const float* __restrict__ coldeap,
     float2* __restrict__ x, const float2* __restrict__ tw, Geo2 g, float scale) {
   AdjRows<G1>::run(hw_block(), Tb, maps, rowfac, coldeap, x, tw, g, scale);
@@ -863,8 +867,7 @@ template <int G1>
 int launch_adj_rows(const float2* Tb, const float2* maps, const float* rowfac, const float* coldeap, void* x,
                     const float2* tw,
                     const Geo2& g, int nb, float scale, cudaStream_t st) {
-  constexpr int ROWS = rows_per_block(G1);
-  const size_t smem = ((size_t)ROWS * row_ld(G1) + g.S1) * sizeof(float2);
+  const size_t smem = ((size_t)ARW_WARPS * row_ld(G1) + g.S1) * sizeof(float2);
   int rc;
   if ((rc = set_smem((const void*)adj_rows_kernel<G1>, smem))) return rc;
   const long long blocks = (long long)nb * g.S0;
