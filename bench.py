@@ -552,7 +552,8 @@ def batched_throughput(dev, steps=3):
     same = all(torch.equal(x, s.result()) for x, s in zip(bs.results(), seq))
     same_r = all(torch.equal(x, s.result()) for x, s in zip(br.results(), seq))
     return {"workload": BATCHED["name"], "batched_graph_s": t_b, "sequential_s": t_s, "speedup": t_s / t_b,
-            "mode": "grouped launches (one per kernel step and kernel shape, all instances), one CUDA graph",
+            "mode": "grouped launches (one per kernel step over the instances of an image shape; shapes on their own "
+                    "streams), one CUDA graph",
             "gpu_launches_per_batch": launches, "identical_to_sequential": bool(same),
             "branch_graph_s": t_r, "branch_gpu_launches_per_batch": launches_r,
             "branch_identical_to_sequential": bool(same_r),

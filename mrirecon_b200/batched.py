@@ -16,8 +16,11 @@ reduction, inverse passes, TV energies and gradient, Armijo, controller,
 update, restart) is ONE launch over all instances, whose blocks find their
 instance and its arguments in a table in kernel parameter space.  Instances
 that differ in a kernel's compile-time shape (the FFT length of their size
-class, the spread tile and variant) take one launch per shape.
-`iters_per_graph` iterations of these launches are captured in one CUDA graph.
+class, the spread tile and variant) take one launch per shape.  With
+split_by_shape (the default) the instances of one image shape form a partition
+recorded on its own and replayed on its own stream, so that size classes do
+not wait for one another at every kernel step.  `iters_per_graph` iterations
+of these launches are captured in one CUDA graph.
 
 Branch mode (grouped=False): the graph forks from the capture stream to one
 stream per instance and joins back; every instance issues its own launches.
@@ -43,7 +46,7 @@ class BatchedSolver:
     """Solve `problems` = [(y, op, regm), ...] with one CGConfig, all in one graph."""
 
     def __init__(self, problems: Sequence[Tuple[torch.Tensor, object, object]], cfg: Optional[CGConfig] = None,
-                 grouped: bool = True):
+                 grouped: bool = True, split_by_shape: bool = True):
         if len(problems) == 0:
             raise ValueError("no problems")
         self.cfg = cfg or CGConfig()
@@ -61,6 +64,16 @@ class BatchedSolver:
         self.grouped = bool(grouped)
         self.lib = _lib.load()
         self.streams = [torch.cuda.Stream(self.device) for _ in self.solvers]
+        # grouped mode: instances of one image shape (one FFT size class) form a
+        # partition whose grouped launches run on a stream of their own, so that
+        # size classes do not wait for one another at every kernel step
+        shapes: dict = {}
+        for i, s in enumerate(self.solvers):
+            key = tuple(s.x.shape) if split_by_shape else ()
+            shapes.setdefault(key, []).append(i)
+        self.partitions: List[List[int]] = list(shapes.values())
+        self._stats = [0, 0]
+        self.part_streams = [torch.cuda.Stream(self.device) for _ in self.partitions]
         self._graph = None
         self._done = torch.zeros(len(self.solvers), dtype=torch.float64, device=self.device)
         self.launch_stats = {"eager": 0, "per_graph": 0, "replays": 0}
@@ -80,18 +93,32 @@ class BatchedSolver:
             main.wait_stream(st)
 
     def _record(self, fn):
-        """fn(s) for every instance inside one recording; the recorded kernel
-        launches are issued as grouped launches on the current stream."""
+        """fn(s) for every instance, one recording per partition; each partition's
+        recorded kernel launches are issued as grouped launches on its own stream,
+        forked from and joined to the current stream."""
         lib = self.lib
-        _lib.check(lib.mrb_group_begin(len(self.solvers)), "group_begin")
-        try:
-            for i, s in enumerate(self.solvers):
-                _lib.check(lib.mrb_group_select(i), "group_select")
-                fn(s)
-        except BaseException:
-            lib.mrb_group_cancel()
-            raise
-        _lib.check(lib.mrb_group_end(_lib.stream_ptr(self.device)), "group_end")
+        main = torch.cuda.current_stream(self.device)
+        one = len(self.partitions) == 1
+        self._stats = [0, 0]
+        for part, st in zip(self.partitions, self.part_streams):
+            if not one:
+                st.wait_stream(main)
+            _lib.check(lib.mrb_group_begin(len(part)), "group_begin")
+            try:
+                for k, i in enumerate(part):
+                    _lib.check(lib.mrb_group_select(k), "group_select")
+                    fn(self.solvers[i])
+            except BaseException:
+                lib.mrb_group_cancel()
+                raise
+            _lib.check(lib.mrb_group_end(_lib.stream_ptr(self.device) if one else st.cuda_stream), "group_end")
+            r, l = ct.c_int64(0), ct.c_int64(0)
+            _lib.check(lib.mrb_group_stats(ct.byref(r), ct.byref(l)), "group_stats")
+            self._stats[0] += int(r.value)
+            self._stats[1] += int(l.value)
+        if not one:
+            for st in self.part_streams:
+                main.wait_stream(st)
 
     def _step(self, fn):
         """fn(s) for every instance: grouped launches or one stream per instance."""
@@ -101,10 +128,8 @@ class BatchedSolver:
             self._fork(fn)
 
     def group_stats(self) -> Tuple[int, int]:
-        """(records, launches) of the last grouped step."""
-        r, l = ct.c_int64(0), ct.c_int64(0)
-        _lib.check(self.lib.mrb_group_stats(ct.byref(r), ct.byref(l)), "group_stats")
-        return int(r.value), int(l.value)
+        """(records, launches) of the last grouped step, summed over the partitions."""
+        return tuple(getattr(self, "_stats", (0, 0)))
 
     def _all_done(self) -> bool:
         torch.stack([s.s[S_DONE] for s in self.solvers], out=self._done)
