@@ -1517,7 +1517,13 @@ __global__ void __launch_bounds__(S3_WARPS * 32) spread3_kernel(SpreadArgs a, Ge
         if (n & 1) w = -w;
         sw[j * 12 + d * 4 + t] = w * ws;
       }
-      reinterpret_cast<int*>(sb + j)[d] = base;
+      // tile-relative first node, modulo G in [-3, G - 4] (grid sides >= T + 3):
+      // tap t of the sample lies at local index rel + t, or outside the tile
+      const int od = d == 0 ? o0 : d == 1 ? o1 : o2;
+      int rel = base - od;
+      rel += rel < -3 ? g.G[d] : 0;
+      rel -= rel > g.G[d] - 4 ? g.G[d] : 0;
+      reinterpret_cast<int*>(sb + j)[d] = rel;
     }
     for (int i = threadIdx.x; i < S3_BATCH * CPS; i += blockDim.x) {
       const int j = i % S3_BATCH, c = i / S3_BATCH;   // lanes along the sample list
@@ -1532,22 +1538,15 @@ __global__ void __launch_bounds__(S3_WARPS * 32) spread3_kernel(SpreadArgs a, Ge
     // visits only the samples whose support meets it
     for (int h = 0; h < nbat; h += 32) {
     int myd0 = 4;
-    if (h + lane < nbat) {
-      myd0 = P0 - sb[h + lane].x;
-      myd0 += myd0 < 0 ? g.G[0] : 0;
-      myd0 -= myd0 >= g.G[0] ? g.G[0] : 0;
-    }
-    unsigned todo = __ballot_sync(0xffffffffu, myd0 < 4);
+    if (h + lane < nbat) myd0 = warp - sb[h + lane].x;   // tap a0 on this plane
+    unsigned todo = __ballot_sync(0xffffffffu, (unsigned)myd0 < 4u);
     while (todo) {
       const int jl = __ffs(todo) - 1;
       todo &= todo - 1;
       const int j = h + jl;
       const int4 bb = sb[j];
       const int d0 = __shfl_sync(0xffffffffu, myd0, jl);
-      int n2 = bb.z + a2;
-      n2 += n2 < 0 ? g.G[2] : 0;
-      n2 -= n2 >= g.G[2] ? g.G[2] : 0;
-      const int l2 = n2 - o2;
+      const int l2 = bb.z + a2;   // below 0 only outside the tile
       const bool in2 = (unsigned)l2 < (unsigned)T && p < (nc + 1) / 2;
       const float* wj = sw + j * 12;
       const float w0 = wj[d0], w2 = wj[8 + a2];
@@ -1555,10 +1554,7 @@ __global__ void __launch_bounds__(S3_WARPS * 32) spread3_kernel(SpreadArgs a, Ge
 #pragma unroll
       for (int r = 0; r < 4 / ROWS; ++r) {
         const int a1 = r * ROWS + arow;
-        int n1 = bb.y + a1;
-        n1 += n1 < 0 ? g.G[1] : 0;
-        n1 -= n1 >= g.G[1] ? g.G[1] : 0;
-        const int l1 = n1 - o1;
+        const int l1 = bb.y + a1;
         if (in2 && (unsigned)l1 < (unsigned)T) {
           const float w = w0 * wj[4 + a1] * w2;   // the per-warp kernel's product order
           float4* c4 = acc4 + ((warp * T + l1) * T + l2) * PPL + p;
@@ -2854,7 +2850,9 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     a.twords = p->twords;
     a.grid = adj_grid(p);
     const bool blk3t = p->spread_kernel == 2 && p->nd == 3 && tg.T == S3_T;  // shared-staging 3D kernel
-    const bool blk3 = (p->spread_kernel == 1 || blk3t) && p->nd == 3 && tg.T == S3_T;   // block-per-tile kernels
+    // block-per-tile kernels (the plain block kernel stages tile-relative bases: grid sides >= T + 3)
+    const bool blk3 = (p->spread_kernel == 1 || blk3t) && p->nd == 3 && tg.T == S3_T &&
+                      (blk3t || (p->G[0] >= S3_T + 3 && p->G[1] >= S3_T + 3 && p->G[2] >= S3_T + 3));
     const bool blk2 = p->spread_kernel == 1 && p->nd == 2 && tg.T == S2_T;
     a.cpi = blk3 || blk2 ? std::min(std::min(p->C, S3_CPB), p->coils_per_item) : p->coils_per_item;
     a.ngroups = (p->C + a.cpi - 1) / a.cpi;
