@@ -1150,7 +1150,9 @@ struct SpreadWarp {
     // pair along the last dim, coil pair); two 128-bit shared loads, one 128-bit
     // global store per coil
     for (int i = lane; i < PAIRS * npair; i += 32) {
-      const int pr = i % npair, r = i / npair;
+      // (cell pair, coil pair) of the task: shifts for 1 or 2 coil pairs (up to 4 coils per item)
+      const int pr = npair == 2 ? (i & 1) : npair == 1 ? 0 : i % npair;
+      const int r = npair == 2 ? (i >> 1) : npair == 1 ? i : i / npair;
       const int l = (r % (T / 2)) * 2;
       const int rr = r / (T / 2);
       const int cl0 = rr * T + l;
