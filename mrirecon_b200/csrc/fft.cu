@@ -31,6 +31,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <vector>
 
@@ -303,7 +304,12 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load
       else Dft<R, DIR>::run(v[c]);
       const int j = (i - k) * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) store(q, j + r * P, v[c][r]);
+      for (int r = 0; r < R; ++r) {
+        // a store that takes (q, j, r P) gets the element j + r P with its
+        // thread-dependent part j apart from the compile-time offset r P
+        if constexpr (std::is_invocable_v<ST, int, int, int, float2>) store(q, j, r * P, v[c][r]);
+        else store(q, j + r * P, v[c][r]);
+      }
     }
   }
   stage_sync<WARP>();
@@ -394,8 +400,14 @@ __global__ void __launch_bounds__(ROW_NT, FwdRows<G1>::MINB) fwd_rows_kernel(con
 }
 
 // forward column pass: grid[vol][:][k1] = FFT_G0(band rows of T[vol][:][k1]),
-// COLS consecutive columns per block
-template <int G0>
+// COLS consecutive columns per block.  BLK: the grid is stored in blocks of
+// 2 x 8 cells (fft.cuh: cell (n0, n1) of a volume at
+// ((n0 / 2) * (G1 / 8) + n1 / 8) * 16 + (n0 % 2) * 8 + n1 % 8, G0 even, G1 a
+// multiple of 8), the 2D interp's layout: a sample's 4 x 4 taps then meet 2
+// to 6 128-byte lines instead of 4 to 8.  The last stage's stores of a warp
+// cover rows 2m and 2m + 1 of 16 columns: whole blocks, as whole rows' lines
+// in the row-major layout.
+template <int G0, bool BLK = false>
 struct FwdCols {
   static constexpr int NT = COL_NT, MINB = (G0 <= 256 ? 3 : 2);
   static constexpr const char* FAMILY = "fwd_cols";
@@ -418,22 +430,41 @@ struct FwdCols {
       if ((unsigned)r >= (unsigned)g.S0 || (!full && k0 + q >= G1)) return make_float2(0.f, 0.f);
       return tv[r * G1 + q];
     };
+    // BLK: 4 x 4 cell blocks; a thread's column k0 + q is fixed, its rows n0 = j + r P
+    // share n0 % 4 (P is a multiple of 4), so the address is a per-thread base plus
+    // a multiple of 4 G1 per r
+    float2* gb = grid + (long long)vol * g.gtot + ((k0 >> 3) << 4);
     auto store = [&](int q, int n0, float2 v) {
       if (full || k0 + q < G1) gv[n0 * G1 + q] = v;
     };
-    if constexpr (radix_at(G0, 0) == 8) {
-      if (centred_half<G0>(g.S0, g.off0)) {
-        fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD, false, true>(sm, tw, load0, store);
-        return;
+    // row n0 = j + rP of the last stage (P even): block row j / 2 + rP / 2, row in block j % 2
+    auto store_blk = [&](int q, int j, int rP, float2 v) {
+      if (full || k0 + q < G1) {
+        const int c = (k0 & 7) + q;   // column k0 + q = 8 (k0 / 8) + c
+        gb[((j >> 1) + (rP >> 1)) * (2 * G1) + (j & 1) * 8 + ((c >> 3) << 4) + (c & 7)] = v;
       }
+    };
+    auto go = [&](auto st) {
+      if constexpr (radix_at(G0, 0) == 8) {
+        if (centred_half<G0>(g.S0, g.off0)) {
+          fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD, false, true>(sm, tw, load0, st);
+          return;
+        }
+      }
+      fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, st);
+    };
+    if constexpr (BLK) {
+      static_assert(span_at(G0, n_stages(G0) - 1) % 2 == 0, "the last stage's span must be even");
+      go(store_blk);
+    } else {
+      go(store);
     }
-    fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
   }
 };
-template <int G0>
+template <int G0, bool BLK>
 __global__ void __launch_bounds__(COL_NT) fwd_cols_kernel(const float2* __restrict__ Tb,
     float2* __restrict__ grid, const float2* __restrict__ tw, Geo2 g) {
-  FwdCols<G0>::run(hw_block(), Tb, grid, tw, g);
+  FwdCols<G0, BLK>::run(hw_block(), Tb, grid, tw, g);
 }
 
 // forward column pass with a coil-interleaved output (3D x pass, see fft.cuh):
@@ -788,15 +819,22 @@ int launch_fwd_rows(const void* x, const float2* maps, const float* rowfac, cons
 }
 
 template <int G0>
-int launch_cols(bool forward, const float2* in, float2* out, const float2* tw, const Geo2& g, int nb, cudaStream_t st) {
+int launch_cols(bool forward, const float2* in, float2* out, const float2* tw, const Geo2& g, int nb, bool blocked,
+                cudaStream_t st) {
   constexpr int COLS = cols_per_block(G0);
   const size_t smem = (size_t)COLS * (G0 | 1) * sizeof(float2);
   const long long blocks = (long long)nb * g.C * ((g.G1 + COLS - 1) / COLS);
   MRB_REQUIRE(blocks < (1LL << 31), "too many columns");
   int rc;
+  if (forward && blocked) {
+    MRB_REQUIRE(G0 % 2 == 0 && g.G1 % 8 == 0, "2 x 8 cell blocks need G0 even and G1 divisible by 8");
+    if ((rc = set_smem((const void*)fwd_cols_kernel<G0, true>, smem))) return rc;
+    return mrb::launch<FwdCols<G0, true>>(fwd_cols_kernel<G0, true>, dim3((unsigned)blocks), smem, st, in, out, tw,
+                                          g);
+  }
   if (forward) {
-    if ((rc = set_smem((const void*)fwd_cols_kernel<G0>, smem))) return rc;
-    return mrb::launch<FwdCols<G0>>(fwd_cols_kernel<G0>, dim3((unsigned)blocks), smem, st, in, out, tw, g);
+    if ((rc = set_smem((const void*)fwd_cols_kernel<G0, false>, smem))) return rc;
+    return mrb::launch<FwdCols<G0>>(fwd_cols_kernel<G0, false>, dim3((unsigned)blocks), smem, st, in, out, tw, g);
   }
   if ((rc = set_smem((const void*)adj_cols_kernel<G0>, smem))) return rc;
   return mrb::launch<AdjCols<G0>>(adj_cols_kernel<G0>, dim3((unsigned)blocks), smem, st, in, out, tw, g);
@@ -911,11 +949,11 @@ int fft2_forward_rows(const void* x, const float2* maps, const float* rowfac, co
 }
 
 int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, int S0, int S1, int G0, int G1, int C,
-                 int nb, const double* skip, cudaStream_t st) {
+                 int nb, const double* skip, cudaStream_t st, int blocked) {
   const Geo2 g = make_geo2(S0, S1, G0, G1, C, skip);
   switch (G0) {
 #define MRB_CASE(n) \
-  case n: return launch_cols<n>(forward != 0, in, out, tw0, g, nb, st);
+  case n: return launch_cols<n>(forward != 0, in, out, tw0, g, nb, blocked != 0, st);
     MRB_FFT_LENGTHS(MRB_CASE)
 #undef MRB_CASE
     default:

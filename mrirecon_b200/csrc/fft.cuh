@@ -26,9 +26,12 @@ int fft2_forward_rows(const void* x, const float2* maps, const float* rowfac, co
                       const float2* tw1, int S0,
                       int S1, int G0, int G1, int C, int nb, int coil_images, const double* skip,
                       cudaStream_t st);
-// forward != 0: T -> grid (nb, C, G0, G1); else grid -> T
+// forward != 0: T -> grid (nb, C, G0, G1); else grid -> T.  blocked (forward
+// only): each coil-frame's grid in blocks of 2 x 8 cells, cell (n0, n1) at
+// ((n0 / 2) * (G1 / 8) + n1 / 8) * 16 + (n0 % 2) * 8 + n1 % 8 (the 2D interp's
+// layout; G0 even, G1 a multiple of 8)
 int fft2_columns(int forward, const float2* in, float2* out, const float2* tw0, int S0, int S1, int G0, int G1, int C,
-                 int nb, const double* skip, cudaStream_t st);
+                 int nb, const double* skip, cudaStream_t st, int blocked = 0);
 // Forward column pass whose output is coil-interleaved: in (nb, C, S0, G1)
 // band rows -> out (nb, G0 * G1 cells, C), for C in {8, 16, 32} (the 3D x pass
 // writing the interp's (cell, coil) grid copy directly)

@@ -54,6 +54,7 @@ struct mrb_plan {
   int spread_kernel = 1;   // 1: block-per-tile kernels (2D tile 16, 3D tile 8) where they apply (3D default)
   int grid_mask = 1;       // fused FFT mode: the spread stores only cell pairs inside some support
   int col_interp = 0;      // fused 2D mode: forward column pass and interp in one kernel (option key 8)
+  int grid_blk = 1;        // fused 2D mode: the forward grid in 2 x 8 cell blocks (option key 9)
   DevBuf strip_start;      // (B * nstrips + 1) per-frame lists of the samples starting in each column strip
   DevBuf strip_entries;    // (B * K) sample indices
   int nstrips = 0;
@@ -418,6 +419,7 @@ struct InterpArgs {
   float gsign;
   const int* seg;      // 3D interleaved interp: segment visiting order (B, nseg) or null
   long long nseg;
+  int blk;             // 2D pair-parallel interp: the grid is in 2 x 8 cell blocks (fwd_cols_kernel<G0, true>)
 };
 
 template <int ND>
@@ -573,6 +575,14 @@ struct Interp2p {
         nidx[d][o] = mrb::wrap_i(n, g.G[d]);
       }
     }
+    // offsets of the tap rows and columns: row-major, or 2 x 8 cell blocks
+    int roff[W], coff[W];
+  #pragma unroll
+    for (int o = 0; o < W; ++o) {
+      const int n0 = nidx[0][o], n1 = nidx[1][o];
+      roff[o] = a.blk ? (n0 >> 1) * (2 * g.G[1]) + (n0 & 1) * 8 : n0 * g.G[1];
+      coff[o] = a.blk ? ((n1 >> 3) << 4) + (n1 & 7) : n1;
+    }
     float s = a.scale * a.gsign;
     if (a.wfwd) s *= a.wfwd[(long long)b * g.K + k];
     const int c = 2 * pr;
@@ -582,11 +592,10 @@ struct Interp2p {
     float2 v0[W][W], v1[W][W];
   #pragma unroll
     for (int i0 = 0; i0 < W; ++i0) {
-      const int roff = nidx[0][i0] * g.G[1];
   #pragma unroll
       for (int i1 = 0; i1 < W; ++i1) {
-        v0[i0][i1] = __ldg(g0 + roff + nidx[1][i1]);
-        v1[i0][i1] = two ? __ldg(g1 + roff + nidx[1][i1]) : make_float2(0.f, 0.f);
+        v0[i0][i1] = __ldg(g0 + roff[i0] + coff[i1]);
+        v1[i0][i1] = two ? __ldg(g1 + roff[i0] + coff[i1]) : make_float2(0.f, 0.f);
       }
     }
     float r0 = 0.f, m0 = 0.f, r1 = 0.f, m1 = 0.f;
@@ -1073,17 +1082,23 @@ struct SpreadWarp {
       if (e + SB < e1) fetch(e + SB, min(SB, e1 - e - SB));
       if (ND == 2 && ntask <= 32) {
         // one task per lane (coil groups of up to 4 coils): the task's coil pair and
-        // tap are fixed for the whole batch; same cells, weights and order as below
+        // tap are fixed for the whole batch; same cells, weights and order as below.
+        // A tap at local index r + t < 0 wraps to G + r + t >= G - 3, inside the
+        // tile only on grids narrower than T + 3: the wrap is skipped on the others.
         const bool act = lane < ntask;
         const int pr = npair == 2 ? (lane & 1) : lane % npair;
         const int tap = npair == 2 ? (lane >> 1) : lane / npair;
         const int ox = tap >> 2, oy = tap & 3;
         float4* accp = reinterpret_cast<float4*>(acc) + pr;
+        auto visit = [&](auto wrap_t) {
+        constexpr bool WRAP = decltype(wrap_t)::value;
         for (int j = 0; j < nbat; ++j) {
           const Base bb = sb[j];
           int lx = bb.x + ox, ly = bb.y + oy;
-          lx += lx < 0 ? g.G[0] : 0;
-          ly += ly < 0 ? g.G[1] : 0;
+          if (WRAP) {
+            lx += lx < 0 ? g.G[0] : 0;
+            ly += ly < 0 ? g.G[1] : 0;
+          }
           if (act && (unsigned)lx < (unsigned)T && (unsigned)ly < (unsigned)T) {
             const float* wj = sw + j * NW;
             const float w = wj[ox] * wj[4 + oy];
@@ -1098,6 +1113,9 @@ struct SpreadWarp {
           }
           __syncwarp();
         }
+        };
+        if (g.G[0] < T + 3 || g.G[1] < T + 3) visit(std::true_type{});
+        else visit(std::false_type{});
         continue;
       }
       for (int j = 0; j < nbat; ++j) {
@@ -2313,6 +2331,10 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
       MRB_REQUIRE(value == 0 || value == 1, "interleaved interp must be 0 or 1");
       p->il = (int)value;
       return 0;
+    case 9:
+      MRB_REQUIRE(value == 0 || value == 1, "blocked forward grid must be 0 or 1");
+      p->grid_blk = (int)value;
+      return 0;
     default:
       return mrb::fail(MRB_EINVAL, "unknown option %d", key);
   }
@@ -2620,6 +2642,15 @@ static bool il2_active(const mrb_plan* p) {
   return p->fft_mode == 1 && p->nd == 2 && p->il == 1 && p->C % 4 == 0 && p->C <= 512 && !col_interp_active(p);
 }
 
+// fused 2D mode with the pair-parallel interp on a planar-coil grid: the
+// forward column pass stores each coil-frame's grid in blocks of 2 x 8 cells
+// (one 128-byte line each), where a sample's 4 x 4 taps meet 2 to 6 lines
+// instead of 4 to 8 lines of 16 cells of a row
+static bool grid_blocked(const mrb_plan* p) {
+  return p->fft_mode == 1 && p->nd == 2 && p->grid_blk == 1 && p->interp_mode == 1 && !il2_active(p) &&
+         !col_interp_active(p) && p->G[0] % 2 == 0 && p->G[1] % 8 == 0;
+}
+
 // the spread writes only touched cell pairs into a grid of its own (fused FFT mode)
 static bool spread_masked(const mrb_plan* p) {
   return p->fft_mode == 1 && p->grid_mask == 1 && p->touch.p != nullptr && p->adj_zero;
@@ -2737,7 +2768,7 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
                                   p->G[1], p->C, nb, p->skip, st);
     if (stage == 1)
       return mrb::fft2_columns(1, p->band.as<float2>(), p->grid.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
-                               p->G[1], p->C, nb, p->skip, st);
+                               p->G[1], p->C, nb, p->skip, st, grid_blocked(p) ? 1 : 0);
     if (stage == 4)
       return mrb::fft2_columns(0, adj_grid(p), p->band.as<float2>(), p->tw0p, p->S[0], p->S[1], p->G[0],
                                p->G[1], p->C, nb, p->skip, st);
@@ -2810,6 +2841,7 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
       return mrb::launch<Interp2Quad>(interp2_il_kernel, dim3((unsigned)nbx, nb), 0, st, a, g, p->kb);
     }
     if (p->nd == 2 && p->interp_mode == 1) {
+      a.blk = grid_blocked(p) ? 1 : 0;
       const long long nbx = (long long)grid_blocks(p->K, 256) * ((p->C + 1) / 2);
       MRB_REQUIRE(nbx < (1LL << 31) && nb <= 65535, "too many samples for the interp");
       return mrb::launch<Interp2p>(interp2p_kernel, dim3((unsigned)nbx, nb), 0, st, a, g, p->kb);

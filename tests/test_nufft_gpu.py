@@ -408,6 +408,28 @@ def test_2d_pair_parallel_interp_identical(cuda, C, nb, B):
         assert torch.equal(ad.A(x), y1)
 
 
+@pytest.mark.parametrize("S,C,nb,B", [((40, 48), 12, 2, 2), ((40, 48), 5, 3, 1), ((320, 160), 3, 1, 1),
+                                      ((48, 40), 1, 4, 2), ((384, 40), 2, 2, 2)])
+def test_2d_blocked_grid_identical(cuda, S, C, nb, B):
+    """Fused 2D mode: the forward column pass storing each coil-frame's grid in
+    2 x 8 cell blocks (option key 9 = 1, the default) and the pair-parallel
+    interp reading it give the samples of the row-major grid bit for bit
+    (grid sides 80 ... 768; column blocks of 16, 12 and 10 columns, the last
+    two starting off an 8-column boundary)."""
+    maps = _rand_c((C,) + S, 77, torch.complex64)
+    traj = phantoms.random_traj(B, 2, 1000, seed=78)
+    x = _rand_c((nb, 1) + S, 79, torch.complex64).to(cuda)
+    ad = _adapter(maps, traj)
+    assert ad.plan.info()["fft_mode"] == 1
+    y1 = ad.A(x)
+    ad.plan.set_option(9, 0)
+    y0 = ad.A(x)
+    assert torch.equal(y0, y1)
+    ad.plan.set_option(9, 1)
+    assert torch.equal(ad.A(x), y1)
+    assert torch.equal(ad.AH(y1), ad.AH(y0))
+
+
 @pytest.mark.parametrize("S,C,nb,B", [((40, 48), 12, 2, 2), ((40, 48), 8, 3, 1), ((32, 32), 16, 1, 1),
                                       ((48, 40), 4, 4, 2), ((320, 160), 4, 1, 1), ((40, 48), 5, 2, 1)])
 def test_2d_interleaved_grid_interp_identical(cuda, S, C, nb, B):
