@@ -885,10 +885,14 @@ struct SpreadArgs {
   long long twords;
 };
 
-// a tile's cell pair (cell, cell + 1; cell even) holds a touched cell, or no bitmap is in use
+// a tile's cell pair (cell, cell + 1; cell even) is stored: no bitmap is in use, or
+// the aligned group of 4 cells around it (one 32-byte sector of a coil row, both
+// pairs in the same tile) holds a touched cell.  The pair's cells that no support
+// reaches hold zeros, so the sector is written whole (no partial-sector write
+// for the memory to merge) and the grid stays the same.
 __device__ __forceinline__ bool pair_touched(const SpreadArgs& a, int b, long long cell) {
   if (a.touch == nullptr) return true;
-  return (__ldg(a.touch + (long long)b * a.twords + (cell >> 5)) >> (cell & 31)) & 3u;
+  return (__ldg(a.touch + (long long)b * a.twords + (cell >> 5)) >> (cell & 28)) & 15u;
 }
 
 constexpr int SPREAD_WARPS = 4;
@@ -1416,7 +1420,7 @@ struct Spread2Taps {
       const float4 a1 = reinterpret_cast<const float4*>(acc + (cl0 + 1) * cps)[pr];
       const int n0 = o0 + rr, n1 = o1 + l;
       const long long cell = (long long)n0 * G1 + n1;
-      const bool ok = n0 < G0 && n1 < G1 && (pout || !a.touch || ((tbits[rr] >> l) & 3u));
+      const bool ok = n0 < G0 && n1 < G1 && (pout || !a.touch || ((tbits[rr] >> (l & ~3)) & 15u));
   #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int cl = 2 * pr + h;
