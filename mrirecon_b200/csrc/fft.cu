@@ -121,8 +121,8 @@ std::vector<float2> host_twiddles(int G) {
 // small DFTs: X_k = sum_n u_n e^{DIR 2 pi i k n / R}, in place
 //
 // Every floating-point operation of the passes is written with its rounding
-// stated (fmaf, __fmul_rn, __fadd_rn, __fsub_rn; the file also compiles with
-// -fmad=false), so the compiler fuses no multiply into an add on its own: a
+// stated (fmaf, __fmul_rn, __fadd_rn, __fsub_rn and their packed pair forms;
+// the file also compiles with -fmad=false), so the compiler fuses no multiply into an add on its own: a
 // pass computes the same bits in every kernel that contains it (the named
 // kernels and their grouped forms).  The butterflies fuse by hand where a
 // scaled term is added (e +- h p).
@@ -141,39 +141,66 @@ template <int DIR>
 __device__ __forceinline__ float2 cmul_di(float2 a) {   // a * (DIR i)
   return DIR > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
 }
+// PK: the same sums, differences and scaled sums as packed pair instructions
+// (sm_100 __fadd2_rn / __ffma2_rn, each component rounded as the scalar form; a - b
+// as fma(b, -1, a), whose product is exact): the same bits in half the issue
+// slots.  Only the inverse row pass uses them (measured 4.5% faster there; the
+// column passes ran 1-4% slower with them).
+template <bool PK>
+__device__ __forceinline__ float2 padd(float2 a, float2 b) {
+  if constexpr (PK) return __fadd2_rn(a, b);
+  else return cadd(a, b);
+}
+template <bool PK>
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+  if constexpr (PK) return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+  else return csub(a, b);
+}
+// a + h b, h real: one fused multiply-add per component
+template <bool PK>
+__device__ __forceinline__ float2 paxpy(float h, float2 b, float2 a) {
+  if constexpr (PK) return __ffma2_rn(make_float2(h, h), b, a);
+  else return make_float2(fmaf(h, b.x, a.x), fmaf(h, b.y, a.y));
+}
+// a + DIR i b, scalar (the sign of the exchanged component folds into the add)
+template <int DIR>
+__device__ __forceinline__ float2 cadd_di(float2 a, float2 b) {
+  return DIR > 0 ? make_float2(__fsub_rn(a.x, b.y), __fadd_rn(a.y, b.x))
+                 : make_float2(__fadd_rn(a.x, b.y), __fsub_rn(a.y, b.x));
+}
 
-template <int R, int DIR>
+template <int R, int DIR, bool PK = false>
 struct Dft;
 
-template <int DIR>
-struct Dft<2, DIR> {
+template <int DIR, bool PK>
+struct Dft<2, DIR, PK> {
   __device__ __forceinline__ static void run(float2* u) {
     const float2 a = u[0], b = u[1];
-    u[0] = cadd(a, b);
-    u[1] = csub(a, b);
+    u[0] = padd<PK>(a, b);
+    u[1] = psub<PK>(a, b);
   }
 };
 
-template <int DIR>
-struct Dft<4, DIR> {
+template <int DIR, bool PK>
+struct Dft<4, DIR, PK> {
   __device__ __forceinline__ static void run(float2* u) {
-    const float2 a0 = cadd(u[0], u[2]), a1 = csub(u[0], u[2]);
-    const float2 a2 = cadd(u[1], u[3]), a3 = cmul_di<DIR>(csub(u[1], u[3]));
-    u[0] = cadd(a0, a2);
-    u[2] = csub(a0, a2);
-    u[1] = cadd(a1, a3);
-    u[3] = csub(a1, a3);
+    const float2 a0 = padd<PK>(u[0], u[2]), a1 = psub<PK>(u[0], u[2]);
+    const float2 a2 = padd<PK>(u[1], u[3]), d = psub<PK>(u[1], u[3]);
+    u[0] = padd<PK>(a0, a2);
+    u[2] = psub<PK>(a0, a2);
+    u[1] = cadd_di<DIR>(a1, d);    // a1 + DIR i d
+    u[3] = cadd_di<-DIR>(a1, d);   // a1 - DIR i d
   }
 };
 
-template <int DIR>
-struct Dft<8, DIR> {
+template <int DIR, bool PK>
+struct Dft<8, DIR, PK> {
   // radix-2 split into the 4-point DFTs of the even and odd samples
   __device__ __forceinline__ static void run(float2* u) {
     float2 e[4] = {u[0], u[2], u[4], u[6]};
     float2 o[4] = {u[1], u[3], u[5], u[7]};
-    Dft<4, DIR>::run(e);
-    Dft<4, DIR>::run(o);
+    Dft<4, DIR, PK>::run(e);
+    Dft<4, DIR, PK>::run(o);
     combine(e, o, u);
   }
   // u = (0, 0, u2, u3, u4, u5, 0, 0): the first stage of a transform whose input
@@ -189,8 +216,8 @@ struct Dft<8, DIR> {
   // Dft<4> of (0, b, c, 0): a0 = c, a1 = -c, a2 = b, a3 = DIR i b
   __device__ __forceinline__ static void half4(float2 b, float2 c, float2* x) {
     const float2 a3 = cmul_di<DIR>(b);
-    x[0] = cadd(c, b);
-    x[2] = csub(c, b);
+    x[0] = padd<PK>(c, b);
+    x[2] = psub<PK>(c, b);
     x[1] = make_float2(__fsub_rn(a3.x, c.x), __fsub_rn(a3.y, c.y));
     x[3] = make_float2(-__fadd_rn(c.x, a3.x), -__fadd_rn(c.y, a3.y));
   }
@@ -198,46 +225,46 @@ struct Dft<8, DIR> {
     const float h = 0.707106781186547524f;
     // o_k * e^{DIR i pi k / 4}: o1 = h p1, p1 = o + DIR i o; o3 = h p3, p3 = DIR i o - o;
     // e_k +- h p_k as one fused multiply-add per component
-    const float2 p1 = cadd(o[1], cmul_di<DIR>(o[1]));
-    const float2 o2 = cmul_di<DIR>(o[2]);
-    const float2 p3 = csub(cmul_di<DIR>(o[3]), o[3]);
-    u[0] = cadd(e[0], o[0]);
-    u[4] = csub(e[0], o[0]);
-    u[1] = make_float2(fmaf(h, p1.x, e[1].x), fmaf(h, p1.y, e[1].y));
-    u[5] = make_float2(fmaf(-h, p1.x, e[1].x), fmaf(-h, p1.y, e[1].y));
-    u[2] = cadd(e[2], o2);
-    u[6] = csub(e[2], o2);
-    u[3] = make_float2(fmaf(h, p3.x, e[3].x), fmaf(h, p3.y, e[3].y));
-    u[7] = make_float2(fmaf(-h, p3.x, e[3].x), fmaf(-h, p3.y, e[3].y));
+    const float2 p1 = cadd_di<DIR>(o[1], o[1]);
+    const float2 q3 = cmul_di<DIR>(o[3]);
+    const float2 p3 = make_float2(__fsub_rn(q3.x, o[3].x), __fsub_rn(q3.y, o[3].y));
+    u[0] = padd<PK>(e[0], o[0]);
+    u[4] = psub<PK>(e[0], o[0]);
+    u[1] = paxpy<PK>(h, p1, e[1]);
+    u[5] = paxpy<PK>(-h, p1, e[1]);
+    u[2] = cadd_di<DIR>(e[2], o[2]);    // e2 + DIR i o2
+    u[6] = cadd_di<-DIR>(e[2], o[2]);   // e2 - DIR i o2
+    u[3] = paxpy<PK>(h, p3, e[3]);
+    u[7] = paxpy<PK>(-h, p3, e[3]);
   }
 };
 
-template <int DIR>
-struct Dft<3, DIR> {
+template <int DIR, bool PK>
+struct Dft<3, DIR, PK> {
   __device__ __forceinline__ static void run(float2* u) {
     const float c1 = -0.5f, s1 = 0.866025403784438647f * (float)DIR;
-    const float2 t1 = cadd(u[1], u[2]), t2 = csub(u[1], u[2]);
-    const float2 m = make_float2(fmaf(c1, t1.x, u[0].x), fmaf(c1, t1.y, u[0].y));
+    const float2 t1 = padd<PK>(u[1], u[2]), t2 = psub<PK>(u[1], u[2]);
+    const float2 m = paxpy<PK>(c1, t1, u[0]);
     // m +- r, r = DIR i s1 t2, as fused multiply-adds
-    u[0] = cadd(u[0], t1);
+    u[0] = padd<PK>(u[0], t1);
     u[1] = make_float2(fmaf(-s1, t2.y, m.x), fmaf(s1, t2.x, m.y));
     u[2] = make_float2(fmaf(s1, t2.y, m.x), fmaf(-s1, t2.x, m.y));
   }
 };
 
-template <int DIR>
-struct Dft<5, DIR> {
+template <int DIR, bool PK>
+struct Dft<5, DIR, PK> {
   __device__ __forceinline__ static void run(float2* u) {
     // cos / sin of 2 pi k / 5
     const float c1 = 0.309016994374947424f, c2 = -0.809016994374947424f;
     const float s1 = 0.951056516295153572f * (float)DIR, s2 = 0.587785252292473129f * (float)DIR;
-    const float2 a1 = cadd(u[1], u[4]), b1 = csub(u[1], u[4]);
-    const float2 a2 = cadd(u[2], u[3]), b2 = csub(u[2], u[3]);
+    const float2 a1 = padd<PK>(u[1], u[4]), b1 = psub<PK>(u[1], u[4]);
+    const float2 a2 = padd<PK>(u[2], u[3]), b2 = psub<PK>(u[2], u[3]);
     const float2 x0 = u[0];
-    const float2 m1 = make_float2(fmaf(c2, a2.x, fmaf(c1, a1.x, x0.x)), fmaf(c2, a2.y, fmaf(c1, a1.y, x0.y)));
-    const float2 m2 = make_float2(fmaf(c1, a2.x, fmaf(c2, a1.x, x0.x)), fmaf(c1, a2.y, fmaf(c2, a1.y, x0.y)));
+    const float2 m1 = paxpy<PK>(c2, a2, paxpy<PK>(c1, a1, x0));
+    const float2 m2 = paxpy<PK>(c1, a2, paxpy<PK>(c2, a1, x0));
     // m_k +- n_k with n1 = i (s1 b1 + s2 b2), n2 = i (s2 b1 - s1 b2), as fused multiply-adds
-    u[0] = cadd(x0, cadd(a1, a2));
+    u[0] = padd<PK>(x0, padd<PK>(a1, a2));
     u[1] = make_float2(fmaf(-s2, b2.y, fmaf(-s1, b1.y, m1.x)), fmaf(s2, b2.x, fmaf(s1, b1.x, m1.y)));
     u[4] = make_float2(fmaf(s2, b2.y, fmaf(s1, b1.y, m1.x)), fmaf(-s2, b2.x, fmaf(-s1, b1.x, m1.y)));
     u[2] = make_float2(fmaf(s1, b2.y, fmaf(-s2, b1.y, m2.x)), fmaf(-s1, b2.x, fmaf(s2, b1.x, m2.y)));
@@ -261,7 +288,7 @@ __device__ __forceinline__ void stage_sync() {
 // MID: the first stage of a transform whose nonzero input is the centred half
 // [G/4, 3G/4): with R = 8 and T = G/8 every butterfly's inputs i + r T are
 // zero for r = 0, 1, 6, 7, so only r = 2..5 are loaded (Dft<8>::run_mid).
-template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool WARP, bool MID, class LD, class ST>
+template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool WARP, bool MID, bool PK, class LD, class ST>
 __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load, ST store) {
   constexpr int R = radix_at(G, S);
   constexpr int P = span_at(G, S);
@@ -300,8 +327,8 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load
           v[c][r] = cmul(v[c][r], t);
         }
       }
-      if constexpr (MID) Dft<8, DIR>::run_mid(v[c]);
-      else Dft<R, DIR>::run(v[c]);
+      if constexpr (MID) Dft<8, DIR, PK>::run_mid(v[c]);
+      else Dft<R, DIR, PK>::run(v[c]);
       const int j = (i - k) * R + k;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
@@ -319,18 +346,18 @@ __device__ __forceinline__ void fft_stage(const float2* __restrict__ tw, LD load
 // through load0, the last stores through store_last, and intermediate results
 // live in buf (row q at q * LD, element e at slot swz(e) when PAD).
 template <int G, int S, int ROWS, int NT, int DIR, bool QFAST, bool PAD, int LD, bool WARP = false, bool MID = false,
-          class LD0, class STL>
+          bool PK = false, class LD0, class STL>
 __device__ __forceinline__ void fft_stages(float2* buf, const float2* tw, LD0 load0, STL store_last) {
   constexpr int NS = n_stages(G);
   constexpr bool MID0 = MID && S == 0;
   if constexpr (S < NS) {
     auto sload = [&](int q, int e) { return buf[q * LD + (PAD ? swz(e) : e)]; };
     auto sstore = [&](int q, int e, float2 v) { buf[q * LD + (PAD ? swz(e) : e)] = v; };
-    if constexpr (S == 0 && S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, MID0>(tw, load0, store_last);
-    else if constexpr (S == 0) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, MID0>(tw, load0, sstore);
-    else if constexpr (S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, false>(tw, sload, store_last);
-    else fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, false>(tw, sload, sstore);
-    fft_stages<G, S + 1, ROWS, NT, DIR, QFAST, PAD, LD, WARP, MID>(buf, tw, load0, store_last);
+    if constexpr (S == 0 && S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, MID0, PK>(tw, load0, store_last);
+    else if constexpr (S == 0) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, MID0, PK>(tw, load0, sstore);
+    else if constexpr (S == NS - 1) fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, false, PK>(tw, sload, store_last);
+    else fft_stage<G, S, ROWS, NT, DIR, QFAST, WARP, false, PK>(tw, sload, sstore);
+    fft_stages<G, S + 1, ROWS, NT, DIR, QFAST, PAD, LD, WARP, MID, PK>(buf, tw, load0, store_last);
   }
 }
 
@@ -746,7 +773,7 @@ struct AdjRows {
         const float2* tb = Tb + (((long long)be * g.C + c0 + warp) * g.S0 + r) * G1;
         auto load0 = [&](int, int n1) -> float2 { return tb[n1]; };
         auto sstore = [&](int, int e, float2 v) { buf[swz(e)] = v; };
-        fft_stages<G1, 0, 1, 32, +1, false, true, LD, true>(buf, tw, load0, sstore);
+        fft_stages<G1, 0, 1, 32, +1, false, true, LD, true, false, true>(buf, tw, load0, sstore);
       }
       __syncthreads();
       for (int i = threadIdx.x; i < g.S1; i += NT) {

@@ -68,6 +68,8 @@ struct mrb_plan {
   bool have_points = false;
   bool have_maps = false;
   DevBuf gx;          // (B, nd, K) float
+  DevBuf tapw;        // 2D: (B, K, 2) float4, the signed kernel weights of each sample's 4 nodes per dim
+  DevBuf tapb;        // 2D: (B, K) int2, each sample's first node floor(x) - 1 per dim
   DevBuf entries;     // (n_entries) int32 sample index, sorted by (frame, tile)
   DevBuf tile_start;  // (B * ntiles + 1) int32
   DevBuf items;      // spread work items int4 (key, chunk, partial slot or -1, chunks of key), heaviest first
@@ -169,6 +171,37 @@ __global__ void coords_kernel(const float* __restrict__ traj, float* __restrict_
   if (i >= n) return;
   int d = (int)((i / g.K) % g.nd);
   gx[i] = mrb::ref_grid_coord(traj[i], g.Gf[d], g.gmax[d]);
+}
+
+// Per-sample tap table (2D, built with the coordinates): the first node
+// floor(x) - 1 and the weights of the 4 nodes n along each dim, with the
+// sample-side sign (-1)^n.  The trajectory is fixed across the operator calls
+// of a solve, so the default spread and interp read 40 bytes per sample
+// instead of evaluating 8 kernel polynomials (the interp once per coil pair).
+// Same fx = x - floor(x), polynomials and sign as the inline evaluation: the
+// same weights bit for bit.
+__global__ void taps2_kernel(const float* __restrict__ gx, float4* __restrict__ tapw, int2* __restrict__ tapb,
+                             Geo g, KBPoly kb) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;   // b * K + k
+  if (i >= (long long)g.B * g.K) return;
+  const long long b = i / g.K, k = i - b * g.K;
+  int base[2];
+  float w[2][4];
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    const float x = gx[(b * 2 + d) * g.K + k];
+    const int fb = (int)floorf(x);
+    const float fx = x - (float)fb;
+    base[d] = fb - 1;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float wd = mrb::kb_tap(kb, q, fx);
+      w[d][q] = ((base[d] + q) & 1) ? -wd : wd;
+    }
+  }
+  tapw[2 * i] = make_float4(w[0][0], w[0][1], w[0][2], w[0][3]);
+  tapw[2 * i + 1] = make_float4(w[1][0], w[1][1], w[1][2], w[1][3]);
+  tapb[i] = make_int2(base[0], base[1]);
 }
 
 constexpr int MAX_TOUCH = 4;   // W = 4 nodes per dim touch at most 4 tiles
@@ -420,6 +453,8 @@ struct InterpArgs {
   const int* seg;      // 3D interleaved interp: segment visiting order (B, nseg) or null
   long long nseg;
   int blk;             // 2D pair-parallel interp: the grid is in 2 x 8 cell blocks (fwd_cols_kernel<G0, true>)
+  const float4* tapw;  // 2D pair-parallel interp: tap table (taps2_kernel) or null
+  const int2* tapb;
 };
 
 template <int ND>
@@ -562,17 +597,33 @@ struct Interp2p {
     const int b = frame_of(be, a.nb, g.B);
     float w[2][W];
     int nidx[2][W];
-  #pragma unroll
-    for (int d = 0; d < 2; ++d) {
-      const float x = a.gx[((long long)b * 2 + d) * g.K + k];
-      const int base = (int)floorf(x);
-      const float fx = x - (float)base;
+    if (a.tapw) {
+      // the tap table: first node floor(x) - 1 >= -1 and nodes up to G + 1, so
+      // one conditional add or subtract wraps them
+      const long long i = (long long)b * g.K + k;
+      const float4 w0 = __ldg(a.tapw + 2 * i), w1 = __ldg(a.tapw + 2 * i + 1);
+      const int2 bb = __ldg(a.tapb + i);
+      w[0][0] = w0.x; w[0][1] = w0.y; w[0][2] = w0.z; w[0][3] = w0.w;
+      w[1][0] = w1.x; w[1][1] = w1.y; w[1][2] = w1.z; w[1][3] = w1.w;
   #pragma unroll
       for (int o = 0; o < W; ++o) {
-        const int n = base - (W / 2 - 1) + o;
-        const float wd = mrb::kb_tap(kb, o, fx);
-        w[d][o] = (n & 1) ? -wd : wd;
-        nidx[d][o] = mrb::wrap_i(n, g.G[d]);
+        const int n0 = bb.x + o, n1 = bb.y + o;
+        nidx[0][o] = n0 < 0 ? n0 + g.G[0] : n0 >= g.G[0] ? n0 - g.G[0] : n0;
+        nidx[1][o] = n1 < 0 ? n1 + g.G[1] : n1 >= g.G[1] ? n1 - g.G[1] : n1;
+      }
+    } else {
+  #pragma unroll
+      for (int d = 0; d < 2; ++d) {
+        const float x = a.gx[((long long)b * 2 + d) * g.K + k];
+        const int base = (int)floorf(x);
+        const float fx = x - (float)base;
+  #pragma unroll
+        for (int o = 0; o < W; ++o) {
+          const int n = base - (W / 2 - 1) + o;
+          const float wd = mrb::kb_tap(kb, o, fx);
+          w[d][o] = (n & 1) ? -wd : wd;
+          nidx[d][o] = mrb::wrap_i(n, g.G[d]);
+        }
       }
     }
     // offsets of the tap rows and columns: row-major, or 2 x 8 cell blocks
@@ -883,6 +934,8 @@ struct SpreadArgs {
   float gsign;
   const unsigned* touch;   // per-frame touched-cell bitmaps: grid cells outside them are not stored
   long long twords;
+  const float4* tapw;      // 2D tap table (taps2_kernel) or null: the weights are evaluated inline
+  const int2* tapb;
 };
 
 // a tile's cell pair (cell, cell + 1; cell even) is stored: no bitmap is in use, or
@@ -1030,14 +1083,25 @@ struct SpreadWarp {
     // the next batch's sample index, coordinates, weight and first coil values
     // are loaded into registers while the warp works on the current batch
     constexpr int PF = 4;
+    // 2D with the tap table: the sample's weights and first nodes instead of its coordinates
+    const bool tab = ND == 2 && a.tapw != nullptr;
     int pk = 0;
     float px[ND], pwa = 1.f;
+    float4 pw0 = make_float4(0.f, 0.f, 0.f, 0.f), pw1 = pw0;
+    int2 pb = make_int2(0, 0);
     float2 py[PF];
     auto fetch = [&](int e, int nbat) {
       if (lane < nbat) {
         pk = a.entries[e + lane];
+        if (tab) {
+          const long long i = (long long)b * g.K + pk;
+          pw0 = __ldg(a.tapw + 2 * i);
+          pw1 = __ldg(a.tapw + 2 * i + 1);
+          pb = __ldg(a.tapb + i);
+        } else {
   #pragma unroll
-        for (int d = 0; d < ND; ++d) px[d] = gxp[(long long)d * g.K + pk];
+          for (int d = 0; d < ND; ++d) px[d] = gxp[(long long)d * g.K + pk];
+        }
         if (a.wadj) pwa = a.wadj[(long long)b * g.K + pk];
   #pragma unroll
         for (int cl = 0; cl < PF; ++cl) py[cl] = cl < nc ? yb[(long long)cl * g.K + pk] : make_float2(0.f, 0.f);
@@ -1051,18 +1115,30 @@ struct SpreadWarp {
         float ws = a.gsign;
         if (a.wadj) ws *= pwa;
         int base[3] = {0, 0, 0};
-  #pragma unroll
-        for (int d = 0; d < ND; ++d) {
-          const float x = px[d];
-          base[d] = (int)floorf(x) - 1;
-          const float fx = x - (float)(base[d] + 1);
+        if (tab) {
+          // the table's signed weights; dim 0 times the sample's scale, as below
+          const float t0[4] = {pw0.x, pw0.y, pw0.z, pw0.w}, t1[4] = {pw1.x, pw1.y, pw1.z, pw1.w};
   #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            const int n = base[d] + q;
-            float w = mrb::kb_tap(kb, q, fx);
-            if (n & 1) w = -w;
-            if (d == 0) w *= ws;
-            sw[lane * NW + d * 4 + q] = w;
+            sw[lane * NW + q] = t0[q] * ws;
+            sw[lane * NW + 4 + q] = t1[q];
+          }
+          base[0] = pb.x;
+          base[1] = pb.y;
+        } else {
+  #pragma unroll
+          for (int d = 0; d < ND; ++d) {
+            const float x = px[d];
+            base[d] = (int)floorf(x) - 1;
+            const float fx = x - (float)(base[d] + 1);
+  #pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int n = base[d] + q;
+              float w = mrb::kb_tap(kb, q, fx);
+              if (n & 1) w = -w;
+              if (d == 0) w *= ws;
+              sw[lane * NW + d * 4 + q] = w;
+            }
           }
         }
         // tile-relative first node r = base - o, taken modulo G into [-3, G - 4]:
@@ -2274,7 +2350,7 @@ extern "C" int mrb_plan_destroy(mrb_plan* p) {
                     &p->wadj, &p->grid, &p->tmp, &p->band, &p->tw0, &p->tw1, &p->psf, &p->ones, &p->grid_il,
                     &p->band2, &p->tw2, &p->rowfac,
                     &p->seg_order, &p->touch, &p->grid_adj,
-                    &p->strip_start, &p->strip_entries})
+                    &p->strip_start, &p->strip_entries, &p->tapw, &p->tapb})
     b->release();
   delete p;
   return 0;
@@ -2354,6 +2430,13 @@ extern "C" int mrb_plan_set_points(mrb_plan* p, const float* traj, mrb_stream_t 
   if ((rc = p->gx.ensure(nall * sizeof(float)))) return rc;
   coords_kernel<<<grid_blocks(nall, 256), 256, 0, st>>>(traj, p->gx.as<float>(), g);
   MRB_LAUNCH_CHECK();
+  if (p->nd == 2 && p->W == 4) {
+    if ((rc = p->tapw.ensure(nBK * 2 * sizeof(float4)))) return rc;
+    if ((rc = p->tapb.ensure(nBK * sizeof(int2)))) return rc;
+    taps2_kernel<<<grid_blocks(nBK, 256), 256, 0, st>>>(p->gx.as<float>(), p->tapw.as<float4>(), p->tapb.as<int2>(),
+                                                        g, p->kb);
+    MRB_LAUNCH_CHECK();
+  }
 
   TileGeo tg{};
   tg.T = p->tile;
@@ -2846,6 +2929,8 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     }
     if (p->nd == 2 && p->interp_mode == 1) {
       a.blk = grid_blocked(p) ? 1 : 0;
+      a.tapw = p->tapw.as<float4>();
+      a.tapb = p->tapb.as<int2>();
       const long long nbx = (long long)grid_blocks(p->K, 256) * ((p->C + 1) / 2);
       MRB_REQUIRE(nbx < (1LL << 31) && nb <= 65535, "too many samples for the interp");
       return mrb::launch<Interp2p>(interp2p_kernel, dim3((unsigned)nbx, nb), 0, st, a, g, p->kb);
@@ -2887,6 +2972,8 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     a.touch = masked ? p->touch.as<unsigned>() : nullptr;
     a.twords = p->twords;
     a.grid = adj_grid(p);
+    a.tapw = p->nd == 2 ? p->tapw.as<float4>() : nullptr;
+    a.tapb = p->nd == 2 ? p->tapb.as<int2>() : nullptr;
     const bool blk3t = p->spread_kernel == 2 && p->nd == 3 && tg.T == S3_T;  // shared-staging 3D kernel
     // block-per-tile kernels (the plain block kernel stages tile-relative bases: grid sides >= T + 3)
     const bool blk3 = (p->spread_kernel == 1 || blk3t) && p->nd == 3 && tg.T == S3_T &&
