@@ -816,30 +816,44 @@ struct NCGUpdate {
     const float t = (float)s[S_T];
     const float beta = (float)s[S_BETA];
     const long long stride = (long long)vb.nx * blockDim.x;
+    // one element: its loaded values in, its stores and its term of <g, d> out
+    auto element = [&](long long i, float2 dv, float2 xv, float2 a, float2 b, float2 gv, float Dv) {
+      // x.add_(d * t) (cg.py:205-207)
+      xv.x = __fadd_rn(xv.x, __fmul_rn(dv.x, t));
+      xv.y = __fadd_rn(xv.y, __fmul_rn(dv.y, t));
+      x[i] = xv;
+      if (gr) {
+        a.x = fmaf(t, b.x, a.x);
+        a.y = fmaf(t, b.y, a.y);
+        gr[i] = a;
+      }
+      if (upd_dir) {
+        // d.mul_(beta); d.addcdiv_(g, D, value=-1)  (directions.py:158-161)
+        float nx = __fadd_rn(__fmul_rn(dv.x, beta), -(gv.x / Dv));
+        float ny = __fadd_rn(__fmul_rn(dv.y, beta), -(gv.y / Dv));
+        d[i] = make_float2(nx, ny);
+        if (g_prev) g_prev[i] = gv;
+        acc[0] += (double)(gv.x * nx + gv.y * ny);
+      }
+    };
+    const float2 z2 = make_float2(0.f, 0.f);
     if (ok) {
-      for (long long i = (long long)vb.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        float2 dv = d[i];
-        float2 xv = x[i];
-        // x.add_(d * t) (cg.py:205-207)
-        xv.x = __fadd_rn(xv.x, __fmul_rn(dv.x, t));
-        xv.y = __fadd_rn(xv.y, __fmul_rn(dv.y, t));
-        x[i] = xv;
-        if (gr) {
-          float2 a = gr[i], b = gAd[i];
-          a.x = fmaf(t, b.x, a.x);
-          a.y = fmaf(t, b.y, a.y);
-          gr[i] = a;
-        }
-        if (upd_dir) {
-          float2 gv = g[i];
-          float Dv = diag ? diag[i % ndiag] : 1.f;
-          // d.mul_(beta); d.addcdiv_(g, D, value=-1)  (directions.py:158-161)
-          float nx = __fadd_rn(__fmul_rn(dv.x, beta), -(gv.x / Dv));
-          float ny = __fadd_rn(__fmul_rn(dv.y, beta), -(gv.y / Dv));
-          d[i] = make_float2(nx, ny);
-          if (g_prev) g_prev[i] = gv;
-          acc[0] += (double)(gv.x * nx + gv.y * ny);
-        }
+      // two elements of the grid-stride sequence per pass, all their loads issued
+      // before either is stored (the buffers are distinct): the same values and
+      // summation order as one element per pass
+      long long i = (long long)vb.x * blockDim.x + threadIdx.x;
+      for (; i + stride < n; i += 2 * stride) {
+        const long long j = i + stride;
+        const float2 dv0 = d[i], dv1 = d[j], xv0 = x[i], xv1 = x[j];
+        const float2 a0 = gr ? gr[i] : z2, b0 = gr ? gAd[i] : z2, a1 = gr ? gr[j] : z2, b1 = gr ? gAd[j] : z2;
+        const float2 g0 = upd_dir ? g[i] : z2, g1 = upd_dir ? g[j] : z2;
+        const float D0 = upd_dir && diag ? diag[i % ndiag] : 1.f, D1 = upd_dir && diag ? diag[j % ndiag] : 1.f;
+        element(i, dv0, xv0, a0, b0, g0, D0);
+        element(j, dv1, xv1, a1, b1, g1, D1);
+      }
+      if (i < n) {
+        element(i, d[i], x[i], gr ? gr[i] : z2, gr ? gAd[i] : z2, upd_dir ? g[i] : z2,
+                upd_dir && diag ? diag[i % ndiag] : 1.f);
       }
     }
     block_reduce_finish<1>(vb, acc, partials, ro);
