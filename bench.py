@@ -85,12 +85,14 @@ def history_rel_diff(f_a, f_b):
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of each
-# stage's kernels on the grasp workload, from one `ncu --set full` capture per
-# kernel of `python bench.py --nufft-only` (spread stage = spread_kernel, which
-# stores only the cell pairs inside some support into a grid whose other cells
-# stay zero from a one-time fill; the small split-tile reduction is not included)
-NCU_TRAFFIC = {"grasp": {"pre": 396.30e6, "fft": 1228.03e6, "interp": 433.49e6, "spread": 338.06e6,
-                         "ifft": 1256.29e6, "post": 454.12e6}}
+# stage's kernels on the grasp workload, from ncu captures of
+# `python bench.py --nufft-only` (fft = the forward column pass storing the grid
+# in 2 x 8 cell blocks, interp = the pair-parallel interp reading it, spread =
+# spread_kernel storing whole 32-byte sectors that hold a touched cell into a
+# grid whose other cells stay zero from a one-time fill, post = the inverse row
+# pass; the small split-tile reduction is not included)
+NCU_TRAFFIC = {"grasp": {"pre": 396.30e6, "fft": 1225.29e6, "interp": 344.36e6, "spread": 281.54e6,
+                         "ifft": 1256.29e6, "post": 455.38e6}}
 
 
 def parse():
