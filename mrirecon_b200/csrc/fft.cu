@@ -496,30 +496,39 @@ __global__ void __launch_bounds__(COL_NT) fwd_cols_kernel(const float2* __restri
 
 // forward column pass with a coil-interleaved output (3D x pass, see fft.cuh):
 // a block transforms IL_ROWS (column, coil) pairs, coil fastest, so that each
-// output row is IL_ROWS contiguous values of the (cell, coil) layout; the band
-// is read CT coils at a time per column
+// output row holds runs of contiguous values of the (cell, coil) layout
 constexpr int IL_ROWS = 32;
+
+// A block takes IL_CG coils of its frame (groups of 8): its band reads per coil
+// and row are IL_ROWS / 8 = 4 consecutive columns, one whole 32-byte sector
+// (with all CT coils in one block they were 2 columns, half a sector), and its
+// stores per cell are IL_CG coils, 64 contiguous bytes of the cell's CT.
+template <int CT>
+__host__ __device__ constexpr int il_cg() { return CT < 8 ? CT : 8; }
 
 template <int G0, int CT>
 __global__ void __launch_bounds__(COL_NT, G0 <= 320 ? 2 : 1) fwd_cols_il_kernel(const float2* __restrict__ Tb, float2* __restrict__ out,
                                                              const float2* __restrict__ tw, Geo2 g) {
   constexpr int LD = G0 | 1;
-  constexpr int CB = IL_ROWS / CT;   // columns per block
+  constexpr int CG = il_cg<CT>();    // coils per block
+  constexpr int CB = IL_ROWS / CG;   // columns per block
   extern __shared__ float2 sm[];
   if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
   const int cblocks = (g.G1 + CB - 1) / CB;
-  const int be = blockIdx.x / cblocks;
-  const int k0 = (blockIdx.x - be * cblocks) * CB;
-  const float2* tb = Tb + (long long)be * CT * g.S0 * g.G1;   // (coil, band row, column)
-  float2* ob = out + (long long)be * g.gtot * CT;              // (cell, coil)
+  const int vg = blockIdx.x / cblocks;   // (frame, coil group)
+  const int k0 = (blockIdx.x - vg * cblocks) * CB;
+  const int be = vg / (CT / CG), c0 = (vg - be * (CT / CG)) * CG;
+  const float2* tb = Tb + ((long long)be * CT + c0) * g.S0 * g.G1;   // (coil, band row, column)
+  float2* ob = out + (long long)be * g.gtot * CT + c0;               // (cell, coil)
   auto load0 = [&](int q, int n0) -> float2 {
-    const int j = q / CT, c = q - j * CT;
+    const int j = q / CG, c = q - j * CG;
     const int r = n0 - g.off0;
     if ((unsigned)r >= (unsigned)g.S0 || k0 + j >= g.G1) return make_float2(0.f, 0.f);
     return tb[((long long)c * g.S0 + r) * g.G1 + k0 + j];
   };
   auto store = [&](int q, int n0, float2 v) {
-    if (k0 + q / CT < g.G1) ob[((long long)n0 * g.G1 + k0) * CT + q] = v;
+    const int j = q / CG, c = q - j * CG;
+    if (k0 + j < g.G1) ob[((long long)n0 * g.G1 + k0 + j) * CT + c] = v;
   };
   fft_stages<G0, 0, IL_ROWS, COL_NT, -1, true, false, LD>(sm, tw, load0, store);
 }
@@ -869,10 +878,11 @@ int launch_cols(bool forward, const float2* in, float2* out, const float2* tw, c
 
 template <int G0, int CT>
 int launch_cols_il(const float2* in, float2* out, const float2* tw, const Geo2& g, int nb, cudaStream_t st) {
-  constexpr int CB = IL_ROWS / CT;
+  constexpr int CG = il_cg<CT>();
+  constexpr int CB = IL_ROWS / CG;
   const size_t smem = (size_t)IL_ROWS * (G0 | 1) * sizeof(float2);
   MRB_REQUIRE(smem <= 200 * 1024, "interleaved column pass needs %zu bytes of shared memory", smem);
-  const long long blocks = (long long)nb * ((g.G1 + CB - 1) / CB);
+  const long long blocks = (long long)nb * (CT / CG) * ((g.G1 + CB - 1) / CB);
   MRB_REQUIRE(blocks < (1LL << 31), "too many columns");
   int rc;
   if ((rc = set_smem((const void*)fwd_cols_il_kernel<G0, CT>, smem))) return rc;
