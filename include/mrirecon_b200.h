@@ -142,7 +142,12 @@ int mrb_plan_destroy(mrb_plan* plan);
  *         sample's 4 x 4 taps meet 2 to 6 128-byte lines instead of 4 to 8, and
  *         a warp's stores still fill whole lines.  Same samples; on the GRASP
  *         workload the interp falls from 107 to 82 us and the column pass
- *         gains 3 us. */
+ *         gains 3 us,
+ * key 10 = 2D: the per-warp spread and the pair-parallel interp read each
+ *         sample's first nodes and signed kernel weights from a table that
+ *         set_points builds with the coordinates (1, the default; 40 bytes per
+ *         sample) or evaluate the kernel polynomials per call (0).  Same
+ *         weights bit for bit. */
 int mrb_plan_set_option(mrb_plan* plan, int key, int64_t value);
 
 /* Trajectory (dev, (B, nd, K) float32 radians in [-pi, pi)): float32 grid

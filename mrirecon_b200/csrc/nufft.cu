@@ -55,6 +55,7 @@ struct mrb_plan {
   int grid_mask = 1;       // fused FFT mode: the spread stores only cell pairs inside some support
   int col_interp = 0;      // fused 2D mode: forward column pass and interp in one kernel (option key 8)
   int grid_blk = 1;        // fused 2D mode: the forward grid in 2 x 8 cell blocks (option key 9)
+  int tap_table = 1;       // 2D: spread and interp read the per-sample tap table (option key 10)
   DevBuf strip_start;      // (B * nstrips + 1) per-frame lists of the samples starting in each column strip
   DevBuf strip_entries;    // (B * K) sample indices
   int nstrips = 0;
@@ -2415,6 +2416,10 @@ extern "C" int mrb_plan_set_option(mrb_plan* p, int key, int64_t value) {
       MRB_REQUIRE(value == 0 || value == 1, "blocked forward grid must be 0 or 1");
       p->grid_blk = (int)value;
       return 0;
+    case 10:
+      MRB_REQUIRE(value == 0 || value == 1, "tap table must be 0 or 1");
+      p->tap_table = (int)value;
+      return 0;
     default:
       return mrb::fail(MRB_EINVAL, "unknown option %d", key);
   }
@@ -2929,8 +2934,8 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     }
     if (p->nd == 2 && p->interp_mode == 1) {
       a.blk = grid_blocked(p) ? 1 : 0;
-      a.tapw = p->tapw.as<float4>();
-      a.tapb = p->tapb.as<int2>();
+      a.tapw = p->tap_table ? p->tapw.as<float4>() : nullptr;
+      a.tapb = p->tap_table ? p->tapb.as<int2>() : nullptr;
       const long long nbx = (long long)grid_blocks(p->K, 256) * ((p->C + 1) / 2);
       MRB_REQUIRE(nbx < (1LL << 31) && nb <= 65535, "too many samples for the interp");
       return mrb::launch<Interp2p>(interp2p_kernel, dim3((unsigned)nbx, nb), 0, st, a, g, p->kb);
@@ -2972,8 +2977,8 @@ static int run_stage(mrb_plan* p, int stage, const void* x, void* y, int nb, cud
     a.touch = masked ? p->touch.as<unsigned>() : nullptr;
     a.twords = p->twords;
     a.grid = adj_grid(p);
-    a.tapw = p->nd == 2 ? p->tapw.as<float4>() : nullptr;
-    a.tapb = p->nd == 2 ? p->tapb.as<int2>() : nullptr;
+    a.tapw = p->nd == 2 && p->tap_table ? p->tapw.as<float4>() : nullptr;
+    a.tapb = p->nd == 2 && p->tap_table ? p->tapb.as<int2>() : nullptr;
     const bool blk3t = p->spread_kernel == 2 && p->nd == 3 && tg.T == S3_T;  // shared-staging 3D kernel
     // block-per-tile kernels (the plain block kernel stages tile-relative bases: grid sides >= T + 3)
     const bool blk3 = (p->spread_kernel == 1 || blk3t) && p->nd == 3 && tg.T == S3_T &&

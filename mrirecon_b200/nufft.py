@@ -32,7 +32,7 @@ from .layout import (AxisSpec, plan_image_layout, plan_kspace_layout, plan_image
 from .roles import Roles
 
 OPT_TILE, OPT_COILS_PER_ITEM, OPT_INTERP_MODE, OPT_CHUNK, OPT_FFT_MODE, OPT_INTERLEAVE, OPT_SPREAD_KERNEL, \
-    OPT_GRID_MASK, OPT_COL_INTERP, OPT_GRID_BLOCKS = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9
+    OPT_GRID_MASK, OPT_COL_INTERP, OPT_GRID_BLOCKS, OPT_TAP_TABLE = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10
 FFT_CUFFT, FFT_FUSED = 0, 1
 _DCF_MODES = {"none": 0, "balanced": 1, "standard": 2}
 

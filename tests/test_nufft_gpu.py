@@ -430,6 +430,26 @@ def test_2d_blocked_grid_identical(cuda, S, C, nb, B):
     assert torch.equal(ad.AH(y1), ad.AH(y0))
 
 
+@pytest.mark.parametrize("fft_mode,C,nb,B", [(1, 12, 2, 2), (1, 3, 3, 1), (0, 4, 2, 2), (1, 1, 1, 1)])
+def test_2d_tap_table_identical(cuda, fft_mode, C, nb, B):
+    """2D spread and interp reading the per-sample tap table built by set_points
+    (option key 10 = 1, the default) give the grids and samples of the inline
+    kernel evaluation bit for bit, with and without adjoint density weights."""
+    maps = _rand_c((C, 40, 48), 80, torch.complex64)
+    traj = phantoms.random_traj(B, 2, 1000, seed=81)
+    dcf = torch.rand(B, 1000, generator=torch.Generator().manual_seed(82)) + 0.5
+    x = _rand_c((nb, 1, 40, 48), 83, torch.complex64).to(cuda)
+    for w in (None, dcf):
+        ad = _adapter(maps, traj, dcf=w, fft_mode=fft_mode)
+        y1 = ad.A(x)
+        x1 = ad.AH(y1)
+        ad.plan.set_option(10, 0)
+        assert torch.equal(ad.A(x), y1)
+        assert torch.equal(ad.AH(y1), x1)
+        ad.plan.set_option(10, 1)
+        assert torch.equal(ad.A(x), y1)
+
+
 @pytest.mark.parametrize("S,C,nb,B", [((40, 48), 12, 2, 2), ((40, 48), 8, 3, 1), ((32, 32), 16, 1, 1),
                                       ((48, 40), 4, 4, 2), ((320, 160), 4, 1, 1), ((40, 48), 5, 2, 1)])
 def test_2d_interleaved_grid_interp_identical(cuda, S, C, nb, B):
