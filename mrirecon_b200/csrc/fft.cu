@@ -372,6 +372,7 @@ struct Geo2 {
   int S0, S1, G0, G1, off0, off1, C;
   long long stot, gtot;
   const double* skip;   // when non-null and non-zero the kernels return at once
+  int nvol;             // volumes of the pass (the forward column pass: nb x C)
 };
 
 // forward row pass: T[row][:] = FFT_G1(pad(x[be][r][:] * S_c * deapod * sign)),
@@ -434,6 +435,18 @@ __global__ void __launch_bounds__(ROW_NT, FwdRows<G1>::MINB) fwd_rows_kernel(con
 // to 6 128-byte lines instead of 4 to 8.  The last stage's stores of a warp
 // cover rows 2m and 2m + 1 of 16 columns: whole blocks, as whole rows' lines
 // in the row-major layout.
+// 16-byte asynchronous copy global -> shared (completes at cp_async_wait_all)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Forward column pass: a block transforms two column tiles (COLS columns of a
+// volume each, tiles 2 x and 2 x + 1 of the pass): the second tile's band rows
+// are copied into shared memory (cp.async, S0 x COLS values after the exchange
+// buffer) while the first is transformed, so its first stage reads them there
+// instead of waiting for global loads.
 template <int G0, bool BLK = false>
 struct FwdCols {
   static constexpr int NT = COL_NT, MINB = (G0 <= 256 ? 3 : 2);
@@ -445,51 +458,73 @@ struct FwdCols {
     extern __shared__ float2 sm[];
     if (g.skip != nullptr && *g.skip != 0.0) return;   // solve already finished
     const int cblocks = (g.G1 + COLS - 1) / COLS;
-    const int vol = vb.x / cblocks;
-    const int k0 = (vb.x - vol * cblocks) * COLS;
+    const long long ntile = (long long)g.nvol * cblocks;
+    const long long t0 = 2LL * vb.x, t1 = t0 + 1;
+    const bool has1 = t1 < ntile;
     // 32-bit offsets inside one volume (at most 1024^3 = 2^30 cells for the compiled lengths)
     const int G1 = g.G1;
-    const bool full = k0 + COLS <= G1;
-    const float2* tv = Tb + (long long)vol * g.S0 * G1 + k0;
-    float2* gv = grid + (long long)vol * g.gtot + k0;
-    auto load0 = [&](int q, int n0) -> float2 {
-      const int r = n0 - g.off0;
-      if ((unsigned)r >= (unsigned)g.S0 || (!full && k0 + q >= G1)) return make_float2(0.f, 0.f);
-      return tv[r * G1 + q];
-    };
-    // BLK: 4 x 4 cell blocks; a thread's column k0 + q is fixed, its rows n0 = j + r P
-    // share n0 % 4 (P is a multiple of 4), so the address is a per-thread base plus
-    // a multiple of 4 G1 per r
-    float2* gb = grid + (long long)vol * g.gtot + ((k0 >> 3) << 4);
-    auto store = [&](int q, int n0, float2 v) {
-      if (full || k0 + q < G1) gv[n0 * G1 + q] = v;
-    };
-    // row n0 = j + rP of the last stage (P even): block row j / 2 + rP / 2, row in block j % 2
-    auto store_blk = [&](int q, int j, int rP, float2 v) {
-      if (full || k0 + q < G1) {
-        const int c = (k0 & 7) + q;   // column k0 + q = 8 (k0 / 8) + c
-        gb[((j >> 1) + (rP >> 1)) * (2 * G1) + (j & 1) * 8 + ((c >> 3) << 4) + (c & 7)] = v;
+    float2* stg = sm + COLS * LD;   // the second tile's band rows, (S0, COLS)
+    if (has1) {
+      const int vol = (int)(t1 / cblocks);
+      const int k0 = (int)(t1 - (long long)vol * cblocks) * COLS;
+      const float2* tv = Tb + (long long)vol * g.S0 * G1 + k0;
+      constexpr int HC = COLS / 2;   // 16-byte pieces per band row (COLS is even)
+      for (int c = threadIdx.x; c < g.S0 * HC; c += COL_NT) {
+        const int r = c / HC, col = 2 * (c - r * HC);
+        if (k0 + col < G1) cp_async16(stg + r * COLS + col, tv + r * G1 + col);
       }
-    };
-    auto go = [&](auto st) {
-      if constexpr (radix_at(G0, 0) == 8) {
-        if (centred_half<G0>(g.S0, g.off0)) {
-          fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD, false, true>(sm, tw, load0, st);
-          return;
+    }
+    auto tile = [&](long long t, bool staged) {
+      const int vol = (int)(t / cblocks);
+      const int k0 = (int)(t - (long long)vol * cblocks) * COLS;
+      const bool full = k0 + COLS <= G1;
+      const float2* tv = Tb + (long long)vol * g.S0 * G1 + k0;
+      float2* gv = grid + (long long)vol * g.gtot + k0;
+      auto load0 = [&](int q, int n0) -> float2 {
+        const int r = n0 - g.off0;
+        if ((unsigned)r >= (unsigned)g.S0 || (!full && k0 + q >= G1)) return make_float2(0.f, 0.f);
+        return staged ? stg[r * COLS + q] : tv[r * G1 + q];
+      };
+      // BLK: 2 x 8 cell blocks; a thread's column k0 + q is fixed and its rows of the
+      // last stage are n0 = j + r P (P even), so the address is a per-thread base plus
+      // a multiple of 2 G1 per r
+      float2* gb = grid + (long long)vol * g.gtot + ((k0 >> 3) << 4);
+      auto store = [&](int q, int n0, float2 v) {
+        if (full || k0 + q < G1) gv[n0 * G1 + q] = v;
+      };
+      // row n0 = j + rP of the last stage (P even): block row j / 2 + rP / 2, row in block j % 2
+      auto store_blk = [&](int q, int j, int rP, float2 v) {
+        if (full || k0 + q < G1) {
+          const int c = (k0 & 7) + q;   // column k0 + q = 8 (k0 / 8) + c
+          gb[((j >> 1) + (rP >> 1)) * (2 * G1) + (j & 1) * 8 + ((c >> 3) << 4) + (c & 7)] = v;
         }
+      };
+      auto go = [&](auto st) {
+        if constexpr (radix_at(G0, 0) == 8) {
+          if (centred_half<G0>(g.S0, g.off0)) {
+            fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD, false, true>(sm, tw, load0, st);
+            return;
+          }
+        }
+        fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, st);
+      };
+      if constexpr (BLK) {
+        static_assert(span_at(G0, n_stages(G0) - 1) % 2 == 0, "the last stage's span must be even");
+        go(store_blk);
+      } else {
+        go(store);
       }
-      fft_stages<G0, 0, COLS, COL_NT, -1, true, false, LD>(sm, tw, load0, st);
     };
-    if constexpr (BLK) {
-      static_assert(span_at(G0, n_stages(G0) - 1) % 2 == 0, "the last stage's span must be even");
-      go(store_blk);
-    } else {
-      go(store);
+    tile(t0, false);
+    if (has1) {
+      cp_async_wait_all();
+      __syncthreads();   // every thread's copies landed (the last stage ended with a barrier)
+      tile(t1, true);
     }
   }
 };
 template <int G0, bool BLK>
-__global__ void __launch_bounds__(COL_NT) fwd_cols_kernel(const float2* __restrict__ Tb,
+__global__ void __launch_bounds__(COL_NT, FwdCols<G0, BLK>::MINB) fwd_cols_kernel(const float2* __restrict__ Tb,
     float2* __restrict__ grid, const float2* __restrict__ tw, Geo2 g) {
   FwdCols<G0, BLK>::run(hw_block(), Tb, grid, tw, g);
 }
@@ -817,7 +852,7 @@ __global__ void __launch_bounds__(AdjRows<G1>::NT, AdjRows<G1>::MINB) adj_rows_k
 }
 
 Geo2 make_geo2(int S0, int S1, int G0, int G1, int C, const double* skip) {
-  return Geo2{S0, S1, G0, G1, G0 / 2 - S0 / 2, G1 / 2 - S1 / 2, C, (long long)S0 * S1, (long long)G0 * G1, skip};
+  return Geo2{S0, S1, G0, G1, G0 / 2 - S0 / 2, G1 / 2 - S1 / 2, C, (long long)S0 * S1, (long long)G0 * G1, skip, 0};
 }
 
 int set_smem(const void* fn, size_t bytes) {
@@ -862,15 +897,22 @@ int launch_cols(bool forward, const float2* in, float2* out, const float2* tw, c
   const long long blocks = (long long)nb * g.C * ((g.G1 + COLS - 1) / COLS);
   MRB_REQUIRE(blocks < (1LL << 31), "too many columns");
   int rc;
-  if (forward && blocked) {
-    MRB_REQUIRE(G0 % 2 == 0 && g.G1 % 8 == 0, "2 x 8 cell blocks need G0 even and G1 divisible by 8");
-    if ((rc = set_smem((const void*)fwd_cols_kernel<G0, true>, smem))) return rc;
-    return mrb::launch<FwdCols<G0, true>>(fwd_cols_kernel<G0, true>, dim3((unsigned)blocks), smem, st, in, out, tw,
-                                          g);
-  }
   if (forward) {
-    if ((rc = set_smem((const void*)fwd_cols_kernel<G0, false>, smem))) return rc;
-    return mrb::launch<FwdCols<G0>>(fwd_cols_kernel<G0, false>, dim3((unsigned)blocks), smem, st, in, out, tw, g);
+    // two column tiles per block, the second one's band rows staged in shared memory
+    Geo2 gf = g;
+    gf.nvol = nb * g.C;
+    const size_t smem_f = smem + (size_t)g.S0 * COLS * sizeof(float2);
+    const long long fblocks = (blocks + 1) / 2;
+    MRB_REQUIRE(g.G1 % 2 == 0, "the forward column pass needs an even row length");
+    if (blocked) {
+      MRB_REQUIRE(G0 % 2 == 0 && g.G1 % 8 == 0, "2 x 8 cell blocks need G0 even and G1 divisible by 8");
+      if ((rc = set_smem((const void*)fwd_cols_kernel<G0, true>, smem_f))) return rc;
+      return mrb::launch<FwdCols<G0, true>>(fwd_cols_kernel<G0, true>, dim3((unsigned)fblocks), smem_f, st, in, out,
+                                            tw, gf);
+    }
+    if ((rc = set_smem((const void*)fwd_cols_kernel<G0, false>, smem_f))) return rc;
+    return mrb::launch<FwdCols<G0>>(fwd_cols_kernel<G0, false>, dim3((unsigned)fblocks), smem_f, st, in, out, tw,
+                                    gf);
   }
   if ((rc = set_smem((const void*)adj_cols_kernel<G0>, smem))) return rc;
   return mrb::launch<AdjCols<G0>>(adj_cols_kernel<G0>, dim3((unsigned)blocks), smem, st, in, out, tw, g);
